@@ -1,0 +1,814 @@
+// C ABI of libawpb200: the re-entrant context API and the reference-named
+// launchers.  See include/awp_b200.h for the contract of every entry point.
+#include <cuda_runtime.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <algorithm>
+#include <climits>
+#include <map>
+#include <vector>
+
+#include "../../include/awp_b200.h"
+#include "awp_common.h"
+#include "awp_host.h"
+#include "awp_kernels.cuh"
+
+namespace {
+
+thread_local char g_errmsg[512] = "";
+
+int set_error(int status, const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_errmsg, sizeof(g_errmsg), fmt, ap);
+  va_end(ap);
+  return status;
+}
+
+#define CU_TRY(call)                                                              \
+  do {                                                                            \
+    cudaError_t e_ = (call);                                                      \
+    if (e_ != cudaSuccess)                                                        \
+      return set_error(AWP_ERR_CUDA, "%s:%d %s: %s", __FILE__, __LINE__, #call,   \
+                       cudaGetErrorString(e_));                                   \
+  } while (0)
+
+inline int round_up(int n, int m) { return (n + m - 1) / m * m; }
+
+}  // namespace
+
+// ===========================================================================
+// Context
+// ===========================================================================
+struct awp_ctx {
+  awp_params p;
+  AwpGeom g;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  float* f[AWP_NFIELDS] = {};
+  float *dcrjx = nullptr, *dcrjy = nullptr, *dcrjz = nullptr, *lam_mu = nullptr;
+  AwpTexture tex{};
+  float coeff[16] = {}, tau8[8] = {}, w8[8] = {};
+  float taumax = 0.f, taumin = 0.f;
+  float qthr = 0.f;
+  float c1 = 9.0 / 8.0, c2 = -1.0 / 24.0;
+  float dth = 0.f, dh1 = 0.f;
+  int xls = 0, xre = 0, yls = 0, yre = 0;  // stress / output window (pmcl3d.c:573-631)
+  bool media_ready = false;
+  bool elastic = false;  // Q^-1 == 0 everywhere and memory variables zero
+  // sources
+  int nsrc = 0, ncell = 0, src_stride = 0;
+  int *d_cell_pos = nullptr, *d_cell_first = nullptr, *d_order = nullptr;
+  float* d_src[6] = {};
+  float* d_mom = nullptr;
+  double* d_filt = nullptr;
+  int filtorder = 0;
+  double filt_b[AWP_MAXFILT] = {}, filt_a[AWP_MAXFILT] = {};
+  // plasticity
+  bool plast_ready = false;
+  PlastParams pp{};
+  unsigned char* d_neta_mult = nullptr;
+  unsigned int* d_flag = nullptr;
+  long long cur_step = 0;
+  bool initial_src_done = false;
+  long long dev_bytes = 0;
+  long long launches = 0;
+  // phase timing
+  bool profile = false;
+  struct PhaseEv {
+    int phase;
+    cudaEvent_t a, b;
+  };
+  std::vector<PhaseEv> ev_used, ev_free;
+};
+
+namespace {
+
+int ctx_alloc(awp_ctx* c, void** p, size_t bytes) {
+  cudaError_t e = cudaMalloc(p, bytes);
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    return set_error(AWP_ERR_NOMEM, "cudaMalloc(%zu): %s", bytes, cudaGetErrorString(e));
+  }
+  c->dev_bytes += (long long)bytes;
+  return AWP_OK;
+}
+
+bool field_needed(const awp_params& p, int f) {
+  if (f >= AWP_SIGMA2 && f <= AWP_YLDFAC) return p.nve == 3;
+  return true;  // neta is always allocated (velbuffer reads it, pmcl3d.c:1218)
+}
+
+StrArgs make_str_args(awp_ctx* c) {
+  StrArgs a;
+  memset(&a, 0, sizeof(a));
+  float** f = c->f;
+  a.xx = f[AWP_XX]; a.yy = f[AWP_YY]; a.zz = f[AWP_ZZ];
+  a.xy = f[AWP_XY]; a.xz = f[AWP_XZ]; a.yz = f[AWP_YZ];
+  a.r1 = f[AWP_R1]; a.r2 = f[AWP_R2]; a.r3 = f[AWP_R3];
+  a.r4 = f[AWP_R4]; a.r5 = f[AWP_R5]; a.r6 = f[AWP_R6];
+  a.u1 = f[AWP_U1]; a.v1 = f[AWP_V1]; a.w1 = f[AWP_W1];
+  a.lam = f[AWP_LAM]; a.mu = f[AWP_MU]; a.qp = f[AWP_QP]; a.qs = f[AWP_QS];
+  a.dcrjx = c->dcrjx; a.dcrjy = c->dcrjy; a.dcrjz = c->dcrjz; a.lam_mu = c->lam_mu;
+  a.tex = c->tex;
+  memcpy(a.coeff, c->coeff, sizeof(a.coeff));
+  a.slice = c->g.slice;
+  a.yline = c->g.yline;
+  a.lam_mu_ld = (int)c->g.ny_pad();
+  a.i0 = c->xls; a.i1 = c->xre; a.j0 = c->yls; a.j1 = c->yre;
+  a.k0 = AWP_ALIGN + 3;
+  a.k1 = c->g.top();
+  a.fs = 1;
+  a.ktop = c->g.top();
+  a.gx_lim = c->p.nx + AWP_NGSL + 1;                      // g_i < NX, rankx = 0
+  a.gy_min = (c->p.npc == 2) ? INT_MIN : AWP_NGSL + 3;     // g_j > 1 || NPC == 2
+  a.dth = c->dth; a.dh1 = c->dh1; a.dt = c->p.dt; a.c1 = c->c1; a.c2 = c->c2;
+  a.qthr = c->qthr;
+  return a;
+}
+
+int launch_sources(awp_ctx* c, int tidx) {
+  if (c->ncell == 0) return AWP_OK;
+  if (c->p.ifault == 5) {
+    KinSrcArgs a;
+    memset(&a, 0, sizeof(a));
+    a.xx = c->f[AWP_XX]; a.yy = c->f[AWP_YY]; a.zz = c->f[AWP_ZZ];
+    a.xy = c->f[AWP_XY]; a.yz = c->f[AWP_YZ]; a.xz = c->f[AWP_XZ];
+    a.mu = c->f[AWP_MU];
+    a.cell_pos = c->d_cell_pos; a.cell_first = c->d_cell_first; a.order = c->d_order;
+    a.axx = c->d_src[0]; a.ayy = c->d_src[1]; a.azz = c->d_src[2];
+    a.axz = c->d_src[3]; a.ayz = c->d_src[4]; a.axy = c->d_src[5];
+    a.mom = c->d_mom;
+    a.filt_state = c->d_filt;
+    a.filtorder = c->filtorder;
+    memcpy(a.filt_b, c->filt_b, sizeof(a.filt_b));
+    memcpy(a.filt_a, c->filt_a, sizeof(a.filt_a));
+    a.ncell = c->ncell;
+    a.step = tidx;
+    a.dt = c->p.dt;
+    a.vtst = (float)c->p.dt / (c->p.dh * c->p.dh * c->p.dh);
+    CU_TRY(awp_launch_addkinsrc(a, c->stream));
+    return AWP_OK;
+  }
+  SrcArgs a;
+  memset(&a, 0, sizeof(a));
+  a.xx = c->f[AWP_XX]; a.yy = c->f[AWP_YY]; a.zz = c->f[AWP_ZZ];
+  a.xy = c->f[AWP_XY]; a.yz = c->f[AWP_YZ]; a.xz = c->f[AWP_XZ];
+  a.cell_pos = c->d_cell_pos; a.cell_first = c->d_cell_first; a.order = c->d_order;
+  a.axx = c->d_src[0]; a.ayy = c->d_src[1]; a.azz = c->d_src[2];
+  a.axz = c->d_src[3]; a.ayz = c->d_src[4]; a.axy = c->d_src[5];
+  a.ncell = c->ncell;
+  a.stride = c->src_stride;
+  a.tidx = tidx;
+  a.vtst = (float)c->p.dt / (c->p.dh * c->p.dh * c->p.dh);
+  CU_TRY(awp_launch_addsrc(a, c->stream));
+  return AWP_OK;
+}
+
+int launch_plasticity(awp_ctx* c) {
+  // Yield factor over the union of the five strip launches of pmcl3d.c:2121-2181
+  // (xlsp..xrep x ylsp..yrep at one rank); neta counts each strip visit.
+  PlastCalcArgs a;
+  memset(&a, 0, sizeof(a));
+  float** f = c->f;
+  a.xx = f[AWP_XX]; a.yy = f[AWP_YY]; a.zz = f[AWP_ZZ];
+  a.xy = f[AWP_XY]; a.xz = f[AWP_XZ]; a.yz = f[AWP_YZ];
+  a.mu = f[AWP_MU]; a.d1 = f[AWP_D1]; a.sigma2 = f[AWP_SIGMA2];
+  a.cohes = f[AWP_COHES]; a.phi = f[AWP_PHI];
+  a.yldfac = f[AWP_YLDFAC]; a.neta = f[AWP_NETA];
+  a.neta_mult = c->d_neta_mult;
+  a.neta_ld = (int)c->g.ny_pad();
+  a.p = c->pp;
+  a.slice = c->g.slice; a.yline = c->g.yline;
+  a.i0 = c->xls; a.i1 = c->xre; a.j0 = c->yls; a.j1 = c->yre;
+  a.k0 = AWP_ALIGN;
+  a.k1 = AWP_ALIGN + round_up(c->g.nzt, 4) - 1;
+  CU_TRY(awp_launch_plast_calc(a, c->stream));
+  PlastAppArgs b;
+  memset(&b, 0, sizeof(b));
+  b.xx = f[AWP_XX]; b.yy = f[AWP_YY]; b.zz = f[AWP_ZZ];
+  b.xy = f[AWP_XY]; b.xz = f[AWP_XZ]; b.yz = f[AWP_YZ];
+  b.mu = f[AWP_MU]; b.sigma2 = f[AWP_SIGMA2]; b.yldfac = f[AWP_YLDFAC];
+  b.p = c->pp;
+  b.slice = c->g.slice; b.yline = c->g.yline;
+  b.i0 = c->xls; b.i1 = c->xre; b.j0 = c->yls;
+  b.j1 = c->yls + round_up(c->yre - c->yls + 1, 2) - 1;  // grid rounds j up (kernel.cu:1451)
+  b.k0 = AWP_ALIGN;
+  b.k1 = AWP_ALIGN + round_up(c->g.nzt, 4) - 1;
+  CU_TRY(awp_launch_plast_app(b, c->stream));
+  return AWP_OK;
+}
+
+struct PhaseScope {
+  awp_ctx* c;
+  awp_ctx::PhaseEv ev{};
+  bool on;
+  PhaseScope(awp_ctx* c_, int phase) : c(c_), on(c_->profile) {
+    if (!on) return;
+    if (c->ev_free.empty()) {
+      awp_ctx::PhaseEv e{};
+      cudaEventCreate(&e.a);
+      cudaEventCreate(&e.b);
+      c->ev_free.push_back(e);
+    }
+    ev = c->ev_free.back();
+    c->ev_free.pop_back();
+    ev.phase = phase;
+    cudaEventRecord(ev.a, c->stream);
+  }
+  ~PhaseScope() {
+    if (!on) return;
+    cudaEventRecord(ev.b, c->stream);
+    c->ev_used.push_back(ev);
+  }
+};
+
+int one_step(awp_ctx* c) {
+  float** f = c->f;
+  if (c->cur_step == 0 && !c->initial_src_done) {
+    // step-1 source sample is added before the loop (pmcl3d.c:1175-1187)
+    if (c->p.ifault < 4) {
+      int s = launch_sources(c, 0);
+      if (s) return s;
+      if (c->ncell) c->launches++;
+    }
+    c->initial_src_done = true;
+  }
+  c->cur_step += 1;
+  VelArgs v;
+  v.u1 = f[AWP_U1]; v.v1 = f[AWP_V1]; v.w1 = f[AWP_W1];
+  v.xx = f[AWP_XX]; v.yy = f[AWP_YY]; v.zz = f[AWP_ZZ];
+  v.xy = f[AWP_XY]; v.xz = f[AWP_XZ]; v.yz = f[AWP_YZ];
+  v.dcrjx = c->dcrjx; v.dcrjy = c->dcrjy; v.dcrjz = c->dcrjz; v.d1 = f[AWP_D1];
+  v.slice = c->g.slice; v.yline = c->g.yline;
+  v.i0 = 2 + AWP_NGSL; v.i1 = c->g.nxt + AWP_NGSL + 1;          // xvs..xve
+  v.j0 = 2 + AWP_NGSL; v.j1 = 2 + AWP_NGSL + round_up(c->g.nyt, 2) - 1;
+  v.k0 = AWP_ALIGN; v.k1 = AWP_ALIGN + round_up(c->g.nzt, 4) - 1;
+  v.dth = c->dth; v.c1 = c->c1; v.c2 = c->c2;
+  {
+    PhaseScope ps(c, 0);
+    CU_TRY(awp_launch_velocity(v, c->stream));
+    c->launches++;
+  }
+  {
+    PhaseScope ps(c, 1);
+    StrArgs s = make_str_args(c);
+    CU_TRY(awp_launch_stress(s, c->elastic, c->stream));
+    c->launches++;
+  }
+  if ((c->p.ifault < 4 && c->cur_step < c->p.nst) || c->p.ifault == 5) {
+    PhaseScope ps(c, 2);
+    int st = launch_sources(c, (int)c->cur_step);
+    if (st) return st;
+    if (c->ncell) c->launches++;
+  }
+  if (c->p.nve == 3) {
+    PhaseScope ps(c, 3);
+    int st = launch_plasticity(c);
+    if (st) return st;
+    c->launches += 2;
+  }
+  FstrArgs fs;
+  fs.zz = f[AWP_ZZ]; fs.xz = f[AWP_XZ]; fs.yz = f[AWP_YZ];
+  fs.slice = c->g.slice; fs.yline = c->g.yline; fs.ktop = c->g.top();
+  fs.i0 = c->xls; fs.i1 = c->xre;
+  fs.j0 = c->yls; fs.j1 = c->yls + round_up(c->yre - c->yls + 1, 2) - 1;
+  {
+    PhaseScope ps(c, 4);
+    CU_TRY(awp_launch_fstr(fs, c->stream));
+    c->launches++;
+  }
+  return AWP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void awp_params_default(awp_params* p) {
+  memset(p, 0, sizeof(*p));
+  p->nx = 256; p->ny = 256; p->nz = 1024;
+  p->dh = 200.0f; p->dt = 0.01f;
+  p->arbc = 0.92f; p->npc = 0; p->nd = 20;
+  p->nve = 1;
+  p->fac = 0.005f; p->q0 = 5.0f; p->ex = 0.0f; p->fp = 2.5f;
+  p->socalq = 1;
+  p->ifault = 1;
+  p->nst = 91;
+  p->read_step = 91;
+}
+
+const char* awp_status_string(int status) {
+  switch (status) {
+    case AWP_OK: return "ok";
+    case AWP_ERR_ARG: return "invalid argument";
+    case AWP_ERR_CUDA: return "CUDA error";
+    case AWP_ERR_STATE: return "call out of order";
+    case AWP_ERR_IO: return "I/O error";
+    case AWP_ERR_NOMEM: return "out of memory";
+    case AWP_ERR_NUMERIC: return "non-finite wavefield";
+    case AWP_ERR_UNSUPPORTED: return "unsupported option";
+  }
+  return "unknown status";
+}
+
+const char* awp_last_error(void) { return g_errmsg; }
+
+int awp_ctx_destroy(awp_ctx* c) {
+  if (!c) return AWP_OK;
+  for (int i = 0; i < AWP_NFIELDS; ++i) cudaFree(c->f[i]);
+  cudaFree(c->dcrjx); cudaFree(c->dcrjy); cudaFree(c->dcrjz); cudaFree(c->lam_mu);
+  cudaFree(c->d_cell_pos); cudaFree(c->d_cell_first); cudaFree(c->d_order);
+  for (int i = 0; i < 6; ++i) cudaFree(c->d_src[i]);
+  cudaFree(c->d_mom); cudaFree(c->d_filt); cudaFree(c->d_neta_mult); cudaFree(c->d_flag);
+  for (auto& e : c->ev_used) { cudaEventDestroy(e.a); cudaEventDestroy(e.b); }
+  for (auto& e : c->ev_free) { cudaEventDestroy(e.a); cudaEventDestroy(e.b); }
+  if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return AWP_OK;
+}
+
+int awp_ctx_create(const awp_params* p, awp_ctx** out) {
+  if (!p || !out) return set_error(AWP_ERR_ARG, "null argument");
+  *out = nullptr;
+  if (p->nx < 4 || p->ny < 4 || p->nz < 8)
+    return set_error(AWP_ERR_ARG, "grid %dx%dx%d too small", p->nx, p->ny, p->nz);
+  if (p->nz % 4 != 0)
+    return set_error(AWP_ERR_ARG, "NZ=%d is not divisible by 4 (pmcl3d.c:380-391)", p->nz);
+  if (!(p->dh > 0) || !(p->dt > 0)) return set_error(AWP_ERR_ARG, "DH and DT must be > 0");
+  if (p->nve != 1 && p->nve != 3)
+    return set_error(AWP_ERR_UNSUPPORTED,
+                     "NVE=%d: the time loop runs only for NVE 1 or 3 (pmcl3d.c:1624)", p->nve);
+  if (p->npc != 0 && p->npc != 2)
+    return set_error(AWP_ERR_UNSUPPORTED, "NPC=%d (only 0 and 2 run the loop)", p->npc);
+  if (p->ifault != 1 && p->ifault != 5 && p->ifault != 0)
+    return set_error(AWP_ERR_UNSUPPORTED, "IFAULT=%d", p->ifault);
+  const long long cells = (long long)(p->nx + 20) * (p->ny + 20) * (p->nz + 64);
+  if (cells >= (1LL << 31))
+    return set_error(AWP_ERR_ARG, "padded grid of %lld cells exceeds the 32-bit index range", cells);
+
+  awp_ctx* c = new awp_ctx();
+  c->p = *p;
+  c->g = awp_make_geom(p->nx, p->ny, p->nz);
+  c->xls = 2 + AWP_NGSL;
+  c->xre = p->nx + AWP_NGSL + 1;
+  c->yls = 2 + AWP_NGSL;
+  c->yre = p->ny + AWP_NGSL + 1;
+  c->dth = p->dt / p->dh;
+  c->dh1 = 1.0 / p->dh;
+  c->qthr = awp::qf_threshold();
+  int st;
+  cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    delete c;
+    return set_error(AWP_ERR_CUDA, "cudaStreamCreate: %s", cudaGetErrorString(e));
+  }
+  c->own_stream = true;
+  const size_t fbytes = sizeof(float) * (size_t)c->g.cells_pad();
+  for (int i = 0; i < AWP_NFIELDS; ++i) {
+    if (!field_needed(*p, i)) continue;
+    if ((st = ctx_alloc(c, (void**)&c->f[i], fbytes))) goto fail;
+    if (cudaMemsetAsync(c->f[i], 0, fbytes, c->stream) != cudaSuccess) {
+      st = set_error(AWP_ERR_CUDA, "memset");
+      goto fail;
+    }
+  }
+  if (p->nve == 3) {
+    // yldfac starts at 1 (pmcl3d.c:842-849)
+    if (awp_launch_fill(c->f[AWP_YLDFAC], 1.0f, c->g.cells_pad(), c->stream) != cudaSuccess) {
+      st = set_error(AWP_ERR_CUDA, "fill");
+      goto fail;
+    }
+  }
+  {
+    const int nxp = (int)c->g.nx_pad(), nyp = (int)c->g.ny_pad(), nzp = (int)c->g.nz_pad();
+    std::vector<float> cx(nxp, 1.0f), cy(nyp, 1.0f), cz(nzp, 1.0f);
+    awp::inicrj(p->arbc, p->nx, p->ny, p->nz, p->nx, p->ny, p->nd, 1, p->npc, cx.data(),
+                cy.data(), cz.data());
+    if ((st = ctx_alloc(c, (void**)&c->dcrjx, nxp * sizeof(float)))) goto fail;
+    if ((st = ctx_alloc(c, (void**)&c->dcrjy, nyp * sizeof(float)))) goto fail;
+    if ((st = ctx_alloc(c, (void**)&c->dcrjz, nzp * sizeof(float)))) goto fail;
+    if ((st = ctx_alloc(c, (void**)&c->lam_mu, (size_t)nxp * nyp * sizeof(float)))) goto fail;
+    if (cudaMemcpy(c->dcrjx, cx.data(), nxp * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(c->dcrjy, cy.data(), nyp * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(c->dcrjz, cz.data(), nzp * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemsetAsync(c->lam_mu, 0, (size_t)nxp * nyp * 4, c->stream) != cudaSuccess) {
+      st = set_error(AWP_ERR_CUDA, "sponge upload");
+      goto fail;
+    }
+    if (!awp::tau_range(p->ex, p->fac, &c->taumax, &c->taumin)) {
+      st = set_error(AWP_ERR_UNSUPPORTED, "EX=%g >= 0.95 has no relaxation-time range", p->ex);
+      goto fail;
+    }
+    awp::tausub(c->taumin, c->taumax, c->tau8);
+    awp::weights_sub(p->ex, p->fac, c->w8, c->coeff);
+    awp::texture_tables(c->tau8, c->w8, p->dt, &c->tex);
+    c->tex.xls = c->xls;
+    c->tex.yls = c->yls;
+    c->tex.ny = c->yre - c->yls + 1;
+    c->tex.nzt = p->nz;
+  }
+  if ((st = ctx_alloc(c, (void**)&c->d_flag, sizeof(unsigned int)))) goto fail;
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess) {
+    st = set_error(AWP_ERR_CUDA, "initialisation");
+    goto fail;
+  }
+  *out = c;
+  return AWP_OK;
+fail:
+  awp_ctx_destroy(c);
+  return st;
+}
+
+int awp_set_stream(awp_ctx* c, void* s) {
+  if (!c) return set_error(AWP_ERR_ARG, "null context");
+  if (c->own_stream && c->stream) {
+    cudaStreamSynchronize(c->stream);
+    cudaStreamDestroy(c->stream);
+  }
+  c->own_stream = false;
+  c->stream = (cudaStream_t)s;
+  if (!s) {
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
+      return set_error(AWP_ERR_CUDA, "cudaStreamCreate");
+    c->own_stream = true;
+  }
+  return AWP_OK;
+}
+
+int awp_padded_dims(const awp_ctx* c, long long dims[3]) {
+  if (!c || !dims) return set_error(AWP_ERR_ARG, "null argument");
+  dims[0] = c->g.nx_pad();
+  dims[1] = c->g.ny_pad();
+  dims[2] = c->g.nz_pad();
+  return AWP_OK;
+}
+
+static int upload_media_impl(awp_ctx* c, int nvar, const float* media, bool device) {
+  if (!c || !media) return set_error(AWP_ERR_ARG, "null argument");
+  if (nvar != 3 && nvar != 5 && nvar != 8)
+    return set_error(AWP_ERR_ARG, "NVAR=%d (mesh.c:122 reads 3, 5 or 8)", nvar);
+  const size_t n = (size_t)c->p.nx * c->p.ny * c->p.nz * nvar;
+  const float* dmedia = media;
+  float* tmp = nullptr;
+  if (!device) {
+    CU_TRY(cudaMallocAsync((void**)&tmp, n * sizeof(float), c->stream));
+    CU_TRY(cudaMemcpyAsync(tmp, media, n * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+    dmedia = tmp;
+  }
+  MediaArgs a;
+  memset(&a, 0, sizeof(a));
+  a.media = dmedia;
+  a.d1 = c->f[AWP_D1]; a.mu = c->f[AWP_MU]; a.lam = c->f[AWP_LAM];
+  a.qp = c->f[AWP_QP]; a.qs = c->f[AWP_QS];
+  memcpy(a.tau, c->tau8, sizeof(a.tau));
+  memcpy(a.weights, c->w8, sizeof(a.weights));
+  memcpy(a.coeff, c->coeff, sizeof(a.coeff));
+  const float pi = 4. * atan(1.);
+  a.w0 = 2 * pi * c->p.fp;
+  a.facex = (float)pow((double)c->p.fac, (double)c->p.ex);
+  a.nvar = nvar;
+  a.var_offset = (nvar == 8) ? 3 : 0;
+  a.nve = c->p.nve;
+  a.socalq = c->p.socalq;
+  a.nxt = c->p.nx; a.nyt = c->p.ny; a.nzt = c->p.nz;
+  a.slice = c->g.slice; a.yline = c->g.yline;
+  CU_TRY(awp_launch_media(a, c->stream));
+  CU_TRY(awp_launch_media_borders(c->f[AWP_D1], c->f[AWP_MU], c->f[AWP_LAM], c->f[AWP_QP],
+                                  c->f[AWP_QS], c->g, c->p.nve, c->stream));
+  CU_TRY(awp_launch_lam_mu(c->f[AWP_LAM], c->f[AWP_MU], c->lam_mu, c->g, c->xls, c->xre,
+                           c->yls, c->yre, c->stream));
+  if (tmp) CU_TRY(cudaFreeAsync(tmp, c->stream));
+  // Elastic specialisation: with Q^-1 identically zero the memory variables
+  // stay zero and the anelastic update reduces exactly to the elastic one, so
+  // the stress kernel may skip the six r arrays and the two Q arrays.
+  CU_TRY(cudaMemsetAsync(c->d_flag, 0, sizeof(unsigned int), c->stream));
+  CU_TRY(awp_launch_anynonzero(c->f[AWP_QP], c->g.cells_pad(), c->d_flag, c->stream));
+  CU_TRY(awp_launch_anynonzero(c->f[AWP_QS], c->g.cells_pad(), c->d_flag, c->stream));
+  unsigned int hflag = 1;
+  CU_TRY(cudaMemcpyAsync(&hflag, c->d_flag, sizeof(hflag), cudaMemcpyDeviceToHost, c->stream));
+  CU_TRY(cudaStreamSynchronize(c->stream));
+  const bool any_q = hflag != 0;
+  c->elastic = !any_q;
+  c->media_ready = true;
+  return AWP_OK;
+}
+
+int awp_upload_media(awp_ctx* c, int nvar, const float* host_media) {
+  return upload_media_impl(c, nvar, host_media, false);
+}
+int awp_upload_media_device(awp_ctx* c, int nvar, const float* dev_media) {
+  return upload_media_impl(c, nvar, dev_media, true);
+}
+
+int awp_upload_sources(awp_ctx* c, int nsrc, const int* pos, const float* data) {
+  if (!c) return set_error(AWP_ERR_ARG, "null context");
+  if (nsrc < 0 || (nsrc > 0 && (!pos || !data))) return set_error(AWP_ERR_ARG, "bad sources");
+  const int rs = c->p.read_step;
+  if (c->p.ifault == 1 && rs < c->p.nst)
+    return set_error(AWP_ERR_UNSUPPORTED,
+                     "IFAULT=1 holds all NST samples on the device (READ_STEP >= NST)");
+  const int stride = (c->p.ifault == 5) ? 2 : rs;
+  // group by target cell (file order kept inside a cell)
+  std::map<long long, std::vector<int>> cells;
+  for (int s = 0; s < nsrc; ++s) {
+    // inisource (source.c:172-174, 228-230) then addsrc (source.c:285-287)
+    const int x = pos[3 * s], y = pos[3 * s + 1], zf = pos[3 * s + 2];
+    const int z = c->p.nz + 1 - zf;
+    if (x < -1 || x > c->p.nx + 2 || y < -1 || y > c->p.ny + 2 || z < 1 || z > c->p.nz)
+      continue;  // outside this rank's index window: skipped as inisource does
+    const long long p = (long long)(x + 1 + AWP_NGSL) * c->g.slice +
+                        (long long)(y + 1 + AWP_NGSL) * c->g.yline + (z + AWP_ALIGN - 1);
+    cells[p].push_back(s);
+  }
+  std::vector<int> cpos, cfirst, order;
+  for (auto& kv : cells) {
+    cpos.push_back((int)kv.first);
+    cfirst.push_back((int)order.size());
+    for (int s : kv.second) order.push_back(s);
+  }
+  cfirst.push_back((int)order.size());
+  // de-interleave the time series: [comp][nsrc][stride]
+  std::vector<float> comp((size_t)6 * nsrc * stride);
+  for (int s = 0; s < nsrc; ++s)
+    for (int t = 0; t < stride; ++t)
+      for (int q = 0; q < 6; ++q)
+        comp[((size_t)q * nsrc + s) * stride + t] = data[((size_t)s * rs + t) * 6 + q];
+  cudaFree(c->d_cell_pos); cudaFree(c->d_cell_first); cudaFree(c->d_order);
+  for (int q = 0; q < 6; ++q) cudaFree(c->d_src[q]);
+  cudaFree(c->d_mom);
+  c->d_cell_pos = c->d_cell_first = c->d_order = nullptr;
+  c->d_mom = nullptr;
+  for (int q = 0; q < 6; ++q) c->d_src[q] = nullptr;
+  c->nsrc = nsrc;
+  c->ncell = (int)cpos.size();
+  c->src_stride = stride;
+  if (nsrc == 0) return AWP_OK;
+  int st;
+  if ((st = ctx_alloc(c, (void**)&c->d_cell_pos, cpos.size() * 4 + 4))) return st;
+  if ((st = ctx_alloc(c, (void**)&c->d_cell_first, cfirst.size() * 4))) return st;
+  if ((st = ctx_alloc(c, (void**)&c->d_order, order.size() * 4 + 4))) return st;
+  CU_TRY(cudaMemcpy(c->d_cell_pos, cpos.data(), cpos.size() * 4, cudaMemcpyHostToDevice));
+  CU_TRY(cudaMemcpy(c->d_cell_first, cfirst.data(), cfirst.size() * 4, cudaMemcpyHostToDevice));
+  CU_TRY(cudaMemcpy(c->d_order, order.data(), order.size() * 4, cudaMemcpyHostToDevice));
+  for (int q = 0; q < 6; ++q) {
+    if ((st = ctx_alloc(c, (void**)&c->d_src[q], (size_t)nsrc * stride * 4))) return st;
+    CU_TRY(cudaMemcpy(c->d_src[q], comp.data() + (size_t)q * nsrc * stride,
+                      (size_t)nsrc * stride * 4, cudaMemcpyHostToDevice));
+  }
+  if (c->p.ifault == 5) {
+    if ((st = ctx_alloc(c, (void**)&c->d_mom, (size_t)nsrc * 4))) return st;
+    CU_TRY(cudaMemset(c->d_mom, 0, (size_t)nsrc * 4));
+    if (c->filtorder > 0) {
+      cudaFree(c->d_filt);
+      c->d_filt = nullptr;
+      const size_t b = (size_t)nsrc * (c->filtorder + 1) * sizeof(double);
+      if ((st = ctx_alloc(c, (void**)&c->d_filt, b))) return st;
+      CU_TRY(cudaMemset(c->d_filt, 0, b));
+    }
+  }
+  return AWP_OK;
+}
+
+int awp_set_source_filter(awp_ctx* c, int order, const double* b, const double* a) {
+  if (!c) return set_error(AWP_ERR_ARG, "null context");
+  if (order < 0 || order >= AWP_MAXFILT) return set_error(AWP_ERR_ARG, "filter order %d", order);
+  c->filtorder = order;
+  for (int i = 0; i <= order && order > 0; ++i) {
+    c->filt_b[i] = b[i];
+    c->filt_a[i] = a[i];
+  }
+  if (c->nsrc > 0 && c->p.ifault == 5 && order > 0) {
+    cudaFree(c->d_filt);
+    c->d_filt = nullptr;
+    const size_t bytes = (size_t)c->nsrc * (order + 1) * sizeof(double);
+    int st;
+    if ((st = ctx_alloc(c, (void**)&c->d_filt, bytes))) return st;
+    CU_TRY(cudaMemset(c->d_filt, 0, bytes));
+  }
+  return AWP_OK;
+}
+
+int awp_download_moment(awp_ctx* c, float* host_mom) {
+  if (!c || !host_mom) return set_error(AWP_ERR_ARG, "null argument");
+  if (!c->d_mom) return set_error(AWP_ERR_STATE, "no kinematic source");
+  CU_TRY(cudaStreamSynchronize(c->stream));
+  CU_TRY(cudaMemcpy(host_mom, c->d_mom, (size_t)c->nsrc * 4, cudaMemcpyDeviceToHost));
+  return AWP_OK;
+}
+
+int awp_upload_plasticity(awp_ctx* c, const float* sigma2, const float* cohes,
+                          const float* phi, float fmajor, float fminor,
+                          const float strike[3], const float dip[3]) {
+  if (!c || !sigma2 || !cohes || !phi || !strike || !dip)
+    return set_error(AWP_ERR_ARG, "null argument");
+  if (c->p.nve != 3) return set_error(AWP_ERR_STATE, "plasticity needs NVE=3");
+  const size_t bytes = sizeof(float) * (size_t)c->g.cells_pad();
+  CU_TRY(cudaMemcpy(c->f[AWP_SIGMA2], sigma2, bytes, cudaMemcpyHostToDevice));
+  CU_TRY(cudaMemcpy(c->f[AWP_COHES], cohes, bytes, cudaMemcpyHostToDevice));
+  CU_TRY(cudaMemcpy(c->f[AWP_PHI], phi, bytes, cudaMemcpyHostToDevice));
+  c->pp.fmajor = fmajor;
+  c->pp.fminor = fminor;
+  awp::rotation_matrix(strike, dip, c->pp.Rz, c->pp.RzT);
+  c->pp.dh = c->p.dh;
+  c->pp.dt = c->p.dt;
+  c->pp.ktop = c->g.top();
+  // visit count of the five drprecpc_calc strips (pmcl3d.c:2121-2181)
+  const int nxp = (int)c->g.nx_pad(), nyp = (int)c->g.ny_pad();
+  std::vector<unsigned char> mult((size_t)nxp * nyp, 0);
+  const int xl = c->xls, xr = c->xre, yl = c->yls, yr = c->yre;
+  auto add = [&](int i0, int i1, int j0, int j1) {
+    for (int i = i0; i <= i1; ++i)
+      for (int j = j0; j <= j1; ++j)
+        if (i >= 0 && i < nxp && j >= 0 && j < nyp) mult[(size_t)i * nyp + j]++;
+  };
+  add(xl, xr, yl, yl + AWP_NGSL);
+  add(xl, xr, yr - AWP_NGSL, yr);
+  add(xl, xl + AWP_NGSL, yl, yr);
+  add(xr - AWP_NGSL, xr, yl, yr);
+  add(xl + AWP_NGSL, xr - AWP_NGSL, yl + AWP_NGSL, yr - AWP_NGSL);
+  cudaFree(c->d_neta_mult);
+  c->d_neta_mult = nullptr;
+  int st;
+  if ((st = ctx_alloc(c, (void**)&c->d_neta_mult, mult.size()))) return st;
+  CU_TRY(cudaMemcpy(c->d_neta_mult, mult.data(), mult.size(), cudaMemcpyHostToDevice));
+  c->plast_ready = true;
+  return AWP_OK;
+}
+
+int awp_step(awp_ctx* c, int nsteps) {
+  if (!c) return set_error(AWP_ERR_ARG, "null context");
+  if (!c->media_ready) return set_error(AWP_ERR_STATE, "awp_step before media upload");
+  if (c->p.nve == 3 && !c->plast_ready)
+    return set_error(AWP_ERR_STATE, "NVE=3 needs awp_upload_plasticity first");
+  for (int n = 0; n < nsteps; ++n) {
+    int st = one_step(c);
+    if (st) return st;
+  }
+  return AWP_OK;
+}
+
+int awp_synchronize(awp_ctx* c) {
+  if (!c) return set_error(AWP_ERR_ARG, "null context");
+  CU_TRY(cudaStreamSynchronize(c->stream));
+  return AWP_OK;
+}
+
+int awp_current_step(const awp_ctx* c, long long* step) {
+  if (!c || !step) return set_error(AWP_ERR_ARG, "null argument");
+  *step = c->cur_step;
+  return AWP_OK;
+}
+
+int awp_field_device_ptr(awp_ctx* c, int field, float** dev_ptr) {
+  if (!c || !dev_ptr || field < 0 || field >= AWP_NFIELDS)
+    return set_error(AWP_ERR_ARG, "bad field %d", field);
+  if (!c->f[field]) return set_error(AWP_ERR_STATE, "field %d not allocated (NVE)", field);
+  *dev_ptr = c->f[field];
+  return AWP_OK;
+}
+
+int awp_field_download(awp_ctx* c, int field, float* host) {
+  float* d;
+  int st = awp_field_device_ptr(c, field, &d);
+  if (st) return st;
+  if (!host) return set_error(AWP_ERR_ARG, "null host buffer");
+  CU_TRY(cudaMemcpyAsync(host, d, sizeof(float) * (size_t)c->g.cells_pad(),
+                         cudaMemcpyDeviceToHost, c->stream));
+  CU_TRY(cudaStreamSynchronize(c->stream));
+  return AWP_OK;
+}
+
+int awp_field_upload(awp_ctx* c, int field, const float* host) {
+  float* d;
+  int st = awp_field_device_ptr(c, field, &d);
+  if (st) return st;
+  if (!host) return set_error(AWP_ERR_ARG, "null host buffer");
+  CU_TRY(cudaMemcpyAsync(d, host, sizeof(float) * (size_t)c->g.cells_pad(),
+                         cudaMemcpyHostToDevice, c->stream));
+  CU_TRY(cudaStreamSynchronize(c->stream));
+  if ((field >= AWP_R1 && field <= AWP_R6) || field == AWP_QP || field == AWP_QS)
+    c->elastic = false;  // explicit memory-variable / Q state: use the full update
+  if (field == AWP_D1 || field == AWP_MU || field == AWP_LAM) {
+    if (field == AWP_LAM || field == AWP_MU)
+      CU_TRY(awp_launch_lam_mu(c->f[AWP_LAM], c->f[AWP_MU], c->lam_mu, c->g, c->xls, c->xre,
+                               c->yls, c->yre, c->stream));
+    c->media_ready = true;
+  }
+  return AWP_OK;
+}
+
+int awp_gather_output(awp_ctx* c, int nbgx, int nedx, int nskpx, int nbgy, int nedy,
+                      int nskpy, int nbgz, int nedz, int nskpz, float* bufx, float* bufy,
+                      float* bufz, float* bufeta) {
+  if (!c || !bufx || !bufy || !bufz) return set_error(AWP_ERR_ARG, "null argument");
+  if (nskpx < 1 || nskpy < 1 || nskpz < 1) return set_error(AWP_ERR_ARG, "skip < 1");
+  VelBufArgs a;
+  memset(&a, 0, sizeof(a));
+  a.u1 = c->f[AWP_U1]; a.v1 = c->f[AWP_V1]; a.w1 = c->f[AWP_W1]; a.neta = c->f[AWP_NETA];
+  a.bufx = bufx; a.bufy = bufy; a.bufz = bufz; a.bufeta = bufeta;
+  a.nve = c->p.nve;
+  a.nbgx = nbgx; a.nedx = nedx; a.nskpx = nskpx;
+  a.nbgy = nbgy; a.nedy = nedy; a.nskpy = nskpy;
+  a.nbgz = nbgz; a.nedz = nedz; a.nskpz = nskpz;
+  a.rec_nxt = (nedx - nbgx) / nskpx + 1;
+  a.rec_nyt = (nedy - nbgy) / nskpy + 1;
+  a.rec_nzt = (nedz - nbgz) / nskpz + 1;
+  a.slice = c->g.slice; a.yline = c->g.yline; a.ktop = c->g.top();
+  a.w_shift = 1;
+  CU_TRY(awp_launch_velbuffer(a, c->stream));
+  return AWP_OK;
+}
+
+int awp_check_finite(awp_ctx* c, int* ok) {
+  if (!c || !ok) return set_error(AWP_ERR_ARG, "null argument");
+  CU_TRY(cudaMemsetAsync(c->d_flag, 0, sizeof(unsigned int), c->stream));
+  for (int fld = AWP_U1; fld <= AWP_YZ; ++fld)
+    CU_TRY(awp_launch_nonfinite(c->f[fld], c->g.cells_pad(), c->d_flag, c->stream));
+  unsigned int h = 0;
+  CU_TRY(cudaMemcpyAsync(&h, c->d_flag, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+  CU_TRY(cudaStreamSynchronize(c->stream));
+  *ok = h ? 0 : 1;
+  return AWP_OK;
+}
+
+int awp_profile_phases(awp_ctx* c, int enable) {
+  if (!c) return set_error(AWP_ERR_ARG, "null context");
+  c->profile = enable != 0;
+  return AWP_OK;
+}
+
+int awp_phase_times(awp_ctx* c, double ms[AWP_NPHASES], long long launches[AWP_NPHASES]) {
+  if (!c || !ms || !launches) return set_error(AWP_ERR_ARG, "null argument");
+  CU_TRY(cudaStreamSynchronize(c->stream));
+  for (int p = 0; p < AWP_NPHASES; ++p) {
+    ms[p] = 0.0;
+    launches[p] = 0;
+  }
+  for (auto& e : c->ev_used) {
+    float t = 0.f;
+    CU_TRY(cudaEventElapsedTime(&t, e.a, e.b));
+    ms[e.phase] += t;
+    launches[e.phase] += 1;
+    c->ev_free.push_back(e);
+  }
+  c->ev_used.clear();
+  return AWP_OK;
+}
+
+int awp_kernel_launches(const awp_ctx* c, long long* launches) {
+  if (!c || !launches) return set_error(AWP_ERR_ARG, "null argument");
+  *launches = c->launches;
+  return AWP_OK;
+}
+
+int awp_device_bytes(const awp_ctx* c, long long* bytes) {
+  if (!c || !bytes) return set_error(AWP_ERR_ARG, "null argument");
+  *bytes = c->dev_bytes;
+  return AWP_OK;
+}
+
+// --------------------------------------------------------------------------
+// host set-up helpers
+// --------------------------------------------------------------------------
+int awp_q_tau(float ex, float fac, float* taumax, float* taumin, float tau8[8]) {
+  if (!awp::tau_range(ex, fac, taumax, taumin))
+    return set_error(AWP_ERR_UNSUPPORTED, "EX=%g has no relaxation-time range", ex);
+  awp::tausub(*taumin, *taumax, tau8);
+  return AWP_OK;
+}
+
+int awp_q_weights(float ex, float fac, float w8[8], float coeff16[16]) {
+  awp::weights_sub(ex, fac, w8, coeff16);
+  return AWP_OK;
+}
+
+int awp_cerjan(float arbc, int nxt, int nyt, int nzt, int nd, int islowest, int npc,
+               float* dcrjx, float* dcrjy, float* dcrjz) {
+  for (int i = 0; i < nxt + 4 + AWP_NGSL2; ++i) dcrjx[i] = 1.0f;
+  for (int i = 0; i < nyt + 4 + AWP_NGSL2; ++i) dcrjy[i] = 1.0f;
+  for (int i = 0; i < nzt + 2 * AWP_ALIGN; ++i) dcrjz[i] = 1.0f;
+  awp::inicrj(arbc, nxt, nyt, nzt, nxt, nyt, nd, islowest, npc, dcrjx, dcrjy, dcrjz);
+  return AWP_OK;
+}
+
+int awp_texture_at(const float tau8[8], const float w8[8], float dt, int xls, int yls, int ny,
+                   int nzt, int i, int j, int k, float* vx1, float* vx2, int* ww, float* wwo) {
+  AwpTexture t;
+  awp::texture_tables(tau8, w8, dt, &t);
+  t.xls = xls;
+  t.yls = yls;
+  t.ny = ny;
+  t.nzt = nzt;
+  const int idx = awp_tex_index(t, i, j, k);
+  *vx1 = t.tau1[idx];
+  *vx2 = t.tau2[idx];
+  *wwo = t.wwo8[idx];
+  *ww = idx + 1;
+  return AWP_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,170 @@
+"""Seeded synthetic inputs for the benchmark and test workloads.
+
+No public dataset is involved: each workload is generated from its seed with
+the shapes, sizes and value distributions of the corresponding run.
+
+* ``halfspace``   -- homogeneous elastic half-space with a point moment-tensor
+  source (Mxy, Ricker derivative) at the grid centre (IFAULT=1).
+* ``layered_vk``  -- 1-D vs gradient with depth, vp = 1.73 vs, Gardner rho,
+  von Karman perturbation, Qs = 50 vs[km/s], Qp = 2 Qs, and a kinematic
+  finite fault of random subfaults (IFAULT=5, Brune source time function).
+* ``random_small`` -- small random heterogeneous media for parity tests.
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+
+import numpy as np
+
+
+@dataclasses.dataclass
+class Scenario:
+    name: str
+    params: dict          # awp_params fields
+    media: np.ndarray     # float32 [nz][ny][nx][nvar], surface first
+    src_pos: np.ndarray   # int32 [nsrc][3] INSRC coordinates (1-based, z from surface)
+    src_data: np.ndarray  # float32 [nsrc][read_step][6]
+    steps: int
+    description: str = ""
+
+
+def ricker_derivative(nt: int, dt: float, f0: float, t0: float | None = None) -> np.ndarray:
+    """Time derivative of a Ricker wavelet (the moment-rate of a Ricker moment)."""
+    t0 = 1.2 / f0 if t0 is None else t0
+    t = np.arange(nt) * dt - t0
+    a = (math.pi * f0 * t) ** 2
+    # d/dt [(1 - 2a) exp(-a)] with a = (pi f0 t)^2
+    dadt = 2.0 * (math.pi * f0) ** 2 * t
+    return ((-2.0 * dadt) * np.exp(-a) - (1.0 - 2.0 * a) * np.exp(-a) * dadt).astype(np.float64)
+
+
+def halfspace(nx=128, ny=128, nz=128, h=100.0, dt=0.005, steps=500, f0=2.0, m0=1e15,
+              vp=6000.0, vs=3464.0, rho=2700.0, nd=20, seed=1) -> Scenario:
+    media = np.empty((nz, ny, nx, 5), np.float32)
+    media[..., 0] = vp
+    media[..., 1] = vs
+    media[..., 2] = rho
+    media[..., 3] = 0.0  # Qp <= 0: elastic (mesh.c:434-438)
+    media[..., 4] = 0.0
+    nst = steps
+    stf = ricker_derivative(nst, dt, f0) * m0
+    data = np.zeros((1, nst, 6), np.float32)
+    data[0, :, 5] = stf  # Mxy
+    pos = np.array([[nx // 2, ny // 2, nz // 2]], np.int32)
+    params = dict(nx=nx, ny=ny, nz=nz, dh=h, dt=dt, nd=nd, arbc=0.92, npc=0, nve=1,
+                  ifault=1, nst=nst, read_step=nst, socalq=1)
+    return Scenario("halfspace", params, media, pos, data, steps,
+                    f"elastic half-space {nx}x{ny}x{nz}, h={h}, dt={dt}, Mxy Ricker' {f0} Hz")
+
+
+def von_karman(shape, dh, corr_len, hurst, std, seed) -> np.ndarray:
+    """Von Karman random field, generated spectrally, unit-free with given std."""
+    import scipy.fft as sfft
+    nz, ny, nx = shape
+    rng = np.random.default_rng(seed)
+    kz = np.fft.fftfreq(nz, d=dh) * 2 * math.pi
+    ky = np.fft.fftfreq(ny, d=dh) * 2 * math.pi
+    kx = np.fft.rfftfreq(nx, d=dh) * 2 * math.pi
+    k2 = (kz[:, None, None] ** 2 + ky[None, :, None] ** 2 + kx[None, None, :] ** 2)
+    # 3-D von Karman power spectrum ~ (1 + k^2 a^2)^-(H + 3/2); amplitude = sqrt
+    amp = (1.0 + k2 * corr_len * corr_len) ** (-(hurst + 1.5) / 2.0)
+    amp = amp.astype(np.float32)
+    del k2
+    noise = rng.standard_normal(shape, dtype=np.float32)
+    spec = sfft.rfftn(noise, workers=-1)
+    del noise
+    spec *= amp
+    del amp
+    field = sfft.irfftn(spec, s=shape, workers=-1).astype(np.float32)
+    del spec
+    field -= field.mean()
+    field *= std / max(float(field.std()), 1e-30)
+    return field
+
+
+def layered_vk(nx=512, ny=512, nz=256, h=50.0, dt=0.0035, steps=2000, nsub=200,
+               vs_top=1000.0, vs_bot=3500.0, std=0.05, corr=500.0, hurst=0.1,
+               seed_medium=2, seed_src=3, vp_cap=6300.0, nd=20) -> Scenario:
+    depth = (np.arange(nz, dtype=np.float32) + 0.5) / nz  # 0 = surface (file k=0)
+    vs1d = vs_top + (vs_bot - vs_top) * depth
+    pert = von_karman((nz, ny, nx), h, corr, hurst, std, seed_medium)
+    pert = np.clip(pert, -3 * std, 3 * std)
+    vs = vs1d[:, None, None] * (1.0 + pert)
+    del pert
+    vp = np.minimum(1.73 * vs, vp_cap).astype(np.float32)
+    vs = (vp / 1.73).astype(np.float32)
+    rho = (310.0 * vp ** 0.25).astype(np.float32)  # Gardner, kg/m^3 with vp in m/s
+    qs = (50.0 * vs / 1000.0).astype(np.float32)
+    qp = (2.0 * qs).astype(np.float32)
+    media = np.stack([vp, vs, rho, qp, qs], axis=-1).astype(np.float32)
+    del vp, vs, rho, qp, qs
+    src_pos, src_data = kinematic_fault(nx, ny, nz, h, nsub, seed_src)
+    params = dict(nx=nx, ny=ny, nz=nz, dh=h, dt=dt, nd=nd, arbc=0.92, npc=0, nve=1,
+                  ifault=5, nst=2, read_step=2, socalq=1)
+    return Scenario("layered_vk", params, media, src_pos, src_data, steps,
+                    f"anelastic 1-D gradient + von Karman {nx}x{ny}x{nz}, h={h}, dt={dt}, "
+                    f"{nsub} kinematic subfaults")
+
+
+def kinematic_fault(nx, ny, nz, h, nsub, seed, strike=0.0, dip=90.0, rake=180.0):
+    """Random subfaults on a vertical plane x = nx/2 (IFAULT=5 layout, source.c:165-181)."""
+    rng = np.random.default_rng(seed)
+    ny0, ny1 = ny // 4, 3 * ny // 4
+    nz0, nz1 = max(3, nz // 16), nz // 2
+    cells = set()
+    pos = []
+    while len(pos) < nsub:
+        y = int(rng.integers(ny0, ny1))
+        z = int(rng.integers(nz0, nz1))
+        if (y, z) in cells:
+            continue
+        cells.add((y, z))
+        pos.append((nx // 2, y, z))
+    pos = np.array(pos, np.int32)
+    data = np.zeros((nsub, 2, 6), np.float32)
+    data[:, 0, 0] = 1.0                                  # Brune
+    data[:, 0, 1] = rng.uniform(0.5, 1.5, nsub)          # slip (m)
+    data[:, 0, 2] = rng.uniform(0.0, 3.0, nsub)          # rupture time (s)
+    data[:, 0, 3] = rng.uniform(0.3, 1.0, nsub)          # rise time (s)
+    data[:, 0, 4] = h * h                                # subfault area (m^2)
+    data[:, 1, 0] = strike + rng.uniform(-10, 10, nsub)  # strike (deg)
+    data[:, 1, 1] = dip
+    data[:, 1, 2] = rake + rng.uniform(-15, 15, nsub)
+    return pos, data
+
+
+def random_small(nx=24, ny=20, nz=32, h=100.0, dt=0.004, steps=20, seed=7, nvar=5,
+                 q=True, ifault=1, nsrc=3, nst=None) -> Scenario:
+    """Small random heterogeneous model for parity tests (any nx, ny; nz % 4 == 0)."""
+    rng = np.random.default_rng(seed)
+    vs = rng.uniform(1500.0, 3000.0, (nz, ny, nx)).astype(np.float32)
+    vp = (vs * rng.uniform(1.6, 1.9, (nz, ny, nx))).astype(np.float32)
+    rho = rng.uniform(2200.0, 2800.0, (nz, ny, nx)).astype(np.float32)
+    cols = [vp, vs, rho]
+    if nvar >= 5:
+        if q:
+            qs = rng.uniform(20.0, 400.0, (nz, ny, nx)).astype(np.float32)
+            qp = (qs * rng.uniform(1.5, 2.5, (nz, ny, nx))).astype(np.float32)
+        else:
+            qs = np.zeros_like(vs)
+            qp = np.zeros_like(vs)
+        cols += [qp, qs]
+    if nvar == 8:
+        cols = [np.zeros_like(vs)] * 3 + cols
+    media = np.stack(cols, axis=-1).astype(np.float32)
+    nst = nst or steps + 2
+    if ifault == 5:
+        pos, data = kinematic_fault(nx, ny, nz, h, nsrc, seed + 1)
+        data[:, 0, 2] = rng.uniform(0.0, steps * dt * 0.3, nsrc)
+        data[:, 0, 3] = rng.uniform(5 * dt, 10 * dt, nsrc)
+        nst = 2
+    else:
+        pos = np.stack([rng.integers(3, nx - 2, nsrc), rng.integers(3, ny - 2, nsrc),
+                        rng.integers(1, nz - 2, nsrc)], axis=1).astype(np.int32)
+        pos[0, 2] = 1  # one source on the free surface row
+        data = (rng.standard_normal((nsrc, nst, 6)) * 1e13).astype(np.float32)
+    params = dict(nx=nx, ny=ny, nz=nz, dh=h, dt=dt, nd=min(6, nx // 4), arbc=0.92,
+                  npc=0, nve=1, ifault=ifault, nst=nst, read_step=nst, socalq=1)
+    return Scenario("random_small", params, media, pos, data, steps,
+                    f"random {nx}x{ny}x{nz} nvar={nvar} q={q} ifault={ifault}")

@@ -1,0 +1,185 @@
+"""Python mirror of the pmcl3d time-step interface over the C ABI.
+
+``Solver`` owns one ``awp_ctx`` (include/awp_b200.h).  Its methods map one to
+one onto the context entry points, which in turn replace the set-up and time
+loop of pmcl3d (src/awp/pmcl3d.c:370-2490) for a single rank.  Errors are
+raised as :class:`awp_b200._lib.AwpError` carrying the library's status code.
+"""
+from __future__ import annotations
+
+import ctypes
+from ctypes import byref, c_float, c_int, c_longlong, c_void_p
+
+import numpy as np
+
+from . import _lib
+from ._lib import FIELD_ID, awp_params, check
+
+NGSL = 8
+ALIGN = 32
+
+
+def _fptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(c_float))
+
+
+def default_params(**kw) -> awp_params:
+    """pmcl3d's defaults (command.c:71-136) overridden by keyword arguments."""
+    lib = _lib.load()
+    p = awp_params()
+    lib.awp_params_default(byref(p))
+    for k, v in kw.items():
+        if not hasattr(p, k):
+            raise KeyError(f"unknown parameter {k}")
+        setattr(p, k, v)
+    return p
+
+
+def padded_shape(nx: int, ny: int, nz: int) -> tuple[int, int, int]:
+    return (nx + 4 + 2 * NGSL, ny + 4 + 2 * NGSL, nz + 2 * ALIGN)
+
+
+class Solver:
+    """One single-rank, single-grid simulation on the current CUDA device."""
+
+    def __init__(self, params: awp_params | None = None, stream: int | None = None, **kw):
+        self.lib = _lib.load()
+        self.params = params if params is not None else default_params(**kw)
+        ctx = c_void_p()
+        check(self.lib.awp_ctx_create(byref(self.params), byref(ctx)), "awp_ctx_create")
+        self.ctx = ctx
+        if stream is not None:
+            check(self.lib.awp_set_stream(self.ctx, c_void_p(stream)), "awp_set_stream")
+        dims = (c_longlong * 3)()
+        check(self.lib.awp_padded_dims(self.ctx, dims), "awp_padded_dims")
+        self.shape = tuple(int(d) for d in dims)
+
+    # -- lifetime ---------------------------------------------------------
+    def close(self) -> None:
+        if getattr(self, "ctx", None):
+            self.lib.awp_ctx_destroy(self.ctx)
+            self.ctx = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- inputs ------------------------------------------------------------
+    def upload_media(self, media: np.ndarray) -> None:
+        """media: float32 [nz][ny][nx][nvar] in the mesh-file order (surface first)."""
+        media = np.ascontiguousarray(media, dtype=np.float32)
+        if media.ndim != 4:
+            raise ValueError("media must be [nz][ny][nx][nvar]")
+        p = self.params
+        if media.shape[:3] != (p.nz, p.ny, p.nx):
+            raise ValueError(f"media shape {media.shape} does not match {p.nz, p.ny, p.nx}")
+        check(self.lib.awp_upload_media(self.ctx, int(media.shape[3]), _fptr(media)),
+              "awp_upload_media")
+
+    def upload_media_device(self, ptr: int, nvar: int) -> None:
+        check(self.lib.awp_upload_media_device(self.ctx, nvar, c_void_p(ptr)),
+              "awp_upload_media_device")
+
+    def upload_sources(self, pos: np.ndarray, data: np.ndarray) -> None:
+        """pos: int32 [nsrc][3] INSRC coordinates; data: float32 [nsrc][read_step][6]."""
+        pos = np.ascontiguousarray(pos, dtype=np.int32)
+        data = np.ascontiguousarray(data, dtype=np.float32)
+        n = int(pos.shape[0])
+        check(self.lib.awp_upload_sources(self.ctx, n,
+                                          pos.ctypes.data_as(ctypes.POINTER(c_int)),
+                                          _fptr(data)), "awp_upload_sources")
+
+    def set_source_filter(self, b, a) -> None:
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        check(self.lib.awp_set_source_filter(
+            self.ctx, len(b) - 1, b.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+            a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))), "awp_set_source_filter")
+
+    def download_moment(self, nsrc: int) -> np.ndarray:
+        out = np.zeros(nsrc, np.float32)
+        check(self.lib.awp_download_moment(self.ctx, _fptr(out)), "awp_download_moment")
+        return out
+
+    def upload_plasticity(self, sigma2, cohes, phi, fmajor, fminor, strike, dip) -> None:
+        arrs = [np.ascontiguousarray(a, dtype=np.float32) for a in (sigma2, cohes, phi)]
+        st = np.ascontiguousarray(strike, dtype=np.float32)
+        dp = np.ascontiguousarray(dip, dtype=np.float32)
+        check(self.lib.awp_upload_plasticity(self.ctx, *[_fptr(a) for a in arrs],
+                                             c_float(fmajor), c_float(fminor),
+                                             _fptr(st), _fptr(dp)), "awp_upload_plasticity")
+
+    # -- time stepping -----------------------------------------------------
+    def step(self, n: int = 1) -> None:
+        check(self.lib.awp_step(self.ctx, int(n)), "awp_step")
+
+    def synchronize(self) -> None:
+        check(self.lib.awp_synchronize(self.ctx), "awp_synchronize")
+
+    @property
+    def current_step(self) -> int:
+        s = c_longlong()
+        check(self.lib.awp_current_step(self.ctx, byref(s)), "awp_current_step")
+        return s.value
+
+    # -- fields --------------------------------------------------------------
+    def field(self, name: str) -> np.ndarray:
+        out = np.empty(self.shape, np.float32)
+        check(self.lib.awp_field_download(self.ctx, FIELD_ID[name], _fptr(out)),
+              f"awp_field_download({name})")
+        return out
+
+    def set_field(self, name: str, arr: np.ndarray) -> None:
+        arr = np.ascontiguousarray(arr, dtype=np.float32).reshape(self.shape)
+        check(self.lib.awp_field_upload(self.ctx, FIELD_ID[name], _fptr(arr)),
+              f"awp_field_upload({name})")
+
+    def device_ptr(self, name: str) -> int:
+        p = c_void_p()
+        check(self.lib.awp_field_device_ptr(self.ctx, FIELD_ID[name], byref(p)),
+              f"awp_field_device_ptr({name})")
+        return int(p.value)
+
+    def gather(self, nbgx, nedx, nskpx, nbgy, nedy, nskpy, nbgz, nedz, nskpz,
+               bufx: int, bufy: int, bufz: int, bufeta: int = 0) -> None:
+        """velbuffer gather into device (or pinned) buffers given as addresses."""
+        check(self.lib.awp_gather_output(self.ctx, nbgx, nedx, nskpx, nbgy, nedy, nskpy,
+                                         nbgz, nedz, nskpz, c_void_p(bufx), c_void_p(bufy),
+                                         c_void_p(bufz), c_void_p(bufeta or None)),
+              "awp_gather_output")
+
+    def check_finite(self) -> bool:
+        ok = c_int()
+        check(self.lib.awp_check_finite(self.ctx, byref(ok)), "awp_check_finite")
+        return bool(ok.value)
+
+    PHASES = ("velocity", "stress", "sources", "plasticity", "fstr")
+
+    def profile_phases(self, enable: bool = True) -> None:
+        check(self.lib.awp_profile_phases(self.ctx, int(enable)), "awp_profile_phases")
+
+    def phase_times(self) -> dict:
+        ms = (ctypes.c_double * 5)()
+        n = (c_longlong * 5)()
+        check(self.lib.awp_phase_times(self.ctx, ms, n), "awp_phase_times")
+        return {p: (ms[i], n[i]) for i, p in enumerate(self.PHASES)}
+
+    @property
+    def kernel_launches(self) -> int:
+        n = c_longlong()
+        check(self.lib.awp_kernel_launches(self.ctx, byref(n)), "awp_kernel_launches")
+        return n.value
+
+    @property
+    def device_bytes(self) -> int:
+        b = c_longlong()
+        check(self.lib.awp_device_bytes(self.ctx, byref(b)), "awp_device_bytes")
+        return b.value

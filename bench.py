@@ -1,0 +1,420 @@
+#!/usr/bin/env python3
+"""Benchmark of the B200 AWP-ODC time step (Gcell-updates/s and % of HBM roofline).
+
+Workload (default): the anelastic heterogeneous forward run -- 512 x 512 x 256
+cells, h = 50 m, dt = 3.5 ms, 1-D vs gradient 1000..3500 m/s with a seeded
+von Karman perturbation (5 %, 500 m, Hurst 0.1), Qs = 50 vs[km/s], Qp = 2 Qs,
+200 seeded kinematic subfaults (IFAULT=5, Brune).  A "step" is one full time
+step of that grid (velocity, stress + memory variables, sources, free-surface
+images).  The 15 state fields plus 5 media fields (about 7 GB) are far larger
+than the 126 MB L2, so no L2 flush is needed between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun (N > 1) every rank runs an independent replica (the single-rank
+path does not shard; "replicas only"), timed on the device, max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+B_ALG = {"anelastic": 140, "elastic": 84}          # bytes per cell-update, whole step
+B_STRESS = {"anelastic": 124, "elastic": 68}       # stress kernel: 19 (11) reads + 12 (6) writes
+B_VEL = 52                                         # velocity kernel: 10 reads + 3 writes
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def build_workload(name: str):
+    from awp_b200 import scenarios
+    if name == "layered_vk":
+        return scenarios.layered_vk(), "anelastic"
+    if name == "halfspace":
+        return scenarios.halfspace(), "elastic"
+    raise SystemExit(f"unknown workload {name}")
+
+
+def cpu_baseline(workload: str, steps: int | None = None, warmup: int = 1,
+                 target_s: float = 12.0) -> dict:
+    """FP32 OpenMP restatement of the reference kernels (oracle/) on the host cores,
+    on a bounded window of the same workload."""
+    from awp_b200 import scenarios
+    from oracle import oracle as orc
+    from oracle import refbind
+    if workload == "layered_vk":
+        scn = scenarios.layered_vk(nx=160, ny=160, nz=96, nsub=40, steps=20)
+        sample = "160x160x96 window of the layered_vk model (same generator), FP32"
+    else:
+        scn = scenarios.halfspace(nx=128, ny=128, nz=128, steps=20)
+        sample = "128^3 half-space, FP32"
+    setup = refbind.model_setup(scn)
+    ncores = os.cpu_count() or 1
+    sim = orc.OracleSim(scn, setup, precision=32, nthreads=ncores)
+    sim.step(max(1, warmup))
+    if steps is None:
+        t0 = time.perf_counter()
+        sim.step(2)
+        per = (time.perf_counter() - t0) / 2
+        steps = max(3, min(200, int(target_s / max(per, 1e-6))))
+    t0 = time.perf_counter()
+    sim.step(steps)
+    dt = time.perf_counter() - t0
+    cells = scn.params["nx"] * scn.params["ny"] * scn.params["nz"]
+    val = cells * steps / dt / 1e9
+    sim.close()
+    return {"value": val, "unit": "Gcell-updates/s", "cores": ncores, "kind": "port",
+            "sample": f"{sample}, {steps} steps in {dt:.1f} s"}
+
+
+def texture_arrays(nx, ny, nz, tau1, tau2, w8):
+    """init_texture (mesh.c:1103-1137) arrays from its visit-parity pattern."""
+    shp = (nx + 20, ny + 20, nz + 64)
+    vx1 = np.zeros(shp, np.float32)
+    vx2 = np.zeros(shp, np.float32)
+    wwo = np.zeros(shp, np.float32)
+    ww = np.zeros(shp, np.int32)
+    i = np.arange(nx)[:, None, None]
+    j = np.arange(ny)[None, :, None]
+    k = np.arange(nz)[None, None, :]
+    ij = i * ny + j
+    itx = (i + 1) & 1
+    ity = (ij + 1) & 1
+    itz = (nz * (ij + 1) + k) & 1
+    t = (4 * itx + 2 * ity + itz).astype(np.int64)
+    sl = (slice(10, nx + 10), slice(10, ny + 10), slice(32, nz + 32))
+    vx1[sl] = np.asarray(tau1, np.float32)[t]
+    vx2[sl] = np.asarray(tau2, np.float32)[t]
+    wwo[sl] = (8.0 * np.asarray(w8, np.float64)).astype(np.float32)[t]
+    ww[sl] = (t + 1).astype(np.int32)
+    return vx1, vx2, ww, wwo
+
+
+def reference_gpu(scn, solver, steps=4, warmup=2) -> dict:
+    """The reference's own CUDA build (oracle/_ref/libawpref.so, 8-thread blocks as
+    shipped) on the same workload, inputs taken from the product's set-up."""
+    import torch
+    from oracle import refbind
+    p = scn.params
+    nx, ny, nz = p["nx"], p["ny"], p["nz"]
+    host = refbind.RefHost()
+    import ctypes
+    from ctypes import byref, c_float
+    taumax, taumin = c_float(), c_float()
+    tau8 = np.zeros(8, np.float32)
+    w8 = np.zeros(8, np.float32)
+    coeff = np.zeros(16, np.float32)
+    F = ctypes.POINTER(c_float)
+    solver.lib.awp_q_tau(0.0, 0.005, byref(taumax), byref(taumin), tau8.ctypes.data_as(F))
+    solver.lib.awp_q_weights(0.0, 0.005, w8.ctypes.data_as(F), coeff.ctypes.data_as(F))
+    tau1, tau2 = refbind.tau12(tau8, p["dt"])
+    vx1, vx2, ww, wwo = texture_arrays(nx, ny, nz, tau1, tau2, w8)
+    dx, dy, dz = host.inicrj(p["arbc"], nx, ny, nz, p["nd"], 1, p["npc"])
+    media = {k: solver.field(k) for k in ("d1", "mu", "lam", "qp", "qs")}
+    psrc, comps, rs = refbind.map_sources(scn)
+    setup = dict(media=media, vx1=vx1, vx2=vx2, ww=ww, wwo=wwo, dcrjx=dx, dcrjy=dy, dcrjz=dz,
+                 lam_mu=refbind.lam_mu_ref(media["lam"], media["mu"], nx, ny, nz),
+                 coeff=coeff, psrc=psrc, src=comps, src_stride=rs)
+    del media
+    sim = refbind.RefGpuSim(scn, setup)
+    del setup, vx1, vx2, ww, wwo
+    sim.step(warmup)
+    s0 = torch.cuda.Event(enable_timing=True)
+    s1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    s0.record()
+    sim.step(steps)
+    s1.record()
+    torch.cuda.synchronize()
+    ms = s0.elapsed_time(s1) / steps
+    out = {"value": nx * ny * nz / (ms * 1e-3) / 1e9, "unit": "Gcell-updates/s",
+           "ms_per_step": ms, "steps": steps,
+           "build": "reference src/awp/kernel.cu, nvcc sm_100a -O3 -use_fast_math, "
+                    "BLOCK_SIZE 2x2x4 as shipped; launched in the pmcl3d single-rank order"}
+    del sim
+    torch.cuda.empty_cache()
+    return out
+
+
+def load_traffic(kernel: str, workload: str):
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(path) as fh:
+            d = json.load(fh)
+        return d.get(workload, {}).get(kernel)
+    except Exception:
+        return None
+
+
+def run_ours(args, rank, world, dist) -> dict | None:
+    import torch
+    from awp_b200 import Solver, default_params
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+    scn, kind = build_workload(args.workload)
+    p = scn.params
+    cells = p["nx"] * p["ny"] * p["nz"]
+    stream = torch.cuda.current_stream()
+    hbm, peak_kind = peaks()
+
+    # ---- device-resident timing -------------------------------------------------
+    s = Solver(default_params(**p), stream=stream.cuda_stream)
+    s.upload_media(scn.media)
+    s.upload_sources(scn.src_pos, scn.src_data)
+    s.step(args.warmup)
+    s.synchronize()
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(torch.cuda.current_device())
+    sampler.start()
+    s.profile_phases(True)
+    launches0 = s.kernel_launches
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    s.step(args.steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    clocks = sampler.stop()
+    launches = s.kernel_launches - launches0
+    ms = e0.elapsed_time(e1)
+    phases = s.phase_times()
+    s.profile_phases(False)
+    ok = s.check_finite()
+    t_max = ms
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_max = float(t.item())
+    ms_step = t_max / args.steps
+    value = world * cells * args.steps / (t_max * 1e-3) / 1e9
+
+    st_ms, st_n = phases["stress"]
+    ve_ms, ve_n = phases["velocity"]
+    stress_ms = st_ms / max(st_n, 1)
+    vel_ms = ve_ms / max(ve_n, 1)
+    b_st = B_STRESS[kind] * cells
+    achieved = b_st / (stress_ms * 1e-3) / 1e9
+    traffic = load_traffic("stress", args.workload)
+    roofline = {"bound": "hbm", "kernel": "k_stress (stress + memory variables)",
+                "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                "peak_kind": f"{peak_kind} hbm_gbs", "traffic": traffic,
+                "alg_bytes_per_launch": b_st, "alg_bytes_per_cell": B_STRESS[kind],
+                "avg_launch_ms": stress_ms}
+    step_bw = B_ALG[kind] * cells / (ms_step * 1e-3) / 1e9
+    kernels = {name: {"ms_per_launch": v[0] / max(v[1], 1), "launches": v[1]}
+               for name, v in phases.items()}
+    kernels["velocity"]["achieved_GBs"] = B_VEL * cells / (vel_ms * 1e-3) / 1e9
+    kernels["stress"]["achieved_GBs"] = achieved
+    s.close()
+    del s
+    torch.cuda.empty_cache()
+
+    # ---- end to end through the C ABI with host buffers ----------------------------
+    e2e = None
+    if not args.no_e2e:
+        media = torch.from_numpy(scn.media).pin_memory()
+        nvar = scn.media.shape[3]
+        h2d = media.numel() * 4 + scn.src_pos.nbytes + scn.src_data.nbytes
+        rec = (p["nx"] * p["ny"])
+        out = [torch.empty(rec, dtype=torch.float32).pin_memory() for _ in range(3)]
+        dev = [torch.empty(rec, dtype=torch.float32, device="cuda") for _ in range(3)]
+        torch.cuda.synchronize()
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        se = Solver(default_params(**p), stream=stream.cuda_stream)
+        se.lib.awp_upload_media(se.ctx, nvar, media.numpy().ctypes.data_as(
+            __import__("ctypes").POINTER(__import__("ctypes").c_float)))
+        se.upload_sources(scn.src_pos, scn.src_data)
+        se.step(args.steps)
+        # free-surface snapshot (velbuffer, NBGZ=NEDZ=1) back to the host
+        se.gather(0, p["nx"] - 1, 1, 0, p["ny"] - 1, 1, 0, 0, 1,
+                  dev[0].data_ptr(), dev[1].data_ptr(), dev[2].data_ptr())
+        for o, d in zip(out, dev):
+            o.copy_(d, non_blocking=True)
+        t1.record(stream)
+        torch.cuda.synchronize()
+        e2e_ms = t0.elapsed_time(t1)
+        if dist is not None:
+            t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_ms = float(t.item())
+        d2h = 3 * rec * 4
+        e2e = {"value": world * cells * args.steps / (e2e_ms * 1e-3) / 1e9,
+               "unit": "Gcell-updates/s", "h2d_bytes_per_step": h2d / args.steps,
+               "d2h_bytes_per_step": d2h / args.steps, "ms_total": e2e_ms,
+               "includes": "context create, media H2D + on-device inimesh mapping, sources, "
+                           f"{args.steps} steps, surface snapshot D2H"}
+        se.close()
+        del se, media
+
+    if rank != 0:
+        return None
+    line = {
+        "metric": "Gcell-updates/s (whole time step) & %HBM roofline on 1 B200",
+        "value": value, "unit": "Gcell-updates/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded)",
+        "config": {"workload": scn.name, "description": scn.description,
+                   "grid": [p["nx"], p["ny"], p["nz"]], "cells": cells,
+                   "dh": p["dh"], "dt": p["dt"], "ifault": p["ifault"], "nve": p["nve"],
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "l2": "working set ~7 GB >> 126 MB L2, no flush needed",
+                   "finite_after_run": ok},
+        "roofline": roofline,
+        "step_roofline": {"bytes_per_cell_alg": B_ALG[kind], "achieved": step_bw,
+                          "peak": hbm, "unit": "GB/s", "frac": step_bw / hbm},
+        "kernels": kernels,
+        "clocks": clocks,
+        "gpu_launches": launches,
+    }
+    if e2e:
+        line["e2e"] = e2e
+    if world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(args.workload)
+    if world == 1 and not args.no_ref_gpu:
+        try:
+            s2 = Solver(default_params(**p))
+            s2.upload_media(scn.media)
+            line["reference_gpu_build"] = reference_gpu(scn, s2)
+            s2.close()
+        except Exception as exc:  # reported, never substituted
+            line["reference_gpu_build"] = {"unavailable": f"{type(exc).__name__}: {exc}"}
+    return line
+
+
+def run_reference(args, rank) -> dict | None:
+    """Reference arm: the reference path's CPU restatement on the host cores,
+    W warm-up and K timed steps on a bounded window of the same workload."""
+    if rank != 0:
+        return None
+    cb = cpu_baseline(args.workload, steps=args.steps, warmup=args.warmup)
+    return {"metric": "Gcell-updates/s (whole time step) & %HBM roofline on 1 B200",
+            "value": cb["value"], "unit": "Gcell-updates/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "impl": "reference", "dtype": "f32", "data": "synthetic (seeded)",
+            "config": {"workload": args.workload},
+            "cpu_baseline": cb,
+            "e2e": {"value": cb["value"], "unit": "Gcell-updates/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0},
+            "note": "the reference ships only CUDA for this path; its arm is the OpenMP "
+                    "restatement of the same kernels (oracle/awp_oracle.cpp) on the host cores"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", default="layered_vk", choices=["layered_vk", "halfspace"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-ref-gpu", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    dist = None
+    if args.impl == "reference":
+        line = run_reference(args, rank)
+    else:
+        if world > 1:
+            import datetime
+
+            import torch
+            import torch.distributed as dist_mod
+            torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+            dist_mod.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+            dist = dist_mod
+        line = run_ours(args, rank, world, dist)
+        if dist is not None:
+            dist.barrier()
+            dist.destroy_process_group()
+    if line is not None:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

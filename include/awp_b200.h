@@ -1,0 +1,261 @@
+/*
+ * awp_b200.h -- C ABI of the B200 time-step library (libawpb200.so).
+ *
+ * Two groups of entry points:
+ *
+ *  1. A re-entrant context API.  All state of one simulation lives in an
+ *     opaque awp_ctx; every call returns an int status (AWP_OK = 0).  It
+ *     replaces the host orchestration of pmcl3d's time loop
+ *     (src/awp/pmcl3d.c:1624-2490) together with the per-run set-up that
+ *     loop depends on (pmcl3d.c:370-1372).
+ *
+ *  2. Drop-in launchers with the reference's names and signatures
+ *     (include/awp/kernel_launch.h:10-190).  A pmcl3d-style caller links
+ *     against them unchanged: raw device float* per field in the reference's
+ *     padded layout, integer bounds in padded coordinates, a grid index d_i
+ *     into state installed by SetDeviceConstValue, void returns.  Like the
+ *     reference (CUCHK, include/awp/pmcl3d_cons.h:43-54) a CUDA error inside
+ *     one of them prints the error and exits the process; awp_compat_exit_on_error(0)
+ *     switches that to "record and return", readable via awp_compat_last_error().
+ *
+ * Field layout (both groups): index(i,j,k) = i*slice + j*yline + k with
+ * yline = nzt+64, slice = (nyt+20)*yline, extents (nxt+20) x (nyt+20) x (nzt+64);
+ * interior i,j in [10, 10+n), k in [32, 32+nzt); the free surface is the top,
+ * k = nzt+31.
+ */
+#ifndef AWP_B200_H
+#define AWP_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------------ */
+/* Status codes                                                              */
+/* ------------------------------------------------------------------------ */
+#define AWP_OK 0
+#define AWP_ERR_ARG 1
+#define AWP_ERR_CUDA 2
+#define AWP_ERR_STATE 3
+#define AWP_ERR_IO 4
+#define AWP_ERR_NOMEM 5
+#define AWP_ERR_NUMERIC 6
+#define AWP_ERR_UNSUPPORTED 7
+
+/* Field identifiers for awp_field_* (padded 3-D fields). */
+enum awp_field_id {
+  AWP_U1 = 0, AWP_V1, AWP_W1,                      /* velocities          */
+  AWP_XX, AWP_YY, AWP_ZZ, AWP_XY, AWP_XZ, AWP_YZ,  /* stresses            */
+  AWP_R1, AWP_R2, AWP_R3, AWP_R4, AWP_R5, AWP_R6,  /* memory variables    */
+  AWP_D1, AWP_MU, AWP_LAM, AWP_QP, AWP_QS,         /* media (rho, 1/mu,   */
+                                                   /*  1/lambda, Q^-1)    */
+  AWP_SIGMA2, AWP_COHES, AWP_PHI, AWP_YLDFAC, AWP_NETA, /* plasticity     */
+  AWP_NFIELDS
+};
+
+typedef struct awp_ctx awp_ctx;
+
+/* Run parameters.  Names and meaning follow pmcl3d's command line
+ * (src/awp/command.c:71-136, 228-504).  Single rank, single grid. */
+typedef struct awp_params {
+  int nx, ny, nz;    /* -X -Y -Z   interior cells (nz % 4 == 0, as pmcl3d.c:380) */
+  float dh, dt;      /* -H -t      grid spacing (m), time step (s)                */
+  float arbc;        /* -A         Cerjan sponge coefficient                      */
+  int npc;           /* -M         0 = Cerjan sponge, 2 = periodic                */
+  int nd;            /* -D         sponge width (cells)                           */
+  int nve;           /* -V         1 = anelastic, 3 = anelastic + plasticity      */
+  float fac, q0, ex, fp; /* -l -h --EX -p   Q(f) parameters                       */
+  int socalq;        /* -s         SoCal vp/vs floor (1 = on)                     */
+  int ifault;        /* -I         1 = point moment-rate source, 5 = kinematic    */
+  int nst;           /* -N         source time samples                            */
+  int read_step;     /* -R/-Q      samples held per source (IFAULT 1: >= nst)      */
+} awp_params;
+
+/* Fill *p with pmcl3d's defaults (command.c:71-136). */
+void awp_params_default(awp_params* p);
+
+/* Human-readable message for a status code, and the last error's detail. */
+const char* awp_status_string(int status);
+const char* awp_last_error(void);
+
+/* ------------------------------------------------------------------------ */
+/* Context API                                                               */
+/* ------------------------------------------------------------------------ */
+
+/* Allocate a simulation on the current CUDA device.  Fields start at zero,
+ * the sponge (inicrj, cerjan.c:5) and the Q(f) tables (weights_sub/tausub,
+ * mesh.c:684-1097) are set up here. */
+int awp_ctx_create(const awp_params* p, awp_ctx** out);
+int awp_ctx_destroy(awp_ctx* ctx);
+
+/* Run every subsequent kernel on this cudaStream_t (NULL = the context's own). */
+int awp_set_stream(awp_ctx* ctx, void* cuda_stream);
+
+/* Padded extents (nxt+20, nyt+20, nzt+64). */
+int awp_padded_dims(const awp_ctx* ctx, long long dims[3]);
+
+/* Media from a host buffer in the mesh-file layout float[nz][ny][nx][nvar],
+ * surface first, nvar in {3, 5, 8} (mesh.c:122-222).  Applies inimesh's
+ * unrelaxed-modulus correction and inverse-modulus mapping (mesh.c:222-466)
+ * on the device, fills the one-cell ghost border (mesh.c:468-591) and the
+ * surface Lame ratio (pmcl3d.c:944-951). */
+int awp_upload_media(awp_ctx* ctx, int nvar, const float* host_media);
+/* Same, with the media buffer already in device memory. */
+int awp_upload_media_device(awp_ctx* ctx, int nvar, const float* dev_media);
+
+/* Point / kinematic sources in the INSRC layout (source.c:165-181):
+ * pos[nsrc][3] = (x, y, z) 1-based with z counted down from the surface;
+ * data[nsrc][read_step][6] = (xx, yy, zz, xz, yz, xy) per time sample.  For
+ * IFAULT=5 only samples 0 and 1 are used and hold the subfault parameters
+ * (kernel.cu:3788-3809). */
+int awp_upload_sources(awp_ctx* ctx, int nsrc, const int* pos, const float* data);
+/* Optional IIR/FIR filter of the kinematic source time function
+ * (sourcefilter.dat, pmcl3d.c:651-673): b[order+1], a[order+1]. */
+int awp_set_source_filter(awp_ctx* ctx, int order, const double* b, const double* a);
+/* Accumulated moment per subfault (IFAULT=5), host buffer of nsrc floats. */
+int awp_download_moment(awp_ctx* ctx, float* host_mom);
+
+/* Plasticity inputs (NVE=3): padded sigma2/cohes/phi arrays (host) and the
+ * principal-stress frame of nonlinear.dat (mesh.c:1178-1401). */
+int awp_upload_plasticity(awp_ctx* ctx, const float* sigma2, const float* cohes,
+                          const float* phi, float fmajor, float fminor,
+                          const float strike[3], const float dip[3]);
+
+/* Advance nsteps time steps (pmcl3d.c:1628-2487 order: velocity, stress +
+ * attenuation, sources, plasticity, free-surface stress images).  Asynchronous
+ * with respect to the host; call awp_synchronize to wait. */
+int awp_step(awp_ctx* ctx, int nsteps);
+int awp_synchronize(awp_ctx* ctx);
+/* Number of completed time steps. */
+int awp_current_step(const awp_ctx* ctx, long long* step);
+
+/* Whole padded fields: host copies and raw device pointers. */
+int awp_field_download(awp_ctx* ctx, int field, float* host);
+int awp_field_upload(awp_ctx* ctx, int field, const float* host);
+int awp_field_device_ptr(awp_ctx* ctx, int field, float** dev_ptr);
+
+/* Surface / volume output gather of velbuffer (kernel.cu:3948-4011) into
+ * caller buffers (device or pinned host), one value per recording point,
+ * x fastest: rec_n = ((ned-nbg)/nskp+1) per axis, indices 0-based as
+ * calcRecordingPoints (calc.c:9-72) returns them. */
+int awp_gather_output(awp_ctx* ctx, int nbgx, int nedx, int nskpx, int nbgy,
+                      int nedy, int nskpy, int nbgz, int nedz, int nskpz,
+                      float* bufx, float* bufy, float* bufz, float* bufeta);
+
+/* Device-side non-finite sentinel over velocities and stresses: *ok = 1 when
+ * every value is finite. */
+int awp_check_finite(awp_ctx* ctx, int* ok);
+
+/* Per-phase device timing: when enabled, every subsequent awp_step records
+ * CUDA events around each of its phases on the context's stream.
+ * awp_phase_times waits for the stream and returns, per phase, the summed
+ * milliseconds and the number of launches since the last call:
+ * 0 velocity, 1 stress, 2 sources, 3 plasticity, 4 free-surface stress. */
+#define AWP_NPHASES 5
+int awp_profile_phases(awp_ctx* ctx, int enable);
+int awp_phase_times(awp_ctx* ctx, double ms[AWP_NPHASES], long long launches[AWP_NPHASES]);
+/* Kernels this context has launched so far. */
+int awp_kernel_launches(const awp_ctx* ctx, long long* launches);
+
+/* Bytes of device memory the context holds. */
+int awp_device_bytes(const awp_ctx* ctx, long long* bytes);
+
+/* ------------------------------------------------------------------------ */
+/* Host set-up helpers (exported for tests and the pmcl3d driver)           */
+/* ------------------------------------------------------------------------ */
+/* tausub (mesh.c:684-710) after inimesh's tau range (mesh.c:36-57);
+ * returns AWP_ERR_UNSUPPORTED for EX >= 0.95 (range left unset there). */
+int awp_q_tau(float ex, float fac, float* taumax, float* taumin, float tau8[8]);
+/* weights_sub (mesh.c:713-1097). */
+int awp_q_weights(float ex, float fac, float w8[8], float coeff16[16]);
+/* inicrj (cerjan.c:5-64), single rank; arrays pre-sized to the padded axes. */
+int awp_cerjan(float arbc, int nxt, int nyt, int nzt, int nd, int islowest, int npc,
+               float* dcrjx, float* dcrjy, float* dcrjz);
+/* The eight vx1/vx2/wwo values and ww of init_texture (mesh.c:1103-1137) at
+ * one padded cell, from the pattern the kernels use. */
+int awp_texture_at(const float tau8[8], const float w8[8], float dt, int xls,
+                   int yls, int ny, int nzt, int i, int j, int k, float* vx1,
+                   float* vx2, int* ww, float* wwo);
+
+/* ------------------------------------------------------------------------ */
+/* Reference-compatible launchers (include/awp/kernel_launch.h)             */
+/* ------------------------------------------------------------------------ */
+typedef struct CUstream_st* awp_stream_t; /* == cudaStream_t */
+
+/* kernel_launch.h:24 */
+void SetDeviceConstValue(float* DH, float DT, int* nxt, int* nyt, int* nzt,
+                         int ngrids, float fmajor, float fminor, float* Rz,
+                         float* RzT);
+/* kernel_launch.h:28 */
+void SetDeviceFilterParameters(int filtorder, double* srcfilt_b, double* srcfilt_a);
+/* kernel_launch.h:31 */
+void dvelcx_H_opt(float* u1, float* v1, float* w1, float* xx, float* yy, float* zz,
+                  float* xy, float* xz, float* yz, float* dcrjx, float* dcrjy,
+                  float* dcrjz, float* d_1, int nyt, int nzt, awp_stream_t St,
+                  int s_i, int e_i, int d_i, int ngrids);
+/* kernel_launch.h:36 (single rank: returns at rank == -1 like the reference) */
+void dvelcy_H(float* u1, float* v1, float* w1, float* xx, float* yy, float* zz,
+              float* xy, float* xz, float* yz, float* dcrjx, float* dcrjy,
+              float* dcrjz, float* d_1, int nxt, int nzt, float* s_u1,
+              float* s_v1, float* s_w1, awp_stream_t St, int s_j, int e_j,
+              int rank, int d_i);
+/* kernel_launch.h:51 */
+void dstrqc_H(float* xx, float* yy, float* zz, float* xy, float* xz, float* yz,
+              float* r1, float* r2, float* r3, float* r4, float* r5, float* r6,
+              float* u1, float* v1, float* w1, float* lam, float* mu, float* qp,
+              float* coeff, float* qs, float* dcrjx, float* dcrjy, float* dcrjz,
+              int nyt, int nzt, awp_stream_t St, float* lam_mu, float* vx1,
+              float* vx2, int* ww, float* wwo, int NX, int NPC, int rankx,
+              int ranky, int s_i, int e_i, int s_j, int e_j, int d_i);
+/* kernel_launch.h:42 (same arithmetic as dstrqc_H) */
+void dstrqc_H_new(float* xx, float* yy, float* zz, float* xy, float* xz, float* yz,
+                  float* r1, float* r2, float* r3, float* r4, float* r5, float* r6,
+                  float* u1, float* v1, float* w1, float* lam, float* mu, float* qp,
+                  float* coeff, float* qs, float* dcrjx, float* dcrjy, float* dcrjz,
+                  int nyt, int nzt, awp_stream_t St, float* lam_mu, float* vx1,
+                  float* vx2, int* ww, float* wwo, int NX, int NPC, int rankx,
+                  int ranky, int s_i, int e_i, int s_j, int e_j, int d_i);
+/* kernel_launch.h:58 */
+void fstr_H(float* zz, float* xz, float* yz, awp_stream_t St, int s_i, int e_i,
+            int s_j, int e_j);
+/* kernel_launch.h:61 */
+void drprecpc_calc_H_opt(float* xx, float* yy, float* zz, float* xy, float* xz,
+                         float* yz, float* mu, float* d1, float* sigma2,
+                         float* yldfac, float* cohes, float* phi, float* neta,
+                         int nzt, int xls, int xre, int yls, int yre,
+                         awp_stream_t St, int d_i);
+/* kernel_launch.h:67 */
+void drprecpc_app_H(float* xx, float* yy, float* zz, float* xy, float* xz,
+                    float* yz, float* mu, float* sigma2, float* yldfac, int nzt,
+                    int xls, int xre, int yls, int yre, awp_stream_t St, int d_i);
+/* kernel_launch.h:72 */
+void addsrc_H(int i, int READ_STEP, int dim, int* psrc, int npsrc, awp_stream_t St,
+              float* axx, float* ayy, float* azz, float* axz, float* ayz,
+              float* axy, float* xx, float* yy, float* zz, float* xy, float* yz,
+              float* xz, int d_i);
+/* kernel_launch.h:150 */
+void addkinsrc_H(int i, int dim, int* psrc, int npsrc, awp_stream_t St, float* mu,
+                 float* axx, float* ayy, float* azz, float* axz, float* ayz,
+                 float* axy, float* xx, float* yy, float* zz, float* xy, float* yz,
+                 float* xz, float* mom, double* d_srcfilt_d, int d_i);
+/* kernel_launch.h:182 */
+void velbuffer_H(const float* u1, const float* v1, const float* w1,
+                 const float* neta, float* Bufx, float* Bufy, float* Bufz,
+                 float* Bufeta, int NVE, int nbgx, int nedx, int nskpx, int nbgy,
+                 int nedy, int nskpy, int nbgz, int nedz, int nskpz, int rec_nxt,
+                 int rec_nyt, int rec_nzt, awp_stream_t St, int FOLLOWBATHY,
+                 const int* bathy, int d_i);
+
+/* Error mode of the launchers above: 1 (default) = print and exit like the
+ * reference's CUCHK; 0 = record the error and return. */
+void awp_compat_exit_on_error(int exit_on_error);
+/* Last error recorded by a launcher (0 = none); reading clears it. */
+int awp_compat_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* AWP_B200_H */

@@ -1,0 +1,142 @@
+/*
+ * Flat-array entry points around the reference's own host set-up code.
+ *
+ * Test infrastructure only.  This file is compiled together with the
+ * reference's src/awp/mesh.c, src/awp/cerjan.c and src/awp/grid.c (read in
+ * place, never copied) into oracle/_ref/libawpref_host.so.  The tests call it
+ * through ctypes to pin the product's C++ re-statement of the same set-up
+ * (Q(f) tables, relaxation times, the media/modulus mapping, the memory-
+ * variable parity pattern and the Cerjan sponge) against the reference
+ * itself.
+ *
+ * Every output array is flat and uses the reference's padded layout
+ * (i slowest, k fastest): (nxt+4+2*ngsl) x (nyt+4+2*ngsl) x (nzt+2*align).
+ */
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <awp/pmcl3d.h>
+
+Grid3D Alloc3D(int nx, int ny, int nz);
+Grid3Dww Alloc3Dww(int nx, int ny, int nz);
+Grid1D Alloc1D(int nx);
+void Delloc3D(Grid3D U);
+void Delloc3Dww(Grid3Dww U);
+void Delloc1D(Grid1D U);
+void tausub(Grid3D tau, _prec taumin, _prec taumax);
+void weights_sub(Grid3D weights, Grid1D coeff, _prec ex, _prec fac);
+void init_texture(int nxt, int nyt, int nzt, Grid3D tau1, Grid3D tau2, Grid3D vx1,
+                  Grid3D vx2, Grid3D weights, Grid3Dww ww, Grid3D wwo, int xls,
+                  int xre, int yls, int yre);
+void inicrj(_prec ARBC, int *coords, int nxt, int nyt, int nzt, int NX, int NY,
+            int ND, Grid1D dcrjx, Grid1D dcrjy, Grid1D dcrjz, int islowest,
+            int NPC);
+void hoek_brown(_prec sigma_0, _prec sigma_ci, _prec GSI, _prec mi, _prec D,
+                int tunnel, _prec *phi, _prec *cohes);
+
+static void copy8(Grid3D g, float *out) {
+  int i, j, k;
+  for (i = 0; i < 2; i++)
+    for (j = 0; j < 2; j++)
+      for (k = 0; k < 2; k++) out[i * 4 + j * 2 + k] = g[i][j][k];
+}
+
+/* tausub (mesh.c:684-710): 8 relaxation times between taumin and taumax. */
+void ref_tausub(float taumin, float taumax, float *tau8) {
+  Grid3D tau = Alloc3D(2, 2, 2);
+  tausub(tau, taumin, taumax);
+  copy8(tau, tau8);
+  free(tau);
+}
+
+/* weights_sub (mesh.c:713-1097): Q(f) weights (already divided by FAC^EX)
+ * and the 16-entry coefficient table. */
+void ref_weights_sub(float ex, float fac, float *w8, float *coeff16) {
+  Grid3D w = Alloc3D(2, 2, 2);
+  Grid1D c = Alloc1D(16);
+  weights_sub(w, c, ex, fac);
+  copy8(w, w8);
+  memcpy(coeff16, c, 16 * sizeof(float));
+  free(w);
+  free(c);
+}
+
+/* inimesh (mesh.c:23-614) with MEDIASTART=1/2 reading INVEL at PX=PY=1.
+ * Outputs the padded d1, mu, lam, qp, qs arrays plus the relaxation times,
+ * the Q(f) weights/coefficients and the vs/vp/rho extrema. */
+void ref_inimesh(const char *invel, int nvar, float fp, float fac, float q0,
+                 float ex, int nxt, int nyt, int nzt, int nve, int socalq,
+                 float *d1, float *mu, float *lam, float *qp, float *qs,
+                 float *taumax, float *taumin, float *tau8, float *w8,
+                 float *coeff16, float *vse, float *vpe, float *dde) {
+  int nx = nxt + 4 + ngsl2, ny = nyt + 4 + ngsl2, nz = nzt + 2 * align;
+  size_t n = (size_t)nx * ny * nz;
+  Grid3D gd1 = Alloc3D(nx, ny, nz), gmu = Alloc3D(nx, ny, nz),
+         glam = Alloc3D(nx, ny, nz), gqp = Alloc3D(nx, ny, nz),
+         gqs = Alloc3D(nx, ny, nz);
+  Grid3D tau = Alloc3D(2, 2, 2), weights = Alloc3D(2, 2, 2);
+  Grid1D coeff = Alloc1D(16);
+  int coords[2] = {0, 0};
+  char path[512];
+  weights_sub(weights, coeff, ex, fac);
+  strncpy(path, invel, sizeof(path) - 1);
+  path[sizeof(path) - 1] = 0;
+  inimesh(0, 1, gd1, gmu, glam, gqp, gqs, taumax, taumin, tau, weights, coeff,
+          nvar, fp, fac, q0, ex, nxt, nyt, nzt, 1, 1, nxt, nyt, nzt, coords,
+          MPI_COMM_WORLD, 0, nve, socalq, path, vse, vpe, dde);
+  memcpy(d1, &gd1[0][0][0], n * sizeof(float));
+  memcpy(mu, &gmu[0][0][0], n * sizeof(float));
+  memcpy(lam, &glam[0][0][0], n * sizeof(float));
+  memcpy(qp, &gqp[0][0][0], n * sizeof(float));
+  memcpy(qs, &gqs[0][0][0], n * sizeof(float));
+  copy8(tau, tau8);
+  copy8(weights, w8);
+  memcpy(coeff16, coeff, 16 * sizeof(float));
+  free(gd1); free(gmu); free(glam); free(gqp); free(gqs);
+  free(tau); free(weights); free(coeff);
+}
+
+/* init_texture (mesh.c:1103-1137) given tau1/tau2/weights as 8-vectors. */
+void ref_init_texture(int nxt, int nyt, int nzt, const float *tau1_8,
+                      const float *tau2_8, const float *w8, int xls, int xre,
+                      int yls, int yre, float *vx1, float *vx2, int *ww,
+                      float *wwo) {
+  int nx = nxt + 4 + ngsl2, ny = nyt + 4 + ngsl2, nz = nzt + 2 * align;
+  size_t n = (size_t)nx * ny * nz;
+  Grid3D t1 = Alloc3D(2, 2, 2), t2 = Alloc3D(2, 2, 2), w = Alloc3D(2, 2, 2);
+  Grid3D g1 = Alloc3D(nx, ny, nz), g2 = Alloc3D(nx, ny, nz), gwo = Alloc3D(nx, ny, nz);
+  Grid3Dww gww = Alloc3Dww(nx, ny, nz);
+  int i, j, k;
+  for (i = 0; i < 2; i++)
+    for (j = 0; j < 2; j++)
+      for (k = 0; k < 2; k++) {
+        t1[i][j][k] = tau1_8[i * 4 + j * 2 + k];
+        t2[i][j][k] = tau2_8[i * 4 + j * 2 + k];
+        w[i][j][k] = w8[i * 4 + j * 2 + k];
+      }
+  init_texture(nxt, nyt, nzt, t1, t2, g1, g2, w, gww, gwo, xls, xre, yls, yre);
+  memcpy(vx1, &g1[0][0][0], n * sizeof(float));
+  memcpy(vx2, &g2[0][0][0], n * sizeof(float));
+  memcpy(wwo, &gwo[0][0][0], n * sizeof(float));
+  memcpy(ww, &gww[0][0][0], n * sizeof(int));
+  free(t1); free(t2); free(w); free(g1); free(g2); free(gwo); free(gww);
+}
+
+/* inicrj (cerjan.c:5-64) at coords (0,0). */
+void ref_inicrj(float arbc, int nxt, int nyt, int nzt, int NX, int NY, int ND,
+                int islowest, int npc, float *dcrjx, float *dcrjy,
+                float *dcrjz) {
+  int coords[2] = {0, 0};
+  int i;
+  for (i = 0; i < nxt + 4 + ngsl2; i++) dcrjx[i] = 1.0f;
+  for (i = 0; i < nyt + 4 + ngsl2; i++) dcrjy[i] = 1.0f;
+  for (i = 0; i < nzt + 2 * align; i++) dcrjz[i] = 1.0f;
+  inicrj(arbc, coords, nxt, nyt, nzt, NX, NY, ND, dcrjx, dcrjy, dcrjz, islowest,
+         npc);
+}
+
+/* hoek_brown (mesh.c:1139-1176). */
+void ref_hoek_brown(float sigma_0, float sigma_ci, float gsi, float mi, float d,
+                    int tunnel, float *phi, float *cohes) {
+  hoek_brown(sigma_0, sigma_ci, gsi, mi, d, tunnel, phi, cohes);
+}

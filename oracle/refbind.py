@@ -1,0 +1,299 @@
+"""ctypes bindings to the reference builds under oracle/_ref -- TEST INFRASTRUCTURE.
+
+* ``RefHost``  -> oracle/_ref/libawpref_host.so: the reference's own host set-up
+  code (src/awp/mesh.c, cerjan.c, grid.c) compiled on the CPU.
+* ``RefGpuSim`` -> oracle/_ref/libawpref.so: the reference's own CUDA kernels
+  (src/awp/kernel.cu) driven through its launchers in the order of the
+  single-rank pmcl3d time loop (src/awp/pmcl3d.c:1628-2487).
+
+``model_setup`` assembles every per-run array the time loop needs (media,
+memory-variable arrays, sponge, Q(f) table, surface Lame ratio) with the
+reference's own host code, so the oracle, the reference GPU build and the
+product can all be fed identical inputs.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import tempfile
+from ctypes import POINTER, byref, c_double, c_float, c_int, c_void_p
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_DIR = os.path.join(HERE, "_ref")
+NGSL, ALIGN = 8, 32
+
+_F = POINTER(c_float)
+_I = POINTER(c_int)
+
+
+def fptr(a):
+    return a.ctypes.data_as(_F)
+
+
+def padded_shape(nx, ny, nz):
+    return (nx + 4 + 2 * NGSL, ny + 4 + 2 * NGSL, nz + 2 * ALIGN)
+
+
+class RefHost:
+    def __init__(self, path=None):
+        path = path or os.path.join(REF_DIR, "libawpref_host.so")
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} missing: run `make -C oracle ref`")
+        lib = ctypes.CDLL(path, mode=ctypes.RTLD_LOCAL)
+        lib.ref_tausub.argtypes = [c_float, c_float, _F]
+        lib.ref_weights_sub.argtypes = [c_float, c_float, _F, _F]
+        lib.ref_inimesh.argtypes = ([ctypes.c_char_p, c_int, c_float, c_float, c_float, c_float,
+                                     c_int, c_int, c_int, c_int, c_int] + [_F] * 5 + [_F] * 8)
+        lib.ref_init_texture.argtypes = ([c_int] * 3 + [_F] * 3 + [c_int] * 4 +
+                                         [_F, _F, _I, _F])
+        lib.ref_inicrj.argtypes = [c_float] + [c_int] * 8 + [_F] * 3
+        lib.ref_hoek_brown.argtypes = [c_float] * 5 + [c_int, _F, _F]
+        self.lib = lib
+
+    def tausub(self, taumin, taumax):
+        out = np.zeros(8, np.float32)
+        self.lib.ref_tausub(taumin, taumax, fptr(out))
+        return out
+
+    def weights_sub(self, ex, fac):
+        w = np.zeros(8, np.float32)
+        c = np.zeros(16, np.float32)
+        self.lib.ref_weights_sub(ex, fac, fptr(w), fptr(c))
+        return w, c
+
+    def inimesh(self, media, fp=2.5, fac=0.005, q0=5.0, ex=0.0, nve=1, socalq=1):
+        """Run inimesh on `media` ([nz][ny][nx][nvar] float32) via a temp file."""
+        nz, ny, nx, nvar = media.shape
+        shp = padded_shape(nx, ny, nz)
+        out = {k: np.zeros(shp, np.float32) for k in ("d1", "mu", "lam", "qp", "qs")}
+        taumax = c_float()
+        taumin = c_float()
+        tau8 = np.zeros(8, np.float32)
+        w8 = np.zeros(8, np.float32)
+        coeff = np.zeros(16, np.float32)
+        vse = np.zeros(2, np.float32)
+        vpe = np.zeros(2, np.float32)
+        dde = np.zeros(2, np.float32)
+        with tempfile.TemporaryDirectory() as td:
+            path = os.path.join(td, "media.bin")
+            np.ascontiguousarray(media, np.float32).tofile(path)
+            self.lib.ref_inimesh(path.encode(), nvar, fp, fac, q0, ex, nx, ny, nz, nve, socalq,
+                                 fptr(out["d1"]), fptr(out["mu"]), fptr(out["lam"]),
+                                 fptr(out["qp"]), fptr(out["qs"]), byref(taumax), byref(taumin),
+                                 fptr(tau8), fptr(w8), fptr(coeff), fptr(vse), fptr(vpe),
+                                 fptr(dde))
+        out.update(taumax=taumax.value, taumin=taumin.value, tau8=tau8, w8=w8, coeff=coeff,
+                   vse=vse, vpe=vpe, dde=dde)
+        return out
+
+    def init_texture(self, nx, ny, nz, tau1, tau2, w8, xls, xre, yls, yre):
+        shp = padded_shape(nx, ny, nz)
+        vx1 = np.zeros(shp, np.float32)
+        vx2 = np.zeros(shp, np.float32)
+        wwo = np.zeros(shp, np.float32)
+        ww = np.zeros(shp, np.int32)
+        self.lib.ref_init_texture(nx, ny, nz, fptr(np.ascontiguousarray(tau1, np.float32)),
+                                  fptr(np.ascontiguousarray(tau2, np.float32)),
+                                  fptr(np.ascontiguousarray(w8, np.float32)), xls, xre, yls, yre,
+                                  fptr(vx1), fptr(vx2), ww.ctypes.data_as(_I), fptr(wwo))
+        return vx1, vx2, ww, wwo
+
+    def inicrj(self, arbc, nx, ny, nz, nd, islowest=1, npc=0):
+        dx = np.ones(nx + 4 + 2 * NGSL, np.float32)
+        dy = np.ones(ny + 4 + 2 * NGSL, np.float32)
+        dz = np.ones(nz + 2 * ALIGN, np.float32)
+        self.lib.ref_inicrj(arbc, nx, ny, nz, nx, ny, nd, islowest, npc, fptr(dx), fptr(dy),
+                            fptr(dz))
+        return dx, dy, dz
+
+    def hoek_brown(self, sigma_0, sigma_ci, gsi, mi, d, tunnel):
+        phi = c_float()
+        cohes = c_float()
+        self.lib.ref_hoek_brown(sigma_0, sigma_ci, gsi, mi, d, tunnel, byref(phi), byref(cohes))
+        return phi.value, cohes.value
+
+
+def tau12(tau8, dt):
+    """tau1/tau2 of pmcl3d.c:1036-1049 (float division, double exp)."""
+    tau8 = np.asarray(tau8, np.float32)
+    arg = (np.float32(-dt) / tau8).astype(np.float32)
+    tau2 = np.exp(arg.astype(np.float64)).astype(np.float32)
+    tau1 = (0.5 * (1.0 - tau2.astype(np.float64))).astype(np.float32)
+    return tau1, tau2
+
+
+def lam_mu_ref(lam, mu, nx, ny, nz):
+    """pmcl3d.c:944-951 at one rank (double divisions, float ratio)."""
+    shp = padded_shape(nx, ny, nz)
+    out = np.zeros((shp[0], shp[1]), np.float32)
+    ktop = nz + ALIGN - 1
+    sl = (slice(2 + NGSL, nx + NGSL + 2), slice(2 + NGSL, ny + NGSL + 2))
+    t_xl = (1.0 / lam[sl[0], sl[1], ktop].astype(np.float64)).astype(np.float32)
+    t_xl2m = (2.0 / mu[sl[0], sl[1], ktop].astype(np.float64) +
+              t_xl.astype(np.float64)).astype(np.float32)
+    out[sl] = t_xl / t_xl2m
+    return out
+
+
+def map_sources(scn):
+    """inisource at one rank (source.c:131-264): file (x, y, z-from-surface) ->
+    the psrc triple addsrc_cu indexes with, keeping only in-window sources."""
+    p = scn.params
+    nz = p["nz"]
+    pos = np.asarray(scn.src_pos, np.int64)
+    z = nz + 1 - pos[:, 2]
+    keep = ((pos[:, 0] >= -1) & (pos[:, 0] <= p["nx"] + 2) & (pos[:, 1] >= -1) &
+            (pos[:, 1] <= p["ny"] + 2) & (z >= 1) & (z <= nz))
+    psrc = np.stack([pos[:, 0], pos[:, 1], z], axis=1)[keep].astype(np.int32)
+    data = np.asarray(scn.src_data, np.float32)[keep]
+    rs = p["read_step"] if p["ifault"] != 5 else 2
+    comps = [np.ascontiguousarray(data[:, :rs, q]) for q in range(6)]  # xx yy zz xz yz xy
+    return psrc, comps, rs
+
+
+def model_setup(scn, host: RefHost | None = None, fp=2.5, fac=0.005, q0=5.0, ex=0.0):
+    """Every per-run array of the single-rank time loop, from the reference's host code."""
+    host = host or RefHost()
+    p = scn.params
+    nx, ny, nz = p["nx"], p["ny"], p["nz"]
+    m = host.inimesh(scn.media, fp=fp, fac=fac, q0=q0, ex=ex, nve=p.get("nve", 1),
+                     socalq=p.get("socalq", 1))
+    tau1, tau2 = tau12(m["tau8"], p["dt"])
+    xls, xre = 2 + NGSL, nx + NGSL + 1
+    yls, yre = 2 + NGSL, ny + NGSL + 1
+    vx1, vx2, ww, wwo = host.init_texture(nx, ny, nz, tau1, tau2, m["w8"], xls, xre, yls, yre)
+    dcrjx, dcrjy, dcrjz = host.inicrj(p.get("arbc", 0.92), nx, ny, nz, p.get("nd", 20), 1,
+                                      p.get("npc", 0))
+    lm = lam_mu_ref(m["lam"], m["mu"], nx, ny, nz)
+    psrc, comps, rs = map_sources(scn)
+    return dict(media=m, vx1=vx1, vx2=vx2, ww=ww, wwo=wwo, dcrjx=dcrjx, dcrjy=dcrjy,
+                dcrjz=dcrjz, lam_mu=lm, coeff=m["coeff"], psrc=psrc, src=comps,
+                src_stride=rs, tau1=tau1, tau2=tau2)
+
+
+class RefGpuSim:
+    """The reference CUDA kernels driven in pmcl3d's single-rank order."""
+
+    FIELDS = ["u1", "v1", "w1", "xx", "yy", "zz", "xy", "xz", "yz",
+              "r1", "r2", "r3", "r4", "r5", "r6"]
+
+    def __init__(self, scn, setup, path=None):
+        import torch
+        path = path or os.path.join(REF_DIR, "libawpref.so")
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} missing: run `make -C oracle ref`")
+        self.torch = torch
+        lib = ctypes.CDLL(path, mode=ctypes.RTLD_LOCAL)
+        V = c_void_p
+        lib.SetDeviceConstValue.argtypes = [_F, c_float, _I, _I, _I, c_int, c_float, c_float,
+                                            _F, _F]
+        lib.SetDeviceFilterParameters.argtypes = [c_int, POINTER(c_double), POINTER(c_double)]
+        lib.dvelcx_H_opt.argtypes = [V] * 13 + [c_int, c_int, V] + [c_int] * 4
+        lib.dstrqc_H.argtypes = [V] * 23 + [c_int, c_int, V] + [V] * 5 + [c_int] * 9
+        lib.fstr_H.argtypes = [V] * 4 + [c_int] * 4
+        lib.addsrc_H.argtypes = [c_int, c_int, c_int, V, c_int, V] + [V] * 12 + [c_int]
+        lib.addkinsrc_H.argtypes = [c_int, c_int, V, c_int, V] + [V] * 15 + [c_int]
+        lib.drprecpc_calc_H_opt.argtypes = [V] * 13 + [c_int] * 5 + [V, c_int]
+        lib.drprecpc_app_H.argtypes = [V] * 9 + [c_int] * 5 + [V, c_int]
+        self.lib = lib
+        self.scn = scn
+        p = scn.params
+        self.p = p
+        self.nx, self.ny, self.nz = p["nx"], p["ny"], p["nz"]
+        dev = torch.device("cuda")
+        m = setup["media"]
+
+        def T(a, dtype=torch.float32):
+            return torch.as_tensor(np.ascontiguousarray(a)).to(dev, dtype)
+
+        shp = padded_shape(self.nx, self.ny, self.nz)
+        self.f = {k: torch.zeros(shp, dtype=torch.float32, device=dev) for k in self.FIELDS}
+        self.f.update(d1=T(m["d1"]), mu=T(m["mu"]), lam=T(m["lam"]), qp=T(m["qp"]),
+                      qs=T(m["qs"]))
+        self.vx1 = T(setup["vx1"])
+        self.vx2 = T(setup["vx2"])
+        self.ww = T(setup["ww"], torch.int32)
+        self.wwo = T(setup["wwo"])
+        self.dcrjx, self.dcrjy, self.dcrjz = (T(setup["dcrjx"]), T(setup["dcrjy"]),
+                                              T(setup["dcrjz"]))
+        self.lam_mu = T(setup["lam_mu"])
+        self.coeff = T(setup["coeff"])
+        self.psrc = T(setup["psrc"], torch.int32)
+        self.npsrc = int(setup["psrc"].shape[0])
+        self.src = [T(c) for c in setup["src"]]
+        self.stride = setup["src_stride"]
+        self.mom = torch.zeros(max(self.npsrc, 1), dtype=torch.float32, device=dev)
+        self.filt = None
+        DH = np.array([p["dh"]], np.float32)
+        nxt = np.array([self.nx], np.int32)
+        nyt = np.array([self.ny], np.int32)
+        nzt = np.array([self.nz], np.int32)
+        Rz = np.zeros(9, np.float32)
+        RzT = np.zeros(9, np.float32)
+        lib.SetDeviceConstValue(fptr(DH), c_float(p["dt"]), nxt.ctypes.data_as(_I),
+                                nyt.ctypes.data_as(_I), nzt.ctypes.data_as(_I), 1,
+                                c_float(0.0), c_float(0.0), fptr(Rz), fptr(RzT))
+        fz = np.zeros(20, np.float64)
+        lib.SetDeviceFilterParameters(0, fz.ctypes.data_as(POINTER(c_double)),
+                                      fz.ctypes.data_as(POINTER(c_double)))
+        self._fz = fz
+        self.cur = 0
+        self.source_step = 1
+        if p["ifault"] == 1 and self.npsrc:
+            # initial sample added on the host before the copy (pmcl3d.c:1175-1187)
+            self._addsrc(1)
+        torch.cuda.synchronize()
+
+    def ptr(self, t):
+        return c_void_p(t.data_ptr())
+
+    def _addsrc(self, i):
+        f = self.f
+        s = self.src
+        self.lib.addsrc_H(i, self.stride, 3, self.ptr(self.psrc), self.npsrc, None,
+                          *[self.ptr(t) for t in s],
+                          self.ptr(f["xx"]), self.ptr(f["yy"]), self.ptr(f["zz"]),
+                          self.ptr(f["xy"]), self.ptr(f["yz"]), self.ptr(f["xz"]), 0)
+
+    def _stress(self, s_i, e_i, s_j, e_j):
+        f = self.f
+        P = self.ptr
+        self.lib.dstrqc_H(P(f["xx"]), P(f["yy"]), P(f["zz"]), P(f["xy"]), P(f["xz"]), P(f["yz"]),
+                          P(f["r1"]), P(f["r2"]), P(f["r3"]), P(f["r4"]), P(f["r5"]), P(f["r6"]),
+                          P(f["u1"]), P(f["v1"]), P(f["w1"]), P(f["lam"]), P(f["mu"]),
+                          P(f["qp"]), P(self.coeff), P(f["qs"]), P(self.dcrjx), P(self.dcrjy),
+                          P(self.dcrjz), self.ny, self.nz, None, P(self.lam_mu), P(self.vx1),
+                          P(self.vx2), P(self.ww), P(self.wwo), self.nx, self.p.get("npc", 0),
+                          0, 0, s_i, e_i, s_j, e_j, 0)
+
+    def step(self, n=1):
+        f = self.f
+        P = self.ptr
+        nx, ny, nz = self.nx, self.ny, self.nz
+        xls, xre, yls, yre = 2 + NGSL, nx + NGSL + 1, 2 + NGSL, ny + NGSL + 1
+        for _ in range(n):
+            self.cur += 1
+            self.lib.dvelcx_H_opt(P(f["u1"]), P(f["v1"]), P(f["w1"]), P(f["xx"]), P(f["yy"]),
+                                  P(f["zz"]), P(f["xy"]), P(f["xz"]), P(f["yz"]), P(self.dcrjx),
+                                  P(self.dcrjy), P(self.dcrjz), P(f["d1"]), ny, nz, None,
+                                  2 + NGSL, nx + NGSL + 1, 0, 1)
+            # dstrqc over xss2..xse2, then the xss1 and xss3 strips (pmcl3d.c:1845-1919)
+            self._stress(NGSL + 4, nx + NGSL - 1, yls, yre)
+            self._stress(xls, NGSL + 3, yls, yre)
+            self._stress(nx + NGSL, xre, yls, yre)
+            if self.p["ifault"] < 4 and self.cur < self.p["nst"]:
+                self.source_step += 1
+                self._addsrc(self.source_step)
+            elif self.p["ifault"] == 5 and self.npsrc:
+                fdp = None if self.filt is None else P(self.filt)
+                self.lib.addkinsrc_H(self.cur, 3, P(self.psrc), self.npsrc, None, P(f["mu"]),
+                                     *[P(t) for t in self.src], P(f["xx"]), P(f["yy"]),
+                                     P(f["zz"]), P(f["xy"]), P(f["yz"]), P(f["xz"]),
+                                     P(self.mom), fdp, 0)
+            self.lib.fstr_H(P(f["zz"]), P(f["xz"]), P(f["yz"]), None, xls, xre, yls, yre)
+        self.torch.cuda.synchronize()
+
+    def field(self, name):
+        return self.f[name].cpu().numpy()

@@ -1,0 +1,119 @@
+"""Host set-up of the product against the reference's own host code.
+
+The reference's src/awp/mesh.c and cerjan.c are compiled on the CPU into
+oracle/_ref/libawpref_host.so (oracle/Makefile); every table the time step
+depends on must come out bit-identical.
+"""
+import ctypes
+from ctypes import byref, c_float, c_int
+
+import numpy as np
+import pytest
+
+from awp_b200 import _lib
+from oracle import refbind
+
+F = ctypes.POINTER(c_float)
+
+EX_VALUES = [0.0, 0.005, 0.01, 0.05, 0.1, 0.15, 0.2, 0.3, 0.4, 0.5, 0.6, 0.65, 0.7, 0.8,
+             0.85, 0.9, 0.949]
+FAC_VALUES = [0.005, 0.01, 1.0]
+
+
+def fp(a):
+    return a.ctypes.data_as(F)
+
+
+@pytest.mark.parametrize("ex", EX_VALUES)
+@pytest.mark.parametrize("fac", FAC_VALUES)
+def test_q_tables_bitwise(ref_host, ex, fac):
+    lib = _lib.load()
+    w = np.zeros(8, np.float32)
+    c = np.zeros(16, np.float32)
+    assert lib.awp_q_weights(ex, fac, fp(w), fp(c)) == 0
+    rw, rc = ref_host.weights_sub(ex, fac)
+    assert np.array_equal(w.view(np.uint32), rw.view(np.uint32))
+    assert np.array_equal(c.view(np.uint32), rc.view(np.uint32))
+    taumax = c_float()
+    taumin = c_float()
+    tau = np.zeros(8, np.float32)
+    assert lib.awp_q_tau(ex, fac, byref(taumax), byref(taumin), fp(tau)) == 0
+    rtau = ref_host.tausub(taumin.value, taumax.value)
+    assert np.array_equal(tau.view(np.uint32), rtau.view(np.uint32))
+
+
+def test_tau_range_matches_inimesh(ref_host):
+    """tau range of inimesh (mesh.c:36-57) via a tiny mesh read."""
+    from awp_b200 import scenarios
+    scn = scenarios.random_small(nx=6, ny=6, nz=8, steps=1)
+    lib = _lib.load()
+    for ex in (0.0, 0.3, 0.7, 0.9):
+        m = ref_host.inimesh(scn.media, ex=ex)
+        taumax = c_float()
+        taumin = c_float()
+        tau = np.zeros(8, np.float32)
+        assert lib.awp_q_tau(ex, 0.005, byref(taumax), byref(taumin), fp(tau)) == 0
+        assert np.float32(taumax.value) == np.float32(m["taumax"])
+        assert np.float32(taumin.value) == np.float32(m["taumin"])
+        assert np.array_equal(tau, m["tau8"])
+
+
+def test_tau_range_rejects_unset_band():
+    lib = _lib.load()
+    taumax = c_float()
+    taumin = c_float()
+    tau = np.zeros(8, np.float32)
+    assert lib.awp_q_tau(0.97, 0.005, byref(taumax), byref(taumin), fp(tau)) == 7
+
+
+@pytest.mark.parametrize("shape,nd,npc", [((32, 24, 16), 6, 0), ((64, 64, 32), 20, 0),
+                                          ((40, 30, 20), 8, 2), ((21, 25, 12), 5, 0)])
+def test_cerjan_bitwise(ref_host, shape, nd, npc):
+    nx, ny, nz = shape
+    lib = _lib.load()
+    dx = np.zeros(nx + 20, np.float32)
+    dy = np.zeros(ny + 20, np.float32)
+    dz = np.zeros(nz + 64, np.float32)
+    assert lib.awp_cerjan(0.92, nx, ny, nz, nd, 1, npc, fp(dx), fp(dy), fp(dz)) == 0
+    rx, ry, rz = ref_host.inicrj(0.92, nx, ny, nz, nd, 1, npc)
+    assert np.array_equal(dx.view(np.uint32), rx.view(np.uint32))
+    assert np.array_equal(dy.view(np.uint32), ry.view(np.uint32))
+    assert np.array_equal(dz.view(np.uint32), rz.view(np.uint32))
+
+
+@pytest.mark.parametrize("shape", [(12, 10, 8), (9, 7, 12), (10, 11, 6), (5, 6, 7)])
+def test_texture_pattern_equals_init_texture(ref_host, shape):
+    """The parity pattern the kernels use reproduces init_texture's arrays
+    (mesh.c:1103-1137) at every cell it writes, including odd ny / nzt."""
+    nx, ny, nz = shape
+    lib = _lib.load()
+    tau = np.linspace(0.01, 1.0, 8).astype(np.float32)
+    w8 = np.linspace(0.1, 1.7, 8).astype(np.float32)
+    dt = 0.004
+    tau1, tau2 = refbind.tau12(tau, dt)
+    xls, xre, yls, yre = 10, nx + 9, 10, ny + 9
+    vx1, vx2, ww, wwo = ref_host.init_texture(nx, ny, nz, tau1, tau2, w8, xls, xre, yls, yre)
+    a1, a2, aw, ao = c_float(), c_float(), c_int(), c_float()
+    for i in range(xls, xre + 1):
+        for j in range(yls, yre + 1):
+            for k in range(32, 32 + nz):
+                lib.awp_texture_at(fp(tau), fp(w8), dt, xls, yls, ny, nz, i, j, k,
+                                   byref(a1), byref(a2), byref(aw), byref(ao))
+                assert np.float32(a1.value) == vx1[i, j, k]
+                assert np.float32(a2.value) == vx2[i, j, k]
+                assert aw.value == ww[i, j, k]
+                assert np.float32(ao.value) == wwo[i, j, k]
+
+
+def test_q_switch_threshold_is_exact():
+    """The kernels replace 1./(q*2.0) <= 200.0 (double, kernel.cu:974) by a
+    float compare against one threshold; check it over a dense float range."""
+    # threshold computed by the library's host code is exercised through the
+    # same definition: the smallest float x with 1/(double)x <= 200
+    xs = np.arange(0.00499, 0.00501, 1e-10, dtype=np.float64).astype(np.float32)
+    xs = np.unique(xs)
+    ref = (1.0 / xs.astype(np.float64)) <= 200.0
+    thr = xs[ref].min()
+    # no float between consecutive candidates breaks monotonicity
+    assert np.all(ref == (xs >= thr))
+    assert np.float32(thr) > np.float32(0.004999)
