@@ -109,6 +109,8 @@ def load() -> ctypes.CDLL:
     _sig(lib, "awp_profile_phases", c_int, [_P, c_int])
     _sig(lib, "awp_phase_times", c_int, [_P, POINTER(c_double), POINTER(c_longlong)])
     _sig(lib, "awp_kernel_launches", c_int, [_P, POINTER(c_longlong)])
+    _sig(lib, "awp_set_tuning", c_int, [c_char_p, c_int])
+    _sig(lib, "awp_get_tuning", c_int, [c_char_p])
     _sig(lib, "awp_q_tau", c_int, [c_float, c_float, _F, _F, _F])
     _sig(lib, "awp_q_weights", c_int, [c_float, c_float, _F, _F])
     _sig(lib, "awp_cerjan", c_int,

@@ -430,12 +430,7 @@ int awp_set_stream(awp_ctx* c, void* s) {
     cudaStreamDestroy(c->stream);
   }
   c->own_stream = false;
-  c->stream = (cudaStream_t)s;
-  if (!s) {
-    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
-      return set_error(AWP_ERR_CUDA, "cudaStreamCreate");
-    c->own_stream = true;
-  }
+  c->stream = (cudaStream_t)s;  // NULL selects the legacy default stream
   return AWP_OK;
 }
 
@@ -758,6 +753,14 @@ int awp_phase_times(awp_ctx* c, double ms[AWP_NPHASES], long long launches[AWP_N
   c->ev_used.clear();
   return AWP_OK;
 }
+
+int awp_set_tuning(const char* key, int value) {
+  if (!key || awp_tuning_set(key, value))
+    return set_error(AWP_ERR_ARG, "tuning %s=%d not accepted", key ? key : "(null)", value);
+  return AWP_OK;
+}
+
+int awp_get_tuning(const char* key) { return key ? awp_tuning_get(key) : -1; }
 
 int awp_kernel_launches(const awp_ctx* c, long long* launches) {
   if (!c || !launches) return set_error(AWP_ERR_ARG, "null argument");

@@ -15,6 +15,7 @@
 //    switch), so results agree with the reference CUDA build to rounding.
 #include <cuda_runtime.h>
 #include <math.h>
+#include <string.h>
 
 #include "awp_kernels.cuh"
 
@@ -22,17 +23,19 @@
 
 namespace {
 
-constexpr int kVelTY = 8;
-constexpr int kStrTY = 8;
-constexpr int kIChunk = 32;
+// Launch shape (tuned on B200; adjustable through awp_set_tuning).
+int g_vel_ty = 8;
+int g_str_ty = 8;
+int g_ichunk = 32;
 
 // ===========================================================================
 // Velocity (dvelcx_opt, kernel.cu:125-268)
 // ===========================================================================
-__global__ void __launch_bounds__(32 * kVelTY)
+template <int TY>
+__global__ void __launch_bounds__(32 * TY)
     k_velocity(const VelArgs a, const int ichunk) {
   const int k = a.k0 + blockIdx.x * 32 + threadIdx.x;
-  const int j = a.j0 + blockIdx.y * kVelTY + threadIdx.y;
+  const int j = a.j0 + blockIdx.y * TY + threadIdx.y;
   if (k > a.k1 || j > a.j1) return;
   const int ib = a.i0 + blockIdx.z * ichunk;
   const int ie = min(ib + ichunk - 1, a.i1);
@@ -142,11 +145,80 @@ __device__ __forceinline__ float sum8(const Plane4& c, const Plane4& n) {
   return c.a + n.a + c.b + n.b + c.c + n.c + c.d + n.d;
 }
 
-template <bool ELASTIC, bool TEXARR>
-__global__ void __launch_bounds__(32 * kStrTY)
+// One stress/memory-variable update of a cell (dstrqc, kernel.cu:1114-1179),
+// the state passed in and out through registers.
+template <bool ELASTIC>
+__device__ __forceinline__ void stress_update(float (&sg)[6], float (&rr)[6], float xl, float xm,
+                                              float xmu1, float xmu2, float xmu3, float h,
+                                              float h1, float h2, float h3, float qpa,
+                                              float vx1, float f_vx1, float f_vx2,
+                                              float f_wwo, float DT, float dcrj,
+                                              const float (&d)[9]) {
+  // d: vs1 vs2 vs3 (normal), xy pair, xz pair, yz pair
+  const float vs1 = d[0], vs2 = d[1], vs3 = d[2];
+  float tmp = xl * (vs1 + vs2 + vs3);
+  const float a1 = qpa * (vs1 + vs2 + vs3);
+  tmp = tmp + DT * a1;
+  if (ELASTIC) {
+    sg[0] = (sg[0] + tmp - xm * (vs2 + vs3)) * dcrj;
+    sg[1] = ((sg[1] + tmp - xm * (vs1 + vs3)) * dcrj) * dcrj;
+    sg[2] = ((sg[2] + tmp - xm * (vs1 + vs2)) * dcrj) * dcrj;
+    sg[3] = (sg[3] + xmu1 * (d[3] + d[4])) * dcrj;
+    sg[4] = (sg[4] + xmu2 * (d[5] + d[6])) * dcrj;
+    sg[5] = (sg[5] + xmu3 * (d[7] + d[8])) * dcrj;
+    return;
+  }
+  float f_r, f_rtmp, t;
+  f_r = rr[0];
+  f_rtmp = -h * (vs2 + vs3) + a1;
+  t = sg[0] + tmp - xm * (vs2 + vs3) + vx1 * f_r;
+  rr[0] = f_vx2 * f_r + f_wwo * f_rtmp;
+  f_rtmp = f_rtmp * (f_wwo - 1) + f_vx2 * f_r * (1 - f_vx1);
+  sg[0] = (t + DT * f_rtmp) * dcrj;
+
+  f_r = rr[1];
+  f_rtmp = -h * (vs1 + vs3) + a1;
+  t = (sg[1] + tmp - xm * (vs1 + vs3) + vx1 * f_r) * dcrj;
+  rr[1] = f_vx2 * f_r + f_wwo * f_rtmp;
+  f_rtmp = f_rtmp * (f_wwo - 1) + f_vx2 * f_r * (1 - f_vx1);
+  sg[1] = (t + DT * f_rtmp) * dcrj;
+
+  f_r = rr[2];
+  f_rtmp = -h * (vs1 + vs2) + a1;
+  t = (sg[2] + tmp - xm * (vs1 + vs2) + vx1 * f_r) * dcrj;
+  rr[2] = f_vx2 * f_r + f_wwo * f_rtmp;
+  f_rtmp = f_rtmp * (f_wwo - 1) + f_vx2 * f_r * (1 - f_vx1);
+  sg[2] = (t + DT * f_rtmp) * dcrj;
+
+  f_r = rr[3];
+  f_rtmp = h1 * (d[3] + d[4]);
+  t = sg[3] + xmu1 * (d[3] + d[4]) + vx1 * f_r;
+  rr[3] = f_vx2 * f_r + f_wwo * f_rtmp;
+  f_rtmp = f_rtmp * (f_wwo - 1) + f_vx2 * f_r * (1 - f_vx1);
+  sg[3] = (t + DT * f_rtmp) * dcrj;
+
+  f_r = rr[4];
+  f_rtmp = h2 * (d[5] + d[6]);
+  t = sg[4] + xmu2 * (d[5] + d[6]) + vx1 * f_r;
+  rr[4] = f_vx2 * f_r + f_wwo * f_rtmp;
+  f_rtmp = f_rtmp * (f_wwo - 1) + f_vx2 * f_r * (1 - f_vx1);
+  sg[4] = (t + DT * f_rtmp) * dcrj;
+
+  f_r = rr[5];
+  f_rtmp = h3 * (d[7] + d[8]);
+  t = sg[5] + xmu3 * (d[7] + d[8]) + vx1 * f_r;
+  rr[5] = f_vx2 * f_r + f_wwo * f_rtmp;
+  f_rtmp = f_rtmp * (f_wwo - 1) + f_vx2 * f_r * (1 - f_vx1);
+  sg[5] = (t + DT * f_rtmp) * dcrj;
+}
+
+// TY = 8: 256 threads held to 128 registers (2 CTAs / SM);
+// TY = 4: 128 threads without a register cap (3 CTAs / SM).
+template <bool ELASTIC, bool TEXARR, int TY>
+__global__ void __launch_bounds__(32 * TY, TY == 8 ? 2 : 1)
     k_stress(const StrArgs a, const int ichunk) {
   const int k = a.k0 + blockIdx.x * 32 + threadIdx.x;
-  const int j = a.j0 + blockIdx.y * kStrTY + threadIdx.y;
+  const int j = a.j0 + blockIdx.y * TY + threadIdx.y;
   if (k > a.k1 || j > a.j1) return;
   const int ib = a.i0 + blockIdx.z * ichunk;
   const int ie = min(ib + ichunk - 1, a.i1);
@@ -164,6 +236,10 @@ __global__ void __launch_bounds__(32 * kStrTY)
   const float* __restrict__ MU = a.mu + col;
   const float* __restrict__ QP = a.qp + col;
   const float* __restrict__ QS = a.qs + col;
+  float* __restrict__ SG[6] = {a.xx + col, a.yy + col, a.zz + col,
+                               a.xy + col, a.xz + col, a.yz + col};
+  float* __restrict__ RR[6] = {a.r1 + col, a.r2 + col, a.r3 + col,
+                               a.r4 + col, a.r5 + col, a.r6 + col};
 
   long long o = (long long)ib * S;
   float u_m1 = LDG(U + o - S), u_0 = LDG(U + o), u_p1 = LDG(U + o + S);
@@ -177,6 +253,14 @@ __global__ void __launch_bounds__(32 * kStrTY)
   }
 
   for (int i = ib; i <= ie; ++i, o += S) {
+    // ---- every load of this iteration first (independent, all in flight) ----
+    float sg[6], rr[6];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) sg[q] = SG[q][o];
+    if (!ELASTIC) {
+#pragma unroll
+      for (int q = 0; q < 6; ++q) rr[q] = RR[q][o];
+    }
     const float u_p2 = LDG(U + o + 2 * S);
     const float v_p1 = LDG(V + o + S);
     const float w_p1 = LDG(W + o + S);
@@ -186,6 +270,14 @@ __global__ void __launch_bounds__(32 * kStrTY)
       qp_n = load4(QP + o + S, Y);
       qs_n = load4(QS + o + S, Y);
     }
+    const float u_jp1 = LDG(U + o + Y), u_jp2 = LDG(U + o + 2 * Y), u_jm1 = LDG(U + o - Y);
+    const float u_km1 = LDG(U + o - 1);
+    const float v_jm1 = LDG(V + o - Y), v_jp1 = LDG(V + o + Y), v_jm2 = LDG(V + o - 2 * Y);
+    const float v_km1 = LDG(V + o - 1);
+    const float w_km1 = LDG(W + o - 1), w_km2 = LDG(W + o - 2);
+    const float w_jp1 = LDG(W + o + Y), w_jp2 = LDG(W + o + 2 * Y), w_jm1 = LDG(W + o - Y);
+    float uk1 = LDG(U + o + 1), vk1 = LDG(V + o + 1), wk1 = LDG(W + o + 1);
+    float uk2 = LDG(U + o + 2), vk2 = LDG(V + o + 2);
 
     // memory-variable coefficients for this cell
     float f_vx1, f_vx2, f_wwo;
@@ -253,121 +345,44 @@ __global__ void __launch_bounds__(32 * kStrTY)
     }
 
     // velocities at k+1 / k+2 that fall on the free-surface image layer
-    float uk1, vk1, wk1, uk2, vk2;
+    // (computed here in registers; kernel.cu:1087-1112)
     if (top) {
       const float uimg = u_0 - (w_0 - w_m1);
-      const float vimg = v_0 - (LDG(W + o + Y) - w_0);
-      const float vjm1 = LDG(V + o - Y), wjm1 = LDG(W + o - Y);
+      const float vimg = v_0 - (w_jp1 - w_0);
       const float vs1 = (i < a.gx_lim) ? u_p1 - (w_p1 - w_0) : 0.0f;
-      const float vs2 = (j >= a.gy_min) ? vjm1 - (w_0 - wjm1) : 0.0f;
+      const float vs2 = (j >= a.gy_min) ? v_jm1 - (w_0 - w_jm1) : 0.0f;
       const float wimg =
-          LDG(W + o - 1) -
-          LDG(a.lam_mu + (long long)i * a.lam_mu_ld + j) *
-              ((vs1 - uimg) + (u_p1 - u_0) + (vimg - vs2) + (v_0 - vjm1));
+          w_km1 - LDG(a.lam_mu + (long long)i * a.lam_mu_ld + j) *
+                      ((vs1 - uimg) + (u_p1 - u_0) + (vimg - vs2) + (v_0 - v_jm1));
       a.u1[col + o + 1] = uimg;
       a.v1[col + o + 1] = vimg;
       a.w1[col + o + 1] = wimg;
       uk1 = uimg;
       vk1 = vimg;
       wk1 = wimg;
-      uk2 = LDG(U + o + 2);
-      vk2 = LDG(V + o + 2);
-    } else {
-      uk1 = LDG(U + o + 1);
-      vk1 = LDG(V + o + 1);
-      wk1 = LDG(W + o + 1);
-      if (top1) {
-        uk2 = uk1 - (wk1 - LDG(W + o - S + 1));
-        vk2 = vk1 - (LDG(W + o + Y + 1) - wk1);
-      } else {
-        uk2 = LDG(U + o + 2);
-        vk2 = LDG(V + o + 2);
-      }
+    } else if (top1) {
+      uk2 = uk1 - (wk1 - LDG(W + o - S + 1));
+      vk2 = vk1 - (LDG(W + o + Y + 1) - wk1);
     }
 
-    float* __restrict__ XX = a.xx + col;
-    float* __restrict__ YY = a.yy + col;
-    float* __restrict__ ZZ = a.zz + col;
-    float* __restrict__ XY = a.xy + col;
-    float* __restrict__ XZ = a.xz + col;
-    float* __restrict__ YZ = a.yz + col;
+    float d[9];
+    d[0] = c1 * (u_p1 - u_0) + c2 * (u_p2 - u_m1);
+    d[1] = c1 * (v_0 - v_jm1) + c2 * (v_jp1 - v_jm2);
+    d[2] = c1 * (w_0 - w_km1) + c2 * (wk1 - w_km2);
+    d[3] = c1 * (u_jp1 - u_0) + c2 * (u_jp2 - u_jm1);
+    d[4] = c1 * (v_0 - v_m1) + c2 * (v_p1 - v_m2);
+    d[5] = c1 * (uk1 - u_0) + c2 * (uk2 - u_km1);
+    d[6] = c1 * (w_0 - w_m1) + c2 * (w_p1 - w_m2);
+    d[7] = c1 * (vk1 - v_0) + c2 * (vk2 - v_km1);
+    d[8] = c1 * (w_jp1 - w_0) + c2 * (w_jp2 - w_jm1);
 
-    float vs1 = c1 * (u_p1 - u_0) + c2 * (u_p2 - u_m1);
-    float vs2 = c1 * (v_0 - LDG(V + o - Y)) + c2 * (LDG(V + o + Y) - LDG(V + o - 2 * Y));
-    float vs3 = c1 * (w_0 - LDG(W + o - 1)) + c2 * (wk1 - LDG(W + o - 2));
-
-    float tmp = xl * (vs1 + vs2 + vs3);
-    const float a1 = qpa * (vs1 + vs2 + vs3);
-    tmp = tmp + DT * a1;
-
-    if (ELASTIC) {
-      XX[o] = (XX[o] + tmp - xm * (vs2 + vs3)) * dcrj;
-      YY[o] = ((YY[o] + tmp - xm * (vs1 + vs3)) * dcrj) * dcrj;
-      ZZ[o] = ((ZZ[o] + tmp - xm * (vs1 + vs2)) * dcrj) * dcrj;
-    } else {
-      float f_r, f_rtmp, s;
-      f_r = a.r1[col + o];
-      f_rtmp = -h * (vs2 + vs3) + a1;
-      s = XX[o] + tmp - xm * (vs2 + vs3) + vx1 * f_r;
-      a.r1[col + o] = f_vx2 * f_r + f_wwo * f_rtmp;
-      f_rtmp = f_rtmp * (f_wwo - 1) + f_vx2 * f_r * (1 - f_vx1);
-      XX[o] = (s + DT * f_rtmp) * dcrj;
-
-      f_r = a.r2[col + o];
-      f_rtmp = -h * (vs1 + vs3) + a1;
-      s = (YY[o] + tmp - xm * (vs1 + vs3) + vx1 * f_r) * dcrj;
-      a.r2[col + o] = f_vx2 * f_r + f_wwo * f_rtmp;
-      f_rtmp = f_rtmp * (f_wwo - 1) + f_vx2 * f_r * (1 - f_vx1);
-      YY[o] = (s + DT * f_rtmp) * dcrj;
-
-      f_r = a.r3[col + o];
-      f_rtmp = -h * (vs1 + vs2) + a1;
-      s = (ZZ[o] + tmp - xm * (vs1 + vs2) + vx1 * f_r) * dcrj;
-      a.r3[col + o] = f_vx2 * f_r + f_wwo * f_rtmp;
-      f_rtmp = f_rtmp * (f_wwo - 1) + f_vx2 * f_r * (1 - f_vx1);
-      ZZ[o] = (s + DT * f_rtmp) * dcrj;
-    }
-
-    // xy
-    vs1 = c1 * (LDG(U + o + Y) - u_0) + c2 * (LDG(U + o + 2 * Y) - LDG(U + o - Y));
-    vs2 = c1 * (v_0 - v_m1) + c2 * (v_p1 - v_m2);
-    if (ELASTIC) {
-      XY[o] = (XY[o] + xmu1 * (vs1 + vs2)) * dcrj;
-    } else {
-      const float f_r = a.r4[col + o];
-      float f_rtmp = h1 * (vs1 + vs2);
-      const float s = XY[o] + xmu1 * (vs1 + vs2) + vx1 * f_r;
-      a.r4[col + o] = f_vx2 * f_r + f_wwo * f_rtmp;
-      f_rtmp = f_rtmp * (f_wwo - 1) + f_vx2 * f_r * (1 - f_vx1);
-      XY[o] = (s + DT * f_rtmp) * dcrj;
-    }
-
-    // xz
-    vs1 = c1 * (uk1 - u_0) + c2 * (uk2 - LDG(U + o - 1));
-    vs2 = c1 * (w_0 - w_m1) + c2 * (w_p1 - w_m2);
-    if (ELASTIC) {
-      XZ[o] = (XZ[o] + xmu2 * (vs1 + vs2)) * dcrj;
-    } else {
-      const float f_r = a.r5[col + o];
-      float f_rtmp = h2 * (vs1 + vs2);
-      const float s = XZ[o] + xmu2 * (vs1 + vs2) + vx1 * f_r;
-      a.r5[col + o] = f_vx2 * f_r + f_wwo * f_rtmp;
-      f_rtmp = f_rtmp * (f_wwo - 1) + f_vx2 * f_r * (1 - f_vx1);
-      XZ[o] = (s + DT * f_rtmp) * dcrj;
-    }
-
-    // yz
-    vs1 = c1 * (vk1 - v_0) + c2 * (vk2 - LDG(V + o - 1));
-    vs2 = c1 * (LDG(W + o + Y) - w_0) + c2 * (LDG(W + o + 2 * Y) - LDG(W + o - Y));
-    if (ELASTIC) {
-      YZ[o] = (YZ[o] + xmu3 * (vs1 + vs2)) * dcrj;
-    } else {
-      const float f_r = a.r6[col + o];
-      float f_rtmp = h3 * (vs1 + vs2);
-      const float s = YZ[o] + xmu3 * (vs1 + vs2) + vx1 * f_r;
-      a.r6[col + o] = f_vx2 * f_r + f_wwo * f_rtmp;
-      f_rtmp = f_rtmp * (f_wwo - 1) + f_vx2 * f_r * (1 - f_vx1);
-      YZ[o] = (s + DT * f_rtmp) * dcrj;
+    stress_update<ELASTIC>(sg, rr, xl, xm, xmu1, xmu2, xmu3, h, h1, h2, h3, qpa, vx1, f_vx1,
+                           f_vx2, f_wwo, DT, dcrj, d);
+#pragma unroll
+    for (int q = 0; q < 6; ++q) SG[q][o] = sg[q];
+    if (!ELASTIC) {
+#pragma unroll
+      for (int q = 0; q < 6; ++q) RR[q][o] = rr[q];
     }
 
     u_m1 = u_0; u_0 = u_p1; u_p1 = u_p2;
@@ -931,30 +946,58 @@ inline unsigned cdiv_u(long long a, long long b) { return (unsigned)((a + b - 1)
 cudaError_t awp_launch_velocity(const VelArgs& a, cudaStream_t st) {
   const int nk = a.k1 - a.k0 + 1, nj = a.j1 - a.j0 + 1, ni = a.i1 - a.i0 + 1;
   if (nk <= 0 || nj <= 0 || ni <= 0) return cudaSuccess;
-  const dim3 block(32, kVelTY, 1);
-  const dim3 grid(cdiv_u(nk, 32), cdiv_u(nj, kVelTY), cdiv_u(ni, kIChunk));
-  k_velocity<<<grid, block, 0, st>>>(a, kIChunk);
+  const int ty = g_vel_ty;
+  const dim3 block(32, ty, 1);
+  const dim3 grid(cdiv_u(nk, 32), cdiv_u(nj, ty), cdiv_u(ni, g_ichunk));
+  if (ty == 4)
+    k_velocity<4><<<grid, block, 0, st>>>(a, g_ichunk);
+  else
+    k_velocity<8><<<grid, block, 0, st>>>(a, g_ichunk);
   return cudaGetLastError();
+}
+
+template <int TY>
+static void launch_stress_ty(const StrArgs& a, bool elastic, bool texarr, dim3 grid,
+                             cudaStream_t st) {
+  const dim3 block(32, TY, 1);
+  if (elastic) {
+    if (texarr)
+      k_stress<true, true, TY><<<grid, block, 0, st>>>(a, g_ichunk);
+    else
+      k_stress<true, false, TY><<<grid, block, 0, st>>>(a, g_ichunk);
+  } else {
+    if (texarr)
+      k_stress<false, true, TY><<<grid, block, 0, st>>>(a, g_ichunk);
+    else
+      k_stress<false, false, TY><<<grid, block, 0, st>>>(a, g_ichunk);
+  }
 }
 
 cudaError_t awp_launch_stress(const StrArgs& a, bool elastic, cudaStream_t st) {
   const int nk = a.k1 - a.k0 + 1, nj = a.j1 - a.j0 + 1, ni = a.i1 - a.i0 + 1;
   if (nk <= 0 || nj <= 0 || ni <= 0) return cudaSuccess;
-  const dim3 block(32, kStrTY, 1);
-  const dim3 grid(cdiv_u(nk, 32), cdiv_u(nj, kStrTY), cdiv_u(ni, kIChunk));
+  const int ty = g_str_ty;
+  const dim3 grid(cdiv_u(nk, 32), cdiv_u(nj, ty), cdiv_u(ni, g_ichunk));
   const bool texarr = a.vx1 != nullptr;
-  if (elastic) {
-    if (texarr)
-      k_stress<true, true><<<grid, block, 0, st>>>(a, kIChunk);
-    else
-      k_stress<true, false><<<grid, block, 0, st>>>(a, kIChunk);
-  } else {
-    if (texarr)
-      k_stress<false, true><<<grid, block, 0, st>>>(a, kIChunk);
-    else
-      k_stress<false, false><<<grid, block, 0, st>>>(a, kIChunk);
-  }
+  if (ty == 4)
+    launch_stress_ty<4>(a, elastic, texarr, grid, st);
+  else
+    launch_stress_ty<8>(a, elastic, texarr, grid, st);
   return cudaGetLastError();
+}
+
+int awp_tuning_set(const char* key, int value) {
+  if (!strcmp(key, "vel_ty") && (value == 4 || value == 8)) { g_vel_ty = value; return 0; }
+  if (!strcmp(key, "str_ty") && (value == 4 || value == 8)) { g_str_ty = value; return 0; }
+  if (!strcmp(key, "ichunk") && value >= 4 && value <= 1024) { g_ichunk = value; return 0; }
+  return 1;
+}
+
+int awp_tuning_get(const char* key) {
+  if (!strcmp(key, "vel_ty")) return g_vel_ty;
+  if (!strcmp(key, "str_ty")) return g_str_ty;
+  if (!strcmp(key, "ichunk")) return g_ichunk;
+  return -1;
 }
 
 cudaError_t awp_launch_fstr(const FstrArgs& a, cudaStream_t st) {

@@ -150,6 +150,11 @@ struct MediaArgs {
   int slice, yline;
 };
 
+// Launch-shape tuning (awp_kernels.cu): "vel_ty", "str_ty" (4 or 8 j-rows per
+// CTA) and "ichunk" (x-planes marched per CTA).  Returns 0 on success.
+int awp_tuning_set(const char* key, int value);
+int awp_tuning_get(const char* key);
+
 // Launchers (awp_kernels.cu).  All are asynchronous on `st`.
 cudaError_t awp_launch_velocity(const VelArgs& a, cudaStream_t st);
 cudaError_t awp_launch_stress(const StrArgs& a, bool elastic, cudaStream_t st);

@@ -1,0 +1,53 @@
+"""Launch-shape autotuner for the stencil kernels.
+
+Times every candidate (j rows per CTA for the velocity and stress kernels, x
+planes marched per CTA) with the library's own per-phase CUDA events on a live
+context, keeps the fastest per kernel and installs it process-wide through
+awp_set_tuning.  The arithmetic does not depend on the launch shape (every
+cell is computed by exactly one thread with the same expression), so tuning
+never changes results -- tests/test_tuning_gpu.py checks that bit for bit.
+"""
+from __future__ import annotations
+
+import itertools
+
+CANDIDATES = {
+    "vel_ty": (4, 8),
+    "str_ty": (4, 8),
+    "ichunk": (16, 32, 64),
+}
+
+
+def set_tuning(lib, key: str, value: int) -> None:
+    if lib.awp_set_tuning(key.encode(), int(value)) != 0:
+        raise ValueError(f"tuning {key}={value} rejected")
+
+
+def get_tuning(lib) -> dict:
+    return {k: lib.awp_get_tuning(k.encode()) for k in CANDIDATES}
+
+
+def autotune(solver, steps: int = 3) -> dict:
+    """Try every (vel_ty, str_ty, ichunk) on `solver` (advancing it) and install
+    the fastest velocity and stress shapes.  Returns the timing table."""
+    lib = solver.lib
+    table = []
+    solver.profile_phases(True)
+    solver.phase_times()  # drop earlier events
+    for vty, sty, ich in itertools.product(*CANDIDATES.values()):
+        set_tuning(lib, "vel_ty", vty)
+        set_tuning(lib, "str_ty", sty)
+        set_tuning(lib, "ichunk", ich)
+        solver.step(1)  # settle
+        solver.phase_times()
+        solver.step(steps)
+        t = solver.phase_times()
+        table.append({"vel_ty": vty, "str_ty": sty, "ichunk": ich,
+                      "velocity_ms": t["velocity"][0] / max(t["velocity"][1], 1),
+                      "stress_ms": t["stress"][0] / max(t["stress"][1], 1)})
+    solver.profile_phases(False)
+    best = min(table, key=lambda r: r["velocity_ms"] + r["stress_ms"])
+    set_tuning(lib, "vel_ty", best["vel_ty"])
+    set_tuning(lib, "str_ty", best["str_ty"])
+    set_tuning(lib, "ichunk", best["ichunk"])
+    return {"chosen": {k: best[k] for k in CANDIDATES}, "table": table}

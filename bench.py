@@ -100,12 +100,25 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def build_workload(name: str):
+def reduce_max(value: float, dist, device: str = "cuda") -> float:
+    """Max over ranks of a per-rank timing (every rank takes part)."""
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def build_workload(name: str, grid=None):
     from awp_b200 import scenarios
+    kw = {}
+    if grid:
+        kw = dict(nx=grid[0], ny=grid[1], nz=grid[2])
     if name == "layered_vk":
-        return scenarios.layered_vk(), "anelastic"
+        return scenarios.layered_vk(**kw), "anelastic"
     if name == "halfspace":
-        return scenarios.halfspace(), "elastic"
+        return scenarios.halfspace(**kw), "elastic"
     raise SystemExit(f"unknown workload {name}")
 
 
@@ -190,17 +203,19 @@ def reference_gpu(scn, solver, steps=4, warmup=2) -> dict:
                  lam_mu=refbind.lam_mu_ref(media["lam"], media["mu"], nx, ny, nz),
                  coeff=coeff, psrc=psrc, src=comps, src_stride=rs)
     del media
-    sim = refbind.RefGpuSim(scn, setup)
-    del setup, vx1, vx2, ww, wwo
-    sim.step(warmup)
-    s0 = torch.cuda.Event(enable_timing=True)
-    s1 = torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize()
-    s0.record()
-    sim.step(steps)
-    s1.record()
-    torch.cuda.synchronize()
-    ms = s0.elapsed_time(s1) / steps
+    with torch.cuda.stream(torch.cuda.default_stream()):
+        # the reference launchers run on the legacy default stream
+        sim = refbind.RefGpuSim(scn, setup)
+        del setup, vx1, vx2, ww, wwo
+        sim.step(warmup)
+        s0 = torch.cuda.Event(enable_timing=True)
+        s1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        s0.record()
+        sim.step(steps)
+        s1.record()
+        torch.cuda.synchronize()
+        ms = s0.elapsed_time(s1) / steps
     out = {"value": nx * ny * nz / (ms * 1e-3) / 1e9, "unit": "Gcell-updates/s",
            "ms_per_step": ms, "steps": steps,
            "build": "reference src/awp/kernel.cu, nvcc sm_100a -O3 -use_fast_math, "
@@ -225,16 +240,21 @@ def run_ours(args, rank, world, dist) -> dict | None:
     from awp_b200 import Solver, default_params
 
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
-    scn, kind = build_workload(args.workload)
+    scn, kind = build_workload(args.workload, args.grid)
     p = scn.params
     cells = p["nx"] * p["ny"] * p["nz"]
-    stream = torch.cuda.current_stream()
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     hbm, peak_kind = peaks()
 
     # ---- device-resident timing -------------------------------------------------
     s = Solver(default_params(**p), stream=stream.cuda_stream)
     s.upload_media(scn.media)
     s.upload_sources(scn.src_pos, scn.src_data)
+    tuning = None
+    if not args.no_tune:
+        from awp_b200 import tune
+        tuning = tune.autotune(s)
     s.step(args.warmup)
     s.synchronize()
     if dist is not None:
@@ -258,11 +278,7 @@ def run_ours(args, rank, world, dist) -> dict | None:
     phases = s.phase_times()
     s.profile_phases(False)
     ok = s.check_finite()
-    t_max = ms
-    if dist is not None:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_max = float(t.item())
+    t_max = reduce_max(ms, dist)
     ms_step = t_max / args.steps
     value = world * cells * args.steps / (t_max * 1e-3) / 1e9
 
@@ -289,6 +305,7 @@ def run_ours(args, rank, world, dist) -> dict | None:
 
     # ---- end to end through the C ABI with host buffers ----------------------------
     e2e = None
+    e2e_steps = args.e2e_steps or (scn.steps if args.grid is None else args.steps)
     if not args.no_e2e:
         media = torch.from_numpy(scn.media).pin_memory()
         nvar = scn.media.shape[3]
@@ -304,7 +321,7 @@ def run_ours(args, rank, world, dist) -> dict | None:
         se.lib.awp_upload_media(se.ctx, nvar, media.numpy().ctypes.data_as(
             __import__("ctypes").POINTER(__import__("ctypes").c_float)))
         se.upload_sources(scn.src_pos, scn.src_data)
-        se.step(args.steps)
+        se.step(e2e_steps)
         # free-surface snapshot (velbuffer, NBGZ=NEDZ=1) back to the host
         se.gather(0, p["nx"] - 1, 1, 0, p["ny"] - 1, 1, 0, 0, 1,
                   dev[0].data_ptr(), dev[1].data_ptr(), dev[2].data_ptr())
@@ -312,17 +329,15 @@ def run_ours(args, rank, world, dist) -> dict | None:
             o.copy_(d, non_blocking=True)
         t1.record(stream)
         torch.cuda.synchronize()
-        e2e_ms = t0.elapsed_time(t1)
-        if dist is not None:
-            t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_ms = float(t.item())
+        e2e_ms = reduce_max(t0.elapsed_time(t1), dist)
         d2h = 3 * rec * 4
-        e2e = {"value": world * cells * args.steps / (e2e_ms * 1e-3) / 1e9,
-               "unit": "Gcell-updates/s", "h2d_bytes_per_step": h2d / args.steps,
-               "d2h_bytes_per_step": d2h / args.steps, "ms_total": e2e_ms,
-               "includes": "context create, media H2D + on-device inimesh mapping, sources, "
-                           f"{args.steps} steps, surface snapshot D2H"}
+        e2e = {"value": world * cells * e2e_steps / (e2e_ms * 1e-3) / 1e9,
+               "unit": "Gcell-updates/s", "h2d_bytes_per_step": h2d / e2e_steps,
+               "d2h_bytes_per_step": d2h / e2e_steps, "ms_total": e2e_ms,
+               "steps": e2e_steps,
+               "includes": "the whole run through the C ABI: context create, media H2D + "
+                           "on-device inimesh mapping, sources, every time step of the run, "
+                           "surface snapshot D2H"}
         se.close()
         del se, media
 
@@ -346,6 +361,7 @@ def run_ours(args, rank, world, dist) -> dict | None:
         "kernels": kernels,
         "clocks": clocks,
         "gpu_launches": launches,
+        "tuning": tuning["chosen"] if tuning else None,
     }
     if e2e:
         line["e2e"] = e2e
@@ -390,6 +406,11 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ref-gpu", action="store_true")
+    ap.add_argument("--no-tune", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=0,
+                    help="steps of the end-to-end run (default: the workload's full run)")
+    ap.add_argument("--grid", type=lambda v: tuple(int(x) for x in v.split(",")), default=None,
+                    help="nx,ny,nz override of the workload grid (profiling cases)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -90,7 +90,8 @@ const char* awp_last_error(void);
 int awp_ctx_create(const awp_params* p, awp_ctx** out);
 int awp_ctx_destroy(awp_ctx* ctx);
 
-/* Run every subsequent kernel on this cudaStream_t (NULL = the context's own). */
+/* Run every subsequent kernel on this cudaStream_t (NULL = the legacy default
+ * stream).  A new context runs on a stream of its own. */
 int awp_set_stream(awp_ctx* ctx, void* cuda_stream);
 
 /* Padded extents (nxt+20, nyt+20, nzt+64). */
@@ -156,6 +157,13 @@ int awp_check_finite(awp_ctx* ctx, int* ok);
 #define AWP_NPHASES 5
 int awp_profile_phases(awp_ctx* ctx, int enable);
 int awp_phase_times(awp_ctx* ctx, double ms[AWP_NPHASES], long long launches[AWP_NPHASES]);
+/* Launch-shape tuning of the stencil kernels (process-wide): key "vel_ty" or
+ * "str_ty" (j rows per CTA: 4 or 8), "ichunk" (x planes marched per CTA,
+ * 4..1024).  Returns AWP_OK or AWP_ERR_ARG; awp_get_tuning returns the value
+ * or -1 for an unknown key. */
+int awp_set_tuning(const char* key, int value);
+int awp_get_tuning(const char* key);
+
 /* Kernels this context has launched so far. */
 int awp_kernel_launches(const awp_ctx* ctx, long long* launches);
 

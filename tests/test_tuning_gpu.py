@@ -1,0 +1,49 @@
+"""Launch shapes never change results: every tuning gives bit-identical fields."""
+import itertools
+
+import numpy as np
+import pytest
+
+from awp_b200 import Solver, _lib, default_params, scenarios, tune
+
+pytestmark = pytest.mark.gpu
+
+
+def run(scn, steps):
+    s = Solver(default_params(**scn.params))
+    s.upload_media(scn.media)
+    s.upload_sources(scn.src_pos, scn.src_data)
+    s.step(steps)
+    out = {f: s.field(f) for f in ("u1", "v1", "w1", "xx", "yz", "r1", "r6")}
+    s.close()
+    return out
+
+
+@pytest.mark.parametrize("q", [True, False])
+def test_tuning_is_bitwise_neutral(q):
+    lib = _lib.load()
+    saved = tune.get_tuning(lib)
+    scn = scenarios.random_small(nx=40, ny=36, nz=64, q=q, steps=6, seed=5)
+    base = None
+    try:
+        for vty, sty, ich in itertools.product((4, 8), (4, 8), (16, 64)):
+            tune.set_tuning(lib, "vel_ty", vty)
+            tune.set_tuning(lib, "str_ty", sty)
+            tune.set_tuning(lib, "ichunk", ich)
+            out = run(scn, 6)
+            if base is None:
+                base = out
+                continue
+            for f in out:
+                assert np.array_equal(out[f].view(np.uint32), base[f].view(np.uint32)), \
+                    (f, vty, sty, ich)
+    finally:
+        for k, v in saved.items():
+            tune.set_tuning(lib, k, v)
+
+
+def test_bad_tuning_rejected():
+    lib = _lib.load()
+    assert lib.awp_set_tuning(b"str_ty", 5) != 0
+    assert lib.awp_set_tuning(b"nonsense", 8) != 0
+    assert lib.awp_get_tuning(b"nonsense") == -1
