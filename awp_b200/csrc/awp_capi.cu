@@ -72,6 +72,7 @@ struct awp_ctx {
   PlastParams pp{};
   unsigned char* d_neta_mult = nullptr;
   unsigned int* d_flag = nullptr;
+  unsigned int* d_ext = nullptr;  // media extrema (6 float bit patterns)
   long long cur_step = 0;
   bool initial_src_done = false;
   long long dev_bytes = 0;
@@ -324,6 +325,7 @@ int awp_ctx_destroy(awp_ctx* c) {
   cudaFree(c->d_cell_pos); cudaFree(c->d_cell_first); cudaFree(c->d_order);
   for (int i = 0; i < 6; ++i) cudaFree(c->d_src[i]);
   cudaFree(c->d_mom); cudaFree(c->d_filt); cudaFree(c->d_neta_mult); cudaFree(c->d_flag);
+  cudaFree(c->d_ext);
   for (auto& e : c->ev_used) { cudaEventDestroy(e.a); cudaEventDestroy(e.b); }
   for (auto& e : c->ev_free) { cudaEventDestroy(e.a); cudaEventDestroy(e.b); }
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
@@ -412,6 +414,7 @@ int awp_ctx_create(const awp_params* p, awp_ctx** out) {
     c->tex.nzt = p->nz;
   }
   if ((st = ctx_alloc(c, (void**)&c->d_flag, sizeof(unsigned int)))) goto fail;
+  if ((st = ctx_alloc(c, (void**)&c->d_ext, 6 * sizeof(unsigned int)))) goto fail;
   if (cudaStreamSynchronize(c->stream) != cudaSuccess) {
     st = set_error(AWP_ERR_CUDA, "initialisation");
     goto fail;
@@ -471,6 +474,11 @@ static int upload_media_impl(awp_ctx* c, int nvar, const float* media, bool devi
   a.socalq = c->p.socalq;
   a.nxt = c->p.nx; a.nyt = c->p.ny; a.nzt = c->p.nz;
   a.slice = c->g.slice; a.yline = c->g.yline;
+  {
+    const unsigned int init[6] = {0x7f800000u, 0u, 0x7f800000u, 0u, 0x7f800000u, 0u};
+    CU_TRY(cudaMemcpyAsync(c->d_ext, init, sizeof(init), cudaMemcpyHostToDevice, c->stream));
+  }
+  a.ext = c->d_ext;
   CU_TRY(awp_launch_media(a, c->stream));
   CU_TRY(awp_launch_media_borders(c->f[AWP_D1], c->f[AWP_MU], c->f[AWP_LAM], c->f[AWP_QP],
                                   c->f[AWP_QS], c->g, c->p.nve, c->stream));
@@ -489,6 +497,38 @@ static int upload_media_impl(awp_ctx* c, int nvar, const float* media, bool devi
   const bool any_q = hflag != 0;
   c->elastic = !any_q;
   c->media_ready = true;
+  return AWP_OK;
+}
+
+int awp_media_extrema(awp_ctx* c, float vse[2], float vpe[2], float dde[2]) {
+  if (!c || !vse || !vpe || !dde) return set_error(AWP_ERR_ARG, "null argument");
+  if (!c->media_ready) return set_error(AWP_ERR_STATE, "no media uploaded");
+  unsigned int h[6];
+  CU_TRY(cudaMemcpyAsync(h, c->d_ext, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+  CU_TRY(cudaStreamSynchronize(c->stream));
+  float v[6];
+  memcpy(v, h, sizeof(v));
+  vse[0] = (h[0] == 0x7f800000u) ? 1.0e10f : v[0];
+  vse[1] = v[1];
+  vpe[0] = v[2];
+  vpe[1] = v[3];
+  dde[0] = v[4];
+  dde[1] = v[5];
+  return AWP_OK;
+}
+
+int awp_alloc_host_pinned(void** ptr, size_t bytes) {
+  if (!ptr) return set_error(AWP_ERR_ARG, "null argument");
+  cudaError_t e = cudaMallocHost(ptr, bytes);
+  if (e != cudaSuccess) {
+    *ptr = nullptr;
+    return set_error(AWP_ERR_NOMEM, "cudaMallocHost(%zu): %s", bytes, cudaGetErrorString(e));
+  }
+  return AWP_OK;
+}
+
+int awp_free_host_pinned(void* ptr) {
+  CU_TRY(cudaFreeHost(ptr));
   return AWP_OK;
 }
 

@@ -804,8 +804,19 @@ __device__ float q_modulus(const MediaArgs& a, float dd, float v, float q) {
   return ddvv;
 }
 
+__device__ __forceinline__ unsigned int warp_min_u(unsigned int v) {
+  for (int o = 16; o; o >>= 1) v = min(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+__device__ __forceinline__ unsigned int warp_max_u(unsigned int v) {
+  for (int o = 16; o; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
 __global__ void k_media(const MediaArgs a) {
   const long long n = (long long)a.nxt * a.nyt * a.nzt;
+  // non-negative floats order like their bit patterns
+  unsigned int e[6] = {0x7f800000u, 0u, 0x7f800000u, 0u, 0x7f800000u, 0u};
   for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n;
        c += (long long)gridDim.x * blockDim.x) {
     const int i = (int)(c % a.nxt);
@@ -834,6 +845,12 @@ __global__ void k_media(const MediaArgs a) {
     const long long p = (long long)(i + 2 + AWP_NGSL) * a.slice +
                         (long long)(j + 2 + AWP_NGSL) * a.yline +
                         (a.nzt + AWP_ALIGN - 1 - k);
+    if (vs > 1.0f) e[0] = min(e[0], __float_as_uint(vs));
+    e[1] = max(e[1], __float_as_uint(fmaxf(vs, 0.f)));
+    e[2] = min(e[2], __float_as_uint(fmaxf(vp, 0.f)));
+    e[3] = max(e[3], __float_as_uint(fmaxf(vp, 0.f)));
+    e[4] = min(e[4], __float_as_uint(fmaxf(dd, 0.f)));
+    e[5] = max(e[5], __float_as_uint(fmaxf(dd, 0.f)));
     a.mu[p] = (float)__ddiv_rn(1., (double)__fmul_rn(__fmul_rn(dd, vs), vs));
     const double vp2 = (double)__fmul_rn(vp, vp);
     const double vs2 = __dmul_rn(__dmul_rn(2., (double)vs), (double)vs);
@@ -850,6 +867,15 @@ __global__ void k_media(const MediaArgs a) {
       }
       a.qp[p] = __fdiv_rn(qpinv, a.facex);
       a.qs[p] = __fdiv_rn(qsinv, a.facex);
+    }
+  }
+  if (a.ext) {
+    for (int q = 0; q < 6; q += 2) {
+      const unsigned int lo = warp_min_u(e[q]), hi = warp_max_u(e[q + 1]);
+      if ((threadIdx.x & 31) == 0) {
+        atomicMin(a.ext + q, lo);
+        atomicMax(a.ext + q + 1, hi);
+      }
     }
   }
 }

@@ -148,6 +148,9 @@ struct MediaArgs {
   int nvar, var_offset, nve, socalq;
   int nxt, nyt, nzt;
   int slice, yline;
+  // extrema of the corrected vs, vp, rho as float bits (mesh.c:455-460):
+  // [vs_min (vs > 1 only), vs_max, vp_min, vp_max, rho_min, rho_max]
+  unsigned int* ext;
 };
 
 // Launch-shape tuning (awp_kernels.cu): "vel_ty", "str_ty" (4 or 8 j-rows per

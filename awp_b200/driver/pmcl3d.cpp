@@ -1,0 +1,598 @@
+// pmcl3d -- single-rank drop-in for the reference's pmcl3d executable.
+//
+// Same command line (src/awp/command.c), same input files (INVEL mesh,
+// INSRC sources, sourcefilter.dat, nonlinear.dat) and the same output files
+// (OUT/SX_0_%07ld, SY, SZ, Eta; the CHKFILE statistics log) as the reference's
+// single-rank run; the time step itself runs in libawpb200 through its C ABI.
+//
+// Scope: one rank (PX = PY = 1, no I/O ranks), one grid, MEDIASTART 0-2,
+// IFAULT 1 and 5, NVE 1 and 3.  Anything else is reported and refused.
+#include <getopt.h>
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <sys/stat.h>
+#include <sys/time.h>
+#include <unistd.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/awp_b200.h"
+
+#define MAXGRIDS 10
+#define NGSL 8
+#define ALIGN 32
+#define NEDZ_EP 160
+
+namespace {
+
+struct Args {
+  float TMAX = 20.00f, DH = 200.0f, DT = 0.01f, ARBC = 0.92f, PHT = 0.1f;
+  int NPC = 0, ND = 20, NSRC[MAXGRIDS] = {1}, NST = 91, NVAR = 3, NVE = 1, MEDIASTART = 0;
+  int IFAULT = 1, READ_STEP = 91, READ_STEP_GPU = 91, NTISKP = 1, WRITE_STEP = 10;
+  int NX = 256, NY = 256, NZ[MAXGRIDS] = {1024}, PX = 1, PY = 1;
+  int NBGX[MAXGRIDS], NEDX[MAXGRIDS], NSKPX[MAXGRIDS];
+  int NBGY[MAXGRIDS], NEDY[MAXGRIDS], NSKPY[MAXGRIDS];
+  int NBGZ[MAXGRIDS], NEDZ[MAXGRIDS], NSKPZ[MAXGRIDS];
+  int IDYNA = 0, SoCalQ = 1;
+  float FAC = 0.005f, Q0 = 5.0f, EX = 0.0f, FP = 2.5f;
+  int NGRIDS = 1, FOLLOWBATHY = 0;
+  std::string INSRC = "input/FAULTPOW", INVEL = "input/media", OUT = "output_sfc";
+  std::string INSRC_I2 = "input_rst/srcpart/split_faults/fault", CHKFILE = "output_ckp/CHKP";
+  std::string INTOPO = "input/topography", SOURCEFILE, RECVFILE, FORCEFILE, SGTFILE;
+  int USETOPO = 0, USESOURCEFILE = 0, USERECVFILE = 0, USEFORCEFILE = 0, USESGTFILE = 0;
+  Args() {
+    for (int p = 0; p < MAXGRIDS; ++p) {
+      NBGX[p] = NBGY[p] = NBGZ[p] = 1;
+      NEDX[p] = NEDY[p] = -1;
+      NEDZ[p] = 1;
+      NSKPX[p] = NSKPY[p] = NSKPZ[p] = 1;
+      if (p) NSRC[p] = 0, NZ[p] = 0;
+    }
+  }
+};
+
+void parsemultiple(const char* arg, int* val) {
+  std::string s(arg);
+  size_t pos = 0;
+  int k = 0;
+  while (k < MAXGRIDS) {
+    size_t e = s.find(',', pos);
+    val[k++] = atoi(s.substr(pos, e == std::string::npos ? std::string::npos : e - pos).c_str());
+    if (e == std::string::npos) break;
+    pos = e + 1;
+  }
+}
+
+// command() of src/awp/command.c:152-546
+void command(int argc, char** argv, Args& a) {
+  static const char* optstring =
+      "-T:H:t:A:P:M:D:S:N:V:B:n:I:R:Q:X:Y:Z:x:y:G:z:i:l:h:30:p:s:r:W:1:2:"
+      "3:11:12:13:21:22:23:100:101:102:103:106:107:109:9:o:c:";
+  static struct option long_options[] = {
+      {"TMAX", required_argument, NULL, 'T'},     {"DH", required_argument, NULL, 'H'},
+      {"DT", required_argument, NULL, 't'},       {"ARBC", required_argument, NULL, 'A'},
+      {"PHT", required_argument, NULL, 'P'},      {"NPC", required_argument, NULL, 'M'},
+      {"ND", required_argument, NULL, 'D'},       {"NSRC", required_argument, NULL, 'S'},
+      {"NST", required_argument, NULL, 'N'},      {"NVE", required_argument, NULL, 'V'},
+      {"MEDIASTART", required_argument, NULL, 'B'}, {"NVAR", required_argument, NULL, 'n'},
+      {"IFAULT", required_argument, NULL, 'I'},   {"READ_STEP", required_argument, NULL, 'R'},
+      {"READ_STEP_GPU", required_argument, NULL, 'Q'}, {"NX", required_argument, NULL, 'X'},
+      {"NY", required_argument, NULL, 'Y'},       {"NZ", required_argument, NULL, 'Z'},
+      {"PX", required_argument, NULL, 'x'},       {"PY", required_argument, NULL, 'y'},
+      {"NGRIDS", required_argument, NULL, 'G'},   {"NBGX", required_argument, NULL, 1},
+      {"NEDX", required_argument, NULL, 2},       {"NSKPX", required_argument, NULL, 3},
+      {"NBGY", required_argument, NULL, 11},      {"NEDY", required_argument, NULL, 12},
+      {"NSKPY", required_argument, NULL, 13},     {"NBGZ", required_argument, NULL, 21},
+      {"NEDZ", required_argument, NULL, 22},      {"NSKPZ", required_argument, NULL, 23},
+      {"IDYNA", required_argument, NULL, 'i'},    {"SoCalQ", required_argument, NULL, 's'},
+      {"FAC", required_argument, NULL, 'l'},      {"Q0", required_argument, NULL, 'h'},
+      {"EX", required_argument, NULL, 30},        {"FP", required_argument, NULL, 'p'},
+      {"NTISKP", required_argument, NULL, 'r'},   {"WRITE_STEP", required_argument, NULL, 'W'},
+      {"INSRC", required_argument, NULL, 100},    {"INVEL", required_argument, NULL, 101},
+      {"OUT", required_argument, NULL, 'o'},      {"INSRC_I2", required_argument, NULL, 102},
+      {"CHKFILE", required_argument, NULL, 'c'},  {"FOLLOWBATHY", required_argument, NULL, 7},
+      {"INTOPO", required_argument, NULL, 103},   {"SOURCEFILE", required_argument, NULL, 107},
+      {"RECVFILE", required_argument, NULL, 109}, {"FORCEFILE", required_argument, NULL, 9},
+      {"SGTFILE", required_argument, NULL, 10},   {0, 0, 0, 0}};
+  int insrcIsSet = 0, readstepGpuIsSet = 0, c;
+  while ((c = getopt_long(argc, argv, optstring, long_options, NULL)) != -1) {
+    switch (c) {
+      case 'T': a.TMAX = atof(optarg); break;
+      case 'H': a.DH = atof(optarg); break;
+      case 't': a.DT = atof(optarg); break;
+      case 'A': a.ARBC = atof(optarg); break;
+      case 'P': a.PHT = atof(optarg); break;
+      case 'M': a.NPC = atoi(optarg); break;
+      case 'D': a.ND = atoi(optarg); break;
+      case 'S': parsemultiple(optarg, a.NSRC); break;
+      case 'N': a.NST = atoi(optarg); break;
+      case 'V': a.NVE = atoi(optarg); break;
+      case 'B': a.MEDIASTART = atoi(optarg); break;
+      case 'n': a.NVAR = atoi(optarg); break;
+      case 'I': a.IFAULT = atoi(optarg); break;
+      case 'R': a.READ_STEP = atoi(optarg); break;
+      case 'Q': readstepGpuIsSet = 1; a.READ_STEP_GPU = atoi(optarg); break;
+      case 'X': a.NX = atoi(optarg); break;
+      case 'Y': a.NY = atoi(optarg); break;
+      case 'Z': parsemultiple(optarg, a.NZ); break;
+      case 'x': a.PX = atoi(optarg); break;
+      case 'y': a.PY = atoi(optarg); break;
+      case 1: parsemultiple(optarg, a.NBGX); break;
+      case 2: parsemultiple(optarg, a.NEDX); break;
+      case 3: parsemultiple(optarg, a.NSKPX); break;
+      case 11: parsemultiple(optarg, a.NBGY); break;
+      case 12: parsemultiple(optarg, a.NEDY); break;
+      case 13: parsemultiple(optarg, a.NSKPY); break;
+      case 21: parsemultiple(optarg, a.NBGZ); break;
+      case 22: parsemultiple(optarg, a.NEDZ); break;
+      case 23: parsemultiple(optarg, a.NSKPZ); break;
+      case 'i': a.IDYNA = atoi(optarg); break;
+      case 's': a.SoCalQ = atoi(optarg); break;
+      case 'l': a.FAC = atof(optarg); break;
+      case 'h': a.Q0 = atof(optarg); break;
+      case 30: a.EX = atof(optarg); break;
+      case 'p': a.FP = atof(optarg); break;
+      case 'r': a.NTISKP = atoi(optarg); break;
+      case 'W': a.WRITE_STEP = atoi(optarg); break;
+      case 100: insrcIsSet = 1; a.INSRC = optarg; break;
+      case 101: a.INVEL = optarg; break;
+      case 'o': a.OUT = optarg; break;
+      case 102: a.INSRC_I2 = optarg; break;
+      case 'c': a.CHKFILE = optarg; break;
+      case 'G': a.NGRIDS = atoi(optarg); break;
+      case 7: a.FOLLOWBATHY = atoi(optarg); break;
+      case 103: a.INTOPO = optarg; a.USETOPO = 1; break;
+      case 107: a.SOURCEFILE = optarg; a.USESOURCEFILE = 1; break;
+      case 109: a.RECVFILE = optarg; a.USERECVFILE = 1; break;
+      case 9: a.FORCEFILE = optarg; a.USEFORCEFILE = 1; break;
+      case 10: a.SGTFILE = optarg; a.USESGTFILE = 1; break;
+      default:
+        printf("Usage: %s \nOptions:\n\t[(-T | --TMAX) <TMAX>]\n\t[(-H | --DH) <DH>]\n"
+               "\t[(-t | --DT) <DT>]\n\t[(-A | --ARBC) <ARBC>]\n\t[(-P | --PHT) <PHT>]\n"
+               "\t[(-M | --NPC) <NPC>]\n\t[(-D | --ND) <ND>]\n\t[(-S | --NSRC) <NSRC>]\n"
+               "\t[(-N | --NST) <NST>]\n",
+               argv[0]);
+        exit(-1);
+    }
+  }
+  if (a.IFAULT == 2 && !insrcIsSet) a.INSRC = "input_rst/srcpart/tpsrc/tpsrc";
+  if (!readstepGpuIsSet) a.READ_STEP_GPU = a.READ_STEP;
+  if (a.NBGX[0] == 0) a.NBGX[0] = 1;
+}
+
+// calcRecordingPoints (src/awp/calc.c:9-72) at coords (0, 0)
+void calc_recording_points(int* nbgx, int* nedx, int* nbgy, int* nedy, int* nbgz, int* nedz,
+                           int* rnx, int* rny, int* rnz, long nxt, long nyt, long nzt, int NBGX,
+                           int NEDX, int NSKPX, int NBGY, int NEDY, int NSKPY, int NBGZ, int NEDZ,
+                           int NSKPZ) {
+  *nbgx = *nedx = *nbgy = *nedy = *nbgz = *nedz = 0;
+  if (NBGX > nxt) *rnx = 0;
+  else if (NEDX < 1) *rnx = 0;
+  else {
+    *nbgx = NBGX - 1;
+    *nedx = (nxt <= NEDX) ? (int)((nxt + NBGX - 1) % NSKPX - NSKPX + nxt) : NEDX - 1;
+    *rnx = (*nedx - *nbgx) / NSKPX + 1;
+  }
+  if (NBGY > nyt) *rny = 0;
+  else if (NEDY < 1) *rny = 0;
+  else {
+    *nbgy = NBGY - 1;
+    *nedy = (nyt <= NEDY) ? (int)((nyt + NBGY - 1) % NSKPY - NSKPY + nyt) : NEDY - 1;
+    *rny = (*nedy - *nbgy) / NSKPY + 1;
+  }
+  if (NBGZ > nzt) *rnz = 0;
+  else {
+    *nbgz = NBGZ - 1;
+    *nedz = NEDZ - 1;
+    *rnz = (*nedz - *nbgz) / NSKPZ + 1;
+  }
+  if (*rnx == 0 || *rny == 0 || *rnz == 0) {
+    *rnx = *rny = *rnz = 0;
+    *nedx = *nbgx - 1;
+    *nedy = *nbgy - 1;
+  }
+}
+
+double now() {
+  struct timeval tv;
+  gettimeofday(&tv, NULL);
+  return tv.tv_sec + 1e-6 * tv.tv_usec;
+}
+
+void die(const char* what, int st) {
+  fprintf(stderr, "pmcl3d: %s failed: %s (%s)\n", what, awp_status_string(st), awp_last_error());
+  exit(1);
+}
+#define AWP(call)                  \
+  do {                             \
+    int st_ = (call);              \
+    if (st_) die(#call, st_);      \
+  } while (0)
+
+// hoek_brown (mesh.c:1139-1176)
+void hoek_brown(float sigma_0, float sigma_ci, float GSI, float mi, float D, int tunnel,
+                float* phi, float* cohes) {
+  double mb, s, a, sigma_cm, sigma_3max, sigma_3n, tmp;
+  mb = (double)mi * exp(((double)GSI - 100.) / (28. - 14. * D));
+  s = exp(((double)GSI - 100.) / (9. - 3. * (double)D));
+  a = 1. / 2. + 1. / 6. * (exp(-(double)GSI / 15.) - exp(-20. / 3.));
+  sigma_cm = (double)sigma_ci * (mb + 4. * s - a * (mb - 8. * s)) * pow(mb / 4. + s, a - 1.) /
+             (2. * (1. + a) * (2. + a));
+  if (tunnel == 0)
+    sigma_3max = sigma_cm * 0.72 * pow(sigma_cm / sigma_0, -0.91);
+  else
+    sigma_3max = sigma_cm * 0.47 * pow(sigma_cm / sigma_0, -0.94);
+  sigma_3n = sigma_3max / sigma_ci;
+  tmp = 6. * a * mb * pow(s + mb * sigma_3n, a - 1.) /
+        (2. * (1. + a) * (2. + a) + 6 * a * mb * pow(s + mb * sigma_3n, a - 1.));
+  const double phi2 = asin(tmp) / M_PI * 180.;
+  const double cohes2 = (sigma_ci * ((1. + 2 * a) * s + (1. - a) * mb * sigma_3n) *
+                         pow(s + mb * sigma_3n, a - 1.)) /
+                        ((1. + a) * (2. + a) *
+                         sqrt(1. + (6 * a * mb * pow(s + mb * sigma_3n, a - 1.)) /
+                                       ((1. + a) * (2. + a))));
+  *phi = (float)phi2;
+  *cohes = (float)cohes2;
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+  Args A;
+  command(argc, argv, A);
+  double time_init = now();
+  if (A.PX != 1 || A.PY != 1) {
+    fprintf(stderr, "pmcl3d: this build runs one rank (PX = PY = 1)\n");
+    return 1;
+  }
+  if (A.NGRIDS != 1) {
+    fprintf(stderr, "pmcl3d: NGRIDS=%d: discontinuous meshes are not part of this build\n",
+            A.NGRIDS);
+    return 1;
+  }
+  if (A.USETOPO || A.USESOURCEFILE || A.USERECVFILE || A.USEFORCEFILE || A.USESGTFILE) {
+    fprintf(stderr, "pmcl3d: INTOPO/SOURCEFILE/RECVFILE/FORCEFILE/SGTFILE are not part of "
+                    "this build\n");
+    return 1;
+  }
+  if (A.NZ[0] % 4 != 0) {  // pmcl3d.c:380-391 (BLOCK_SIZE_Z = 4)
+    fprintf(stderr, "NZT for grid 0 is not divisble by BLOCK_SIZE_Z.\nNZT = %d, BLOCK_SIZE_Z=4\n",
+            A.NZ[0]);
+    return 0;
+  }
+  const int nxt = A.NX, nyt = A.NY, nzt = A.NZ[0];
+  const long nt = (int)(A.TMAX / A.DT) + 1;
+
+  // recording points (pmcl3d.c:425-471)
+  int p = 0;
+  if (A.NEDX[p] == -1) A.NEDX[p] = A.NX;
+  if (A.NEDY[p] == -1) A.NEDY[p] = A.NY;
+  if (A.NEDZ[p] == -1) A.NEDZ[p] = A.NZ[p];
+  A.NEDX[p] = A.NEDX[p] - (A.NEDX[p] - A.NBGX[p]) % A.NSKPX[p];
+  A.NEDY[p] = A.NEDY[p] - (A.NEDY[p] - A.NBGY[p]) % A.NSKPY[p];
+  A.NEDZ[p] = A.NEDZ[p] - (A.NEDZ[p] - A.NBGZ[p]) % A.NSKPZ[p];
+  const int recNX = (A.NEDX[p] - A.NBGX[p]) / A.NSKPX[p] + 1;
+  const int recNY = (A.NEDY[p] - A.NBGY[p]) / A.NSKPY[p] + 1;
+  const int recNZ = (A.NEDZ[p] - A.NBGZ[p]) / A.NSKPZ[p] + 1;
+  int rnbgx, rnedx, rnbgy, rnedy, rnbgz, rnedz, rnx, rny, rnz;
+  calc_recording_points(&rnbgx, &rnedx, &rnbgy, &rnedy, &rnbgz, &rnedz, &rnx, &rny, &rnz, nxt,
+                        nyt, nzt, A.NBGX[p], A.NEDX[p], A.NSKPX[p], A.NBGY[p], A.NEDY[p],
+                        A.NSKPY[p], A.NBGZ[p], A.NEDZ[p], A.NSKPZ[p]);
+
+  awp_params P;
+  awp_params_default(&P);
+  P.nx = nxt; P.ny = nyt; P.nz = nzt;
+  P.dh = A.DH; P.dt = A.DT; P.arbc = A.ARBC; P.npc = A.NPC; P.nd = A.ND;
+  P.nve = (A.NVE == 3) ? 3 : 1;
+  P.fac = A.FAC; P.q0 = A.Q0; P.ex = A.EX; P.fp = A.FP; P.socalq = A.SoCalQ;
+  P.ifault = A.IFAULT; P.nst = A.NST; P.read_step = A.READ_STEP_GPU;
+  if (A.IFAULT != 1 && A.IFAULT != 5) {
+    fprintf(stderr, "pmcl3d: IFAULT=%d sources are not part of this build\n", A.IFAULT);
+    return 1;
+  }
+  if (A.IFAULT == 5 && (A.NST != 2 || A.READ_STEP != 2)) {  // pmcl3d.c:680-688
+    fprintf(stderr, "IFAULT=5 requires NST = READ_STEP =2.\nQuitting.");
+    return -1;
+  }
+  awp_ctx* ctx = nullptr;
+  AWP(awp_ctx_create(&P, &ctx));
+
+  // ---- sources (inisource, source.c:131-264; sourcefilter.dat, pmcl3d.c:651-675)
+  int filtorder = 0;
+  double fb[20] = {0}, fa[20] = {0};
+  if (access("sourcefilter.dat", F_OK) != -1) {
+    FILE* f = fopen("sourcefilter.dat", "r");
+    if (fscanf(f, "%d\n", &filtorder) != 1) filtorder = 0;
+    printf("Order of source filter: %d.  Parameters:\n", filtorder);
+    for (int k = 0; k < filtorder + 1 && k < 20; k++) {
+      if (fscanf(f, "%le %le\n", fb + k, fa + k) != 2) break;
+      printf("b[%d]=%le, a[%d]=%le\n", k, fb[k], k, fa[k]);
+    }
+    fclose(f);
+    AWP(awp_set_source_filter(ctx, filtorder, fb, fa));
+  }
+  std::vector<int> spos;
+  std::vector<float> sdat;
+  int nsrc = 0;
+  if (A.NSRC[0] > 0) {
+    char name[512];
+    snprintf(name, sizeof(name), "%s_%d", A.INSRC.c_str(), 0);
+    FILE* f = fopen(name, "rb");
+    if (!f) {
+      printf("can't open file %s", name);
+    } else {
+      std::vector<float> tmp((size_t)A.NST * 6);
+      const int rs = A.READ_STEP_GPU;
+      for (int i = 0; i < A.NSRC[0]; ++i) {
+        int t3[3];
+        if (fread(t3, sizeof(int), 3, f) != 3 ||
+            fread(tmp.data(), sizeof(float), tmp.size(), f) != tmp.size())
+          break;
+        spos.insert(spos.end(), t3, t3 + 3);
+        for (int j = 0; j < rs; ++j)
+          for (int q = 0; q < 6; ++q) sdat.push_back(j < A.NST ? tmp[(size_t)j * 6 + q] : 0.f);
+        ++nsrc;
+      }
+      fclose(f);
+    }
+    if (nsrc) AWP(awp_upload_sources(ctx, nsrc, spos.data(), sdat.data()));
+  }
+  if (A.IFAULT == 5) printf("Using IFAULT=5: kinematic source.\n");
+
+  // ---- media (inimesh, mesh.c:23-614) ---------------------------------------
+  float vse[2] = {0, 0}, vpe[2] = {0, 0}, dde[2] = {0, 0};
+  long long dims[3];
+  AWP(awp_padded_dims(ctx, dims));
+  const size_t ncell = (size_t)dims[0] * dims[1] * dims[2];
+  if (A.MEDIASTART == 0) {
+    float vp, vs, dd;
+    if (A.IDYNA == 1) vp = 6000.0, vs = 3464.0, dd = 2670.0;
+    else vp = 1500.0, vs = 500.0, dd = 2000.0;
+    std::vector<float> lam(ncell, (float)(1. / (dd * (vp * vp - 2. * vs * vs)))),
+        mu(ncell, (float)(1. / (dd * vs * vs))), d1(ncell, dd);
+    AWP(awp_field_upload(ctx, AWP_D1, d1.data()));
+    AWP(awp_field_upload(ctx, AWP_MU, mu.data()));
+    AWP(awp_field_upload(ctx, AWP_LAM, lam.data()));
+    vse[0] = vse[1] = vs; vpe[0] = vpe[1] = vp; dde[0] = dde[1] = dd;
+  } else if (A.MEDIASTART == 1 || A.MEDIASTART == 2) {
+    char name[512];
+    snprintf(name, sizeof(name), "%s_%d", A.INVEL.c_str(), 0);
+    const size_t n = (size_t)A.NVAR * nxt * nyt * nzt;
+    std::vector<float> m(n);
+    FILE* f = fopen(name, "rb");
+    if (!f || fread(m.data(), sizeof(float), n, f) != n) {
+      printf("can't open file %s", name);
+      return 1;
+    }
+    fclose(f);
+    AWP(awp_upload_media(ctx, A.NVAR, m.data()));
+    AWP(awp_media_extrema(ctx, vse, vpe, dde));
+  } else {
+    fprintf(stderr, "pmcl3d: MEDIASTART=%d (partitioned meshes) is not part of this build\n",
+            A.MEDIASTART);
+    return 1;
+  }
+
+  // ---- CHK statistics file (writeCHK, io.c:9-43) -----------------------------
+  FILE* fchk = fopen(A.CHKFILE.c_str(), "w");
+  if (fchk) {
+    fprintf(fchk, "-------------------------------------------------------------\n");
+    fprintf(fchk, "GRID NUMBER:\t%d\n", 0);
+    fprintf(fchk, "STABILITY CRITERIA .5 > CMAX*DT/DX:\t%f\n", vpe[1] * A.DT / A.DH);
+    fprintf(fchk, "# OF X,Y,Z NODES PER PROC:\t%d, %d, %d\n", nxt, nyt, nzt);
+    fprintf(fchk, "DISCRETIZATION IN SPACE:\t%f\n", A.DH);
+    fprintf(fchk, "HIGHEST P-VELOCITY ENCOUNTERED:\t%f\n", vpe[1]);
+    fprintf(fchk, "LOWEST P-VELOCITY ENCOUNTERED:\t%f\n", vpe[0]);
+    fprintf(fchk, "HIGHEST S-VELOCITY ENCOUNTERED:\t%f\n", vse[1]);
+    fprintf(fchk, "LOWEST S-VELOCITY ENCOUNTERED:\t%f\n", vse[0]);
+    fprintf(fchk, "HIGHEST DENSITY ENCOUNTERED:\t%f\n", dde[1]);
+    fprintf(fchk, "LOWEST  DENSITY ENCOUNTERED:\t%f\n", dde[0]);
+    fprintf(fchk, "-------------------------------------------------------------\n");
+    fprintf(fchk, "# OF TIME STEPS:\t%ld\n", nt);
+    fprintf(fchk, "DISCRETIZATION IN TIME:\t%f\n", A.DT);
+    fprintf(fchk, "PML REFLECTION COEFFICIENT:\t%f\n", A.ARBC);
+    fprintf(fchk, "SKIP OF SEISMOGRAMS IN TIME (LOOP COUNTER):\t%d\n", A.NTISKP);
+    fprintf(fchk, "ABC CONDITION, PML=1 OR CERJAN=0:\t%d\n", A.NPC);
+    fprintf(fchk, "FD SCHEME, ELASTIC=0,VISCO=1,ELASTO-PLASTIC=2,VISCO-ELASTO-PLASTIC=3:\t%d\n",
+            A.NVE);
+    fprintf(fchk, "Q, FAC,Q0,EX,FP:\t%f, %f, %f, %f\n", A.FAC, A.Q0, A.EX, A.FP);
+    fclose(fchk);
+  }
+
+  // ---- plasticity set-up (inidrpr_hoekbrown_light, mesh.c:1178-1401) ----------
+  if (A.NVE == 3) {
+    std::vector<float> d1(ncell), mu(ncell), lam(ncell), sigma2(ncell, 0.f), cohes(ncell, 0.f),
+        phi(ncell, 0.f);
+    AWP(awp_field_download(ctx, AWP_D1, d1.data()));
+    AWP(awp_field_download(ctx, AWP_MU, mu.data()));
+    AWP(awp_field_download(ctx, AWP_LAM, lam.data()));
+    float strike[3] = {0, 0, 0}, dip[3] = {0, 90, 0}, fmajor = 0, fminor = 0, sigma_ci = 0, GSI = 0,
+          mi = 0, gsi100 = 1;
+    int sigma_ci_type = 0, fltpos = 0;
+    FILE* fid = fopen("nonlinear.dat", "r");
+    if (!fid) {
+      perror("could not open nonlinear.dat");
+      return 1;
+    }
+    char line[512];
+    if (fgets(line, sizeof line, fid)) sscanf(line, "%f %f", strike, strike + 2);
+    if (fgets(line, sizeof line, fid)) sscanf(line, "%f %f", &fmajor, &fminor);
+    if (fgets(line, sizeof line, fid)) sscanf(line, "%d %f", &sigma_ci_type, &sigma_ci);
+    if (fgets(line, sizeof line, fid)) sscanf(line, "%f", &GSI);
+    if (fgets(line, sizeof line, fid)) sscanf(line, "%f", &mi);
+    if (fgets(line, sizeof line, fid)) sscanf(line, "%f", &gsi100);
+    if (fgets(line, sizeof line, fid)) sscanf(line, "%d", &fltpos);
+    fclose(fid);
+    const long S = dims[1] * dims[2], Y = dims[2];
+    auto at = [&](int i, int j, int k) { return (size_t)(i * S + j * Y + k); };
+    const int sInd = nzt + ALIGN - 1;
+    const float dh = A.DH;
+    for (int j = 2; j < nyt + 2 + 2 * NGSL; j++)
+      for (int i = 2; i < nxt + 2 + 2 * NGSL; i++) {
+        sigma2[at(i, j, sInd)] = -dh / 2. * d1[at(i, j, sInd)] * 9.81;
+        sigma2[at(i, j, sInd + 1)] = sigma2[at(i, j, sInd)];
+        for (int k = sInd - 1; k >= ALIGN - 2; k--)
+          sigma2[at(i, j, k)] = sigma2[at(i, j, k + 1)] - dh * d1[at(i, j, k)] * 9.81;
+      }
+    for (int k = ALIGN; k <= sInd + 1; k++)
+      for (int j = 2; j < nyt + 2 + 2 * NGSL; j++)
+        for (int i = 2; i < nxt + 2 + 2 * NGSL; i++) {
+          const float depth = 0.5 * dh + dh * (sInd - k);
+          float GSI_wallrock = GSI + (100. - GSI) * (depth - 0.5 * dh) / gsi100, GSI_core, GSI_d;
+          if (GSI_wallrock > 100) GSI_wallrock = 100;
+          if (depth < 4000.) GSI_core = GSI;
+          else if (depth >= 4000. && depth <= 6000.)
+            GSI_core = GSI + (depth - 4000.) / 2000. * (GSI_wallrock - GSI);
+          else GSI_core = GSI_wallrock;
+          const int ypos = j - 2 - NGSL;
+          const float fltdist = fabsf((float)ypos + 0.5 - (float)fltpos) * dh;
+          if (fltdist < 225.) GSI_d = GSI_core;
+          else if (fltdist >= 225. && fltdist <= 750.)
+            GSI_d = GSI_core + (GSI_wallrock - GSI_core) * (fltdist - 225.) / (750. - 225.);
+          else GSI_d = GSI_wallrock;
+          const size_t q = at(i, j, k);
+          if (sigma_ci_type == 3) {
+            const float tvp = sqrt((1. / lam[q] + 2. / mu[q]) / d1[q]);
+            const float itime = 1. / tvp / 3.28 * 1.e6;
+            sigma_ci = 1.4138e7 * powf(itime, -3.) * 1.e6;
+          } else if (sigma_ci_type == 12) {
+            const float tvp = sqrt((1. / lam[q] + 2. / mu[q]) / d1[q]) / 1.e3;
+            sigma_ci = 0.77 * pow(tvp, 2.93) * 1.e6;
+          }
+          hoek_brown(-sigma2[q], sigma_ci, GSI_d, mi, 0, 1, &phi[q], &cohes[q]);
+          const float tvs = sqrtf(1. / (mu[q] * d1[q]));
+          if (tvs > 2000.) cohes[q] = 1.e12;
+          else if (tvs < 750.) {
+            cohes[q] = 0.f;
+            phi[q] = 35.f;
+          }
+        }
+    // no yielding around source nodes (pmcl3d.c:963-988)
+    for (int s = 0; s < nsrc; ++s) {
+      const int idx = spos[3 * s] + 1 + NGSL, idy = spos[3 * s + 1] + 1 + NGSL;
+      const int idz = (nzt + 1 - spos[3 * s + 2]) + ALIGN - 1;
+      for (int xi = idx - 1; xi < idx + 2; xi++)
+        for (int yi = idy - 2; yi < idy + 2; yi++)
+          for (int zi = idz - 1; zi < idz + 2; zi++) {
+            const bool dox = xi >= 0 && xi < nxt + 2 * NGSL + 1;
+            const bool doy = yi >= 0 && yi < nyt + 2 * NGSL + 1;
+            const bool doz = zi >= 0 && yi < nzt + 2 * NGSL + 1;
+            if (dox && doy && doz) cohes[at(xi, yi, zi)] = 1.e18;
+          }
+    }
+    AWP(awp_upload_plasticity(ctx, sigma2.data(), cohes.data(), phi.data(), fmajor, fminor,
+                              strike, dip));
+  }
+
+  // ---- output buffers ------------------------------------------------------------
+  const size_t rec = (size_t)rnx * rny * rnz;
+  std::vector<float> Bufx(rec * A.WRITE_STEP), Bufy(rec * A.WRITE_STEP), Bufz(rec * A.WRITE_STEP),
+      Bufeta(A.NVE == 3 ? rec * A.WRITE_STEP : 0);
+  float *d_bx = nullptr, *d_by = nullptr, *d_bz = nullptr, *d_be = nullptr;
+  std::vector<float> stage(rec);
+  if (rec) {
+    // device staging through the library's own allocation-free API is not
+    // needed: the gather writes straight into host-visible pinned memory
+    AWP(awp_alloc_host_pinned((void**)&d_bx, rec * sizeof(float)));
+    AWP(awp_alloc_host_pinned((void**)&d_by, rec * sizeof(float)));
+    AWP(awp_alloc_host_pinned((void**)&d_bz, rec * sizeof(float)));
+    if (A.NVE == 3) AWP(awp_alloc_host_pinned((void**)&d_be, rec * sizeof(float)));
+  }
+  mkdir(A.OUT.c_str(), 0755);
+  fchk = fopen(A.CHKFILE.c_str(), "a+");
+
+  time_init = now() - time_init;
+  printf("Initialization completed in %f s.\n", time_init);
+  printf("Time step \t Time \t\t Elapsed time \t sec per time step \t Time steps per sec \t "
+         "Percentage completed\n");
+  printf("---------------------------------------------------------------------------------"
+         "------------------------------------\n");
+  double time_un = 0;
+  long cur_step = 0;
+  if ((A.NPC == 0 || A.NPC == 2) && (A.NVE == 1 || A.NVE == 3)) {
+    time_un -= now();
+    for (cur_step = 1; cur_step <= nt; cur_step++) {
+      AWP(awp_step(ctx, 1));
+      if (cur_step % 10 == 0) {
+        AWP(awp_synchronize(ctx));
+        const double elapsed = now() + time_un;
+        const double step_s = elapsed / cur_step;
+        printf("%ld  \t\t %4.3f s \t %4.3f s \t %3.5f s/step \t %5.3f step/s \t %2.2f %%  \n",
+               cur_step, cur_step * A.DT, elapsed, step_s, 1.0 / step_s,
+               100 * (double)cur_step / (double)(nt - 1));
+        fflush(stdout);
+      }
+      if (cur_step % A.NTISKP == 0) {
+        if (rec) {
+          AWP(awp_gather_output(ctx, rnbgx, rnedx, A.NSKPX[0], rnbgy, rnedy, A.NSKPY[0], rnbgz,
+                                rnedz, A.NSKPZ[0], d_bx, d_by, d_bz, d_be));
+          AWP(awp_synchronize(ctx));
+          const long idtmp = ((cur_step / A.NTISKP + A.WRITE_STEP - 1) % A.WRITE_STEP) * rec;
+          memcpy(Bufx.data() + idtmp, d_bx, rec * 4);
+          memcpy(Bufy.data() + idtmp, d_by, rec * 4);
+          memcpy(Bufz.data() + idtmp, d_bz, rec * 4);
+          if (A.NVE == 3) memcpy(Bufeta.data() + idtmp, d_be, rec * 4);
+        }
+        if ((cur_step / A.NTISKP) % A.WRITE_STEP == 0 && rec) {
+          // file view of pmcl3d.c:489-521 at one rank: WRITE_STEP x rec_NZ x
+          // rec_NY x rec_NX floats, this rank's rec_nzt x rec_nyt x rec_nxt
+          // points at the origin (rows beyond them stay empty)
+          const char* base[4] = {"SX", "SY", "SZ", "Eta"};
+          std::vector<float>* bufs[4] = {&Bufx, &Bufy, &Bufz, &Bufeta};
+          const size_t fsz = (size_t)A.WRITE_STEP * recNZ * recNY * recNX;
+          std::vector<float> file(fsz);
+          for (int c = 0; c < (A.NVE == 3 ? 4 : 3); ++c) {
+            std::fill(file.begin(), file.end(), 0.f);
+            const float* b = bufs[c]->data();
+            for (int t = 0; t < A.WRITE_STEP; ++t)
+              for (int z = 0; z < rnz; ++z)
+                for (int y = 0; y < rny; ++y)
+                  memcpy(&file[(((size_t)t * recNZ + z) * recNY + y) * recNX],
+                         b + (((size_t)t * rnz + z) * rny + y) * rnx, rnx * sizeof(float));
+            char fn[600];
+            snprintf(fn, sizeof fn, "%s/%s_%1d_%07ld", A.OUT.c_str(), base[c], 0, cur_step);
+            FILE* fo = fopen(fn, "wb");
+            if (!fo) die("open output", AWP_ERR_IO);
+            fwrite(file.data(), sizeof(float), fsz, fo);
+            fclose(fo);
+          }
+        }
+        // statistics line (pmcl3d.c:2426-2437): the reference prints its host
+        // copies of u1/v1/w1, which are never refreshed from the device, so the
+        // values are the initial zeros
+        if (fchk) {
+          fprintf(fchk, "%ld :\t%e\t%e\t%e\n", cur_step, 0.0, 0.0, 0.0);
+          fflush(fchk);
+        }
+      }
+    }
+    AWP(awp_synchronize(ctx));
+    time_un += now();
+  }
+  if (A.IFAULT == 5 && nsrc) {
+    std::vector<float> mom(nsrc);
+    AWP(awp_download_moment(ctx, mom.data()));
+    float tmom = 0.0f;
+    for (float m : mom) tmom += m;
+    printf("rank %d: moment=%e\n", 0, tmom);
+    const float mag = 2. / 3. * (log10f(tmom) - 9.1);
+    printf("Total M0=%e, Mw=%4.1f\n", tmom, mag);
+  }
+  if (fchk) {
+    fprintf(fchk, "END\n");
+    fclose(fchk);
+  }
+  if (nt > 0 && cur_step > 1)
+    printf("%ld steps in %.3f s: %.6f s per time step, %.3f Gcell-updates/s\n", cur_step - 1,
+           time_un, time_un / (cur_step - 1),
+           (double)nxt * nyt * nzt * (cur_step - 1) / time_un / 1e9);
+  if (d_bx) awp_free_host_pinned(d_bx);
+  if (d_by) awp_free_host_pinned(d_by);
+  if (d_bz) awp_free_host_pinned(d_bz);
+  if (d_be) awp_free_host_pinned(d_be);
+  awp_ctx_destroy(ctx);
+  return 0;
+}

@@ -105,6 +105,13 @@ int awp_padded_dims(const awp_ctx* ctx, long long dims[3]);
 int awp_upload_media(awp_ctx* ctx, int nvar, const float* host_media);
 /* Same, with the media buffer already in device memory. */
 int awp_upload_media_device(awp_ctx* ctx, int nvar, const float* dev_media);
+/* Extrema of the corrected vs (vs > 1 m/s only), vp and rho of the last media
+ * upload, as inimesh reports them for the CHK file (mesh.c:455-460, io.c:23-31). */
+int awp_media_extrema(awp_ctx* ctx, float vse[2], float vpe[2], float dde[2]);
+
+/* Page-locked host buffers (for awp_gather_output targets). */
+int awp_alloc_host_pinned(void** ptr, size_t bytes);
+int awp_free_host_pinned(void* ptr);
 
 /* Point / kinematic sources in the INSRC layout (source.c:165-181):
  * pos[nsrc][3] = (x, y, z) 1-based with z counted down from the surface;

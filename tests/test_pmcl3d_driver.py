@@ -1,0 +1,93 @@
+"""The pmcl3d command-line drop-in: argument handling (CPU) and a full run with
+the reference's input and output files (GPU)."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from awp_b200 import Solver, default_params, scenarios
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+PMCL3D = os.path.join(ROOT, "awp_b200", "bin", "pmcl3d")
+
+
+def run(args, cwd, timeout=300):
+    return subprocess.run([PMCL3D] + [str(a) for a in args], cwd=cwd, capture_output=True,
+                          text=True, timeout=timeout)
+
+
+def test_binary_exists():
+    assert os.access(PMCL3D, os.X_OK)
+
+
+def test_rejects_multi_rank(tmp_path):
+    r = run(["-x", "2"], tmp_path)
+    assert r.returncode == 1 and "one rank" in r.stderr
+
+
+def test_nz_block_rule(tmp_path):
+    # pmcl3d.c:380-391: NZ must be divisible by BLOCK_SIZE_Z (4); the reference
+    # prints the message and returns 0
+    r = run(["-Z", "30"], tmp_path)
+    assert r.returncode == 0 and "not divisble by BLOCK_SIZE_Z" in r.stderr
+
+
+def test_unknown_option_prints_usage(tmp_path):
+    r = run(["--BOGUS", "1"], tmp_path)
+    assert r.returncode != 0
+
+
+def write_inputs(scn, d):
+    scn.media.astype(np.float32).tofile(os.path.join(d, "media_0"))
+    with open(os.path.join(d, "src_0"), "wb") as fh:
+        for s in range(scn.src_pos.shape[0]):
+            np.asarray(scn.src_pos[s], np.int32).tofile(fh)
+            np.asarray(scn.src_data[s], np.float32).tofile(fh)
+
+
+@pytest.mark.gpu
+def test_full_run_matches_library(tmp_path):
+    scn = scenarios.random_small(nx=24, ny=20, nz=32, steps=12, seed=9, ifault=1, nsrc=2)
+    p = scn.params
+    write_inputs(scn, tmp_path)
+    ntiskp, wstep, nt = 2, 3, 12
+    tmax = (nt - 1) * p["dt"] + p["dt"] * 0.5
+    args = ["-X", p["nx"], "-Y", p["ny"], "-Z", p["nz"], "-H", p["dh"], "-t", p["dt"],
+            "-T", tmax, "-D", p["nd"], "-A", p["arbc"], "-V", 1, "-B", 1, "-n", 5,
+            "-I", 1, "-S", scn.src_pos.shape[0], "-N", p["nst"], "-R", p["nst"],
+            "--INVEL", "media", "--INSRC", "src", "-o", "out", "-c", "chk",
+            "-r", ntiskp, "-W", wstep, "--NBGX", 1, "--NEDX", p["nx"], "--NSKPX", 2,
+            "--NBGY", 1, "--NSKPY", 3, "--NBGZ", 1, "--NEDZ", 3, "--NSKPZ", 1]
+    r = run(args, tmp_path)
+    assert r.returncode == 0, r.stderr + r.stdout
+    # the same run through the library
+    s = Solver(default_params(**p))
+    s.upload_media(scn.media)
+    s.upload_sources(scn.src_pos, scn.src_data)
+    import torch
+    rnx = (p["nx"] - 1) // 2 + 1
+    nedy = p["ny"] - (p["ny"] - 1) % 3
+    rny = (nedy - 1) // 3 + 1
+    rnz = 3
+    rec = rnx * rny * rnz
+    bufs = [torch.zeros(rec, device="cuda") for _ in range(3)]
+    frames = {c: [] for c in "XYZ"}
+    nedx = p["nx"] - (p["nx"] - 1) % 2
+    for step in range(1, nt + 1):
+        s.step(1)
+        if step % ntiskp == 0:
+            s.gather(0, nedx - 1, 2, 0, nedy - 1, 3, 0, 2, 1, *[b.data_ptr() for b in bufs])
+            for c, b in zip("XYZ", bufs):
+                frames[c].append(b.cpu().numpy().copy())
+    s.close()
+    for step in range(ntiskp * wstep, nt + 1, ntiskp * wstep):
+        n0 = step // ntiskp - wstep
+        for c in "XYZ":
+            f = os.path.join(tmp_path, "out", f"S{c}_0_{step:07d}")
+            got = np.fromfile(f, np.float32)
+            want = np.concatenate(frames[c][n0:n0 + wstep])
+            assert got.shape == want.shape, (c, got.shape, want.shape)
+            assert np.array_equal(got, want), (c, step)
+    chk = open(os.path.join(tmp_path, "chk")).read()
+    assert "STABILITY CRITERIA" in chk and chk.strip().endswith("END")
