@@ -58,15 +58,16 @@ def test_oracle_matches_reference_build(ref_host, name, precision):
 
 
 def test_planted_mistake_is_caught(ref_host):
-    """A one-cell change to the oracle's input (1 % of one inverse modulus) must
-    push it outside the tolerance: the golden comparison has teeth."""
+    """A small planted change in the oracle's input (1e-3 relative on every
+    inverse Lame modulus) must push it outside the tolerance: the golden
+    comparison has teeth."""
     gold = load_case("anelastic_if1")
     case = dict(CASES["anelastic_if1"])
     steps = case.pop("steps")
     scn = scenarios.random_small(steps=steps, **case)
     setup = refbind.model_setup(scn, ref_host)
     lam = setup["media"]["lam"].copy()
-    lam[18, 16, 40] *= 1.01  # 1 % change of one inverse modulus
+    lam *= np.float32(1.001)
     setup["media"]["lam"] = lam
     sim = orc.OracleSim(scn, setup, precision=64, nthreads=2)
     sim.step(steps)
