@@ -40,6 +40,11 @@ inline int round_up(int n, int m) { return (n + m - 1) / m * m; }
 
 }  // namespace
 
+// Lets other translation units of the library report through awp_last_error.
+void awp_internal_set_error(const char* msg) {
+  snprintf(g_errmsg, sizeof(g_errmsg), "%s", msg);
+}
+
 // ===========================================================================
 // Context
 // ===========================================================================

@@ -156,6 +156,29 @@ int awp_gather_output(awp_ctx* ctx, int nbgx, int nedx, int nskpx, int nbgy,
  * every value is finite. */
 int awp_check_finite(awp_ctx* ctx, int* ok);
 
+/* Allocation-free non-finite check -- no counterpart in the reference.
+ *
+ * For callers that own all the device memory they may use and cannot ask the
+ * CUDA allocator for more (a host code running the wavefield in its own
+ * pre-reserved pool, or a watchdog thread checking a running simulation
+ * between steps, where cudaMalloc could fail on a full device and cudaFree
+ * would wait for the whole device).  awp_check_finite needs a context, which
+ * allocates; this call allocates nothing.
+ *
+ * fields: host array of nfields device pointers, each to n floats.  On return
+ * ok[f] = 1 when every value of field f is finite, else 0.  Work is queued on
+ * `stream` (a cudaStream_t, NULL = legacy default stream) and the call waits
+ * for it.  nfields above AWP_NOALLOC_MAX_FIELDS is rejected with AWP_ERR_ARG.
+ *
+ * Scratch is one fixed device array of AWP_NOALLOC_MAX_FIELDS flags per GPU,
+ * held by every GPU that loads the library until the process exits.  The
+ * first call on a device looks its address up (and caches it), so make that
+ * first call before any stream capture.  All calls share the array: calls
+ * whose work overlaps on the GPU (other threads or streams) race on it. */
+#define AWP_NOALLOC_MAX_FIELDS 32
+int awp_check_finite_noalloc(const float* const* fields, int nfields, long long n, int* ok,
+                             void* stream);
+
 /* Per-phase device timing: when enabled, every subsequent awp_step records
  * CUDA events around each of its phases on the context's stream.
  * awp_phase_times waits for the stream and returns, per phase, the summed
