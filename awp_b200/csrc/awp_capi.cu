@@ -15,6 +15,7 @@
 #include "awp_common.h"
 #include "awp_host.h"
 #include "awp_kernels.cuh"
+#include "awp_tma.cuh"
 
 namespace {
 
@@ -78,6 +79,9 @@ struct awp_ctx {
   unsigned char* d_neta_mult = nullptr;
   unsigned int* d_flag = nullptr;
   unsigned int* d_ext = nullptr;  // media extrema (6 float bit patterns)
+  int* d_err = nullptr;           // pipeline-wait error word of the TMA kernels
+  bool tma_ok = false;            // tensor maps encoded for this context
+  TmaMaps vel_maps{}, str_maps{};
   long long cur_step = 0;
   bool initial_src_done = false;
   long long dev_bytes = 0;
@@ -208,6 +212,28 @@ int launch_plasticity(awp_ctx* c) {
   return AWP_OK;
 }
 
+// Tensor maps over the context's fields for the TMA-pipelined kernels.
+bool build_tma_maps(awp_ctx* c) {
+  int hx, hy, mx, my, ox, oy;
+  awp_tma_box(0, &hx, &hy);
+  awp_tma_box(1, &mx, &my);
+  awp_tma_box(2, &ox, &oy);
+  float** f = c->f;
+  const int vh[6] = {AWP_XX, AWP_YY, AWP_ZZ, AWP_XY, AWP_XZ, AWP_YZ};
+  const int vo[3] = {AWP_U1, AWP_V1, AWP_W1};
+  const int sm[4] = {AWP_LAM, AWP_MU, AWP_QP, AWP_QS};
+  const int so[12] = {AWP_XX, AWP_YY, AWP_ZZ, AWP_XY, AWP_XZ, AWP_YZ,
+                      AWP_R1, AWP_R2, AWP_R3, AWP_R4, AWP_R5, AWP_R6};
+  int bad = 0;
+  for (int q = 0; q < 6; ++q) bad |= awp_tma_encode(&c->vel_maps.halo[q], f[vh[q]], c->g, hx, hy);
+  bad |= awp_tma_encode(&c->vel_maps.media[0], f[AWP_D1], c->g, mx, my);
+  for (int q = 0; q < 3; ++q) bad |= awp_tma_encode(&c->vel_maps.own[q], f[vo[q]], c->g, ox, oy);
+  for (int q = 0; q < 3; ++q) bad |= awp_tma_encode(&c->str_maps.halo[q], f[vo[q]], c->g, hx, hy);
+  for (int q = 0; q < 4; ++q) bad |= awp_tma_encode(&c->str_maps.media[q], f[sm[q]], c->g, mx, my);
+  for (int q = 0; q < 12; ++q) bad |= awp_tma_encode(&c->str_maps.own[q], f[so[q]], c->g, ox, oy);
+  return bad == 0;
+}
+
 struct PhaseScope {
   awp_ctx* c;
   awp_ctx::PhaseEv ev{};
@@ -254,15 +280,24 @@ int one_step(awp_ctx* c) {
   v.j0 = 2 + AWP_NGSL; v.j1 = 2 + AWP_NGSL + round_up(c->g.nyt, 2) - 1;
   v.k0 = AWP_ALIGN; v.k1 = AWP_ALIGN + round_up(c->g.nzt, 4) - 1;
   v.dth = c->dth; v.c1 = c->c1; v.c2 = c->c2;
+  const bool tma = c->tma_ok && awp_tuning_get("tma") == 1;
   {
     PhaseScope ps(c, 0);
-    CU_TRY(awp_launch_velocity(v, c->stream));
+    if (tma)
+      CU_TRY(awp_launch_velocity_tma(v, c->vel_maps, awp_tuning_get("ichunk"), c->d_err,
+                                     c->stream));
+    else
+      CU_TRY(awp_launch_velocity(v, c->stream));
     c->launches++;
   }
   {
     PhaseScope ps(c, 1);
     StrArgs s = make_str_args(c);
-    CU_TRY(awp_launch_stress(s, c->elastic, c->stream));
+    if (tma)
+      CU_TRY(awp_launch_stress_tma(s, c->str_maps, c->elastic, awp_tuning_get("ichunk"),
+                                   c->d_err, c->stream));
+    else
+      CU_TRY(awp_launch_stress(s, c->elastic, c->stream));
     c->launches++;
   }
   if ((c->p.ifault < 4 && c->cur_step < c->p.nst) || c->p.ifault == 5) {
@@ -331,6 +366,7 @@ int awp_ctx_destroy(awp_ctx* c) {
   for (int i = 0; i < 6; ++i) cudaFree(c->d_src[i]);
   cudaFree(c->d_mom); cudaFree(c->d_filt); cudaFree(c->d_neta_mult); cudaFree(c->d_flag);
   cudaFree(c->d_ext);
+  cudaFree(c->d_err);
   for (auto& e : c->ev_used) { cudaEventDestroy(e.a); cudaEventDestroy(e.b); }
   for (auto& e : c->ev_free) { cudaEventDestroy(e.a); cudaEventDestroy(e.b); }
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
@@ -420,6 +456,12 @@ int awp_ctx_create(const awp_params* p, awp_ctx** out) {
   }
   if ((st = ctx_alloc(c, (void**)&c->d_flag, sizeof(unsigned int)))) goto fail;
   if ((st = ctx_alloc(c, (void**)&c->d_ext, 6 * sizeof(unsigned int)))) goto fail;
+  if ((st = ctx_alloc(c, (void**)&c->d_err, sizeof(int)))) goto fail;
+  if (cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream) != cudaSuccess) {
+    st = set_error(AWP_ERR_CUDA, "memset");
+    goto fail;
+  }
+  c->tma_ok = build_tma_maps(c);
   if (cudaStreamSynchronize(c->stream) != cudaSuccess) {
     st = set_error(AWP_ERR_CUDA, "initialisation");
     goto fail;
@@ -694,6 +736,10 @@ int awp_step(awp_ctx* c, int nsteps) {
 int awp_synchronize(awp_ctx* c) {
   if (!c) return set_error(AWP_ERR_ARG, "null context");
   CU_TRY(cudaStreamSynchronize(c->stream));
+  int err = 0;
+  CU_TRY(cudaMemcpy(&err, c->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (err)
+    return set_error(AWP_ERR_CUDA, "a TMA pipeline wait ran out of its iteration limit");
   return AWP_OK;
 }
 

@@ -18,6 +18,7 @@
 #include <string.h>
 
 #include "awp_kernels.cuh"
+#include "awp_stencil.cuh"
 
 #define LDG(p) __ldg(p)
 
@@ -27,6 +28,7 @@ namespace {
 int g_vel_ty = 8;
 int g_str_ty = 8;
 int g_ichunk = 32;
+int g_tma = 1;  // context API: TMA-pipelined kernels (1) or the read-only-path kernels (0)
 
 // ===========================================================================
 // Velocity (dvelcx_opt, kernel.cu:125-268)
@@ -109,23 +111,6 @@ __global__ void __launch_bounds__(32 * TY)
 // Stress + attenuation (dstrqc, kernel.cu:880-1197)
 // ===========================================================================
 
-// Q(f) weight (kernel.cu:974-1040).  The reference switches on
-// 1./(q*2.0) <= 200.0 evaluated in double; for float q that is exactly
-// (2q >= qthr) for positive q, true for negative q and -0, false for +0/NaN.
-__device__ __forceinline__ float qf_weight(float q, float wwo, float c0, float c1,
-                                           float qthr) {
-  const float x = 2.0f * q;
-  const bool low = (x >= qthr) || (x < 0.f) || (x == 0.f && signbit(x));
-  float w;
-  if (low) {
-    const double xd = 2.0 * (double)q;
-    w = (float)((double)c0 * xd * xd + (double)c1 * xd);
-  } else {
-    w = 2.0f * wwo * q;
-  }
-  return w / wwo;
-}
-
 struct Plane4 {  // one field at (j,k), (j-1,k), (j,k-1), (j-1,k-1) of a plane
   float a, b, c, d;
 };
@@ -145,75 +130,6 @@ __device__ __forceinline__ float sum8(const Plane4& c, const Plane4& n) {
   return c.a + n.a + c.b + n.b + c.c + n.c + c.d + n.d;
 }
 
-// One stress/memory-variable update of a cell (dstrqc, kernel.cu:1114-1179),
-// the state passed in and out through registers.
-template <bool ELASTIC>
-__device__ __forceinline__ void stress_update(float (&sg)[6], float (&rr)[6], float xl, float xm,
-                                              float xmu1, float xmu2, float xmu3, float h,
-                                              float h1, float h2, float h3, float qpa,
-                                              float vx1, float f_vx1, float f_vx2,
-                                              float f_wwo, float DT, float dcrj,
-                                              const float (&d)[9]) {
-  // d: vs1 vs2 vs3 (normal), xy pair, xz pair, yz pair
-  const float vs1 = d[0], vs2 = d[1], vs3 = d[2];
-  float tmp = xl * (vs1 + vs2 + vs3);
-  const float a1 = qpa * (vs1 + vs2 + vs3);
-  tmp = tmp + DT * a1;
-  if (ELASTIC) {
-    sg[0] = (sg[0] + tmp - xm * (vs2 + vs3)) * dcrj;
-    sg[1] = ((sg[1] + tmp - xm * (vs1 + vs3)) * dcrj) * dcrj;
-    sg[2] = ((sg[2] + tmp - xm * (vs1 + vs2)) * dcrj) * dcrj;
-    sg[3] = (sg[3] + xmu1 * (d[3] + d[4])) * dcrj;
-    sg[4] = (sg[4] + xmu2 * (d[5] + d[6])) * dcrj;
-    sg[5] = (sg[5] + xmu3 * (d[7] + d[8])) * dcrj;
-    return;
-  }
-  float f_r, f_rtmp, t;
-  f_r = rr[0];
-  f_rtmp = -h * (vs2 + vs3) + a1;
-  t = sg[0] + tmp - xm * (vs2 + vs3) + vx1 * f_r;
-  rr[0] = f_vx2 * f_r + f_wwo * f_rtmp;
-  f_rtmp = f_rtmp * (f_wwo - 1) + f_vx2 * f_r * (1 - f_vx1);
-  sg[0] = (t + DT * f_rtmp) * dcrj;
-
-  f_r = rr[1];
-  f_rtmp = -h * (vs1 + vs3) + a1;
-  t = (sg[1] + tmp - xm * (vs1 + vs3) + vx1 * f_r) * dcrj;
-  rr[1] = f_vx2 * f_r + f_wwo * f_rtmp;
-  f_rtmp = f_rtmp * (f_wwo - 1) + f_vx2 * f_r * (1 - f_vx1);
-  sg[1] = (t + DT * f_rtmp) * dcrj;
-
-  f_r = rr[2];
-  f_rtmp = -h * (vs1 + vs2) + a1;
-  t = (sg[2] + tmp - xm * (vs1 + vs2) + vx1 * f_r) * dcrj;
-  rr[2] = f_vx2 * f_r + f_wwo * f_rtmp;
-  f_rtmp = f_rtmp * (f_wwo - 1) + f_vx2 * f_r * (1 - f_vx1);
-  sg[2] = (t + DT * f_rtmp) * dcrj;
-
-  f_r = rr[3];
-  f_rtmp = h1 * (d[3] + d[4]);
-  t = sg[3] + xmu1 * (d[3] + d[4]) + vx1 * f_r;
-  rr[3] = f_vx2 * f_r + f_wwo * f_rtmp;
-  f_rtmp = f_rtmp * (f_wwo - 1) + f_vx2 * f_r * (1 - f_vx1);
-  sg[3] = (t + DT * f_rtmp) * dcrj;
-
-  f_r = rr[4];
-  f_rtmp = h2 * (d[5] + d[6]);
-  t = sg[4] + xmu2 * (d[5] + d[6]) + vx1 * f_r;
-  rr[4] = f_vx2 * f_r + f_wwo * f_rtmp;
-  f_rtmp = f_rtmp * (f_wwo - 1) + f_vx2 * f_r * (1 - f_vx1);
-  sg[4] = (t + DT * f_rtmp) * dcrj;
-
-  f_r = rr[5];
-  f_rtmp = h3 * (d[7] + d[8]);
-  t = sg[5] + xmu3 * (d[7] + d[8]) + vx1 * f_r;
-  rr[5] = f_vx2 * f_r + f_wwo * f_rtmp;
-  f_rtmp = f_rtmp * (f_wwo - 1) + f_vx2 * f_r * (1 - f_vx1);
-  sg[5] = (t + DT * f_rtmp) * dcrj;
-}
-
-// TY = 8: 256 threads held to 128 registers (2 CTAs / SM);
-// TY = 4: 128 threads without a register cap (3 CTAs / SM).
 template <bool ELASTIC, bool TEXARR, int TY>
 __global__ void __launch_bounds__(32 * TY, TY == 8 ? 2 : 1)
     k_stress(const StrArgs a, const int ichunk) {
@@ -314,11 +230,11 @@ __global__ void __launch_bounds__(32 * TY, TY == 8 ? 2 : 1)
         cc1 = a.coeff[cidx + 1];
       }
       const float qpaw =
-          qf_weight(0.0625f * sum8(qp_c, qp_n), f_wwo, cc0, cc1, a.qthr);
-      const float hw = qf_weight(0.0625f * sum8(qs_c, qs_n), f_wwo, cc0, cc1, a.qthr);
-      const float h1w = qf_weight(0.25f * (qs_c.a + qs_c.c), f_wwo, cc0, cc1, a.qthr);
-      const float h2w = qf_weight(0.25f * (qs_c.a + qs_c.b), f_wwo, cc0, cc1, a.qthr);
-      const float h3w = qf_weight(0.25f * (qs_c.a + qs_n.a), f_wwo, cc0, cc1, a.qthr);
+          awp_qf_weight(0.0625f * sum8(qp_c, qp_n), f_wwo, cc0, cc1, a.qthr);
+      const float hw = awp_qf_weight(0.0625f * sum8(qs_c, qs_n), f_wwo, cc0, cc1, a.qthr);
+      const float h1w = awp_qf_weight(0.25f * (qs_c.a + qs_c.c), f_wwo, cc0, cc1, a.qthr);
+      const float h2w = awp_qf_weight(0.25f * (qs_c.a + qs_c.b), f_wwo, cc0, cc1, a.qthr);
+      const float h3w = awp_qf_weight(0.25f * (qs_c.a + qs_n.a), f_wwo, cc0, cc1, a.qthr);
       h = -xm * hw * dh1;
       h1 = -xmu1 * h1w * dh1;
       h2 = -xmu2 * h2w * dh1;
@@ -376,7 +292,7 @@ __global__ void __launch_bounds__(32 * TY, TY == 8 ? 2 : 1)
     d[7] = c1 * (vk1 - v_0) + c2 * (vk2 - v_km1);
     d[8] = c1 * (w_jp1 - w_0) + c2 * (w_jp2 - w_jm1);
 
-    stress_update<ELASTIC>(sg, rr, xl, xm, xmu1, xmu2, xmu3, h, h1, h2, h3, qpa, vx1, f_vx1,
+    awp_stress_update<ELASTIC>(sg, rr, xl, xm, xmu1, xmu2, xmu3, h, h1, h2, h3, qpa, vx1, f_vx1,
                            f_vx2, f_wwo, DT, dcrj, d);
 #pragma unroll
     for (int q = 0; q < 6; ++q) SG[q][o] = sg[q];
@@ -1016,6 +932,7 @@ int awp_tuning_set(const char* key, int value) {
   if (!strcmp(key, "vel_ty") && (value == 4 || value == 8)) { g_vel_ty = value; return 0; }
   if (!strcmp(key, "str_ty") && (value == 4 || value == 8)) { g_str_ty = value; return 0; }
   if (!strcmp(key, "ichunk") && value >= 4 && value <= 1024) { g_ichunk = value; return 0; }
+  if (!strcmp(key, "tma") && (value == 0 || value == 1)) { g_tma = value; return 0; }
   return 1;
 }
 
@@ -1023,6 +940,7 @@ int awp_tuning_get(const char* key) {
   if (!strcmp(key, "vel_ty")) return g_vel_ty;
   if (!strcmp(key, "str_ty")) return g_str_ty;
   if (!strcmp(key, "ichunk")) return g_ichunk;
+  if (!strcmp(key, "tma")) return g_tma;
   return -1;
 }
 

@@ -1,0 +1,573 @@
+// TMA-pipelined stencil kernels for the context API (sm_100a).
+//
+// Each CTA owns a tile of 32 k (one 128-byte line) x 8 j and marches a chunk of
+// x planes.  Per plane, one elected thread issues cp.async.bulk.tensor loads of
+// the plane's tiles (with the j/k halo the stencil needs) into shared-memory
+// rings; completion is tracked by one mbarrier per ring slot.  The loads run
+// several planes ahead of the arithmetic, so the HBM latency is hidden by the
+// pipeline rather than by occupancy, and every x plane of every field is read
+// from HBM once per chunk.  Results are stored straight from registers with
+// coalesced 128-byte rows.
+//
+// Tile boxes (x = k fastest, y = j, z = i), all 16-byte aligned in x:
+//   halo   : k in [kb-4, kb+36), j in [jb-2, jb+10)   40 x 12 floats
+//   media  : k in [kb-4, kb+32), j in [jb-1, jb+8)    36 x  9 floats
+//   own    : k in [kb,   kb+32), j in [jb,   jb+8)    32 x  8 floats
+//
+// Every wait on an mbarrier is bounded; a wait that runs out sets the
+// context's error word and the whole CTA leaves the march together.
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <cudaTypedefs.h>
+#include <math.h>
+#include <stdint.h>
+
+#include "awp_kernels.cuh"
+#include "awp_stencil.cuh"
+#include "awp_tma.cuh"
+
+#define LDG(p) __ldg(p)
+
+namespace {
+
+constexpr int TZ = 32, TY = 8, NT = TZ * TY;
+constexpr int HX = 40, HY = 12, HTILE = HX * HY;     // halo tile (floats)
+constexpr int MX = 36, MY = 9, MTILE_B = MX * MY * 4; // media tile bytes (1296)
+constexpr int MTILE = 352;                            // media tile stride (floats, 1408 B)
+constexpr int OTILE = TZ * TY;                        // own tile (floats)
+constexpr int DH_ = 7;                                // halo ring depth (planes i-2..i+2 + 2)
+constexpr int DM_ = 4;                                // media ring depth (planes i, i+1 + 2)
+constexpr int DO_ = 3;                                // own ring depth (plane i + 2)
+constexpr unsigned kSpinLimit = 1u << 26;
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+  return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// bounded wait: false when the limit ran out
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
+  for (unsigned n = 0; n < kSpinLimit; ++n)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+__device__ __forceinline__ void tma_load3(void* dst, const CUtensorMap* map, uint64_t* bar,
+                                          int x, int y, int z) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// One ring of per-plane slots with their mbarriers.
+struct Ring {
+  float* buf;
+  uint64_t* bar;
+  int depth, slot_floats, base;  // base = first plane of the march for this ring
+  __device__ int slot(int p) const { return (p - base) % depth; }
+  __device__ unsigned parity(int p) const { return ((p - base) / depth) & 1; }
+  __device__ float* at(int p) const { return buf + slot(p) * slot_floats; }
+  __device__ uint64_t* b(int p) const { return bar + slot(p); }
+};
+
+// ===========================================================================
+// Stress + memory variables (dstrqc, kernel.cu:880-1197), same arithmetic as
+// k_stress in awp_kernels.cu (see there for the term-by-term citation).
+// ===========================================================================
+template <bool ELASTIC>
+__global__ void __launch_bounds__(NT, 2)
+    k_stress_tma(const StrArgs a, const __grid_constant__ TmaMaps tm, const int ichunk,
+                 int* err) {
+  constexpr int NM = ELASTIC ? 2 : 4;   // lam, mu (, qp, qs)
+  constexpr int NO = ELASTIC ? 6 : 12;  // xx..yz (, r1..r6)
+  extern __shared__ __align__(128) float smem[];
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TZ + tx;
+  const int kb = AWP_ALIGN + blockIdx.x * TZ;
+  const int jb = a.j0 + blockIdx.y * TY;
+  const int k = kb + tx, j = jb + ty;
+  const int ib = a.i0 + blockIdx.z * ichunk;
+  const int ie = min(ib + ichunk - 1, a.i1);
+  const bool active = (k >= a.k0) && (k <= a.k1) && (j <= a.j1);
+
+  Ring rh{smem, nullptr, DH_, 3 * HTILE, ib - 2};
+  Ring rm{rh.buf + DH_ * 3 * HTILE, nullptr, DM_, NM * MTILE, ib};
+  Ring ro{rm.buf + DM_ * NM * MTILE, nullptr, DO_, NO * OTILE, ib};
+  uint64_t* bars = reinterpret_cast<uint64_t*>(ro.buf + DO_ * NO * OTILE);
+  rh.bar = bars;
+  rm.bar = bars + DH_;
+  ro.bar = bars + DH_ + DM_;
+
+  // producer: one thread issues a plane's tiles and arms its barrier
+  auto issue_halo = [&](int p) {
+    if (p > ie + 2) return;
+    mbar_expect_tx(rh.b(p), 3 * HTILE * 4);
+    float* d = rh.at(p);
+    for (int f = 0; f < 3; ++f) tma_load3(d + f * HTILE, &tm.halo[f], rh.b(p), kb - 4, jb - 2, p);
+  };
+  auto issue_media = [&](int p) {
+    if (p > ie + 1) return;
+    mbar_expect_tx(rm.b(p), NM * MTILE_B);
+    float* d = rm.at(p);
+    for (int f = 0; f < NM; ++f) tma_load3(d + f * MTILE, &tm.media[f], rm.b(p), kb - 4, jb - 1, p);
+  };
+  auto issue_own = [&](int p) {
+    if (p > ie) return;
+    mbar_expect_tx(ro.b(p), NO * OTILE * 4);
+    float* d = ro.at(p);
+    for (int f = 0; f < NO; ++f) tma_load3(d + f * OTILE, &tm.own[f], ro.b(p), kb, jb, p);
+  };
+
+  if (tid == 0) {
+    for (int q = 0; q < DH_ + DM_ + DO_; ++q) mbar_init(bars + q, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  // next plane to issue per ring (meaningful in the producer thread only)
+  int nh = ib - 2, nm = ib, no = ib;
+  if (tid == 0) {
+    for (; nh < ib - 2 + DH_; ++nh) issue_halo(nh);
+    for (; nm < ib + DM_; ++nm) issue_media(nm);
+    for (; no < ib + DO_; ++no) issue_own(no);
+  }
+
+  const int S = a.slice, Y = a.yline;
+  const float c1 = a.c1, c2 = a.c2, DT = a.dt, dth = a.dth, dh1 = a.dh1;
+  const float dcy = LDG(a.dcrjy + min(j, a.j1)), dcz = LDG(a.dcrjz + min(max(k, a.k0), a.k1));
+  const long long col = (long long)j * Y + k;
+  const bool top = a.fs && (k == a.ktop);
+  const bool top1 = a.fs && (k == a.ktop - 1);
+  float* __restrict__ SG[6] = {a.xx, a.yy, a.zz, a.xy, a.xz, a.yz};
+  float* __restrict__ RR[6] = {a.r1, a.r2, a.r3, a.r4, a.r5, a.r6};
+  const int hoff = (ty + 2) * HX + (tx + 4);
+  const int moff = (ty + 1) * MX + (tx + 4);
+  const int ooff = ty * TZ + tx;
+  bool ok = true, aborted = false;
+
+  for (int i = ib; i <= ie; ++i) {
+    // ---- wait for the planes this step reads for the first time ------------
+    if (i == ib) {
+      for (int p = ib - 2; p <= ib + 2 && ok; ++p) ok = mbar_wait(rh.b(p), rh.parity(p));
+      if (ok) ok = mbar_wait(rm.b(ib), rm.parity(ib));
+    } else {
+      ok = mbar_wait(rh.b(i + 2), rh.parity(i + 2));
+    }
+    if (ok) ok = mbar_wait(rm.b(i + 1), rm.parity(i + 1));
+    if (ok) ok = mbar_wait(ro.b(i), ro.parity(i));
+    if (__syncthreads_or(!ok)) {
+      aborted = true;
+      break;
+    }
+
+    const float* Hm2 = rh.at(i - 2) + hoff;
+    const float* Hm1 = rh.at(i - 1) + hoff;
+    const float* H0 = rh.at(i) + hoff;
+    const float* Hp1 = rh.at(i + 1) + hoff;
+    const float* Hp2 = rh.at(i + 2) + hoff;
+    // field f of a halo plane: + f * HTILE; neighbour (dj, dk): + dj * HX + dk
+    const float u_m1 = Hm1[0], u_0 = H0[0], u_p1 = Hp1[0], u_p2 = Hp2[0];
+    const float v_m2 = Hm2[HTILE], v_m1 = Hm1[HTILE], v_0 = H0[HTILE], v_p1 = Hp1[HTILE];
+    const float w_m2 = Hm2[2 * HTILE], w_m1 = Hm1[2 * HTILE], w_0 = H0[2 * HTILE],
+                w_p1 = Hp1[2 * HTILE];
+    const float* U0 = H0;
+    const float* V0 = H0 + HTILE;
+    const float* W0 = H0 + 2 * HTILE;
+    const float u_jp1 = U0[HX], u_jp2 = U0[2 * HX], u_jm1 = U0[-HX], u_km1 = U0[-1];
+    const float v_jm1 = V0[-HX], v_jp1 = V0[HX], v_jm2 = V0[-2 * HX], v_km1 = V0[-1];
+    const float w_km1 = W0[-1], w_km2 = W0[-2], w_jp1 = W0[HX], w_jp2 = W0[2 * HX],
+                w_jm1 = W0[-HX];
+    float uk1 = U0[1], vk1 = V0[1], wk1 = W0[1], uk2 = U0[2], vk2 = V0[2];
+
+    const float* Mc = rm.at(i) + moff;
+    const float* Mn = rm.at(i + 1) + moff;
+    // (j,k), (j-1,k), (j,k-1), (j-1,k-1) of a media tile
+    auto m4 = [&](const float* m, int f, float& pa, float& pb, float& pc, float& pd) {
+      const float* q = m + f * MTILE;
+      pa = q[0];
+      pb = q[-MX];
+      pc = q[-1];
+      pd = q[-MX - 1];
+    };
+    float la, lb, lc, ld, na, nb, nc, nd;
+    m4(Mc, 0, la, lb, lc, ld);
+    m4(Mn, 0, na, nb, nc, nd);
+    float xl = (float)(8.0 / (double)(la + na + lb + nb + lc + nc + ld + nd));
+    float ma, mb, mc, md, pa, pb, pc, pd;
+    m4(Mc, 1, ma, mb, mc, md);
+    m4(Mn, 1, pa, pb, pc, pd);
+    float xm = (float)(16.0 / (double)(ma + pa + mb + pb + mc + pc + md + pd));
+    float xmu1 = (float)(2.0 / (double)(ma + mc));
+    float xmu2 = (float)(2.0 / (double)(ma + mb));
+    float xmu3 = (float)(2.0 / (double)(ma + pa));
+    xl = xl + xm;
+
+    const int t = awp_tex_index(a.tex, i, j, k);
+    const float f_vx1 = a.tex.tau1[t], f_vx2 = a.tex.tau2[t], f_wwo = a.tex.wwo8[t];
+    float h = 0.f, h1 = 0.f, h2 = 0.f, h3 = 0.f, qpa = 0.f;
+    if (!ELASTIC) {
+      const float cc0 = a.coeff[2 * t], cc1 = a.coeff[2 * t + 1];
+      float qa, qb, qc, qd, ra, rb, rc, rd;
+      m4(Mc, 2, qa, qb, qc, qd);
+      m4(Mn, 2, ra, rb, rc, rd);
+      const float qpaw = awp_qf_weight(0.0625f * (qa + ra + qb + rb + qc + rc + qd + rd), f_wwo,
+                                     cc0, cc1, a.qthr);
+      m4(Mc, 3, qa, qb, qc, qd);
+      m4(Mn, 3, ra, rb, rc, rd);
+      const float hw = awp_qf_weight(0.0625f * (qa + ra + qb + rb + qc + rc + qd + rd), f_wwo,
+                                   cc0, cc1, a.qthr);
+      const float h1w = awp_qf_weight(0.25f * (qa + qc), f_wwo, cc0, cc1, a.qthr);
+      const float h2w = awp_qf_weight(0.25f * (qa + qb), f_wwo, cc0, cc1, a.qthr);
+      const float h3w = awp_qf_weight(0.25f * (qa + ra), f_wwo, cc0, cc1, a.qthr);
+      h = -xm * hw * dh1;
+      h1 = -xmu1 * h1w * dh1;
+      h2 = -xmu2 * h2w * dh1;
+      h3 = -xmu3 * h3w * dh1;
+      qpa = -qpaw * xl * dh1;
+    }
+    xm = xm * dth;
+    xmu1 = xmu1 * dth;
+    xmu2 = xmu2 * dth;
+    xmu3 = xmu3 * dth;
+    xl = xl * dth;
+    float vx1 = 0.f;
+    if (!ELASTIC) {
+      h = h * f_vx1;
+      h1 = h1 * f_vx1;
+      h2 = h2 * f_vx1;
+      h3 = h3 * f_vx1;
+      qpa = qpa * f_vx1;
+      xm = xm + DT * h;
+      xmu1 = xmu1 + DT * h1;
+      xmu2 = xmu2 + DT * h2;
+      xmu3 = xmu3 + DT * h3;
+      vx1 = DT * (1 + f_vx2 * f_vx1);
+    }
+    const float dcrj = LDG(a.dcrjx + i) * dcy * dcz;
+    const long long o = (long long)i * S;
+
+    if (top && active) {
+      const float uimg = u_0 - (w_0 - w_m1);
+      const float vimg = v_0 - (w_jp1 - w_0);
+      const float vs1 = (i < a.gx_lim) ? u_p1 - (w_p1 - w_0) : 0.0f;
+      const float vs2 = (j >= a.gy_min) ? v_jm1 - (w_0 - w_jm1) : 0.0f;
+      const float wimg =
+          w_km1 - LDG(a.lam_mu + (long long)i * a.lam_mu_ld + j) *
+                      ((vs1 - uimg) + (u_p1 - u_0) + (vimg - vs2) + (v_0 - v_jm1));
+      a.u1[col + o + 1] = uimg;
+      a.v1[col + o + 1] = vimg;
+      a.w1[col + o + 1] = wimg;
+      uk1 = uimg;
+      vk1 = vimg;
+      wk1 = wimg;
+    } else if (top1) {
+      uk2 = uk1 - (wk1 - Hm1[2 * HTILE + 1]);
+      vk2 = vk1 - (W0[HX + 1] - wk1);
+    }
+
+    float d[9];
+    d[0] = c1 * (u_p1 - u_0) + c2 * (u_p2 - u_m1);
+    d[1] = c1 * (v_0 - v_jm1) + c2 * (v_jp1 - v_jm2);
+    d[2] = c1 * (w_0 - w_km1) + c2 * (wk1 - w_km2);
+    d[3] = c1 * (u_jp1 - u_0) + c2 * (u_jp2 - u_jm1);
+    d[4] = c1 * (v_0 - v_m1) + c2 * (v_p1 - v_m2);
+    d[5] = c1 * (uk1 - u_0) + c2 * (uk2 - u_km1);
+    d[6] = c1 * (w_0 - w_m1) + c2 * (w_p1 - w_m2);
+    d[7] = c1 * (vk1 - v_0) + c2 * (vk2 - v_km1);
+    d[8] = c1 * (w_jp1 - w_0) + c2 * (w_jp2 - w_jm1);
+
+    const float* O = ro.at(i) + ooff;
+    float sg[6], rr[6];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) sg[q] = O[q * OTILE];
+    if (!ELASTIC) {
+#pragma unroll
+      for (int q = 0; q < 6; ++q) rr[q] = O[(6 + q) * OTILE];
+    }
+    awp_stress_update<ELASTIC>(sg, rr, xl, xm, xmu1, xmu2, xmu3, h, h1, h2, h3, qpa, vx1, f_vx1,
+                               f_vx2, f_wwo, DT, dcrj, d);
+    if (active) {
+#pragma unroll
+      for (int q = 0; q < 6; ++q) SG[q][col + o] = sg[q];
+      if (!ELASTIC) {
+#pragma unroll
+        for (int q = 0; q < 6; ++q) RR[q][col + o] = rr[q];
+      }
+    }
+
+    // ---- every thread is done with halo plane i-2, media plane i, own plane i
+    __syncthreads();
+    if (tid == 0) {
+      issue_halo(nh++);
+      issue_media(nm++);
+      issue_own(no++);
+    }
+  }
+  if (aborted) {
+    if (tid == 0) {
+      atomicExch(err, 1);
+      // let copies still in flight land before the CTA's shared memory is released
+      for (int p = max(nh - DH_, ib - 2); p < nh && p <= ie + 2; ++p)
+        (void)mbar_wait(rh.b(p), rh.parity(p));
+      for (int p = max(nm - DM_, ib); p < nm && p <= ie + 1; ++p)
+        (void)mbar_wait(rm.b(p), rm.parity(p));
+      for (int p = max(no - DO_, ib); p < no && p <= ie; ++p)
+        (void)mbar_wait(ro.b(p), ro.parity(p));
+    }
+    __syncthreads();
+  }
+}
+
+// ===========================================================================
+// Velocity (dvelcx_opt, kernel.cu:125-268), same arithmetic as k_velocity.
+// Rings: stress halo tiles (6 fields, planes i-2..i+2), density (planes i,
+// i+1), own velocity tiles (plane i).
+// ===========================================================================
+__global__ void __launch_bounds__(NT, 2)
+    k_velocity_tma(const VelArgs a, const __grid_constant__ TmaMaps tm, const int ichunk,
+                   int* err) {
+  extern __shared__ __align__(128) float smem[];
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TZ + tx;
+  const int kb = AWP_ALIGN + blockIdx.x * TZ;
+  const int jb = a.j0 + blockIdx.y * TY;
+  const int k = kb + tx, j = jb + ty;
+  const int ib = a.i0 + blockIdx.z * ichunk;
+  const int ie = min(ib + ichunk - 1, a.i1);
+  const bool active = (k >= a.k0) && (k <= a.k1) && (j <= a.j1);
+
+  Ring rh{smem, nullptr, DH_, 6 * HTILE, ib - 2};
+  Ring rm{rh.buf + DH_ * 6 * HTILE, nullptr, DM_, MTILE, ib};
+  Ring ro{rm.buf + DM_ * MTILE, nullptr, DO_, 3 * OTILE, ib};
+  uint64_t* bars = reinterpret_cast<uint64_t*>(ro.buf + DO_ * 3 * OTILE);
+  rh.bar = bars;
+  rm.bar = bars + DH_;
+  ro.bar = bars + DH_ + DM_;
+
+  auto issue_halo = [&](int p) {
+    if (p > ie + 2) return;
+    mbar_expect_tx(rh.b(p), 6 * HTILE * 4);
+    float* d = rh.at(p);
+    for (int f = 0; f < 6; ++f) tma_load3(d + f * HTILE, &tm.halo[f], rh.b(p), kb - 4, jb - 2, p);
+  };
+  auto issue_media = [&](int p) {
+    if (p > ie + 1) return;
+    mbar_expect_tx(rm.b(p), MTILE_B);
+    tma_load3(rm.at(p), &tm.media[0], rm.b(p), kb - 4, jb - 1, p);
+  };
+  auto issue_own = [&](int p) {
+    if (p > ie) return;
+    mbar_expect_tx(ro.b(p), 3 * OTILE * 4);
+    float* d = ro.at(p);
+    for (int f = 0; f < 3; ++f) tma_load3(d + f * OTILE, &tm.own[f], ro.b(p), kb, jb, p);
+  };
+
+  if (tid == 0) {
+    for (int q = 0; q < DH_ + DM_ + DO_; ++q) mbar_init(bars + q, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  // next plane to issue per ring (meaningful in the producer thread only)
+  int nh = ib - 2, nm = ib, no = ib;
+  if (tid == 0) {
+    for (; nh < ib - 2 + DH_; ++nh) issue_halo(nh);
+    for (; nm < ib + DM_; ++nm) issue_media(nm);
+    for (; no < ib + DO_; ++no) issue_own(no);
+  }
+
+  const int S = a.slice, Y = a.yline;
+  const float c1 = a.c1, c2 = a.c2, dth = a.dth;
+  const float dcy = LDG(a.dcrjy + min(j, a.j1)), dcz = LDG(a.dcrjz + min(k, a.k1));
+  const long long col = (long long)j * Y + k;
+  const int hoff = (ty + 2) * HX + (tx + 4);
+  const int moff = (ty + 1) * MX + (tx + 4);
+  const int ooff = ty * TZ + tx;
+  bool ok = true, aborted = false;
+
+  for (int i = ib; i <= ie; ++i) {
+    if (i == ib) {
+      for (int p = ib - 2; p <= ib + 2 && ok; ++p) ok = mbar_wait(rh.b(p), rh.parity(p));
+      if (ok) ok = mbar_wait(rm.b(ib), rm.parity(ib));
+    } else {
+      ok = mbar_wait(rh.b(i + 2), rh.parity(i + 2));
+    }
+    if (ok) ok = mbar_wait(rm.b(i + 1), rm.parity(i + 1));
+    if (ok) ok = mbar_wait(ro.b(i), ro.parity(i));
+    if (__syncthreads_or(!ok)) {
+      aborted = true;
+      break;
+    }
+
+    // halo fields: 0 xx, 1 yy, 2 zz, 3 xy, 4 xz, 5 yz
+    const float* Hm2 = rh.at(i - 2) + hoff;
+    const float* Hm1 = rh.at(i - 1) + hoff;
+    const float* H0 = rh.at(i) + hoff;
+    const float* Hp1 = rh.at(i + 1) + hoff;
+    const float* Hp2 = rh.at(i + 2) + hoff;
+    const float xx_m2 = Hm2[0], xx_m1 = Hm1[0], xx_0 = H0[0], xx_p1 = Hp1[0];
+    const float xy_m1 = Hm1[3 * HTILE], xy_0 = H0[3 * HTILE], xy_p1 = Hp1[3 * HTILE],
+                xy_p2 = Hp2[3 * HTILE];
+    const float xz_m1 = Hm1[4 * HTILE], xz_0 = H0[4 * HTILE], xz_p1 = Hp1[4 * HTILE],
+                xz_p2 = Hp2[4 * HTILE];
+    const float* YY = H0 + HTILE;
+    const float* ZZ = H0 + 2 * HTILE;
+    const float* XY = H0 + 3 * HTILE;
+    const float* XZ = H0 + 4 * HTILE;
+    const float* YZ = H0 + 5 * HTILE;
+    const float yz_0 = YZ[0];
+
+    const float* Dc = rm.at(i) + moff;
+    const float* Dn = rm.at(i + 1) + moff;
+    const float d_0 = Dc[0], d_0j = Dc[-MX], d_0k = Dc[-1], d_0jk = Dc[-MX - 1];
+    const float d_p = Dn[0], d_pj = Dn[-MX], d_pk = Dn[-1];
+
+    float fd1 = 0.25f * (d_0 + d_0j + d_0k + d_0jk);
+    float fd2 = 0.25f * (d_0 + d_p + d_0k + d_pk);
+    float fd3 = 0.25f * (d_0 + d_p + d_0j + d_pj);
+    fd1 = dth / fd1;
+    fd2 = dth / fd2;
+    fd3 = dth / fd3;
+    const float dcrj = LDG(a.dcrjx + i) * dcy * dcz;
+
+    const float* O = ro.at(i) + ooff;
+    const float u = (O[0] + fd1 * (c1 * (xx_0 - xx_m1) + c2 * (xx_p1 - xx_m2) +
+                                   c1 * (xy_0 - XY[-HX]) + c2 * (XY[HX] - XY[-2 * HX]) +
+                                   c1 * (xz_0 - XZ[-1]) + c2 * (XZ[1] - XZ[-2]))) *
+                    dcrj;
+    const float v = (O[OTILE] + fd2 * (c1 * (xy_p1 - xy_0) + c2 * (xy_p2 - xy_m1) +
+                                       c1 * (YY[HX] - YY[0]) + c2 * (YY[2 * HX] - YY[-HX]) +
+                                       c1 * (yz_0 - YZ[-1]) + c2 * (YZ[1] - YZ[-2]))) *
+                    dcrj;
+    const float w = (O[2 * OTILE] + fd3 * (c1 * (xz_p1 - xz_0) + c2 * (xz_p2 - xz_m1) +
+                                           c1 * (yz_0 - YZ[-HX]) + c2 * (YZ[HX] - YZ[-2 * HX]) +
+                                           c1 * (ZZ[1] - ZZ[0]) + c2 * (ZZ[2] - ZZ[-1]))) *
+                    dcrj;
+    if (active) {
+      const long long o = (long long)i * S + col;
+      a.u1[o] = u;
+      a.v1[o] = v;
+      a.w1[o] = w;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      issue_halo(nh++);
+      issue_media(nm++);
+      issue_own(no++);
+    }
+  }
+  if (aborted) {
+    if (tid == 0) {
+      atomicExch(err, 1);
+      for (int p = max(nh - DH_, ib - 2); p < nh && p <= ie + 2; ++p)
+        (void)mbar_wait(rh.b(p), rh.parity(p));
+      for (int p = max(nm - DM_, ib); p < nm && p <= ie + 1; ++p)
+        (void)mbar_wait(rm.b(p), rm.parity(p));
+      for (int p = max(no - DO_, ib); p < no && p <= ie; ++p)
+        (void)mbar_wait(ro.b(p), ro.parity(p));
+    }
+    __syncthreads();
+  }
+}
+
+inline unsigned cdiv_u(long long a, long long b) { return (unsigned)((a + b - 1) / b); }
+
+size_t stress_smem(bool elastic) {
+  const int nm = elastic ? 2 : 4, no = elastic ? 6 : 12;
+  return sizeof(float) * ((size_t)DH_ * 3 * HTILE + (size_t)DM_ * nm * MTILE +
+                          (size_t)DO_ * no * OTILE) +
+         sizeof(uint64_t) * (DH_ + DM_ + DO_);
+}
+size_t velocity_smem() {
+  return sizeof(float) * ((size_t)DH_ * 6 * HTILE + (size_t)DM_ * MTILE + (size_t)DO_ * 3 * OTILE) +
+         sizeof(uint64_t) * (DH_ + DM_ + DO_);
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }
+  return fn;
+}
+
+}  // namespace
+
+int awp_tma_encode(CUtensorMap* map, const float* base, const AwpGeom& g, int box_x, int box_y) {
+  auto fn = encode_fn();
+  if (!fn) return 1;
+  const cuuint64_t dims[3] = {(cuuint64_t)g.nz_pad(), (cuuint64_t)g.ny_pad(),
+                              (cuuint64_t)g.nx_pad()};
+  const cuuint64_t strides[2] = {(cuuint64_t)g.yline * 4, (cuuint64_t)g.slice * 4};
+  const cuuint32_t box[3] = {(cuuint32_t)box_x, (cuuint32_t)box_y, 1};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  const CUresult r =
+      fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(base), dims, strides, box,
+         estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+         CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? 0 : 2;
+}
+
+int awp_tma_box(int group, int* bx, int* by) {
+  switch (group) {
+    case 0: *bx = HX; *by = HY; return 0;   // halo
+    case 1: *bx = MX; *by = MY; return 0;   // media
+    case 2: *bx = TZ; *by = TY; return 0;   // own
+  }
+  return 1;
+}
+
+cudaError_t awp_launch_stress_tma(const StrArgs& a, const TmaMaps& tm, bool elastic, int ichunk,
+                                  int* err, cudaStream_t st) {
+  const int nk = a.k1 - AWP_ALIGN + 1, nj = a.j1 - a.j0 + 1, ni = a.i1 - a.i0 + 1;
+  if (nk <= 0 || nj <= 0 || ni <= 0) return cudaSuccess;
+  const dim3 block(TZ, TY, 1);
+  const dim3 grid(cdiv_u(nk, TZ), cdiv_u(nj, TY), cdiv_u(ni, ichunk));
+  const size_t sm = stress_smem(elastic);
+  cudaError_t e;
+  if (elastic) {
+    e = cudaFuncSetAttribute(k_stress_tma<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sm);
+    if (e != cudaSuccess) return e;
+    k_stress_tma<true><<<grid, block, sm, st>>>(a, tm, ichunk, err);
+  } else {
+    e = cudaFuncSetAttribute(k_stress_tma<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sm);
+    if (e != cudaSuccess) return e;
+    k_stress_tma<false><<<grid, block, sm, st>>>(a, tm, ichunk, err);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t awp_launch_velocity_tma(const VelArgs& a, const TmaMaps& tm, int ichunk, int* err,
+                                    cudaStream_t st) {
+  const int nk = a.k1 - AWP_ALIGN + 1, nj = a.j1 - a.j0 + 1, ni = a.i1 - a.i0 + 1;
+  if (nk <= 0 || nj <= 0 || ni <= 0) return cudaSuccess;
+  const dim3 block(TZ, TY, 1);
+  const dim3 grid(cdiv_u(nk, TZ), cdiv_u(nj, TY), cdiv_u(ni, ichunk));
+  const size_t sm = velocity_smem();
+  cudaError_t e =
+      cudaFuncSetAttribute(k_velocity_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  if (e != cudaSuccess) return e;
+  k_velocity_tma<<<grid, block, sm, st>>>(a, tm, ichunk, err);
+  return cudaGetLastError();
+}

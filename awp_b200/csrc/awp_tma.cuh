@@ -1,0 +1,29 @@
+// TMA-pipelined stencil kernels (awp_tma.cu): tensor maps and launchers.
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include "awp_common.h"
+#include "awp_kernels.cuh"
+
+// Tensor maps of the fields one kernel streams, grouped by tile shape:
+//   halo  (40 x 12 box): fields read with their j/k neighbours
+//   media (36 x  9 box): fields read at (j|j-1, k|k-1) of planes i and i+1
+//   own   (32 x  8 box): fields read and written at the cell itself
+// velocity kernel: halo = xx yy zz xy xz yz, media = d1, own = u1 v1 w1
+// stress kernel  : halo = u1 v1 w1, media = lam mu qp qs, own = xx..yz r1..r6
+struct TmaMaps {
+  CUtensorMap halo[6];
+  CUtensorMap media[4];
+  CUtensorMap own[12];
+};
+
+// Encode one 3-D tensor map over a padded field; group 0 halo, 1 media, 2 own.
+int awp_tma_box(int group, int* box_x, int* box_y);
+int awp_tma_encode(CUtensorMap* map, const float* base, const AwpGeom& g, int box_x, int box_y);
+
+cudaError_t awp_launch_stress_tma(const StrArgs& a, const TmaMaps& tm, bool elastic, int ichunk,
+                                  int* err, cudaStream_t st);
+cudaError_t awp_launch_velocity_tma(const VelArgs& a, const TmaMaps& tm, int ichunk, int* err,
+                                    cudaStream_t st);

@@ -12,6 +12,7 @@ from __future__ import annotations
 import itertools
 
 CANDIDATES = {
+    "tma": (1, 0),
     "vel_ty": (4, 8),
     "str_ty": (4, 8),
     "ichunk": (16, 32, 64),
@@ -34,7 +35,10 @@ def autotune(solver, steps: int = 3) -> dict:
     table = []
     solver.profile_phases(True)
     solver.phase_times()  # drop earlier events
-    for vty, sty, ich in itertools.product(*CANDIDATES.values()):
+    for tma, vty, sty, ich in itertools.product(*CANDIDATES.values()):
+        if tma and (vty, sty) != (8, 8):
+            continue  # the TMA kernels have one tile shape (32 x 8)
+        set_tuning(lib, "tma", tma)
         set_tuning(lib, "vel_ty", vty)
         set_tuning(lib, "str_ty", sty)
         set_tuning(lib, "ichunk", ich)
@@ -42,12 +46,11 @@ def autotune(solver, steps: int = 3) -> dict:
         solver.phase_times()
         solver.step(steps)
         t = solver.phase_times()
-        table.append({"vel_ty": vty, "str_ty": sty, "ichunk": ich,
+        table.append({"tma": tma, "vel_ty": vty, "str_ty": sty, "ichunk": ich,
                       "velocity_ms": t["velocity"][0] / max(t["velocity"][1], 1),
                       "stress_ms": t["stress"][0] / max(t["stress"][1], 1)})
     solver.profile_phases(False)
     best = min(table, key=lambda r: r["velocity_ms"] + r["stress_ms"])
-    set_tuning(lib, "vel_ty", best["vel_ty"])
-    set_tuning(lib, "str_ty", best["str_ty"])
-    set_tuning(lib, "ichunk", best["ichunk"])
+    for key in CANDIDATES:
+        set_tuning(lib, key, best[key])
     return {"chosen": {k: best[k] for k in CANDIDATES}, "table": table}

@@ -78,6 +78,7 @@ def test_full_run_matches_library(tmp_path):
         s.step(1)
         if step % ntiskp == 0:
             s.gather(0, nedx - 1, 2, 0, nedy - 1, 3, 0, 2, 1, *[b.data_ptr() for b in bufs])
+            s.synchronize()  # the gather runs on the context's stream
             for c, b in zip("XYZ", bufs):
                 frames[c].append(b.cpu().numpy().copy())
     s.close()

@@ -23,10 +23,14 @@ def run(scn, steps):
 def test_tuning_is_bitwise_neutral(q):
     lib = _lib.load()
     saved = tune.get_tuning(lib)
-    scn = scenarios.random_small(nx=40, ny=36, nz=64, q=q, steps=6, seed=5)
+    # odd sizes: partial tiles in j and k, chunk remainders in i
+    scn = scenarios.random_small(nx=41, ny=37, nz=68, q=q, steps=6, seed=5)
     base = None
     try:
-        for vty, sty, ich in itertools.product((4, 8), (4, 8), (16, 64)):
+        for tma, vty, sty, ich in itertools.product((1, 0), (4, 8), (4, 8), (16, 64)):
+            if tma and (vty, sty) != (8, 8):
+                continue
+            tune.set_tuning(lib, "tma", tma)
             tune.set_tuning(lib, "vel_ty", vty)
             tune.set_tuning(lib, "str_ty", sty)
             tune.set_tuning(lib, "ichunk", ich)
@@ -36,7 +40,7 @@ def test_tuning_is_bitwise_neutral(q):
                 continue
             for f in out:
                 assert np.array_equal(out[f].view(np.uint32), base[f].view(np.uint32)), \
-                    (f, vty, sty, ich)
+                    (f, tma, vty, sty, ich)
     finally:
         for k, v in saved.items():
             tune.set_tuning(lib, k, v)
