@@ -213,11 +213,16 @@ __global__ void __launch_bounds__(32 * TY, TY == 8 ? 2 : 1)
     }
     const float dcrj = LDG(a.dcrjx + i) * dcy * dcz;
 
-    float xl = (float)(8.0 / (double)sum8(lam_c, lam_n));
-    float xm = (float)(16.0 / (double)sum8(mu_c, mu_n));
-    float xmu1 = (float)(2.0 / (double)(mu_c.a + mu_c.c));
-    float xmu2 = (float)(2.0 / (double)(mu_c.a + mu_c.b));
-    float xmu3 = (float)(2.0 / (double)(mu_c.a + mu_n.a));
+    // The reference divides in double and rounds to float ((float)(8.0/(double)x),
+    // kernel.cu:962-969).  For float operands that equals the correctly rounded
+    // float quotient: double rounding is innocuous for division when the wider
+    // format has at least 2p+2 = 50 bits (53 here).  tests/test_host_setup.py
+    // checks the identity; the float division costs a fraction of the double one.
+    float xl = __fdiv_rn(8.0f, sum8(lam_c, lam_n));
+    float xm = __fdiv_rn(16.0f, sum8(mu_c, mu_n));
+    float xmu1 = __fdiv_rn(2.0f, (mu_c.a + mu_c.c));
+    float xmu2 = __fdiv_rn(2.0f, (mu_c.a + mu_c.b));
+    float xmu3 = __fdiv_rn(2.0f, (mu_c.a + mu_n.a));
     xl = xl + xm;
     float h = 0.f, h1 = 0.f, h2 = 0.f, h3 = 0.f, qpa = 0.f;
     if (!ELASTIC) {

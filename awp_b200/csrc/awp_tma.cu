@@ -208,14 +208,15 @@ __global__ void __launch_bounds__(NT, 2)
     float la, lb, lc, ld, na, nb, nc, nd;
     m4(Mc, 0, la, lb, lc, ld);
     m4(Mn, 0, na, nb, nc, nd);
-    float xl = (float)(8.0 / (double)(la + na + lb + nb + lc + nc + ld + nd));
+    // float quotients equal the reference's double-then-float ones (see k_stress)
+    float xl = __fdiv_rn(8.0f, (la + na + lb + nb + lc + nc + ld + nd));
     float ma, mb, mc, md, pa, pb, pc, pd;
     m4(Mc, 1, ma, mb, mc, md);
     m4(Mn, 1, pa, pb, pc, pd);
-    float xm = (float)(16.0 / (double)(ma + pa + mb + pb + mc + pc + md + pd));
-    float xmu1 = (float)(2.0 / (double)(ma + mc));
-    float xmu2 = (float)(2.0 / (double)(ma + mb));
-    float xmu3 = (float)(2.0 / (double)(ma + pa));
+    float xm = __fdiv_rn(16.0f, (ma + pa + mb + pb + mc + pc + md + pd));
+    float xmu1 = __fdiv_rn(2.0f, (ma + mc));
+    float xmu2 = __fdiv_rn(2.0f, (ma + mb));
+    float xmu3 = __fdiv_rn(2.0f, (ma + pa));
     xl = xl + xm;
 
     const int t = awp_tex_index(a.tex, i, j, k);

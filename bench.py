@@ -362,6 +362,7 @@ def run_ours(args, rank, world, dist) -> dict | None:
         "clocks": clocks,
         "gpu_launches": launches,
         "tuning": tuning["chosen"] if tuning else None,
+        "tuning_table": tuning["table"] if tuning else None,
     }
     if e2e:
         line["e2e"] = e2e

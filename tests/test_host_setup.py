@@ -117,3 +117,22 @@ def test_q_switch_threshold_is_exact():
     # no float between consecutive candidates breaks monotonicity
     assert np.all(ref == (xs >= thr))
     assert np.float32(thr) > np.float32(0.004999)
+
+
+def test_double_then_float_division_equals_float_division():
+    """The stress kernels compute the reference's (float)(C/(double)x) harmonic
+    averages (kernel.cu:962-969) as correctly rounded float divisions; check
+    the identity on many floats, including quotients next to float midpoints."""
+    rng = np.random.default_rng(0)
+    x = np.concatenate([
+        rng.uniform(1e-12, 1e-8, 2_000_000).astype(np.float32),      # inverse moduli sums
+        (rng.standard_normal(2_000_000) * 1e3).astype(np.float32),
+        np.frombuffer(rng.integers(0x00800000, 0x7f000000, 2_000_000, dtype=np.uint32)
+                      .tobytes(), np.float32),
+    ])
+    x = x[np.isfinite(x) & (x != 0)]
+    for c in (2.0, 8.0, 16.0):
+        ref = (c / x.astype(np.float64)).astype(np.float32)
+        mine = np.float32(c) / x
+        ok = np.isfinite(ref)
+        assert np.array_equal(ref[ok].view(np.uint32), mine[ok].view(np.uint32))

@@ -44,6 +44,7 @@ CASES = [
     dict(nx=24, ny=20, nz=32, q=True, ifault=5, steps=30, nsrc=4),
     dict(nx=16, ny=18, nz=24, nvar=3, ifault=1, steps=12),   # Q from vs (mesh.c:226-236)
     dict(nx=18, ny=16, nz=20, nvar=8, ifault=1, steps=12),
+    dict(nx=41, ny=37, nz=68, q=True, ifault=1, steps=6),    # partial tiles in j, k and i
 ]
 
 
@@ -69,8 +70,20 @@ def test_media_matches_reference_host(case):
     s.close()
 
 
+@pytest.fixture(params=[1, 0], ids=["tma", "ldg"])
+def kernel_family(request):
+    """Run the context API on the TMA-pipelined (1) or read-only-path (0) kernels."""
+    from awp_b200 import _lib, tune
+    lib = _lib.load()
+    saved = tune.get_tuning(lib)
+    tune.set_tuning(lib, "tma", request.param)
+    yield request.param
+    for k, v in saved.items():
+        tune.set_tuning(lib, k, v)
+
+
 @pytest.mark.parametrize("case", CASES, ids=lambda c: "-".join(f"{k}{v}" for k, v in c.items()))
-def test_time_loop_parity(case):
+def test_time_loop_parity(case, kernel_family):
     case = dict(case)
     steps = case.pop("steps")
     scn = scenarios.random_small(steps=steps, **case)
