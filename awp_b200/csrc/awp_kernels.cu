@@ -24,9 +24,8 @@
 
 namespace {
 
-// Launch shape (tuned on B200; adjustable through awp_set_tuning).
-int g_vel_ty = 8;
-int g_str_ty = 8;
+// Launch shape (tuned on B200; adjustable through awp_set_tuning).  Tiles are
+// 32 k x 8 j for every kernel; the chunk of x planes and the kernel family vary.
 int g_ichunk = 32;
 int g_tma = 1;  // context API: TMA-pipelined kernels (1) or the read-only-path kernels (0)
 
@@ -893,13 +892,9 @@ inline unsigned cdiv_u(long long a, long long b) { return (unsigned)((a + b - 1)
 cudaError_t awp_launch_velocity(const VelArgs& a, cudaStream_t st) {
   const int nk = a.k1 - a.k0 + 1, nj = a.j1 - a.j0 + 1, ni = a.i1 - a.i0 + 1;
   if (nk <= 0 || nj <= 0 || ni <= 0) return cudaSuccess;
-  const int ty = g_vel_ty;
-  const dim3 block(32, ty, 1);
-  const dim3 grid(cdiv_u(nk, 32), cdiv_u(nj, ty), cdiv_u(ni, g_ichunk));
-  if (ty == 4)
-    k_velocity<4><<<grid, block, 0, st>>>(a, g_ichunk);
-  else
-    k_velocity<8><<<grid, block, 0, st>>>(a, g_ichunk);
+  const dim3 block(32, 8, 1);
+  const dim3 grid(cdiv_u(nk, 32), cdiv_u(nj, 8), cdiv_u(ni, g_ichunk));
+  k_velocity<8><<<grid, block, 0, st>>>(a, g_ichunk);
   return cudaGetLastError();
 }
 
@@ -923,27 +918,18 @@ static void launch_stress_ty(const StrArgs& a, bool elastic, bool texarr, dim3 g
 cudaError_t awp_launch_stress(const StrArgs& a, bool elastic, cudaStream_t st) {
   const int nk = a.k1 - a.k0 + 1, nj = a.j1 - a.j0 + 1, ni = a.i1 - a.i0 + 1;
   if (nk <= 0 || nj <= 0 || ni <= 0) return cudaSuccess;
-  const int ty = g_str_ty;
-  const dim3 grid(cdiv_u(nk, 32), cdiv_u(nj, ty), cdiv_u(ni, g_ichunk));
-  const bool texarr = a.vx1 != nullptr;
-  if (ty == 4)
-    launch_stress_ty<4>(a, elastic, texarr, grid, st);
-  else
-    launch_stress_ty<8>(a, elastic, texarr, grid, st);
+  const dim3 grid(cdiv_u(nk, 32), cdiv_u(nj, 8), cdiv_u(ni, g_ichunk));
+  launch_stress_ty<8>(a, elastic, a.vx1 != nullptr, grid, st);
   return cudaGetLastError();
 }
 
 int awp_tuning_set(const char* key, int value) {
-  if (!strcmp(key, "vel_ty") && (value == 4 || value == 8)) { g_vel_ty = value; return 0; }
-  if (!strcmp(key, "str_ty") && (value == 4 || value == 8)) { g_str_ty = value; return 0; }
   if (!strcmp(key, "ichunk") && value >= 4 && value <= 1024) { g_ichunk = value; return 0; }
   if (!strcmp(key, "tma") && (value == 0 || value == 1)) { g_tma = value; return 0; }
   return 1;
 }
 
 int awp_tuning_get(const char* key) {
-  if (!strcmp(key, "vel_ty")) return g_vel_ty;
-  if (!strcmp(key, "str_ty")) return g_str_ty;
   if (!strcmp(key, "ichunk")) return g_ichunk;
   if (!strcmp(key, "tma")) return g_tma;
   return -1;

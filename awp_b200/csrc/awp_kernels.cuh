@@ -153,8 +153,8 @@ struct MediaArgs {
   unsigned int* ext;
 };
 
-// Launch-shape tuning (awp_kernels.cu): "vel_ty", "str_ty" (4 or 8 j-rows per
-// CTA) and "ichunk" (x-planes marched per CTA).  Returns 0 on success.
+// Launch-shape tuning (awp_kernels.cu): "ichunk" (x-planes marched per CTA) and
+// "tma" (kernel family of the context API).  Returns 0 on success.
 int awp_tuning_set(const char* key, int value);
 int awp_tuning_get(const char* key);
 

@@ -1,6 +1,6 @@
 """Launch-shape autotuner for the stencil kernels.
 
-Times every candidate (j rows per CTA for the velocity and stress kernels, x
+Times every candidate (kernel family: TMA-pipelined or read-only path; x
 planes marched per CTA) with the library's own per-phase CUDA events on a live
 context, keeps the fastest per kernel and installs it process-wide through
 awp_set_tuning.  The arithmetic does not depend on the launch shape (every
@@ -13,8 +13,6 @@ import itertools
 
 CANDIDATES = {
     "tma": (1, 0),
-    "vel_ty": (4, 8),
-    "str_ty": (4, 8),
     "ichunk": (16, 32, 64),
 }
 
@@ -29,24 +27,20 @@ def get_tuning(lib) -> dict:
 
 
 def autotune(solver, steps: int = 3) -> dict:
-    """Try every (vel_ty, str_ty, ichunk) on `solver` (advancing it) and install
-    the fastest velocity and stress shapes.  Returns the timing table."""
+    """Try every (kernel family, ichunk) on `solver` (advancing it) and install
+    the fastest.  Returns the timing table."""
     lib = solver.lib
     table = []
     solver.profile_phases(True)
     solver.phase_times()  # drop earlier events
-    for tma, vty, sty, ich in itertools.product(*CANDIDATES.values()):
-        if tma and (vty, sty) != (8, 8):
-            continue  # the TMA kernels have one tile shape (32 x 8)
+    for tma, ich in itertools.product(*CANDIDATES.values()):
         set_tuning(lib, "tma", tma)
-        set_tuning(lib, "vel_ty", vty)
-        set_tuning(lib, "str_ty", sty)
         set_tuning(lib, "ichunk", ich)
         solver.step(1)  # settle
         solver.phase_times()
         solver.step(steps)
         t = solver.phase_times()
-        table.append({"tma": tma, "vel_ty": vty, "str_ty": sty, "ichunk": ich,
+        table.append({"tma": tma, "ichunk": ich,
                       "velocity_ms": t["velocity"][0] / max(t["velocity"][1], 1),
                       "stress_ms": t["stress"][0] / max(t["stress"][1], 1)})
     solver.profile_phases(False)

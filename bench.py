@@ -252,7 +252,10 @@ def run_ours(args, rank, world, dist) -> dict | None:
     s.upload_media(scn.media)
     s.upload_sources(scn.src_pos, scn.src_data)
     tuning = None
-    if not args.no_tune:
+    if args.tma is not None:
+        from awp_b200 import tune
+        tune.set_tuning(s.lib, "tma", args.tma)
+    elif not args.no_tune:
         from awp_b200 import tune
         tuning = tune.autotune(s)
     s.step(args.warmup)
@@ -408,6 +411,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ref-gpu", action="store_true")
     ap.add_argument("--no-tune", action="store_true")
+    ap.add_argument("--tma", type=int, choices=[0, 1], default=None,
+                    help="force the kernel family (profiling cases; implies --no-tune)")
     ap.add_argument("--e2e-steps", type=int, default=0,
                     help="steps of the end-to-end run (default: the workload's full run)")
     ap.add_argument("--grid", type=lambda v: tuple(int(x) for x in v.split(",")), default=None,

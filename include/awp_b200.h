@@ -187,10 +187,9 @@ int awp_check_finite_noalloc(const float* const* fields, int nfields, long long 
 #define AWP_NPHASES 5
 int awp_profile_phases(awp_ctx* ctx, int enable);
 int awp_phase_times(awp_ctx* ctx, double ms[AWP_NPHASES], long long launches[AWP_NPHASES]);
-/* Launch-shape tuning of the stencil kernels (process-wide): key "vel_ty" or
- * "str_ty" (j rows per CTA: 4 or 8), "ichunk" (x planes marched per CTA,
- * 4..1024), "tma" (1: the context API runs the TMA-pipelined kernels, 0: the
- * read-only-path kernels; results are identical).  Returns AWP_OK or AWP_ERR_ARG; awp_get_tuning returns the value
+/* Launch-shape tuning of the stencil kernels (process-wide): key "ichunk"
+ * (x planes marched per CTA, 4..1024) and "tma" (1: the context API runs the
+ * TMA-pipelined kernels, 0: the read-only-path kernels; results are identical).  Returns AWP_OK or AWP_ERR_ARG; awp_get_tuning returns the value
  * or -1 for an unknown key. */
 int awp_set_tuning(const char* key, int value);
 int awp_get_tuning(const char* key);

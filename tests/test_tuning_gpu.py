@@ -27,12 +27,8 @@ def test_tuning_is_bitwise_neutral(q):
     scn = scenarios.random_small(nx=41, ny=37, nz=68, q=q, steps=6, seed=5)
     base = None
     try:
-        for tma, vty, sty, ich in itertools.product((1, 0), (4, 8), (4, 8), (16, 64)):
-            if tma and (vty, sty) != (8, 8):
-                continue
+        for tma, ich in itertools.product((1, 0), (16, 32, 64)):
             tune.set_tuning(lib, "tma", tma)
-            tune.set_tuning(lib, "vel_ty", vty)
-            tune.set_tuning(lib, "str_ty", sty)
             tune.set_tuning(lib, "ichunk", ich)
             out = run(scn, 6)
             if base is None:
@@ -40,7 +36,7 @@ def test_tuning_is_bitwise_neutral(q):
                 continue
             for f in out:
                 assert np.array_equal(out[f].view(np.uint32), base[f].view(np.uint32)), \
-                    (f, tma, vty, sty, ich)
+                    (f, tma, ich)
     finally:
         for k, v in saved.items():
             tune.set_tuning(lib, k, v)
@@ -48,6 +44,7 @@ def test_tuning_is_bitwise_neutral(q):
 
 def test_bad_tuning_rejected():
     lib = _lib.load()
-    assert lib.awp_set_tuning(b"str_ty", 5) != 0
+    assert lib.awp_set_tuning(b"ichunk", 2) != 0
+    assert lib.awp_set_tuning(b"tma", 2) != 0
     assert lib.awp_set_tuning(b"nonsense", 8) != 0
     assert lib.awp_get_tuning(b"nonsense") == -1
