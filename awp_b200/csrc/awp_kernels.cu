@@ -72,32 +72,20 @@ __global__ void __launch_bounds__(32 * TY)
     const float d_0jk = LDG(D + o - Y - 1);
     const float yz_0 = LDG(YZ + o);
 
-    float fd1 = 0.25f * (d_0 + d_0j + d_0k + d_0jk);
-    float fd2 = 0.25f * (d_0 + d_p + d_0k + d_pk);
-    float fd3 = 0.25f * (d_0 + d_p + d_0j + d_pj);
-    fd1 = dth / fd1;
-    fd2 = dth / fd2;
-    fd3 = dth / fd3;
+    const float fd1 = awp_vel_factor(dth, d_0, d_0j, d_0k, d_0jk);
+    const float fd2 = awp_vel_factor(dth, d_0, d_p, d_0k, d_pk);
+    const float fd3 = awp_vel_factor(dth, d_0, d_p, d_0j, d_pj);
     const float dcrj = LDG(a.dcrjx + i) * dcy * dcz;
 
-    U[o] = (U[o] + fd1 * (c1 * (xx_0 - xx_m1) + c2 * (xx_p1 - xx_m2) +
-                          c1 * (xy_0 - LDG(XY + o - Y)) +
-                          c2 * (LDG(XY + o + Y) - LDG(XY + o - 2 * Y)) +
-                          c1 * (xz_0 - LDG(XZ + o - 1)) +
-                          c2 * (LDG(XZ + o + 1) - LDG(XZ + o - 2)))) *
-           dcrj;
-    V[o] = (V[o] + fd2 * (c1 * (xy_p1 - xy_0) + c2 * (xy_p2 - xy_m1) +
-                          c1 * (LDG(YY + o + Y) - LDG(YY + o)) +
-                          c2 * (LDG(YY + o + 2 * Y) - LDG(YY + o - Y)) +
-                          c1 * (yz_0 - LDG(YZ + o - 1)) +
-                          c2 * (LDG(YZ + o + 1) - LDG(YZ + o - 2)))) *
-           dcrj;
-    W[o] = (W[o] + fd3 * (c1 * (xz_p1 - xz_0) + c2 * (xz_p2 - xz_m1) +
-                          c1 * (yz_0 - LDG(YZ + o - Y)) +
-                          c2 * (LDG(YZ + o + Y) - LDG(YZ + o - 2 * Y)) +
-                          c1 * (LDG(ZZ + o + 1) - LDG(ZZ + o)) +
-                          c2 * (LDG(ZZ + o + 2) - LDG(ZZ + o - 1)))) *
-           dcrj;
+    U[o] = awp_vel_update(U[o], fd1, c1, c2, xx_0 - xx_m1, xx_p1 - xx_m2,
+                          xy_0 - LDG(XY + o - Y), LDG(XY + o + Y) - LDG(XY + o - 2 * Y),
+                          xz_0 - LDG(XZ + o - 1), LDG(XZ + o + 1) - LDG(XZ + o - 2), dcrj);
+    V[o] = awp_vel_update(V[o], fd2, c1, c2, xy_p1 - xy_0, xy_p2 - xy_m1,
+                          LDG(YY + o + Y) - LDG(YY + o), LDG(YY + o + 2 * Y) - LDG(YY + o - Y),
+                          yz_0 - LDG(YZ + o - 1), LDG(YZ + o + 1) - LDG(YZ + o - 2), dcrj);
+    W[o] = awp_vel_update(W[o], fd3, c1, c2, xz_p1 - xz_0, xz_p2 - xz_m1,
+                          yz_0 - LDG(YZ + o - Y), LDG(YZ + o + Y) - LDG(YZ + o - 2 * Y),
+                          LDG(ZZ + o + 1) - LDG(ZZ + o), LDG(ZZ + o + 2) - LDG(ZZ + o - 1), dcrj);
 
     xx_m2 = xx_m1; xx_m1 = xx_0; xx_0 = xx_p1;
     xy_m1 = xy_0; xy_0 = xy_p1; xy_p1 = xy_p2;
@@ -212,20 +200,8 @@ __global__ void __launch_bounds__(32 * TY, TY == 8 ? 2 : 1)
     }
     const float dcrj = LDG(a.dcrjx + i) * dcy * dcz;
 
-    // The reference divides in double and rounds to float ((float)(8.0/(double)x),
-    // kernel.cu:962-969).  For float operands that equals the correctly rounded
-    // float quotient: double rounding is innocuous for division when the wider
-    // format has at least 2p+2 = 50 bits (53 here).  tests/test_host_setup.py
-    // checks the identity; the float division costs a fraction of the double one.
-    float xl = __fdiv_rn(8.0f, sum8(lam_c, lam_n));
-    float xm = __fdiv_rn(16.0f, sum8(mu_c, mu_n));
-    float xmu1 = __fdiv_rn(2.0f, (mu_c.a + mu_c.c));
-    float xmu2 = __fdiv_rn(2.0f, (mu_c.a + mu_c.b));
-    float xmu3 = __fdiv_rn(2.0f, (mu_c.a + mu_n.a));
-    xl = xl + xm;
-    float h = 0.f, h1 = 0.f, h2 = 0.f, h3 = 0.f, qpa = 0.f;
+    float cc0 = 0.f, cc1 = 0.f;
     if (!ELASTIC) {
-      float cc0, cc1;
       if (a.coeff_dev) {
         cc0 = LDG(a.coeff_dev + cidx);
         cc1 = LDG(a.coeff_dev + cidx + 1);
@@ -233,36 +209,11 @@ __global__ void __launch_bounds__(32 * TY, TY == 8 ? 2 : 1)
         cc0 = a.coeff[cidx];
         cc1 = a.coeff[cidx + 1];
       }
-      const float qpaw =
-          awp_qf_weight(0.0625f * sum8(qp_c, qp_n), f_wwo, cc0, cc1, a.qthr);
-      const float hw = awp_qf_weight(0.0625f * sum8(qs_c, qs_n), f_wwo, cc0, cc1, a.qthr);
-      const float h1w = awp_qf_weight(0.25f * (qs_c.a + qs_c.c), f_wwo, cc0, cc1, a.qthr);
-      const float h2w = awp_qf_weight(0.25f * (qs_c.a + qs_c.b), f_wwo, cc0, cc1, a.qthr);
-      const float h3w = awp_qf_weight(0.25f * (qs_c.a + qs_n.a), f_wwo, cc0, cc1, a.qthr);
-      h = -xm * hw * dh1;
-      h1 = -xmu1 * h1w * dh1;
-      h2 = -xmu2 * h2w * dh1;
-      h3 = -xmu3 * h3w * dh1;
-      qpa = -qpaw * xl * dh1;
     }
-    xm = xm * dth;
-    xmu1 = xmu1 * dth;
-    xmu2 = xmu2 * dth;
-    xmu3 = xmu3 * dth;
-    xl = xl * dth;
-    float vx1 = 0.f;
-    if (!ELASTIC) {
-      h = h * f_vx1;
-      h1 = h1 * f_vx1;
-      h2 = h2 * f_vx1;
-      h3 = h3 * f_vx1;
-      qpa = qpa * f_vx1;
-      xm = xm + DT * h;
-      xmu1 = xmu1 + DT * h1;
-      xmu2 = xmu2 + DT * h2;
-      xmu3 = xmu3 + DT * h3;
-      vx1 = DT * (1 + f_vx2 * f_vx1);
-    }
+    const AwpStrCoef cf = awp_stress_coef<ELASTIC>(
+        sum8(lam_c, lam_n), sum8(mu_c, mu_n), mu_c.a, mu_c.c, mu_c.b, mu_n.a,
+        sum8(qp_c, qp_n), sum8(qs_c, qs_n), qs_c.a, qs_c.c, qs_c.b, qs_n.a, f_vx1, f_vx2, f_wwo,
+        cc0, cc1, a.qthr, dth, dh1, DT);
 
     // velocities at k+1 / k+2 that fall on the free-surface image layer
     // (computed here in registers; kernel.cu:1087-1112)
@@ -271,9 +222,9 @@ __global__ void __launch_bounds__(32 * TY, TY == 8 ? 2 : 1)
       const float vimg = v_0 - (w_jp1 - w_0);
       const float vs1 = (i < a.gx_lim) ? u_p1 - (w_p1 - w_0) : 0.0f;
       const float vs2 = (j >= a.gy_min) ? v_jm1 - (w_0 - w_jm1) : 0.0f;
-      const float wimg =
-          w_km1 - LDG(a.lam_mu + (long long)i * a.lam_mu_ld + j) *
-                      ((vs1 - uimg) + (u_p1 - u_0) + (vimg - vs2) + (v_0 - v_jm1));
+      const float wimg = __fmaf_rn(
+          -LDG(a.lam_mu + (long long)i * a.lam_mu_ld + j),
+          __fadd_rn(__fadd_rn(__fadd_rn(vs1 - uimg, u_p1 - u_0), vimg - vs2), v_0 - v_jm1), w_km1);
       a.u1[col + o + 1] = uimg;
       a.v1[col + o + 1] = vimg;
       a.w1[col + o + 1] = wimg;
@@ -286,18 +237,17 @@ __global__ void __launch_bounds__(32 * TY, TY == 8 ? 2 : 1)
     }
 
     float d[9];
-    d[0] = c1 * (u_p1 - u_0) + c2 * (u_p2 - u_m1);
-    d[1] = c1 * (v_0 - v_jm1) + c2 * (v_jp1 - v_jm2);
-    d[2] = c1 * (w_0 - w_km1) + c2 * (wk1 - w_km2);
-    d[3] = c1 * (u_jp1 - u_0) + c2 * (u_jp2 - u_jm1);
-    d[4] = c1 * (v_0 - v_m1) + c2 * (v_p1 - v_m2);
-    d[5] = c1 * (uk1 - u_0) + c2 * (uk2 - u_km1);
-    d[6] = c1 * (w_0 - w_m1) + c2 * (w_p1 - w_m2);
-    d[7] = c1 * (vk1 - v_0) + c2 * (vk2 - v_km1);
-    d[8] = c1 * (w_jp1 - w_0) + c2 * (w_jp2 - w_jm1);
+    d[0] = awp_d4(c1, c2, u_p1, u_0, u_p2, u_m1);
+    d[1] = awp_d4(c1, c2, v_0, v_jm1, v_jp1, v_jm2);
+    d[2] = awp_d4(c1, c2, w_0, w_km1, wk1, w_km2);
+    d[3] = awp_d4(c1, c2, u_jp1, u_0, u_jp2, u_jm1);
+    d[4] = awp_d4(c1, c2, v_0, v_m1, v_p1, v_m2);
+    d[5] = awp_d4(c1, c2, uk1, u_0, uk2, u_km1);
+    d[6] = awp_d4(c1, c2, w_0, w_m1, w_p1, w_m2);
+    d[7] = awp_d4(c1, c2, vk1, v_0, vk2, v_km1);
+    d[8] = awp_d4(c1, c2, w_jp1, w_0, w_jp2, w_jm1);
 
-    awp_stress_update<ELASTIC>(sg, rr, xl, xm, xmu1, xmu2, xmu3, h, h1, h2, h3, qpa, vx1, f_vx1,
-                           f_vx2, f_wwo, DT, dcrj, d);
+    awp_stress_update<ELASTIC>(sg, rr, cf, f_vx1, f_vx2, f_wwo, DT, dcrj, d);
 #pragma unroll
     for (int q = 0; q < 6; ++q) SG[q][o] = sg[q];
     if (!ELASTIC) {

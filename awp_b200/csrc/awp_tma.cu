@@ -208,58 +208,27 @@ __global__ void __launch_bounds__(NT, 2)
     float la, lb, lc, ld, na, nb, nc, nd;
     m4(Mc, 0, la, lb, lc, ld);
     m4(Mn, 0, na, nb, nc, nd);
-    // float quotients equal the reference's double-then-float ones (see k_stress)
-    float xl = __fdiv_rn(8.0f, (la + na + lb + nb + lc + nc + ld + nd));
     float ma, mb, mc, md, pa, pb, pc, pd;
     m4(Mc, 1, ma, mb, mc, md);
     m4(Mn, 1, pa, pb, pc, pd);
-    float xm = __fdiv_rn(16.0f, (ma + pa + mb + pb + mc + pc + md + pd));
-    float xmu1 = __fdiv_rn(2.0f, (ma + mc));
-    float xmu2 = __fdiv_rn(2.0f, (ma + mb));
-    float xmu3 = __fdiv_rn(2.0f, (ma + pa));
-    xl = xl + xm;
-
     const int t = awp_tex_index(a.tex, i, j, k);
     const float f_vx1 = a.tex.tau1[t], f_vx2 = a.tex.tau2[t], f_wwo = a.tex.wwo8[t];
-    float h = 0.f, h1 = 0.f, h2 = 0.f, h3 = 0.f, qpa = 0.f;
+    float QP8 = 0.f, QS8 = 0.f, qa = 0.f, qb = 0.f, qc = 0.f, ra = 0.f, cc0 = 0.f, cc1 = 0.f;
     if (!ELASTIC) {
-      const float cc0 = a.coeff[2 * t], cc1 = a.coeff[2 * t + 1];
-      float qa, qb, qc, qd, ra, rb, rc, rd;
+      cc0 = a.coeff[2 * t];
+      cc1 = a.coeff[2 * t + 1];
+      float qd, rb, rc, rd;
       m4(Mc, 2, qa, qb, qc, qd);
       m4(Mn, 2, ra, rb, rc, rd);
-      const float qpaw = awp_qf_weight(0.0625f * (qa + ra + qb + rb + qc + rc + qd + rd), f_wwo,
-                                     cc0, cc1, a.qthr);
+      QP8 = qa + ra + qb + rb + qc + rc + qd + rd;
       m4(Mc, 3, qa, qb, qc, qd);
       m4(Mn, 3, ra, rb, rc, rd);
-      const float hw = awp_qf_weight(0.0625f * (qa + ra + qb + rb + qc + rc + qd + rd), f_wwo,
-                                   cc0, cc1, a.qthr);
-      const float h1w = awp_qf_weight(0.25f * (qa + qc), f_wwo, cc0, cc1, a.qthr);
-      const float h2w = awp_qf_weight(0.25f * (qa + qb), f_wwo, cc0, cc1, a.qthr);
-      const float h3w = awp_qf_weight(0.25f * (qa + ra), f_wwo, cc0, cc1, a.qthr);
-      h = -xm * hw * dh1;
-      h1 = -xmu1 * h1w * dh1;
-      h2 = -xmu2 * h2w * dh1;
-      h3 = -xmu3 * h3w * dh1;
-      qpa = -qpaw * xl * dh1;
+      QS8 = qa + ra + qb + rb + qc + rc + qd + rd;
     }
-    xm = xm * dth;
-    xmu1 = xmu1 * dth;
-    xmu2 = xmu2 * dth;
-    xmu3 = xmu3 * dth;
-    xl = xl * dth;
-    float vx1 = 0.f;
-    if (!ELASTIC) {
-      h = h * f_vx1;
-      h1 = h1 * f_vx1;
-      h2 = h2 * f_vx1;
-      h3 = h3 * f_vx1;
-      qpa = qpa * f_vx1;
-      xm = xm + DT * h;
-      xmu1 = xmu1 + DT * h1;
-      xmu2 = xmu2 + DT * h2;
-      xmu3 = xmu3 + DT * h3;
-      vx1 = DT * (1 + f_vx2 * f_vx1);
-    }
+    // eight-cell sums in the reference's order: pos, ip1, jm1, ijk, km1, ik1, jk1, ijk1
+    const AwpStrCoef cf = awp_stress_coef<ELASTIC>(
+        la + na + lb + nb + lc + nc + ld + nd, ma + pa + mb + pb + mc + pc + md + pd, ma, mc, mb,
+        pa, QP8, QS8, qa, qc, qb, ra, f_vx1, f_vx2, f_wwo, cc0, cc1, a.qthr, dth, dh1, DT);
     const float dcrj = LDG(a.dcrjx + i) * dcy * dcz;
     const long long o = (long long)i * S;
 
@@ -268,9 +237,9 @@ __global__ void __launch_bounds__(NT, 2)
       const float vimg = v_0 - (w_jp1 - w_0);
       const float vs1 = (i < a.gx_lim) ? u_p1 - (w_p1 - w_0) : 0.0f;
       const float vs2 = (j >= a.gy_min) ? v_jm1 - (w_0 - w_jm1) : 0.0f;
-      const float wimg =
-          w_km1 - LDG(a.lam_mu + (long long)i * a.lam_mu_ld + j) *
-                      ((vs1 - uimg) + (u_p1 - u_0) + (vimg - vs2) + (v_0 - v_jm1));
+      const float wimg = __fmaf_rn(
+          -LDG(a.lam_mu + (long long)i * a.lam_mu_ld + j),
+          __fadd_rn(__fadd_rn(__fadd_rn(vs1 - uimg, u_p1 - u_0), vimg - vs2), v_0 - v_jm1), w_km1);
       a.u1[col + o + 1] = uimg;
       a.v1[col + o + 1] = vimg;
       a.w1[col + o + 1] = wimg;
@@ -283,15 +252,15 @@ __global__ void __launch_bounds__(NT, 2)
     }
 
     float d[9];
-    d[0] = c1 * (u_p1 - u_0) + c2 * (u_p2 - u_m1);
-    d[1] = c1 * (v_0 - v_jm1) + c2 * (v_jp1 - v_jm2);
-    d[2] = c1 * (w_0 - w_km1) + c2 * (wk1 - w_km2);
-    d[3] = c1 * (u_jp1 - u_0) + c2 * (u_jp2 - u_jm1);
-    d[4] = c1 * (v_0 - v_m1) + c2 * (v_p1 - v_m2);
-    d[5] = c1 * (uk1 - u_0) + c2 * (uk2 - u_km1);
-    d[6] = c1 * (w_0 - w_m1) + c2 * (w_p1 - w_m2);
-    d[7] = c1 * (vk1 - v_0) + c2 * (vk2 - v_km1);
-    d[8] = c1 * (w_jp1 - w_0) + c2 * (w_jp2 - w_jm1);
+    d[0] = awp_d4(c1, c2, u_p1, u_0, u_p2, u_m1);
+    d[1] = awp_d4(c1, c2, v_0, v_jm1, v_jp1, v_jm2);
+    d[2] = awp_d4(c1, c2, w_0, w_km1, wk1, w_km2);
+    d[3] = awp_d4(c1, c2, u_jp1, u_0, u_jp2, u_jm1);
+    d[4] = awp_d4(c1, c2, v_0, v_m1, v_p1, v_m2);
+    d[5] = awp_d4(c1, c2, uk1, u_0, uk2, u_km1);
+    d[6] = awp_d4(c1, c2, w_0, w_m1, w_p1, w_m2);
+    d[7] = awp_d4(c1, c2, vk1, v_0, vk2, v_km1);
+    d[8] = awp_d4(c1, c2, w_jp1, w_0, w_jp2, w_jm1);
 
     const float* O = ro.at(i) + ooff;
     float sg[6], rr[6];
@@ -301,8 +270,7 @@ __global__ void __launch_bounds__(NT, 2)
 #pragma unroll
       for (int q = 0; q < 6; ++q) rr[q] = O[(6 + q) * OTILE];
     }
-    awp_stress_update<ELASTIC>(sg, rr, xl, xm, xmu1, xmu2, xmu3, h, h1, h2, h3, qpa, vx1, f_vx1,
-                               f_vx2, f_wwo, DT, dcrj, d);
+    awp_stress_update<ELASTIC>(sg, rr, cf, f_vx1, f_vx2, f_wwo, DT, dcrj, d);
     if (active) {
 #pragma unroll
       for (int q = 0; q < 6; ++q) SG[q][col + o] = sg[q];
@@ -437,27 +405,21 @@ __global__ void __launch_bounds__(NT, 2)
     const float d_0 = Dc[0], d_0j = Dc[-MX], d_0k = Dc[-1], d_0jk = Dc[-MX - 1];
     const float d_p = Dn[0], d_pj = Dn[-MX], d_pk = Dn[-1];
 
-    float fd1 = 0.25f * (d_0 + d_0j + d_0k + d_0jk);
-    float fd2 = 0.25f * (d_0 + d_p + d_0k + d_pk);
-    float fd3 = 0.25f * (d_0 + d_p + d_0j + d_pj);
-    fd1 = dth / fd1;
-    fd2 = dth / fd2;
-    fd3 = dth / fd3;
+    const float fd1 = awp_vel_factor(dth, d_0, d_0j, d_0k, d_0jk);
+    const float fd2 = awp_vel_factor(dth, d_0, d_p, d_0k, d_pk);
+    const float fd3 = awp_vel_factor(dth, d_0, d_p, d_0j, d_pj);
     const float dcrj = LDG(a.dcrjx + i) * dcy * dcz;
 
     const float* O = ro.at(i) + ooff;
-    const float u = (O[0] + fd1 * (c1 * (xx_0 - xx_m1) + c2 * (xx_p1 - xx_m2) +
-                                   c1 * (xy_0 - XY[-HX]) + c2 * (XY[HX] - XY[-2 * HX]) +
-                                   c1 * (xz_0 - XZ[-1]) + c2 * (XZ[1] - XZ[-2]))) *
-                    dcrj;
-    const float v = (O[OTILE] + fd2 * (c1 * (xy_p1 - xy_0) + c2 * (xy_p2 - xy_m1) +
-                                       c1 * (YY[HX] - YY[0]) + c2 * (YY[2 * HX] - YY[-HX]) +
-                                       c1 * (yz_0 - YZ[-1]) + c2 * (YZ[1] - YZ[-2]))) *
-                    dcrj;
-    const float w = (O[2 * OTILE] + fd3 * (c1 * (xz_p1 - xz_0) + c2 * (xz_p2 - xz_m1) +
-                                           c1 * (yz_0 - YZ[-HX]) + c2 * (YZ[HX] - YZ[-2 * HX]) +
-                                           c1 * (ZZ[1] - ZZ[0]) + c2 * (ZZ[2] - ZZ[-1]))) *
-                    dcrj;
+    const float u = awp_vel_update(O[0], fd1, c1, c2, xx_0 - xx_m1, xx_p1 - xx_m2,
+                                   xy_0 - XY[-HX], XY[HX] - XY[-2 * HX], xz_0 - XZ[-1],
+                                   XZ[1] - XZ[-2], dcrj);
+    const float v = awp_vel_update(O[OTILE], fd2, c1, c2, xy_p1 - xy_0, xy_p2 - xy_m1,
+                                   YY[HX] - YY[0], YY[2 * HX] - YY[-HX], yz_0 - YZ[-1],
+                                   YZ[1] - YZ[-2], dcrj);
+    const float w = awp_vel_update(O[2 * OTILE], fd3, c1, c2, xz_p1 - xz_0, xz_p2 - xz_m1,
+                                   yz_0 - YZ[-HX], YZ[HX] - YZ[-2 * HX], ZZ[1] - ZZ[0],
+                                   ZZ[2] - ZZ[-1], dcrj);
     if (active) {
       const long long o = (long long)i * S + col;
       a.u1[o] = u;

@@ -140,3 +140,13 @@ void ref_hoek_brown(float sigma_0, float sigma_ci, float gsi, float mi, float d,
                     int tunnel, float *phi, float *cohes) {
   hoek_brown(sigma_0, sigma_ci, gsi, mi, d, tunnel, phi, cohes);
 }
+
+/* rotation_matrix (mesh.c:1370-1401): principal-stress rotation from the
+ * strike and dip angles (degrees) of nonlinear.dat. */
+void rotation_matrix(_prec *strike, _prec *dip, _prec *Rz, _prec *RzT);
+void ref_rotation_matrix(const float *strike, const float *dip, float *Rz, float *RzT) {
+  float s[3], d[3];
+  memcpy(s, strike, sizeof(s));
+  memcpy(d, dip, sizeof(d));
+  rotation_matrix(s, d, Rz, RzT);
+}

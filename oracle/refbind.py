@@ -50,6 +50,7 @@ class RefHost:
                                          [_F, _F, _I, _F])
         lib.ref_inicrj.argtypes = [c_float] + [c_int] * 8 + [_F] * 3
         lib.ref_hoek_brown.argtypes = [c_float] * 5 + [c_int, _F, _F]
+        lib.ref_rotation_matrix.argtypes = [_F, _F, _F, _F]
         self.lib = lib
 
     def tausub(self, taumin, taumax):
@@ -113,6 +114,56 @@ class RefHost:
         cohes = c_float()
         self.lib.ref_hoek_brown(sigma_0, sigma_ci, gsi, mi, d, tunnel, byref(phi), byref(cohes))
         return phi.value, cohes.value
+
+
+    def rotation_matrix(self, strike, dip):
+        """rotation_matrix (mesh.c:1370-1401): Rz, RzT from strike/dip in degrees."""
+        st = np.ascontiguousarray(strike, np.float32)
+        dp = np.ascontiguousarray(dip, np.float32)
+        rz = np.zeros(9, np.float32)
+        rzt = np.zeros(9, np.float32)
+        self.lib.ref_rotation_matrix(fptr(st), fptr(dp), fptr(rz), fptr(rzt))
+        return rz, rzt
+
+
+def lithostatic_sigma2(d1, nx, ny, nz, dh):
+    """Vertical lithostatic stress of inidrpr_hoekbrown_light (mesh.c:1274-1282):
+    -dh/2 rho g at the surface cell (and the image above it), then one cell of
+    rho g dh more per cell downwards, evaluated in double and stored as float
+    at every step like the reference."""
+    shp = padded_shape(nx, ny, nz)
+    s2 = np.zeros(shp, np.float32)
+    top = nz + ALIGN - 1
+    sl = (slice(2, nx + 2 + 2 * NGSL), slice(2, ny + 2 + 2 * NGSL))
+    d = d1[sl[0], sl[1], :].astype(np.float64)
+    cur = (-dh / 2.0 * d[:, :, top] * 9.81).astype(np.float32)
+    s2[sl[0], sl[1], top] = cur
+    s2[sl[0], sl[1], top + 1] = cur
+    for k in range(top - 1, ALIGN - 3, -1):
+        cur = (cur.astype(np.float64) - dh * d[:, :, k] * 9.81).astype(np.float32)
+        s2[sl[0], sl[1], k] = cur
+    return s2
+
+
+def plasticity_inputs(scn, setup, seed=7, cohes=(2e4, 2e5), phi=(25.0, 35.0),
+                      strike=(40.0, 0.0, 130.0), fmajor=1.6, fminor=0.5, host=None):
+    """Drucker-Prager inputs on the padded grid: lithostatic sigma2 from the
+    density, seeded cohesion and friction angle per cell, the principal-stress
+    ratios and the rotation of nonlinear.dat (dip fixed to 0/90/0 as in
+    mesh.c:1199-1204).  Low cohesions make cells near the sources yield."""
+    host = host or RefHost()
+    p = scn.params
+    nx, ny, nz = p["nx"], p["ny"], p["nz"]
+    shp = padded_shape(nx, ny, nz)
+    rng = np.random.default_rng(seed)
+    sigma2 = lithostatic_sigma2(setup["media"]["d1"], nx, ny, nz, p["dh"])
+    coh = rng.uniform(cohes[0], cohes[1], shp).astype(np.float32)
+    ph = rng.uniform(phi[0], phi[1], shp).astype(np.float32)
+    dip = np.array([0.0, 90.0, 0.0], np.float32)
+    st = np.array(strike, np.float32)
+    rz, rzt = host.rotation_matrix(st, dip)
+    return dict(sigma2=sigma2, cohes=coh, phi=ph, fmajor=np.float32(fmajor),
+                fminor=np.float32(fminor), strike=st, dip=dip, Rz=rz, RzT=rzt)
 
 
 def tau12(tau8, dt):
@@ -232,9 +283,19 @@ class RefGpuSim:
         nzt = np.array([self.nz], np.int32)
         Rz = np.zeros(9, np.float32)
         RzT = np.zeros(9, np.float32)
+        fmajor = fminor = 0.0
+        self.nve = p.get("nve", 1)
+        if self.nve == 3:
+            pl = setup["plast"]
+            Rz = np.ascontiguousarray(pl["Rz"], np.float32)
+            RzT = np.ascontiguousarray(pl["RzT"], np.float32)
+            fmajor, fminor = float(pl["fmajor"]), float(pl["fminor"])
+            self.f.update(sigma2=T(pl["sigma2"]), cohes=T(pl["cohes"]), phi=T(pl["phi"]))
+            self.f["yldfac"] = torch.ones(shp, dtype=torch.float32, device=dev)
+        self.f["neta"] = torch.zeros(shp, dtype=torch.float32, device=dev)
         lib.SetDeviceConstValue(fptr(DH), c_float(p["dt"]), nxt.ctypes.data_as(_I),
                                 nyt.ctypes.data_as(_I), nzt.ctypes.data_as(_I), 1,
-                                c_float(0.0), c_float(0.0), fptr(Rz), fptr(RzT))
+                                c_float(fmajor), c_float(fminor), fptr(Rz), fptr(RzT))
         fz = np.zeros(20, np.float64)
         lib.SetDeviceFilterParameters(0, fz.ctypes.data_as(POINTER(c_double)),
                                       fz.ctypes.data_as(POINTER(c_double)))
@@ -268,19 +329,47 @@ class RefGpuSim:
                           P(self.vx2), P(self.ww), P(self.wwo), self.nx, self.p.get("npc", 0),
                           0, 0, s_i, e_i, s_j, e_j, 0)
 
+    def _calc(self, s_i, e_i, s_j, e_j):
+        f = self.f
+        P = self.ptr
+        self.lib.drprecpc_calc_H_opt(P(f["xx"]), P(f["yy"]), P(f["zz"]), P(f["xy"]), P(f["xz"]),
+                                     P(f["yz"]), P(f["mu"]), P(f["d1"]), P(f["sigma2"]),
+                                     P(f["yldfac"]), P(f["cohes"]), P(f["phi"]), P(f["neta"]),
+                                     self.nz, s_i, e_i, s_j, e_j, None, 0)
+
+    def margins(self):
+        """yls2/yre2 of pmcl3d.c:621-627 at one rank (ylsp = yls, yrep = yre)."""
+        yls, yre = 2 + NGSL, self.ny + NGSL + 1
+        yls2 = int(yls + int(yre - yls) * 0.25)
+        if yls2 % 2 != 0:
+            yls2 += 1
+        yre2 = int(yls + int(yre - yls) * 0.75)
+        if yre2 % 2 == 0:
+            yre2 -= 1
+        return max(yls2, yls + NGSL + 2), min(yre2, yre - NGSL - 2)
+
     def step(self, n=1):
         f = self.f
         P = self.ptr
         nx, ny, nz = self.nx, self.ny, self.nz
         xls, xre, yls, yre = 2 + NGSL, nx + NGSL + 1, 2 + NGSL, ny + NGSL + 1
+        yls2, yre2 = self.margins()
+        if self.nve == 3 and yre2 < yls2:
+            raise ValueError("NVE=3 needs a non-empty middle stress region (pmcl3d.c:621-627)")
         for _ in range(n):
             self.cur += 1
             self.lib.dvelcx_H_opt(P(f["u1"]), P(f["v1"]), P(f["w1"]), P(f["xx"]), P(f["yy"]),
                                   P(f["zz"]), P(f["xy"]), P(f["xz"]), P(f["yz"]), P(self.dcrjx),
                                   P(self.dcrjy), P(self.dcrjz), P(f["d1"]), ny, nz, None,
                                   2 + NGSL, nx + NGSL + 1, 0, 1)
-            # dstrqc over xss2..xse2, then the xss1 and xss3 strips (pmcl3d.c:1845-1919)
-            self._stress(NGSL + 4, nx + NGSL - 1, yls, yre)
+            if self.nve == 3:
+                # NVE=3: the middle y band of xss2..xse2 waits until after the
+                # sources and the first yield-factor strips (pmcl3d.c:1858-1879, 2139-2148)
+                self._stress(NGSL + 4, nx + NGSL - 1, yls, yls2 - 1)
+                self._stress(NGSL + 4, nx + NGSL - 1, yre2 + 1, yre)
+            else:
+                # dstrqc over xss2..xse2, then the xss1 and xss3 strips (pmcl3d.c:1845-1919)
+                self._stress(NGSL + 4, nx + NGSL - 1, yls, yre)
             self._stress(xls, NGSL + 3, yls, yre)
             self._stress(nx + NGSL, xre, yls, yre)
             if self.p["ifault"] < 4 and self.cur < self.p["nst"]:
@@ -292,6 +381,17 @@ class RefGpuSim:
                                      *[P(t) for t in self.src], P(f["xx"]), P(f["yy"]),
                                      P(f["zz"]), P(f["xy"]), P(f["yz"]), P(f["xz"]),
                                      P(self.mom), fdp, 0)
+            if self.nve == 3:
+                # pmcl3d.c:2110-2209 at one rank (xlsp = xls, ...)
+                self._calc(xls, xre, yls, yls + NGSL)
+                self._calc(xls, xre, yre - NGSL, yre)
+                self._stress(NGSL + 4, nx + NGSL - 1, yls2, yre2)
+                self._calc(xls, xls + NGSL, yls, yre)
+                self._calc(xre - NGSL, xre, yls, yre)
+                self._calc(xls + NGSL, xre - NGSL, yls + NGSL, yre - NGSL)
+                self.lib.drprecpc_app_H(P(f["xx"]), P(f["yy"]), P(f["zz"]), P(f["xy"]),
+                                        P(f["xz"]), P(f["yz"]), P(f["mu"]), P(f["sigma2"]),
+                                        P(f["yldfac"]), nz, xls, xre, yls, yre, None, 0)
             self.lib.fstr_H(P(f["zz"]), P(f["xz"]), P(f["yz"]), None, xls, xre, yls, yre)
         self.torch.cuda.synchronize()
 
