@@ -15,6 +15,8 @@
 #include "awp_common.h"
 #include "awp_host.h"
 #include "awp_kernels.cuh"
+#include "awp_pointsets.h"
+#include "awp_points.h"
 #include "awp_tma.cuh"
 
 namespace {
@@ -84,6 +86,8 @@ struct awp_ctx {
   TmaMaps vel_maps{}, str_maps{};
   long long cur_step = 0;
   bool initial_src_done = false;
+  RecvState* recv = nullptr;     // RECVFILE receivers
+  SrcFileState* srcf = nullptr;  // SOURCEFILE moment-tensor sources
   long long dev_bytes = 0;
   long long launches = 0;
   // phase timing
@@ -300,6 +304,14 @@ int one_step(awp_ctx* c) {
       CU_TRY(awp_launch_stress(s, c->elastic, c->stream));
     c->launches++;
   }
+  if (c->srcf) {  // sources_read + sources_add_cartesian (pmcl3d.c:1987-2004)
+    PhaseScope ps(c, 2);
+    float* const stress[6] = {f[AWP_XX], f[AWP_YY], f[AWP_ZZ], f[AWP_XY], f[AWP_XZ], f[AWP_YZ]};
+    if (awp_srcf_read(c->srcf, c->cur_step, c->stream, g_errmsg, sizeof(g_errmsg)) ||
+        awp_srcf_add(c->srcf, c->cur_step, stress, c->stream, &c->launches, g_errmsg,
+                     sizeof(g_errmsg)))
+      return AWP_ERR_IO;
+  }
   if ((c->p.ifault < 4 && c->cur_step < c->p.nst) || c->p.ifault == 5) {
     PhaseScope ps(c, 2);
     int st = launch_sources(c, (int)c->cur_step);
@@ -322,6 +334,10 @@ int one_step(awp_ctx* c) {
     CU_TRY(awp_launch_fstr(fs, c->stream));
     c->launches++;
   }
+  if (c->recv &&  // receivers_write (pmcl3d.c:2246-2247)
+      awp_recv_record(c->recv, c->cur_step, f[AWP_U1], f[AWP_V1], f[AWP_W1], c->stream,
+                      &c->launches, g_errmsg, sizeof(g_errmsg)))
+    return AWP_ERR_IO;
   return AWP_OK;
 }
 
@@ -360,6 +376,9 @@ const char* awp_last_error(void) { return g_errmsg; }
 
 int awp_ctx_destroy(awp_ctx* c) {
   if (!c) return AWP_OK;
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  awp_recv_destroy(c->recv);
+  awp_srcf_destroy(c->srcf);
   for (int i = 0; i < AWP_NFIELDS; ++i) cudaFree(c->f[i]);
   cudaFree(c->dcrjx); cudaFree(c->dcrjy); cudaFree(c->dcrjz); cudaFree(c->lam_mu);
   cudaFree(c->d_cell_pos); cudaFree(c->d_cell_first); cudaFree(c->d_order);
@@ -807,6 +826,93 @@ int awp_gather_output(awp_ctx* c, int nbgx, int nedx, int nskpx, int nbgy, int n
   a.w_shift = 1;
   CU_TRY(awp_launch_velbuffer(a, c->stream));
   return AWP_OK;
+}
+
+int awp_receivers_init(awp_ctx* c, const char* recvfile, long long nt) {
+  if (!c || !recvfile) return set_error(AWP_ERR_ARG, "null argument");
+  if (nt < 1) return set_error(AWP_ERR_ARG, "nt must be >= 1");
+  if (c->recv) return set_error(AWP_ERR_STATE, "receivers already initialised");
+  RecvState* r = nullptr;
+  const int e = awp_recv_create(recvfile, nt, c->g, c->p.dh, &r, g_errmsg, sizeof(g_errmsg));
+  if (e) return e < 0 ? AWP_ERR_CUDA : AWP_ERR_IO;
+  c->recv = r;
+  // the reference records the state before the first step (pmcl3d.c:1603-1605)
+  if (awp_recv_record(c->recv, c->cur_step, c->f[AWP_U1], c->f[AWP_V1], c->f[AWP_W1], c->stream,
+                      &c->launches, g_errmsg, sizeof(g_errmsg)))
+    return AWP_ERR_IO;
+  return AWP_OK;
+}
+
+int awp_receivers_count(awp_ctx* c, int counts[3]) {
+  if (!c || !counts) return set_error(AWP_ERR_ARG, "null argument");
+  for (int q = 0; q < 3; ++q) counts[q] = awp_recv_length(c->recv, q);
+  return AWP_OK;
+}
+
+int awp_sourcefile_init(awp_ctx* c, const char* sourcefile) {
+  if (!c || !sourcefile) return set_error(AWP_ERR_ARG, "null argument");
+  if (c->srcf) return set_error(AWP_ERR_STATE, "SOURCEFILE already initialised");
+  SrcFileState* s = nullptr;
+  const int e = awp_srcf_create(sourcefile, c->g, c->p.dh, c->p.dt, &s, g_errmsg,
+                                sizeof(g_errmsg));
+  if (e) return e < 0 ? AWP_ERR_CUDA : AWP_ERR_IO;
+  c->srcf = s;
+  // sources_read(0) before the loop (pmcl3d.c:1607)
+  if (awp_srcf_read(c->srcf, c->cur_step, c->stream, g_errmsg, sizeof(g_errmsg)))
+    return AWP_ERR_IO;
+  return AWP_OK;
+}
+
+int awp_input_read(const char* path, long long hdr[8], char* file, int filecap, float* x,
+                   float* y, float* z, int* type, long long cap) {
+  if (!path || !hdr) return AWP_ERR_ARG;
+  awp::InputFile in;
+  const int e = awp::read_input(path, &in);
+  if (e) return e;
+  hdr[0] = (long long)in.length;
+  hdr[1] = (long long)in.gpu_buffer_size;
+  hdr[2] = (long long)in.cpu_buffer_size;
+  hdr[3] = (long long)in.steps;
+  hdr[4] = (long long)in.num_writes;
+  hdr[5] = in.stride;
+  hdr[6] = in.degree;
+  hdr[7] = in.major;
+  if (file && filecap > 0) snprintf(file, (size_t)filecap, "%s", in.file.c_str());
+  for (size_t i = 0; i < in.length && (long long)i < cap; ++i) {
+    if (x) x[i] = in.x[i];
+    if (y) y[i] = in.y[i];
+    if (z) z[i] = in.z[i];
+    if (type) type[i] = in.type[i];
+  }
+  return 0;
+}
+
+int awp_point_coefs(const char* path, int grid_type, int nxt, int nyt, int nzt, float h,
+                    long long cap, int* count, int* indices, int* ix, int* iy, int* iz, float* lx,
+                    float* ly, float* lz) {
+  if (!path || !count || grid_type < 0 || grid_type > 8) return AWP_ERR_ARG;
+  awp::InputFile in;
+  int e = awp::read_input(path, &in);
+  if (e) return e;
+  awp::BlockDesc b{nxt, nyt, nzt, h, 0};
+  awp::PointSet ps;
+  e = awp::point_set_init(in, (awp::GridType)grid_type, &b, 1, &ps);
+  if (e) return e;
+  const awp::BlockInterp& bi = ps.block[0];
+  *count = bi.num_query;
+  const int nb = bi.num_basis;
+  for (int q = 0; q < bi.num_query && q < cap; ++q) {
+    indices[q] = ps.indices[bi.ridx[q]];
+    ix[q] = bi.ix[q];
+    iy[q] = bi.iy[q];
+    iz[q] = bi.iz[q];
+    for (int d = 0; d < nb; ++d) {
+      lx[(size_t)q * nb + d] = bi.lx[(size_t)q * nb + d];
+      ly[(size_t)q * nb + d] = bi.ly[(size_t)q * nb + d];
+      lz[(size_t)q * nb + d] = bi.lz[(size_t)q * nb + d];
+    }
+  }
+  return 0;
 }
 
 int awp_check_finite(awp_ctx* c, int* ok) {

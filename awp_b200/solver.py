@@ -117,6 +117,20 @@ class Solver:
                                              c_float(fmajor), c_float(fminor),
                                              _fptr(st), _fptr(dp)), "awp_upload_plasticity")
 
+    def receivers(self, recvfile: str, nt: int) -> None:
+        """RECVFILE receivers (ASCII v2); records the current step at once."""
+        check(self.lib.awp_receivers_init(self.ctx, recvfile.encode(), int(nt)),
+              "awp_receivers_init")
+
+    def receiver_counts(self) -> tuple[int, int, int]:
+        c = (c_int * 3)()
+        check(self.lib.awp_receivers_count(self.ctx, c), "awp_receivers_count")
+        return tuple(int(v) for v in c)
+
+    def sourcefile(self, sourcefile: str) -> None:
+        """SOURCEFILE moment-tensor sources (ASCII v2 + <file>_<xx..yz> rates)."""
+        check(self.lib.awp_sourcefile_init(self.ctx, sourcefile.encode()), "awp_sourcefile_init")
+
     # -- time stepping -----------------------------------------------------
     def step(self, n: int = 1) -> None:
         check(self.lib.awp_step(self.ctx, int(n)), "awp_step")

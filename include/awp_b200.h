@@ -131,9 +131,47 @@ int awp_upload_plasticity(awp_ctx* ctx, const float* sigma2, const float* cohes,
                           const float* phi, float fmajor, float fminor,
                           const float strike[3], const float dip[3]);
 
+/* Receivers of an ASCII v2 RECVFILE (replaces receivers_init,
+ * src/topography/receivers/receivers.c:22-42, and the receivers_write calls of
+ * pmcl3d.c:1603-1605 and 2246-2247).  The velocities are interpolated with
+ * Lagrange weights of the file's degree every `stride` steps, staged through
+ * a device ring of gpu_buffer_size samples and a host ring of cpu_buffer_size
+ * device rings, and written as "<file>_<x|y|z>_<step>" (float32, receiver-major,
+ * num_writes rings per file, receiver.c:47-113).  nt = number of time steps of
+ * the run (pmcl3d's TMAX/DT + 1), used only for the zero padding of the file
+ * step.  The current state is recorded at once (step 0 before the first
+ * awp_step).  Set-up errors of the reference (unreadable or malformed file,
+ * AWP error codes 101..901 of include/awp/error.h) return AWP_ERR_IO with the
+ * code in awp_last_error(). */
+int awp_receivers_init(awp_ctx* ctx, const char* recvfile, long long nt);
+/* Receivers inside the domain per component (x, y, z). */
+int awp_receivers_count(awp_ctx* ctx, int counts[3]);
+
+/* Moment-tensor sources of an ASCII v2 SOURCEFILE (replaces sources_init /
+ * sources_read / sources_add_cartesian, src/topography/sources/sources.c:27-78,
+ * and their calls at pmcl3d.c:1563-1565, 1607, 1987-2004).  Rates are read
+ * from "<file>_<xx|yy|zz|xy|xz|yz>" (float32, source-major, `steps` samples
+ * each) in blocks of gpu_buffer_size*cpu_buffer_size samples and added every
+ * `stride` steps with Lagrange weights: sigma -= dt/h^3 * w * M(t). */
+int awp_sourcefile_init(awp_ctx* ctx, const char* sourcefile);
+
+/* Host-only helpers (no context, no GPU) that expose the point-set set-up for
+ * checks: the ASCII v2 reader (readers/input.c:35-42; hdr = length,
+ * gpu_buffer_size, cpu_buffer_size, steps, num_writes, stride, degree, major
+ * version) and the Lagrange interpolation of one staggered component
+ * (grid_type 0..8 = x, y, z, xx, yy, zz, xy, xz, yz) on one grid block
+ * (source.c:137-400).  They return 0 or the reference's error code. */
+int awp_input_read(const char* path, long long hdr[8], char* file, int filecap, float* x,
+                   float* y, float* z, int* type, long long cap);
+int awp_point_coefs(const char* path, int grid_type, int nxt, int nyt, int nzt, float h,
+                    long long cap, int* count, int* indices, int* ix, int* iy, int* iz,
+                    float* lx, float* ly, float* lz);
+
 /* Advance nsteps time steps (pmcl3d.c:1628-2487 order: velocity, stress +
- * attenuation, sources, plasticity, free-surface stress images).  Asynchronous
- * with respect to the host; call awp_synchronize to wait. */
+ * attenuation, SOURCEFILE and INSRC sources, plasticity, free-surface stress
+ * images, receivers).  Asynchronous with respect to the host except when a
+ * receiver ring is written to disk or a source ring is refilled from disk;
+ * call awp_synchronize to wait. */
 int awp_step(awp_ctx* ctx, int nsteps);
 int awp_synchronize(awp_ctx* ctx);
 /* Number of completed time steps. */

@@ -31,6 +31,9 @@ struct Base {
   virtual void set_filter(int order, const double* b, const double* a) = 0;
   virtual void get_moment(float* m) = 0;
   virtual void set_plasticity(float fmajor, float fminor, const float* Rz, const float* RzT) = 0;
+  virtual void add_point_sources(int field, int nq, int nb, const int* ix, const int* iy,
+                                 const int* iz, const float* lx, const float* ly, const float* lz,
+                                 int nsamples, const float* values, int stride) = 0;
   virtual void step(int nve, int n) = 0;
   virtual long long current() = 0;
   virtual void gather(int nbgx, int nedx, int nskpx, int nbgy, int nedy, int nskpy, int nbgz,
@@ -56,6 +59,13 @@ struct Oracle : Base {
   std::vector<double> filt_state;
   // plasticity
   T fmajor = 0, fminor = 0, Rz[9] = {}, RzT[9] = {};
+  // SOURCEFILE moment tensors, one entry per stress component
+  struct PointSrc {
+    int field, nq, nb, nsamples, stride;
+    std::vector<int> ix, iy, iz;
+    std::vector<float> lx, ly, lz, values;  // values[nsamples][nq]
+  };
+  std::vector<PointSrc> psrcs;
   long long cur = 0;
   bool initial_done = false;
 
@@ -588,6 +598,42 @@ struct Oracle : Base {
         for (int k = ALIGN; k <= kc1; k++) plast_app_cell(i, j, k);
   }
 
+  void add_point_sources(int field, int nq, int nb, const int* ix, const int* iy, const int* iz,
+                         const float* lx, const float* ly, const float* lz, int nsamples,
+                         const float* values, int stride) override {
+    PointSrc p;
+    p.field = field; p.nq = nq; p.nb = nb; p.nsamples = nsamples; p.stride = stride;
+    p.ix.assign(ix, ix + nq); p.iy.assign(iy, iy + nq); p.iz.assign(iz, iz + nq);
+    p.lx.assign(lx, lx + (size_t)nq * nb); p.ly.assign(ly, ly + (size_t)nq * nb);
+    p.lz.assign(lz, lz + (size_t)nq * nb);
+    p.values.assign(values, values + (size_t)nsamples * nq);
+    psrcs.push_back(p);
+  }
+
+  // cusource_add_cartesian (topography/sources/source.cu:24-49): every
+  // `stride` steps, sigma(cell) -= dt/h^3 * lx*ly*lz * M(step/stride), in
+  // query order; cells of the metric grid sit at (2 + ix, 2 + iy, align + iz).
+  void point_sources() {
+    const T dthh = DT / (DH * DH * DH);
+    for (const PointSrc& p : psrcs) {
+      if (cur % p.stride != 0) continue;
+      const long long smp = cur / p.stride;
+      if (smp >= p.nsamples) continue;
+      T* F = f[p.field].data();
+      for (int q = 0; q < p.nq; ++q) {
+        const T v = (T)p.values[(size_t)smp * p.nq + q];
+        for (int i = 0; i < p.nb; ++i)
+          for (int j = 0; j < p.nb; ++j)
+            for (int k = 0; k < p.nb; ++k) {
+              const long long pos =
+                  idx(2 + p.ix[q] + i, 2 + p.iy[q] + j, ALIGN + p.iz[q] + k);
+              F[pos] -= dthh * (T)p.lx[(size_t)q * p.nb + i] * (T)p.ly[(size_t)q * p.nb + j] *
+                        (T)p.lz[(size_t)q * p.nb + k] * v;
+            }
+      }
+    }
+  }
+
   void step(int nve, int n) override {
     for (int s = 0; s < n; ++s) {
       if (cur == 0 && !initial_done) {
@@ -597,6 +643,7 @@ struct Oracle : Base {
       cur += 1;
       velocity();
       stress();
+      point_sources();  // sources_add_cartesian (pmcl3d.c:1987-2004)
       if (ifault == 1 && cur < nst) addsrc((int)cur);
       if (ifault == 5) addkinsrc((int)cur);
       if (nve == 3) plasticity();
@@ -666,6 +713,11 @@ void oracle_get_moment(oracle* o, float* m) { o->impl->get_moment(m); }
 void oracle_set_plasticity(oracle* o, float fmajor, float fminor, const float* Rz,
                            const float* RzT) {
   o->impl->set_plasticity(fmajor, fminor, Rz, RzT);
+}
+void oracle_add_point_sources(oracle* o, int field, int nq, int nb, const int* ix,
+                              const int* iy, const int* iz, const float* lx, const float* ly,
+                              const float* lz, int nsamples, const float* values, int stride) {
+  o->impl->add_point_sources(field, nq, nb, ix, iy, iz, lx, ly, lz, nsamples, values, stride);
 }
 void oracle_step(oracle* o, int nve, int n) { o->impl->step(nve, n); }
 long long oracle_current_step(oracle* o) { return o->impl->current(); }

@@ -53,6 +53,12 @@ void oracle_set_plasticity(oracle* o, float fmajor, float fminor, const float* R
                            const float* RzT);
 
 /* nve: 1 or 3.  Advances n steps in pmcl3d order. */
+/* SOURCEFILE moment-tensor component on stress field `field` (oracle field
+ * index): queries with first indices ix/iy/iz on the metric grid and Lagrange
+ * weights l*[nq][nb]; values[nsamples][nq] applied every `stride` steps. */
+void oracle_add_point_sources(oracle* o, int field, int nq, int nb, const int* ix,
+                              const int* iy, const int* iz, const float* lx, const float* ly,
+                              const float* lz, int nsamples, const float* values, int stride);
 void oracle_step(oracle* o, int nve, int n);
 long long oracle_current_step(oracle* o);
 

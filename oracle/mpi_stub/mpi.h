@@ -1,6 +1,7 @@
 /*
  * Single-rank MPI stand-in used ONLY to compile the reference's host C files
- * (src/awp/mesh.c, src/awp/cerjan.c, src/awp/grid.c) into the CPU checker
+ * (src/awp/mesh.c, src/awp/cerjan.c, src/awp/grid.c, and the point-set set-up
+ * files listed in oracle/Makefile) into the CPU checker
  * library oracle/_ref/libawpref_host.so.  It is test infrastructure: the
  * product never includes it.
  *
@@ -34,6 +35,10 @@ typedef int MPI_File;
 #define MPI_DOUBLE ((MPI_Datatype)sizeof(double))
 #define MPI_INT ((MPI_Datatype)sizeof(int))
 #define MPI_OFFSET ((MPI_Datatype)sizeof(long long))
+#define MPI_BYTE ((MPI_Datatype)1)
+#ifndef MPI_AINT
+#define MPI_AINT ((MPI_Datatype)sizeof(long long))
+#endif
 #define MPI_MAX 1
 #define MPI_MIN 2
 #define MPI_SUM 3

@@ -50,6 +50,8 @@ def load():
         lib.oracle_get_moment.argtypes = [c_void_p, _F]
         lib.oracle_set_plasticity.argtypes = [c_void_p, c_float, c_float, _F, _F]
         lib.oracle_step.argtypes = [c_void_p, c_int, c_int]
+        lib.oracle_add_point_sources.argtypes = ([c_void_p, c_int, c_int, c_int] + [_I] * 3 +
+                                                 [_F] * 3 + [c_int, _F, c_int])
         lib.oracle_current_step.restype = c_longlong
         lib.oracle_current_step.argtypes = [c_void_p]
         lib.oracle_gather.argtypes = [c_void_p] + [c_int] * 9 + [_F] * 3
@@ -102,6 +104,19 @@ class OracleSim:
         a = np.ascontiguousarray(a, np.float64)
         self.lib.oracle_set_filter(self.o, len(b) - 1, b.ctypes.data_as(POINTER(c_double)),
                                    a.ctypes.data_as(POINTER(c_double)))
+
+    def add_point_sources(self, field, coefs, values, stride):
+        """coefs: ix/iy/iz [nq], lx/ly/lz [nq][nb]; values [nsamples][nq]."""
+        I = lambda a: np.ascontiguousarray(a, np.int32).ctypes.data_as(_I)  # noqa: E731
+        keep = [np.ascontiguousarray(coefs[k], np.int32) for k in ("ix", "iy", "iz")]
+        keepf = [np.ascontiguousarray(coefs[k], np.float32) for k in ("lx", "ly", "lz")]
+        vals = np.ascontiguousarray(values, np.float32)
+        nq, nb = keepf[0].shape
+        self.lib.oracle_add_point_sources(self.o, FIELD[field], nq, nb,
+                                          *[a.ctypes.data_as(_I) for a in keep],
+                                          *[fp(a) for a in keepf], vals.shape[0], fp(vals),
+                                          stride)
+        del I
 
     def step(self, n=1):
         self.lib.oracle_step(self.o, self.p.get("nve", 1), n)

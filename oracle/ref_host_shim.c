@@ -150,3 +150,103 @@ void ref_rotation_matrix(const float *strike, const float *dip, float *Rz, float
   memcpy(d, dip, sizeof(d));
   rotation_matrix(s, d, Rz, RzT);
 }
+
+/* ------------------------------------------------------------------------ */
+/* Point sets (RECVFILE / SOURCEFILE): the reference's ASCII v2 reader and   */
+/* its interpolation set-up, one rank, one grid block, no topography.        */
+/* ------------------------------------------------------------------------ */
+#include <readers/input.h>
+#include <grid/grid_3d.h>
+#include <grid/shift.h>
+#include <topography/grids.h>
+#include <interpolation/interpolation.h>
+#include <mpi/distribute.h>
+#include <topography/sources/source.h> /* SOURCE_OFFSET_X */
+
+static input_t g_input;
+static int g_input_ok = 0;
+
+/* input_init (readers/input.c:35-42).  hdr[] = length, gpu_buffer_size,
+ * cpu_buffer_size, steps, num_writes, stride, degree, major version. */
+int ref_input_read(const char *path, long long *hdr, char *file, int filecap) {
+  if (g_input_ok) input_finalize(&g_input);
+  memset(&g_input, 0, sizeof(g_input));
+  int err = input_init(&g_input, path);
+  g_input_ok = (err == 0);
+  if (err) return err;
+  hdr[0] = (long long)g_input.length;
+  hdr[1] = (long long)g_input.gpu_buffer_size;
+  hdr[2] = (long long)g_input.cpu_buffer_size;
+  hdr[3] = (long long)g_input.steps;
+  hdr[4] = (long long)g_input.num_writes;
+  hdr[5] = g_input.stride;
+  hdr[6] = g_input.degree;
+  hdr[7] = g_input.version.major;
+  snprintf(file, filecap, "%s", g_input.file);
+  return 0;
+}
+
+void ref_input_data(float *x, float *y, float *z, int *type) {
+  for (size_t i = 0; i < g_input.length; ++i) {
+    x[i] = g_input.x[i];
+    y[i] = g_input.y[i];
+    z[i] = g_input.z[i];
+    type[i] = g_input.type[i];
+  }
+}
+
+/* The interpolation set-up of source_init_common (topography/sources/
+ * source.c:137-400) for the last file read, at one rank, one grid block,
+ * no topography.  grid_type follows enum grid_types (X=0, Y, Z, XX, YY, ZZ,
+ * XY, XZ, YZ).  The reference's building blocks do the work (grids_init,
+ * dist_indices, grid_init_metric_grid, grid_data_init,
+ * interp_lagrange1_coef); the few lines of glue restate source.c:193-205 and
+ * 288-360.  Returns the number of owned points, or -err. */
+int ref_point_coefs(int grid_type, int nxt, int nyt, int nzt, float h, int *indices,
+                    int *ix, int *iy, int *iz, float *lx, float *ly, float *lz) {
+  grids_t grids = grids_init(nxt, nyt, nzt, 0, 0, 0, 0, h);
+  grid3_t grid = grids_select((enum grid_types)grid_type, &grids);
+  size_t n = g_input.length;
+  prec dm0 = 0;
+  prec *x = malloc(sizeof(prec) * n), *y = malloc(sizeof(prec) * n),
+       *z = malloc(sizeof(prec) * n);
+  for (size_t i = 0; i < n; ++i) {
+    x[i] = g_input.x[i] + SOURCE_OFFSET_X * grid.gridspacing;
+    y[i] = g_input.y[i];
+    z[i] = g_input.z[i];
+    /* DM offsets of the top block are zero, but adding them turns -0 into +0
+     * (source.c:201-203) */
+    x[i] = x[i] + dm0;
+    y[i] = y[i] + dm0;
+    z[i] = z[i] + dm0;
+  }
+  int *idx = NULL;
+  size_t len = 0;
+  int err = dist_indices(&idx, &len, x, y, n, grid);
+  if (err) return -err;
+  prec block_height = grid.gridspacing * (grid.size.z - 1);
+  prec lower = 0 - block_height + 0;
+  grid3_t full = grid_init_metric_grid(grid.inner_size, grid.shift, grid.coordinate,
+                                       grid.boundary1, grid.boundary2, grid.gridspacing);
+  grid_data_t xyz;
+  grid_data_init(&xyz, full);
+  int deg = g_input.degree, nb = deg + 1;
+  prec *xloc = calloc(sizeof(prec), nb);
+  for (size_t q = 0; q < len; ++q) {
+    int s = idx[q];
+    prec zz = z[s];
+    if (g_input.type[s] == INPUT_VOLUME_COORD) zz = zz - lower;
+    else if (g_input.type[s] == INPUT_SURFACE_COORD) zz = block_height;
+    indices[q] = s;
+    err = interp_lagrange1_coef(xloc, &lx[q * nb], &ix[q], xyz.x, grid_boundary_size(full).x,
+                                x[s], deg);
+    err = interp_lagrange1_coef(xloc, &ly[q * nb], &iy[q], xyz.y, grid_boundary_size(full).y,
+                                y[s], deg);
+    err = interp_lagrange1_coef(xloc, &lz[q * nb], &iz[q], xyz.z, grid_boundary_size(full).z,
+                                zz, deg);
+  }
+  free(xloc);
+  grid_data_free(&xyz);
+  free(x); free(y); free(z); free(idx);
+  return (int)len;
+}

@@ -51,6 +51,10 @@ class RefHost:
         lib.ref_inicrj.argtypes = [c_float] + [c_int] * 8 + [_F] * 3
         lib.ref_hoek_brown.argtypes = [c_float] * 5 + [c_int, _F, _F]
         lib.ref_rotation_matrix.argtypes = [_F, _F, _F, _F]
+        lib.ref_input_read.argtypes = [ctypes.c_char_p, POINTER(ctypes.c_longlong),
+                                       ctypes.c_char_p, c_int]
+        lib.ref_input_data.argtypes = [_F, _F, _F, _I]
+        lib.ref_point_coefs.argtypes = [c_int, c_int, c_int, c_int, c_float] + [_I] * 4 + [_F] * 3
         self.lib = lib
 
     def tausub(self, taumin, taumax):
@@ -124,6 +128,91 @@ class RefHost:
         rzt = np.zeros(9, np.float32)
         self.lib.ref_rotation_matrix(fptr(st), fptr(dp), fptr(rz), fptr(rzt))
         return rz, rzt
+
+
+    def input_read(self, path):
+        """input_init (readers/input.c:35-42): (status, header dict, x, y, z, type)."""
+        hdr = (ctypes.c_longlong * 8)()
+        fname = ctypes.create_string_buffer(2048)
+        err = self.lib.ref_input_read(path.encode(), hdr, fname, 2048)
+        if err:
+            return err, None, None, None, None, None
+        n = int(hdr[0])
+        x = np.zeros(n, np.float32)
+        y = np.zeros(n, np.float32)
+        z = np.zeros(n, np.float32)
+        t = np.zeros(n, np.int32)
+        self.lib.ref_input_data(fptr(x), fptr(y), fptr(z), t.ctypes.data_as(_I))
+        keys = ["length", "gpu_buffer_size", "cpu_buffer_size", "steps", "num_writes", "stride",
+                "degree", "major"]
+        h = {k: int(v) for k, v in zip(keys, hdr)}
+        h["file"] = fname.value.decode()
+        return 0, h, x, y, z, t
+
+    def point_coefs(self, path, grid_type, nx, ny, nz, h):
+        """The interpolation set-up of source_init_common for one component,
+        built from the reference's own routines (see ref_host_shim.c)."""
+        err, hdr, *_ = self.input_read(path)
+        assert err == 0, err
+        n = hdr["length"]
+        nb = hdr["degree"] + 1
+        idx = np.zeros(n, np.int32)
+        ix = np.zeros(n, np.int32)
+        iy = np.zeros(n, np.int32)
+        iz = np.zeros(n, np.int32)
+        lx = np.zeros(n * nb, np.float32)
+        ly = np.zeros(n * nb, np.float32)
+        lz = np.zeros(n * nb, np.float32)
+        I = lambda a: a.ctypes.data_as(_I)  # noqa: E731
+        cnt = self.lib.ref_point_coefs(grid_type, nx, ny, nz, h, I(idx), I(ix), I(iy), I(iz),
+                                       fptr(lx), fptr(ly), fptr(lz))
+        assert cnt >= 0, cnt
+        return dict(indices=idx[:cnt], ix=ix[:cnt], iy=iy[:cnt], iz=iz[:cnt],
+                    lx=lx[:cnt * nb].reshape(cnt, nb), ly=ly[:cnt * nb].reshape(cnt, nb),
+                    lz=lz[:cnt * nb].reshape(cnt, nb))
+
+
+class RefPoints:
+    """The reference's own point-set device code for one component
+    (interpolation.cu cuinterp_interp_H, source.cu cusource_add_cartesian_H),
+    set up from an ASCII v2 file by ref_points_shim.c."""
+
+    _lib = None
+
+    @classmethod
+    def lib(cls):
+        if cls._lib is None:
+            path = os.path.join(REF_DIR, "libawpref_points.so")
+            if not os.path.exists(path):
+                raise FileNotFoundError(f"{path} missing: run `make -C oracle ref`")
+            lib = ctypes.CDLL(path, mode=ctypes.RTLD_LOCAL)
+            lib.ref_pts_create.restype = c_void_p
+            lib.ref_pts_create.argtypes = [ctypes.c_char_p, c_int, c_int, c_int, c_int, c_float,
+                                           _I]
+            lib.ref_pts_interp.argtypes = [c_void_p, c_void_p, c_void_p]
+            lib.ref_pts_srcadd.argtypes = [c_void_p, c_void_p, c_void_p, c_float, c_float]
+            lib.ref_pts_destroy.argtypes = [c_void_p]
+            cls._lib = lib
+        return cls._lib
+
+    def __init__(self, path, grid_type, nx, ny, nz, h):
+        lib = self.lib()
+        n = c_int(0)
+        self.h = lib.ref_pts_create(path.encode(), grid_type, nx, ny, nz, h, byref(n))
+        if not self.h:
+            raise RuntimeError("reference point-set set-up failed")
+        self.count = n.value
+
+    def interp(self, d_out_ptr, d_in_ptr):
+        self.lib().ref_pts_interp(self.h, c_void_p(d_out_ptr), c_void_p(d_in_ptr))
+
+    def srcadd(self, d_field_ptr, d_values_ptr, h, dt):
+        self.lib().ref_pts_srcadd(self.h, c_void_p(d_field_ptr), c_void_p(d_values_ptr), h, dt)
+
+    def close(self):
+        if self.h:
+            self.lib().ref_pts_destroy(self.h)
+            self.h = None
 
 
 def lithostatic_sigma2(d1, nx, ny, nz, dh):
@@ -302,6 +391,11 @@ class RefGpuSim:
         self._fz = fz
         self.cur = 0
         self.source_step = 1
+        # callables(sim, step): after the stress update (SOURCEFILE adds,
+        # pmcl3d.c:1987-2004) and after the free-surface imaging (receivers,
+        # pmcl3d.c:2246-2247)
+        self.after_stress = []
+        self.after_step = []
         if p["ifault"] == 1 and self.npsrc:
             # initial sample added on the host before the copy (pmcl3d.c:1175-1187)
             self._addsrc(1)
@@ -372,6 +466,8 @@ class RefGpuSim:
                 self._stress(NGSL + 4, nx + NGSL - 1, yls, yre)
             self._stress(xls, NGSL + 3, yls, yre)
             self._stress(nx + NGSL, xre, yls, yre)
+            for hook in self.after_stress:
+                hook(self, self.cur)
             if self.p["ifault"] < 4 and self.cur < self.p["nst"]:
                 self.source_step += 1
                 self._addsrc(self.source_step)
@@ -393,6 +489,8 @@ class RefGpuSim:
                                         P(f["xz"]), P(f["yz"]), P(f["mu"]), P(f["sigma2"]),
                                         P(f["yldfac"]), nz, xls, xre, yls, yre, None, 0)
             self.lib.fstr_H(P(f["zz"]), P(f["xz"]), P(f["yz"]), None, xls, xre, yls, yre)
+            for hook in self.after_step:
+                hook(self, self.cur)
         self.torch.cuda.synchronize()
 
     def field(self, name):
