@@ -1,9 +1,11 @@
 // pmcl3d -- single-rank drop-in for the reference's pmcl3d executable.
 //
 // Same command line (src/awp/command.c), same input files (INVEL mesh,
-// INSRC sources, sourcefilter.dat, nonlinear.dat) and the same output files
-// (OUT/SX_0_%07ld, SY, SZ, Eta; the CHKFILE statistics log) as the reference's
-// single-rank run; the time step itself runs in libawpb200 through its C ABI.
+// INSRC sources, sourcefilter.dat, nonlinear.dat, SOURCEFILE and RECVFILE
+// point sets) and the same output files (OUT/SX_0_%07ld, SY, SZ, Eta; the
+// CHKFILE statistics log; the receiver files <file>_<x|y|z>_<step>) as the
+// reference's single-rank run; the time step itself runs in libawpb200
+// through its C ABI.
 //
 // Scope: one rank (PX = PY = 1, no I/O ranks), one grid, MEDIASTART 0-2,
 // IFAULT 1 and 5, NVE 1 and 3.  Anything else is reported and refused.
@@ -253,9 +255,8 @@ int main(int argc, char** argv) {
             A.NGRIDS);
     return 1;
   }
-  if (A.USETOPO || A.USESOURCEFILE || A.USERECVFILE || A.USEFORCEFILE || A.USESGTFILE) {
-    fprintf(stderr, "pmcl3d: INTOPO/SOURCEFILE/RECVFILE/FORCEFILE/SGTFILE are not part of "
-                    "this build\n");
+  if (A.USETOPO || A.USEFORCEFILE || A.USESGTFILE) {
+    fprintf(stderr, "pmcl3d: INTOPO/FORCEFILE/SGTFILE are not part of this build\n");
     return 1;
   }
   if (A.NZ[0] % 4 != 0) {  // pmcl3d.c:380-391 (BLOCK_SIZE_Z = 4)
@@ -486,6 +487,10 @@ int main(int argc, char** argv) {
     AWP(awp_upload_plasticity(ctx, sigma2.data(), cohes.data(), phi.data(), fmajor, fminor,
                               strike, dip));
   }
+
+  // ---- SOURCEFILE / RECVFILE point sets (pmcl3d.c:1563-1568, 1603-1607) ---------
+  if (A.USESOURCEFILE) AWP(awp_sourcefile_init(ctx, A.SOURCEFILE.c_str()));
+  if (A.USERECVFILE) AWP(awp_receivers_init(ctx, A.RECVFILE.c_str(), nt));
 
   // ---- output buffers ------------------------------------------------------------
   const size_t rec = (size_t)rnx * rny * rnz;

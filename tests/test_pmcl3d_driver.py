@@ -92,3 +92,53 @@ def test_full_run_matches_library(tmp_path):
             assert np.array_equal(got, want), (c, step)
     chk = open(os.path.join(tmp_path, "chk")).read()
     assert "STABILITY CRITERIA" in chk and chk.strip().endswith("END")
+
+
+def test_recvfile_needs_readable_file(tmp_path):
+    scn = scenarios.random_small(nx=16, ny=16, nz=16, steps=2, seed=9, ifault=1, nsrc=1)
+    write_inputs(scn, tmp_path)
+    r = run(["-X", 16, "-Y", 16, "-Z", 16, "-T", 0.01, "-B", 1, "-n", 5, "--INVEL", "media",
+             "--INSRC", "src", "--RECVFILE", "missing.txt"], tmp_path)
+    assert r.returncode != 0
+
+
+@pytest.mark.gpu
+def test_point_sets_match_library(tmp_path):
+    """--SOURCEFILE and --RECVFILE through the executable give the same receiver
+    files as the same run through the library."""
+    from awp_b200 import pointfiles
+    scn = scenarios.random_small(nx=24, ny=20, nz=32, steps=12, seed=9, ifault=1, nsrc=2)
+    p = scn.params
+    write_inputs(scn, tmp_path)
+    nt = 12
+    tmax = (nt - 1) * p["dt"] + p["dt"] * 0.5
+    h = p["dh"]
+    os.makedirs(tmp_path / "lib", exist_ok=True)
+    for d in (tmp_path, tmp_path / "lib"):
+        pointfiles.write_input(str(d / "src.txt"), str(d / "msrc"), [[8 * h, 9 * h, -12 * h]],
+                               degree=3, gpu_buffer_size=2, cpu_buffer_size=3, steps=12)
+        rates = np.linspace(0, 1, 12 * 6, dtype=np.float32).reshape(1, 12, 6) * 1e14
+        pointfiles.write_source_rates(str(d / "msrc"), rates)
+        pointfiles.write_input(str(d / "recv.txt"), str(d / "rcv"),
+                               [[5 * h, 6 * h, 0.0], [9.5 * h, 7 * h, -3 * h]], [1, 0],
+                               degree=3, gpu_buffer_size=3, cpu_buffer_size=2, num_writes=2)
+    args = ["-X", p["nx"], "-Y", p["ny"], "-Z", p["nz"], "-H", p["dh"], "-t", p["dt"],
+            "-T", tmax, "-D", p["nd"], "-A", p["arbc"], "-V", 1, "-B", 1, "-n", 5,
+            "-I", 1, "-S", scn.src_pos.shape[0], "-N", p["nst"], "-R", p["nst"],
+            "--INVEL", "media", "--INSRC", "src", "-o", "out", "-c", "chk",
+            "--SOURCEFILE", str(tmp_path / "src.txt"), "--RECVFILE", str(tmp_path / "recv.txt")]
+    r = run(args, tmp_path)
+    assert r.returncode == 0, r.stderr + r.stdout
+    s = Solver(default_params(**p))
+    s.upload_media(scn.media)
+    s.upload_sources(scn.src_pos, scn.src_data)
+    s.sourcefile(str(tmp_path / "lib" / "src.txt"))
+    s.receivers(str(tmp_path / "lib" / "recv.txt"), nt)
+    s.step(nt)
+    s.synchronize()
+    s.close()
+    got = pointfiles.read_receiver_series(str(tmp_path / "rcv"), 2, nt, 3, 2, 2, 1)
+    want = pointfiles.read_receiver_series(str(tmp_path / "lib" / "rcv"), 2, nt, 3, 2, 2, 1)
+    for c in "xyz":
+        assert got[c].shape == (2, 12) and np.any(got[c] != 0)
+        assert np.array_equal(got[c], want[c]), c
