@@ -54,6 +54,8 @@ class awp_params(ctypes.Structure):
         ("ifault", c_int),
         ("nst", c_int),
         ("read_step", c_int),
+        ("grid", c_int),
+        ("ngrids", c_int),
     ]
 
 
@@ -105,6 +107,11 @@ def load() -> ctypes.CDLL:
     _sig(lib, "awp_gather_output", c_int,
          [_P] + [c_int] * 9 + [c_void_p] * 4)
     _sig(lib, "awp_check_finite", c_int, [_P, _I])
+    _sig(lib, "awp_mesh_create", c_int, [POINTER(awp_params), c_int, POINTER(c_void_p)])
+    _sig(lib, "awp_mesh_destroy", c_int, [_P])
+    _sig(lib, "awp_mesh_grid", c_int, [_P, c_int, POINTER(c_void_p)])
+    _sig(lib, "awp_mesh_step", c_int, [_P, c_int])
+    _sig(lib, "awp_mesh_synchronize", c_int, [_P])
     _sig(lib, "awp_receivers_init", c_int, [_P, c_char_p, c_longlong])
     _sig(lib, "awp_receivers_count", c_int, [_P, _I])
     _sig(lib, "awp_sourcefile_init", c_int, [_P, c_char_p])

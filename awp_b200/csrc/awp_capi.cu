@@ -13,6 +13,7 @@
 
 #include "../../include/awp_b200.h"
 #include "awp_common.h"
+#include "awp_dm.cuh"
 #include "awp_host.h"
 #include "awp_kernels.cuh"
 #include "awp_pointsets.h"
@@ -133,9 +134,11 @@ StrArgs make_str_args(awp_ctx* c) {
   a.yline = c->g.yline;
   a.lam_mu_ld = (int)c->g.ny_pad();
   a.i0 = c->xls; a.i1 = c->xre; a.j0 = c->yls; a.j1 = c->yre;
+  // dstrqc: k from align+3 to maxk (kernel.cu:900-911); the free-surface
+  // images belong to the top grid only
   a.k0 = AWP_ALIGN + 3;
-  a.k1 = c->g.top();
-  a.fs = 1;
+  a.k1 = (c->p.grid == 0) ? c->g.top() : c->g.top() - 2;
+  a.fs = (c->p.grid == 0) ? 1 : 0;
   a.ktop = c->g.top();
   a.gx_lim = c->p.nx + AWP_NGSL + 1;                      // g_i < NX, rankx = 0
   a.gy_min = (c->p.npc == 2) ? INT_MIN : AWP_NGSL + 3;     // g_j > 1 || NPC == 2
@@ -262,8 +265,11 @@ struct PhaseScope {
   }
 };
 
-int one_step(awp_ctx* c) {
-  float** f = c->f;
+// ---- one time step in phases (pmcl3d.c:1628-2487 at one rank) --------------
+// A single grid runs them in order (one_step); a discontinuous mesh
+// interleaves them with the coupling kernels (mesh_step).
+
+int phase_begin(awp_ctx* c) {
   if (c->cur_step == 0 && !c->initial_src_done) {
     // step-1 source sample is added before the loop (pmcl3d.c:1175-1187)
     if (c->p.ifault < 4) {
@@ -274,6 +280,11 @@ int one_step(awp_ctx* c) {
     c->initial_src_done = true;
   }
   c->cur_step += 1;
+  return AWP_OK;
+}
+
+int phase_velocity(awp_ctx* c) {
+  float** f = c->f;
   VelArgs v;
   v.u1 = f[AWP_U1]; v.v1 = f[AWP_V1]; v.w1 = f[AWP_W1];
   v.xx = f[AWP_XX]; v.yy = f[AWP_YY]; v.zz = f[AWP_ZZ];
@@ -282,28 +293,39 @@ int one_step(awp_ctx* c) {
   v.slice = c->g.slice; v.yline = c->g.yline;
   v.i0 = 2 + AWP_NGSL; v.i1 = c->g.nxt + AWP_NGSL + 1;          // xvs..xve
   v.j0 = 2 + AWP_NGSL; v.j1 = 2 + AWP_NGSL + round_up(c->g.nyt, 2) - 1;
-  v.k0 = AWP_ALIGN; v.k1 = AWP_ALIGN + round_up(c->g.nzt, 4) - 1;
+  // dvelcx_opt leaves the interface layers of a mesh to dvelc2 / intp3d /
+  // swap3: k <= nzt+align-3 below the top grid, k >= align+3 above the
+  // bottom grid (kernel.cu:146-147)
+  v.k0 = (c->p.grid < c->p.ngrids - 1) ? AWP_ALIGN + 3 : AWP_ALIGN;
+  v.k1 = AWP_ALIGN + round_up(c->g.nzt, 4) - 1;
+  if (c->p.grid > 0) v.k1 = std::min(v.k1, c->g.nzt + AWP_ALIGN - 3);
   v.dth = c->dth; v.c1 = c->c1; v.c2 = c->c2;
   const bool tma = c->tma_ok && awp_tuning_get("tma") == 1;
-  {
-    PhaseScope ps(c, 0);
-    if (tma)
-      CU_TRY(awp_launch_velocity_tma(v, c->vel_maps, awp_tuning_get("ichunk"), c->d_err,
-                                     c->stream));
-    else
-      CU_TRY(awp_launch_velocity(v, c->stream));
-    c->launches++;
-  }
-  {
-    PhaseScope ps(c, 1);
-    StrArgs s = make_str_args(c);
-    if (tma)
-      CU_TRY(awp_launch_stress_tma(s, c->str_maps, c->elastic, awp_tuning_get("ichunk"),
-                                   c->d_err, c->stream));
-    else
-      CU_TRY(awp_launch_stress(s, c->elastic, c->stream));
-    c->launches++;
-  }
+  PhaseScope ps(c, 0);
+  if (tma)
+    CU_TRY(awp_launch_velocity_tma(v, c->vel_maps, awp_tuning_get("ichunk"), c->d_err,
+                                   c->stream));
+  else
+    CU_TRY(awp_launch_velocity(v, c->stream));
+  c->launches++;
+  return AWP_OK;
+}
+
+int phase_stress(awp_ctx* c) {
+  const bool tma = c->tma_ok && awp_tuning_get("tma") == 1;
+  PhaseScope ps(c, 1);
+  StrArgs s = make_str_args(c);
+  if (tma)
+    CU_TRY(awp_launch_stress_tma(s, c->str_maps, c->elastic, awp_tuning_get("ichunk"),
+                                 c->d_err, c->stream));
+  else
+    CU_TRY(awp_launch_stress(s, c->elastic, c->stream));
+  c->launches++;
+  return AWP_OK;
+}
+
+int phase_sources(awp_ctx* c) {
+  float** f = c->f;
   if (c->srcf) {  // sources_read + sources_add_cartesian (pmcl3d.c:1987-2004)
     PhaseScope ps(c, 2);
     float* const stress[6] = {f[AWP_XX], f[AWP_YY], f[AWP_ZZ], f[AWP_XY], f[AWP_XZ], f[AWP_YZ]};
@@ -318,26 +340,179 @@ int one_step(awp_ctx* c) {
     if (st) return st;
     if (c->ncell) c->launches++;
   }
-  if (c->p.nve == 3) {
-    PhaseScope ps(c, 3);
-    int st = launch_plasticity(c);
-    if (st) return st;
-    c->launches += 2;
-  }
+  return AWP_OK;
+}
+
+int phase_plasticity(awp_ctx* c) {
+  if (c->p.nve != 3) return AWP_OK;
+  PhaseScope ps(c, 3);
+  int st = launch_plasticity(c);
+  if (st) return st;
+  c->launches += 2;
+  return AWP_OK;
+}
+
+int phase_fstr(awp_ctx* c) {
+  if (c->p.grid != 0) return AWP_OK;  // fstr_H on grid 0 only (pmcl3d.c:2243)
+  float** f = c->f;
   FstrArgs fs;
   fs.zz = f[AWP_ZZ]; fs.xz = f[AWP_XZ]; fs.yz = f[AWP_YZ];
   fs.slice = c->g.slice; fs.yline = c->g.yline; fs.ktop = c->g.top();
   fs.i0 = c->xls; fs.i1 = c->xre;
   fs.j0 = c->yls; fs.j1 = c->yls + round_up(c->yre - c->yls + 1, 2) - 1;
-  {
-    PhaseScope ps(c, 4);
-    CU_TRY(awp_launch_fstr(fs, c->stream));
-    c->launches++;
-  }
+  PhaseScope ps(c, 4);
+  CU_TRY(awp_launch_fstr(fs, c->stream));
+  c->launches++;
+  return AWP_OK;
+}
+
+int phase_receivers(awp_ctx* c) {
+  float** f = c->f;
   if (c->recv &&  // receivers_write (pmcl3d.c:2246-2247)
       awp_recv_record(c->recv, c->cur_step, f[AWP_U1], f[AWP_V1], f[AWP_W1], c->stream,
                       &c->launches, g_errmsg, sizeof(g_errmsg)))
     return AWP_ERR_IO;
+  return AWP_OK;
+}
+
+int one_step(awp_ctx* c) {
+  int st;
+  if ((st = phase_begin(c))) return st;
+  if ((st = phase_velocity(c))) return st;
+  if ((st = phase_stress(c))) return st;
+  if ((st = phase_sources(c))) return st;
+  if ((st = phase_plasticity(c))) return st;
+  if ((st = phase_fstr(c))) return st;
+  return phase_receivers(c);
+}
+
+}  // namespace
+
+namespace {
+
+DmGrid dm_grid(awp_ctx* c) {
+  DmGrid g;
+  float** f = c->f;
+  g.u1 = f[AWP_U1]; g.v1 = f[AWP_V1]; g.w1 = f[AWP_W1];
+  g.xx = f[AWP_XX]; g.yy = f[AWP_YY]; g.zz = f[AWP_ZZ];
+  g.xy = f[AWP_XY]; g.xz = f[AWP_XZ]; g.yz = f[AWP_YZ];
+  g.nxt = c->g.nxt; g.nyt = c->g.nyt; g.nzt = c->g.nzt;
+  g.slice = c->g.slice; g.yline = c->g.yline;
+  return g;
+}
+
+int dm_interfaces(awp_ctx* const* g, int n, cudaStream_t st) {
+  for (int p = 1; p < n; ++p) {  // coarse -> fine (pmcl3d.c:1767-1772, 2057-2062)
+    DmPairArgs a{dm_grid(g[p]), dm_grid(g[p - 1])};
+    CU_TRY(awp_launch_intp3d(a, st));
+    g[p]->launches++;
+  }
+  for (int p = 0; p < n - 1; ++p) {  // fine -> coarse (pmcl3d.c:1802-1806, 2085-2090)
+    DmPairArgs a{dm_grid(g[p + 1]), dm_grid(g[p])};
+    CU_TRY(awp_launch_swap3(a, st));
+    g[p]->launches++;
+  }
+  return AWP_OK;
+}
+
+int dm_velocity(awp_ctx* c) {  // dvelc2 (pmcl3d.c:1729-1732)
+  DmVel2Args a;
+  a.g = dm_grid(c);
+  a.d1 = c->f[AWP_D1];
+  a.dcrjx = c->dcrjx; a.dcrjy = c->dcrjy; a.dcrjz = c->dcrjz;
+  a.dth = c->dth;
+  CU_TRY(awp_launch_dvelc2(a, c->stream));
+  c->launches++;
+  return AWP_OK;
+}
+
+int dm_stress(awp_ctx* c) {  // dstrqc2 over xss1..xse3 x yls..yre (pmcl3d.c:1936-1948)
+  DmStr2Args a;
+  memset(&a, 0, sizeof(a));
+  float** f = c->f;
+  a.g = dm_grid(c);
+  a.r1 = f[AWP_R1]; a.r2 = f[AWP_R2]; a.r3 = f[AWP_R3];
+  a.r4 = f[AWP_R4]; a.r5 = f[AWP_R5]; a.r6 = f[AWP_R6];
+  a.lam = f[AWP_LAM]; a.mu = f[AWP_MU]; a.qp = f[AWP_QP]; a.qs = f[AWP_QS];
+  a.dcrjx = c->dcrjx; a.dcrjy = c->dcrjy; a.dcrjz = c->dcrjz;
+  a.tex = c->tex;
+  memcpy(a.coeff, c->coeff, sizeof(a.coeff));
+  a.i0 = c->xls; a.i1 = c->xre; a.j0 = c->yls; a.j1 = c->yre;
+  a.dth = c->dth; a.dh1 = c->dh1; a.dt = c->p.dt;
+  CU_TRY(awp_launch_dstrqc2(a, c->stream));
+  c->launches++;
+  return AWP_OK;
+}
+
+}  // namespace
+
+struct awp_mesh {
+  int ngrids = 0;
+  awp_ctx* g[AWP_MAXGRIDS] = {};
+  cudaStream_t stream = nullptr;
+  bool prepared = false;
+};
+
+namespace {
+
+// checkmesh of the media (pmcl3d.c:892-899): the coarse grid's top three
+// levels take the finer grid's values; then each grid's elastic
+// specialisation is decided on the corrected Q.
+int mesh_prepare(awp_mesh* m) {
+  for (int p = 0; p < m->ngrids; ++p)
+    if (!m->g[p]->media_ready)
+      return set_error(AWP_ERR_STATE, "grid %d has no media (awp_upload_media first)", p);
+  for (int p = 1; p < m->ngrids; ++p) {
+    awp_ctx *lo = m->g[p], *hi = m->g[p - 1];
+    DmCheckArgs a;
+    const int fid[5] = {AWP_D1, AWP_MU, AWP_LAM, AWP_QP, AWP_QS};
+    for (int q = 0; q < 5; ++q) {
+      a.lo[q] = lo->f[fid[q]];
+      a.hi[q] = hi->f[fid[q]];
+    }
+    a.nf = 5;
+    a.glo = dm_grid(lo);
+    a.ghi = dm_grid(hi);
+    CU_TRY(awp_launch_checkmesh(a, m->stream));
+  }
+  for (int p = 1; p < m->ngrids; ++p) {
+    awp_ctx* c = m->g[p];
+    unsigned int hflag = 1;
+    CU_TRY(cudaMemsetAsync(c->d_flag, 0, sizeof(unsigned int), m->stream));
+    CU_TRY(awp_launch_anynonzero(c->f[AWP_QP], c->g.cells_pad(), c->d_flag, m->stream));
+    CU_TRY(awp_launch_anynonzero(c->f[AWP_QS], c->g.cells_pad(), c->d_flag, m->stream));
+    CU_TRY(cudaMemcpyAsync(&hflag, c->d_flag, sizeof(hflag), cudaMemcpyDeviceToHost, m->stream));
+    CU_TRY(cudaStreamSynchronize(m->stream));
+    c->elastic = (hflag == 0);
+  }
+  m->prepared = true;
+  return AWP_OK;
+}
+
+// One time step of the whole stack in pmcl3d's order (pmcl3d.c:1628-2490).
+int mesh_step(awp_mesh* m) {
+  awp_ctx* const* g = m->g;
+  const int n = m->ngrids;
+  int st;
+  for (int p = 0; p < n; ++p)
+    if ((st = phase_begin(g[p]))) return st;
+  for (int p = 0; p < n; ++p)
+    if ((st = phase_velocity(g[p]))) return st;
+  for (int p = 0; p < n - 1; ++p)
+    if ((st = dm_velocity(g[p]))) return st;
+  if ((st = dm_interfaces(g, n, m->stream))) return st;
+  for (int p = 0; p < n; ++p)
+    if ((st = phase_stress(g[p]))) return st;
+  for (int p = 0; p < n - 1; ++p)
+    if ((st = dm_stress(g[p]))) return st;
+  for (int p = 0; p < n; ++p)
+    if ((st = phase_sources(g[p]))) return st;
+  if ((st = dm_interfaces(g, n, m->stream))) return st;
+  for (int p = 0; p < n; ++p)
+    if ((st = phase_plasticity(g[p]))) return st;
+  if ((st = phase_fstr(g[0]))) return st;
+  for (int p = 0; p < n; ++p)
+    if ((st = phase_receivers(g[p]))) return st;
   return AWP_OK;
 }
 
@@ -356,6 +531,8 @@ void awp_params_default(awp_params* p) {
   p->ifault = 1;
   p->nst = 91;
   p->read_step = 91;
+  p->grid = 0;
+  p->ngrids = 1;
 }
 
 const char* awp_status_string(int status) {
@@ -401,6 +578,9 @@ int awp_ctx_create(const awp_params* p, awp_ctx** out) {
   if (p->nz % 4 != 0)
     return set_error(AWP_ERR_ARG, "NZ=%d is not divisible by 4 (pmcl3d.c:380-391)", p->nz);
   if (!(p->dh > 0) || !(p->dt > 0)) return set_error(AWP_ERR_ARG, "DH and DT must be > 0");
+  if (p->ngrids < 1 || p->ngrids > AWP_MAXGRIDS || p->grid < 0 || p->grid >= p->ngrids)
+    return set_error(AWP_ERR_ARG, "grid %d of %d (at most %d grids)", p->grid, p->ngrids,
+                     AWP_MAXGRIDS);
   if (p->nve != 1 && p->nve != 3)
     return set_error(AWP_ERR_UNSUPPORTED,
                      "NVE=%d: the time loop runs only for NVE 1 or 3 (pmcl3d.c:1624)", p->nve);
@@ -448,7 +628,9 @@ int awp_ctx_create(const awp_params* p, awp_ctx** out) {
   {
     const int nxp = (int)c->g.nx_pad(), nyp = (int)c->g.ny_pad(), nzp = (int)c->g.nz_pad();
     std::vector<float> cx(nxp, 1.0f), cy(nyp, 1.0f), cz(nzp, 1.0f);
-    awp::inicrj(p->arbc, p->nx, p->ny, p->nz, p->nx, p->ny, p->nd, 1, p->npc, cx.data(),
+    // the bottom sponge belongs to the lowest grid only (pmcl3d.c:1026-1028)
+    awp::inicrj(p->arbc, p->nx, p->ny, p->nz, p->nx, p->ny, p->nd,
+                p->grid == p->ngrids - 1 ? 1 : 0, p->npc, cx.data(),
                 cy.data(), cz.data());
     if ((st = ctx_alloc(c, (void**)&c->dcrjx, nxp * sizeof(float)))) goto fail;
     if ((st = ctx_alloc(c, (void**)&c->dcrjy, nyp * sizeof(float)))) goto fail;
@@ -745,6 +927,8 @@ int awp_step(awp_ctx* c, int nsteps) {
   if (!c->media_ready) return set_error(AWP_ERR_STATE, "awp_step before media upload");
   if (c->p.nve == 3 && !c->plast_ready)
     return set_error(AWP_ERR_STATE, "NVE=3 needs awp_upload_plasticity first");
+  if (c->p.ngrids > 1)
+    return set_error(AWP_ERR_STATE, "grid %d of a mesh: step the mesh (awp_mesh_step)", c->p.grid);
   for (int n = 0; n < nsteps; ++n) {
     int st = one_step(c);
     if (st) return st;
@@ -915,6 +1099,91 @@ int awp_point_coefs(const char* path, int grid_type, int nxt, int nyt, int nzt, 
   return 0;
 }
 
+int awp_mesh_destroy(awp_mesh* m) {
+  if (!m) return AWP_OK;
+  if (m->stream) cudaStreamSynchronize(m->stream);
+  for (int p = 0; p < m->ngrids; ++p) awp_ctx_destroy(m->g[p]);
+  if (m->stream) cudaStreamDestroy(m->stream);
+  delete m;
+  return AWP_OK;
+}
+
+int awp_mesh_create(const awp_params* grids, int ngrids, awp_mesh** out) {
+  if (!grids || !out) return set_error(AWP_ERR_ARG, "null argument");
+  *out = nullptr;
+  if (ngrids < 1 || ngrids > AWP_MAXGRIDS)
+    return set_error(AWP_ERR_ARG, "ngrids=%d (1..%d)", ngrids, AWP_MAXGRIDS);
+  for (int p = 0; p < ngrids; ++p) {
+    const awp_params& q = grids[p];
+    if (q.grid != p || q.ngrids != ngrids)
+      return set_error(AWP_ERR_ARG, "grid %d: params.grid/ngrids must be %d/%d", p, p, ngrids);
+    if (p > 0) {  // each block 3x coarser than the one above (pmcl3d.c:370-378)
+      const awp_params& f = grids[p - 1];
+      if (f.nx != 3 * q.nx || f.ny != 3 * q.ny)
+        return set_error(AWP_ERR_ARG, "grid %d: NX, NY must be 1/3 of grid %d's", p, p - 1);
+      if (f.dt != q.dt) return set_error(AWP_ERR_ARG, "grids must share DT");
+      if (q.nz < 8) return set_error(AWP_ERR_ARG, "grid %d: NZ too small for the interface", p);
+    }
+    if (p < ngrids - 1 && q.nz < 12)
+      return set_error(AWP_ERR_ARG, "grid %d: NZ too small for the interface", p);
+  }
+  awp_mesh* m = new awp_mesh();
+  cudaError_t e = cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    delete m;
+    return set_error(AWP_ERR_CUDA, "cudaStreamCreate: %s", cudaGetErrorString(e));
+  }
+  for (int p = 0; p < ngrids; ++p) {
+    int st = awp_ctx_create(&grids[p], &m->g[p]);
+    if (st) {
+      awp_mesh_destroy(m);
+      return st;
+    }
+    m->ngrids = p + 1;
+    awp_set_stream(m->g[p], m->stream);
+    if (p > 0) {
+      AwpTexture& t = m->g[p]->tex;
+      t.dm = 1;
+      t.nx = grids[p].nx;
+      t.f_ny = grids[p - 1].ny;
+      t.f_nzt = grids[p - 1].nz;
+    }
+  }
+  *out = m;
+  return AWP_OK;
+}
+
+int awp_mesh_grid(awp_mesh* m, int p, awp_ctx** ctx) {
+  if (!m || !ctx || p < 0 || p >= m->ngrids) return set_error(AWP_ERR_ARG, "bad grid %d", p);
+  *ctx = m->g[p];
+  return AWP_OK;
+}
+
+int awp_mesh_step(awp_mesh* m, int nsteps) {
+  if (!m) return set_error(AWP_ERR_ARG, "null mesh");
+  if (!m->prepared) {
+    int st = mesh_prepare(m);
+    if (st) return st;
+  }
+  for (int p = 0; p < m->ngrids; ++p)
+    if (m->g[p]->p.nve == 3 && !m->g[p]->plast_ready)
+      return set_error(AWP_ERR_STATE, "grid %d: NVE=3 needs awp_upload_plasticity first", p);
+  for (int s = 0; s < nsteps; ++s) {
+    int st = mesh_step(m);
+    if (st) return st;
+  }
+  return AWP_OK;
+}
+
+int awp_mesh_synchronize(awp_mesh* m) {
+  if (!m) return set_error(AWP_ERR_ARG, "null mesh");
+  for (int p = 0; p < m->ngrids; ++p) {
+    int st = awp_synchronize(m->g[p]);
+    if (st) return st;
+  }
+  return AWP_OK;
+}
+
 int awp_check_finite(awp_ctx* c, int* ok) {
   if (!c || !ok) return set_error(AWP_ERR_ARG, "null argument");
   CU_TRY(cudaMemsetAsync(c->d_flag, 0, sizeof(unsigned int), c->stream));
@@ -997,7 +1266,7 @@ int awp_cerjan(float arbc, int nxt, int nyt, int nzt, int nd, int islowest, int 
 
 int awp_texture_at(const float tau8[8], const float w8[8], float dt, int xls, int yls, int ny,
                    int nzt, int i, int j, int k, float* vx1, float* vx2, int* ww, float* wwo) {
-  AwpTexture t;
+  AwpTexture t{};
   awp::texture_tables(tau8, w8, dt, &t);
   t.xls = xls;
   t.yls = yls;

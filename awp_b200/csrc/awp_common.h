@@ -60,16 +60,34 @@ struct AwpTexture {
   int xls, yls;    // first (i, j) visited by init_texture
   int ny;          // yre - yls + 1
   int nzt;         // z cells of the grid
+  // Discontinuous mesh: on a grid with a finer grid above it, the top three
+  // levels hold the finer grid's values at the co-located points (checkmesh
+  // of the texture arrays, pmcl3d.c:1051-1057 with mesh.c:1404-1443).
+  int dm;          // 1 on such a grid
+  int nx;          // interior cells in x of this grid
+  int f_ny, f_nzt; // the finer grid's interior cells in y and z
 };
+
+AWP_HD int awp_tex_index_base(long long di, long long dj, int ny, int nzt, int kk) {
+  const long long ij = di * ny + dj;  // visits of the (i, j) loop before this one
+  const int itx = (int)((di + 1) & 1);
+  const int ity = (int)((ij + 1) & 1);
+  const int itz = (int)(((long long)nzt * (ij + 1) + kk) & 1);
+  return 4 * itx + 2 * ity + itz;
+}
 
 // Index into the eight-entry tables (= ww - 1 of the reference).
 AWP_HD int awp_tex_index(const AwpTexture& t, int i, int j, int k) {
-  const long long di = i - t.xls, dj = j - t.yls;
-  const long long ij = di * t.ny + dj;  // visits of the (i, j) loop before this one
-  const int itx = (int)((di + 1) & 1);
-  const int ity = (int)((ij + 1) & 1);
-  const int itz = (int)(((long long)t.nzt * (ij + 1) + (k - AWP_ALIGN)) & 1);
-  return 4 * itx + 2 * ity + itz;
+  if (t.dm) {
+    const int l = k - (AWP_ALIGN + t.nzt - 3);
+    if (l >= 0 && l < 3 && i >= t.xls && i < t.xls + t.nx && j >= t.yls && j < t.yls + t.ny) {
+      const int ih = (i - 2 - AWP_NGSL) * 3 + 2 + AWP_NGSL;
+      const int jh = (j - 2 - AWP_NGSL) * 3 + 3 + AWP_NGSL;
+      return awp_tex_index_base(ih - (2 + AWP_NGSL), jh - (2 + AWP_NGSL), t.f_ny, t.f_nzt,
+                                1 + 3 * l);
+    }
+  }
+  return awp_tex_index_base(i - t.xls, j - t.yls, t.ny, t.nzt, k - AWP_ALIGN);
 }
 
 // Status codes are the AWP_OK / AWP_ERR_* values of include/awp_b200.h.

@@ -168,3 +168,33 @@ def random_small(nx=24, ny=20, nz=32, h=100.0, dt=0.004, steps=20, seed=7, nvar=
                   npc=0, nve=1, ifault=ifault, nst=nst, read_step=nst, socalq=1)
     return Scenario("random_small", params, media, pos, data, steps,
                     f"random {nx}x{ny}x{nz} nvar={nvar} q={q} ifault={ifault}")
+
+
+def dm_small(nxc=10, nyc=8, nzs=(36, 24), h_coarse=150.0, dt=0.004, steps=12, q=True, seed=31,
+             nsrc=1):
+    """A discontinuous mesh of len(nzs) blocks for parity tests: block p has
+    (3^(n-1-p) nxc) x (3^(n-1-p) nyc) x nzs[p] cells at h_coarse / 3^(n-1-p),
+    random media per block, point sources next to every interface.  Returns one
+    Scenario per block (params carry grid / ngrids, ND scaled like
+    pmcl3d.c:1026 does)."""
+    n = len(nzs)
+    out = []
+    for p in range(n):
+        f = 3 ** (n - 1 - p)
+        sub = random_small(nx=nxc * f, ny=nyc * f, nz=nzs[p], q=q, ifault=1, steps=steps,
+                           seed=seed + p, nsrc=nsrc if p == 0 else 1)
+        sub.params.update(dh=h_coarse / f, dt=dt, nd=2 * f, grid=p, ngrids=n)
+        # one source a few cells above each interface and one below it, so the
+        # wavefield crosses the interfaces in both directions within a few steps
+        nxp, nyp, nzp = sub.params["nx"], sub.params["ny"], sub.params["nz"]
+        pos = []
+        if p < n - 1:
+            pos.append([nxp // 2, nyp // 2, nzp - 4])  # 4 cells above the block's bottom
+        if p > 0:
+            pos.append([nxp // 2 + 1, nyp // 2, 4])    # 4 cells below the block's top
+        k = len(pos)
+        sub.src_pos = np.asarray(pos, np.int32).reshape(k, 3)
+        sub.src_data = sub.src_data[:1].repeat(k, 0)[:k]
+        sub.name = f"dm_small_{p}"
+        out.append(sub)
+    return out

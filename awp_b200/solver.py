@@ -40,7 +40,8 @@ def padded_shape(nx: int, ny: int, nz: int) -> tuple[int, int, int]:
 
 
 class Solver:
-    """One single-rank, single-grid simulation on the current CUDA device."""
+    """One single-rank, single-grid simulation on the current CUDA device
+    (or one block of a :class:`Mesh`, which owns it)."""
 
     def __init__(self, params: awp_params | None = None, stream: int | None = None, **kw):
         self.lib = _lib.load()
@@ -54,8 +55,23 @@ class Solver:
         check(self.lib.awp_padded_dims(self.ctx, dims), "awp_padded_dims")
         self.shape = tuple(int(d) for d in dims)
 
+    @classmethod
+    def _borrow(cls, lib, ctx, params, owner):
+        s = cls.__new__(cls)
+        s.lib = lib
+        s.params = params
+        s.ctx = ctx
+        s._owner = owner  # the Mesh destroys the context
+        dims = (c_longlong * 3)()
+        check(lib.awp_padded_dims(ctx, dims), "awp_padded_dims")
+        s.shape = tuple(int(d) for d in dims)
+        return s
+
     # -- lifetime ---------------------------------------------------------
     def close(self) -> None:
+        if getattr(self, "_owner", None) is not None:
+            self.ctx = None
+            return
         if getattr(self, "ctx", None):
             self.lib.awp_ctx_destroy(self.ctx)
             self.ctx = None
@@ -197,3 +213,44 @@ class Solver:
         b = c_longlong()
         check(self.lib.awp_device_bytes(self.ctx, byref(b)), "awp_device_bytes")
         return b.value
+
+
+class Mesh:
+    """A discontinuous mesh: blocks 0 (top, finest) .. n-1, each 3x coarser in
+    x and y than the one above.  ``grid(p)`` gives block p's Solver for
+    uploads and field access; ``step`` advances the whole mesh."""
+
+    def __init__(self, params_list):
+        self.lib = _lib.load()
+        n = len(params_list)
+        arr = (awp_params * n)(*params_list)
+        m = c_void_p()
+        check(self.lib.awp_mesh_create(arr, n, byref(m)), "awp_mesh_create")
+        self.mesh = m
+        self.grids = []
+        for p in range(n):
+            ctx = c_void_p()
+            check(self.lib.awp_mesh_grid(self.mesh, p, byref(ctx)), "awp_mesh_grid")
+            self.grids.append(Solver._borrow(self.lib, ctx, params_list[p], self))
+
+    def grid(self, p: int) -> Solver:
+        return self.grids[p]
+
+    def step(self, n: int = 1) -> None:
+        check(self.lib.awp_mesh_step(self.mesh, int(n)), "awp_mesh_step")
+
+    def synchronize(self) -> None:
+        check(self.lib.awp_mesh_synchronize(self.mesh), "awp_mesh_synchronize")
+
+    def close(self) -> None:
+        if getattr(self, "mesh", None):
+            for g in self.grids:
+                g.ctx = None
+            self.lib.awp_mesh_destroy(self.mesh)
+            self.mesh = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

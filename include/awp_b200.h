@@ -71,6 +71,8 @@ typedef struct awp_params {
   int ifault;        /* -I         1 = point moment-rate source, 5 = kinematic    */
   int nst;           /* -N         source time samples                            */
   int read_step;     /* -R/-Q      samples held per source (IFAULT 1: >= nst)      */
+  int grid;          /*            block of a discontinuous mesh, 0 = top (finest)  */
+  int ngrids;        /* -G         blocks of the mesh (1 = a single grid)          */
 } awp_params;
 
 /* Fill *p with pmcl3d's defaults (command.c:71-136). */
@@ -166,6 +168,29 @@ int awp_input_read(const char* path, long long hdr[8], char* file, int filecap, 
 int awp_point_coefs(const char* path, int grid_type, int nxt, int nyt, int nzt, float h,
                     long long cap, int* count, int* indices, int* ix, int* iy, int* iz,
                     float* lx, float* ly, float* lz);
+
+/* ------------------------------------------------------------------------ */
+/* Discontinuous mesh (DM): a vertical stack of grids, grid 0 on top, each   */
+/* block 3x coarser in x and y than the one above (pmcl3d.c:370-378).        */
+/* ------------------------------------------------------------------------ */
+typedef struct awp_mesh awp_mesh;
+/* grids[p] describes block p (params.grid = p, params.ngrids = ngrids; NX, NY,
+ * DH, ND already scaled per block as pmcl3d does: NX*3^(ngrids-1-p), ...).
+ * Every block shares one stream. */
+int awp_mesh_create(const awp_params* grids, int ngrids, awp_mesh** out);
+int awp_mesh_destroy(awp_mesh* mesh);
+/* The context of block p, for its uploads (media, sources, plasticity) and
+ * field access.  awp_step on it is refused; step the mesh instead. */
+int awp_mesh_grid(awp_mesh* mesh, int p, awp_ctx** ctx);
+/* Advance the whole mesh (pmcl3d.c:1628-2490 with ngrids > 1): velocity of
+ * every block; the 2nd-order interface update dvelc2 (kernel.cu:2289-2343);
+ * coarse-to-fine interpolation intp3d (kernel.cu:2359-2561) and fine-to-coarse
+ * window average swap3 (kernel.cu:3032-3217); stress of every block; dstrqc2
+ * (kernel.cu:2564-2767); sources; intp3d and swap3 again; plasticity; the
+ * free-surface images of block 0.  The first call applies checkmesh
+ * (mesh.c:1404-1443) to the media of every coarser block. */
+int awp_mesh_step(awp_mesh* mesh, int nsteps);
+int awp_mesh_synchronize(awp_mesh* mesh);
 
 /* Advance nsteps time steps (pmcl3d.c:1628-2487 order: velocity, stress +
  * attenuation, SOURCEFILE and INSRC sources, plasticity, free-surface stress

@@ -250,3 +250,36 @@ int ref_point_coefs(int grid_type, int nxt, int nyt, int nzt, float h, int *indi
   free(x); free(y); free(z); free(idx);
   return (int)len;
 }
+
+/* checkmesh / checkmesh_ww (mesh.c:1404-1478) on flat padded arrays: the
+ * coarse grid "l" takes the fine grid "h"'s values at its top three levels. */
+int checkmesh(int nxtl, int nytl, int nztl, int nxth, int nyth, int nzth, Grid3D varl,
+              Grid3D varh, int pl, int ph, char *varname);
+int checkmesh_ww(int nxtl, int nytl, int nztl, int nxth, int nyth, int nzth, Grid3Dww varl,
+                 Grid3Dww varh, int pl, int ph, char *varname);
+int ref_checkmesh(int nxtl, int nytl, int nztl, int nxth, int nyth, int nzth, float *varl,
+                  const float *varh) {
+  int nxl = nxtl + 4 + ngsl2, nyl = nytl + 4 + ngsl2, nzl = nztl + 2 * align;
+  int nxh = nxth + 4 + ngsl2, nyh = nyth + 4 + ngsl2, nzh = nzth + 2 * align;
+  Grid3D l = Alloc3D(nxl, nyl, nzl), h = Alloc3D(nxh, nyh, nzh);
+  memcpy(&l[0][0][0], varl, sizeof(float) * (size_t)nxl * nyl * nzl);
+  memcpy(&h[0][0][0], varh, sizeof(float) * (size_t)nxh * nyh * nzh);
+  int c = checkmesh(nxtl, nytl, nztl, nxth, nyth, nzth, l, h, 1, 0, "var");
+  memcpy(varl, &l[0][0][0], sizeof(float) * (size_t)nxl * nyl * nzl);
+  free(l);
+  free(h);
+  return c;
+}
+int ref_checkmesh_ww(int nxtl, int nytl, int nztl, int nxth, int nyth, int nzth, int *varl,
+                     const int *varh) {
+  int nxl = nxtl + 4 + ngsl2, nyl = nytl + 4 + ngsl2, nzl = nztl + 2 * align;
+  int nxh = nxth + 4 + ngsl2, nyh = nyth + 4 + ngsl2, nzh = nzth + 2 * align;
+  Grid3Dww l = Alloc3Dww(nxl, nyl, nzl), h = Alloc3Dww(nxh, nyh, nzh);
+  memcpy(&l[0][0][0], varl, sizeof(int) * (size_t)nxl * nyl * nzl);
+  memcpy(&h[0][0][0], varh, sizeof(int) * (size_t)nxh * nyh * nzh);
+  int c = checkmesh_ww(nxtl, nytl, nztl, nxth, nyth, nzth, l, h, 1, 0, "ww");
+  memcpy(varl, &l[0][0][0], sizeof(int) * (size_t)nxl * nyl * nzl);
+  free(l);
+  free(h);
+  return c;
+}

@@ -51,6 +51,8 @@ class RefHost:
         lib.ref_inicrj.argtypes = [c_float] + [c_int] * 8 + [_F] * 3
         lib.ref_hoek_brown.argtypes = [c_float] * 5 + [c_int, _F, _F]
         lib.ref_rotation_matrix.argtypes = [_F, _F, _F, _F]
+        lib.ref_checkmesh.argtypes = [c_int] * 6 + [_F, _F]
+        lib.ref_checkmesh_ww.argtypes = [c_int] * 6 + [_I, _I]
         lib.ref_input_read.argtypes = [ctypes.c_char_p, POINTER(ctypes.c_longlong),
                                        ctypes.c_char_p, c_int]
         lib.ref_input_data.argtypes = [_F, _F, _F, _I]
@@ -120,6 +122,14 @@ class RefHost:
         return phi.value, cohes.value
 
 
+    def checkmesh(self, lo, hi, nl, nh):
+        """checkmesh (mesh.c:1404-1443): lo (coarse, padded) corrected in place
+        from hi (fine) at the coarse grid's top three levels; nl/nh = (nx, ny, nz)."""
+        if lo.dtype == np.int32:
+            return self.lib.ref_checkmesh_ww(*nl, *nh, lo.ctypes.data_as(_I),
+                                             np.ascontiguousarray(hi).ctypes.data_as(_I))
+        return self.lib.ref_checkmesh(*nl, *nh, fptr(lo), fptr(np.ascontiguousarray(hi)))
+
     def rotation_matrix(self, strike, dip):
         """rotation_matrix (mesh.c:1370-1401): Rz, RzT from strike/dip in degrees."""
         st = np.ascontiguousarray(strike, np.float32)
@@ -170,6 +180,127 @@ class RefHost:
         return dict(indices=idx[:cnt], ix=ix[:cnt], iy=iy[:cnt], iz=iz[:cnt],
                     lx=lx[:cnt * nb].reshape(cnt, nb), ly=ly[:cnt * nb].reshape(cnt, nb),
                     lz=lz[:cnt * nb].reshape(cnt, nb))
+
+
+def mesh_setup(scns, host: RefHost | None = None):
+    """Per-block set-up of a discontinuous mesh at one rank from the
+    reference's host code: inimesh per block, then checkmesh of every coarser
+    block's media against the block above (pmcl3d.c:879-901), init_texture per
+    block and checkmesh of the texture arrays (pmcl3d.c:1049-1059), inicrj with
+    the bottom sponge on the lowest block only (pmcl3d.c:1014-1033)."""
+    host = host or RefHost()
+    setups = []
+    for p, scn in enumerate(scns):
+        st = model_setup(scn, host)
+        q = scn.params
+        n = q["ngrids"]
+        dx, dy, dz = host.inicrj(q.get("arbc", 0.92), q["nx"], q["ny"], q["nz"], q["nd"],
+                                 1 if p == n - 1 else 0, q.get("npc", 0))
+        st.update(dcrjx=dx, dcrjy=dy, dcrjz=dz)
+        setups.append(st)
+    for p in range(1, len(scns)):
+        nl = tuple(scns[p].params[k] for k in ("nx", "ny", "nz"))
+        nh = tuple(scns[p - 1].params[k] for k in ("nx", "ny", "nz"))
+        for k in ("d1", "mu", "lam", "qp", "qs"):
+            host.checkmesh(setups[p]["media"][k], setups[p - 1]["media"][k], nl, nh)
+        for k in ("vx1", "vx2", "wwo", "ww"):
+            host.checkmesh(setups[p][k], setups[p - 1][k], nl, nh)
+    return setups
+
+
+class RefMeshSim:
+    """The reference CUDA kernels on a discontinuous mesh, driven in pmcl3d's
+    single-rank order with ngrids > 1 (pmcl3d.c:1628-2490): dvelcx per block,
+    dvelc2, intp3d, swap3 (swap-area exchanges are no-ops at one rank), dstrqc
+    per block, dstrqc2, sources, intp3d, swap3, fstr on block 0."""
+
+    def __init__(self, scns, setups, path=None):
+        import torch
+        self.torch = torch
+        self.n = len(scns)
+        self.sims = [RefGpuSim(s, st, path=path, defer_consts=True)
+                     for s, st in zip(scns, setups)]
+        lib = self.sims[0].lib
+        self.lib = lib
+        V = c_void_p
+        lib.dvelc2_H.argtypes = [V] * 13 + [c_int, c_int, V, c_int]
+        lib.dstrqc2_H.argtypes = [V] * 22 + [c_int, c_int, V] + [V] * 5 + [c_int] * 5
+        lib.intp3d_H.argtypes = [V] * 18 + [c_int, c_int, c_int, V, c_int]
+        lib.swap_H.argtypes = [V] * 18 + [c_int, c_int] + [V] * 4 + [c_int, V, c_int]
+        DH = np.array([s.params["dh"] for s in scns], np.float32)
+        nxt = np.array([s.params["nx"] for s in scns], np.int32)
+        nyt = np.array([s.params["ny"] for s in scns], np.int32)
+        nzt = np.array([s.params["nz"] for s in scns], np.int32)
+        z9 = np.zeros(9, np.float32)
+        lib.SetDeviceConstValue(fptr(DH), c_float(scns[0].params["dt"]), nxt.ctypes.data_as(_I),
+                                nyt.ctypes.data_as(_I), nzt.ctypes.data_as(_I), self.n,
+                                c_float(0.0), c_float(0.0), fptr(z9), fptr(z9))
+        # zeroed swap-area buffers (never read at one rank, pmcl3d.c:1434-1508)
+        self.zbuf = torch.zeros(1 << 16, device="cuda")
+        for p, sim in enumerate(self.sims):
+            sim.grid = p
+            sim.ngrids = self.n
+            # the initial sample goes into every block with sources (pmcl3d.c:1175-1187)
+            if sim.p["ifault"] == 1 and sim.npsrc:
+                sim._addsrc(1)
+        torch.cuda.synchronize()
+
+    def _fields(self, sim, order):
+        return [c_void_p(sim.f[k].data_ptr()) for k in order]
+
+    def _interfaces(self):
+        V9 = ["u1", "v1", "w1", "xx", "yy", "zz", "xy", "xz", "yz"]
+        S9 = ["xx", "yy", "zz", "xy", "xz", "yz", "u1", "v1", "w1"]
+        for p in range(1, self.n):
+            lo, hi = self.sims[p], self.sims[p - 1]
+            self.lib.intp3d_H(*self._fields(lo, V9), *self._fields(hi, V9), lo.nx, lo.ny, 0,
+                              None, p)
+        zb = c_void_p(self.zbuf.data_ptr())
+        for p in range(self.n - 1):
+            lo, hi = self.sims[p + 1], self.sims[p]
+            self.lib.swap_H(*self._fields(lo, S9), *self._fields(hi, S9), lo.nx, lo.ny,
+                            zb, zb, zb, zb, 0, None, p)
+
+    def step(self, n=1):
+        lib = self.lib
+        for _ in range(n):
+            for sim in self.sims:
+                sim.cur += 1
+                sim.velocity()
+            for p in range(self.n - 1):
+                sim = self.sims[p]
+                f = sim.f
+                P = sim.ptr
+                lib.dvelc2_H(P(f["u1"]), P(f["v1"]), P(f["w1"]), P(f["xx"]), P(f["yy"]),
+                             P(f["zz"]), P(f["xy"]), P(f["xz"]), P(f["yz"]), P(sim.dcrjx),
+                             P(sim.dcrjy), P(sim.dcrjz), P(f["d1"]), sim.nx, sim.ny, None, p)
+            self._interfaces()
+            for sim in self.sims:
+                sim.stress_all()
+            for p in range(self.n - 1):
+                sim = self.sims[p]
+                f = sim.f
+                P = sim.ptr
+                xls, xre, yls, yre = 2 + NGSL, sim.nx + NGSL + 1, 2 + NGSL, sim.ny + NGSL + 1
+                lib.dstrqc2_H(*[P(f[k]) for k in ("xx", "yy", "zz", "xy", "xz", "yz", "r1", "r2",
+                                                  "r3", "r4", "r5", "r6", "u1", "v1", "w1",
+                                                  "lam", "mu", "qp", "qs")],
+                              P(sim.dcrjx), P(sim.dcrjy), P(sim.dcrjz), sim.nx, sim.ny, None,
+                              P(sim.coeff), P(sim.vx1), P(sim.vx2), P(sim.ww), P(sim.wwo),
+                              xls, xre, yls, yre, p)
+            for sim in self.sims:
+                sim.sources()
+            self._interfaces()
+            sim0 = self.sims[0]
+            nx, ny = sim0.nx, sim0.ny
+            P = sim0.ptr
+            f = sim0.f
+            lib.fstr_H(P(f["zz"]), P(f["xz"]), P(f["yz"]), None, 2 + NGSL, nx + NGSL + 1,
+                       2 + NGSL, ny + NGSL + 1)
+        self.torch.cuda.synchronize()
+
+    def field(self, p, name):
+        return self.sims[p].field(name)
 
 
 class RefPoints:
@@ -319,8 +450,9 @@ class RefGpuSim:
     FIELDS = ["u1", "v1", "w1", "xx", "yy", "zz", "xy", "xz", "yz",
               "r1", "r2", "r3", "r4", "r5", "r6"]
 
-    def __init__(self, scn, setup, path=None):
+    def __init__(self, scn, setup, path=None, defer_consts=False):
         import torch
+        self.grid, self.ngrids = 0, 1
         path = path or os.path.join(REF_DIR, "libawpref.so")
         if not os.path.exists(path):
             raise FileNotFoundError(f"{path} missing: run `make -C oracle ref`")
@@ -382,9 +514,10 @@ class RefGpuSim:
             self.f.update(sigma2=T(pl["sigma2"]), cohes=T(pl["cohes"]), phi=T(pl["phi"]))
             self.f["yldfac"] = torch.ones(shp, dtype=torch.float32, device=dev)
         self.f["neta"] = torch.zeros(shp, dtype=torch.float32, device=dev)
-        lib.SetDeviceConstValue(fptr(DH), c_float(p["dt"]), nxt.ctypes.data_as(_I),
-                                nyt.ctypes.data_as(_I), nzt.ctypes.data_as(_I), 1,
-                                c_float(fmajor), c_float(fminor), fptr(Rz), fptr(RzT))
+        if not defer_consts:
+            lib.SetDeviceConstValue(fptr(DH), c_float(p["dt"]), nxt.ctypes.data_as(_I),
+                                    nyt.ctypes.data_as(_I), nzt.ctypes.data_as(_I), 1,
+                                    c_float(fmajor), c_float(fminor), fptr(Rz), fptr(RzT))
         fz = np.zeros(20, np.float64)
         lib.SetDeviceFilterParameters(0, fz.ctypes.data_as(POINTER(c_double)),
                                       fz.ctypes.data_as(POINTER(c_double)))
@@ -396,7 +529,7 @@ class RefGpuSim:
         # pmcl3d.c:2246-2247)
         self.after_stress = []
         self.after_step = []
-        if p["ifault"] == 1 and self.npsrc:
+        if p["ifault"] == 1 and self.npsrc and not defer_consts:
             # initial sample added on the host before the copy (pmcl3d.c:1175-1187)
             self._addsrc(1)
         torch.cuda.synchronize()
@@ -410,7 +543,7 @@ class RefGpuSim:
         self.lib.addsrc_H(i, self.stride, 3, self.ptr(self.psrc), self.npsrc, None,
                           *[self.ptr(t) for t in s],
                           self.ptr(f["xx"]), self.ptr(f["yy"]), self.ptr(f["zz"]),
-                          self.ptr(f["xy"]), self.ptr(f["yz"]), self.ptr(f["xz"]), 0)
+                          self.ptr(f["xy"]), self.ptr(f["yz"]), self.ptr(f["xz"]), self.grid)
 
     def _stress(self, s_i, e_i, s_j, e_j):
         f = self.f
@@ -421,7 +554,7 @@ class RefGpuSim:
                           P(f["qp"]), P(self.coeff), P(f["qs"]), P(self.dcrjx), P(self.dcrjy),
                           P(self.dcrjz), self.ny, self.nz, None, P(self.lam_mu), P(self.vx1),
                           P(self.vx2), P(self.ww), P(self.wwo), self.nx, self.p.get("npc", 0),
-                          0, 0, s_i, e_i, s_j, e_j, 0)
+                          0, 0, s_i, e_i, s_j, e_j, self.grid)
 
     def _calc(self, s_i, e_i, s_j, e_j):
         f = self.f
@@ -429,7 +562,7 @@ class RefGpuSim:
         self.lib.drprecpc_calc_H_opt(P(f["xx"]), P(f["yy"]), P(f["zz"]), P(f["xy"]), P(f["xz"]),
                                      P(f["yz"]), P(f["mu"]), P(f["d1"]), P(f["sigma2"]),
                                      P(f["yldfac"]), P(f["cohes"]), P(f["phi"]), P(f["neta"]),
-                                     self.nz, s_i, e_i, s_j, e_j, None, 0)
+                                     self.nz, s_i, e_i, s_j, e_j, None, self.grid)
 
     def margins(self):
         """yls2/yre2 of pmcl3d.c:621-627 at one rank (ylsp = yls, yrep = yre)."""
@@ -442,52 +575,78 @@ class RefGpuSim:
             yre2 -= 1
         return max(yls2, yls + NGSL + 2), min(yre2, yre - NGSL - 2)
 
+    def velocity(self):
+        f = self.f
+        P = self.ptr
+        self.lib.dvelcx_H_opt(P(f["u1"]), P(f["v1"]), P(f["w1"]), P(f["xx"]), P(f["yy"]),
+                              P(f["zz"]), P(f["xy"]), P(f["xz"]), P(f["yz"]), P(self.dcrjx),
+                              P(self.dcrjy), P(self.dcrjz), P(f["d1"]), self.ny, self.nz, None,
+                              2 + NGSL, self.nx + NGSL + 1, self.grid, self.ngrids)
+
+    def stress_all(self):
+        """Stress in pmcl3d's launch order (pmcl3d.c:1841-1924); NVE=3 leaves
+        the middle y band of xss2..xse2 for later (pmcl3d.c:1858-1879)."""
+        nx = self.nx
+        yls, yre = 2 + NGSL, self.ny + NGSL + 1
+        xls, xre = 2 + NGSL, nx + NGSL + 1
+        if self.nve == 3:
+            yls2, yre2 = self.margins()
+            self._stress(NGSL + 4, nx + NGSL - 1, yls, yls2 - 1)
+            self._stress(NGSL + 4, nx + NGSL - 1, yre2 + 1, yre)
+        else:
+            # dstrqc over xss2..xse2, then the xss1 and xss3 strips (pmcl3d.c:1845-1919)
+            self._stress(NGSL + 4, nx + NGSL - 1, yls, yre)
+        self._stress(xls, NGSL + 3, yls, yre)
+        self._stress(nx + NGSL, xre, yls, yre)
+        for hook in self.after_stress:
+            hook(self, self.cur)
+
+    def sources(self):
+        f = self.f
+        P = self.ptr
+        if self.p["ifault"] < 4 and self.cur < self.p["nst"]:
+            self.source_step += 1
+            if self.npsrc:
+                self._addsrc(self.source_step)
+        elif self.p["ifault"] == 5 and self.npsrc:
+            fdp = None if self.filt is None else P(self.filt)
+            self.lib.addkinsrc_H(self.cur, 3, P(self.psrc), self.npsrc, None, P(f["mu"]),
+                                 *[P(t) for t in self.src], P(f["xx"]), P(f["yy"]),
+                                 P(f["zz"]), P(f["xy"]), P(f["yz"]), P(f["xz"]),
+                                 P(self.mom), fdp, self.grid)
+
+    def plasticity(self):
+        f = self.f
+        P = self.ptr
+        nx = self.nx
+        xls, xre, yls, yre = 2 + NGSL, nx + NGSL + 1, 2 + NGSL, self.ny + NGSL + 1
+        yls2, yre2 = self.margins()
+        # pmcl3d.c:2110-2209 at one rank (xlsp = xls, ...)
+        self._calc(xls, xre, yls, yls + NGSL)
+        self._calc(xls, xre, yre - NGSL, yre)
+        self._stress(NGSL + 4, nx + NGSL - 1, yls2, yre2)
+        self._calc(xls, xls + NGSL, yls, yre)
+        self._calc(xre - NGSL, xre, yls, yre)
+        self._calc(xls + NGSL, xre - NGSL, yls + NGSL, yre - NGSL)
+        self.lib.drprecpc_app_H(P(f["xx"]), P(f["yy"]), P(f["zz"]), P(f["xy"]),
+                                P(f["xz"]), P(f["yz"]), P(f["mu"]), P(f["sigma2"]),
+                                P(f["yldfac"]), self.nz, xls, xre, yls, yre, None, self.grid)
+
     def step(self, n=1):
         f = self.f
         P = self.ptr
-        nx, ny, nz = self.nx, self.ny, self.nz
+        nx, ny = self.nx, self.ny
         xls, xre, yls, yre = 2 + NGSL, nx + NGSL + 1, 2 + NGSL, ny + NGSL + 1
         yls2, yre2 = self.margins()
         if self.nve == 3 and yre2 < yls2:
             raise ValueError("NVE=3 needs a non-empty middle stress region (pmcl3d.c:621-627)")
         for _ in range(n):
             self.cur += 1
-            self.lib.dvelcx_H_opt(P(f["u1"]), P(f["v1"]), P(f["w1"]), P(f["xx"]), P(f["yy"]),
-                                  P(f["zz"]), P(f["xy"]), P(f["xz"]), P(f["yz"]), P(self.dcrjx),
-                                  P(self.dcrjy), P(self.dcrjz), P(f["d1"]), ny, nz, None,
-                                  2 + NGSL, nx + NGSL + 1, 0, 1)
+            self.velocity()
+            self.stress_all()
+            self.sources()
             if self.nve == 3:
-                # NVE=3: the middle y band of xss2..xse2 waits until after the
-                # sources and the first yield-factor strips (pmcl3d.c:1858-1879, 2139-2148)
-                self._stress(NGSL + 4, nx + NGSL - 1, yls, yls2 - 1)
-                self._stress(NGSL + 4, nx + NGSL - 1, yre2 + 1, yre)
-            else:
-                # dstrqc over xss2..xse2, then the xss1 and xss3 strips (pmcl3d.c:1845-1919)
-                self._stress(NGSL + 4, nx + NGSL - 1, yls, yre)
-            self._stress(xls, NGSL + 3, yls, yre)
-            self._stress(nx + NGSL, xre, yls, yre)
-            for hook in self.after_stress:
-                hook(self, self.cur)
-            if self.p["ifault"] < 4 and self.cur < self.p["nst"]:
-                self.source_step += 1
-                self._addsrc(self.source_step)
-            elif self.p["ifault"] == 5 and self.npsrc:
-                fdp = None if self.filt is None else P(self.filt)
-                self.lib.addkinsrc_H(self.cur, 3, P(self.psrc), self.npsrc, None, P(f["mu"]),
-                                     *[P(t) for t in self.src], P(f["xx"]), P(f["yy"]),
-                                     P(f["zz"]), P(f["xy"]), P(f["yz"]), P(f["xz"]),
-                                     P(self.mom), fdp, 0)
-            if self.nve == 3:
-                # pmcl3d.c:2110-2209 at one rank (xlsp = xls, ...)
-                self._calc(xls, xre, yls, yls + NGSL)
-                self._calc(xls, xre, yre - NGSL, yre)
-                self._stress(NGSL + 4, nx + NGSL - 1, yls2, yre2)
-                self._calc(xls, xls + NGSL, yls, yre)
-                self._calc(xre - NGSL, xre, yls, yre)
-                self._calc(xls + NGSL, xre - NGSL, yls + NGSL, yre - NGSL)
-                self.lib.drprecpc_app_H(P(f["xx"]), P(f["yy"]), P(f["zz"]), P(f["xy"]),
-                                        P(f["xz"]), P(f["yz"]), P(f["mu"]), P(f["sigma2"]),
-                                        P(f["yldfac"]), nz, xls, xre, yls, yre, None, 0)
+                self.plasticity()
             self.lib.fstr_H(P(f["zz"]), P(f["xz"]), P(f["yz"]), None, xls, xre, yls, yre)
             for hook in self.after_step:
                 hook(self, self.cur)

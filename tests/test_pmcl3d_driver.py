@@ -116,8 +116,9 @@ def test_point_sets_match_library(tmp_path):
     os.makedirs(tmp_path / "lib", exist_ok=True)
     for d in (tmp_path, tmp_path / "lib"):
         pointfiles.write_input(str(d / "src.txt"), str(d / "msrc"), [[8 * h, 9 * h, -12 * h]],
-                               degree=3, gpu_buffer_size=2, cpu_buffer_size=3, steps=12)
-        rates = np.linspace(0, 1, 12 * 6, dtype=np.float32).reshape(1, 12, 6) * 1e14
+                               degree=3, gpu_buffer_size=2, cpu_buffer_size=3, steps=18)
+        # the ring is refilled at steps 0, 6 and 12: three blocks of 6 samples
+        rates = np.linspace(0, 1, 18 * 6, dtype=np.float32).reshape(1, 18, 6) * 1e14
         pointfiles.write_source_rates(str(d / "msrc"), rates)
         pointfiles.write_input(str(d / "recv.txt"), str(d / "rcv"),
                                [[5 * h, 6 * h, 0.0], [9.5 * h, 7 * h, -3 * h]], [1, 0],
