@@ -300,7 +300,7 @@ int phase_velocity(awp_ctx* c) {
   v.k1 = AWP_ALIGN + round_up(c->g.nzt, 4) - 1;
   if (c->p.grid > 0) v.k1 = std::min(v.k1, c->g.nzt + AWP_ALIGN - 3);
   v.dth = c->dth; v.c1 = c->c1; v.c2 = c->c2;
-  const bool tma = c->tma_ok && awp_tuning_get("tma") == 1;
+  const bool tma = c->tma_ok && awp_tuning_get("tma_vel") == 1;
   PhaseScope ps(c, 0);
   if (tma)
     CU_TRY(awp_launch_velocity_tma(v, c->vel_maps, awp_tuning_get("ichunk"), c->d_err,
@@ -312,7 +312,7 @@ int phase_velocity(awp_ctx* c) {
 }
 
 int phase_stress(awp_ctx* c) {
-  const bool tma = c->tma_ok && awp_tuning_get("tma") == 1;
+  const bool tma = c->tma_ok && awp_tuning_get("tma_str") == 1;
   PhaseScope ps(c, 1);
   StrArgs s = make_str_args(c);
   if (tma)

@@ -68,12 +68,16 @@ struct AwpTexture {
   int f_ny, f_nzt; // the finer grid's interior cells in y and z
 };
 
+// Parity index of init_texture's visit counters (mesh.c:1103-1137) for the
+// cell (di, dj, kk) relative to the loop start: itx = parity of di + 1, ity =
+// parity of di*ny + dj + 1, itz = parity of nzt*(di*ny + dj + 1) + kk.  Only
+// the low bits matter, so the products reduce to bit operations.
 AWP_HD int awp_tex_index_base(long long di, long long dj, int ny, int nzt, int kk) {
-  const long long ij = di * ny + dj;  // visits of the (i, j) loop before this one
-  const int itx = (int)((di + 1) & 1);
-  const int ity = (int)((ij + 1) & 1);
-  const int itz = (int)(((long long)nzt * (ij + 1) + kk) & 1);
-  return 4 * itx + 2 * ity + itz;
+  const int pdi = (int)(di & 1);
+  const int pij1 = ((pdi & ny) + (int)(dj & 1) + 1) & 1;  // parity of di*ny + dj + 1
+  const int itx = pdi ^ 1;
+  const int itz = ((nzt & pij1) + kk) & 1;
+  return 4 * itx + 2 * pij1 + itz;
 }
 
 // Index into the eight-entry tables (= ww - 1 of the reference).

@@ -27,7 +27,9 @@ namespace {
 // Launch shape (tuned on B200; adjustable through awp_set_tuning).  Tiles are
 // 32 k x 8 j for every kernel; the chunk of x planes and the kernel family vary.
 int g_ichunk = 32;
-int g_tma = 1;  // context API: TMA-pipelined kernels (1) or the read-only-path kernels (0)
+// context API kernel family per half-step: TMA-pipelined (1) or read-only path (0)
+int g_tma_vel = 0;
+int g_tma_str = 1;
 
 // ===========================================================================
 // Velocity (dvelcx_opt, kernel.cu:125-268)
@@ -875,13 +877,19 @@ cudaError_t awp_launch_stress(const StrArgs& a, bool elastic, cudaStream_t st) {
 
 int awp_tuning_set(const char* key, int value) {
   if (!strcmp(key, "ichunk") && value >= 4 && value <= 1024) { g_ichunk = value; return 0; }
-  if (!strcmp(key, "tma") && (value == 0 || value == 1)) { g_tma = value; return 0; }
+  if (value == 0 || value == 1) {
+    if (!strcmp(key, "tma")) { g_tma_vel = g_tma_str = value; return 0; }  // both half-steps
+    if (!strcmp(key, "tma_vel")) { g_tma_vel = value; return 0; }
+    if (!strcmp(key, "tma_str")) { g_tma_str = value; return 0; }
+  }
   return 1;
 }
 
 int awp_tuning_get(const char* key) {
   if (!strcmp(key, "ichunk")) return g_ichunk;
-  if (!strcmp(key, "tma")) return g_tma;
+  if (!strcmp(key, "tma")) return g_tma_vel == g_tma_str ? g_tma_str : -1;
+  if (!strcmp(key, "tma_vel")) return g_tma_vel;
+  if (!strcmp(key, "tma_str")) return g_tma_str;
   return -1;
 }
 

@@ -84,9 +84,26 @@ struct Ring {
   int depth, slot_floats, base;  // base = first plane of the march for this ring
   __device__ int slot(int p) const { return (p - base) % depth; }
   __device__ unsigned parity(int p) const { return ((p - base) / depth) & 1; }
-  __device__ float* at(int p) const { return buf + slot(p) * slot_floats; }
   __device__ uint64_t* b(int p) const { return bar + slot(p); }
 };
+
+// Slot and mbarrier phase of one plane in a ring: plane p of a march lives in
+// slot (p - base) % depth with phase ((p - base) / depth) & 1; the march
+// advances these incrementally instead of dividing.
+struct Cursor {
+  int slot;
+  unsigned phase;
+  __device__ void next(int depth) {
+    if (++slot == depth) {
+      slot = 0;
+      phase ^= 1u;
+    }
+  }
+};
+__device__ __forceinline__ int wrap_add(int s, int d, int depth) {
+  s += d;
+  return s >= depth ? s - depth : s;
+}
 
 // ===========================================================================
 // Stress + memory variables (dstrqc, kernel.cu:880-1197), same arithmetic as
@@ -116,23 +133,31 @@ __global__ void __launch_bounds__(NT, 2)
   ro.bar = bars + DH_ + DM_;
 
   // producer: one thread issues a plane's tiles and arms its barrier
+  // producer (thread 0): slot of the next plane each ring receives
+  int ish = 0, ism = 0, iso = 0;
   auto issue_halo = [&](int p) {
     if (p > ie + 2) return;
-    mbar_expect_tx(rh.b(p), 3 * HTILE * 4);
-    float* d = rh.at(p);
-    for (int f = 0; f < 3; ++f) tma_load3(d + f * HTILE, &tm.halo[f], rh.b(p), kb - 4, jb - 2, p);
+    uint64_t* b = rh.bar + ish;
+    mbar_expect_tx(b, 3 * HTILE * 4);
+    float* d = rh.buf + ish * rh.slot_floats;
+    for (int f = 0; f < 3; ++f) tma_load3(d + f * HTILE, &tm.halo[f], b, kb - 4, jb - 2, p);
+    ish = wrap_add(ish, 1, DH_);
   };
   auto issue_media = [&](int p) {
     if (p > ie + 1) return;
-    mbar_expect_tx(rm.b(p), NM * MTILE_B);
-    float* d = rm.at(p);
-    for (int f = 0; f < NM; ++f) tma_load3(d + f * MTILE, &tm.media[f], rm.b(p), kb - 4, jb - 1, p);
+    uint64_t* b = rm.bar + ism;
+    mbar_expect_tx(b, NM * MTILE_B);
+    float* d = rm.buf + ism * rm.slot_floats;
+    for (int f = 0; f < NM; ++f) tma_load3(d + f * MTILE, &tm.media[f], b, kb - 4, jb - 1, p);
+    ism = wrap_add(ism, 1, DM_);
   };
   auto issue_own = [&](int p) {
     if (p > ie) return;
-    mbar_expect_tx(ro.b(p), NO * OTILE * 4);
-    float* d = ro.at(p);
-    for (int f = 0; f < NO; ++f) tma_load3(d + f * OTILE, &tm.own[f], ro.b(p), kb, jb, p);
+    uint64_t* b = ro.bar + iso;
+    mbar_expect_tx(b, NO * OTILE * 4);
+    float* d = ro.buf + iso * ro.slot_floats;
+    for (int f = 0; f < NO; ++f) tma_load3(d + f * OTILE, &tm.own[f], b, kb, jb, p);
+    iso = wrap_add(iso, 1, DO_);
   };
 
   if (tid == 0) {
@@ -161,26 +186,38 @@ __global__ void __launch_bounds__(NT, 2)
   const int ooff = ty * TZ + tx;
   bool ok = true, aborted = false;
 
+  // consumers: the plane each ring waits for next (halo i+2, media i+1, own i)
+  // and the slots of the oldest planes read (halo i-2, media i)
+  Cursor wh{4, 0u}, wm{1, 0u}, wo{0, 0u};
+  int sh = 0, sm = 0;
   for (int i = ib; i <= ie; ++i) {
     // ---- wait for the planes this step reads for the first time ------------
     if (i == ib) {
-      for (int p = ib - 2; p <= ib + 2 && ok; ++p) ok = mbar_wait(rh.b(p), rh.parity(p));
-      if (ok) ok = mbar_wait(rm.b(ib), rm.parity(ib));
-    } else {
-      ok = mbar_wait(rh.b(i + 2), rh.parity(i + 2));
+      for (int q = 0; q < 4 && ok; ++q) ok = mbar_wait(rh.bar + q, 0u);  // planes ib-2..ib+1
+      if (ok) ok = mbar_wait(rm.bar, 0u);                                  // plane ib
     }
-    if (ok) ok = mbar_wait(rm.b(i + 1), rm.parity(i + 1));
-    if (ok) ok = mbar_wait(ro.b(i), ro.parity(i));
+    if (ok) ok = mbar_wait(rh.bar + wh.slot, wh.phase);
+    if (ok) ok = mbar_wait(rm.bar + wm.slot, wm.phase);
+    if (ok) ok = mbar_wait(ro.bar + wo.slot, wo.phase);
+    // one barrier per plane: it also tells the producer that every thread is
+    // done with the previous step's oldest planes, whose slots it refills
     if (__syncthreads_or(!ok)) {
       aborted = true;
       break;
     }
+    if (tid == 0 && i > ib) {
+      issue_halo(nh++);
+      issue_media(nm++);
+      issue_own(no++);
+    }
+    const int sh1 = wrap_add(sh, 1, DH_), sh2 = wrap_add(sh, 2, DH_), sh3 = wrap_add(sh, 3, DH_),
+              sh4 = wrap_add(sh, 4, DH_), sm1 = wrap_add(sm, 1, DM_);
 
-    const float* Hm2 = rh.at(i - 2) + hoff;
-    const float* Hm1 = rh.at(i - 1) + hoff;
-    const float* H0 = rh.at(i) + hoff;
-    const float* Hp1 = rh.at(i + 1) + hoff;
-    const float* Hp2 = rh.at(i + 2) + hoff;
+    const float* Hm2 = rh.buf + sh * rh.slot_floats + hoff;
+    const float* Hm1 = rh.buf + sh1 * rh.slot_floats + hoff;
+    const float* H0 = rh.buf + sh2 * rh.slot_floats + hoff;
+    const float* Hp1 = rh.buf + sh3 * rh.slot_floats + hoff;
+    const float* Hp2 = rh.buf + sh4 * rh.slot_floats + hoff;
     // field f of a halo plane: + f * HTILE; neighbour (dj, dk): + dj * HX + dk
     const float u_m1 = Hm1[0], u_0 = H0[0], u_p1 = Hp1[0], u_p2 = Hp2[0];
     const float v_m2 = Hm2[HTILE], v_m1 = Hm1[HTILE], v_0 = H0[HTILE], v_p1 = Hp1[HTILE];
@@ -195,8 +232,8 @@ __global__ void __launch_bounds__(NT, 2)
                 w_jm1 = W0[-HX];
     float uk1 = U0[1], vk1 = V0[1], wk1 = W0[1], uk2 = U0[2], vk2 = V0[2];
 
-    const float* Mc = rm.at(i) + moff;
-    const float* Mn = rm.at(i + 1) + moff;
+    const float* Mc = rm.buf + sm * rm.slot_floats + moff;
+    const float* Mn = rm.buf + sm1 * rm.slot_floats + moff;
     // (j,k), (j-1,k), (j,k-1), (j-1,k-1) of a media tile
     auto m4 = [&](const float* m, int f, float& pa, float& pb, float& pc, float& pd) {
       const float* q = m + f * MTILE;
@@ -262,7 +299,7 @@ __global__ void __launch_bounds__(NT, 2)
     d[7] = awp_d4(c1, c2, vk1, v_0, vk2, v_km1);
     d[8] = awp_d4(c1, c2, w_jp1, w_0, w_jp2, w_jm1);
 
-    const float* O = ro.at(i) + ooff;
+    const float* O = ro.buf + wo.slot * ro.slot_floats + ooff;
     float sg[6], rr[6];
 #pragma unroll
     for (int q = 0; q < 6; ++q) sg[q] = O[q * OTILE];
@@ -280,13 +317,11 @@ __global__ void __launch_bounds__(NT, 2)
       }
     }
 
-    // ---- every thread is done with halo plane i-2, media plane i, own plane i
-    __syncthreads();
-    if (tid == 0) {
-      issue_halo(nh++);
-      issue_media(nm++);
-      issue_own(no++);
-    }
+    wh.next(DH_);
+    wm.next(DM_);
+    wo.next(DO_);
+    sh = sh1;
+    sm = sm1;
   }
   if (aborted) {
     if (tid == 0) {
@@ -328,22 +363,30 @@ __global__ void __launch_bounds__(NT, 2)
   rm.bar = bars + DH_;
   ro.bar = bars + DH_ + DM_;
 
+  // producer (thread 0): slot of the next plane each ring receives
+  int ish = 0, ism = 0, iso = 0;
   auto issue_halo = [&](int p) {
     if (p > ie + 2) return;
-    mbar_expect_tx(rh.b(p), 6 * HTILE * 4);
-    float* d = rh.at(p);
-    for (int f = 0; f < 6; ++f) tma_load3(d + f * HTILE, &tm.halo[f], rh.b(p), kb - 4, jb - 2, p);
+    uint64_t* b = rh.bar + ish;
+    mbar_expect_tx(b, 6 * HTILE * 4);
+    float* d = rh.buf + ish * rh.slot_floats;
+    for (int f = 0; f < 6; ++f) tma_load3(d + f * HTILE, &tm.halo[f], b, kb - 4, jb - 2, p);
+    ish = wrap_add(ish, 1, DH_);
   };
   auto issue_media = [&](int p) {
     if (p > ie + 1) return;
-    mbar_expect_tx(rm.b(p), MTILE_B);
-    tma_load3(rm.at(p), &tm.media[0], rm.b(p), kb - 4, jb - 1, p);
+    uint64_t* b = rm.bar + ism;
+    mbar_expect_tx(b, MTILE_B);
+    tma_load3(rm.buf + ism * rm.slot_floats, &tm.media[0], b, kb - 4, jb - 1, p);
+    ism = wrap_add(ism, 1, DM_);
   };
   auto issue_own = [&](int p) {
     if (p > ie) return;
-    mbar_expect_tx(ro.b(p), 3 * OTILE * 4);
-    float* d = ro.at(p);
-    for (int f = 0; f < 3; ++f) tma_load3(d + f * OTILE, &tm.own[f], ro.b(p), kb, jb, p);
+    uint64_t* b = ro.bar + iso;
+    mbar_expect_tx(b, 3 * OTILE * 4);
+    float* d = ro.buf + iso * ro.slot_floats;
+    for (int f = 0; f < 3; ++f) tma_load3(d + f * OTILE, &tm.own[f], b, kb, jb, p);
+    iso = wrap_add(iso, 1, DO_);
   };
 
   if (tid == 0) {
@@ -368,26 +411,39 @@ __global__ void __launch_bounds__(NT, 2)
   const int ooff = ty * TZ + tx;
   bool ok = true, aborted = false;
 
+  // consumers: the plane each ring waits for next (halo i+2, media i+1, own i)
+  // and the slots of the oldest planes read (halo i-2, media i)
+  Cursor wh{4, 0u}, wm{1, 0u}, wo{0, 0u};
+  int sh = 0, sm = 0;
   for (int i = ib; i <= ie; ++i) {
+    // ---- wait for the planes this step reads for the first time ------------
     if (i == ib) {
-      for (int p = ib - 2; p <= ib + 2 && ok; ++p) ok = mbar_wait(rh.b(p), rh.parity(p));
-      if (ok) ok = mbar_wait(rm.b(ib), rm.parity(ib));
-    } else {
-      ok = mbar_wait(rh.b(i + 2), rh.parity(i + 2));
+      for (int q = 0; q < 4 && ok; ++q) ok = mbar_wait(rh.bar + q, 0u);  // planes ib-2..ib+1
+      if (ok) ok = mbar_wait(rm.bar, 0u);                                  // plane ib
     }
-    if (ok) ok = mbar_wait(rm.b(i + 1), rm.parity(i + 1));
-    if (ok) ok = mbar_wait(ro.b(i), ro.parity(i));
+    if (ok) ok = mbar_wait(rh.bar + wh.slot, wh.phase);
+    if (ok) ok = mbar_wait(rm.bar + wm.slot, wm.phase);
+    if (ok) ok = mbar_wait(ro.bar + wo.slot, wo.phase);
+    // one barrier per plane: it also tells the producer that every thread is
+    // done with the previous step's oldest planes, whose slots it refills
     if (__syncthreads_or(!ok)) {
       aborted = true;
       break;
     }
+    if (tid == 0 && i > ib) {
+      issue_halo(nh++);
+      issue_media(nm++);
+      issue_own(no++);
+    }
+    const int sh1 = wrap_add(sh, 1, DH_), sh2 = wrap_add(sh, 2, DH_), sh3 = wrap_add(sh, 3, DH_),
+              sh4 = wrap_add(sh, 4, DH_), sm1 = wrap_add(sm, 1, DM_);
 
     // halo fields: 0 xx, 1 yy, 2 zz, 3 xy, 4 xz, 5 yz
-    const float* Hm2 = rh.at(i - 2) + hoff;
-    const float* Hm1 = rh.at(i - 1) + hoff;
-    const float* H0 = rh.at(i) + hoff;
-    const float* Hp1 = rh.at(i + 1) + hoff;
-    const float* Hp2 = rh.at(i + 2) + hoff;
+    const float* Hm2 = rh.buf + sh * rh.slot_floats + hoff;
+    const float* Hm1 = rh.buf + sh1 * rh.slot_floats + hoff;
+    const float* H0 = rh.buf + sh2 * rh.slot_floats + hoff;
+    const float* Hp1 = rh.buf + sh3 * rh.slot_floats + hoff;
+    const float* Hp2 = rh.buf + sh4 * rh.slot_floats + hoff;
     const float xx_m2 = Hm2[0], xx_m1 = Hm1[0], xx_0 = H0[0], xx_p1 = Hp1[0];
     const float xy_m1 = Hm1[3 * HTILE], xy_0 = H0[3 * HTILE], xy_p1 = Hp1[3 * HTILE],
                 xy_p2 = Hp2[3 * HTILE];
@@ -400,8 +456,8 @@ __global__ void __launch_bounds__(NT, 2)
     const float* YZ = H0 + 5 * HTILE;
     const float yz_0 = YZ[0];
 
-    const float* Dc = rm.at(i) + moff;
-    const float* Dn = rm.at(i + 1) + moff;
+    const float* Dc = rm.buf + sm * rm.slot_floats + moff;
+    const float* Dn = rm.buf + sm1 * rm.slot_floats + moff;
     const float d_0 = Dc[0], d_0j = Dc[-MX], d_0k = Dc[-1], d_0jk = Dc[-MX - 1];
     const float d_p = Dn[0], d_pj = Dn[-MX], d_pk = Dn[-1];
 
@@ -410,7 +466,7 @@ __global__ void __launch_bounds__(NT, 2)
     const float fd3 = awp_vel_factor(dth, d_0, d_p, d_0j, d_pj);
     const float dcrj = LDG(a.dcrjx + i) * dcy * dcz;
 
-    const float* O = ro.at(i) + ooff;
+    const float* O = ro.buf + wo.slot * ro.slot_floats + ooff;
     const float u = awp_vel_update(O[0], fd1, c1, c2, xx_0 - xx_m1, xx_p1 - xx_m2,
                                    xy_0 - XY[-HX], XY[HX] - XY[-2 * HX], xz_0 - XZ[-1],
                                    XZ[1] - XZ[-2], dcrj);
@@ -426,12 +482,11 @@ __global__ void __launch_bounds__(NT, 2)
       a.v1[o] = v;
       a.w1[o] = w;
     }
-    __syncthreads();
-    if (tid == 0) {
-      issue_halo(nh++);
-      issue_media(nm++);
-      issue_own(no++);
-    }
+    wh.next(DH_);
+    wm.next(DM_);
+    wo.next(DO_);
+    sh = sh1;
+    sm = sm1;
   }
   if (aborted) {
     if (tid == 0) {

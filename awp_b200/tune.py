@@ -15,6 +15,7 @@ CANDIDATES = {
     "tma": (1, 0),
     "ichunk": (16, 32, 64),
 }
+KEYS = ("tma_vel", "tma_str", "ichunk")
 
 
 def set_tuning(lib, key: str, value: int) -> None:
@@ -23,12 +24,13 @@ def set_tuning(lib, key: str, value: int) -> None:
 
 
 def get_tuning(lib) -> dict:
-    return {k: lib.awp_get_tuning(k.encode()) for k in CANDIDATES}
+    return {k: lib.awp_get_tuning(k.encode()) for k in KEYS}
 
 
 def autotune(solver, steps: int = 3) -> dict:
-    """Try every (kernel family, ichunk) on `solver` (advancing it) and install
-    the fastest.  Returns the timing table."""
+    """Time every (kernel family, ichunk) on `solver` (advancing it), then
+    install the fastest family per half-step and the ichunk that minimises
+    their sum.  Returns the choice and the timing table."""
     lib = solver.lib
     table = []
     solver.profile_phases(True)
@@ -44,7 +46,16 @@ def autotune(solver, steps: int = 3) -> dict:
                       "velocity_ms": t["velocity"][0] / max(t["velocity"][1], 1),
                       "stress_ms": t["stress"][0] / max(t["stress"][1], 1)})
     solver.profile_phases(False)
-    best = min(table, key=lambda r: r["velocity_ms"] + r["stress_ms"])
-    for key in CANDIDATES:
-        set_tuning(lib, key, best[key])
-    return {"chosen": {k: best[k] for k in CANDIDATES}, "table": table}
+    best = None
+    for ich in CANDIDATES["ichunk"]:
+        rows = [r for r in table if r["ichunk"] == ich]
+        v = min(rows, key=lambda r: r["velocity_ms"])
+        s = min(rows, key=lambda r: r["stress_ms"])
+        cand = (v["velocity_ms"] + s["stress_ms"], ich, v["tma"], s["tma"])
+        if best is None or cand < best:
+            best = cand
+    _, ich, tv, ts = best
+    chosen = {"tma_vel": tv, "tma_str": ts, "ichunk": ich}
+    for k, v in chosen.items():
+        set_tuning(lib, k, v)
+    return {"chosen": chosen, "table": table}

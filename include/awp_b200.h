@@ -251,8 +251,10 @@ int awp_check_finite_noalloc(const float* const* fields, int nfields, long long 
 int awp_profile_phases(awp_ctx* ctx, int enable);
 int awp_phase_times(awp_ctx* ctx, double ms[AWP_NPHASES], long long launches[AWP_NPHASES]);
 /* Launch-shape tuning of the stencil kernels (process-wide): key "ichunk"
- * (x planes marched per CTA, 4..1024) and "tma" (1: the context API runs the
- * TMA-pipelined kernels, 0: the read-only-path kernels; results are identical).  Returns AWP_OK or AWP_ERR_ARG; awp_get_tuning returns the value
+ * (x planes marched per CTA, 4..1024), "tma_vel" / "tma_str" (1: the context
+ * API runs the TMA-pipelined velocity / stress kernel, 0: the read-only-path
+ * one; results are bit-identical) and "tma" (sets both; reads -1 when they
+ * differ).  Returns AWP_OK or AWP_ERR_ARG; awp_get_tuning returns the value
  * or -1 for an unknown key. */
 int awp_set_tuning(const char* key, int value);
 int awp_get_tuning(const char* key);

@@ -27,8 +27,9 @@ def test_tuning_is_bitwise_neutral(q):
     scn = scenarios.random_small(nx=41, ny=37, nz=68, q=q, steps=6, seed=5)
     base = None
     try:
-        for tma, ich in itertools.product((1, 0), (16, 32, 64)):
-            tune.set_tuning(lib, "tma", tma)
+        for tv, ts, ich in itertools.product((1, 0), (1, 0), (16, 64)):
+            tune.set_tuning(lib, "tma_vel", tv)
+            tune.set_tuning(lib, "tma_str", ts)
             tune.set_tuning(lib, "ichunk", ich)
             out = run(scn, 6)
             if base is None:
@@ -36,7 +37,7 @@ def test_tuning_is_bitwise_neutral(q):
                 continue
             for f in out:
                 assert np.array_equal(out[f].view(np.uint32), base[f].view(np.uint32)), \
-                    (f, tma, ich)
+                    (f, tv, ts, ich)
     finally:
         for k, v in saved.items():
             tune.set_tuning(lib, k, v)
