@@ -115,6 +115,7 @@ def load() -> ctypes.CDLL:
     _sig(lib, "awp_receivers_init", c_int, [_P, c_char_p, c_longlong])
     _sig(lib, "awp_receivers_count", c_int, [_P, _I])
     _sig(lib, "awp_sourcefile_init", c_int, [_P, c_char_p])
+    _sig(lib, "awp_topo_metrics", c_int, [c_char_p, c_int, c_int, c_int, c_float, _F])
     _sig(lib, "awp_input_read", c_int,
          [c_char_p, POINTER(c_longlong), c_char_p, c_int, _F, _F, _F, _I, c_longlong])
     _sig(lib, "awp_point_coefs", c_int,

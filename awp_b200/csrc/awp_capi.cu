@@ -19,6 +19,7 @@
 #include "awp_pointsets.h"
 #include "awp_points.h"
 #include "awp_tma.cuh"
+#include "awp_topo.h"
 
 namespace {
 
@@ -1182,6 +1183,22 @@ int awp_mesh_synchronize(awp_mesh* m) {
     if (st) return st;
   }
   return AWP_OK;
+}
+
+int awp_topo_metrics(const char* path, int nx, int ny, int nz, float h, float* out) {
+  if (!path || !out || nx < 1 || ny < 1 || nz < 12) return AWP_ERR_ARG;
+  awp::TopoMetrics m;
+  awp::topo_init_metrics(&m, nx, ny, nz, h);
+  const int e = awp::topo_read_file(path, nx, ny, &m.f);
+  if (e) return e;
+  awp::topo_build_metrics(&m);
+  const size_t nf = m.f.size(), ng = m.g.size();
+  const std::vector<float>* fa[10] = {&m.f, &m.f_1, &m.f_2, &m.f_c, &m.f1_1,
+                                      &m.f1_2, &m.f1_c, &m.f2_1, &m.f2_2, &m.f2_c};
+  for (int q = 0; q < 10; ++q) memcpy(out + q * nf, fa[q]->data(), nf * sizeof(float));
+  const std::vector<float>* ga[4] = {&m.g, &m.g_c, &m.g3, &m.g3_c};
+  for (int q = 0; q < 4; ++q) memcpy(out + 10 * nf + q * ng, ga[q]->data(), ng * sizeof(float));
+  return 0;
 }
 
 int awp_check_finite(awp_ctx* c, int* ok) {

@@ -198,3 +198,29 @@ def dm_small(nxc=10, nyc=8, nzs=(36, 24), h_coarse=150.0, dt=0.004, steps=12, q=
         sub.name = f"dm_small_{p}"
         out.append(sub)
     return out
+
+
+def write_topography(path, nx, ny, h, amplitude=1000.0, width=5000.0, rough_rms=100.0,
+                     seed=4, padding=8):
+    """Topography file of the reference format (serial_reader.c:9-62): int32
+    nx, ny, padding, then float32 elevation (m) [nx + 2 padding][ny + 2 padding]
+    with y fastest.  A Gaussian hill at the centre plus seeded smooth
+    roughness (rms `rough_rms`)."""
+    rng = np.random.default_rng(seed)
+    gx = (np.arange(nx + 2 * padding) - padding) * h
+    gy = (np.arange(ny + 2 * padding) - padding) * h
+    X, Y = np.meshgrid(gx, gy, indexing="ij")
+    xc, yc = 0.5 * (nx - 1) * h, 0.5 * (ny - 1) * h
+    elev = amplitude * np.exp(-((X - xc) ** 2 + (Y - yc) ** 2) / (2.0 * width ** 2))
+    if rough_rms > 0:
+        noise = rng.standard_normal(X.shape)
+        # smooth with a 5-point box twice (fractal-like small-scale relief)
+        for _ in range(2):
+            noise = (noise + np.roll(noise, 1, 0) + np.roll(noise, -1, 0) +
+                     np.roll(noise, 1, 1) + np.roll(noise, -1, 1)) / 5.0
+        noise *= rough_rms / max(noise.std(), 1e-30)
+        elev = elev + noise
+    with open(path, "wb") as fh:
+        np.asarray([nx, ny, padding], np.int32).tofile(fh)
+        elev.astype(np.float32).tofile(fh)
+    return elev.astype(np.float32)

@@ -192,6 +192,14 @@ int awp_mesh_grid(awp_mesh* mesh, int p, awp_ctx** ctx);
 int awp_mesh_step(awp_mesh* mesh, int nsteps);
 int awp_mesh_synchronize(awp_mesh* mesh);
 
+/* Host-only helper (no context, no GPU): the metric arrays of a topography
+ * file (INTOPO) for an nx x ny x nz grid of spacing h, as topo_init_metrics /
+ * topo_init_geometry / topo_build compute them (src/topography/topography.c:
+ * 238-262).  out = the ten f arrays f, f_1, f_2, f_c, f1_1, f1_2, f1_c, f2_1,
+ * f2_2, f2_c ((nx+20) x (ny+84) each), then g, g_c, g3, g3_c (nz+64 each).
+ * Returns 0 or the reference's error code (101 unreadable, 902 sizes). */
+int awp_topo_metrics(const char* path, int nx, int ny, int nz, float h, float* out);
+
 /* Advance nsteps time steps (pmcl3d.c:1628-2487 order: velocity, stress +
  * attenuation, SOURCEFILE and INSRC sources, plasticity, free-surface stress
  * images, receivers).  Asynchronous with respect to the host except when a

@@ -283,3 +283,66 @@ int ref_checkmesh_ww(int nxtl, int nytl, int nztl, int nxth, int nyth, int nzth,
   free(h);
   return c;
 }
+
+/* ------------------------------------------------------------------------ */
+/* Topography metrics: the reference's reader, geometry and metric code      */
+/* (readers/serial_reader.c, geometry/geometry.c, metrics/metrics.c,         */
+/* metrics/kernel.c) in the order of topo_init_metrics / topo_init_geometry / */
+/* topo_build (topography.c:238-262), one rank.  The f_grid_t / g_grid_t set- */
+/* up restates metrics_init_f / metrics_init_g (metrics.c:14-37, 194-211)     */
+/* with zero-filled host arrays and no device copies.                         */
+/* out: f, f_1, f_2, f_c, f1_1, f1_2, f1_c, f2_1, f2_2, f2_c (each mx*my),     */
+/* then g, g_c, g3, g3_c (each nz + 2 align).  Returns the reader's status.   */
+/* ------------------------------------------------------------------------ */
+#include <topography/metrics/metrics.h>
+#include <topography/geometry/geometry.h>
+#include <topography/readers/serial_reader.h>
+
+int ref_topo_metrics(const char *path, int nx, int ny, int nz, float h, float *out) {
+  f_grid_t f;
+  memset(&f, 0, sizeof(f));
+  f.size[0] = nx; f.size[1] = ny; f.size[2] = 1;
+  f.mem[0] = nx + 4 + 2 * ngsl; f.mem[1] = ny + 4 + 2 * ngsl + 2 * align; f.mem[2] = 1;
+  f.bounds_x[0] = -ngsl; f.bounds_x[1] = nx + ngsl;
+  f.bounds_y[0] = -ngsl; f.bounds_y[1] = ny + ngsl;
+  f.bounds_stress_x[0] = -ngsl / 2; f.bounds_stress_x[1] = nx + ngsl / 2;
+  f.bounds_stress_y[0] = -ngsl / 2; f.bounds_stress_y[1] = ny + ngsl / 2;
+  f.offset[0] = 2 + ngsl; f.offset[1] = 2 + ngsl + align; f.offset[2] = 0;
+  f.hi = 1.0 / h;
+  f.line = f.mem[2];
+  f.slice = f.mem[1] * f.mem[2];
+  size_t nf = (size_t)f.mem[0] * f.mem[1];
+  prec **farr[10] = {&f.f, &f.f_1, &f.f_2, &f.f_c, &f.f1_1, &f.f1_2, &f.f1_c, &f.f2_1,
+                     &f.f2_2, &f.f2_c};
+  for (int q = 0; q < 10; ++q) *farr[q] = calloc(nf, sizeof(prec));
+  g_grid_t g;
+  memset(&g, 0, sizeof(g));
+  g.size = nz; g.mem = nz + 2 * align; g.bounds_z[0] = 0; g.bounds_z[1] = nz;
+  g.offset = align; g.hi = 1.0 / h; g.line = g.mem;
+  prec **garr[4] = {&g.g, &g.g_c, &g.g3, &g.g3_c};
+  for (int q = 0; q < 4; ++q) *garr[q] = calloc(g.mem, sizeof(prec));
+  int coord[2] = {0, 0};
+  int err = topo_read_serial(path, 0, 1, 1, coord, nx, ny, 0, &f.f);
+  if (err) return err;
+  geom_no_grid_stretching(&g);
+  int3_t size = {.x = nx, .y = ny, .z = nz};
+  int3_t shift = {.x = 1, .y = 0, .z = 0};
+  int3_t c3 = {.x = 0, .y = 0, .z = 0};
+  int3_t b1 = {.x = 0, .y = 0, .z = 0};
+  int3_t b2 = {.x = 0, .y = 0, .z = 1};
+  grid3_t tg = grid_init_metric_grid(size, shift, c3, b1, b2, h);
+  geom_custom(&f, tg, 1, 1, f.f);
+  metrics_interpolate_f(&f);
+  metrics_differentiate_f(&f);
+  metrics_interpolate_g(&g);
+  metrics_differentiate_g(&g);
+  for (int q = 0; q < 10; ++q) {
+    memcpy(out + q * nf, *farr[q], nf * sizeof(float));
+    free(*farr[q]);
+  }
+  for (int q = 0; q < 4; ++q) {
+    memcpy(out + 10 * nf + (size_t)q * g.mem, *garr[q], g.mem * sizeof(float));
+    free(*garr[q]);
+  }
+  return 0;
+}
