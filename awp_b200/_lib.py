@@ -116,11 +116,15 @@ def load() -> ctypes.CDLL:
     _sig(lib, "awp_receivers_count", c_int, [_P, _I])
     _sig(lib, "awp_sourcefile_init", c_int, [_P, c_char_p])
     _sig(lib, "awp_topo_metrics", c_int, [c_char_p, c_int, c_int, c_int, c_float, _F])
+    _sig(lib, "awp_topography_init", c_int, [_P, c_char_p])
     _sig(lib, "awp_input_read", c_int,
          [c_char_p, POINTER(c_longlong), c_char_p, c_int, _F, _F, _F, _I, c_longlong])
     _sig(lib, "awp_point_coefs", c_int,
          [c_char_p, c_int, c_int, c_int, c_int, c_float, c_longlong, _I, _I, _I, _I, _I,
           _F, _F, _F])
+    _sig(lib, "awp_point_coefs_topo", c_int,
+         [c_char_p, c_char_p, c_int, c_int, c_int, c_int, c_float, c_longlong, _I, _I, _I, _I,
+          _I, _F, _F, _F])
     _sig(lib, "awp_device_bytes", c_int, [_P, POINTER(c_longlong)])
     _sig(lib, "awp_profile_phases", c_int, [_P, c_int])
     _sig(lib, "awp_phase_times", c_int, [_P, POINTER(c_double), POINTER(c_longlong)])

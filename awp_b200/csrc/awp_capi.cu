@@ -20,6 +20,7 @@
 #include "awp_points.h"
 #include "awp_tma.cuh"
 #include "awp_topo.h"
+#include "awp_topo_kern.cuh"
 
 namespace {
 
@@ -90,6 +91,10 @@ struct awp_ctx {
   bool initial_src_done = false;
   RecvState* recv = nullptr;     // RECVFILE receivers
   SrcFileState* srcf = nullptr;  // SOURCEFILE moment-tensor sources
+  // curvilinear topography of the top grid (topo_t of the reference)
+  awp::TopoMetrics* topo = nullptr;  // host metrics (point-set set-up)
+  float* d_topo = nullptr;           // f arrays then g arrays, one allocation
+  TopoArgs targs{};                  // device pointers and constants
   long long dev_bytes = 0;
   long long launches = 0;
   // phase timing
@@ -284,6 +289,26 @@ int phase_begin(awp_ctx* c) {
   return AWP_OK;
 }
 
+// Kernel arguments of the curvilinear half-steps: the wavefield, media and
+// texture of the context plus the metric arrays of awp_topography_init.
+TopoArgs topo_args(awp_ctx* c) {
+  TopoArgs a = c->targs;
+  float** f = c->f;
+  a.u1 = f[AWP_U1]; a.v1 = f[AWP_V1]; a.w1 = f[AWP_W1];
+  a.xx = f[AWP_XX]; a.yy = f[AWP_YY]; a.zz = f[AWP_ZZ];
+  a.xy = f[AWP_XY]; a.xz = f[AWP_XZ]; a.yz = f[AWP_YZ];
+  a.r1 = f[AWP_R1]; a.r2 = f[AWP_R2]; a.r3 = f[AWP_R3];
+  a.r4 = f[AWP_R4]; a.r5 = f[AWP_R5]; a.r6 = f[AWP_R6];
+  a.d1 = f[AWP_D1]; a.lam = f[AWP_LAM]; a.mu = f[AWP_MU]; a.qp = f[AWP_QP]; a.qs = f[AWP_QS];
+  a.dcrjx = c->dcrjx; a.dcrjy = c->dcrjy; a.dcrjz = c->dcrjz;
+  a.tex = c->tex;
+  memcpy(a.coeff, c->coeff, sizeof(a.coeff));
+  a.qthr = c->qthr;
+  a.slice = c->g.slice; a.yline = c->g.yline;
+  a.nx = c->g.nxt; a.ny = c->g.nyt; a.nz = c->g.nzt;
+  return a;
+}
+
 int phase_velocity(awp_ctx* c) {
   float** f = c->f;
   VelArgs v;
@@ -301,6 +326,12 @@ int phase_velocity(awp_ctx* c) {
   v.k1 = AWP_ALIGN + round_up(c->g.nzt, 4) - 1;
   if (c->p.grid > 0) v.k1 = std::min(v.k1, c->g.nzt + AWP_ALIGN - 3);
   v.dth = c->dth; v.c1 = c->c1; v.c2 = c->c2;
+  if (c->topo) {  // topo_velocity_*_H replace dvelc[xy] on the top grid (pmcl3d.c:1661-1698)
+    PhaseScope ps(c, 0);
+    CU_TRY(awp_launch_topo_velocity(topo_args(c), c->stream));
+    c->launches++;
+    return AWP_OK;
+  }
   const bool tma = c->tma_ok && awp_tuning_get("tma_vel") == 1;
   PhaseScope ps(c, 0);
   if (tma)
@@ -313,6 +344,12 @@ int phase_velocity(awp_ctx* c) {
 }
 
 int phase_stress(awp_ctx* c) {
+  if (c->topo) {  // topo_stress_*_H replace dstrqc on the top grid (pmcl3d.c:1843-1924)
+    PhaseScope ps(c, 1);
+    CU_TRY(awp_launch_topo_stress(topo_args(c), c->elastic, c->stream));
+    c->launches++;
+    return AWP_OK;
+  }
   const bool tma = c->tma_ok && awp_tuning_get("tma_str") == 1;
   PhaseScope ps(c, 1);
   StrArgs s = make_str_args(c);
@@ -557,6 +594,8 @@ int awp_ctx_destroy(awp_ctx* c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   awp_recv_destroy(c->recv);
   awp_srcf_destroy(c->srcf);
+  delete c->topo;
+  cudaFree(c->d_topo);
   for (int i = 0; i < AWP_NFIELDS; ++i) cudaFree(c->f[i]);
   cudaFree(c->dcrjx); cudaFree(c->dcrjy); cudaFree(c->dcrjz); cudaFree(c->lam_mu);
   cudaFree(c->d_cell_pos); cudaFree(c->d_cell_first); cudaFree(c->d_order);
@@ -1018,7 +1057,8 @@ int awp_receivers_init(awp_ctx* c, const char* recvfile, long long nt) {
   if (nt < 1) return set_error(AWP_ERR_ARG, "nt must be >= 1");
   if (c->recv) return set_error(AWP_ERR_STATE, "receivers already initialised");
   RecvState* r = nullptr;
-  const int e = awp_recv_create(recvfile, nt, c->g, c->p.dh, &r, g_errmsg, sizeof(g_errmsg));
+  const int e = awp_recv_create(recvfile, nt, c->g, c->p.dh, c->topo, &r, g_errmsg,
+                                sizeof(g_errmsg));
   if (e) return e < 0 ? AWP_ERR_CUDA : AWP_ERR_IO;
   c->recv = r;
   // the reference records the state before the first step (pmcl3d.c:1603-1605)
@@ -1038,7 +1078,7 @@ int awp_sourcefile_init(awp_ctx* c, const char* sourcefile) {
   if (!c || !sourcefile) return set_error(AWP_ERR_ARG, "null argument");
   if (c->srcf) return set_error(AWP_ERR_STATE, "SOURCEFILE already initialised");
   SrcFileState* s = nullptr;
-  const int e = awp_srcf_create(sourcefile, c->g, c->p.dh, c->p.dt, &s, g_errmsg,
+  const int e = awp_srcf_create(sourcefile, c->g, c->p.dh, c->p.dt, c->topo, &s, g_errmsg,
                                 sizeof(g_errmsg));
   if (e) return e < 0 ? AWP_ERR_CUDA : AWP_ERR_IO;
   c->srcf = s;
@@ -1072,16 +1112,24 @@ int awp_input_read(const char* path, long long hdr[8], char* file, int filecap, 
   return 0;
 }
 
-int awp_point_coefs(const char* path, int grid_type, int nxt, int nyt, int nzt, float h,
-                    long long cap, int* count, int* indices, int* ix, int* iy, int* iz, float* lx,
-                    float* ly, float* lz) {
+static int point_coefs(const char* path, const char* intopo, int grid_type, int nxt, int nyt,
+                       int nzt, float h, long long cap, int* count, int* indices, int* ix,
+                       int* iy, int* iz, float* lx, float* ly, float* lz) {
   if (!path || !count || grid_type < 0 || grid_type > 8) return AWP_ERR_ARG;
   awp::InputFile in;
   int e = awp::read_input(path, &in);
   if (e) return e;
-  awp::BlockDesc b{nxt, nyt, nzt, h, 0};
+  awp::TopoMetrics m;
+  if (intopo) {
+    if (nzt < 12) return AWP_ERR_ARG;
+    awp::topo_init_metrics(&m, nxt, nyt, nzt, h);
+    e = awp::topo_read_file(intopo, nxt, nyt, &m.f);
+    if (e) return e;
+    awp::topo_build_metrics(&m);
+  }
+  awp::BlockDesc b{nxt, nyt, nzt, h, intopo ? 1 : 0};
   awp::PointSet ps;
-  e = awp::point_set_init(in, (awp::GridType)grid_type, &b, 1, &ps);
+  e = awp::point_set_init(in, (awp::GridType)grid_type, &b, 1, &ps, intopo ? &m : nullptr);
   if (e) return e;
   const awp::BlockInterp& bi = ps.block[0];
   *count = bi.num_query;
@@ -1098,6 +1146,21 @@ int awp_point_coefs(const char* path, int grid_type, int nxt, int nyt, int nzt, 
     }
   }
   return 0;
+}
+
+int awp_point_coefs(const char* path, int grid_type, int nxt, int nyt, int nzt, float h,
+                    long long cap, int* count, int* indices, int* ix, int* iy, int* iz, float* lx,
+                    float* ly, float* lz) {
+  return point_coefs(path, nullptr, grid_type, nxt, nyt, nzt, h, cap, count, indices, ix, iy, iz,
+                     lx, ly, lz);
+}
+
+int awp_point_coefs_topo(const char* path, const char* intopo, int grid_type, int nxt, int nyt,
+                         int nzt, float h, long long cap, int* count, int* indices, int* ix,
+                         int* iy, int* iz, float* lx, float* ly, float* lz) {
+  if (!intopo) return AWP_ERR_ARG;
+  return point_coefs(path, intopo, grid_type, nxt, nyt, nzt, h, cap, count, indices, ix, iy, iz,
+                     lx, ly, lz);
 }
 
 int awp_mesh_destroy(awp_mesh* m) {
@@ -1199,6 +1262,70 @@ int awp_topo_metrics(const char* path, int nx, int ny, int nz, float h, float* o
   const std::vector<float>* ga[4] = {&m.g, &m.g_c, &m.g3, &m.g3_c};
   for (int q = 0; q < 4; ++q) memcpy(out + 10 * nf + q * ng, ga[q]->data(), ng * sizeof(float));
   return 0;
+}
+
+int awp_topography_init(awp_ctx* c, const char* intopo) {
+  if (!c || !intopo) return set_error(AWP_ERR_ARG, "null argument");
+  if (c->topo) return set_error(AWP_ERR_STATE, "topography already initialised");
+  if (c->recv || c->srcf)
+    return set_error(AWP_ERR_STATE,
+                     "topography must be initialised before receivers and SOURCEFILE sources");
+  if (c->p.grid != 0)
+    return set_error(AWP_ERR_ARG, "topography belongs to the top grid (grid 0) only");
+  const int nx = c->g.nxt, ny = c->g.nyt, nz = c->g.nzt;
+  if (nz < 12) return set_error(AWP_ERR_ARG, "topography needs nzt >= 12 (got %d)", nz);
+  awp::TopoMetrics* m = new awp::TopoMetrics();
+  awp::topo_init_metrics(m, nx, ny, nz, c->p.dh);
+  const int e = awp::topo_read_file(intopo, nx, ny, &m->f);
+  if (e) {
+    delete m;
+    return set_error(e == 902 ? AWP_ERR_ARG : AWP_ERR_IO,
+                     e == 902 ? "%s: grid size or padding inconsistent with the context"
+                              : "%s: cannot read the topography file",
+                     intopo);
+  }
+  awp::topo_build_metrics(m);
+  const size_t nf = m->f.size(), ng = m->g.size();
+  float* d = nullptr;
+  if (ctx_alloc(c, (void**)&d, sizeof(float) * (10 * nf + 4 * ng))) {
+    delete m;
+    return AWP_ERR_NOMEM;
+  }
+  const std::vector<float>* fa[10] = {&m->f, &m->f_1, &m->f_2, &m->f_c, &m->f1_1,
+                                      &m->f1_2, &m->f1_c, &m->f2_1, &m->f2_2, &m->f2_c};
+  const std::vector<float>* ga[4] = {&m->g, &m->g_c, &m->g3, &m->g3_c};
+  cudaError_t ce = cudaSuccess;
+  for (int q = 0; q < 10 && ce == cudaSuccess; ++q)
+    ce = cudaMemcpy(d + q * nf, fa[q]->data(), nf * sizeof(float), cudaMemcpyHostToDevice);
+  for (int q = 0; q < 4 && ce == cudaSuccess; ++q)
+    ce = cudaMemcpy(d + 10 * nf + q * ng, ga[q]->data(), ng * sizeof(float),
+                    cudaMemcpyHostToDevice);
+  if (ce != cudaSuccess) {
+    cudaFree(d);
+    delete m;
+    return set_error(AWP_ERR_CUDA, "topography upload: %s", cudaGetErrorString(ce));
+  }
+  TopoArgs& t = c->targs;
+  t = TopoArgs{};
+  t.f = d; t.f_1 = d + nf; t.f_2 = d + 2 * nf; t.f_c = d + 3 * nf;
+  t.f1_1 = d + 4 * nf; t.f1_2 = d + 5 * nf; t.f1_c = d + 6 * nf;
+  t.f2_1 = d + 7 * nf; t.f2_2 = d + 8 * nf; t.f2_c = d + 9 * nf;
+  t.g = d + 10 * nf; t.g_c = d + 10 * nf + ng; t.g3 = d + 10 * nf + 2 * ng;
+  t.g3_c = d + 10 * nf + 3 * ng;
+  t.fld = m->ld;
+  // topo_init (topography.c:69) and topo_set_constants (stress_attenuation.cu:19-23)
+  const float h = c->p.dh, dt = c->p.dt;
+  t.nu = dt / h;
+  t.DT = t.nu * h;
+  t.dth = t.DT / h;
+  t.dh1 = (float)(1.0 / (double)h);
+  // stress window of a rank on every domain boundary: ngsl/2 cells in from
+  // each side (topo_set_stress_bounds_*, topography.c:379-420)
+  t.s_i = AWP_NGSL / 2; t.e_i = nx - AWP_NGSL / 2;
+  t.s_j = AWP_NGSL / 2; t.e_j = ny - AWP_NGSL / 2;
+  c->d_topo = d;
+  c->topo = m;
+  return AWP_OK;
 }
 
 int awp_check_finite(awp_ctx* c, int* ok) {

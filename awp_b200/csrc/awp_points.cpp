@@ -12,6 +12,7 @@
 #include <algorithm>
 
 #include "awp_common.h"
+#include "awp_topo.h"
 
 namespace awp {
 
@@ -304,7 +305,7 @@ int lagrange_coef(float* l, int* first, const float* x, int n, float query, int 
 }
 
 int point_set_init(const InputFile& in, GridType type, const BlockDesc* blocks, int ngrids,
-                   PointSet* out) {
+                   PointSet* out, const TopoMetrics* topo) {
   *out = PointSet();
   out->type = type;
   out->ngrids = ngrids;
@@ -360,24 +361,54 @@ int point_set_init(const InputFile& in, GridType type, const BlockDesc* blocks, 
   float overlap = 0.f, lower = 0.f;
   for (int j = 0; j < ngrids; ++j) {
     const CompGrid& g = cg[j];
-    // no topography metrics here: block height of a regular block
-    const float block_height = g.h * (g.size[2] - 1);
+    const bool curv = topo != nullptr && j == 0;
+    // the curvilinear block's height excludes its ghost point (source.c:268-273)
+    const float block_height = g.h * (g.size[2] - (curv ? 2 : 1));
     lower = lower - block_height + overlap;
     std::vector<float> qx, qy, qz;
     std::vector<int> ridx;
     for (size_t i = 0; i < len; ++i) {
       if (gown[i] != j) continue;
       const int src = out->indices[i];
-      float zz = z[src];
-      if (in.type[src] == 1) {
-        zz = block_height;  // surface coordinates (only in the top block)
-      } else if (in.type[src] == 0) {
-        zz = zz - lower;
-      }
       ridx.push_back((int)i);
       qx.push_back(x[src]);
       qy.push_back(y[src]);
-      qz.push_back(zz);
+      qz.push_back(z[src]);
+    }
+    if (curv && !ridx.empty()) {
+      // metrics_interpolate_f_point (metrics/metrics.c:171-204) on the
+      // topography grid with ngsl padding -- grid_node(), shift (1, 0, 0)
+      // (grid/shift.c:76-80) -- then the map to parameter space
+      CompGrid mg = comp_grid(blocks[0], GT_YZ, AWP_NGSL);
+      mg.shift[0] = 1;
+      std::vector<float> mx, my, mz;
+      fill_dir(mx, mg, 0);
+      fill_dir(my, mg, 1);
+      fill_dir(mz, mg, 2);
+      const int nb = in.degree + 1;
+      std::vector<float> lx(nb), ly(nb);
+      for (size_t q = 0; q < ridx.size(); ++q) {
+        int ix = 0, iy = 0;
+        lagrange_coef(lx.data(), &ix, mx.data(), mg.size[0], qx[q], in.degree);
+        lagrange_coef(ly.data(), &iy, my.data(), mg.size[1], qy[q], in.degree);
+        float fq = 0.0f;
+        for (int a = 0; a < nb; ++a)
+          for (int b = 0; b < nb; ++b)
+            fq += lx[a] * ly[b] * topo->f[(size_t)topo->fidx(ix + a - AWP_NGSL, iy + b - AWP_NGSL)];
+        const int src = out->indices[ridx[q]];
+        if (in.type[src] == 0)
+          qz[q] = (block_height + qz[q]) / fq;
+        else if (in.type[src] == 1)
+          qz[q] = mz[mg.size[2] - 2];
+      }
+    } else {
+      for (size_t q = 0; q < ridx.size(); ++q) {
+        const int src = out->indices[ridx[q]];
+        if (in.type[src] == 1)
+          qz[q] = block_height;  // surface coordinates (only in the top block)
+        else if (in.type[src] == 0)
+          qz[q] = qz[q] - lower;
+      }
     }
     overlap = (float)((double)g.h * kOverlap);
     if (ridx.empty()) continue;

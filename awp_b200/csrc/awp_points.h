@@ -88,9 +88,14 @@ struct BlockInterp {
   std::vector<float> lx, ly, lz;  // [num_query][num_basis]
 };
 
-// source_init_common (topography/sources/source.c:137-520) at one rank
-// without topography: which points lie in the domain (`indices`, into the
-// input), their grid block, and the interpolation on each block.
+// source_init_common (topography/sources/source.c:137-520) at one rank:
+// which points lie in the domain (`indices`, into the input), their grid
+// block, and the interpolation on each block.  With `topo` (the metrics of a
+// curvilinear top block, blocks[0].topography = 1) the vertical coordinate of
+// the top block's points is mapped to parameter space through the surface
+// function interpolated at the point (source.c:283-340):
+//   volume points  z' = (h (nz - 2) + z) / f(x, y),  surface points z' = h (nz - 2).
+struct TopoMetrics;
 struct PointSet {
   GridType type = GT_X;
   int ngrids = 0;
@@ -98,7 +103,7 @@ struct PointSet {
   BlockInterp block[10];           // per grid block
 };
 int point_set_init(const InputFile& in, GridType type, const BlockDesc* blocks, int ngrids,
-                   PointSet* out);
+                   PointSet* out, const TopoMetrics* topo = nullptr);
 
 // Ring-buffer schedule of buffers/buffer.c:44-95.
 struct RingSchedule {

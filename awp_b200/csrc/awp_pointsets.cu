@@ -24,6 +24,7 @@
 
 #include "awp_pointsets.h"
 #include "awp_points.h"
+#include "awp_topo.h"
 
 namespace {
 
@@ -97,13 +98,13 @@ int upload(T** d, const std::vector<T>& h, char* msg, size_t cap) {
   return 0;
 }
 
-awp::BlockDesc block_of(const AwpGeom& g, float h) {
+awp::BlockDesc block_of(const AwpGeom& g, float h, const awp::TopoMetrics* topo) {
   awp::BlockDesc b;
   b.nxt = g.nxt;
   b.nyt = g.nyt;
   b.nzt = g.nzt;
   b.h = h;
-  b.topography = 0;
+  b.topography = topo ? 1 : 0;
   return b;
 }
 
@@ -160,7 +161,8 @@ int awp_recv_length(const RecvState* r, int comp) {
   return (r && comp >= 0 && comp < 3) ? r->len[comp] : 0;
 }
 
-int awp_recv_create(const char* path, long long nt, const AwpGeom& g, float h, RecvState** out,
+int awp_recv_create(const char* path, long long nt, const AwpGeom& g, float h,
+                    const awp::TopoMetrics* topo, RecvState** out,
                     char* msg, size_t cap) {
   *out = nullptr;
   RecvState* r = new RecvState();
@@ -175,13 +177,13 @@ int awp_recv_create(const char* path, long long nt, const AwpGeom& g, float h, R
     return fail(msg, cap, awp::PE_PARSE_ARG,
                 "RECVFILE: degree 0..7, stride >= 1 and nonzero buffer sizes are required");
   }
-  const awp::BlockDesc b = block_of(g, h);
+  const awp::BlockDesc b = block_of(g, h, topo);
   const char* names[3] = {"x", "y", "z"};
   std::vector<int4> q;
   std::vector<float> l;
   r->nb = r->in.degree + 1;
   for (int c = 0; c < 3; ++c) {
-    e = awp::point_set_init(r->in, (awp::GridType)(awp::GT_X + c), &b, 1, &r->ps[c]);
+    e = awp::point_set_init(r->in, (awp::GridType)(awp::GT_X + c), &b, 1, &r->ps[c], topo);
     if (e) {
       awp_recv_destroy(r);
       return setup_error(e, "RECVFILE", msg, cap);
@@ -294,7 +296,8 @@ void awp_srcf_destroy(SrcFileState* s) {
   delete s;
 }
 
-int awp_srcf_create(const char* path, const AwpGeom& g, float h, float dt, SrcFileState** out,
+int awp_srcf_create(const char* path, const AwpGeom& g, float h, float dt,
+                    const awp::TopoMetrics* topo, SrcFileState** out,
                     char* msg, size_t cap) {
   *out = nullptr;
   SrcFileState* s = new SrcFileState();
@@ -309,13 +312,13 @@ int awp_srcf_create(const char* path, const AwpGeom& g, float h, float dt, SrcFi
     return fail(msg, cap, awp::PE_PARSE_ARG,
                 "SOURCEFILE: degree 0..7, stride >= 1 and nonzero buffer sizes are required");
   }
-  const awp::BlockDesc b = block_of(g, h);
+  const awp::BlockDesc b = block_of(g, h, topo);
   const char* names[6] = {"xx", "yy", "zz", "xy", "xz", "yz"};
   std::vector<long long> pos;
   std::vector<int> comp, first, src;
   std::vector<float> w;
   for (int c = 0; c < 6; ++c) {
-    e = awp::point_set_init(s->in, (awp::GridType)(awp::GT_XX + c), &b, 1, &s->ps[c]);
+    e = awp::point_set_init(s->in, (awp::GridType)(awp::GT_XX + c), &b, 1, &s->ps[c], topo);
     if (e) {
       awp_srcf_destroy(s);
       return setup_error(e, "SOURCEFILE", msg, cap);
@@ -331,10 +334,31 @@ int awp_srcf_create(const char* path, const AwpGeom& g, float h, float dt, SrcFi
       comp.push_back(c);
       first.push_back((int)w.size() + ca.first[n] - ca.first[0]);
     }
-    for (size_t n = 0; n < ca.w.size(); ++n) {
-      w.push_back(ca.w[n]);
-      src.push_back(s->off[c] + ca.src[n]);
+    // sources_add_curvilinear (sources.c:79-101, source.cu:65-100): each
+    // contribution is divided by the Jacobian f g of its cell, with the
+    // component's staggered f and vertical metric
+    const std::vector<float>* jf[6] = {nullptr};
+    const std::vector<float>* jg[6] = {nullptr};
+    if (topo) {
+      const std::vector<float>* F[6] = {&topo->f_c, &topo->f_c, &topo->f_c,
+                                        &topo->f,   &topo->f_1, &topo->f_2};
+      const std::vector<float>* G[6] = {&topo->g3_c, &topo->g3_c, &topo->g3_c,
+                                        &topo->g3_c, &topo->g3,   &topo->g3};
+      jf[c] = F[c];
+      jg[c] = G[c];
     }
+    for (size_t n = 0; n + 1 < ca.first.size(); ++n)
+      for (int m = ca.first[n]; m < ca.first[n + 1]; ++m) {
+        float wm = ca.w[m];
+        if (topo) {
+          const long long p = ca.cell_pos[n];
+          const long long ia = p / g.slice, jb = (p % g.slice) / g.yline, kk = p % g.yline;
+          const float J = (*jf[c])[(size_t)(ia * topo->ld + jb + AWP_ALIGN)] * (*jg[c])[(size_t)kk];
+          wm = wm * (float)(1.0 / (double)J);
+        }
+        w.push_back(wm);
+        src.push_back(s->off[c] + ca.src[m]);
+      }
   }
   first.push_back((int)w.size());
   s->ncell = (int)pos.size();

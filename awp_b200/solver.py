@@ -133,6 +133,11 @@ class Solver:
                                              c_float(fmajor), c_float(fminor),
                                              _fptr(st), _fptr(dp)), "awp_upload_plasticity")
 
+    def topography(self, intopo: str) -> None:
+        """Curvilinear topography of this (top) grid from an INTOPO elevation
+        file; call before receivers() and sourcefile()."""
+        check(self.lib.awp_topography_init(self.ctx, intopo.encode()), "awp_topography_init")
+
     def receivers(self, recvfile: str, nt: int) -> None:
         """RECVFILE receivers (ASCII v2); records the current step at once."""
         check(self.lib.awp_receivers_init(self.ctx, recvfile.encode(), int(nt)),

@@ -168,6 +168,11 @@ int awp_input_read(const char* path, long long hdr[8], char* file, int filecap, 
 int awp_point_coefs(const char* path, int grid_type, int nxt, int nyt, int nzt, float h,
                     long long cap, int* count, int* indices, int* ix, int* iy, int* iz,
                     float* lx, float* ly, float* lz);
+/* The same on the curvilinear top block of the topography file `intopo`
+ * (vertical coordinate mapped through the surface function, source.c:283-340). */
+int awp_point_coefs_topo(const char* path, const char* intopo, int grid_type, int nxt, int nyt,
+                         int nzt, float h, long long cap, int* count, int* indices, int* ix,
+                         int* iy, int* iz, float* lx, float* ly, float* lz);
 
 /* ------------------------------------------------------------------------ */
 /* Discontinuous mesh (DM): a vertical stack of grids, grid 0 on top, each   */
@@ -199,6 +204,22 @@ int awp_mesh_synchronize(awp_mesh* mesh);
  * f2_2, f2_c ((nx+20) x (ny+84) each), then g, g_c, g3, g3_c (nz+64 each).
  * Returns 0 or the reference's error code (101 unreadable, 902 sizes). */
 int awp_topo_metrics(const char* path, int nx, int ny, int nz, float h, float* out);
+
+/* Curvilinear topography of the top grid (INTOPO; replaces topo_init /
+ * topo_bind / topo_init_metrics / topo_init_grid / topo_init_geometry /
+ * topo_build / topo_set_constants, pmcl3d.c:1522-1550).  Reads the elevation
+ * file (int32 nx, ny, padding; float32 [nx+2 padding][ny+2 padding], y
+ * fastest), builds the metrics and from then on the context's velocity and
+ * stress half-steps are the curvilinear ones (topo_velocity_*_H,
+ * topo_stress_*_H: interior operators below the top six points, boundary
+ * closures on them, stress window ngsl/2 cells in from each side).  Receivers
+ * and SOURCEFILE sources initialised afterwards are placed through the
+ * surface function and the SOURCEFILE moments divided by the cell Jacobian
+ * (sources_add_curvilinear).  Only on grid 0, nzt >= 12, and before
+ * awp_receivers_init / awp_sourcefile_init (AWP_ERR_STATE otherwise).
+ * Returns AWP_ERR_IO for an unreadable file, AWP_ERR_ARG for sizes or padding
+ * that do not fit the context. */
+int awp_topography_init(awp_ctx* ctx, const char* intopo);
 
 /* Advance nsteps time steps (pmcl3d.c:1628-2487 order: velocity, stress +
  * attenuation, SOURCEFILE and INSRC sources, plasticity, free-surface stress

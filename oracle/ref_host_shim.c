@@ -202,9 +202,24 @@ void ref_input_data(float *x, float *y, float *z, int *type) {
  * dist_indices, grid_init_metric_grid, grid_data_init,
  * interp_lagrange1_coef); the few lines of glue restate source.c:193-205 and
  * 288-360.  Returns the number of owned points, or -err. */
+static int point_coefs(int grid_type, int nxt, int nyt, int nzt, float h, const float *ftopo,
+                       int *indices, int *ix, int *iy, int *iz, float *lx, float *ly,
+                       float *lz);
 int ref_point_coefs(int grid_type, int nxt, int nyt, int nzt, float h, int *indices,
                     int *ix, int *iy, int *iz, float *lx, float *ly, float *lz) {
-  grids_t grids = grids_init(nxt, nyt, nzt, 0, 0, 0, 0, h);
+  return point_coefs(grid_type, nxt, nyt, nzt, h, NULL, indices, ix, iy, iz, lx, ly, lz);
+}
+/* The curvilinear top block: ftopo = the normalised surface function (host
+ * layout of f_grid_t.f); the vertical map of source.c:268-340. */
+int ref_point_coefs_topo(int grid_type, int nxt, int nyt, int nzt, float h, const float *ftopo,
+                         int *indices, int *ix, int *iy, int *iz, float *lx, float *ly,
+                         float *lz) {
+  return point_coefs(grid_type, nxt, nyt, nzt, h, ftopo, indices, ix, iy, iz, lx, ly, lz);
+}
+static int point_coefs(int grid_type, int nxt, int nyt, int nzt, float h, const float *ftopo,
+                       int *indices, int *ix, int *iy, int *iz, float *lx, float *ly,
+                       float *lz) {
+  grids_t grids = grids_init(nxt, nyt, nzt, 0, 0, 0, ftopo != NULL, h);
   grid3_t grid = grids_select((enum grid_types)grid_type, &grids);
   size_t n = g_input.length;
   prec dm0 = 0;
@@ -224,7 +239,7 @@ int ref_point_coefs(int grid_type, int nxt, int nyt, int nzt, float h, int *indi
   size_t len = 0;
   int err = dist_indices(&idx, &len, x, y, n, grid);
   if (err) return -err;
-  prec block_height = grid.gridspacing * (grid.size.z - 1);
+  prec block_height = grid.gridspacing * (grid.size.z - (ftopo ? 2 : 1));
   prec lower = 0 - block_height + 0;
   grid3_t full = grid_init_metric_grid(grid.inner_size, grid.shift, grid.coordinate,
                                        grid.boundary1, grid.boundary2, grid.gridspacing);
@@ -232,10 +247,43 @@ int ref_point_coefs(int grid_type, int nxt, int nyt, int nzt, float h, int *indi
   grid_data_init(&xyz, full);
   int deg = g_input.degree, nb = deg + 1;
   prec *xloc = calloc(sizeof(prec), nb);
+  prec *fi = NULL, *z1 = NULL;
+  int zsize = 0;
+  if (ftopo) {
+    /* f_grid_t of metrics_init_f (metrics.c:14-33) on the caller's host f */
+    f_grid_t fg;
+    memset(&fg, 0, sizeof(fg));
+    fg.offset[0] = 2 + ngsl;
+    fg.offset[1] = 2 + ngsl + align;
+    fg.bounds_x[0] = -ngsl;
+    fg.bounds_y[0] = -ngsl;
+    fg.slice = (nyt + 4 + 2 * ngsl + 2 * align) * 1;
+    fg.f = (prec *)ftopo;
+    grid3_t mg = grid_init_metric_grid(grid.inner_size, grid_node(), grid.coordinate,
+                                       grid.boundary1, grid.boundary2, grid.gridspacing);
+    grid1_t xg = grid_grid1_x(mg), yg = grid_grid1_y(mg), zg = grid_grid1_z(mg);
+    prec *x1 = malloc(sizeof(prec) * xg.size), *y1 = malloc(sizeof(prec) * yg.size);
+    z1 = malloc(sizeof(prec) * zg.size);
+    zsize = zg.size;
+    grid_fill1(x1, xg);
+    grid_fill1(y1, yg);
+    grid_fill1(z1, zg);
+    prec *qx = malloc(sizeof(prec) * len), *qy = malloc(sizeof(prec) * len);
+    for (size_t q = 0; q < len; ++q) {
+      qx[q] = x[idx[q]];
+      qy[q] = y[idx[q]];
+    }
+    fi = malloc(sizeof(prec) * len);
+    metrics_interpolate_f_point(&fg, fi, fg.f, x1, y1, mg, qx, qy, (int)len, deg);
+    free(x1); free(y1); free(qx); free(qy);
+  }
   for (size_t q = 0; q < len; ++q) {
     int s = idx[q];
     prec zz = z[s];
-    if (g_input.type[s] == INPUT_VOLUME_COORD) zz = zz - lower;
+    if (ftopo) {
+      if (g_input.type[s] == INPUT_VOLUME_COORD) zz = (block_height + zz) / fi[q];
+      else if (g_input.type[s] == INPUT_SURFACE_COORD) zz = z1[zsize - 2];
+    } else if (g_input.type[s] == INPUT_VOLUME_COORD) zz = zz - lower;
     else if (g_input.type[s] == INPUT_SURFACE_COORD) zz = block_height;
     indices[q] = s;
     err = interp_lagrange1_coef(xloc, &lx[q * nb], &ix[q], xyz.x, grid_boundary_size(full).x,
@@ -246,6 +294,8 @@ int ref_point_coefs(int grid_type, int nxt, int nyt, int nzt, float h, int *indi
                                 zz, deg);
   }
   free(xloc);
+  free(fi);
+  free(z1);
   grid_data_free(&xyz);
   free(x); free(y); free(z); free(idx);
   return (int)len;

@@ -6,7 +6,7 @@
  * into oracle/_ref/libawpref_points.so by oracle/Makefile from the reference
  * sources where they lie.
  *
- * Set-up at one rank, one grid block, no topography: the reference's reader
+ * Set-up at one rank, one grid block (optionally the curvilinear top block): the reference's reader
  * (input_init), grids_init / grids_select, dist_indices, grid_init_metric_grid
  * and grid_data_init do the work; the glue restates source.c:193-205 and
  * 288-360 (offset by -h/2 in x, zero DM offsets, vertical mapping).
@@ -23,19 +23,24 @@
 #include <topography/grids.h>
 #include <topography/sources/source.cuh>
 #include <topography/sources/source.h>
+#include <topography/metrics/metrics.h>
+#include <grid/shift.h>
 
 typedef struct {
   cu_interp_t I;
   int length;
 } ref_pts_t;
 
-/* Returns a handle (NULL on failure); *count = owned points. */
-void *ref_pts_create(const char *path, int grid_type, int nxt, int nyt, int nzt, float h,
-                     int *count) {
+/* Returns a handle (NULL on failure); *count = owned points.  With `ftopo`
+ * (the normalised surface function of the topography metrics, host copy of
+ * f_grid_t.f) the block is curvilinear: closed top boundary and the vertical
+ * map of source.c:268-340 through metrics_interpolate_f_point. */
+static void *pts_create(const char *path, int grid_type, int nxt, int nyt, int nzt, float h,
+                        const float *ftopo, int *count) {
   input_t in;
   memset(&in, 0, sizeof(in));
   if (input_init(&in, path) != 0) return NULL;
-  grids_t grids = grids_init(nxt, nyt, nzt, 0, 0, 0, 0, h);
+  grids_t grids = grids_init(nxt, nyt, nzt, 0, 0, 0, ftopo != NULL, h);
   grid3_t grid = grids_select((enum grid_types)grid_type, &grids);
   size_t n = in.length;
   prec dm0 = 0;
@@ -52,7 +57,7 @@ void *ref_pts_create(const char *path, int grid_type, int nxt, int nyt, int nzt,
   int *idx = NULL;
   size_t len = 0;
   if (dist_indices(&idx, &len, x, y, n, grid) != 0 || len == 0) return NULL;
-  prec block_height = grid.gridspacing * (grid.size.z - 1);
+  prec block_height = grid.gridspacing * (grid.size.z - (ftopo ? 2 : 1));
   prec lower = 0 - block_height + 0;
   prec *qx = malloc(sizeof(prec) * len), *qy = malloc(sizeof(prec) * len),
        *qz = malloc(sizeof(prec) * len);
@@ -62,9 +67,33 @@ void *ref_pts_create(const char *path, int grid_type, int nxt, int nyt, int nzt,
     qx[q] = x[s];
     qy[q] = y[s];
     qz[q] = z[s];
-    if (in.type[s] == INPUT_VOLUME_COORD) qz[q] = qz[q] - lower;
-    else if (in.type[s] == INPUT_SURFACE_COORD) qz[q] = block_height;
+    if (!ftopo) {
+      if (in.type[s] == INPUT_VOLUME_COORD) qz[q] = qz[q] - lower;
+      else if (in.type[s] == INPUT_SURFACE_COORD) qz[q] = block_height;
+    }
     ridx[q] = (int)q;
+  }
+  if (ftopo) {
+    grid3_t mg = grid_init_metric_grid(grid.inner_size, grid_node(), grid.coordinate,
+                                       grid.boundary1, grid.boundary2, grid.gridspacing);
+    grid1_t xg = grid_grid1_x(mg), yg = grid_grid1_y(mg), zg = grid_grid1_z(mg);
+    prec *x1 = malloc(sizeof(prec) * xg.size), *y1 = malloc(sizeof(prec) * yg.size),
+         *z1 = malloc(sizeof(prec) * zg.size);
+    grid_fill1(x1, xg);
+    grid_fill1(y1, yg);
+    grid_fill1(z1, zg);
+    int size[3] = {nxt, nyt, nzt};
+    f_grid_t fg = metrics_init_f(size, h);
+    memcpy(fg.f, ftopo, sizeof(float) * fg.mem[0] * fg.mem[1]);
+    prec *fi = malloc(sizeof(prec) * len);
+    metrics_interpolate_f_point(&fg, fi, fg.f, x1, y1, mg, qx, qy, (int)len, in.degree);
+    for (size_t q = 0; q < len; ++q) {
+      int s = idx[q];
+      if (in.type[s] == INPUT_VOLUME_COORD) qz[q] = (block_height + qz[q]) / fi[q];
+      else if (in.type[s] == INPUT_SURFACE_COORD) qz[q] = z1[zg.size - 2];
+    }
+    metrics_free_f(&fg);
+    free(fi); free(x1); free(y1); free(z1);
   }
   grid3_t full = grid_init_metric_grid(grid.inner_size, grid.shift, grid.coordinate,
                                        grid.boundary1, grid.boundary2, grid.gridspacing);
@@ -86,6 +115,16 @@ void *ref_pts_create(const char *path, int grid_type, int nxt, int nyt, int nzt,
   return p;
 }
 
+void *ref_pts_create(const char *path, int grid_type, int nxt, int nyt, int nzt, float h,
+                     int *count) {
+  return pts_create(path, grid_type, nxt, nyt, nzt, h, NULL, count);
+}
+
+void *ref_pts_create_topo(const char *path, int grid_type, int nxt, int nyt, int nzt, float h,
+                          const float *ftopo, int *count) {
+  return pts_create(path, grid_type, nxt, nyt, nzt, h, ftopo, count);
+}
+
 /* cuinterp_interp_H: d_out[q] = sum l * d_in (the receiver gather). */
 void ref_pts_interp(void *h, float *d_out, const float *d_in) {
   ref_pts_t *p = (ref_pts_t *)h;
@@ -96,6 +135,13 @@ void ref_pts_interp(void *h, float *d_out, const float *d_in) {
 void ref_pts_srcadd(void *h, float *d_field, const float *d_values, float hh, float dt) {
   ref_pts_t *p = (ref_pts_t *)h;
   cusource_add_cartesian_H(&p->I, d_field, d_values, hh, dt);
+}
+
+/* cusource_add_curvilinear_H: as above, divided by the cell Jacobian f dg. */
+void ref_pts_srcadd_curv(void *h, float *d_field, const float *d_values, float hh, float dt,
+                         const float *d_f, int ny, const float *d_dg) {
+  ref_pts_t *p = (ref_pts_t *)h;
+  cusource_add_curvilinear_H(&p->I, d_field, d_values, hh, dt, d_f, ny, d_dg);
 }
 
 void ref_pts_destroy(void *h) {

@@ -159,9 +159,10 @@ class RefHost:
         h["file"] = fname.value.decode()
         return 0, h, x, y, z, t
 
-    def point_coefs(self, path, grid_type, nx, ny, nz, h):
+    def point_coefs(self, path, grid_type, nx, ny, nz, h, ftopo=None):
         """The interpolation set-up of source_init_common for one component,
-        built from the reference's own routines (see ref_host_shim.c)."""
+        built from the reference's own routines (see ref_host_shim.c); with
+        `ftopo` (the normalised surface function) on the curvilinear block."""
         err, hdr, *_ = self.input_read(path)
         assert err == 0, err
         n = hdr["length"]
@@ -174,8 +175,15 @@ class RefHost:
         ly = np.zeros(n * nb, np.float32)
         lz = np.zeros(n * nb, np.float32)
         I = lambda a: a.ctypes.data_as(_I)  # noqa: E731
-        cnt = self.lib.ref_point_coefs(grid_type, nx, ny, nz, h, I(idx), I(ix), I(iy), I(iz),
-                                       fptr(lx), fptr(ly), fptr(lz))
+        if ftopo is None:
+            cnt = self.lib.ref_point_coefs(grid_type, nx, ny, nz, h, I(idx), I(ix), I(iy), I(iz),
+                                           fptr(lx), fptr(ly), fptr(lz))
+        else:
+            f = np.ascontiguousarray(ftopo, np.float32)
+            self.lib.ref_point_coefs_topo.argtypes = [c_int, c_int, c_int, c_int, c_float, _F] + \
+                [_I] * 4 + [_F] * 3
+            cnt = self.lib.ref_point_coefs_topo(grid_type, nx, ny, nz, h, fptr(f), I(idx), I(ix),
+                                                I(iy), I(iz), fptr(lx), fptr(ly), fptr(lz))
         assert cnt >= 0, cnt
         return dict(indices=idx[:cnt], ix=ix[:cnt], iy=iy[:cnt], iz=iz[:cnt],
                     lx=lx[:cnt * nb].reshape(cnt, nb), ly=ly[:cnt * nb].reshape(cnt, nb),
@@ -320,16 +328,29 @@ class RefPoints:
             lib.ref_pts_create.restype = c_void_p
             lib.ref_pts_create.argtypes = [ctypes.c_char_p, c_int, c_int, c_int, c_int, c_float,
                                            _I]
+            lib.ref_pts_create_topo.restype = c_void_p
+            lib.ref_pts_create_topo.argtypes = [ctypes.c_char_p, c_int, c_int, c_int, c_int,
+                                                c_float, _F, _I]
+            lib.ref_pts_srcadd_curv.argtypes = [c_void_p, c_void_p, c_void_p, c_float, c_float,
+                                                c_void_p, c_int, c_void_p]
             lib.ref_pts_interp.argtypes = [c_void_p, c_void_p, c_void_p]
             lib.ref_pts_srcadd.argtypes = [c_void_p, c_void_p, c_void_p, c_float, c_float]
             lib.ref_pts_destroy.argtypes = [c_void_p]
             cls._lib = lib
         return cls._lib
 
-    def __init__(self, path, grid_type, nx, ny, nz, h):
+    def __init__(self, path, grid_type, nx, ny, nz, h, ftopo=None):
+        """`ftopo`: the normalised surface function (the first f array of
+        awp_topo_metrics) for a curvilinear block, else None."""
         lib = self.lib()
         n = c_int(0)
-        self.h = lib.ref_pts_create(path.encode(), grid_type, nx, ny, nz, h, byref(n))
+        if ftopo is None:
+            self.h = lib.ref_pts_create(path.encode(), grid_type, nx, ny, nz, h, byref(n))
+        else:
+            self._f = np.ascontiguousarray(ftopo, np.float32)
+            self.h = lib.ref_pts_create_topo(path.encode(), grid_type, nx, ny, nz, h,
+                                             fptr(self._f), byref(n))
+        self.ny = ny
         if not self.h:
             raise RuntimeError("reference point-set set-up failed")
         self.count = n.value
@@ -339,6 +360,10 @@ class RefPoints:
 
     def srcadd(self, d_field_ptr, d_values_ptr, h, dt):
         self.lib().ref_pts_srcadd(self.h, c_void_p(d_field_ptr), c_void_p(d_values_ptr), h, dt)
+
+    def srcadd_curv(self, d_field_ptr, d_values_ptr, h, dt, d_f_ptr, d_dg_ptr):
+        self.lib().ref_pts_srcadd_curv(self.h, c_void_p(d_field_ptr), c_void_p(d_values_ptr), h,
+                                       dt, c_void_p(d_f_ptr), self.ny, c_void_p(d_dg_ptr))
 
     def close(self):
         if self.h:
@@ -654,3 +679,59 @@ class RefGpuSim:
 
     def field(self, name):
         return self.f[name].cpu().numpy()
+
+
+class RefTopoSim(RefGpuSim):
+    """RefGpuSim with the reference's curvilinear topography on its grid
+    (oracle/_ref/libawpref_topo.so: topo_init ... topo_set_constants, then
+    topo_velocity_interior_H and topo_stress_{interior,left,right}_H in place of
+    dvelcx / dstrqc, pmcl3d.c:1522-1548, 1661-1698, 1841-1924).  The
+    free-surface imaging, sources and receivers stay the Cartesian ones, as in
+    pmcl3d.  NVE=3 is not modelled: with topography the reference's plasticity
+    branch runs the Cartesian dstrqc on the curvilinear grid."""
+
+    def __init__(self, scn, setup, intopo, path=None, topo_path=None):
+        if scn.params.get("nve", 1) == 3:
+            raise ValueError("RefTopoSim models NVE 1 and 2 only")
+        super().__init__(scn, setup, path=path)
+        topo_path = topo_path or os.path.join(REF_DIR, "libawpref_topo.so")
+        if not os.path.exists(topo_path):
+            raise FileNotFoundError(f"{topo_path} missing: run `make -C oracle ref`")
+        tl = ctypes.CDLL(topo_path, mode=ctypes.RTLD_LOCAL)
+        tl.ref_topo_create.restype = c_void_p
+        tl.ref_topo_create.argtypes = [ctypes.c_char_p, c_int, c_int, c_int, c_float, c_float,
+                                       POINTER(c_void_p)]
+        tl.ref_topo_velocity.argtypes = [c_void_p]
+        tl.ref_topo_stress.argtypes = [c_void_p]
+        tl.ref_topo_destroy.argtypes = [c_void_p]
+        tl.ref_topo_metric_ptrs.argtypes = [c_void_p, POINTER(c_void_p), POINTER(c_int)]
+        self.tl = tl
+        f = self.f
+        order = [f["d1"], f["lam"], f["mu"], f["qp"], self.coeff, f["qs"], self.vx1, self.vx2,
+                 self.ww, self.wwo, f["xx"], f["yy"], f["zz"], f["xy"], f["xz"], f["yz"],
+                 f["r1"], f["r2"], f["r3"], f["r4"], f["r5"], f["r6"], f["u1"], f["v1"], f["w1"],
+                 self.dcrjx, self.dcrjy, self.dcrjz]
+        arr = (c_void_p * len(order))(*[t.data_ptr() for t in order])
+        p = self.p
+        self.T = tl.ref_topo_create(intopo.encode(), self.nx, self.ny, self.nz, c_float(p["dt"]),
+                                    c_float(p["dh"]), arr)
+        self._keep = (order, arr)
+
+    def metric_ptrs(self):
+        out = (c_void_p * 6)()
+        ld = c_int(0)
+        self.tl.ref_topo_metric_ptrs(self.T, out, byref(ld))
+        return list(out), ld.value
+
+    def velocity(self):
+        self.tl.ref_topo_velocity(self.T)
+
+    def stress_all(self):
+        self.tl.ref_topo_stress(self.T)
+        for hook in self.after_stress:
+            hook(self, self.cur)
+
+    def close(self):
+        if getattr(self, "T", None):
+            self.tl.ref_topo_destroy(self.T)
+            self.T = None

@@ -81,3 +81,52 @@ def test_bad_topography_files(tmp_path):
     scenarios.write_topography(path, 24, 20, 50.0, padding=4)
     assert product(path, 24, 20, 32, 50.0)[0] == 902          # padding < ngsl
     assert product(str(tmp_path / "none.bin"), 24, 20, 32, 50.0)[0] == 101
+
+
+def product_coefs_topo(path, intopo, grid_type, nx, ny, nz, h, degree):
+    lib = _lib.load()
+    n = 4096
+    nb = degree + 1
+    cnt = ctypes.c_int()
+    I = ctypes.POINTER(ctypes.c_int)
+    arrs = [np.zeros(n, np.int32) for _ in range(4)]
+    ls = [np.zeros(n * nb, np.float32) for _ in range(3)]
+    err = lib.awp_point_coefs_topo(path.encode(), intopo.encode(), grid_type, nx, ny, nz, h, n,
+                                   ctypes.byref(cnt), *[a.ctypes.data_as(I) for a in arrs],
+                                   *[a.ctypes.data_as(F) for a in ls])
+    c = cnt.value
+    return err, dict(indices=arrs[0][:c], ix=arrs[1][:c], iy=arrs[2][:c], iz=arrs[3][:c],
+                     lx=ls[0][:c * nb].reshape(c, nb), ly=ls[1][:c * nb].reshape(c, nb),
+                     lz=ls[2][:c * nb].reshape(c, nb))
+
+
+@pytest.mark.parametrize("degree", [1, 3])
+@pytest.mark.parametrize("grid_type", range(9))
+def test_curvilinear_point_coefs_match_reference(ref_host, tmp_path, degree, grid_type):
+    """Receivers / SOURCEFILE points on the curvilinear block: the vertical
+    coordinate through the surface function interpolated at the point
+    (metrics_interpolate_f_point, source.c:283-340), then the usual Lagrange
+    set-up -- against the reference's own routines, bit for bit."""
+    from awp_b200 import pointfiles
+    nx, ny, nz, h = 28, 24, 32, 100.0
+    intopo = str(tmp_path / "topo.bin")
+    depth = h * (nz - 2)
+    scenarios.write_topography(intopo, nx, ny, h, amplitude=0.15 * depth, width=5 * h,
+                               rough_rms=0.02 * depth, seed=5)
+    rng = np.random.default_rng(11 + grid_type)
+    n = 14
+    coords = np.stack([rng.uniform(2 * h, (nx - 3) * h, n), rng.uniform(2 * h, (ny - 3) * h, n),
+                       -rng.uniform(0.0, 0.7 * nz * h, n)], 1)
+    types = np.zeros(n, np.int32)
+    types[:4] = 1
+    path = str(tmp_path / "pts.txt")
+    pointfiles.write_input(path, str(tmp_path / "out"), coords, types, degree=degree)
+    e1, mine = product_coefs_topo(path, intopo, grid_type, nx, ny, nz, h, degree)
+    assert e1 == 0
+    _, f = product(intopo, nx, ny, nz, h)
+    ref = ref_host.point_coefs(path, grid_type, nx, ny, nz, h, ftopo=f["f"])
+    assert len(mine["ix"]) == len(ref["ix"]) == n
+    for k in ("indices", "ix", "iy", "iz"):
+        assert np.array_equal(mine[k], ref[k]), k
+    for k in ("lx", "ly", "lz"):
+        assert np.array_equal(mine[k].view(np.uint32), ref[k].view(np.uint32)), k
