@@ -2,7 +2,7 @@
 //
 // Same command line (src/awp/command.c), same input files (INVEL mesh,
 // INSRC sources, sourcefilter.dat, nonlinear.dat, SOURCEFILE and RECVFILE
-// point sets) and the same output files (OUT/SX_0_%07ld, SY, SZ, Eta; the
+// point sets, INTOPO topography) and the same output files (OUT/SX_0_%07ld, SY, SZ, Eta; the
 // CHKFILE statistics log; the receiver files <file>_<x|y|z>_<step>) as the
 // reference's single-rank run; the time step itself runs in libawpb200
 // through its C ABI.
@@ -255,8 +255,8 @@ int main(int argc, char** argv) {
             A.NGRIDS);
     return 1;
   }
-  if (A.USETOPO || A.USEFORCEFILE || A.USESGTFILE) {
-    fprintf(stderr, "pmcl3d: INTOPO/FORCEFILE/SGTFILE are not part of this build\n");
+  if (A.USEFORCEFILE || A.USESGTFILE) {
+    fprintf(stderr, "pmcl3d: FORCEFILE/SGTFILE are not part of this build\n");
     return 1;
   }
   if (A.NZ[0] % 4 != 0) {  // pmcl3d.c:380-391 (BLOCK_SIZE_Z = 4)
@@ -487,6 +487,9 @@ int main(int argc, char** argv) {
     AWP(awp_upload_plasticity(ctx, sigma2.data(), cohes.data(), phi.data(), fmajor, fminor,
                               strike, dip));
   }
+
+  // ---- curvilinear topography of grid 0 (pmcl3d.c:1522-1548) --------------------
+  if (A.USETOPO) AWP(awp_topography_init(ctx, A.INTOPO.c_str()));
 
   // ---- SOURCEFILE / RECVFILE point sets (pmcl3d.c:1563-1568, 1603-1607) ---------
   if (A.USESOURCEFILE) AWP(awp_sourcefile_init(ctx, A.SOURCEFILE.c_str()));

@@ -248,11 +248,25 @@ def run_ours(args, rank, world, dist) -> dict | None:
     hbm, peak_kind = peaks()
 
     # ---- device-resident timing -------------------------------------------------
+    topo_path = None
+    if args.topography:
+        # a Gaussian hill with rough relief over the workload's surface (the
+        # curvilinear top-grid operators replace the Cartesian ones)
+        import tempfile
+        from awp_b200 import scenarios as _sc
+        topo_path = os.path.join(tempfile.mkdtemp(prefix="awp_topo_"), "topography.bin")
+        depth = p["dh"] * (p["nz"] - 2)
+        _sc.write_topography(topo_path, p["nx"], p["ny"], p["dh"], amplitude=0.1 * depth,
+                             width=0.2 * p["nx"] * p["dh"], rough_rms=0.005 * depth, seed=3)
     s = Solver(default_params(**p), stream=stream.cuda_stream)
     s.upload_media(scn.media)
     s.upload_sources(scn.src_pos, scn.src_data)
+    if topo_path:
+        s.topography(topo_path)
     tuning = None
-    if args.tma is not None:
+    if topo_path:
+        pass  # the tuning keys select Cartesian kernel families only
+    elif args.tma is not None:
         from awp_b200 import tune
         tune.set_tuning(s.lib, "tma", args.tma)
     elif not args.no_tune:
@@ -291,8 +305,17 @@ def run_ours(args, rank, world, dist) -> dict | None:
     vel_ms = ve_ms / max(ve_n, 1)
     b_st = B_STRESS[kind] * cells
     achieved = b_st / (stress_ms * 1e-3) / 1e9
-    traffic = load_traffic("stress", args.workload)
-    roofline = {"bound": "hbm", "kernel": "k_stress (stress + memory variables)",
+    if topo_path:
+        tkey = "topo_stress"
+    else:
+        # the stress kernel family the run used (autotuned, forced or default)
+        from awp_b200 import tune as _tune
+        tkey = "stress_tma" if _tune.get_tuning(s.lib)["tma_str"] == 1 else "stress"
+    traffic = load_traffic(tkey, args.workload)
+    kname = {"topo_stress": "k_topo_stress (curvilinear stress + memory variables)",
+             "stress_tma": "k_stress_tma (TMA-pipelined stress + memory variables)",
+             "stress": "k_stress (stress + memory variables)"}[tkey]
+    roofline = {"bound": "hbm", "kernel": kname,
                 "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                 "peak_kind": f"{peak_kind} hbm_gbs", "traffic": traffic,
                 "alg_bytes_per_launch": b_st, "alg_bytes_per_cell": B_STRESS[kind],
@@ -324,6 +347,8 @@ def run_ours(args, rank, world, dist) -> dict | None:
         se.lib.awp_upload_media(se.ctx, nvar, media.numpy().ctypes.data_as(
             __import__("ctypes").POINTER(__import__("ctypes").c_float)))
         se.upload_sources(scn.src_pos, scn.src_data)
+        if topo_path:
+            se.topography(topo_path)
         se.step(e2e_steps)
         # free-surface snapshot (velbuffer, NBGZ=NEDZ=1) back to the host
         se.gather(0, p["nx"] - 1, 1, 0, p["ny"] - 1, 1, 0, 0, 1,
@@ -357,6 +382,8 @@ def run_ours(args, rank, world, dist) -> dict | None:
                    "dh": p["dh"], "dt": p["dt"], "ifault": p["ifault"], "nve": p["nve"],
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                    "l2": "working set ~7 GB >> 126 MB L2, no flush needed",
+                   "topography": ("Gaussian hill + rough relief (curvilinear top grid)"
+                                  if topo_path else None),
                    "finite_after_run": ok},
         "roofline": roofline,
         "step_roofline": {"bytes_per_cell_alg": B_ALG[kind], "achieved": step_bw,
@@ -407,6 +434,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="layered_vk", choices=["layered_vk", "halfspace"])
+    ap.add_argument("--topography", action="store_true",
+                    help="curvilinear top grid (INTOPO) on the same workload")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ref-gpu", action="store_true")

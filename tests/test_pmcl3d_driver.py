@@ -103,13 +103,20 @@ def test_recvfile_needs_readable_file(tmp_path):
 
 
 @pytest.mark.gpu
-def test_point_sets_match_library(tmp_path):
-    """--SOURCEFILE and --RECVFILE through the executable give the same receiver
-    files as the same run through the library."""
+@pytest.mark.parametrize("topo", [False, True])
+def test_point_sets_match_library(tmp_path, topo):
+    """--SOURCEFILE and --RECVFILE (and --INTOPO) through the executable give the
+    same receiver files as the same run through the library."""
     from awp_b200 import pointfiles
     scn = scenarios.random_small(nx=24, ny=20, nz=32, steps=12, seed=9, ifault=1, nsrc=2)
     p = scn.params
     write_inputs(scn, tmp_path)
+    topo_args = []
+    if topo:
+        scenarios.write_topography(str(tmp_path / "topo.bin"), p["nx"], p["ny"], p["dh"],
+                                   amplitude=0.1 * p["dh"] * p["nz"], width=5 * p["dh"],
+                                   rough_rms=0.0)
+        topo_args = ["--INTOPO", str(tmp_path / "topo.bin")]
     nt = 12
     tmax = (nt - 1) * p["dt"] + p["dt"] * 0.5
     h = p["dh"]
@@ -128,11 +135,13 @@ def test_point_sets_match_library(tmp_path):
             "-I", 1, "-S", scn.src_pos.shape[0], "-N", p["nst"], "-R", p["nst"],
             "--INVEL", "media", "--INSRC", "src", "-o", "out", "-c", "chk",
             "--SOURCEFILE", str(tmp_path / "src.txt"), "--RECVFILE", str(tmp_path / "recv.txt")]
-    r = run(args, tmp_path)
+    r = run(args + topo_args, tmp_path)
     assert r.returncode == 0, r.stderr + r.stdout
     s = Solver(default_params(**p))
     s.upload_media(scn.media)
     s.upload_sources(scn.src_pos, scn.src_data)
+    if topo:
+        s.topography(str(tmp_path / "topo.bin"))
     s.sourcefile(str(tmp_path / "lib" / "src.txt"))
     s.receivers(str(tmp_path / "lib" / "recv.txt"), nt)
     s.step(nt)
