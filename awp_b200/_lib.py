@@ -112,6 +112,16 @@ def load() -> ctypes.CDLL:
     _sig(lib, "awp_mesh_grid", c_int, [_P, c_int, POINTER(c_void_p)])
     _sig(lib, "awp_mesh_step", c_int, [_P, c_int])
     _sig(lib, "awp_mesh_synchronize", c_int, [_P])
+    _sig(lib, "awp_batch_create", c_int, [POINTER(c_void_p), c_int, POINTER(c_void_p)])
+    _sig(lib, "awp_batch_destroy", c_int, [_P])
+    _sig(lib, "awp_batch_step", c_int, [_P, c_int])
+    _sig(lib, "awp_batch_synchronize", c_int, [_P])
+    _sig(lib, "awp_batch_set_shape", c_int, [_P, c_int, c_int])
+    _sig(lib, "awp_batch_get_shape", c_int, [_P, _I, _I])
+    _sig(lib, "awp_batch_set_graph", c_int, [_P, c_int])
+    _sig(lib, "awp_batch_set_mode", c_int, [_P, c_int])
+    _sig(lib, "awp_batch_get_mode", c_int, [_P])
+    _sig(lib, "awp_batch_info", c_int, [_P, POINTER(c_longlong)])
     _sig(lib, "awp_receivers_init", c_int, [_P, c_char_p, c_longlong])
     _sig(lib, "awp_receivers_count", c_int, [_P, _I])
     _sig(lib, "awp_sourcefile_init", c_int, [_P, c_char_p])

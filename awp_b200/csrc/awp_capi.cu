@@ -153,29 +153,28 @@ StrArgs make_str_args(awp_ctx* c) {
   return a;
 }
 
-int launch_sources(awp_ctx* c, int tidx) {
-  if (c->ncell == 0) return AWP_OK;
-  if (c->p.ifault == 5) {
-    KinSrcArgs a;
-    memset(&a, 0, sizeof(a));
-    a.xx = c->f[AWP_XX]; a.yy = c->f[AWP_YY]; a.zz = c->f[AWP_ZZ];
-    a.xy = c->f[AWP_XY]; a.yz = c->f[AWP_YZ]; a.xz = c->f[AWP_XZ];
-    a.mu = c->f[AWP_MU];
-    a.cell_pos = c->d_cell_pos; a.cell_first = c->d_cell_first; a.order = c->d_order;
-    a.axx = c->d_src[0]; a.ayy = c->d_src[1]; a.azz = c->d_src[2];
-    a.axz = c->d_src[3]; a.ayz = c->d_src[4]; a.axy = c->d_src[5];
-    a.mom = c->d_mom;
-    a.filt_state = c->d_filt;
-    a.filtorder = c->filtorder;
-    memcpy(a.filt_b, c->filt_b, sizeof(a.filt_b));
-    memcpy(a.filt_a, c->filt_a, sizeof(a.filt_a));
-    a.ncell = c->ncell;
-    a.step = tidx;
-    a.dt = c->p.dt;
-    a.vtst = (float)c->p.dt / (c->p.dh * c->p.dh * c->p.dh);
-    CU_TRY(awp_launch_addkinsrc(a, c->stream));
-    return AWP_OK;
-  }
+KinSrcArgs make_kin_args(awp_ctx* c, int step) {
+  KinSrcArgs a;
+  memset(&a, 0, sizeof(a));
+  a.xx = c->f[AWP_XX]; a.yy = c->f[AWP_YY]; a.zz = c->f[AWP_ZZ];
+  a.xy = c->f[AWP_XY]; a.yz = c->f[AWP_YZ]; a.xz = c->f[AWP_XZ];
+  a.mu = c->f[AWP_MU];
+  a.cell_pos = c->d_cell_pos; a.cell_first = c->d_cell_first; a.order = c->d_order;
+  a.axx = c->d_src[0]; a.ayy = c->d_src[1]; a.azz = c->d_src[2];
+  a.axz = c->d_src[3]; a.ayz = c->d_src[4]; a.axy = c->d_src[5];
+  a.mom = c->d_mom;
+  a.filt_state = c->d_filt;
+  a.filtorder = c->filtorder;
+  memcpy(a.filt_b, c->filt_b, sizeof(a.filt_b));
+  memcpy(a.filt_a, c->filt_a, sizeof(a.filt_a));
+  a.ncell = c->ncell;
+  a.step = step;
+  a.dt = c->p.dt;
+  a.vtst = (float)c->p.dt / (c->p.dh * c->p.dh * c->p.dh);
+  return a;
+}
+
+SrcArgs make_src_args(awp_ctx* c, int tidx) {
   SrcArgs a;
   memset(&a, 0, sizeof(a));
   a.xx = c->f[AWP_XX]; a.yy = c->f[AWP_YY]; a.zz = c->f[AWP_ZZ];
@@ -187,7 +186,15 @@ int launch_sources(awp_ctx* c, int tidx) {
   a.stride = c->src_stride;
   a.tidx = tidx;
   a.vtst = (float)c->p.dt / (c->p.dh * c->p.dh * c->p.dh);
-  CU_TRY(awp_launch_addsrc(a, c->stream));
+  return a;
+}
+
+int launch_sources(awp_ctx* c, int tidx) {
+  if (c->ncell == 0) return AWP_OK;
+  if (c->p.ifault == 5)
+    CU_TRY(awp_launch_addkinsrc(make_kin_args(c, tidx), c->stream));
+  else
+    CU_TRY(awp_launch_addsrc(make_src_args(c, tidx), c->stream));
   return AWP_OK;
 }
 
@@ -309,7 +316,7 @@ TopoArgs topo_args(awp_ctx* c) {
   return a;
 }
 
-int phase_velocity(awp_ctx* c) {
+VelArgs make_vel_args(awp_ctx* c) {
   float** f = c->f;
   VelArgs v;
   v.u1 = f[AWP_U1]; v.v1 = f[AWP_V1]; v.w1 = f[AWP_W1];
@@ -326,6 +333,11 @@ int phase_velocity(awp_ctx* c) {
   v.k1 = AWP_ALIGN + round_up(c->g.nzt, 4) - 1;
   if (c->p.grid > 0) v.k1 = std::min(v.k1, c->g.nzt + AWP_ALIGN - 3);
   v.dth = c->dth; v.c1 = c->c1; v.c2 = c->c2;
+  return v;
+}
+
+int phase_velocity(awp_ctx* c) {
+  const VelArgs v = make_vel_args(c);
   if (c->topo) {  // topo_velocity_*_H replace dvelc[xy] on the top grid (pmcl3d.c:1661-1698)
     PhaseScope ps(c, 0);
     CU_TRY(awp_launch_topo_velocity(topo_args(c), c->stream));
@@ -390,14 +402,19 @@ int phase_plasticity(awp_ctx* c) {
   return AWP_OK;
 }
 
-int phase_fstr(awp_ctx* c) {
-  if (c->p.grid != 0) return AWP_OK;  // fstr_H on grid 0 only (pmcl3d.c:2243)
+FstrArgs make_fstr_args(awp_ctx* c) {
   float** f = c->f;
   FstrArgs fs;
   fs.zz = f[AWP_ZZ]; fs.xz = f[AWP_XZ]; fs.yz = f[AWP_YZ];
   fs.slice = c->g.slice; fs.yline = c->g.yline; fs.ktop = c->g.top();
   fs.i0 = c->xls; fs.i1 = c->xre;
   fs.j0 = c->yls; fs.j1 = c->yls + round_up(c->yre - c->yls + 1, 2) - 1;
+  return fs;
+}
+
+int phase_fstr(awp_ctx* c) {
+  if (c->p.grid != 0) return AWP_OK;  // fstr_H on grid 0 only (pmcl3d.c:2243)
+  const FstrArgs fs = make_fstr_args(c);
   PhaseScope ps(c, 4);
   CU_TRY(awp_launch_fstr(fs, c->stream));
   c->launches++;
@@ -1262,6 +1279,370 @@ int awp_topo_metrics(const char* path, int nx, int ny, int nz, float h, float* o
   const std::vector<float>* ga[4] = {&m.g, &m.g_c, &m.g3, &m.g3_c};
   for (int q = 0; q < 4; ++q) memcpy(out + 10 * nf + q * ng, ga[q]->data(), ng * sizeof(float));
   return 0;
+}
+
+}  // extern "C"
+
+// ===========================================================================
+// Batched instances
+// ===========================================================================
+struct awp_batch {
+  std::vector<awp_ctx*> ctx;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev = nullptr;
+  BatchInst* d_inst = nullptr;
+  int4 *d_vt = nullptr, *d_st = nullptr, *d_ste = nullptr;
+  int2 *d_src = nullptr, *d_rows = nullptr;
+  int* d_cnt = nullptr;   // [3] tile counters
+  int* d_step = nullptr;  // steps taken (device copy of cur_step)
+  BatchLaunch L{};
+  int ty = 8, ichunk = 16;
+  int mode = 0;  // 0: persistent tile-queue launches; 1: graph of each instance's own launches
+  std::vector<cudaStream_t> cs;   // mode 1: one capture stream per instance
+  std::vector<cudaEvent_t> join;  // mode 1: branch joins
+  cudaEvent_t fork = nullptr;
+  long long launches_per_step = 0;
+  bool use_graph = true;
+  bool dirty = true;  // tile lists / graph to rebuild
+  long long step = 0;
+  long long cells = 0;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+};
+
+namespace {
+
+void batch_free_lists(awp_batch* b) {
+  cudaFree(b->d_vt); cudaFree(b->d_st); cudaFree(b->d_ste);
+  b->d_vt = b->d_st = b->d_ste = nullptr;
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  b->exec = nullptr;
+  b->graph = nullptr;
+}
+
+template <class T>
+int upload_vec(T** d, const std::vector<T>& h) {
+  *d = nullptr;
+  if (h.empty()) return AWP_OK;
+  CU_TRY(cudaMalloc((void**)d, sizeof(T) * h.size()));
+  CU_TRY(cudaMemcpy(*d, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice));
+  return AWP_OK;
+}
+
+// Mode 1: one step of every instance as parallel branches of one graph, each
+// branch the instance's own tuned launches (velocity, stress, sources at the
+// device step, free-surface images); the step counter advances after the join.
+int batch_capture_instances(awp_batch* b) {
+  if (b->cs.empty()) {
+    b->cs.assign(b->ctx.size(), nullptr);
+    b->join.assign(b->ctx.size(), nullptr);
+    for (size_t q = 0; q < b->ctx.size(); ++q) {
+      CU_TRY(cudaStreamCreateWithFlags(&b->cs[q], cudaStreamNonBlocking));
+      CU_TRY(cudaEventCreateWithFlags(&b->join[q], cudaEventDisableTiming));
+    }
+    CU_TRY(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
+  }
+  CU_TRY(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+  int st = AWP_OK;
+  long long l0 = 0;
+  for (awp_ctx* c : b->ctx) l0 += c->launches;
+  cudaError_t ce = cudaEventRecord(b->fork, b->stream);
+  for (size_t q = 0; q < b->ctx.size() && !st && ce == cudaSuccess; ++q) {
+    awp_ctx* c = b->ctx[q];
+    cudaStream_t saved = c->stream;
+    const bool prof = c->profile;
+    c->stream = b->cs[q];
+    c->profile = false;
+    ce = cudaStreamWaitEvent(b->cs[q], b->fork, 0);
+    if (ce == cudaSuccess) st = phase_velocity(c);
+    if (!st && ce == cudaSuccess) st = phase_stress(c);
+    if (!st && ce == cudaSuccess && c->ncell > 0) {
+      if (c->p.ifault == 5) {
+        const KinSrcArgs k = make_kin_args(c, 0);
+        ce = awp_launch_sources_dev(nullptr, &k, b->d_step, 0, c->stream);
+        c->launches++;
+      } else if (c->p.ifault < 4) {
+        const SrcArgs a = make_src_args(c, 0);
+        ce = awp_launch_sources_dev(&a, nullptr, b->d_step, c->p.nst, c->stream);
+        c->launches++;
+      }
+    }
+    if (!st && ce == cudaSuccess) st = phase_fstr(c);
+    if (!st && ce == cudaSuccess) ce = cudaEventRecord(b->join[q], b->cs[q]);
+    if (!st && ce == cudaSuccess) ce = cudaStreamWaitEvent(b->stream, b->join[q], 0);
+    c->stream = saved;
+    c->profile = prof;
+  }
+  if (!st && ce == cudaSuccess) {
+    ce = awp_launch_step_advance(b->d_step, b->stream);
+    b->ctx[0]->launches++;
+  }
+  cudaGraph_t g = nullptr;
+  const cudaError_t ee = cudaStreamEndCapture(b->stream, &g);
+  long long l1 = 0;
+  for (awp_ctx* c : b->ctx) l1 += c->launches;
+  b->ctx[0]->launches -= (l1 - l0);  // counted per replay instead
+  b->launches_per_step = l1 - l0;
+  if (st || ce != cudaSuccess || ee != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    if (st) return st;
+    return set_error(AWP_ERR_CUDA, "batch graph capture: %s",
+                     cudaGetErrorString(ce != cudaSuccess ? ce : ee));
+  }
+  b->graph = g;
+  CU_TRY(cudaGraphInstantiate(&b->exec, g, 0));
+  return AWP_OK;
+}
+
+// Tile lists for the current shape (tile 32 k x ty j x ichunk i), the
+// persistent grid sizes, and the captured one-step graph.
+int batch_build(awp_batch* b) {
+  batch_free_lists(b);
+  if (b->mode == 1) {
+    const int e = batch_capture_instances(b);
+    if (!e) b->dirty = false;
+    return e;
+  }
+  std::vector<int4> vt, st, ste;
+  for (size_t n = 0; n < b->ctx.size(); ++n) {
+    awp_ctx* c = b->ctx[n];
+    const VelArgs v = make_vel_args(c);
+    const int gx = (v.k1 - v.k0 + 32) / 32, gy = (v.j1 - v.j0 + b->ty) / b->ty,
+              gz = (v.i1 - v.i0 + b->ichunk) / b->ichunk;
+    for (int z = 0; z < gz; ++z)
+      for (int y = 0; y < gy; ++y)
+        for (int x = 0; x < gx; ++x) vt.push_back(make_int4((int)n, x, y, z));
+    const StrArgs a = make_str_args(c);
+    const int sx = (a.k1 - a.k0 + 32) / 32, sy = (a.j1 - a.j0 + b->ty) / b->ty,
+              sz = (a.i1 - a.i0 + b->ichunk) / b->ichunk;
+    std::vector<int4>& dst = c->elastic ? ste : st;
+    for (int z = 0; z < sz; ++z)
+      for (int y = 0; y < sy; ++y)
+        for (int x = 0; x < sx; ++x) dst.push_back(make_int4((int)n, x, y, z));
+  }
+  int e;
+  if ((e = upload_vec(&b->d_vt, vt)) || (e = upload_vec(&b->d_st, st)) ||
+      (e = upload_vec(&b->d_ste, ste)))
+    return e;
+  int bv = 0, bs = 0;
+  if (awp_batch_blocks_per_sm(b->ty, &bv, &bs))
+    return set_error(AWP_ERR_CUDA, "batch occupancy query failed");
+  int dev = 0, nsm = 0;
+  CU_TRY(cudaGetDevice(&dev));
+  CU_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  BatchLaunch& L = b->L;
+  L.inst = b->d_inst;
+  L.vtiles = b->d_vt; L.stiles = b->d_st; L.stiles_el = b->d_ste;
+  L.nvtiles = (int)vt.size(); L.nstiles = (int)st.size(); L.nstiles_el = (int)ste.size();
+  L.counters = b->d_cnt; L.step = b->d_step;
+  L.ty = b->ty; L.ichunk = b->ichunk;
+  L.grid_vel = std::max(1, std::min(nsm * std::max(bv, 1), L.nvtiles));
+  L.grid_str = std::max(1, std::min(nsm * std::max(bs, 1), std::max(L.nstiles, L.nstiles_el)));
+  b->launches_per_step = 1 + (L.nstiles > 0) + (L.nstiles_el > 0) + (L.nsrc > 0) + 1;
+  if (b->use_graph) {
+    CU_TRY(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    cudaError_t le = awp_launch_batch_step(L, b->stream);
+    cudaGraph_t g = nullptr;
+    cudaError_t ce = cudaStreamEndCapture(b->stream, &g);
+    if (le != cudaSuccess || ce != cudaSuccess) {
+      if (g) cudaGraphDestroy(g);
+      return set_error(AWP_ERR_CUDA, "batch graph capture: %s",
+                       cudaGetErrorString(le != cudaSuccess ? le : ce));
+    }
+    b->graph = g;
+    CU_TRY(cudaGraphInstantiate(&b->exec, g, 0));
+  }
+  b->dirty = false;
+  return AWP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int awp_batch_destroy(awp_batch* b) {
+  if (!b) return AWP_OK;
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  batch_free_lists(b);
+  cudaFree(b->d_inst); cudaFree(b->d_src); cudaFree(b->d_rows);
+  cudaFree(b->d_cnt); cudaFree(b->d_step);
+  for (cudaStream_t x : b->cs) if (x) cudaStreamDestroy(x);
+  for (cudaEvent_t x : b->join) if (x) cudaEventDestroy(x);
+  if (b->fork) cudaEventDestroy(b->fork);
+  if (b->ev) cudaEventDestroy(b->ev);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+  return AWP_OK;
+}
+
+int awp_batch_create(awp_ctx* const* ctxs, int n, awp_batch** out) {
+  if (!ctxs || !out || n < 1) return set_error(AWP_ERR_ARG, "null argument or n < 1");
+  *out = nullptr;
+  for (int q = 0; q < n; ++q) {
+    awp_ctx* c = ctxs[q];
+    if (!c) return set_error(AWP_ERR_ARG, "instance %d is null", q);
+    if (!c->media_ready) return set_error(AWP_ERR_STATE, "instance %d: media not uploaded", q);
+    if (c->p.ngrids != 1 || c->p.nve == 3 || c->topo || c->recv || c->srcf)
+      return set_error(AWP_ERR_UNSUPPORTED,
+                       "instance %d: a batch holds single-grid Cartesian runs without "
+                       "plasticity, receivers or SOURCEFILE sources", q);
+    if (c->cur_step != ctxs[0]->cur_step)
+      return set_error(AWP_ERR_STATE, "instances must start at the same step");
+    for (int r = 0; r < q; ++r)
+      if (ctxs[r] == c) return set_error(AWP_ERR_ARG, "instance %d appears twice", q);
+  }
+  awp_batch* b = new awp_batch();
+  b->ctx.assign(ctxs, ctxs + n);
+  b->step = ctxs[0]->cur_step;
+  if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&b->ev, cudaEventDisableTiming) != cudaSuccess) {
+    awp_batch_destroy(b);
+    return set_error(AWP_ERR_CUDA, "batch stream/event creation failed");
+  }
+  std::vector<BatchInst> inst(n);
+  std::vector<int2> src, rows;
+  for (int q = 0; q < n; ++q) {
+    awp_ctx* c = ctxs[q];
+    BatchInst& I = inst[q];
+    memset(&I, 0, sizeof(I));
+    I.v = make_vel_args(c);
+    I.s = make_str_args(c);
+    I.f = make_fstr_args(c);
+    I.src = make_src_args(c, 0);
+    I.kin = make_kin_args(c, 0);
+    I.elastic = c->elastic ? 1 : 0;
+    I.ifault = c->p.ifault;
+    I.nst = c->p.nst;
+    if (c->ncell > 0 && (c->p.ifault < 4 || c->p.ifault == 5))
+      for (int k = 0; k < c->ncell; ++k) src.push_back(make_int2(q, k));
+    for (int i = I.f.i0; i <= I.f.i1; ++i) rows.push_back(make_int2(q, i));
+    b->cells += (long long)c->p.nx * c->p.ny * c->p.nz;
+  }
+  int e;
+  if ((e = upload_vec(&b->d_inst, inst)) || (e = upload_vec(&b->d_src, src)) ||
+      (e = upload_vec(&b->d_rows, rows))) {
+    awp_batch_destroy(b);
+    return e;
+  }
+  if (cudaMalloc((void**)&b->d_cnt, 3 * sizeof(int)) != cudaSuccess ||
+      cudaMalloc((void**)&b->d_step, sizeof(int)) != cudaSuccess) {
+    awp_batch_destroy(b);
+    return set_error(AWP_ERR_NOMEM, "batch counters");
+  }
+  b->L.src_cells = b->d_src;
+  b->L.nsrc = (int)src.size();
+  b->L.rows = b->d_rows;
+  b->L.nrows = (int)rows.size();
+  const int st = (int)b->step;
+  if (cudaMemcpy(b->d_step, &st, sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess) {
+    awp_batch_destroy(b);
+    return set_error(AWP_ERR_CUDA, "batch step upload");
+  }
+  *out = b;
+  return AWP_OK;
+}
+
+int awp_batch_set_shape(awp_batch* b, int ty, int ichunk) {
+  if (!b) return set_error(AWP_ERR_ARG, "null batch");
+  if ((ty != 4 && ty != 8) || ichunk < 1 || ichunk > 1024)
+    return set_error(AWP_ERR_ARG, "tile shape: ty 4 or 8, ichunk 1..1024");
+  if (ty != b->ty || ichunk != b->ichunk) {
+    b->ty = ty;
+    b->ichunk = ichunk;
+    b->dirty = true;
+  }
+  return AWP_OK;
+}
+
+int awp_batch_set_mode(awp_batch* b, int mode) {
+  if (!b) return set_error(AWP_ERR_ARG, "null batch");
+  if (mode != 0 && mode != 1) return set_error(AWP_ERR_ARG, "batch mode 0 or 1");
+  if (mode != b->mode) {
+    b->mode = mode;
+    b->dirty = true;
+  }
+  return AWP_OK;
+}
+
+int awp_batch_get_mode(const awp_batch* b) { return b ? b->mode : -1; }
+
+int awp_batch_get_shape(const awp_batch* b, int* ty, int* ichunk) {
+  if (!b || !ty || !ichunk) return set_error(AWP_ERR_ARG, "null argument");
+  *ty = b->ty;
+  *ichunk = b->ichunk;
+  return AWP_OK;
+}
+
+int awp_batch_set_graph(awp_batch* b, int use_graph) {
+  if (!b) return set_error(AWP_ERR_ARG, "null batch");
+  if ((use_graph != 0) != b->use_graph) {
+    b->use_graph = use_graph != 0;
+    b->dirty = true;
+  }
+  return AWP_OK;
+}
+
+int awp_batch_step(awp_batch* b, int nsteps) {
+  if (!b) return set_error(AWP_ERR_ARG, "null batch");
+  if (nsteps < 0) return set_error(AWP_ERR_ARG, "nsteps < 0");
+  for (awp_ctx* c : b->ctx)
+    if (c->cur_step != b->step)
+      return set_error(AWP_ERR_STATE, "an instance was stepped outside the batch");
+  if (nsteps == 0) return AWP_OK;
+  // order after each instance's earlier work; the step-1 source sample of
+  // IFAULT < 4 is added before the first step (pmcl3d.c:1175-1187)
+  for (awp_ctx* c : b->ctx) {
+    if (c->cur_step == 0 && !c->initial_src_done) {
+      if (c->p.ifault < 4) {
+        int s = launch_sources(c, 0);
+        if (s) return s;
+        if (c->ncell) c->launches++;
+      }
+      c->initial_src_done = true;
+    }
+    CU_TRY(cudaEventRecord(b->ev, c->stream));
+    CU_TRY(cudaStreamWaitEvent(b->stream, b->ev, 0));
+  }
+  if (b->dirty) {
+    int e = batch_build(b);
+    if (e) return e;
+  }
+  for (int n = 0; n < nsteps; ++n) {
+    if (b->use_graph || b->mode == 1)
+      CU_TRY(cudaGraphLaunch(b->exec, b->stream));
+    else
+      CU_TRY(awp_launch_batch_step(b->L, b->stream));
+  }
+  CU_TRY(cudaEventRecord(b->ev, b->stream));
+  for (awp_ctx* c : b->ctx) {
+    CU_TRY(cudaStreamWaitEvent(c->stream, b->ev, 0));
+    c->cur_step += nsteps;
+  }
+  b->ctx[0]->launches += b->launches_per_step * nsteps;
+  b->step += nsteps;
+  return AWP_OK;
+}
+
+int awp_batch_synchronize(awp_batch* b) {
+  if (!b) return set_error(AWP_ERR_ARG, "null batch");
+  CU_TRY(cudaStreamSynchronize(b->stream));
+  return AWP_OK;
+}
+
+int awp_batch_info(awp_batch* b, long long info[6]) {
+  if (!b || !info) return set_error(AWP_ERR_ARG, "null argument");
+  if (b->dirty) {
+    int e = batch_build(b);
+    if (e) return e;
+  }
+  info[0] = (long long)b->ctx.size();
+  info[1] = b->cells;
+  info[2] = b->L.nvtiles;
+  info[3] = (long long)b->L.nstiles + b->L.nstiles_el;
+  info[4] = b->L.grid_vel;
+  info[5] = b->L.grid_str;
+  return AWP_OK;
 }
 
 int awp_topography_init(awp_ctx* c, const char* intopo) {

@@ -34,13 +34,15 @@ int g_tma_str = 1;
 // ===========================================================================
 // Velocity (dvelcx_opt, kernel.cu:125-268)
 // ===========================================================================
+// One 32 k x TY j x ichunk i tile (tile coordinates bx, by, bz), thread (tx, ty).
 template <int TY>
-__global__ void __launch_bounds__(32 * TY)
-    k_velocity(const VelArgs a, const int ichunk) {
-  const int k = a.k0 + blockIdx.x * 32 + threadIdx.x;
-  const int j = a.j0 + blockIdx.y * TY + threadIdx.y;
+__device__ __forceinline__ void vel_tile(const VelArgs& a, const int bx, const int by,
+                                         const int bz, const int ichunk, const int tx,
+                                         const int ty) {
+  const int k = a.k0 + bx * 32 + tx;
+  const int j = a.j0 + by * TY + ty;
   if (k > a.k1 || j > a.j1) return;
-  const int ib = a.i0 + blockIdx.z * ichunk;
+  const int ib = a.i0 + bz * ichunk;
   const int ie = min(ib + ichunk - 1, a.i1);
   const int S = a.slice, Y = a.yline;
   const float c1 = a.c1, c2 = a.c2, dth = a.dth;
@@ -96,6 +98,12 @@ __global__ void __launch_bounds__(32 * TY)
   }
 }
 
+template <int TY>
+__global__ void __launch_bounds__(32 * TY)
+    k_velocity(const VelArgs a, const int ichunk) {
+  vel_tile<TY>(a, blockIdx.x, blockIdx.y, blockIdx.z, ichunk, threadIdx.x, threadIdx.y);
+}
+
 // ===========================================================================
 // Stress + attenuation (dstrqc, kernel.cu:880-1197)
 // ===========================================================================
@@ -120,12 +128,13 @@ __device__ __forceinline__ float sum8(const Plane4& c, const Plane4& n) {
 }
 
 template <bool ELASTIC, bool TEXARR, int TY>
-__global__ void __launch_bounds__(32 * TY, TY == 8 ? 2 : 1)
-    k_stress(const StrArgs a, const int ichunk) {
-  const int k = a.k0 + blockIdx.x * 32 + threadIdx.x;
-  const int j = a.j0 + blockIdx.y * TY + threadIdx.y;
+__device__ __forceinline__ void str_tile(const StrArgs& a, const int bx, const int by,
+                                         const int bz, const int ichunk, const int tx,
+                                         const int ty) {
+  const int k = a.k0 + bx * 32 + tx;
+  const int j = a.j0 + by * TY + ty;
   if (k > a.k1 || j > a.j1) return;
-  const int ib = a.i0 + blockIdx.z * ichunk;
+  const int ib = a.i0 + bz * ichunk;
   const int ie = min(ib + ichunk - 1, a.i1);
   const int S = a.slice, Y = a.yline;
   const float c1 = a.c1, c2 = a.c2, DT = a.dt, dth = a.dth, dh1 = a.dh1;
@@ -269,12 +278,17 @@ __global__ void __launch_bounds__(32 * TY, TY == 8 ? 2 : 1)
   }
 }
 
+template <bool ELASTIC, bool TEXARR, int TY>
+__global__ void __launch_bounds__(32 * TY, TY == 8 ? 2 : 1)
+    k_stress(const StrArgs a, const int ichunk) {
+  str_tile<ELASTIC, TEXARR, TY>(a, blockIdx.x, blockIdx.y, blockIdx.z, ichunk, threadIdx.x,
+                                threadIdx.y);
+}
+
 // ===========================================================================
 // Free-surface stress imaging (fstr, kernel.cu:1616-1647)
 // ===========================================================================
-__global__ void k_fstr(const FstrArgs a) {
-  const int j = a.j0 + blockIdx.x * blockDim.x + threadIdx.x;
-  const int i = a.i0 + blockIdx.y;
+__device__ __forceinline__ void fstr_cell(const FstrArgs& a, const int i, const int j) {
   if (j > a.j1 || i > a.i1) return;
   const long long p = (long long)i * a.slice + (long long)j * a.yline + a.ktop;
   a.zz[p + 1] = -a.zz[p];
@@ -285,6 +299,10 @@ __global__ void k_fstr(const FstrArgs a) {
   a.yz[p + 2] = -a.yz[p - 2];
   a.xz[p] = 0.0f;
   a.yz[p] = 0.0f;
+}
+
+__global__ void k_fstr(const FstrArgs a) {
+  fstr_cell(a, a.i0 + blockIdx.y, a.j0 + blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // ===========================================================================
@@ -310,9 +328,7 @@ __global__ void k_addsrc_direct(const SrcArgs a) {
   a.xy[p] = a.xy[p] - a.vtst * a.axy[t];
 }
 
-__global__ void k_addsrc(const SrcArgs a) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= a.ncell) return;
+__device__ __forceinline__ void addsrc_cell(const SrcArgs& a, const int c) {
   const long long p = a.cell_pos[c];
   float sxx = a.xx[p], syy = a.yy[p], szz = a.zz[p];
   float sxz = a.xz[p], syz = a.yz[p], sxy = a.xy[p];
@@ -331,6 +347,12 @@ __global__ void k_addsrc(const SrcArgs a) {
   a.xz[p] = sxz;
   a.yz[p] = syz;
   a.xy[p] = sxy;
+}
+
+__global__ void k_addsrc(const SrcArgs a) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= a.ncell) return;
+  addsrc_cell(a, c);
 }
 
 // ===========================================================================
@@ -380,12 +402,10 @@ __device__ double iir_step(int order, const double* b, const double* aa, double 
   return y;
 }
 
-__global__ void k_addkinsrc(const KinSrcArgs a) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= a.ncell) return;
+__device__ __forceinline__ void addkinsrc_cell(const KinSrcArgs& a, const int c, const int step) {
   const bool direct = a.cell_pos == nullptr;
   const long long p = direct ? src_cell(a.psrc, c, a.dim, a.slice, a.yline) : a.cell_pos[c];
-  const float atime = a.step * a.dt;
+  const float atime = step * a.dt;
   float sxx = a.xx[p], syy = a.yy[p], szz = a.zz[p];
   float sxz = a.xz[p], syz = a.yz[p], sxy = a.xy[p];
   const int n0 = direct ? 0 : a.cell_first[c], n1 = direct ? 1 : a.cell_first[c + 1];
@@ -430,6 +450,12 @@ __global__ void k_addkinsrc(const KinSrcArgs a) {
   a.xz[p] = sxz;
   a.yz[p] = syz;
   a.xy[p] = sxy;
+}
+
+__global__ void k_addkinsrc(const KinSrcArgs a) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= a.ncell) return;
+  addkinsrc_cell(a, c, a.step);
 }
 
 // ===========================================================================
@@ -839,6 +865,99 @@ inline unsigned cdiv_u(long long a, long long b) { return (unsigned)((a + b - 1)
 }  // namespace
 
 // ===========================================================================
+// Batched instances (many independent simulations, one persistent launch per
+// half-step).  CTAs pull tiles (instance, tile coordinates) from a global
+// counter and run the same per-tile bodies as the one-simulation kernels, so
+// each instance's arithmetic is unchanged.
+// ===========================================================================
+__device__ __forceinline__ int next_tile(int* counter, int* s_tile) {
+  __syncthreads();  // every thread has read the previous tile
+  if (threadIdx.x == 0 && threadIdx.y == 0) *s_tile = atomicAdd(counter, 1);
+  __syncthreads();
+  return *s_tile;
+}
+
+template <int TY>
+__global__ void __launch_bounds__(32 * TY)
+    k_batch_velocity(const BatchInst* __restrict__ inst, const int4* __restrict__ tiles,
+                     const int ntiles, int* counter, const int ichunk) {
+  __shared__ int s_tile;
+  for (;;) {
+    const int t = next_tile(counter, &s_tile);
+    if (t >= ntiles) return;
+    const int4 d = tiles[t];
+    const VelArgs a = inst[d.x].v;
+    vel_tile<TY>(a, d.y, d.z, d.w, ichunk, threadIdx.x, threadIdx.y);
+  }
+}
+
+// Elastic and anelastic instances have separate tile lists and launches, so
+// each launch carries one stress variant (register pressure as k_stress).
+template <bool ELASTIC, int TY>
+__global__ void __launch_bounds__(32 * TY, TY == 8 ? 2 : 1)
+    k_batch_stress(const BatchInst* __restrict__ inst, const int4* __restrict__ tiles,
+                   const int ntiles, int* counter, const int ichunk) {
+  __shared__ int s_tile;
+  for (;;) {
+    const int t = next_tile(counter, &s_tile);
+    if (t >= ntiles) return;
+    const int4 d = tiles[t];
+    const StrArgs& a = inst[d.x].s;  // read in place (dynamically indexed tables)
+    str_tile<ELASTIC, false, TY>(a, d.y, d.z, d.w, ichunk, threadIdx.x, threadIdx.y);
+  }
+}
+
+// Sources of every instance at step *step + 1 (the step being taken), with the
+// schedule of one_step: IFAULT < 4 while the step is below NST, IFAULT 5 always.
+__global__ void k_batch_sources(const BatchInst* __restrict__ inst,
+                                const int2* __restrict__ cells, const int n,
+                                const int* __restrict__ step) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  const int2 e = cells[q];
+  const BatchInst& I = inst[e.x];
+  const int cur = *step + 1;
+  if (I.ifault == 5) {
+    addkinsrc_cell(I.kin, e.y, cur);
+  } else if (I.ifault < 4 && cur < I.nst) {
+    SrcArgs a = I.src;
+    a.tidx = cur;
+    addsrc_cell(a, e.y);
+  }
+}
+
+// Sources of one instance at step *step + 1 read from device memory (replayable
+// graphs): the schedule of one_step, IFAULT < 4 while the step is below NST.
+__global__ void k_addsrc_dev(const SrcArgs a, const int* __restrict__ step, const int nst) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int cur = *step + 1;
+  if (c >= a.ncell || cur >= nst) return;
+  SrcArgs b = a;
+  b.tidx = cur;
+  addsrc_cell(b, c);
+}
+
+__global__ void k_addkinsrc_dev(const KinSrcArgs a, const int* __restrict__ step) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= a.ncell) return;
+  addkinsrc_cell(a, c, *step + 1);
+}
+
+__global__ void k_step_advance(int* step) { *step = *step + 1; }
+
+// Free-surface imaging of every instance (one CTA per (instance, x row)); the
+// first thread then advances the batch's step counter.
+__global__ void k_batch_fstr(const BatchInst* __restrict__ inst, const int2* __restrict__ rows,
+                             const int n, int* step) {
+  for (int r = blockIdx.x; r < n; r += gridDim.x) {
+    const int2 e = rows[r];
+    const FstrArgs& a = inst[e.x].f;
+    for (int j = a.j0 + threadIdx.x; j <= a.j1; j += blockDim.x) fstr_cell(a, e.y, j);
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) *step = *step + 1;
+}
+
+// ===========================================================================
 // launchers
 // ===========================================================================
 cudaError_t awp_launch_velocity(const VelArgs& a, cudaStream_t st) {
@@ -971,5 +1090,60 @@ cudaError_t awp_launch_anynonzero(const float* p, long long n, unsigned int* fla
 cudaError_t awp_launch_nonfinite(const float* p, long long n, unsigned int* flag,
                                  cudaStream_t st) {
   k_nonfinite<<<148 * 8, 256, 0, st>>>(p, n, flag);
+  return cudaGetLastError();
+}
+
+int awp_batch_blocks_per_sm(int ty, int* vel, int* str) {
+  cudaError_t e;
+  if (ty == 8) {
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(vel, k_batch_velocity<8>, 256, 0);
+    if (e == cudaSuccess)
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(str, k_batch_stress<false, 8>, 256, 0);
+  } else if (ty == 4) {
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(vel, k_batch_velocity<4>, 128, 0);
+    if (e == cudaSuccess)
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(str, k_batch_stress<false, 4>, 128, 0);
+  } else {
+    return 1;
+  }
+  return e == cudaSuccess ? 0 : 2;
+}
+
+template <int TY>
+static void launch_batch_halfsteps(const BatchLaunch& b, cudaStream_t st) {
+  const dim3 block(32, TY);
+  k_batch_velocity<TY><<<b.grid_vel, block, 0, st>>>(b.inst, b.vtiles, b.nvtiles, b.counters,
+                                                     b.ichunk);
+  if (b.nstiles > 0)
+    k_batch_stress<false, TY><<<b.grid_str, block, 0, st>>>(b.inst, b.stiles, b.nstiles,
+                                                            b.counters + 1, b.ichunk);
+  if (b.nstiles_el > 0)
+    k_batch_stress<true, TY><<<b.grid_str, block, 0, st>>>(b.inst, b.stiles_el, b.nstiles_el,
+                                                           b.counters + 2, b.ichunk);
+}
+
+cudaError_t awp_launch_batch_step(const BatchLaunch& b, cudaStream_t st) {
+  cudaError_t e = cudaMemsetAsync(b.counters, 0, 3 * sizeof(int), st);
+  if (e != cudaSuccess) return e;
+  if (b.ty == 8)
+    launch_batch_halfsteps<8>(b, st);
+  else
+    launch_batch_halfsteps<4>(b, st);
+  if (b.nsrc > 0)
+    k_batch_sources<<<cdiv_u(b.nsrc, 128), 128, 0, st>>>(b.inst, b.src_cells, b.nsrc, b.step);
+  k_batch_fstr<<<b.nrows > 0 ? b.nrows : 1, 128, 0, st>>>(b.inst, b.rows, b.nrows, b.step);
+  return cudaGetLastError();
+}
+
+cudaError_t awp_launch_sources_dev(const SrcArgs* a, const KinSrcArgs* k, const int* step,
+                                   int nst, cudaStream_t st) {
+  if (a && a->ncell > 0)
+    k_addsrc_dev<<<cdiv_u(a->ncell, 128), 128, 0, st>>>(*a, step, nst);
+  if (k && k->ncell > 0) k_addkinsrc_dev<<<cdiv_u(k->ncell, 128), 128, 0, st>>>(*k, step);
+  return cudaGetLastError();
+}
+
+cudaError_t awp_launch_step_advance(int* step, cudaStream_t st) {
+  k_step_advance<<<1, 1, 0, st>>>(step);
   return cudaGetLastError();
 }

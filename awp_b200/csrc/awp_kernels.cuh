@@ -179,3 +179,43 @@ cudaError_t awp_launch_anynonzero(const float* p, long long n, unsigned int* fla
                                   cudaStream_t st);
 cudaError_t awp_launch_nonfinite(const float* p, long long n, unsigned int* flag,
                                  cudaStream_t st);
+
+// ---------------------------------------------------------------------------
+// Batched instances: the per-step launches of many independent single-grid
+// simulations (awp_batch_* of the C ABI).  Each instance carries the argument
+// blocks its one-simulation launches would take; tiles index into them.
+// ---------------------------------------------------------------------------
+struct BatchInst {
+  VelArgs v;
+  StrArgs s;
+  FstrArgs f;
+  SrcArgs src;
+  KinSrcArgs kin;
+  int elastic;  // stress without memory variables (Q^-1 == 0)
+  int ifault, nst;
+};
+
+struct BatchLaunch {
+  const BatchInst* inst;
+  const int4* vtiles;  // (instance, tile x, tile y, tile z) of the velocity launch
+  const int4* stiles;     // same for the stress launch of the anelastic instances
+  const int4* stiles_el;  // ... and of the elastic ones
+  const int2* src_cells;  // (instance, source cell)
+  const int2* rows;       // (instance, padded x index) of the free-surface rows
+  int nvtiles, nstiles, nstiles_el, nsrc, nrows;
+  int* counters;  // [3] tile counters (reset by the launcher)
+  int* step;      // steps taken so far (advanced on the device)
+  int ty, ichunk, grid_vel, grid_str;
+};
+
+// One time step of every instance: velocity, stress (anelastic, elastic),
+// sources, free-surface images and the step counter; a 12-byte memset and up
+// to five kernels, all capturable in a CUDA graph.
+cudaError_t awp_launch_batch_step(const BatchLaunch& b, cudaStream_t st);
+// Resident CTAs per SM of the persistent kernels for tiles 32 x ty (ty = 4, 8).
+int awp_batch_blocks_per_sm(int ty, int* vel, int* str);
+// Sources of one instance at the step held in device memory (*step + 1), for
+// graphs replayed step after step; either argument block may be null.
+cudaError_t awp_launch_sources_dev(const SrcArgs* a, const KinSrcArgs* k, const int* step,
+                                   int nst, cudaStream_t st);
+cudaError_t awp_launch_step_advance(int* step, cudaStream_t st);

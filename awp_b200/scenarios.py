@@ -170,6 +170,25 @@ def random_small(nx=24, ny=20, nz=32, h=100.0, dt=0.004, steps=20, seed=7, nvar=
                     f"random {nx}x{ny}x{nz} nvar={nvar} q={q} ifault={ifault}")
 
 
+def batch_ensemble(n=96, seed=6, steps=1000, lo=(64, 64, 64), hi=(256, 256, 128), h=100.0,
+                   dt=0.004):
+    """An ensemble of independent simulations of uneven sizes for the batched
+    path: grid sizes drawn from `seed` uniformly between `lo` and `hi` (nz a
+    multiple of 4), each with its own seeded random anelastic medium and a
+    random moment-tensor point source (IFAULT 1, seeded moment-rate samples)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for q in range(n):
+        nx = int(rng.integers(lo[0], hi[0] + 1))
+        ny = int(rng.integers(lo[1], hi[1] + 1))
+        nz = int(rng.integers(lo[2] // 4, hi[2] // 4 + 1)) * 4
+        sc = random_small(nx=nx, ny=ny, nz=nz, h=h, dt=dt, steps=steps, seed=seed * 1000 + q,
+                          q=True, ifault=1, nsrc=1)
+        sc.name = f"batch_{q}"
+        out.append(sc)
+    return out
+
+
 def dm_small(nxc=10, nyc=8, nzs=(36, 24), h_coarse=150.0, dt=0.004, steps=12, q=True, seed=31,
              nsrc=1):
     """A discontinuous mesh of len(nzs) blocks for parity tests: block p has

@@ -259,3 +259,73 @@ class Mesh:
             self.close()
         except Exception:
             pass
+
+
+class Batch:
+    """Many independent single-grid simulations advanced together
+    (awp_batch_*): one persistent launch per half-step over the tiles of every
+    instance, the step replayed as a CUDA graph.  ``solvers`` are ordinary
+    Solvers set up as for ``step``; keep them alive while the batch lives."""
+
+    def __init__(self, solvers):
+        self.lib = _lib.load()
+        self.solvers = list(solvers)
+        n = len(self.solvers)
+        arr = (c_void_p * n)(*[s.ctx for s in self.solvers])
+        b = c_void_p()
+        check(self.lib.awp_batch_create(arr, n, byref(b)), "awp_batch_create")
+        self.batch = b
+
+    def step(self, n: int = 1) -> None:
+        check(self.lib.awp_batch_step(self.batch, int(n)), "awp_batch_step")
+
+    def synchronize(self) -> None:
+        check(self.lib.awp_batch_synchronize(self.batch), "awp_batch_synchronize")
+
+    def set_shape(self, ty: int, ichunk: int) -> None:
+        check(self.lib.awp_batch_set_shape(self.batch, int(ty), int(ichunk)),
+              "awp_batch_set_shape")
+
+    @property
+    def shape(self) -> tuple[int, int]:
+        ty, ich = c_int(), c_int()
+        check(self.lib.awp_batch_get_shape(self.batch, byref(ty), byref(ich)),
+              "awp_batch_get_shape")
+        return ty.value, ich.value
+
+    def set_graph(self, use_graph: bool) -> None:
+        check(self.lib.awp_batch_set_graph(self.batch, int(bool(use_graph))),
+              "awp_batch_set_graph")
+
+    def set_mode(self, mode: int) -> None:
+        """0: persistent tile-queue launches; 1: graph of each instance's own
+        launches as parallel branches."""
+        check(self.lib.awp_batch_set_mode(self.batch, int(mode)), "awp_batch_set_mode")
+
+    @property
+    def mode(self) -> int:
+        return self.lib.awp_batch_get_mode(self.batch)
+
+    def info(self) -> dict:
+        v = (c_longlong * 6)()
+        check(self.lib.awp_batch_info(self.batch, v), "awp_batch_info")
+        keys = ("instances", "cells", "velocity_tiles", "stress_tiles", "grid_velocity",
+                "grid_stress")
+        return dict(zip(keys, (int(x) for x in v)))
+
+    def close(self) -> None:
+        if getattr(self, "batch", None):
+            self.lib.awp_batch_destroy(self.batch)
+            self.batch = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

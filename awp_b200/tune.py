@@ -59,3 +59,33 @@ def autotune(solver, steps: int = 3) -> dict:
     for k, v in chosen.items():
         set_tuning(lib, k, v)
     return {"chosen": chosen, "table": table}
+
+
+BATCH_CANDIDATES = {"ty": (8, 4), "ichunk": (8, 16, 32)}
+
+
+def autotune_batch(batch, steps: int = 3, timer=None) -> dict:
+    """Pick the batched execution: the persistent tile-queue mode with its
+    tile shape (ty j rows x ichunk x planes, threads per CTA = 32 ty), or the
+    graph of the instances' own launches, by timing `steps` batched steps per
+    candidate (advancing the instances); `timer(fn)` returns the milliseconds
+    fn takes.  No choice changes results (each cell is computed by the same
+    expression)."""
+    table = []
+    batch.set_mode(0)
+    for ty, ich in itertools.product(*BATCH_CANDIDATES.values()):
+        batch.set_shape(ty, ich)
+        batch.step(1)  # build the tile lists and the graph
+        batch.synchronize()
+        ms = timer(lambda: batch.step(steps))
+        table.append({"mode": 0, "ty": ty, "ichunk": ich, "ms_per_step": ms / steps})
+    batch.set_mode(1)
+    batch.step(1)
+    batch.synchronize()
+    ms = timer(lambda: batch.step(steps))
+    table.append({"mode": 1, "ty": None, "ichunk": None, "ms_per_step": ms / steps})
+    best = min(table, key=lambda r: r["ms_per_step"])
+    batch.set_mode(best["mode"])
+    if best["mode"] == 0:
+        batch.set_shape(best["ty"], best["ichunk"])
+    return {"chosen": {k: best[k] for k in ("mode", "ty", "ichunk")}, "table": table}

@@ -427,13 +427,114 @@ def run_reference(args, rank) -> dict | None:
                     "restatement of the same kernels (oracle/awp_oracle.cpp) on the host cores"}
 
 
+def run_batched(args) -> dict:
+    """Batched ensemble: the same instances advanced (a) by the plain path,
+    one context per simulation, each on its own stream (so independent
+    simulations may overlap on the GPU), and (b) by awp_batch_step (persistent
+    tile-queue launches, one CUDA graph per step).  Both timed on the device
+    with CUDA events; value = batched Gcell-updates/s."""
+    import torch
+    from awp_b200 import Batch, Solver, default_params, scenarios, tune
+
+    ens = scenarios.batch_ensemble(n=args.batch_n, seed=6, steps=args.steps + args.warmup + 64)
+    cells = sum(sc.params["nx"] * sc.params["ny"] * sc.params["nz"] for sc in ens)
+    root = torch.cuda.Stream()
+    streams = [torch.cuda.Stream() for _ in ens]
+    solvers = []
+    for sc, st in zip(ens, streams):
+        s = Solver(default_params(**sc.params), stream=st.cuda_stream)
+        s.upload_media(sc.media)
+        s.upload_sources(sc.src_pos, sc.src_data)
+        solvers.append(s)
+    torch.cuda.synchronize()
+
+    def timed(fn):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(root)
+        for st in streams:
+            st.wait_event(e0)
+        fn()
+        for st in streams:
+            root.wait_stream(st)
+        e1.record(root)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    def plain(k):
+        for s in solvers:
+            s.step(k)
+
+    def plain_seq(k):  # one simulation after another
+        for q, s in enumerate(solvers):
+            if q:
+                streams[q].wait_stream(streams[q - 1])
+            s.step(k)
+
+    timed(lambda: plain(args.warmup))
+    sampler = ClockSampler(torch.cuda.current_device())
+    sampler.start()
+    ms_plain = timed(lambda: plain(args.steps))
+    ms_seq = timed(lambda: plain_seq(args.steps))
+    launches_plain = sum(s.kernel_launches for s in solvers)
+
+    b = Batch(solvers)
+    tuning = tune.autotune_batch(b, steps=3, timer=timed)
+    b.step(args.warmup)
+    b.synchronize()
+    l0 = sum(s.kernel_launches for s in solvers)
+    ms_batch = timed(lambda: b.step(args.steps))
+    launches_batch = sum(s.kernel_launches for s in solvers) - l0
+    clocks = sampler.stop()
+    info = b.info()
+    ok = all(s.check_finite() for s in solvers)
+    b.close()
+    for s in solvers:
+        s.close()
+    hbm, peak_kind = peaks()
+    v_b = cells * args.steps / (ms_batch * 1e-3) / 1e9
+    v_p = cells * args.steps / (ms_plain * 1e-3) / 1e9
+    v_s = cells * args.steps / (ms_seq * 1e-3) / 1e9
+    step_bw = 140 * cells / (ms_batch / args.steps * 1e-3) / 1e9
+    sizes = [[sc.params["nx"], sc.params["ny"], sc.params["nz"]] for sc in ens]
+    return {
+        "metric": "batched vs plain Gcell-updates/s (ensemble of uneven grids) on 1 B200",
+        "value": v_b, "unit": "Gcell-updates/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_batch / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+        "config": {"workload": f"batched ensemble of {len(ens)} anelastic grids",
+                   "sizes_drawn": "nx, ny in [64, 256], nz in [64, 128] (seed 6)",
+                   "cells": cells, "instances": len(ens), "first_sizes": sizes[:8],
+                   "l2": "working set of tens of GB >> 126 MB L2, no flush needed",
+                   "finite_after_run": ok},
+        "plain": {"value": v_s, "ms_per_step": ms_seq / args.steps,
+                  "kernel_launches_per_step": launches_plain / max(2 * args.steps + args.warmup, 1),
+                  "mode": "one context per simulation, the simulations one after another"},
+        "plain_concurrent": {"value": v_p, "ms_per_step": ms_plain / args.steps,
+                             "mode": "one context per simulation, each on its own stream, "
+                                     "all enqueued together (the GPU overlaps them)"},
+        "batched_over_plain": v_b / v_s,
+        "batched_over_plain_concurrent": v_b / v_p,
+        "batch": {"tuning": tuning["chosen"], "tuning_table": tuning["table"], **info,
+                  "graph": True},
+        "step_roofline": {"bytes_per_cell_alg": 140, "achieved": step_bw, "peak": hbm,
+                          "unit": "GB/s", "frac": step_bw / hbm,
+                          "peak_kind": f"{peak_kind} hbm_gbs"},
+        "clocks": clocks,
+        "gpu_launches": launches_batch,
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", default="layered_vk", choices=["layered_vk", "halfspace"])
+    ap.add_argument("--workload", default="layered_vk",
+                    choices=["layered_vk", "halfspace", "batched"])
+    ap.add_argument("--batch-n", type=int, default=96,
+                    help="instances of the batched ensemble (--workload batched)")
     ap.add_argument("--topography", action="store_true",
                     help="curvilinear top grid (INTOPO) on the same workload")
     ap.add_argument("--no-e2e", action="store_true")
@@ -455,6 +556,8 @@ def main():
     dist = None
     if args.impl == "reference":
         line = run_reference(args, rank)
+    elif args.workload == "batched":
+        line = run_batched(args) if rank == 0 else None
     else:
         if world > 1:
             import datetime

@@ -197,6 +197,40 @@ int awp_mesh_grid(awp_mesh* mesh, int p, awp_ctx** ctx);
 int awp_mesh_step(awp_mesh* mesh, int nsteps);
 int awp_mesh_synchronize(awp_mesh* mesh);
 
+/* ------------------------------------------------------------------------ */
+/* Batched instances: many independent single-grid simulations of uneven     */
+/* sizes (source ensembles, shots) advanced together.                        */
+/* ------------------------------------------------------------------------ */
+typedef struct awp_batch awp_batch;
+/* The instances are ordinary contexts, set up as for awp_step (media,
+ * sources); single grid, Cartesian, NVE 1/2, no receivers or SOURCEFILE
+ * (AWP_ERR_UNSUPPORTED otherwise), all at the same step.  The batch keeps
+ * pointers to them; destroy the batch before its contexts. */
+int awp_batch_create(awp_ctx* const* ctxs, int n, awp_batch** out);
+int awp_batch_destroy(awp_batch* batch);
+/* Advance every instance nsteps, each step one persistent launch per
+ * half-step over a tile queue of all instances (CTAs pull 32 k x ty j x ichunk
+ * i tiles from a global counter), then the sources and free-surface images of
+ * all instances; the step is one CUDA graph replayed nsteps times.  Each
+ * instance's arithmetic is that of awp_step, bit for bit.  Ordered after
+ * earlier work on the contexts' streams and before later work on them. */
+int awp_batch_step(awp_batch* batch, int nsteps);
+int awp_batch_synchronize(awp_batch* batch);
+/* Tile shape (ty = 4 or 8 j rows, ichunk x planes per tile; default 8, 16)
+ * and graph replay (1, default) or direct launches (0). */
+int awp_batch_set_shape(awp_batch* batch, int ty, int ichunk);
+int awp_batch_get_shape(const awp_batch* batch, int* ty, int* ichunk);
+int awp_batch_set_graph(awp_batch* batch, int use_graph);
+/* Execution mode: 0 (default) the persistent tile-queue launches above;
+ * 1 one graph per step whose parallel branches are each instance's own tuned
+ * launches (velocity, stress, sources at the device-held step, free-surface
+ * images), the step counter advanced after the join.  Same results. */
+int awp_batch_set_mode(awp_batch* batch, int mode);
+int awp_batch_get_mode(const awp_batch* batch);
+/* info = instances, interior cells, velocity tiles, stress tiles, persistent
+ * CTAs of the velocity and stress launches. */
+int awp_batch_info(awp_batch* batch, long long info[6]);
+
 /* Host-only helper (no context, no GPU): the metric arrays of a topography
  * file (INTOPO) for an nx x ny x nz grid of spacing h, as topo_init_metrics /
  * topo_init_geometry / topo_build compute them (src/topography/topography.c:
