@@ -127,6 +127,11 @@ def load() -> ctypes.CDLL:
     _sig(lib, "awp_sourcefile_init", c_int, [_P, c_char_p])
     _sig(lib, "awp_topo_metrics", c_int, [c_char_p, c_int, c_int, c_int, c_float, _F])
     _sig(lib, "awp_topography_init", c_int, [_P, c_char_p])
+    _sig(lib, "awp_set_moduli", c_int, [_P, _F, _F, _F])
+    _sig(lib, "awp_reset", c_int, [_P])
+    _sig(lib, "awp_seismograms", c_int, [_P, c_int, c_int, _I, _I, _F])
+    _sig(lib, "awp_misfit_gradient", c_int,
+         [_P, c_int, c_int, _I, _I, _F, c_int, POINTER(c_double), _F, _F, _F, _F])
     _sig(lib, "awp_input_read", c_int,
          [c_char_p, POINTER(c_longlong), c_char_p, c_int, _F, _F, _F, _I, c_longlong])
     _sig(lib, "awp_point_coefs", c_int,

@@ -1,0 +1,98 @@
+"""Seismogram misfit and its material gradient through the C ABI.
+
+``misfit_gradient`` runs the checkpointed forward / discrete-adjoint pair of
+``awp_misfit_gradient`` (include/awp_b200.h); ``Misfit`` wraps it as a
+``torch.autograd.Function`` of the Lame moduli and the density, so a model
+held as torch tensors can be optimised with torch's optimisers.  Receivers
+are velocity samples at interior cells: ``rec_xyz`` [nrec][3] = (x, y, z) with
+z counted from the surface, ``rec_comp`` [nrec] = 0 (vx), 1 (vy), 2 (vz).
+Model arrays are [nz][ny][nx], surface first (the mesh-file order).
+"""
+from __future__ import annotations
+
+import ctypes
+from ctypes import byref, c_double
+
+import numpy as np
+
+from ._lib import check
+
+_F = ctypes.POINTER(ctypes.c_float)
+_I = ctypes.POINTER(ctypes.c_int)
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, np.float32)
+
+
+def _i32(a):
+    return np.ascontiguousarray(a, np.int32)
+
+
+def seismograms(solver, nsteps: int, rec_xyz, rec_comp) -> np.ndarray:
+    """nsteps forward steps from the solver's current state; samples
+    [nsteps][nrec] taken after each step."""
+    xyz, comp = _i32(rec_xyz).reshape(-1, 3), _i32(rec_comp).reshape(-1)
+    out = np.zeros((nsteps, comp.size), np.float32)
+    check(solver.lib.awp_seismograms(solver.ctx, int(nsteps), comp.size, xyz.ctypes.data_as(_I),
+                                     comp.ctypes.data_as(_I), out.ctypes.data_as(_F)),
+          "awp_seismograms")
+    return out
+
+
+def misfit_gradient(solver, nsteps: int, rec_xyz, rec_comp, d_obs, nsnap: int = 0):
+    """J = 1/2 sum (seis - d_obs)^2 over nsteps steps from the solver's current
+    state, and dJ/dlambda, dJ/dmu, dJ/drho ([nz][ny][nx]).  Returns
+    (J, seis, g_lambda, g_mu, g_rho)."""
+    xyz, comp = _i32(rec_xyz).reshape(-1, 3), _i32(rec_comp).reshape(-1)
+    d = _f32(d_obs).reshape(nsteps, comp.size)
+    p = solver.params
+    shape = (p.nz, p.ny, p.nx)
+    seis = np.zeros((nsteps, comp.size), np.float32)
+    g = [np.zeros(shape, np.float32) for _ in range(3)]
+    J = c_double()
+    check(solver.lib.awp_misfit_gradient(solver.ctx, int(nsteps), comp.size,
+                                         xyz.ctypes.data_as(_I), comp.ctypes.data_as(_I),
+                                         d.ctypes.data_as(_F), int(nsnap), byref(J),
+                                         seis.ctypes.data_as(_F),
+                                         *[x.ctypes.data_as(_F) for x in g]),
+          "awp_misfit_gradient")
+    return J.value, seis, g[0], g[1], g[2]
+
+
+def _autograd_function():
+    import torch
+
+    class Misfit(torch.autograd.Function):
+        """J(lambda, mu, rho) of one shot: set the model, reset the wavefield,
+        run forward and adjoint; backward returns the stored gradients."""
+
+        @staticmethod
+        def forward(ctx, lam, mu, rho, solver, nsteps, rec_xyz, rec_comp, d_obs, nsnap=0):
+            solver.set_moduli(lam.detach().cpu().numpy(), mu.detach().cpu().numpy(),
+                              rho.detach().cpu().numpy())
+            solver.reset()
+            J, _, gl, gm, gr = misfit_gradient(solver, nsteps, rec_xyz, rec_comp, d_obs, nsnap)
+            dev = lam.device
+            ctx.save_for_backward(torch.from_numpy(gl).to(dev), torch.from_numpy(gm).to(dev),
+                                  torch.from_numpy(gr).to(dev))
+            return torch.tensor(J, dtype=torch.float64, device=dev)
+
+        @staticmethod
+        def backward(ctx, gJ):
+            gl, gm, gr = ctx.saved_tensors
+            s = gJ.to(gl.dtype)
+            return s * gl, s * gm, s * gr, None, None, None, None, None, None
+
+    return Misfit
+
+
+_MISFIT = None
+
+
+def misfit(lam, mu, rho, solver, nsteps, rec_xyz, rec_comp, d_obs, nsnap: int = 0):
+    """Differentiable misfit of torch tensors lam, mu, rho ([nz][ny][nx])."""
+    global _MISFIT
+    if _MISFIT is None:
+        _MISFIT = _autograd_function()
+    return _MISFIT.apply(lam, mu, rho, solver, nsteps, rec_xyz, rec_comp, d_obs, nsnap)

@@ -1,0 +1,518 @@
+// Discrete adjoint of the single-grid time step and the material gradient of
+// a seismogram misfit.
+//
+// The forward step (one_step: dvelcx, dstrqc with its free-surface velocity
+// images, point sources, fstr) is linear in the wavefield state for fixed
+// materials, so its adjoint is the transpose of each map in reverse order:
+//
+//   fstr^T -> stress^T (memory variables, strain rates, then the images) ->
+//   velocity^T
+//
+// Every transpose is written in gather form (each thread owns one output
+// cell and reads the neighbours whose forward stencils touched it), so no
+// atomics are needed and the result is deterministic.  The gradient terms use
+// the forward state of the same step (stresses before it for the density
+// term, velocities after it for the moduli terms).  Derivation, per map:
+//
+//   velocity  u' = (u + fd(rho) * D(sigma)) * dc          (dvelcx, kernel.cu:222-253)
+//   stress    s' = K (s + P(e) + a r + DT (Q(e)(w-1) + g r)),  r' = b r + w Q(e)
+//             (yy, zz carry K twice; dstrqc, kernel.cu:1114-1179)
+//   images    u(top+1) = u - (w - w_{i-1}), v(top+1) = v - (w_{j+1} - w),
+//             w(top+1) = w(top-1) - lam_mu * Z(u, v, w)     (kernel.cu:1087-1112)
+//   fstr      zz(top+1) = -zz(top), ..., xz(top) = yz(top) = 0  (kernel.cu:1616-1647)
+#include "awp_adjoint.cuh"
+
+#include "awp_stencil.cuh"
+
+namespace {
+
+enum { LU, LV, LW, LXX, LYY, LZZ, LXY, LXZ, LYZ, LR1, LR2, LR3, LR4, LR5, LR6 };
+enum { E1, E2, E3, E4, E5, E6, GL8, GM8, GP1, GP2, GP3 };
+enum { VA, VB, VC, VEA, VEB, VEC };
+
+// ---------------------------------------------------------------------------
+// fstr^T over the imaged columns (i, j) of the top layer
+// ---------------------------------------------------------------------------
+__global__ void k_adj_fstr(const AdjArgs a) {
+  const int j = a.sj0 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = a.si0 + blockIdx.y;
+  if (j > a.fj1 || i > a.si1) return;
+  const long long p = (long long)i * a.g.slice + (long long)j * a.g.yline + a.g.top();
+  float* zz = a.L[LZZ];
+  float* xz = a.L[LXZ];
+  float* yz = a.L[LYZ];
+  // forward: zz(t+1) = -zz(t); zz(t+2) = -zz(t-1); xz(t+1) = -xz(t-1);
+  // xz(t+2) = -xz(t-2); yz likewise; xz(t) = yz(t) = 0
+  zz[p] -= zz[p + 1];
+  zz[p - 1] -= zz[p + 2];
+  zz[p + 1] = 0.f;
+  zz[p + 2] = 0.f;
+  xz[p - 1] -= xz[p + 1];
+  xz[p - 2] -= xz[p + 2];
+  xz[p] = 0.f;
+  xz[p + 1] = 0.f;
+  xz[p + 2] = 0.f;
+  yz[p - 1] -= yz[p + 1];
+  yz[p - 2] -= yz[p + 2];
+  yz[p] = 0.f;
+  yz[p + 1] = 0.f;
+  yz[p + 2] = 0.f;
+}
+
+// ---------------------------------------------------------------------------
+// stress^T, pointwise part: memory variables and stresses in place, adjoint
+// strain rates and the material weights of the cell into E[]
+// ---------------------------------------------------------------------------
+template <bool ELASTIC>
+__global__ void k_adj_stress_cell(const AdjArgs a) {
+  const int k = a.sk0 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = a.sj0 + blockIdx.y;
+  const int i = a.si0 + blockIdx.z;
+  if (k > a.sk1 || j > a.sj1 || i > a.si1) return;
+  const long long S = a.g.slice, Y = a.g.yline;
+  const long long p = (long long)i * S + (long long)j * Y + k;
+  const float c1 = a.c1, c2 = a.c2, DT = a.dt;
+
+  // forward strain rates from the velocities after the step
+  const float* u = a.fu;
+  const float* v = a.fv;
+  const float* w = a.fw;
+  const float vs1 = c1 * (u[p + S] - u[p]) + c2 * (u[p + 2 * S] - u[p - S]);
+  const float vs2 = c1 * (v[p] - v[p - Y]) + c2 * (v[p + Y] - v[p - 2 * Y]);
+  const float vs3 = c1 * (w[p] - w[p - 1]) + c2 * (w[p + 1] - w[p - 2]);
+  const float e4 = c1 * (u[p + Y] - u[p]) + c2 * (u[p + 2 * Y] - u[p - Y]) +
+                   c1 * (v[p] - v[p - S]) + c2 * (v[p + S] - v[p - 2 * S]);
+  const float e5 = c1 * (u[p + 1] - u[p]) + c2 * (u[p + 2] - u[p - 1]) +
+                   c1 * (w[p] - w[p - S]) + c2 * (w[p + S] - w[p - 2 * S]);
+  const float e6 = c1 * (v[p + 1] - v[p]) + c2 * (v[p + 2] - v[p - 1]) +
+                   c1 * (w[p + Y] - w[p]) + c2 * (w[p + 2 * Y] - w[p - Y]);
+
+  // materials of the cell (kernel.cu:962-1070)
+  auto sum8 = [&](const float* m) {
+    return m[p] + m[p + S] + m[p - Y] + m[p + S - Y] + m[p - 1] + m[p + S - 1] + m[p - Y - 1] +
+           m[p + S - Y - 1];
+  };
+  const float L8 = sum8(a.lam), M8 = sum8(a.mu);
+  const float P1 = a.mu[p] + a.mu[p - 1], P2 = a.mu[p] + a.mu[p - Y], P3 = a.mu[p] + a.mu[p + S];
+  const float xm_raw = 16.0f / M8;
+  const float xl_raw = 8.0f / L8 + xm_raw;
+  const float m1_raw = 2.0f / P1, m2_raw = 2.0f / P2, m3_raw = 2.0f / P3;
+  const int t = awp_tex_index(a.tex, i, j, k);
+  const float fvx1 = a.tex.tau1[t], fvx2 = a.tex.tau2[t], wwo = a.tex.wwo8[t];
+  float c_xm = a.dth, c_h = 0.f, c_q = 0.f, c_m[3] = {a.dth, a.dth, a.dth}, c_hh[3] = {0, 0, 0};
+  if (!ELASTIC) {
+    const float cc0 = a.coeff[2 * t], cc1 = a.coeff[2 * t + 1];
+    const float hw = awp_qf_weight(0.0625f * sum8(a.qs), wwo, cc0, cc1, a.qthr);
+    const float qpaw = awp_qf_weight(0.0625f * sum8(a.qp), wwo, cc0, cc1, a.qthr);
+    const float hiw[3] = {awp_qf_weight(0.25f * (a.qs[p] + a.qs[p - 1]), wwo, cc0, cc1, a.qthr),
+                          awp_qf_weight(0.25f * (a.qs[p] + a.qs[p - Y]), wwo, cc0, cc1, a.qthr),
+                          awp_qf_weight(0.25f * (a.qs[p] + a.qs[p + S]), wwo, cc0, cc1, a.qthr)};
+    c_h = -hw * a.dh1 * fvx1;
+    c_xm = a.dth + DT * c_h;
+    c_q = -qpaw * a.dh1 * fvx1;
+    for (int q = 0; q < 3; ++q) {
+      c_hh[q] = -hiw[q] * a.dh1 * fvx1;
+      c_m[q] = a.dth + DT * c_hh[q];
+    }
+  }
+  const float xm = xm_raw * c_xm, h = xm_raw * c_h, xl = xl_raw * a.dth, qpa = xl_raw * c_q;
+  const float xmu[3] = {m1_raw * c_m[0], m2_raw * c_m[1], m3_raw * c_m[2]};
+  const float hh[3] = {m1_raw * c_hh[0], m2_raw * c_hh[1], m3_raw * c_hh[2]};
+  const float K = a.dcrjx[i] * a.dcrjy[j] * a.dcrjz[k];
+  const float al = DT * (1.0f + fvx2 * fvx1);   // coefficient of r in sigma
+  const float be = fvx2, ga = fvx2 * (1.0f - fvx1);
+
+  float* L = nullptr;
+  // normal components
+  float PX, PY, PZ, QX = 0.f, QY = 0.f, QZ = 0.f;
+  {
+    L = a.L[LXX];
+    const float lx = L[p];
+    PX = K * lx;
+    L[p] = K * lx;
+    L = a.L[LYY];
+    const float ly = L[p];
+    PY = K * K * ly;
+    L[p] = K * K * ly;
+    L = a.L[LZZ];
+    const float lz = L[p];
+    PZ = K * K * lz;
+    L[p] = K * K * lz;
+    if (!ELASTIC) {
+      float* R1 = a.L[LR1];
+      float* R2 = a.L[LR2];
+      float* R3 = a.L[LR3];
+      const float r1 = R1[p], r2 = R2[p], r3 = R3[p];
+      QX = DT * (wwo - 1.0f) * K * lx + wwo * r1;
+      QY = DT * (wwo - 1.0f) * K * ly + wwo * r2;
+      QZ = DT * (wwo - 1.0f) * K * lz + wwo * r3;
+      R1[p] = (al + DT * ga) * K * lx + be * r1;
+      R2[p] = al * K * K * ly + DT * ga * K * ly + be * r2;
+      R3[p] = al * K * K * lz + DT * ga * K * lz + be * r3;
+    }
+  }
+  const float sP = PX + PY + PZ, sQ = QX + QY + QZ;
+  const float A = xl + DT * qpa;
+  const float s123 = vs1 + vs2 + vs3;
+  float* const* E = a.E;
+  E[E1][p] = A * sP - xm * (PY + PZ) + qpa * sQ - h * (QY + QZ);
+  E[E2][p] = A * sP - xm * (PX + PZ) + qpa * sQ - h * (QX + QZ);
+  E[E3][p] = A * sP - xm * (PX + PY) + qpa * sQ - h * (QX + QY);
+  const float G_xl = s123 * sP;
+  const float G_qpa = DT * s123 * sP + s123 * sQ;
+  const float G_xm = -((vs2 + vs3) * PX + (vs1 + vs3) * PY + (vs1 + vs2) * PZ);
+  const float G_h = -((vs2 + vs3) * QX + (vs1 + vs3) * QY + (vs1 + vs2) * QZ);
+
+  // shear components
+  const float es[3] = {e4, e5, e6};
+  const int ls[3] = {LXY, LXZ, LYZ}, lr[3] = {LR4, LR5, LR6};
+  float GP[3];
+  for (int q = 0; q < 3; ++q) {
+    float* Ls = a.L[ls[q]];
+    const float l = Ls[p];
+    Ls[p] = K * l;
+    float lrv = 0.f;
+    if (!ELASTIC) {
+      float* Rq = a.L[lr[q]];
+      lrv = Rq[p];
+      Rq[p] = (al + DT * ga) * K * l + be * lrv;
+    }
+    E[E4 + q][p] = (xmu[q] + DT * hh[q] * (wwo - 1.0f)) * K * l + wwo * hh[q] * lrv;
+    const float G_xmu = es[q] * K * l;
+    const float G_hq = es[q] * (DT * (wwo - 1.0f) * K * l + wwo * lrv);
+    const float Pq = q == 0 ? P1 : (q == 1 ? P2 : P3);
+    GP[q] = -2.0f / (Pq * Pq) * (G_xmu * c_m[q] + G_hq * c_hh[q]);
+  }
+  // chain to the eight-cell sums
+  const float G_xlraw = G_xl * a.dth + G_qpa * c_q;
+  const float G_xmraw = G_xm * c_xm + G_h * c_h + G_xlraw;
+  E[GL8][p] = -8.0f / (L8 * L8) * G_xlraw;
+  E[GM8][p] = -16.0f / (M8 * M8) * G_xmraw;
+  E[GP1][p] = GP[0];
+  E[GP2][p] = GP[1];
+  E[GP3][p] = GP[2];
+}
+
+// ---------------------------------------------------------------------------
+// stress^T, gather part: adjoint strain rates -> adjoint velocities (images
+// and the untouched k = top+2 values included); material weights -> the
+// gradients of 1/lambda and 1/mu
+// ---------------------------------------------------------------------------
+__global__ void k_adj_stress_gather(const AdjArgs a) {
+  const int k = a.sk0 - 2 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = a.sj0 - 2 + blockIdx.y;
+  const int i = a.si0 - 2 + blockIdx.z;
+  if (k > a.sk1 + 2 || j > a.sj1 + 2 || i > a.si1 + 2) return;
+  const long long S = a.g.slice, Y = a.g.yline;
+  const long long q = (long long)i * S + (long long)j * Y + k;
+  const float c1 = a.c1, c2 = a.c2;
+  const float* e1 = a.E[E1];
+  const float* e2 = a.E[E2];
+  const float* e3 = a.E[E3];
+  const float* e4 = a.E[E4];
+  const float* e5 = a.E[E5];
+  const float* e6 = a.E[E6];
+  a.L[LU][q] += c1 * (e1[q - S] - e1[q]) + c2 * (e1[q - 2 * S] - e1[q + S]) +
+                c1 * (e4[q - Y] - e4[q]) + c2 * (e4[q - 2 * Y] - e4[q + Y]) +
+                c1 * (e5[q - 1] - e5[q]) + c2 * (e5[q - 2] - e5[q + 1]);
+  a.L[LV][q] += c1 * (e2[q] - e2[q + Y]) + c2 * (e2[q - Y] - e2[q + 2 * Y]) +
+                c1 * (e4[q] - e4[q + S]) + c2 * (e4[q - S] - e4[q + 2 * S]) +
+                c1 * (e6[q - 1] - e6[q]) + c2 * (e6[q - 2] - e6[q + 1]);
+  a.L[LW][q] += c1 * (e3[q] - e3[q + 1]) + c2 * (e3[q - 1] - e3[q + 2]) +
+                c1 * (e5[q] - e5[q + S]) + c2 * (e5[q - S] - e5[q + 2 * S]) +
+                c1 * (e6[q - Y] - e6[q]) + c2 * (e6[q - 2 * Y] - e6[q + Y]);
+  // box8(p) = {p, p+S, p-Y, p+S-Y, p-1, p+S-1, p-Y-1, p+S-Y-1} contains q for
+  // p in {q, q-S, q+Y, q-S+Y, q+1, q-S+1, q+Y+1, q-S+Y+1}
+  auto box = [&](const float* x) {
+    return x[q] + x[q - S] + x[q + Y] + x[q - S + Y] + x[q + 1] + x[q - S + 1] + x[q + Y + 1] +
+           x[q - S + Y + 1];
+  };
+  a.glam[q] += box(a.E[GL8]);
+  a.gmu[q] += box(a.E[GM8]) + a.E[GP1][q] + a.E[GP1][q + 1] + a.E[GP2][q] + a.E[GP2][q + Y] +
+              a.E[GP3][q] + a.E[GP3][q - S];
+}
+
+// ---------------------------------------------------------------------------
+// images^T over the imaged columns: the adjoint of the image values (top+1)
+// goes to the velocities they were made from, and to lam_mu; the images are
+// overwritten each step, so their adjoint is cleared
+// ---------------------------------------------------------------------------
+__global__ void k_adj_images(const AdjArgs a) {
+  // targets: the imaged columns and the one-column ring the images also read
+  const int j = a.sj0 - 1 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = a.si0 - 1 + blockIdx.y;
+  if (j > a.sj1 + 1 || i > a.si1 + 1) return;
+  const long long S = a.g.slice, Y = a.g.yline;
+  const long long p = (long long)i * S + (long long)j * Y + a.g.top();
+  const float* Lu = a.L[LU];
+  const float* Lv = a.L[LV];
+  const float* Lw = a.L[LW];
+  // adjoints of the images of column (ii, jj), zero outside the imaged window
+  auto win = [&](int ii, int jj) { return ii >= a.si0 && ii <= a.si1 && jj >= a.sj0 && jj <= a.sj1; };
+  auto col = [&](int ii, int jj) { return (long long)ii * S + (long long)jj * Y + a.g.top(); };
+  auto Au = [&](int ii, int jj) { return win(ii, jj) ? Lu[col(ii, jj) + 1] : 0.f; };
+  auto Av = [&](int ii, int jj) { return win(ii, jj) ? Lv[col(ii, jj) + 1] : 0.f; };
+  auto Aw = [&](int ii, int jj) { return win(ii, jj) ? Lw[col(ii, jj) + 1] : 0.f; };
+  auto lm = [&](int ii, int jj) { return a.lam_mu[(long long)ii * a.lam_mu_ld + jj]; };
+  auto m1 = [&](int ii) { return ii < a.gx_lim ? 1.0f : 0.0f; };
+  auto m2 = [&](int jj) { return jj >= a.gy_min ? 1.0f : 0.0f; };
+  // lZ(ii, jj) = adjoint of Z at column (ii, jj): -lam_mu * A_w
+  auto lZ = [&](int ii, int jj) { return win(ii, jj) ? -lm(ii, jj) * Aw(ii, jj) : 0.f; };
+  // Z = m1 (u_{i+1} - w_{i+1} + w) - (u - w + w_{i-1}) + (u_{i+1} - u)
+  //     + (v - w_{j+1} + w) - m2 (v_{j-1} - w + w_{j-1}) + (v - v_{j-1})
+  const float du = Au(i, j) - 2.0f * lZ(i, j) + (m1(i - 1) + 1.0f) * lZ(i - 1, j);
+  const float dv = Av(i, j) + 2.0f * lZ(i, j) - (m2(j + 1) + 1.0f) * lZ(i, j + 1);
+  const float dw = -Au(i, j) + Au(i + 1, j) + Av(i, j) - Av(i, j - 1) +
+                   (m1(i) + 2.0f + m2(j)) * lZ(i, j) - m1(i - 1) * lZ(i - 1, j) -
+                   lZ(i + 1, j) - lZ(i, j - 1) - m2(j + 1) * lZ(i, j + 1);
+  // lam_mu gradient: d wimg / d lam_mu = -Z
+  if (win(i, j)) {
+    const float* u = a.fu;
+    const float* v = a.fv;
+    const float* w = a.fw;
+    const float Z = m1(i) * (u[p + S] - w[p + S] + w[p]) - (u[p] - w[p] + w[p - S]) +
+                    (u[p + S] - u[p]) + (v[p] - w[p + Y] + w[p]) -
+                    m2(j) * (v[p - Y] - w[p] + w[p - Y]) + (v[p] - v[p - Y]);
+    a.glm[(long long)i * a.lam_mu_ld + j] += -Z * Aw(i, j);
+  }
+  // the image writes and reads of this column are all done by this thread
+  // for (i, j); neighbours only read the image adjoints, so defer the updates
+  // to the second kernel below
+  a.E[E1][p] = du;
+  a.E[E2][p] = dv;
+  a.E[E3][p] = dw;
+  a.E[E4][p] = Aw(i, j);  // to w(top-1)
+}
+
+__global__ void k_adj_images_apply(const AdjArgs a) {
+  const int j = a.sj0 - 1 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = a.si0 - 1 + blockIdx.y;
+  if (j > a.sj1 + 1 || i > a.si1 + 1) return;
+  const long long p = (long long)i * a.g.slice + (long long)j * a.g.yline + a.g.top();
+  a.L[LU][p] += a.E[E1][p];
+  a.L[LV][p] += a.E[E2][p];
+  a.L[LW][p] += a.E[E3][p];
+  if (i >= a.si0 && i <= a.si1 && j >= a.sj0 && j <= a.sj1) {
+    a.L[LW][p - 1] += a.E[E4][p];
+    a.L[LU][p + 1] = 0.f;
+    a.L[LV][p + 1] = 0.f;
+    a.L[LW][p + 1] = 0.f;
+    a.L[LU][p + 2] = 0.f;
+    a.L[LV][p + 2] = 0.f;
+    a.L[LW][p + 2] = 0.f;
+  }
+  // the temporaries at the top layer return to zero for the next step (cells
+  // outside the stress range must read zero in the strain-rate gather)
+  a.E[E1][p] = 0.f;
+  a.E[E2][p] = 0.f;
+  a.E[E3][p] = 0.f;
+  a.E[E4][p] = 0.f;
+}
+
+// ---------------------------------------------------------------------------
+// velocity^T, pointwise part
+// ---------------------------------------------------------------------------
+__global__ void k_adj_vel_cell(const AdjArgs a) {
+  const int k = a.vk0 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = a.vj0 + blockIdx.y;
+  const int i = a.vi0 + blockIdx.z;
+  if (k > a.vk1 || j > a.vj1 || i > a.vi1) return;
+  const long long S = a.g.slice, Y = a.g.yline;
+  const long long p = (long long)i * S + (long long)j * Y + k;
+  const float c1 = a.c1, c2 = a.c2;
+  const float* d = a.d1;
+  const float r1 = 0.25f * (d[p] + d[p - Y] + d[p - 1] + d[p - Y - 1]);
+  const float r2 = 0.25f * (d[p] + d[p + S] + d[p - 1] + d[p + S - 1]);
+  const float r3 = 0.25f * (d[p] + d[p + S] + d[p - Y] + d[p + S - Y]);
+  const float fd1 = a.dth / r1, fd2 = a.dth / r2, fd3 = a.dth / r3;
+  const float dc = a.dcrjx[i] * a.dcrjy[j] * a.dcrjz[k];
+  const float* xx = a.fxx;
+  const float* yy = a.fyy;
+  const float* zz = a.fzz;
+  const float* xy = a.fxy;
+  const float* xz = a.fxz;
+  const float* yz = a.fyz;
+  const float Du = c1 * (xx[p] - xx[p - S]) + c2 * (xx[p + S] - xx[p - 2 * S]) +
+                   c1 * (xy[p] - xy[p - Y]) + c2 * (xy[p + Y] - xy[p - 2 * Y]) +
+                   c1 * (xz[p] - xz[p - 1]) + c2 * (xz[p + 1] - xz[p - 2]);
+  const float Dv = c1 * (xy[p + S] - xy[p]) + c2 * (xy[p + 2 * S] - xy[p - S]) +
+                   c1 * (yy[p + Y] - yy[p]) + c2 * (yy[p + 2 * Y] - yy[p - Y]) +
+                   c1 * (yz[p] - yz[p - 1]) + c2 * (yz[p + 1] - yz[p - 2]);
+  const float Dw = c1 * (xz[p + S] - xz[p]) + c2 * (xz[p + 2 * S] - xz[p - S]) +
+                   c1 * (yz[p] - yz[p - Y]) + c2 * (yz[p + Y] - yz[p - 2 * Y]) +
+                   c1 * (zz[p + 1] - zz[p]) + c2 * (zz[p + 2] - zz[p - 1]);
+  const float lu = a.L[LU][p], lv = a.L[LV][p], lw = a.L[LW][p];
+  a.L[LU][p] = dc * lu;
+  a.L[LV][p] = dc * lv;
+  a.L[LW][p] = dc * lw;
+  a.V[VA][p] = fd1 * dc * lu;
+  a.V[VB][p] = fd2 * dc * lv;
+  a.V[VC][p] = fd3 * dc * lw;
+  // d fd / d rho_avg = -fd / rho_avg, each of the four densities weighs 1/4
+  a.V[VEA][p] = -0.25f * fd1 / r1 * Du * dc * lu;
+  a.V[VEB][p] = -0.25f * fd2 / r2 * Dv * dc * lv;
+  a.V[VEC][p] = -0.25f * fd3 / r3 * Dw * dc * lw;
+}
+
+// ---------------------------------------------------------------------------
+// velocity^T, gather part: weighted adjoint velocities -> adjoint stresses;
+// density weights -> the density gradient
+// ---------------------------------------------------------------------------
+__global__ void k_adj_vel_gather(const AdjArgs a) {
+  const int k = a.vk0 - 2 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = a.vj0 - 2 + blockIdx.y;
+  const int i = a.vi0 - 2 + blockIdx.z;
+  if (k > a.vk1 + 2 || j > a.vj1 + 2 || i > a.vi1 + 2) return;
+  const long long S = a.g.slice, Y = a.g.yline;
+  const long long q = (long long)i * S + (long long)j * Y + k;
+  const float c1 = a.c1, c2 = a.c2;
+  const float* A = a.V[VA];
+  const float* B = a.V[VB];
+  const float* C = a.V[VC];
+  a.L[LXX][q] += c1 * (A[q] - A[q + S]) + c2 * (A[q - S] - A[q + 2 * S]);
+  a.L[LXY][q] += c1 * (A[q] - A[q + Y]) + c2 * (A[q - Y] - A[q + 2 * Y]) +
+                 c1 * (B[q - S] - B[q]) + c2 * (B[q - 2 * S] - B[q + S]);
+  a.L[LXZ][q] += c1 * (A[q] - A[q + 1]) + c2 * (A[q - 1] - A[q + 2]) +
+                 c1 * (C[q - S] - C[q]) + c2 * (C[q - 2 * S] - C[q + S]);
+  a.L[LYY][q] += c1 * (B[q - Y] - B[q]) + c2 * (B[q - 2 * Y] - B[q + Y]);
+  a.L[LYZ][q] += c1 * (B[q] - B[q + 1]) + c2 * (B[q - 1] - B[q + 2]) +
+                 c1 * (C[q] - C[q + Y]) + c2 * (C[q - Y] - C[q + 2 * Y]);
+  a.L[LZZ][q] += c1 * (C[q - 1] - C[q]) + c2 * (C[q - 2] - C[q + 1]);
+  const float* ea = a.V[VEA];
+  const float* eb = a.V[VEB];
+  const float* ec = a.V[VEC];
+  a.gd[q] += ea[q] + ea[q + Y] + ea[q + 1] + ea[q + Y + 1] + eb[q] + eb[q - S] + eb[q + 1] +
+             eb[q - S + 1] + ec[q] + ec[q - S] + ec[q + Y] + ec[q - S + Y];
+}
+
+__global__ void k_adj_inject(float* Lu, float* Lv, float* Lw, const long long* idx,
+                             const int* comp, const float* res, int n) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  for (int r = 0; r < n; ++r) {
+    float* L = comp[r] == 0 ? Lu : (comp[r] == 1 ? Lv : Lw);
+    L[idx[r]] += res[r];
+  }
+}
+
+__global__ void k_sample(const float* u, const float* v, const float* w, const long long* idx,
+                         const int* comp, int n, float* out) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  const float* f = comp[r] == 0 ? u : (comp[r] == 1 ? v : w);
+  out[r] = f[idx[r]];
+}
+
+// ---------------------------------------------------------------------------
+// gradients on the padded arrays -> interior lambda, mu, rho
+// ---------------------------------------------------------------------------
+__global__ void k_adj_fold(const AdjArgs a, float* g_lambda, float* g_mu, float* g_rho) {
+  const long long n = (long long)a.g.nxt * a.g.nyt * a.g.nzt;
+  const long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  const int x = (int)(c % a.g.nxt), y = (int)((c / a.g.nxt) % a.g.nyt),
+            z = (int)(c / ((long long)a.g.nxt * a.g.nyt));
+  const int lo = 2 + AWP_NGSL, hix = a.g.nxt + 1 + AWP_NGSL, hiy = a.g.nyt + 1 + AWP_NGSL;
+  const int kb = AWP_ALIGN, kt = a.g.nzt + AWP_ALIGN - 1;
+  const int i = x + lo, j = y + lo, k = kt - z;
+  // the border fill copies (i, j, k) into the ghost cells that clamp onto it
+  int is[2] = {i, 0}, js[2] = {j, 0}, ks[2] = {k, 0};
+  int ni = 1, nj = 1, nk = 1;
+  if (i == lo) is[ni++] = lo - 1;
+  if (i == hix) is[ni++] = hix + 1;
+  if (j == lo) js[nj++] = lo - 1;
+  if (j == hiy) js[nj++] = hiy + 1;
+  if (k == kb) ks[nk++] = kb - 1;
+  if (k == kt) ks[nk++] = kt + 1;
+  float gl = 0.f, gm = 0.f, gr = 0.f;
+  for (int ii = 0; ii < ni; ++ii)
+    for (int jj = 0; jj < nj; ++jj)
+      for (int kk = 0; kk < nk; ++kk) {
+        const long long p = (long long)is[ii] * a.g.slice + (long long)js[jj] * a.g.yline + ks[kk];
+        gl += a.glam[p];
+        gm += a.gmu[p];
+        gr += a.gd[p];
+      }
+  const long long p0 = (long long)i * a.g.slice + (long long)j * a.g.yline + k;
+  const float il = a.lam[p0], im = a.mu[p0];  // 1/lambda, 1/mu
+  float g_l = -il * il * gl;                  // d(1/lambda)/d lambda = -1/lambda^2
+  float g_m = -im * im * gm;
+  if (k == kt && i >= a.si0 && i <= a.si1 && j >= a.sj0 && j <= a.sj1) {
+    // lam_mu = lambda / (lambda + 2 mu)
+    const float lm = 1.0f / il, mm = 1.0f / im, den = lm + 2.0f * mm;
+    const float glm = a.glm[(long long)i * a.lam_mu_ld + j];
+    g_l += glm * 2.0f * mm / (den * den);
+    g_m += -glm * 2.0f * lm / (den * den);
+  }
+  g_lambda[c] = g_l;
+  g_mu[c] = g_m;
+  g_rho[c] = gr;
+}
+
+__global__ void k_set_moduli(const float* lambda, const float* mu_, const float* rho, float* lam,
+                             float* mu, float* d1, const AwpGeom g) {
+  // every cell of the one-cell shell around the interior takes the clamped
+  // interior value (the border fill of the media set-up)
+  const int lo = 2 + AWP_NGSL, hix = g.nxt + 1 + AWP_NGSL, hiy = g.nyt + 1 + AWP_NGSL;
+  const int kb = AWP_ALIGN, kt = g.nzt + AWP_ALIGN - 1;
+  const int k = kb - 1 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = lo - 1 + blockIdx.y;
+  const int i = lo - 1 + blockIdx.z;
+  if (k > kt + 1 || j > hiy + 1 || i > hix + 1) return;
+  const int ci = min(max(i, lo), hix), cj = min(max(j, lo), hiy), ck = min(max(k, kb), kt);
+  const long long c = (long long)(kt - ck) * g.nxt * g.nyt + (long long)(cj - lo) * g.nxt + (ci - lo);
+  const long long p = (long long)i * g.slice + (long long)j * g.yline + k;
+  lam[p] = __frcp_rn(lambda[c]);  // correctly rounded (the build divides approximately)
+  mu[p] = __frcp_rn(mu_[c]);
+  d1[p] = rho[c];
+}
+
+inline unsigned cdiv(long long a, long long b) { return (unsigned)((a + b - 1) / b); }
+
+}  // namespace
+
+cudaError_t awp_launch_adjoint_step(const AdjArgs& a, cudaStream_t st) {
+  const int fj = a.fj1 - a.sj0 + 1, si = a.si1 - a.si0 + 1, sj = a.sj1 - a.sj0 + 1,
+            sk = a.sk1 - a.sk0 + 1;
+  k_adj_fstr<<<dim3(cdiv(fj, 128), si), 128, 0, st>>>(a);
+  if (a.elastic)
+    k_adj_stress_cell<true><<<dim3(cdiv(sk, 32), sj, si), 32, 0, st>>>(a);
+  else
+    k_adj_stress_cell<false><<<dim3(cdiv(sk, 32), sj, si), 32, 0, st>>>(a);
+  k_adj_stress_gather<<<dim3(cdiv(sk + 4, 32), sj + 4, si + 4), 32, 0, st>>>(a);
+  k_adj_images<<<dim3(cdiv(sj + 2, 128), si + 2), 128, 0, st>>>(a);
+  k_adj_images_apply<<<dim3(cdiv(sj + 2, 128), si + 2), 128, 0, st>>>(a);
+  const int vi = a.vi1 - a.vi0 + 1, vj = a.vj1 - a.vj0 + 1, vk = a.vk1 - a.vk0 + 1;
+  k_adj_vel_cell<<<dim3(cdiv(vk, 32), vj, vi), 32, 0, st>>>(a);
+  k_adj_vel_gather<<<dim3(cdiv(vk + 4, 32), vj + 4, vi + 4), 32, 0, st>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t awp_launch_adjoint_inject(float* const L[3], const long long* idx, const int* comp,
+                                      const float* res, int nrec, cudaStream_t st) {
+  if (nrec <= 0) return cudaSuccess;
+  k_adj_inject<<<1, 1, 0, st>>>(L[0], L[1], L[2], idx, comp, res, nrec);
+  return cudaGetLastError();
+}
+
+cudaError_t awp_launch_sample(const float* u, const float* v, const float* w,
+                              const long long* idx, const int* comp, int nrec, float* out,
+                              cudaStream_t st) {
+  if (nrec <= 0) return cudaSuccess;
+  k_sample<<<cdiv(nrec, 128), 128, 0, st>>>(u, v, w, idx, comp, nrec, out);
+  return cudaGetLastError();
+}
+
+cudaError_t awp_launch_adjoint_fold(const AdjArgs& a, float* g_lambda, float* g_mu,
+                                    float* g_rho, cudaStream_t st) {
+  const long long n = (long long)a.g.nxt * a.g.nyt * a.g.nzt;
+  k_adj_fold<<<cdiv(n, 256), 256, 0, st>>>(a, g_lambda, g_mu, g_rho);
+  return cudaGetLastError();
+}
+
+cudaError_t awp_launch_set_moduli(const float* lambda, const float* mu_, const float* rho,
+                                  float* lam, float* mu, float* d1, const AwpGeom& g,
+                                  cudaStream_t st) {
+  const dim3 grid(cdiv(g.nzt + 2, 64), g.nyt + 2, g.nxt + 2);
+  k_set_moduli<<<grid, 64, 0, st>>>(lambda, mu_, rho, lam, mu, d1, g);
+  return cudaGetLastError();
+}

@@ -1,0 +1,59 @@
+// Discrete adjoint of the single-grid time step (velocity, stress with memory
+// variables, free-surface images) and the gradient of a seismogram misfit with
+// respect to the materials.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "awp_common.h"
+
+struct AdjArgs {
+  // forward state: stresses before the step (velocity half), velocities after
+  // the step (stress half, free-surface images included)
+  const float *fxx, *fyy, *fzz, *fxy, *fxz, *fyz;
+  const float *fu, *fv, *fw;
+  // adjoint state, updated in place (u v w xx yy zz xy xz yz r1..r6)
+  float* L[15];
+  // temporaries (zero outside the ranges that write them)
+  float* E[11];  // stress half: adjoint strain rates (6), material weights (5)
+  float* V[6];   // velocity half: weighted adjoint velocities (3), density weights (3)
+  // gradients on the padded kernel arrays: rho, 1/lambda, 1/mu, and the
+  // surface Lame ratio lam_mu (2-D)
+  float *gd, *glam, *gmu, *glm;
+  // media and constants of the forward step
+  const float *d1, *lam, *mu, *qp, *qs, *lam_mu;
+  const float *dcrjx, *dcrjy, *dcrjz;
+  AwpTexture tex;
+  float coeff[16];
+  float dth, dh1, dt, c1, c2, qthr;
+  int elastic;
+  AwpGeom g;
+  int vi0, vi1, vj0, vj1, vk0, vk1;  // velocity update range (inclusive, padded)
+  int si0, si1, sj0, sj1, sk0, sk1;  // stress update range
+  int fj1;                           // last j row of the free-surface imaging
+  int gx_lim, gy_min, lam_mu_ld;
+};
+
+// One step backwards: imaging, stress (+ memory variables, images), velocity;
+// accumulates the material gradients of that step.
+cudaError_t awp_launch_adjoint_step(const AdjArgs& a, cudaStream_t st);
+
+// Receiver terms: L[comp][idx[r]] += res[r] (one thread, receivers in order).
+cudaError_t awp_launch_adjoint_inject(float* const L[3], const long long* idx, const int* comp,
+                                      const float* res, int nrec, cudaStream_t st);
+// Seismogram samples of the current state: out[r] = field(comp[r])[idx[r]].
+cudaError_t awp_launch_sample(const float* u, const float* v, const float* w,
+                              const long long* idx, const int* comp, int nrec, float* out,
+                              cudaStream_t st);
+
+// Gradients on the padded arrays -> interior lambda, mu, rho (layout
+// [nz][ny][nx], surface first): the border-fill copies folded back, the
+// reciprocal moduli and the surface Lame ratio chained through.
+cudaError_t awp_launch_adjoint_fold(const AdjArgs& a, float* g_lambda, float* g_mu,
+                                    float* g_rho, cudaStream_t st);
+
+// Moduli and density from interior arrays ([nz][ny][nx], surface first) into
+// the padded kernel arrays (1/lambda, 1/mu, rho), one-cell border included.
+cudaError_t awp_launch_set_moduli(const float* lambda, const float* mu_, const float* rho,
+                                  float* lam, float* mu, float* d1, const AwpGeom& g,
+                                  cudaStream_t st);

@@ -21,6 +21,7 @@
 #include "awp_tma.cuh"
 #include "awp_topo.h"
 #include "awp_topo_kern.cuh"
+#include "awp_adjoint.cuh"
 
 namespace {
 
@@ -282,9 +283,9 @@ struct PhaseScope {
 // A single grid runs them in order (one_step); a discontinuous mesh
 // interleaves them with the coupling kernels (mesh_step).
 
-int phase_begin(awp_ctx* c) {
+// The step-1 source sample is added before the loop (pmcl3d.c:1175-1187).
+int initial_source(awp_ctx* c) {
   if (c->cur_step == 0 && !c->initial_src_done) {
-    // step-1 source sample is added before the loop (pmcl3d.c:1175-1187)
     if (c->p.ifault < 4) {
       int s = launch_sources(c, 0);
       if (s) return s;
@@ -292,6 +293,12 @@ int phase_begin(awp_ctx* c) {
     }
     c->initial_src_done = true;
   }
+  return AWP_OK;
+}
+
+int phase_begin(awp_ctx* c) {
+  const int s = initial_source(c);
+  if (s) return s;
   c->cur_step += 1;
   return AWP_OK;
 }
@@ -1706,6 +1713,271 @@ int awp_topography_init(awp_ctx* c, const char* intopo) {
   t.s_j = AWP_NGSL / 2; t.e_j = ny - AWP_NGSL / 2;
   c->d_topo = d;
   c->topo = m;
+  return AWP_OK;
+}
+
+// ===========================================================================
+// Materials, reset, seismograms and the adjoint gradient
+// ===========================================================================
+}  // extern "C"
+
+namespace {
+
+int check_adjoint_ctx(awp_ctx* c) {
+  if (!c) return set_error(AWP_ERR_ARG, "null context");
+  if (!c->media_ready) return set_error(AWP_ERR_STATE, "media not uploaded");
+  if (c->p.ngrids != 1 || c->p.nve == 3 || c->topo || c->recv || c->srcf)
+    return set_error(AWP_ERR_UNSUPPORTED,
+                     "the adjoint covers single-grid Cartesian runs without plasticity, "
+                     "receiver files or SOURCEFILE sources");
+  if (c->ncell > 0 && c->p.ifault != 1)
+    return set_error(AWP_ERR_UNSUPPORTED,
+                     "the adjoint takes IFAULT 1 sources (the kinematic source depends on mu)");
+  return AWP_OK;
+}
+
+// device copies of receiver positions (padded linear index) and components
+int upload_receivers(awp_ctx* c, int nrec, const int* xyz, const int* comp, long long** d_idx,
+                     int** d_comp) {
+  std::vector<long long> idx(nrec);
+  for (int r = 0; r < nrec; ++r) {
+    const int x = xyz[3 * r], y = xyz[3 * r + 1], z = xyz[3 * r + 2];
+    if (x < 0 || x >= c->g.nxt || y < 0 || y >= c->g.nyt || z < 0 || z >= c->g.nzt ||
+        comp[r] < 0 || comp[r] > 2)
+      return set_error(AWP_ERR_ARG, "receiver %d outside the grid or bad component", r);
+    idx[r] = (long long)(x + 2 + AWP_NGSL) * c->g.slice +
+             (long long)(y + 2 + AWP_NGSL) * c->g.yline + (c->g.top() - z);
+  }
+  CU_TRY(cudaMalloc((void**)d_idx, sizeof(long long) * std::max(nrec, 1)));
+  CU_TRY(cudaMalloc((void**)d_comp, sizeof(int) * std::max(nrec, 1)));
+  CU_TRY(cudaMemcpy(*d_idx, idx.data(), sizeof(long long) * nrec, cudaMemcpyHostToDevice));
+  CU_TRY(cudaMemcpy(*d_comp, comp, sizeof(int) * nrec, cudaMemcpyHostToDevice));
+  return AWP_OK;
+}
+
+struct DevBuf {  // owned device allocations of one call
+  std::vector<void*> p;
+  ~DevBuf() {
+    for (void* q : p) cudaFree(q);
+  }
+  float* f(size_t n) {
+    void* q = nullptr;
+    if (cudaMalloc(&q, n * sizeof(float)) != cudaSuccess) return nullptr;
+    p.push_back(q);
+    return (float*)q;
+  }
+};
+
+}  // namespace
+
+extern "C" {
+
+int awp_set_moduli(awp_ctx* c, const float* lambda, const float* mu, const float* rho) {
+  if (!c || !lambda || !mu || !rho) return set_error(AWP_ERR_ARG, "null argument");
+  if (!c->media_ready) return set_error(AWP_ERR_STATE, "upload media first (Q and layout)");
+  const size_t n = (size_t)c->g.nxt * c->g.nyt * c->g.nzt;
+  DevBuf b;
+  float *dl = b.f(n), *dm = b.f(n), *dr = b.f(n);
+  if (!dl || !dm || !dr) return set_error(AWP_ERR_NOMEM, "moduli staging");
+  CU_TRY(cudaMemcpyAsync(dl, lambda, n * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+  CU_TRY(cudaMemcpyAsync(dm, mu, n * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+  CU_TRY(cudaMemcpyAsync(dr, rho, n * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+  CU_TRY(awp_launch_set_moduli(dl, dm, dr, c->f[AWP_LAM], c->f[AWP_MU], c->f[AWP_D1], c->g,
+                               c->stream));
+  CU_TRY(awp_launch_lam_mu(c->f[AWP_LAM], c->f[AWP_MU], c->lam_mu, c->g, c->xls, c->xre, c->yls,
+                           c->yre, c->stream));
+  CU_TRY(cudaStreamSynchronize(c->stream));
+  return AWP_OK;
+}
+
+int awp_reset(awp_ctx* c) {
+  if (!c) return set_error(AWP_ERR_ARG, "null context");
+  const size_t bytes = sizeof(float) * (size_t)c->g.cells_pad();
+  for (int fld = AWP_U1; fld <= AWP_R6; ++fld)
+    CU_TRY(cudaMemsetAsync(c->f[fld], 0, bytes, c->stream));
+  c->cur_step = 0;
+  c->initial_src_done = false;
+  CU_TRY(cudaStreamSynchronize(c->stream));
+  return AWP_OK;
+}
+
+int awp_seismograms(awp_ctx* c, int nsteps, int nrec, const int* rec_xyz, const int* rec_comp,
+                    float* seis) {
+  int e = check_adjoint_ctx(c);
+  if (e) return e;
+  if (nsteps < 0 || nrec < 1 || !rec_xyz || !rec_comp || !seis)
+    return set_error(AWP_ERR_ARG, "bad receiver arguments");
+  long long* d_idx = nullptr;
+  int* d_comp = nullptr;
+  e = upload_receivers(c, nrec, rec_xyz, rec_comp, &d_idx, &d_comp);
+  DevBuf b;
+  b.p.push_back(d_idx);
+  b.p.push_back(d_comp);
+  if (e) return e;
+  float* d_seis = b.f((size_t)std::max(nsteps, 1) * nrec);
+  if (!d_seis) return set_error(AWP_ERR_NOMEM, "seismogram buffer");
+  for (int n = 0; n < nsteps; ++n) {
+    if ((e = one_step(c))) return e;
+    CU_TRY(awp_launch_sample(c->f[AWP_U1], c->f[AWP_V1], c->f[AWP_W1], d_idx, d_comp, nrec,
+                             d_seis + (size_t)n * nrec, c->stream));
+  }
+  CU_TRY(cudaMemcpyAsync(seis, d_seis, sizeof(float) * (size_t)nsteps * nrec,
+                         cudaMemcpyDeviceToHost, c->stream));
+  CU_TRY(cudaStreamSynchronize(c->stream));
+  return AWP_OK;
+}
+
+int awp_misfit_gradient(awp_ctx* c, int nsteps, int nrec, const int* rec_xyz, const int* rec_comp,
+                        const float* d_obs, int nsnap, double* misfit, float* seis,
+                        float* g_lambda, float* g_mu, float* g_rho) {
+  int e = check_adjoint_ctx(c);
+  if (e) return e;
+  if (nsteps < 1 || nrec < 1 || !rec_xyz || !rec_comp || !d_obs || !misfit)
+    return set_error(AWP_ERR_ARG, "bad arguments");
+  const size_t cp = (size_t)c->g.cells_pad();
+  const size_t fb = cp * sizeof(float);
+  // snapshot spacing: sqrt(N) unless given
+  int L = nsnap > 0 ? (nsteps + nsnap - 1) / nsnap : (int)ceil(sqrt((double)nsteps));
+  L = std::max(1, std::min(L, nsteps));
+  const int nseg = (nsteps + L - 1) / L;
+  const size_t fields = (size_t)(nseg + 1) * 15 + (size_t)L * 9 + 15 + 17 + 3;
+  size_t freeb = 0, totb = 0;
+  CU_TRY(cudaMemGetInfo(&freeb, &totb));
+  if (fields * fb + (64u << 20) > freeb)
+    return set_error(AWP_ERR_NOMEM,
+                     "adjoint needs %.1f GB (%zu fields of %.1f MB: %d snapshots, %d-step "
+                     "segments), %.1f GB free",
+                     fields * fb / 1e9, fields, fb / 1e6, nseg + 1, L, freeb / 1e9);
+  DevBuf b;
+  long long* d_idx = nullptr;
+  int* d_comp = nullptr;
+  e = upload_receivers(c, nrec, rec_xyz, rec_comp, &d_idx, &d_comp);
+  b.p.push_back(d_idx);
+  b.p.push_back(d_comp);
+  if (e) return e;
+  float* d_seis = b.f((size_t)nsteps * nrec);
+  float* d_res = b.f((size_t)nsteps * nrec);
+  if (!d_seis || !d_res) return set_error(AWP_ERR_NOMEM, "seismogram buffers");
+  cudaStream_t st = c->stream;
+
+  // ---- forward pass with snapshots X_{sL} and the final state ---------------------
+  std::vector<float*> snap((size_t)(nseg + 1) * 15, nullptr);
+  for (auto& q : snap)
+    if (!(q = b.f(cp))) return set_error(AWP_ERR_NOMEM, "snapshots");
+  std::vector<long long> snap_step(nseg + 1);
+  std::vector<char> snap_init(nseg + 1);
+  auto save = [&](int s) -> int {
+    for (int fld = 0; fld < 15; ++fld)
+      CU_TRY(cudaMemcpyAsync(snap[(size_t)s * 15 + fld], c->f[fld], fb, cudaMemcpyDeviceToDevice, st));
+    snap_step[s] = c->cur_step;
+    snap_init[s] = c->initial_src_done;
+    return AWP_OK;
+  };
+  auto restore = [&](int s) -> int {
+    for (int fld = 0; fld < 15; ++fld)
+      CU_TRY(cudaMemcpyAsync(c->f[fld], snap[(size_t)s * 15 + fld], fb, cudaMemcpyDeviceToDevice, st));
+    c->cur_step = snap_step[s];
+    c->initial_src_done = snap_init[s] != 0;
+    return AWP_OK;
+  };
+  for (int n = 0; n < nsteps; ++n) {
+    if (n % L == 0 && (e = save(n / L))) return e;
+    if ((e = one_step(c))) return e;
+    CU_TRY(awp_launch_sample(c->f[AWP_U1], c->f[AWP_V1], c->f[AWP_W1], d_idx, d_comp, nrec,
+                             d_seis + (size_t)n * nrec, st));
+  }
+  if ((e = save(nseg))) return e;  // the final state, restored at the end
+
+  // ---- misfit and residuals ---------------------------------------------------------
+  std::vector<float> hs((size_t)nsteps * nrec), hr((size_t)nsteps * nrec);
+  CU_TRY(cudaMemcpyAsync(hs.data(), d_seis, sizeof(float) * hs.size(), cudaMemcpyDeviceToHost, st));
+  CU_TRY(cudaStreamSynchronize(st));
+  double J = 0.0;
+  for (size_t q = 0; q < hs.size(); ++q) {
+    hr[q] = hs[q] - d_obs[q];
+    J += 0.5 * (double)hr[q] * (double)hr[q];
+  }
+  *misfit = J;
+  if (seis) memcpy(seis, hs.data(), sizeof(float) * hs.size());
+  CU_TRY(cudaMemcpyAsync(d_res, hr.data(), sizeof(float) * hr.size(), cudaMemcpyHostToDevice, st));
+
+  // ---- adjoint state, temporaries, gradients (zeroed) --------------------------------
+  AdjArgs a;
+  memset(&a, 0, sizeof(a));
+  for (int q = 0; q < 15; ++q)
+    if (!(a.L[q] = b.f(cp))) return set_error(AWP_ERR_NOMEM, "adjoint fields");
+  for (int q = 0; q < 11; ++q)
+    if (!(a.E[q] = b.f(cp))) return set_error(AWP_ERR_NOMEM, "adjoint temporaries");
+  for (int q = 0; q < 6; ++q)
+    if (!(a.V[q] = b.f(cp))) return set_error(AWP_ERR_NOMEM, "adjoint temporaries");
+  if (!(a.gd = b.f(cp)) || !(a.glam = b.f(cp)) || !(a.gmu = b.f(cp)) ||
+      !(a.glm = b.f((size_t)c->g.nx_pad() * c->g.ny_pad())))
+    return set_error(AWP_ERR_NOMEM, "gradients");
+  for (int q = 0; q < 15; ++q) CU_TRY(cudaMemsetAsync(a.L[q], 0, fb, st));
+  for (int q = 0; q < 11; ++q) CU_TRY(cudaMemsetAsync(a.E[q], 0, fb, st));
+  for (int q = 0; q < 6; ++q) CU_TRY(cudaMemsetAsync(a.V[q], 0, fb, st));
+  CU_TRY(cudaMemsetAsync(a.gd, 0, fb, st));
+  CU_TRY(cudaMemsetAsync(a.glam, 0, fb, st));
+  CU_TRY(cudaMemsetAsync(a.gmu, 0, fb, st));
+  CU_TRY(cudaMemsetAsync(a.glm, 0, sizeof(float) * c->g.nx_pad() * c->g.ny_pad(), st));
+  a.d1 = c->f[AWP_D1]; a.lam = c->f[AWP_LAM]; a.mu = c->f[AWP_MU];
+  a.qp = c->f[AWP_QP]; a.qs = c->f[AWP_QS]; a.lam_mu = c->lam_mu;
+  a.dcrjx = c->dcrjx; a.dcrjy = c->dcrjy; a.dcrjz = c->dcrjz;
+  a.tex = c->tex;
+  memcpy(a.coeff, c->coeff, sizeof(a.coeff));
+  a.dth = c->dth; a.dh1 = c->dh1; a.dt = c->p.dt; a.c1 = c->c1; a.c2 = c->c2; a.qthr = c->qthr;
+  a.elastic = c->elastic ? 1 : 0;
+  a.g = c->g;
+  {
+    const VelArgs v = make_vel_args(c);
+    a.vi0 = v.i0; a.vi1 = v.i1; a.vj0 = v.j0; a.vj1 = v.j1; a.vk0 = v.k0; a.vk1 = v.k1;
+    const StrArgs sa = make_str_args(c);
+    a.si0 = sa.i0; a.si1 = sa.i1; a.sj0 = sa.j0; a.sj1 = sa.j1; a.sk0 = sa.k0; a.sk1 = sa.k1;
+    a.gx_lim = sa.gx_lim; a.gy_min = sa.gy_min; a.lam_mu_ld = sa.lam_mu_ld;
+    a.fj1 = make_fstr_args(c).j1;
+  }
+  // segment store: stresses before and velocities after each step of a segment
+  std::vector<float*> seg((size_t)L * 9, nullptr);
+  for (auto& q : seg)
+    if (!(q = b.f(cp))) return set_error(AWP_ERR_NOMEM, "segment store");
+  float* const Lvel[3] = {a.L[0], a.L[1], a.L[2]};
+
+  // ---- backward sweep over the segments ----------------------------------------------
+  for (int s = nseg - 1; s >= 0; --s) {
+    const int n0 = s * L, n1 = std::min(nsteps, n0 + L);
+    if ((e = restore(s))) return e;
+    for (int n = n0; n < n1; ++n) {
+      float** slot = &seg[(size_t)(n - n0) * 9];
+      // the stresses the velocity update of this step reads include the
+      // step-1 source sample added before the first step
+      if ((e = initial_source(c))) return e;
+      for (int q = 0; q < 6; ++q)
+        CU_TRY(cudaMemcpyAsync(slot[q], c->f[AWP_XX + q], fb, cudaMemcpyDeviceToDevice, st));
+      if ((e = one_step(c))) return e;
+      for (int q = 0; q < 3; ++q)
+        CU_TRY(cudaMemcpyAsync(slot[6 + q], c->f[AWP_U1 + q], fb, cudaMemcpyDeviceToDevice, st));
+    }
+    for (int n = n1 - 1; n >= n0; --n) {
+      // the misfit term of the state after step n (its sample index is n)
+      CU_TRY(awp_launch_adjoint_inject(Lvel, d_idx, d_comp, d_res + (size_t)n * nrec, nrec, st));
+      float** slot = &seg[(size_t)(n - n0) * 9];
+      a.fxx = slot[0]; a.fyy = slot[1]; a.fzz = slot[2];
+      a.fxy = slot[3]; a.fxz = slot[4]; a.fyz = slot[5];
+      a.fu = slot[6]; a.fv = slot[7]; a.fw = slot[8];
+      CU_TRY(awp_launch_adjoint_step(a, st));
+    }
+  }
+
+  // ---- gradients to the host; the context ends on the final forward state -----------
+  const size_t ni = (size_t)c->g.nxt * c->g.nyt * c->g.nzt;
+  float *gl = b.f(ni), *gm = b.f(ni), *gr = b.f(ni);
+  if (!gl || !gm || !gr) return set_error(AWP_ERR_NOMEM, "gradient staging");
+  CU_TRY(awp_launch_adjoint_fold(a, gl, gm, gr, st));
+  if (g_lambda) CU_TRY(cudaMemcpyAsync(g_lambda, gl, ni * sizeof(float), cudaMemcpyDeviceToHost, st));
+  if (g_mu) CU_TRY(cudaMemcpyAsync(g_mu, gm, ni * sizeof(float), cudaMemcpyDeviceToHost, st));
+  if (g_rho) CU_TRY(cudaMemcpyAsync(g_rho, gr, ni * sizeof(float), cudaMemcpyDeviceToHost, st));
+  if ((e = restore(nseg))) return e;
+  CU_TRY(cudaStreamSynchronize(st));
   return AWP_OK;
 }
 

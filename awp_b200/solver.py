@@ -133,6 +133,19 @@ class Solver:
                                              c_float(fmajor), c_float(fminor),
                                              _fptr(st), _fptr(dp)), "awp_upload_plasticity")
 
+    def set_moduli(self, lam: np.ndarray, mu: np.ndarray, rho: np.ndarray) -> None:
+        """Lame moduli and density of the interior, arrays [nz][ny][nx] (surface
+        first), into the kernel arrays; Q stays from the media upload."""
+        a = [np.ascontiguousarray(x, np.float32) for x in (lam, mu, rho)]
+        n = self.params.nx * self.params.ny * self.params.nz
+        if any(x.size != n for x in a):
+            raise ValueError("moduli arrays must have nz*ny*nx elements")
+        check(self.lib.awp_set_moduli(self.ctx, *[_fptr(x) for x in a]), "awp_set_moduli")
+
+    def reset(self) -> None:
+        """Wavefield and memory variables to zero, back to step 0."""
+        check(self.lib.awp_reset(self.ctx), "awp_reset")
+
     def topography(self, intopo: str) -> None:
         """Curvilinear topography of this (top) grid from an INTOPO elevation
         file; call before receivers() and sourcefile()."""

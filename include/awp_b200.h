@@ -231,6 +231,38 @@ int awp_batch_get_mode(const awp_batch* batch);
  * CTAs of the velocity and stress launches. */
 int awp_batch_info(awp_batch* batch, long long info[6]);
 
+/* ------------------------------------------------------------------------ */
+/* Materials, seismograms and the adjoint gradient (single grid, Cartesian,  */
+/* NVE 1/2, IFAULT 1 sources)                                                */
+/* ------------------------------------------------------------------------ */
+/* Lame moduli and density of the interior, host arrays [nz][ny][nx] (surface
+ * first, the mesh-file order), into the kernel arrays (1/lambda, 1/mu, rho
+ * with the one-cell border copy of the media set-up) and the surface ratio
+ * lambda/(lambda+2mu).  Q and the memory-variable set-up of the last media
+ * upload stay (upload media first). */
+int awp_set_moduli(awp_ctx* ctx, const float* lambda, const float* mu, const float* rho);
+/* Wavefield and memory variables to zero, step counter to 0 (sources start
+ * over). */
+int awp_reset(awp_ctx* ctx);
+/* nsteps forward steps, sampling after each step the velocity component
+ * rec_comp[r] (0 u, 1 v, 2 w) at interior cell rec_xyz[r] = (x, y, z), z counted
+ * from the surface: seis[nsteps][nrec] (host). */
+int awp_seismograms(awp_ctx* ctx, int nsteps, int nrec, const int* rec_xyz, const int* rec_comp,
+                    float* seis);
+/* The same forward run with the misfit J = 1/2 sum_n sum_r (seis - d_obs)^2
+ * and its gradient with respect to lambda, mu, rho of every interior cell
+ * (host arrays [nz][ny][nx], surface first; Q held fixed), by the discrete
+ * adjoint of the time step: hand-written transposes of the velocity, stress,
+ * memory-variable, free-surface-image and imaging updates.  The forward
+ * states are kept as nsnap snapshots in device memory (0: ceil(sqrt(nsteps)))
+ * and each segment between snapshots is run forward again before its
+ * backward sweep.  The context ends on the state after nsteps steps.  seis
+ * (optional) receives the samples.  AWP_ERR_NOMEM when the snapshots do not
+ * fit, with the size in awp_last_error. */
+int awp_misfit_gradient(awp_ctx* ctx, int nsteps, int nrec, const int* rec_xyz, const int* rec_comp,
+                        const float* d_obs, int nsnap, double* misfit, float* seis,
+                        float* g_lambda, float* g_mu, float* g_rho);
+
 /* Host-only helper (no context, no GPU): the metric arrays of a topography
  * file (INTOPO) for an nx x ny x nz grid of spacing h, as topo_init_metrics /
  * topo_init_geometry / topo_build compute them (src/topography/topography.c:

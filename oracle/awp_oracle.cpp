@@ -17,6 +17,49 @@ namespace {
 
 constexpr int NGSL = 8, NGSL2 = 16, ALIGN = 32, MAXFILT = 20;
 
+// Dual number (value, tangent) in double: the oracle instantiated on it
+// carries the exact derivative of every state value along one direction of
+// the materials (tangent-linear mode), the discrete derivative the adjoint
+// gradient must reproduce.  Branches compare values.
+struct Dual {
+  double v = 0.0, d = 0.0;
+  Dual() = default;
+  Dual(double x) : v(x) {}  // NOLINT (implicit from constants and floats)
+  Dual(double x, double y) : v(x), d(y) {}
+  explicit operator double() const { return v; }
+  explicit operator float() const { return (float)v; }
+  explicit operator int() const { return (int)v; }
+  Dual& operator+=(const Dual& b) { v += b.v; d += b.d; return *this; }
+  Dual& operator-=(const Dual& b) { v -= b.v; d -= b.d; return *this; }
+  Dual& operator*=(const Dual& b) { d = d * b.v + v * b.d; v *= b.v; return *this; }
+  Dual& operator/=(const Dual& b) { d = (d * b.v - v * b.d) / (b.v * b.v); v /= b.v; return *this; }
+};
+inline Dual operator+(Dual a, const Dual& b) { return a += b; }
+inline Dual operator-(Dual a, const Dual& b) { return a -= b; }
+inline Dual operator*(Dual a, const Dual& b) { return a *= b; }
+inline Dual operator/(Dual a, const Dual& b) { return a /= b; }
+inline Dual operator-(const Dual& a) { return Dual(-a.v, -a.d); }
+inline bool operator<(const Dual& a, const Dual& b) { return a.v < b.v; }
+inline bool operator<=(const Dual& a, const Dual& b) { return a.v <= b.v; }
+inline bool operator>(const Dual& a, const Dual& b) { return a.v > b.v; }
+inline bool operator>=(const Dual& a, const Dual& b) { return a.v >= b.v; }
+inline bool operator==(const Dual& a, const Dual& b) { return a.v == b.v; }
+inline bool operator!=(const Dual& a, const Dual& b) { return a.v != b.v; }
+using ::cos;  // keep the double overloads visible beside the Dual ones
+using ::exp;
+using ::sin;
+using ::sqrt;
+inline Dual sin(const Dual& a) { return Dual(::sin(a.v), ::cos(a.v) * a.d); }
+inline Dual cos(const Dual& a) { return Dual(::cos(a.v), -::sin(a.v) * a.d); }
+inline Dual exp(const Dual& a) { const double e = ::exp(a.v); return Dual(e, e * a.d); }
+inline Dual sqrt(const Dual& a) { const double r = ::sqrt(a.v); return Dual(r, a.d / (2.0 * r)); }
+inline double tangent(const Dual& a) { return a.d; }
+inline double tangent(double) { return 0.0; }
+inline double tangent(float) { return 0.0; }
+inline void set_tangent(Dual& a, double t) { a.d = t; }
+inline void set_tangent(double&, double) {}
+inline void set_tangent(float&, double) {}
+
 struct Base {
   virtual ~Base() {}
   virtual void set_field(int f, const float* s) = 0;
@@ -38,6 +81,8 @@ struct Base {
   virtual long long current() = 0;
   virtual void gather(int nbgx, int nedx, int nskpx, int nbgy, int nedy, int nskpy, int nbgz,
                       int nedz, int nskpz, float* bx, float* by, float* bz) = 0;
+  virtual void set_tangent_field(int f, const double* t) = 0;
+  virtual void get_tangent_field(int f, double* t) = 0;
 };
 
 template <typename T>
@@ -105,6 +150,12 @@ struct Oracle : Base {
     for (long long n = 0; n < ncell; ++n) d[n] = (double)f[fi][n];
   }
   void set_ww(const int* w) override { memcpy(ww.data(), w, sizeof(int) * ncell); }
+  void set_tangent_field(int fi, const double* t) override {
+    for (long long n = 0; n < ncell; ++n) set_tangent(f[fi][n], t[n]);
+  }
+  void get_tangent_field(int fi, double* t) override {
+    for (long long n = 0; n < ncell; ++n) t[n] = tangent(f[fi][n]);
+  }
   void set_sponge(const float* x, const float* y, const float* z) override {
     for (size_t n = 0; n < dcrjx.size(); ++n) dcrjx[n] = x[n];
     for (size_t n = 0; n < dcrjy.size(); ++n) dcrjy[n] = y[n];
@@ -682,6 +733,8 @@ oracle* oracle_create(int precision, int nxt, int nyt, int nzt, float dh, float 
   if (nthreads <= 0) nthreads = omp_get_max_threads();
   if (precision == 32)
     o->impl = new Oracle<float>(nxt, nyt, nzt, dh, dt, npc, nthreads);
+  else if (precision == 65)
+    o->impl = new Oracle<Dual>(nxt, nyt, nzt, dh, dt, npc, nthreads);
   else
     o->impl = new Oracle<double>(nxt, nyt, nzt, dh, dt, npc, nthreads);
   return o;
@@ -720,6 +773,10 @@ void oracle_add_point_sources(oracle* o, int field, int nq, int nb, const int* i
   o->impl->add_point_sources(field, nq, nb, ix, iy, iz, lx, ly, lz, nsamples, values, stride);
 }
 void oracle_step(oracle* o, int nve, int n) { o->impl->step(nve, n); }
+void oracle_set_tangent(oracle* o, int field, const double* t) {
+  o->impl->set_tangent_field(field, t);
+}
+void oracle_get_tangent(oracle* o, int field, double* t) { o->impl->get_tangent_field(field, t); }
 long long oracle_current_step(oracle* o) { return o->impl->current(); }
 void oracle_gather(oracle* o, int nbgx, int nedx, int nskpx, int nbgy, int nedy, int nskpy,
                    int nbgz, int nedz, int nskpz, float* bx, float* by, float* bz) {

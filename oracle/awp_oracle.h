@@ -21,7 +21,9 @@ extern "C" {
 
 typedef struct oracle oracle;
 
-/* precision: 32 or 64.  nx, ny: global sizes for the free-surface edge test
+/* precision: 32, 64, or 65 = FP64 dual numbers (value + tangent: the exact
+ * derivative of the discrete scheme along one direction, tangent-linear
+ * mode).  nx, ny: global sizes for the free-surface edge test
  * (kernel.cu:1092-1097); npc: 0 sponge, 2 periodic. */
 oracle* oracle_create(int precision, int nxt, int nyt, int nzt, float dh, float dt,
                       int npc, int nthreads);
@@ -60,6 +62,9 @@ void oracle_add_point_sources(oracle* o, int field, int nq, int nb, const int* i
                               const int* iy, const int* iz, const float* lx, const float* ly,
                               const float* lz, int nsamples, const float* values, int stride);
 void oracle_step(oracle* o, int nve, int n);
+/* Tangent part of a field (precision 65; a no-op / zeros otherwise). */
+void oracle_set_tangent(oracle* o, int field, const double* t);
+void oracle_get_tangent(oracle* o, int field, double* t);
 long long oracle_current_step(oracle* o);
 
 /* velbuffer gather (kernel.cu:3948-4011) for grid 0 without FOLLOWBATHY. */

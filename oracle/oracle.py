@@ -55,6 +55,8 @@ def load():
         lib.oracle_current_step.restype = c_longlong
         lib.oracle_current_step.argtypes = [c_void_p]
         lib.oracle_gather.argtypes = [c_void_p] + [c_int] * 9 + [_F] * 3
+        lib.oracle_set_tangent.argtypes = [c_void_p, c_int, POINTER(c_double)]
+        lib.oracle_get_tangent.argtypes = [c_void_p, c_int, POINTER(c_double)]
         _lib = lib
     return _lib
 
@@ -93,6 +95,19 @@ class OracleSim:
     def set_field(self, name, arr):
         self.lib.oracle_set_field(self.o, FIELD[name],
                                   fp(np.ascontiguousarray(arr, np.float32).reshape(self.shape)))
+
+    def set_tangent(self, name, arr):
+        """Tangent part of a field (precision 65, dual numbers)."""
+        a = np.ascontiguousarray(arr, np.float64).reshape(self.shape)
+        self.lib.oracle_set_tangent(self.o, FIELD[name], a.ctypes.data_as(POINTER(c_double)))
+
+    def tangent(self, name):
+        out = np.empty(self.shape, np.float64)
+        self.lib.oracle_get_tangent(self.o, FIELD[name], out.ctypes.data_as(POINTER(c_double)))
+        return out
+
+    def compute_lam_mu(self):
+        self.lib.oracle_compute_lam_mu(self.o)
 
     def set_plasticity(self, fmajor, fminor, Rz, RzT):
         self.lib.oracle_set_plasticity(self.o, fmajor, fminor,

@@ -1,0 +1,152 @@
+"""Adjoint gradient of the seismogram misfit (awp_misfit_gradient).
+
+The GPU gradient (hand-written discrete-adjoint kernels, FP32, checkpointed)
+is checked along seeded directions dm = (dlambda, dmu, drho) against
+  * the FP64 oracle's exact derivative of the same discrete scheme (the oracle
+    run on dual numbers: tangent-linear mode, oracle/awp_oracle.cpp), and
+  * central finite differences of the FP32 GPU misfit, eps = 1e-3 relative.
+Elastic and anelastic (memory variables on) models; receivers at the free
+surface and inside."""
+import numpy as np
+import pytest
+import torch
+
+from awp_b200 import Solver, adjoint, default_params, scenarios
+from oracle import oracle as orc
+from oracle import refbind
+
+pytestmark = pytest.mark.gpu
+
+
+def moduli(scn):
+    m = scn.media
+    vp, vs, rho = (m[..., q].astype(np.float64) for q in range(3))
+    mu = rho * vs * vs
+    lam = rho * (vp * vp - 2 * vs * vs)
+    return lam.astype(np.float32), mu.astype(np.float32), rho.astype(np.float32)
+
+
+def padded(x, p):
+    """Interior [nz][ny][nx] (surface first) -> padded kernel layout with the
+    one-cell border copy of the media set-up."""
+    nx, ny, nz = p["nx"], p["ny"], p["nz"]
+    out = np.zeros(refbind.padded_shape(nx, ny, nz), x.dtype)
+    core = np.ascontiguousarray(x.transpose(2, 1, 0)[:, :, ::-1])
+    out[9:nx + 11, 9:ny + 11, 31:nz + 33] = np.pad(core, 1, mode="edge")
+    return out
+
+
+def receivers(scn):
+    p = scn.params
+    sx, sy = int(scn.src_pos[0, 0]) - 1, int(scn.src_pos[0, 1]) - 1
+    xyz = [(sx + 2, sy, 0), (sx - 3, sy + 2, 0), (sx, sy - 3, 0), (sx + 1, sy + 1, 3),
+           (sx - 2, sy - 1, 5), (sx + 3, sy + 3, 2)]
+    xyz = [(min(max(x, 0), p["nx"] - 1), min(max(y, 0), p["ny"] - 1), z) for x, y, z in xyz]
+    comp = [0, 1, 2, 2, 0, 1]
+    return np.asarray(xyz, np.int32), np.asarray(comp, np.int32)
+
+
+def setup_case(q, seed=11, steps=40):
+    scn = scenarios.random_small(nx=16, ny=16, nz=16, q=q, ifault=1, steps=steps, seed=seed,
+                                 nsrc=1)
+    s = Solver(default_params(**scn.params))
+    s.upload_media(scn.media)
+    s.upload_sources(scn.src_pos, scn.src_data)
+    lam, mu, rho = moduli(scn)
+    rng = np.random.default_rng(seed + 1)
+    pert = [(1 + 0.05 * rng.standard_normal(lam.shape)).astype(np.float32) for _ in range(3)]
+    xyz, comp = receivers(scn)
+    s.set_moduli(lam * pert[0], mu * pert[1], rho * pert[2])
+    s.reset()
+    d_obs = adjoint.seismograms(s, steps, xyz, comp)
+    return scn, s, (lam, mu, rho), xyz, comp, d_obs
+
+
+def J_at(s, m, steps, xyz, comp, d_obs):
+    s.set_moduli(*m)
+    s.reset()
+    seis = adjoint.seismograms(s, steps, xyz, comp).astype(np.float64)
+    return 0.5 * float(np.sum((seis - d_obs) ** 2))
+
+
+def oracle_directional(scn, m, dm, steps, xyz, comp, d_obs):
+    """sum_n sum_r (s - d) ds along dm, by the FP64 dual-number oracle."""
+    p = scn.params
+    setup = refbind.model_setup(scn)
+    o = orc.OracleSim(scn, setup, precision=65)
+    lam, mu, rho = (x.astype(np.float64) for x in m)
+    dl, dmu, dr = (x.astype(np.float64) for x in dm)
+    o.set_field("lam", padded((np.float32(1) / m[0]).astype(np.float32), p))
+    o.set_field("mu", padded((np.float32(1) / m[1]).astype(np.float32), p))
+    o.set_field("d1", padded(m[2], p))
+    o.set_tangent("lam", padded(-dl / (lam * lam), p))
+    o.set_tangent("mu", padded(-dmu / (mu * mu), p))
+    o.set_tangent("d1", padded(dr, p))
+    o.compute_lam_mu()
+    names = ["u1", "v1", "w1"]
+    idx = [(x + 10, y + 10, p["nz"] + 31 - z) for x, y, z in xyz]
+    total = 0.0
+    for n in range(steps):
+        o.step(1)
+        vals = {f: o.field(f, f64=True) for f in set(names[c] for c in comp)}
+        tans = {f: o.tangent(f) for f in vals}
+        for r, (c, ix) in enumerate(zip(comp, idx)):
+            total += (vals[names[c]][ix] - d_obs[n, r]) * tans[names[c]][ix]
+    o.close()
+    return total
+
+
+@pytest.mark.parametrize("q", [True, False])
+def test_gradient_matches_oracle_and_finite_differences(q):
+    steps = 40
+    scn, s, m, xyz, comp, d_obs = setup_case(q, steps=steps)
+    s.set_moduli(*m)
+    s.reset()
+    J, seis, gl, gm, gr = adjoint.misfit_gradient(s, steps, xyz, comp, d_obs)
+    assert J > 0 and np.isfinite(J)
+    assert s.current_step == steps
+    assert np.all(np.isfinite(gl)) and np.all(np.isfinite(gm)) and np.all(np.isfinite(gr))
+    rng = np.random.default_rng(5)
+    eps = 1e-3
+    for d in range(3):
+        dm = tuple((x * rng.standard_normal(x.shape)).astype(np.float64) for x in m)
+        adj = float(np.sum(gl * dm[0]) + np.sum(gm * dm[1]) + np.sum(gr * dm[2]))
+        tan = oracle_directional(scn, m, dm, steps, xyz, comp, d_obs)
+        assert abs(adj - tan) <= 1e-3 * abs(tan), (d, adj, tan)
+        mp = tuple((x + eps * y).astype(np.float32) for x, y in zip(m, dm))
+        mm = tuple((x - eps * y).astype(np.float32) for x, y in zip(m, dm))
+        fd = (J_at(s, mp, steps, xyz, comp, d_obs) - J_at(s, mm, steps, xyz, comp, d_obs)) / (2 * eps)
+        assert abs(adj - fd) <= 1e-3 * abs(adj), (d, adj, fd)
+        print(f"direction {d}: adjoint {adj:.6e}  oracle tangent {tan:.6e}  FD {fd:.6e}")
+    s.close()
+
+
+def test_checkpoint_count_does_not_change_the_gradient():
+    steps = 24
+    scn, s, m, xyz, comp, d_obs = setup_case(True, seed=21, steps=steps)
+    out = []
+    for nsnap in (1, 5, 24):
+        s.set_moduli(*m)
+        s.reset()
+        out.append(adjoint.misfit_gradient(s, steps, xyz, comp, d_obs, nsnap=nsnap))
+    for o in out[1:]:
+        assert o[0] == out[0][0]
+        for a, b in zip(o[2:], out[0][2:]):
+            assert np.array_equal(a, b)
+    s.close()
+
+
+def test_torch_autograd_function():
+    steps = 16
+    scn, s, m, xyz, comp, d_obs = setup_case(True, seed=31, steps=steps)
+    t = [torch.tensor(x, requires_grad=True) for x in m]
+    J = adjoint.misfit(*t, s, steps, xyz, comp, d_obs)
+    J.backward()
+    s.set_moduli(*m)
+    s.reset()
+    J2, _, gl, gm, gr = adjoint.misfit_gradient(s, steps, xyz, comp, d_obs)
+    assert float(J) == J2
+    assert np.array_equal(t[0].grad.numpy(), gl)
+    assert np.array_equal(t[1].grad.numpy(), gm)
+    assert np.array_equal(t[2].grad.numpy(), gr)
+    s.close()
