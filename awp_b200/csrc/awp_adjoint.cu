@@ -8,6 +8,9 @@
 //   fstr^T -> stress^T (memory variables, strain rates, then the images) ->
 //   velocity^T
 //
+// The density term needs the stress divergence the velocity update applied;
+// it is recovered from the velocities before and after the step
+// (fd * D(sigma) = u'/dc - u), so the segment store holds velocities only.
 // Every transpose is written in gather form (each thread owns one output
 // cell and reads the neighbours whose forward stencils touched it), so no
 // atomics are needed and the result is deterministic.  The gradient terms use
@@ -65,8 +68,8 @@ __global__ void k_adj_fstr(const AdjArgs a) {
 // ---------------------------------------------------------------------------
 template <bool ELASTIC>
 __global__ void k_adj_stress_cell(const AdjArgs a) {
-  const int k = a.sk0 + blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = a.sj0 + blockIdx.y;
+  const int k = a.sk0 + blockIdx.x * 32 + threadIdx.x;
+  const int j = a.sj0 + blockIdx.y * 4 + threadIdx.y;
   const int i = a.si0 + blockIdx.z;
   if (k > a.sk1 || j > a.sj1 || i > a.si1) return;
   const long long S = a.g.slice, Y = a.g.yline;
@@ -199,8 +202,8 @@ __global__ void k_adj_stress_cell(const AdjArgs a) {
 // gradients of 1/lambda and 1/mu
 // ---------------------------------------------------------------------------
 __global__ void k_adj_stress_gather(const AdjArgs a) {
-  const int k = a.sk0 - 2 + blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = a.sj0 - 2 + blockIdx.y;
+  const int k = a.sk0 - 2 + blockIdx.x * 32 + threadIdx.x;
+  const int j = a.sj0 - 2 + blockIdx.y * 4 + threadIdx.y;
   const int i = a.si0 - 2 + blockIdx.z;
   if (k > a.sk1 + 2 || j > a.sj1 + 2 || i > a.si1 + 2) return;
   const long long S = a.g.slice, Y = a.g.yline;
@@ -313,34 +316,22 @@ __global__ void k_adj_images_apply(const AdjArgs a) {
 // velocity^T, pointwise part
 // ---------------------------------------------------------------------------
 __global__ void k_adj_vel_cell(const AdjArgs a) {
-  const int k = a.vk0 + blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = a.vj0 + blockIdx.y;
+  const int k = a.vk0 + blockIdx.x * 32 + threadIdx.x;
+  const int j = a.vj0 + blockIdx.y * 4 + threadIdx.y;
   const int i = a.vi0 + blockIdx.z;
   if (k > a.vk1 || j > a.vj1 || i > a.vi1) return;
   const long long S = a.g.slice, Y = a.g.yline;
   const long long p = (long long)i * S + (long long)j * Y + k;
-  const float c1 = a.c1, c2 = a.c2;
   const float* d = a.d1;
   const float r1 = 0.25f * (d[p] + d[p - Y] + d[p - 1] + d[p - Y - 1]);
   const float r2 = 0.25f * (d[p] + d[p + S] + d[p - 1] + d[p + S - 1]);
   const float r3 = 0.25f * (d[p] + d[p + S] + d[p - Y] + d[p + S - Y]);
   const float fd1 = a.dth / r1, fd2 = a.dth / r2, fd3 = a.dth / r3;
   const float dc = a.dcrjx[i] * a.dcrjy[j] * a.dcrjz[k];
-  const float* xx = a.fxx;
-  const float* yy = a.fyy;
-  const float* zz = a.fzz;
-  const float* xy = a.fxy;
-  const float* xz = a.fxz;
-  const float* yz = a.fyz;
-  const float Du = c1 * (xx[p] - xx[p - S]) + c2 * (xx[p + S] - xx[p - 2 * S]) +
-                   c1 * (xy[p] - xy[p - Y]) + c2 * (xy[p + Y] - xy[p - 2 * Y]) +
-                   c1 * (xz[p] - xz[p - 1]) + c2 * (xz[p + 1] - xz[p - 2]);
-  const float Dv = c1 * (xy[p + S] - xy[p]) + c2 * (xy[p + 2 * S] - xy[p - S]) +
-                   c1 * (yy[p + Y] - yy[p]) + c2 * (yy[p + 2 * Y] - yy[p - Y]) +
-                   c1 * (yz[p] - yz[p - 1]) + c2 * (yz[p + 1] - yz[p - 2]);
-  const float Dw = c1 * (xz[p + S] - xz[p]) + c2 * (xz[p + 2 * S] - xz[p - S]) +
-                   c1 * (yz[p] - yz[p - Y]) + c2 * (yz[p + Y] - yz[p - 2 * Y]) +
-                   c1 * (zz[p + 1] - zz[p]) + c2 * (zz[p + 2] - zz[p - 1]);
+  // fd * D(sigma) * dc of the forward update = u' - dc u
+  const float su = a.fu[p] - dc * a.bu[p];
+  const float sv = a.fv[p] - dc * a.bv[p];
+  const float sw = a.fw[p] - dc * a.bw[p];
   const float lu = a.L[LU][p], lv = a.L[LV][p], lw = a.L[LW][p];
   a.L[LU][p] = dc * lu;
   a.L[LV][p] = dc * lv;
@@ -348,10 +339,11 @@ __global__ void k_adj_vel_cell(const AdjArgs a) {
   a.V[VA][p] = fd1 * dc * lu;
   a.V[VB][p] = fd2 * dc * lv;
   a.V[VC][p] = fd3 * dc * lw;
-  // d fd / d rho_avg = -fd / rho_avg, each of the four densities weighs 1/4
-  a.V[VEA][p] = -0.25f * fd1 / r1 * Du * dc * lu;
-  a.V[VEB][p] = -0.25f * fd2 / r2 * Dv * dc * lv;
-  a.V[VEC][p] = -0.25f * fd3 / r3 * Dw * dc * lw;
+  // d fd / d rho_avg = -fd / rho_avg, each of the four densities weighs 1/4:
+  // d u' / d d(q) = -1/4 * (fd D dc) / rho_avg
+  a.V[VEA][p] = -0.25f / r1 * su * lu;
+  a.V[VEB][p] = -0.25f / r2 * sv * lv;
+  a.V[VEC][p] = -0.25f / r3 * sw * lw;
 }
 
 // ---------------------------------------------------------------------------
@@ -359,8 +351,8 @@ __global__ void k_adj_vel_cell(const AdjArgs a) {
 // density weights -> the density gradient
 // ---------------------------------------------------------------------------
 __global__ void k_adj_vel_gather(const AdjArgs a) {
-  const int k = a.vk0 - 2 + blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = a.vj0 - 2 + blockIdx.y;
+  const int k = a.vk0 - 2 + blockIdx.x * 32 + threadIdx.x;
+  const int j = a.vj0 - 2 + blockIdx.y * 4 + threadIdx.y;
   const int i = a.vi0 - 2 + blockIdx.z;
   if (k > a.vk1 + 2 || j > a.vj1 + 2 || i > a.vi1 + 2) return;
   const long long S = a.g.slice, Y = a.g.yline;
@@ -473,17 +465,18 @@ inline unsigned cdiv(long long a, long long b) { return (unsigned)((a + b - 1) /
 cudaError_t awp_launch_adjoint_step(const AdjArgs& a, cudaStream_t st) {
   const int fj = a.fj1 - a.sj0 + 1, si = a.si1 - a.si0 + 1, sj = a.sj1 - a.sj0 + 1,
             sk = a.sk1 - a.sk0 + 1;
+  const dim3 blk(32, 4);
   k_adj_fstr<<<dim3(cdiv(fj, 128), si), 128, 0, st>>>(a);
   if (a.elastic)
-    k_adj_stress_cell<true><<<dim3(cdiv(sk, 32), sj, si), 32, 0, st>>>(a);
+    k_adj_stress_cell<true><<<dim3(cdiv(sk, 32), cdiv(sj, 4), si), blk, 0, st>>>(a);
   else
-    k_adj_stress_cell<false><<<dim3(cdiv(sk, 32), sj, si), 32, 0, st>>>(a);
-  k_adj_stress_gather<<<dim3(cdiv(sk + 4, 32), sj + 4, si + 4), 32, 0, st>>>(a);
+    k_adj_stress_cell<false><<<dim3(cdiv(sk, 32), cdiv(sj, 4), si), blk, 0, st>>>(a);
+  k_adj_stress_gather<<<dim3(cdiv(sk + 4, 32), cdiv(sj + 4, 4), si + 4), blk, 0, st>>>(a);
   k_adj_images<<<dim3(cdiv(sj + 2, 128), si + 2), 128, 0, st>>>(a);
   k_adj_images_apply<<<dim3(cdiv(sj + 2, 128), si + 2), 128, 0, st>>>(a);
   const int vi = a.vi1 - a.vi0 + 1, vj = a.vj1 - a.vj0 + 1, vk = a.vk1 - a.vk0 + 1;
-  k_adj_vel_cell<<<dim3(cdiv(vk, 32), vj, vi), 32, 0, st>>>(a);
-  k_adj_vel_gather<<<dim3(cdiv(vk + 4, 32), vj + 4, vi + 4), 32, 0, st>>>(a);
+  k_adj_vel_cell<<<dim3(cdiv(vk, 32), cdiv(vj, 4), vi), blk, 0, st>>>(a);
+  k_adj_vel_gather<<<dim3(cdiv(vk + 4, 32), cdiv(vj + 4, 4), vi + 4), blk, 0, st>>>(a);
   return cudaGetLastError();
 }
 

@@ -8,9 +8,9 @@
 #include "awp_common.h"
 
 struct AdjArgs {
-  // forward state: stresses before the step (velocity half), velocities after
-  // the step (stress half, free-surface images included)
-  const float *fxx, *fyy, *fzz, *fxy, *fxz, *fyz;
+  // forward state: velocities before the step (velocity half) and after it
+  // (both halves; free-surface images included)
+  const float *bu, *bv, *bw;
   const float *fu, *fv, *fw;
   // adjoint state, updated in place (u v w xx yy zz xy xz yz r1..r6)
   float* L[15];

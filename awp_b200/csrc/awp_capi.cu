@@ -1840,7 +1840,7 @@ int awp_misfit_gradient(awp_ctx* c, int nsteps, int nrec, const int* rec_xyz, co
   int L = nsnap > 0 ? (nsteps + nsnap - 1) / nsnap : (int)ceil(sqrt((double)nsteps));
   L = std::max(1, std::min(L, nsteps));
   const int nseg = (nsteps + L - 1) / L;
-  const size_t fields = (size_t)(nseg + 1) * 15 + (size_t)L * 9 + 15 + 17 + 3;
+  const size_t fields = (size_t)(nseg + 1) * 15 + (size_t)(L + 1) * 3 + 15 + 17 + 3;
   size_t freeb = 0, totb = 0;
   CU_TRY(cudaMemGetInfo(&freeb, &totb));
   if (fields * fb + (64u << 20) > freeb)
@@ -1936,8 +1936,9 @@ int awp_misfit_gradient(awp_ctx* c, int nsteps, int nrec, const int* rec_xyz, co
     a.gx_lim = sa.gx_lim; a.gy_min = sa.gy_min; a.lam_mu_ld = sa.lam_mu_ld;
     a.fj1 = make_fstr_args(c).j1;
   }
-  // segment store: stresses before and velocities after each step of a segment
-  std::vector<float*> seg((size_t)L * 9, nullptr);
+  // segment store: the velocities at the start of a segment and after each
+  // of its steps (slot 0 = start)
+  std::vector<float*> seg((size_t)(L + 1) * 3, nullptr);
   for (auto& q : seg)
     if (!(q = b.f(cp))) return set_error(AWP_ERR_NOMEM, "segment store");
   float* const Lvel[3] = {a.L[0], a.L[1], a.L[2]};
@@ -1946,24 +1947,21 @@ int awp_misfit_gradient(awp_ctx* c, int nsteps, int nrec, const int* rec_xyz, co
   for (int s = nseg - 1; s >= 0; --s) {
     const int n0 = s * L, n1 = std::min(nsteps, n0 + L);
     if ((e = restore(s))) return e;
+    for (int q = 0; q < 3; ++q)
+      CU_TRY(cudaMemcpyAsync(seg[q], c->f[AWP_U1 + q], fb, cudaMemcpyDeviceToDevice, st));
     for (int n = n0; n < n1; ++n) {
-      float** slot = &seg[(size_t)(n - n0) * 9];
-      // the stresses the velocity update of this step reads include the
-      // step-1 source sample added before the first step
-      if ((e = initial_source(c))) return e;
-      for (int q = 0; q < 6; ++q)
-        CU_TRY(cudaMemcpyAsync(slot[q], c->f[AWP_XX + q], fb, cudaMemcpyDeviceToDevice, st));
       if ((e = one_step(c))) return e;
+      float** slot = &seg[(size_t)(n - n0 + 1) * 3];
       for (int q = 0; q < 3; ++q)
-        CU_TRY(cudaMemcpyAsync(slot[6 + q], c->f[AWP_U1 + q], fb, cudaMemcpyDeviceToDevice, st));
+        CU_TRY(cudaMemcpyAsync(slot[q], c->f[AWP_U1 + q], fb, cudaMemcpyDeviceToDevice, st));
     }
     for (int n = n1 - 1; n >= n0; --n) {
       // the misfit term of the state after step n (its sample index is n)
       CU_TRY(awp_launch_adjoint_inject(Lvel, d_idx, d_comp, d_res + (size_t)n * nrec, nrec, st));
-      float** slot = &seg[(size_t)(n - n0) * 9];
-      a.fxx = slot[0]; a.fyy = slot[1]; a.fzz = slot[2];
-      a.fxy = slot[3]; a.fxz = slot[4]; a.fyz = slot[5];
-      a.fu = slot[6]; a.fv = slot[7]; a.fw = slot[8];
+      float** before = &seg[(size_t)(n - n0) * 3];
+      float** after = &seg[(size_t)(n - n0 + 1) * 3];
+      a.bu = before[0]; a.bv = before[1]; a.bw = before[2];
+      a.fu = after[0]; a.fv = after[1]; a.fw = after[2];
       CU_TRY(awp_launch_adjoint_step(a, st));
     }
   }

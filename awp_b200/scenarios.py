@@ -107,6 +107,43 @@ def layered_vk(nx=512, ny=512, nz=256, h=50.0, dt=0.0035, steps=2000, nsub=200,
                     f"{nsub} kinematic subfaults")
 
 
+def adjoint_case(nx=256, ny=256, nz=128, h=100.0, dt=0.005, steps=1500, nrec=64, seed=5,
+                 smooth_m=1000.0, f0=2.0, m0=1e15):
+    """Misfit-gradient workload: true model = the anelastic 1-D gradient + von
+    Karman medium (seeded), start model = the same smoothed by a Gaussian of
+    `smooth_m` metres; a moment-tensor point source (IFAULT 1, Mxy Ricker') at
+    a quarter depth and `nrec` surface receivers on a seeded random layout.
+    Returns (scenario of the start model, (lam, mu, rho) true, (lam, mu, rho)
+    start, rec_xyz, rec_comp); moduli arrays [nz][ny][nx], surface first."""
+    import scipy.ndimage as ndi
+    true = layered_vk(nx=nx, ny=ny, nz=nz, h=h, dt=dt, steps=steps, nsub=1, seed_medium=seed,
+                      seed_src=seed + 1)
+    med = true.media
+    sig = smooth_m / h
+    start_media = med.copy()
+    for q in range(3):
+        start_media[..., q] = ndi.gaussian_filter(med[..., q], sig, mode="nearest")
+
+    def moduli(m):
+        vp, vs, rho = (m[..., q].astype(np.float64) for q in range(3))
+        return ((rho * (vp * vp - 2 * vs * vs)).astype(np.float32),
+                (rho * vs * vs).astype(np.float32), rho.astype(np.float32))
+
+    nst = steps + 1
+    data = np.zeros((1, nst, 6), np.float32)
+    data[0, :, 5] = ricker_derivative(nst, dt, f0) * m0
+    pos = np.array([[nx // 2, ny // 2, nz - nz // 4]], np.int32)
+    params = dict(true.params, ifault=1, nst=nst, read_step=nst)
+    scn = Scenario("adjoint_case", params, start_media, pos, data, steps,
+                   f"misfit gradient {nx}x{ny}x{nz}, h={h}, dt={dt}, {steps} steps, "
+                   f"{nrec} surface receivers, start model smoothed by {smooth_m:g} m")
+    rng = np.random.default_rng(seed + 2)
+    xyz = np.stack([rng.integers(nx // 8, nx - nx // 8, nrec), rng.integers(ny // 8, ny - ny // 8, nrec),
+                    np.zeros(nrec, np.int64)], 1).astype(np.int32)
+    comp = rng.integers(0, 3, nrec).astype(np.int32)
+    return scn, moduli(med), moduli(start_media), xyz, comp
+
+
 def kinematic_fault(nx, ny, nz, h, nsub, seed, strike=0.0, dip=90.0, rake=180.0):
     """Random subfaults on a vertical plane x = nx/2 (IFAULT=5 layout, source.c:165-181)."""
     rng = np.random.default_rng(seed)

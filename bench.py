@@ -525,6 +525,81 @@ def run_batched(args) -> dict:
     }
 
 
+def run_adjoint(args) -> dict:
+    """Misfit gradient (discrete adjoint, sqrt(N) snapshots): its cost against
+    the forward run of the same steps, and central finite differences of the
+    misfit along seeded directions (eps = 1e-3 relative)."""
+    import torch
+    from awp_b200 import Solver, adjoint, default_params, scenarios
+
+    nx, ny, nz = args.grid if args.grid else (256, 256, 128)
+    steps = args.adj_steps
+    scn, m_true, m0, xyz, comp = scenarios.adjoint_case(nx=nx, ny=ny, nz=nz, steps=steps)
+    stream = torch.cuda.Stream()
+    s = Solver(default_params(**scn.params), stream=stream.cuda_stream)
+    s.upload_media(scn.media)
+    s.upload_sources(scn.src_pos, scn.src_data)
+    s.set_moduli(*m_true)
+    s.reset()
+    d_obs = adjoint.seismograms(s, steps, xyz, comp)
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        out = fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1), out
+
+    s.set_moduli(*m0)
+    s.reset()
+    adjoint.seismograms(s, min(steps, 20), xyz, comp)  # warm-up
+    sampler = ClockSampler(torch.cuda.current_device())
+    sampler.start()
+    s.reset()
+    ms_fwd, _ = timed(lambda: adjoint.seismograms(s, steps, xyz, comp))
+    s.reset()
+    ms_adj, (J, seis, gl, gm, gr) = timed(
+        lambda: adjoint.misfit_gradient(s, steps, xyz, comp, d_obs))
+    clocks = sampler.stop()
+    # finite differences along seeded relative directions
+    rng = np.random.default_rng(8)
+    eps = 1e-3
+    fd_rows = []
+    for d in range(args.fd_dirs):
+        dm = [(x * rng.standard_normal(x.shape)).astype(np.float64) for x in m0]
+        adj_dir = float(sum(np.sum(g.astype(np.float64) * x) for g, x in zip((gl, gm, gr), dm)))
+        Js = []
+        for sgn in (1.0, -1.0):
+            mp = [(x + sgn * eps * y).astype(np.float32) for x, y in zip(m0, dm)]
+            s.set_moduli(*mp)
+            s.reset()
+            sp = adjoint.seismograms(s, steps, xyz, comp).astype(np.float64)
+            Js.append(0.5 * float(np.sum((sp - d_obs) ** 2)))
+        fd = (Js[0] - Js[1]) / (2 * eps)
+        fd_rows.append({"adjoint": adj_dir, "fd": fd,
+                        "rel_err": abs(adj_dir - fd) / max(abs(fd), 1e-300)})
+    cells = nx * ny * nz
+    s.close()
+    return {
+        "metric": "adjoint gradient cost / forward cost (sqrt(N) snapshots) on 1 B200",
+        "value": ms_adj / ms_fwd, "unit": "x forward", "n_gpus": 1, "steps": steps,
+        "warmup": 1, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded)",
+        "config": {"workload": scn.description, "grid": [nx, ny, nz], "cells": cells,
+                   "receivers": int(len(comp)), "snapshots": int(np.ceil(np.sqrt(steps))) + 1,
+                   "l2": "state of GBs >> 126 MB L2, no flush needed"},
+        "forward_ms": ms_fwd, "adjoint_ms": ms_adj,
+        "forward_gcell_updates_s": cells * steps / (ms_fwd * 1e-3) / 1e9,
+        "misfit": J,
+        "fd_check": {"eps_rel": eps, "directions": fd_rows,
+                     "max_rel_err": max(r["rel_err"] for r in fd_rows) if fd_rows else None},
+        "clocks": clocks,
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -532,7 +607,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="layered_vk",
-                    choices=["layered_vk", "halfspace", "batched"])
+                    choices=["layered_vk", "halfspace", "batched", "adjoint"])
+    ap.add_argument("--adj-steps", type=int, default=1500,
+                    help="time steps of the misfit-gradient run (--workload adjoint)")
+    ap.add_argument("--fd-dirs", type=int, default=8,
+                    help="finite-difference directions (--workload adjoint)")
     ap.add_argument("--batch-n", type=int, default=96,
                     help="instances of the batched ensemble (--workload batched)")
     ap.add_argument("--topography", action="store_true",
@@ -558,6 +637,8 @@ def main():
         line = run_reference(args, rank)
     elif args.workload == "batched":
         line = run_batched(args) if rank == 0 else None
+    elif args.workload == "adjoint":
+        line = run_adjoint(args) if rank == 0 else None
     else:
         if world > 1:
             import datetime
