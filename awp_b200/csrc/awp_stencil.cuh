@@ -3,21 +3,23 @@
 
 #include <math.h>
 
-// Q(f) weight (kernel.cu:974-1040).  The reference switches on
-// 1./(q*2.0) <= 200.0 evaluated in double; for float q that is exactly
-// (2q >= qthr) for positive q, true for negative q and -0, false for +0/NaN.
+// Q(f) weight (kernel.cu:974-1040) before its division by wwo.  The reference
+// switches on 1./(q*2.0) <= 200.0 evaluated in double; for float q that is
+// exactly (2q >= qthr) for positive q, true for negative q and -0, false for
+// +0/NaN.  The reference evaluates the polynomial c0 (2q)^2 + c1 (2q) in
+// double; here it is float (the two differ by about one float ulp, far below
+// the 1e-5 parity bar, at a fraction of the instructions).
+__device__ __forceinline__ float awp_qf_weight_num(float q, float wwo, float c0, float c1,
+                                               float qthr) {
+  const float x = __fmul_rn(2.0f, q);
+  const bool low = (x >= qthr) || (x < 0.f) || (x == 0.f && signbit(x));
+  return low ? __fmaf_rn(__fmul_rn(c0, x), x, __fmul_rn(c1, x))
+             : __fmul_rn(__fmul_rn(2.0f, wwo), q);
+}
+
 __device__ __forceinline__ float awp_qf_weight(float q, float wwo, float c0, float c1,
                                            float qthr) {
-  const float x = 2.0f * q;
-  const bool low = (x >= qthr) || (x < 0.f) || (x == 0.f && signbit(x));
-  float w;
-  if (low) {
-    const double xd = 2.0 * (double)q;
-    w = (float)__fma_rn(__dmul_rn((double)c0, xd), xd, __dmul_rn((double)c1, xd));
-  } else {
-    w = __fmul_rn(__fmul_rn(2.0f, wwo), q);
-  }
-  return w / wwo;  // a division is never contracted; '/' keeps the build's division mode
+  return awp_qf_weight_num(q, wwo, c0, c1, qthr) / wwo;  // the build's division mode
 }
 
 // ---------------------------------------------------------------------------
@@ -62,10 +64,12 @@ struct AwpStrCoef {
 
 // L8, M8, QP8, QS8: the eight-cell sums of lam, mu, qp, qs in the reference's
 // order; mu0 = mu(i,j,k), muk = mu(i,j,k-1), muj = mu(i,j-1,k), mui = mu(i+1,j,k)
-// (same for qs).  The reference divides in double and rounds to float
-// ((float)(8.0/(double)x)); for float operands that equals the correctly
-// rounded float quotient (double rounding is innocuous for division when the
-// wider format has at least 2p+2 = 50 bits, and double has 53).
+// (same for qs).  The reference divides in double ((float)(8.0/(double)x),
+// the correctly rounded quotient); here the five harmonic-mean quotients and
+// the five Q(f) weights use the hardware reciprocal (within two ulp of the
+// correctly rounded value), which keeps the stress update off the division
+// slow path; the parity tests hold the result to the reference build at
+// relative L2 1e-5.
 template <bool ELASTIC>
 __device__ __forceinline__ AwpStrCoef awp_stress_coef(float L8, float M8, float mu0, float muk,
                                                       float muj, float mui, float QP8, float QS8,
@@ -74,19 +78,25 @@ __device__ __forceinline__ AwpStrCoef awp_stress_coef(float L8, float M8, float 
                                                       float cc0, float cc1, float qthr,
                                                       float dth, float dh1, float DT) {
   AwpStrCoef r;
-  float xl = __fdiv_rn(8.0f, L8);
-  float xm = __fdiv_rn(16.0f, M8);
-  float xmu1 = __fdiv_rn(2.0f, __fadd_rn(mu0, muk));
-  float xmu2 = __fdiv_rn(2.0f, __fadd_rn(mu0, muj));
-  float xmu3 = __fdiv_rn(2.0f, __fadd_rn(mu0, mui));
+  float xl = __fdividef(8.0f, L8);
+  float xm = __fdividef(16.0f, M8);
+  float xmu1 = __fdividef(2.0f, __fadd_rn(mu0, muk));
+  float xmu2 = __fdividef(2.0f, __fadd_rn(mu0, muj));
+  float xmu3 = __fdividef(2.0f, __fadd_rn(mu0, mui));
   xl = __fadd_rn(xl, xm);
   float h = 0.f, h1 = 0.f, h2 = 0.f, h3 = 0.f, qpa = 0.f;
   if (!ELASTIC) {
-    const float qpaw = awp_qf_weight(__fmul_rn(0.0625f, QP8), f_wwo, cc0, cc1, qthr);
-    const float hw = awp_qf_weight(__fmul_rn(0.0625f, QS8), f_wwo, cc0, cc1, qthr);
-    const float h1w = awp_qf_weight(__fmul_rn(0.25f, __fadd_rn(qs0, qsk)), f_wwo, cc0, cc1, qthr);
-    const float h2w = awp_qf_weight(__fmul_rn(0.25f, __fadd_rn(qs0, qsj)), f_wwo, cc0, cc1, qthr);
-    const float h3w = awp_qf_weight(__fmul_rn(0.25f, __fadd_rn(qs0, qsi)), f_wwo, cc0, cc1, qthr);
+    const float iw = __fdividef(1.0f, f_wwo);
+    const float qpaw =
+        __fmul_rn(awp_qf_weight_num(__fmul_rn(0.0625f, QP8), f_wwo, cc0, cc1, qthr), iw);
+    const float hw =
+        __fmul_rn(awp_qf_weight_num(__fmul_rn(0.0625f, QS8), f_wwo, cc0, cc1, qthr), iw);
+    const float h1w = __fmul_rn(
+        awp_qf_weight_num(__fmul_rn(0.25f, __fadd_rn(qs0, qsk)), f_wwo, cc0, cc1, qthr), iw);
+    const float h2w = __fmul_rn(
+        awp_qf_weight_num(__fmul_rn(0.25f, __fadd_rn(qs0, qsj)), f_wwo, cc0, cc1, qthr), iw);
+    const float h3w = __fmul_rn(
+        awp_qf_weight_num(__fmul_rn(0.25f, __fadd_rn(qs0, qsi)), f_wwo, cc0, cc1, qthr), iw);
     h = __fmul_rn(__fmul_rn(-xm, hw), dh1);
     h1 = __fmul_rn(__fmul_rn(-xmu1, h1w), dh1);
     h2 = __fmul_rn(__fmul_rn(-xmu2, h2w), dh1);

@@ -190,6 +190,9 @@ __global__ void __launch_bounds__(NT, 2)
   // and the slots of the oldest planes read (halo i-2, media i)
   Cursor wh{4, 0u}, wm{1, 0u}, wo{0, 0u};
   int sh = 0, sm = 0;
+  // media of the current x plane at (j,k), (j-1,k), (j,k-1), (j-1,k-1): the
+  // next plane's values of one step are the current plane's of the next
+  float cl[4], cmu[4], cqp[4], cqs[4];
   for (int i = ib; i <= ie; ++i) {
     // ---- wait for the planes this step reads for the first time ------------
     if (i == ib) {
@@ -242,30 +245,43 @@ __global__ void __launch_bounds__(NT, 2)
       pc = q[-1];
       pd = q[-MX - 1];
     };
-    float la, lb, lc, ld, na, nb, nc, nd;
-    m4(Mc, 0, la, lb, lc, ld);
-    m4(Mn, 0, na, nb, nc, nd);
-    float ma, mb, mc, md, pa, pb, pc, pd;
-    m4(Mc, 1, ma, mb, mc, md);
-    m4(Mn, 1, pa, pb, pc, pd);
+    if (i == ib) {
+      m4(Mc, 0, cl[0], cl[1], cl[2], cl[3]);
+      m4(Mc, 1, cmu[0], cmu[1], cmu[2], cmu[3]);
+      if (!ELASTIC) {
+        m4(Mc, 2, cqp[0], cqp[1], cqp[2], cqp[3]);
+        m4(Mc, 3, cqs[0], cqs[1], cqs[2], cqs[3]);
+      }
+    }
+    float nl[4], nmu[4], nqp[4], nqs[4];
+    m4(Mn, 0, nl[0], nl[1], nl[2], nl[3]);
+    m4(Mn, 1, nmu[0], nmu[1], nmu[2], nmu[3]);
     const int t = awp_tex_index(a.tex, i, j, k);
     const float f_vx1 = a.tex.tau1[t], f_vx2 = a.tex.tau2[t], f_wwo = a.tex.wwo8[t];
-    float QP8 = 0.f, QS8 = 0.f, qa = 0.f, qb = 0.f, qc = 0.f, ra = 0.f, cc0 = 0.f, cc1 = 0.f;
+    float QP8 = 0.f, QS8 = 0.f, cc0 = 0.f, cc1 = 0.f;
     if (!ELASTIC) {
       cc0 = a.coeff[2 * t];
       cc1 = a.coeff[2 * t + 1];
-      float qd, rb, rc, rd;
-      m4(Mc, 2, qa, qb, qc, qd);
-      m4(Mn, 2, ra, rb, rc, rd);
-      QP8 = qa + ra + qb + rb + qc + rc + qd + rd;
-      m4(Mc, 3, qa, qb, qc, qd);
-      m4(Mn, 3, ra, rb, rc, rd);
-      QS8 = qa + ra + qb + rb + qc + rc + qd + rd;
+      m4(Mn, 2, nqp[0], nqp[1], nqp[2], nqp[3]);
+      m4(Mn, 3, nqs[0], nqs[1], nqs[2], nqs[3]);
+      QP8 = cqp[0] + nqp[0] + cqp[1] + nqp[1] + cqp[2] + nqp[2] + cqp[3] + nqp[3];
+      QS8 = cqs[0] + nqs[0] + cqs[1] + nqs[1] + cqs[2] + nqs[2] + cqs[3] + nqs[3];
     }
     // eight-cell sums in the reference's order: pos, ip1, jm1, ijk, km1, ik1, jk1, ijk1
     const AwpStrCoef cf = awp_stress_coef<ELASTIC>(
-        la + na + lb + nb + lc + nc + ld + nd, ma + pa + mb + pb + mc + pc + md + pd, ma, mc, mb,
-        pa, QP8, QS8, qa, qc, qb, ra, f_vx1, f_vx2, f_wwo, cc0, cc1, a.qthr, dth, dh1, DT);
+        cl[0] + nl[0] + cl[1] + nl[1] + cl[2] + nl[2] + cl[3] + nl[3],
+        cmu[0] + nmu[0] + cmu[1] + nmu[1] + cmu[2] + nmu[2] + cmu[3] + nmu[3], cmu[0], cmu[2],
+        cmu[1], nmu[0], QP8, QS8, cqs[0], cqs[2], cqs[1], nqs[0], f_vx1, f_vx2, f_wwo, cc0, cc1,
+        a.qthr, dth, dh1, DT);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      cl[q] = nl[q];
+      cmu[q] = nmu[q];
+      if (!ELASTIC) {
+        cqp[q] = nqp[q];
+        cqs[q] = nqs[q];
+      }
+    }
     const float dcrj = LDG(a.dcrjx + i) * dcy * dcz;
     const long long o = (long long)i * S;
 

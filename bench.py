@@ -595,9 +595,42 @@ def run_adjoint(args) -> dict:
         "forward_gcell_updates_s": cells * steps / (ms_fwd * 1e-3) / 1e9,
         "misfit": J,
         "fd_check": {"eps_rel": eps, "directions": fd_rows,
-                     "max_rel_err": max(r["rel_err"] for r in fd_rows) if fd_rows else None},
+                     "max_rel_err": max(r["rel_err"] for r in fd_rows) if fd_rows else None,
+                     # errors against the typical size of a directional derivative
+                     # (one seeded direction can be nearly orthogonal to the gradient)
+                     "max_err_over_rms_fd": (max(abs(r["adjoint"] - r["fd"]) for r in fd_rows) /
+                                             max(float(np.sqrt(np.mean([r["fd"] ** 2 for r in fd_rows]))),
+                                                 1e-300)) if fd_rows else None},
         "clocks": clocks,
     }
+
+
+def run_extras(args) -> dict:
+    """The other two parts of the metric, as sub-objects of the headline line:
+    batched vs plain on the 96-instance ensemble, and the adjoint gradient's
+    cost against the forward run (with its finite-difference check)."""
+    out = {}
+    sub = argparse.Namespace(**{**vars(args), "steps": 20, "warmup": 3, "batch_n": 96,
+                                "adj_steps": 1500, "fd_dirs": 8, "grid": None})
+    try:
+        b = run_batched(sub)
+        out["batched"] = {k: b[k] for k in ("metric", "value", "unit", "ms_per_step", "plain",
+                                             "plain_concurrent", "batched_over_plain",
+                                             "batched_over_plain_concurrent", "gpu_launches")}
+        out["batched"]["config"] = {k: b["config"][k] for k in ("workload", "cells", "instances",
+                                                              "sizes_drawn")}
+        out["batched"]["tuning"] = b["batch"]["tuning"]
+    except Exception as exc:  # reported, never substituted
+        out["batched"] = {"unavailable": f"{type(exc).__name__}: {exc}"}
+    try:
+        a = run_adjoint(sub)
+        out["adjoint"] = {k: a[k] for k in ("metric", "value", "unit", "forward_ms",
+                                             "adjoint_ms", "misfit")}
+        out["adjoint"]["config"] = a["config"]
+        out["adjoint"]["fd_check"] = a["fd_check"]
+    except Exception as exc:
+        out["adjoint"] = {"unavailable": f"{type(exc).__name__}: {exc}"}
+    return out
 
 
 def main():
@@ -617,6 +650,8 @@ def main():
     ap.add_argument("--topography", action="store_true",
                     help="curvilinear top grid (INTOPO) on the same workload")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the batched and adjoint sub-measurements of the default line")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ref-gpu", action="store_true")
     ap.add_argument("--no-tune", action="store_true")
@@ -652,6 +687,10 @@ def main():
         if dist is not None:
             dist.barrier()
             dist.destroy_process_group()
+    if (line is not None and args.impl == "ours" and world == 1 and
+            args.workload == "layered_vk" and not args.no_extras and args.grid is None and
+            not args.topography):
+        line.update(run_extras(args))
     if line is not None:
         print(json.dumps(line), flush=True)
 
