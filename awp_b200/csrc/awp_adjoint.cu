@@ -8,6 +8,11 @@
 //   fstr^T -> stress^T (memory variables, strain rates, then the images) ->
 //   velocity^T
 //
+// (the fstr transpose is folded into the stress kernel's top three cells; the
+// imaged values above the surface are cleared with the velocity images).  The
+// free-surface imaging of the rows beyond the stress range (the extra row of
+// an odd ny) acts on values that stay zero, so it has no transpose to apply.
+//
 // The density term needs the stress divergence the velocity update applied;
 // it is recovered from the velocities before and after the step
 // (fd * D(sigma) = u'/dc - u), so the segment store holds velocities only.
@@ -32,35 +37,6 @@ namespace {
 enum { LU, LV, LW, LXX, LYY, LZZ, LXY, LXZ, LYZ, LR1, LR2, LR3, LR4, LR5, LR6 };
 enum { E1, E2, E3, E4, E5, E6, GL8, GM8, GP1, GP2, GP3 };
 enum { VA, VB, VC, VEA, VEB, VEC };
-
-// ---------------------------------------------------------------------------
-// fstr^T over the imaged columns (i, j) of the top layer
-// ---------------------------------------------------------------------------
-__global__ void k_adj_fstr(const AdjArgs a) {
-  const int j = a.sj0 + blockIdx.x * blockDim.x + threadIdx.x;
-  const int i = a.si0 + blockIdx.y;
-  if (j > a.fj1 || i > a.si1) return;
-  const long long p = (long long)i * a.g.slice + (long long)j * a.g.yline + a.g.top();
-  float* zz = a.L[LZZ];
-  float* xz = a.L[LXZ];
-  float* yz = a.L[LYZ];
-  // forward: zz(t+1) = -zz(t); zz(t+2) = -zz(t-1); xz(t+1) = -xz(t-1);
-  // xz(t+2) = -xz(t-2); yz likewise; xz(t) = yz(t) = 0
-  zz[p] -= zz[p + 1];
-  zz[p - 1] -= zz[p + 2];
-  zz[p + 1] = 0.f;
-  zz[p + 2] = 0.f;
-  xz[p - 1] -= xz[p + 1];
-  xz[p - 2] -= xz[p + 2];
-  xz[p] = 0.f;
-  xz[p + 1] = 0.f;
-  xz[p + 2] = 0.f;
-  yz[p - 1] -= yz[p + 1];
-  yz[p - 2] -= yz[p + 2];
-  yz[p] = 0.f;
-  yz[p + 1] = 0.f;
-  yz[p + 2] = 0.f;
-}
 
 // ---------------------------------------------------------------------------
 // stress^T, pointwise part: memory variables and stresses in place, adjoint
@@ -125,6 +101,25 @@ __global__ void k_adj_stress_cell(const AdjArgs a) {
   const float al = DT * (1.0f + fvx2 * fvx1);   // coefficient of r in sigma
   const float be = fvx2, ga = fvx2 * (1.0f - fvx1);
 
+  // fstr^T of this column's top three cells (the imaged values above the
+  // surface are cleared later, in k_adj_images_apply): zz(t) += -zz(t+1),
+  // zz(t-1) += -zz(t+2), xz/yz(t-1) += -xz/yz(t+1), xz/yz(t-2) += -xz/yz(t+2),
+  // xz/yz(t) after the imaging is zero
+  const int top = a.g.top();
+  auto fs = [&](int f) -> float {  // adjoint of the field after the stress update
+    const float* Lf = a.L[f];
+    float v = Lf[p];
+    if (k == top) {
+      if (f == LZZ) v -= Lf[p + 1];
+      if (f == LXZ || f == LYZ) v = 0.f;
+    } else if (k == top - 1) {
+      if (f == LZZ) v -= Lf[p + 3];
+      if (f == LXZ || f == LYZ) v -= Lf[p + 2];
+    } else if (k == top - 2) {
+      if (f == LXZ || f == LYZ) v -= Lf[p + 4];
+    }
+    return v;
+  };
   float* L = nullptr;
   // normal components
   float PX, PY, PZ, QX = 0.f, QY = 0.f, QZ = 0.f;
@@ -138,7 +133,7 @@ __global__ void k_adj_stress_cell(const AdjArgs a) {
     PY = K * K * ly;
     L[p] = K * K * ly;
     L = a.L[LZZ];
-    const float lz = L[p];
+    const float lz = fs(LZZ);
     PZ = K * K * lz;
     L[p] = K * K * lz;
     if (!ELASTIC) {
@@ -172,7 +167,7 @@ __global__ void k_adj_stress_cell(const AdjArgs a) {
   float GP[3];
   for (int q = 0; q < 3; ++q) {
     float* Ls = a.L[ls[q]];
-    const float l = Ls[p];
+    const float l = fs(ls[q]);
     Ls[p] = K * l;
     float lrv = 0.f;
     if (!ELASTIC) {
@@ -303,6 +298,14 @@ __global__ void k_adj_images_apply(const AdjArgs a) {
     a.L[LU][p + 2] = 0.f;
     a.L[LV][p + 2] = 0.f;
     a.L[LW][p + 2] = 0.f;
+    // the imaged stresses above the surface (fstr writes them each step;
+    // their transpose went to the cells below in k_adj_stress_cell)
+    a.L[LZZ][p + 1] = 0.f;
+    a.L[LZZ][p + 2] = 0.f;
+    a.L[LXZ][p + 1] = 0.f;
+    a.L[LXZ][p + 2] = 0.f;
+    a.L[LYZ][p + 1] = 0.f;
+    a.L[LYZ][p + 2] = 0.f;
   }
   // the temporaries at the top layer return to zero for the next step (cells
   // outside the stress range must read zero in the strain-rate gather)
@@ -377,13 +380,18 @@ __global__ void k_adj_vel_gather(const AdjArgs a) {
              eb[q - S + 1] + ec[q] + ec[q - S] + ec[q + Y] + ec[q - S + Y];
 }
 
+// One thread per distinct (component, cell); receivers sharing a cell are
+// added in receiver order (first[c] .. first[c+1] of order[]).
 __global__ void k_adj_inject(float* Lu, float* Lv, float* Lw, const long long* idx,
-                             const int* comp, const float* res, int n) {
-  if (blockIdx.x != 0 || threadIdx.x != 0) return;
-  for (int r = 0; r < n; ++r) {
-    float* L = comp[r] == 0 ? Lu : (comp[r] == 1 ? Lv : Lw);
-    L[idx[r]] += res[r];
-  }
+                             const int* comp, const int* first, const int* order, int ncell,
+                             const float* res) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncell) return;
+  const int r0 = order[first[c]];
+  float* L = comp[r0] == 0 ? Lu : (comp[r0] == 1 ? Lv : Lw);
+  float acc = L[idx[r0]];
+  for (int n = first[c]; n < first[c + 1]; ++n) acc += res[order[n]];
+  L[idx[r0]] = acc;
 }
 
 __global__ void k_sample(const float* u, const float* v, const float* w, const long long* idx,
@@ -463,10 +471,9 @@ inline unsigned cdiv(long long a, long long b) { return (unsigned)((a + b - 1) /
 }  // namespace
 
 cudaError_t awp_launch_adjoint_step(const AdjArgs& a, cudaStream_t st) {
-  const int fj = a.fj1 - a.sj0 + 1, si = a.si1 - a.si0 + 1, sj = a.sj1 - a.sj0 + 1,
-            sk = a.sk1 - a.sk0 + 1;
+  const int si = a.si1 - a.si0 + 1, sj = a.sj1 - a.sj0 + 1, sk = a.sk1 - a.sk0 + 1;
   const dim3 blk(32, 4);
-  k_adj_fstr<<<dim3(cdiv(fj, 128), si), 128, 0, st>>>(a);
+  // the imaging (fstr) transpose runs inside k_adj_stress_cell
   if (a.elastic)
     k_adj_stress_cell<true><<<dim3(cdiv(sk, 32), cdiv(sj, 4), si), blk, 0, st>>>(a);
   else
@@ -481,9 +488,11 @@ cudaError_t awp_launch_adjoint_step(const AdjArgs& a, cudaStream_t st) {
 }
 
 cudaError_t awp_launch_adjoint_inject(float* const L[3], const long long* idx, const int* comp,
-                                      const float* res, int nrec, cudaStream_t st) {
-  if (nrec <= 0) return cudaSuccess;
-  k_adj_inject<<<1, 1, 0, st>>>(L[0], L[1], L[2], idx, comp, res, nrec);
+                                      const int* first, const int* order, int ncell,
+                                      const float* res, cudaStream_t st) {
+  if (ncell <= 0) return cudaSuccess;
+  k_adj_inject<<<cdiv(ncell, 128), 128, 0, st>>>(L[0], L[1], L[2], idx, comp, first, order,
+                                                 ncell, res);
   return cudaGetLastError();
 }
 

@@ -38,9 +38,11 @@ struct AdjArgs {
 // accumulates the material gradients of that step.
 cudaError_t awp_launch_adjoint_step(const AdjArgs& a, cudaStream_t st);
 
-// Receiver terms: L[comp][idx[r]] += res[r] (one thread, receivers in order).
+// Receiver terms: L[comp][idx[r]] += res[r], one thread per distinct
+// (component, cell) c adding the receivers order[first[c] .. first[c+1]) in order.
 cudaError_t awp_launch_adjoint_inject(float* const L[3], const long long* idx, const int* comp,
-                                      const float* res, int nrec, cudaStream_t st);
+                                      const int* first, const int* order, int ncell,
+                                      const float* res, cudaStream_t st);
 // Seismogram samples of the current state: out[r] = field(comp[r])[idx[r]].
 cudaError_t awp_launch_sample(const float* u, const float* v, const float* w,
                               const long long* idx, const int* comp, int nrec, float* out,

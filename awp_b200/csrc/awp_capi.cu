@@ -96,6 +96,9 @@ struct awp_ctx {
   awp::TopoMetrics* topo = nullptr;  // host metrics (point-set set-up)
   float* d_topo = nullptr;           // f arrays then g arrays, one allocation
   TopoArgs targs{};                  // device pointers and constants
+  // adjoint workspace, kept between gradient calls of the same size
+  float* adj_slab = nullptr;
+  size_t adj_slab_fields = 0;
   long long dev_bytes = 0;
   long long launches = 0;
   // phase timing
@@ -620,6 +623,7 @@ int awp_ctx_destroy(awp_ctx* c) {
   awp_srcf_destroy(c->srcf);
   delete c->topo;
   cudaFree(c->d_topo);
+  cudaFree(c->adj_slab);
   for (int i = 0; i < AWP_NFIELDS; ++i) cudaFree(c->f[i]);
   cudaFree(c->dcrjx); cudaFree(c->dcrjy); cudaFree(c->dcrjz); cudaFree(c->lam_mu);
   cudaFree(c->d_cell_pos); cudaFree(c->d_cell_first); cudaFree(c->d_order);
@@ -1841,13 +1845,27 @@ int awp_misfit_gradient(awp_ctx* c, int nsteps, int nrec, const int* rec_xyz, co
   L = std::max(1, std::min(L, nsteps));
   const int nseg = (nsteps + L - 1) / L;
   const size_t fields = (size_t)(nseg + 1) * 15 + (size_t)(L + 1) * 3 + 15 + 17 + 3;
-  size_t freeb = 0, totb = 0;
-  CU_TRY(cudaMemGetInfo(&freeb, &totb));
-  if (fields * fb + (64u << 20) > freeb)
-    return set_error(AWP_ERR_NOMEM,
-                     "adjoint needs %.1f GB (%zu fields of %.1f MB: %d snapshots, %d-step "
-                     "segments), %.1f GB free",
-                     fields * fb / 1e9, fields, fb / 1e6, nseg + 1, L, freeb / 1e9);
+  // one slab for snapshots, segment store, adjoint state, temporaries and
+  // gradients, kept in the context for the next call
+  if (c->adj_slab_fields < fields) {
+    cudaFree(c->adj_slab);
+    c->adj_slab = nullptr;
+    c->adj_slab_fields = 0;
+    size_t freeb = 0, totb = 0;
+    CU_TRY(cudaMemGetInfo(&freeb, &totb));
+    if (fields * fb + (64u << 20) > freeb)
+      return set_error(AWP_ERR_NOMEM,
+                       "adjoint needs %.1f GB (%zu fields of %.1f MB: %d snapshots, %d-step "
+                       "segments), %.1f GB free",
+                       fields * fb / 1e9, fields, fb / 1e6, nseg + 1, L, freeb / 1e9);
+    if (cudaMalloc((void**)&c->adj_slab, fields * fb) != cudaSuccess) {
+      c->adj_slab = nullptr;
+      return set_error(AWP_ERR_NOMEM, "adjoint workspace of %.1f GB", fields * fb / 1e9);
+    }
+    c->adj_slab_fields = fields;
+  }
+  size_t slab_next = 0;
+  auto take = [&]() -> float* { return c->adj_slab + (slab_next++) * cp; };
   DevBuf b;
   long long* d_idx = nullptr;
   int* d_comp = nullptr;
@@ -1862,8 +1880,7 @@ int awp_misfit_gradient(awp_ctx* c, int nsteps, int nrec, const int* rec_xyz, co
 
   // ---- forward pass with snapshots X_{sL} and the final state ---------------------
   std::vector<float*> snap((size_t)(nseg + 1) * 15, nullptr);
-  for (auto& q : snap)
-    if (!(q = b.f(cp))) return set_error(AWP_ERR_NOMEM, "snapshots");
+  for (auto& q : snap) q = take();
   std::vector<long long> snap_step(nseg + 1);
   std::vector<char> snap_init(nseg + 1);
   auto save = [&](int s) -> int {
@@ -1904,21 +1921,17 @@ int awp_misfit_gradient(awp_ctx* c, int nsteps, int nrec, const int* rec_xyz, co
   // ---- adjoint state, temporaries, gradients (zeroed) --------------------------------
   AdjArgs a;
   memset(&a, 0, sizeof(a));
-  for (int q = 0; q < 15; ++q)
-    if (!(a.L[q] = b.f(cp))) return set_error(AWP_ERR_NOMEM, "adjoint fields");
-  for (int q = 0; q < 11; ++q)
-    if (!(a.E[q] = b.f(cp))) return set_error(AWP_ERR_NOMEM, "adjoint temporaries");
-  for (int q = 0; q < 6; ++q)
-    if (!(a.V[q] = b.f(cp))) return set_error(AWP_ERR_NOMEM, "adjoint temporaries");
-  if (!(a.gd = b.f(cp)) || !(a.glam = b.f(cp)) || !(a.gmu = b.f(cp)) ||
-      !(a.glm = b.f((size_t)c->g.nx_pad() * c->g.ny_pad())))
+  // adjoint state, temporaries, gradients: 35 consecutive fields of the slab
+  float* const zero0 = c->adj_slab + slab_next * cp;
+  for (int q = 0; q < 15; ++q) a.L[q] = take();
+  for (int q = 0; q < 11; ++q) a.E[q] = take();
+  for (int q = 0; q < 6; ++q) a.V[q] = take();
+  a.gd = take();
+  a.glam = take();
+  a.gmu = take();
+  CU_TRY(cudaMemsetAsync(zero0, 0, 35 * fb, st));
+  if (!(a.glm = b.f((size_t)c->g.nx_pad() * c->g.ny_pad())))
     return set_error(AWP_ERR_NOMEM, "gradients");
-  for (int q = 0; q < 15; ++q) CU_TRY(cudaMemsetAsync(a.L[q], 0, fb, st));
-  for (int q = 0; q < 11; ++q) CU_TRY(cudaMemsetAsync(a.E[q], 0, fb, st));
-  for (int q = 0; q < 6; ++q) CU_TRY(cudaMemsetAsync(a.V[q], 0, fb, st));
-  CU_TRY(cudaMemsetAsync(a.gd, 0, fb, st));
-  CU_TRY(cudaMemsetAsync(a.glam, 0, fb, st));
-  CU_TRY(cudaMemsetAsync(a.gmu, 0, fb, st));
   CU_TRY(cudaMemsetAsync(a.glm, 0, sizeof(float) * c->g.nx_pad() * c->g.ny_pad(), st));
   a.d1 = c->f[AWP_D1]; a.lam = c->f[AWP_LAM]; a.mu = c->f[AWP_MU];
   a.qp = c->f[AWP_QP]; a.qs = c->f[AWP_QS]; a.lam_mu = c->lam_mu;
@@ -1939,9 +1952,36 @@ int awp_misfit_gradient(awp_ctx* c, int nsteps, int nrec, const int* rec_xyz, co
   // segment store: the velocities at the start of a segment and after each
   // of its steps (slot 0 = start)
   std::vector<float*> seg((size_t)(L + 1) * 3, nullptr);
-  for (auto& q : seg)
-    if (!(q = b.f(cp))) return set_error(AWP_ERR_NOMEM, "segment store");
+  for (auto& q : seg) q = take();
   float* const Lvel[3] = {a.L[0], a.L[1], a.L[2]};
+  // receivers grouped by (component, cell) for the residual injection
+  int* d_first = nullptr;
+  int* d_order = nullptr;
+  int ncell_rec = 0;
+  {
+    std::vector<std::pair<long long, int>> key(nrec);
+    for (int r = 0; r < nrec; ++r) {
+      const int x = rec_xyz[3 * r], y = rec_xyz[3 * r + 1], z = rec_xyz[3 * r + 2];
+      key[r] = {((long long)rec_comp[r] << 48) | (((long long)x * c->g.nyt + y) * c->g.nzt + z), r};
+    }
+    std::stable_sort(key.begin(), key.end(),
+                     [](const std::pair<long long, int>& u, const std::pair<long long, int>& v) {
+                       return u.first < v.first;
+                     });
+    std::vector<int> first, order(nrec);
+    for (int r = 0; r < nrec; ++r) {
+      if (r == 0 || key[r].first != key[r - 1].first) first.push_back(r);
+      order[r] = key[r].second;
+    }
+    ncell_rec = (int)first.size();
+    first.push_back(nrec);
+    CU_TRY(cudaMalloc((void**)&d_first, sizeof(int) * first.size()));
+    b.p.push_back(d_first);
+    CU_TRY(cudaMalloc((void**)&d_order, sizeof(int) * order.size()));
+    b.p.push_back(d_order);
+    CU_TRY(cudaMemcpy(d_first, first.data(), sizeof(int) * first.size(), cudaMemcpyHostToDevice));
+    CU_TRY(cudaMemcpy(d_order, order.data(), sizeof(int) * order.size(), cudaMemcpyHostToDevice));
+  }
 
   // ---- backward sweep over the segments ----------------------------------------------
   for (int s = nseg - 1; s >= 0; --s) {
@@ -1957,7 +1997,8 @@ int awp_misfit_gradient(awp_ctx* c, int nsteps, int nrec, const int* rec_xyz, co
     }
     for (int n = n1 - 1; n >= n0; --n) {
       // the misfit term of the state after step n (its sample index is n)
-      CU_TRY(awp_launch_adjoint_inject(Lvel, d_idx, d_comp, d_res + (size_t)n * nrec, nrec, st));
+      CU_TRY(awp_launch_adjoint_inject(Lvel, d_idx, d_comp, d_first, d_order, ncell_rec,
+                                       d_res + (size_t)n * nrec, st));
       float** before = &seg[(size_t)(n - n0) * 3];
       float** after = &seg[(size_t)(n - n0 + 1) * 3];
       a.bu = before[0]; a.bv = before[1]; a.bw = before[2];
