@@ -1841,12 +1841,42 @@ int awp_misfit_gradient(awp_ctx* c, int nsteps, int nrec, const int* rec_xyz, co
   const size_t cp = (size_t)c->g.cells_pad();
   const size_t fb = cp * sizeof(float);
   // snapshot spacing: sqrt(N) unless given
-  int L = nsnap > 0 ? (nsteps + nsnap - 1) / nsnap : (int)ceil(sqrt((double)nsteps));
-  L = std::max(1, std::min(L, nsteps));
-  const int nseg = (nsteps + L - 1) / L;
-  const size_t fields = (size_t)(nseg + 1) * 15 + (size_t)(L + 1) * 3 + 15 + 17 + 3;
-  // one slab for snapshots, segment store, adjoint state, temporaries and
-  // gradients, kept in the context for the next call
+  // Two-level storage.  The last M steps keep their velocities from the first
+  // forward pass (no recomputation); the first H = N - M steps are covered by
+  // snapshots every L = ceil(sqrt(H)) steps and run forward again, one segment
+  // at a time, before their backward sweep.  nsnap > 0 fixes the snapshot
+  // count and stores no tail; nsnap = 0 takes the largest M that fits in 90 %
+  // of the free device memory (counting the workspace already held).
+  auto plan = [&](int M, int* Lp, int* nsegp) -> size_t {
+    const int H = nsteps - M;
+    int Lh = H > 0 ? (nsnap > 0 ? (H + nsnap - 1) / nsnap : (int)ceil(sqrt((double)H))) : 1;
+    Lh = std::max(1, std::min(Lh, std::max(H, 1)));
+    *Lp = Lh;
+    *nsegp = H > 0 ? (H + Lh - 1) / Lh : 0;
+    return (size_t)(*nsegp + 1) * 15 + (size_t)(H > 0 ? Lh + 1 : 0) * 3 +
+           (size_t)(M > 0 ? M + 1 : 0) * 3 + 15 + 17 + 3;
+  };
+  int M = 0, L = 1, nseg = 0;
+  size_t fields = plan(0, &L, &nseg);
+  if (nsnap <= 0) {
+    size_t freeb = 0, totb = 0;
+    CU_TRY(cudaMemGetInfo(&freeb, &totb));
+    const double budget = 0.9 * (double)(freeb + c->adj_slab_fields * fb) - (256u << 20);
+    int lo = 0, hi = nsteps;  // largest M whose plan fits the budget
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) / 2;
+      int Lm, nm;
+      if ((double)plan(mid, &Lm, &nm) * fb <= budget)
+        lo = mid;
+      else
+        hi = mid - 1;
+    }
+    M = lo;
+    fields = plan(M, &L, &nseg);
+  }
+  const int H = nsteps - M;
+  // one slab for snapshots, stores, adjoint state, temporaries and gradients,
+  // kept in the context for the next call
   if (c->adj_slab_fields < fields) {
     cudaFree(c->adj_slab);
     c->adj_slab = nullptr;
@@ -1897,9 +1927,19 @@ int awp_misfit_gradient(awp_ctx* c, int nsteps, int nrec, const int* rec_xyz, co
     c->initial_src_done = snap_init[s] != 0;
     return AWP_OK;
   };
+  // tail store: the velocities at step H and after each later step
+  std::vector<float*> tail((size_t)(M > 0 ? M + 1 : 0) * 3, nullptr);
+  for (auto& q : tail) q = take();
+  auto keep_vel = [&](float** dst) -> int {
+    for (int q = 0; q < 3; ++q)
+      CU_TRY(cudaMemcpyAsync(dst[q], c->f[AWP_U1 + q], fb, cudaMemcpyDeviceToDevice, st));
+    return AWP_OK;
+  };
   for (int n = 0; n < nsteps; ++n) {
-    if (n % L == 0 && (e = save(n / L))) return e;
+    if (n < H && n % L == 0 && (e = save(n / L))) return e;
+    if (n == H && M > 0 && (e = keep_vel(&tail[0]))) return e;
     if ((e = one_step(c))) return e;
+    if (n >= H && (e = keep_vel(&tail[(size_t)(n - H + 1) * 3]))) return e;
     CU_TRY(awp_launch_sample(c->f[AWP_U1], c->f[AWP_V1], c->f[AWP_W1], d_idx, d_comp, nrec,
                              d_seis + (size_t)n * nrec, st));
   }
@@ -1951,7 +1991,7 @@ int awp_misfit_gradient(awp_ctx* c, int nsteps, int nrec, const int* rec_xyz, co
   }
   // segment store: the velocities at the start of a segment and after each
   // of its steps (slot 0 = start)
-  std::vector<float*> seg((size_t)(L + 1) * 3, nullptr);
+  std::vector<float*> seg((size_t)(H > 0 ? L + 1 : 0) * 3, nullptr);
   for (auto& q : seg) q = take();
   float* const Lvel[3] = {a.L[0], a.L[1], a.L[2]};
   // receivers grouped by (component, cell) for the residual injection
@@ -1983,9 +2023,20 @@ int awp_misfit_gradient(awp_ctx* c, int nsteps, int nrec, const int* rec_xyz, co
     CU_TRY(cudaMemcpy(d_order, order.data(), sizeof(int) * order.size(), cudaMemcpyHostToDevice));
   }
 
-  // ---- backward sweep over the segments ----------------------------------------------
+  // ---- backward sweep: the stored tail, then the recomputed segments ---------------
+  auto back_step = [&](int n, float** before, float** after) -> int {
+    // the misfit term of the state after step n (its sample index is n)
+    CU_TRY(awp_launch_adjoint_inject(Lvel, d_idx, d_comp, d_first, d_order, ncell_rec,
+                                     d_res + (size_t)n * nrec, st));
+    a.bu = before[0]; a.bv = before[1]; a.bw = before[2];
+    a.fu = after[0]; a.fv = after[1]; a.fw = after[2];
+    CU_TRY(awp_launch_adjoint_step(a, st));
+    return AWP_OK;
+  };
+  for (int n = nsteps - 1; n >= H; --n)
+    if ((e = back_step(n, &tail[(size_t)(n - H) * 3], &tail[(size_t)(n - H + 1) * 3]))) return e;
   for (int s = nseg - 1; s >= 0; --s) {
-    const int n0 = s * L, n1 = std::min(nsteps, n0 + L);
+    const int n0 = s * L, n1 = std::min(H, n0 + L);
     if ((e = restore(s))) return e;
     for (int q = 0; q < 3; ++q)
       CU_TRY(cudaMemcpyAsync(seg[q], c->f[AWP_U1 + q], fb, cudaMemcpyDeviceToDevice, st));
@@ -1995,16 +2046,9 @@ int awp_misfit_gradient(awp_ctx* c, int nsteps, int nrec, const int* rec_xyz, co
       for (int q = 0; q < 3; ++q)
         CU_TRY(cudaMemcpyAsync(slot[q], c->f[AWP_U1 + q], fb, cudaMemcpyDeviceToDevice, st));
     }
-    for (int n = n1 - 1; n >= n0; --n) {
-      // the misfit term of the state after step n (its sample index is n)
-      CU_TRY(awp_launch_adjoint_inject(Lvel, d_idx, d_comp, d_first, d_order, ncell_rec,
-                                       d_res + (size_t)n * nrec, st));
-      float** before = &seg[(size_t)(n - n0) * 3];
-      float** after = &seg[(size_t)(n - n0 + 1) * 3];
-      a.bu = before[0]; a.bv = before[1]; a.bw = before[2];
-      a.fu = after[0]; a.fv = after[1]; a.fw = after[2];
-      CU_TRY(awp_launch_adjoint_step(a, st));
-    }
+    for (int n = n1 - 1; n >= n0; --n)
+      if ((e = back_step(n, &seg[(size_t)(n - n0) * 3], &seg[(size_t)(n - n0 + 1) * 3])))
+        return e;
   }
 
   // ---- gradients to the host; the context ends on the final forward state -----------

@@ -253,12 +253,16 @@ int awp_seismograms(awp_ctx* ctx, int nsteps, int nrec, const int* rec_xyz, cons
  * and its gradient with respect to lambda, mu, rho of every interior cell
  * (host arrays [nz][ny][nx], surface first; Q held fixed), by the discrete
  * adjoint of the time step: hand-written transposes of the velocity, stress,
- * memory-variable, free-surface-image and imaging updates.  The forward
- * states are kept as nsnap snapshots in device memory (0: ceil(sqrt(nsteps)))
- * and each segment between snapshots is run forward again before its
- * backward sweep.  The context ends on the state after nsteps steps.  seis
- * (optional) receives the samples.  AWP_ERR_NOMEM when the snapshots do not
- * fit, with the size in awp_last_error. */
+ * memory-variable, free-surface-image and imaging updates.  Forward states:
+ * with nsnap > 0, nsnap full-state snapshots in device memory, each segment
+ * between them run forward again before its backward sweep (revolve-style,
+ * about sqrt(nsteps) snapshots); with nsnap = 0, the velocities of as many of
+ * the last steps as fit in 90 % of the free device memory are kept from the
+ * first forward pass and only the earlier steps are snapshotted (every
+ * ceil(sqrt) steps) and recomputed.  The workspace stays allocated in the
+ * context for the next call.  The context ends on the state after nsteps
+ * steps.  seis (optional) receives the samples.  AWP_ERR_NOMEM when the
+ * snapshots do not fit, with the size in awp_last_error. */
 int awp_misfit_gradient(awp_ctx* ctx, int nsteps, int nrec, const int* rec_xyz, const int* rec_comp,
                         const float* d_obs, int nsnap, double* misfit, float* seis,
                         float* g_lambda, float* g_mu, float* g_rho);

@@ -125,7 +125,7 @@ def test_checkpoint_count_does_not_change_the_gradient():
     steps = 24
     scn, s, m, xyz, comp, d_obs = setup_case(True, seed=21, steps=steps)
     out = []
-    for nsnap in (1, 5, 24):
+    for nsnap in (1, 5, 24, 0):  # 0: the velocities of as many last steps as fit are kept
         s.set_moduli(*m)
         s.reset()
         out.append(adjoint.misfit_gradient(s, steps, xyz, comp, d_obs, nsnap=nsnap))
