@@ -120,42 +120,27 @@ __global__ void k_adj_stress_cell(const AdjArgs a) {
     }
     return v;
   };
-  float* L = nullptr;
+  // every load of the adjoint state before the first store: the stores below
+  // go to other arrays (or other cells of the same array), and issuing the
+  // loads together keeps them from waiting on one another
+  const float lx = a.L[LXX][p], ly = a.L[LYY][p], lz = fs(LZZ);
+  const float ls[3] = {fs(LXY), fs(LXZ), fs(LYZ)};
+  float rv[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  if (!ELASTIC)
+    for (int q = 0; q < 6; ++q) rv[q] = a.L[LR1 + q][p];
   // normal components
   float PX, PY, PZ, QX = 0.f, QY = 0.f, QZ = 0.f;
-  {
-    L = a.L[LXX];
-    const float lx = L[p];
-    PX = K * lx;
-    L[p] = K * lx;
-    L = a.L[LYY];
-    const float ly = L[p];
-    PY = K * K * ly;
-    L[p] = K * K * ly;
-    L = a.L[LZZ];
-    const float lz = fs(LZZ);
-    PZ = K * K * lz;
-    L[p] = K * K * lz;
-    if (!ELASTIC) {
-      float* R1 = a.L[LR1];
-      float* R2 = a.L[LR2];
-      float* R3 = a.L[LR3];
-      const float r1 = R1[p], r2 = R2[p], r3 = R3[p];
-      QX = DT * (wwo - 1.0f) * K * lx + wwo * r1;
-      QY = DT * (wwo - 1.0f) * K * ly + wwo * r2;
-      QZ = DT * (wwo - 1.0f) * K * lz + wwo * r3;
-      R1[p] = (al + DT * ga) * K * lx + be * r1;
-      R2[p] = al * K * K * ly + DT * ga * K * ly + be * r2;
-      R3[p] = al * K * K * lz + DT * ga * K * lz + be * r3;
-    }
+  PX = K * lx;
+  PY = K * K * ly;
+  PZ = K * K * lz;
+  if (!ELASTIC) {
+    QX = DT * (wwo - 1.0f) * K * lx + wwo * rv[0];
+    QY = DT * (wwo - 1.0f) * K * ly + wwo * rv[1];
+    QZ = DT * (wwo - 1.0f) * K * lz + wwo * rv[2];
   }
   const float sP = PX + PY + PZ, sQ = QX + QY + QZ;
   const float A = xl + DT * qpa;
   const float s123 = vs1 + vs2 + vs3;
-  float* const* E = a.E;
-  E[E1][p] = A * sP - xm * (PY + PZ) + qpa * sQ - h * (QY + QZ);
-  E[E2][p] = A * sP - xm * (PX + PZ) + qpa * sQ - h * (QX + QZ);
-  E[E3][p] = A * sP - xm * (PX + PY) + qpa * sQ - h * (QX + QY);
   const float G_xl = s123 * sP;
   const float G_qpa = DT * s123 * sP + s123 * sQ;
   const float G_xm = -((vs2 + vs3) * PX + (vs1 + vs3) * PY + (vs1 + vs2) * PZ);
@@ -163,24 +148,34 @@ __global__ void k_adj_stress_cell(const AdjArgs a) {
 
   // shear components
   const float es[3] = {e4, e5, e6};
-  const int ls[3] = {LXY, LXZ, LYZ}, lr[3] = {LR4, LR5, LR6};
-  float GP[3];
+  float GP[3], ES[3];
   for (int q = 0; q < 3; ++q) {
-    float* Ls = a.L[ls[q]];
-    const float l = fs(ls[q]);
-    Ls[p] = K * l;
-    float lrv = 0.f;
-    if (!ELASTIC) {
-      float* Rq = a.L[lr[q]];
-      lrv = Rq[p];
-      Rq[p] = (al + DT * ga) * K * l + be * lrv;
-    }
-    E[E4 + q][p] = (xmu[q] + DT * hh[q] * (wwo - 1.0f)) * K * l + wwo * hh[q] * lrv;
+    const float l = ls[q], lrv = rv[3 + q];
+    ES[q] = (xmu[q] + DT * hh[q] * (wwo - 1.0f)) * K * l + wwo * hh[q] * lrv;
     const float G_xmu = es[q] * K * l;
     const float G_hq = es[q] * (DT * (wwo - 1.0f) * K * l + wwo * lrv);
     const float Pq = q == 0 ? P1 : (q == 1 ? P2 : P3);
     GP[q] = -2.0f / (Pq * Pq) * (G_xmu * c_m[q] + G_hq * c_hh[q]);
   }
+
+  // stores: the adjoint state in place, then the temporaries
+  a.L[LXX][p] = K * lx;
+  a.L[LYY][p] = K * K * ly;
+  a.L[LZZ][p] = K * K * lz;
+  a.L[LXY][p] = K * ls[0];
+  a.L[LXZ][p] = K * ls[1];
+  a.L[LYZ][p] = K * ls[2];
+  if (!ELASTIC) {
+    a.L[LR1][p] = (al + DT * ga) * K * lx + be * rv[0];
+    a.L[LR2][p] = al * K * K * ly + DT * ga * K * ly + be * rv[1];
+    a.L[LR3][p] = al * K * K * lz + DT * ga * K * lz + be * rv[2];
+    for (int q = 0; q < 3; ++q) a.L[LR4 + q][p] = (al + DT * ga) * K * ls[q] + be * rv[3 + q];
+  }
+  float* const* E = a.E;
+  E[E1][p] = A * sP - xm * (PY + PZ) + qpa * sQ - h * (QY + QZ);
+  E[E2][p] = A * sP - xm * (PX + PZ) + qpa * sQ - h * (QX + QZ);
+  E[E3][p] = A * sP - xm * (PX + PY) + qpa * sQ - h * (QX + QY);
+  for (int q = 0; q < 3; ++q) E[E4 + q][p] = ES[q];
   // chain to the eight-cell sums
   const float G_xlraw = G_xl * a.dth + G_qpa * c_q;
   const float G_xmraw = G_xm * c_xm + G_h * c_h + G_xlraw;
@@ -210,24 +205,33 @@ __global__ void k_adj_stress_gather(const AdjArgs a) {
   const float* e4 = a.E[E4];
   const float* e5 = a.E[E5];
   const float* e6 = a.E[E6];
-  a.L[LU][q] += c1 * (e1[q - S] - e1[q]) + c2 * (e1[q - 2 * S] - e1[q + S]) +
-                c1 * (e4[q - Y] - e4[q]) + c2 * (e4[q - 2 * Y] - e4[q + Y]) +
-                c1 * (e5[q - 1] - e5[q]) + c2 * (e5[q - 2] - e5[q + 1]);
-  a.L[LV][q] += c1 * (e2[q] - e2[q + Y]) + c2 * (e2[q - Y] - e2[q + 2 * Y]) +
-                c1 * (e4[q] - e4[q + S]) + c2 * (e4[q - S] - e4[q + 2 * S]) +
-                c1 * (e6[q - 1] - e6[q]) + c2 * (e6[q - 2] - e6[q + 1]);
-  a.L[LW][q] += c1 * (e3[q] - e3[q + 1]) + c2 * (e3[q - 1] - e3[q + 2]) +
-                c1 * (e5[q] - e5[q + S]) + c2 * (e5[q - S] - e5[q + 2 * S]) +
-                c1 * (e6[q - Y] - e6[q]) + c2 * (e6[q - 2 * Y] - e6[q + Y]);
+  // the sums first, then the read-modify-writes, so that no load waits
+  // behind a store
+  const float du = c1 * (e1[q - S] - e1[q]) + c2 * (e1[q - 2 * S] - e1[q + S]) +
+                   c1 * (e4[q - Y] - e4[q]) + c2 * (e4[q - 2 * Y] - e4[q + Y]) +
+                   c1 * (e5[q - 1] - e5[q]) + c2 * (e5[q - 2] - e5[q + 1]);
+  const float dv = c1 * (e2[q] - e2[q + Y]) + c2 * (e2[q - Y] - e2[q + 2 * Y]) +
+                   c1 * (e4[q] - e4[q + S]) + c2 * (e4[q - S] - e4[q + 2 * S]) +
+                   c1 * (e6[q - 1] - e6[q]) + c2 * (e6[q - 2] - e6[q + 1]);
+  const float dw = c1 * (e3[q] - e3[q + 1]) + c2 * (e3[q - 1] - e3[q + 2]) +
+                   c1 * (e5[q] - e5[q + S]) + c2 * (e5[q - S] - e5[q + 2 * S]) +
+                   c1 * (e6[q - Y] - e6[q]) + c2 * (e6[q - 2 * Y] - e6[q + Y]);
   // box8(p) = {p, p+S, p-Y, p+S-Y, p-1, p+S-1, p-Y-1, p+S-Y-1} contains q for
   // p in {q, q-S, q+Y, q-S+Y, q+1, q-S+1, q+Y+1, q-S+Y+1}
   auto box = [&](const float* x) {
     return x[q] + x[q - S] + x[q + Y] + x[q - S + Y] + x[q + 1] + x[q - S + 1] + x[q + Y + 1] +
            x[q - S + Y + 1];
   };
-  a.glam[q] += box(a.E[GL8]);
-  a.gmu[q] += box(a.E[GM8]) + a.E[GP1][q] + a.E[GP1][q + 1] + a.E[GP2][q] + a.E[GP2][q + Y] +
-              a.E[GP3][q] + a.E[GP3][q - S];
+  const float dl = box(a.E[GL8]);
+  const float dm = box(a.E[GM8]) + a.E[GP1][q] + a.E[GP1][q + 1] + a.E[GP2][q] + a.E[GP2][q + Y] +
+                   a.E[GP3][q] + a.E[GP3][q - S];
+  const float lu = a.L[LU][q], lv = a.L[LV][q], lw = a.L[LW][q];
+  const float gl = a.glam[q], gm = a.gmu[q];
+  a.L[LU][q] = lu + du;
+  a.L[LV][q] = lv + dv;
+  a.L[LW][q] = lw + dw;
+  a.glam[q] = gl + dl;
+  a.gmu[q] = gm + dm;
 }
 
 // ---------------------------------------------------------------------------
@@ -364,20 +368,31 @@ __global__ void k_adj_vel_gather(const AdjArgs a) {
   const float* A = a.V[VA];
   const float* B = a.V[VB];
   const float* C = a.V[VC];
-  a.L[LXX][q] += c1 * (A[q] - A[q + S]) + c2 * (A[q - S] - A[q + 2 * S]);
-  a.L[LXY][q] += c1 * (A[q] - A[q + Y]) + c2 * (A[q - Y] - A[q + 2 * Y]) +
-                 c1 * (B[q - S] - B[q]) + c2 * (B[q - 2 * S] - B[q + S]);
-  a.L[LXZ][q] += c1 * (A[q] - A[q + 1]) + c2 * (A[q - 1] - A[q + 2]) +
-                 c1 * (C[q - S] - C[q]) + c2 * (C[q - 2 * S] - C[q + S]);
-  a.L[LYY][q] += c1 * (B[q - Y] - B[q]) + c2 * (B[q - 2 * Y] - B[q + Y]);
-  a.L[LYZ][q] += c1 * (B[q] - B[q + 1]) + c2 * (B[q - 1] - B[q + 2]) +
-                 c1 * (C[q] - C[q + Y]) + c2 * (C[q - Y] - C[q + 2 * Y]);
-  a.L[LZZ][q] += c1 * (C[q - 1] - C[q]) + c2 * (C[q - 2] - C[q + 1]);
+  // the sums first, then the read-modify-writes (no load behind a store)
+  const float dxx = c1 * (A[q] - A[q + S]) + c2 * (A[q - S] - A[q + 2 * S]);
+  const float dxy = c1 * (A[q] - A[q + Y]) + c2 * (A[q - Y] - A[q + 2 * Y]) +
+                    c1 * (B[q - S] - B[q]) + c2 * (B[q - 2 * S] - B[q + S]);
+  const float dxz = c1 * (A[q] - A[q + 1]) + c2 * (A[q - 1] - A[q + 2]) +
+                    c1 * (C[q - S] - C[q]) + c2 * (C[q - 2 * S] - C[q + S]);
+  const float dyy = c1 * (B[q - Y] - B[q]) + c2 * (B[q - 2 * Y] - B[q + Y]);
+  const float dyz = c1 * (B[q] - B[q + 1]) + c2 * (B[q - 1] - B[q + 2]) +
+                    c1 * (C[q] - C[q + Y]) + c2 * (C[q - Y] - C[q + 2 * Y]);
+  const float dzz = c1 * (C[q - 1] - C[q]) + c2 * (C[q - 2] - C[q + 1]);
   const float* ea = a.V[VEA];
   const float* eb = a.V[VEB];
   const float* ec = a.V[VEC];
-  a.gd[q] += ea[q] + ea[q + Y] + ea[q + 1] + ea[q + Y + 1] + eb[q] + eb[q - S] + eb[q + 1] +
-             eb[q - S + 1] + ec[q] + ec[q - S] + ec[q + Y] + ec[q - S + Y];
+  const float dd = ea[q] + ea[q + Y] + ea[q + 1] + ea[q + Y + 1] + eb[q] + eb[q - S] + eb[q + 1] +
+                   eb[q - S + 1] + ec[q] + ec[q - S] + ec[q + Y] + ec[q - S + Y];
+  const float lxx = a.L[LXX][q], lxy = a.L[LXY][q], lxz = a.L[LXZ][q];
+  const float lyy = a.L[LYY][q], lyz = a.L[LYZ][q], lzz = a.L[LZZ][q];
+  const float gd = a.gd[q];
+  a.L[LXX][q] = lxx + dxx;
+  a.L[LXY][q] = lxy + dxy;
+  a.L[LXZ][q] = lxz + dxz;
+  a.L[LYY][q] = lyy + dyy;
+  a.L[LYZ][q] = lyz + dyz;
+  a.L[LZZ][q] = lzz + dzz;
+  a.gd[q] = gd + dd;
 }
 
 // One thread per distinct (component, cell); receivers sharing a cell are
