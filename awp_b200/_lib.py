@@ -132,6 +132,8 @@ def load() -> ctypes.CDLL:
     _sig(lib, "awp_seismograms", c_int, [_P, c_int, c_int, _I, _I, _F])
     _sig(lib, "awp_misfit_gradient", c_int,
          [_P, c_int, c_int, _I, _I, _F, c_int, POINTER(c_double), _F, _F, _F, _F])
+    _sig(lib, "awp_adjoint_plan", c_int,
+         [_P, c_int, c_int, _I, _I, _I, POINTER(c_double)])
     _sig(lib, "awp_input_read", c_int,
          [c_char_p, POINTER(c_longlong), c_char_p, c_int, _F, _F, _F, _I, c_longlong])
     _sig(lib, "awp_point_coefs", c_int,

@@ -60,6 +60,17 @@ def misfit_gradient(solver, nsteps: int, rec_xyz, rec_comp, d_obs, nsnap: int = 
     return J.value, seis, g[0], g[1], g[2]
 
 
+def adjoint_plan(solver, nsteps: int, nsnap: int = 0) -> dict:
+    """The forward-state storage ``misfit_gradient`` would use now: steps whose
+    velocities are kept, the recomputed segment length, the snapshot count and
+    the workspace in GB."""
+    m, l, n, gb = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), c_double()
+    check(solver.lib.awp_adjoint_plan(solver.ctx, int(nsteps), int(nsnap), byref(m), byref(l),
+                                      byref(n), byref(gb)), "awp_adjoint_plan")
+    return {"tail_steps": m.value, "segment_steps": l.value, "snapshots": n.value,
+            "workspace_gb": gb.value}
+
+
 def _autograd_function():
     import torch
 

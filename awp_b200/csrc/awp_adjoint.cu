@@ -52,19 +52,21 @@ __global__ void k_adj_stress_cell(const AdjArgs a) {
   const long long p = (long long)i * S + (long long)j * Y + k;
   const float c1 = a.c1, c2 = a.c2, DT = a.dt;
 
-  // forward strain rates from the velocities after the step
+  // forward strain rates from the velocities after the step (VelBox layout)
   const float* u = a.fu;
   const float* v = a.fv;
   const float* w = a.fw;
-  const float vs1 = c1 * (u[p + S] - u[p]) + c2 * (u[p + 2 * S] - u[p - S]);
-  const float vs2 = c1 * (v[p] - v[p - Y]) + c2 * (v[p + Y] - v[p - 2 * Y]);
-  const float vs3 = c1 * (w[p] - w[p - 1]) + c2 * (w[p + 1] - w[p - 2]);
-  const float e4 = c1 * (u[p + Y] - u[p]) + c2 * (u[p + 2 * Y] - u[p - Y]) +
-                   c1 * (v[p] - v[p - S]) + c2 * (v[p + S] - v[p - 2 * S]);
-  const float e5 = c1 * (u[p + 1] - u[p]) + c2 * (u[p + 2] - u[p - 1]) +
-                   c1 * (w[p] - w[p - S]) + c2 * (w[p + S] - w[p - 2 * S]);
-  const float e6 = c1 * (v[p + 1] - v[p]) + c2 * (v[p + 2] - v[p - 1]) +
-                   c1 * (w[p + Y] - w[p]) + c2 * (w[p + 2 * Y] - w[p - Y]);
+  const long long VS = a.vb.S, VY = a.vb.Y;
+  const long long pv = (long long)i * VS + (long long)j * VY + k - a.vb.off;
+  const float vs1 = c1 * (u[pv + VS] - u[pv]) + c2 * (u[pv + 2 * VS] - u[pv - VS]);
+  const float vs2 = c1 * (v[pv] - v[pv - VY]) + c2 * (v[pv + VY] - v[pv - 2 * VY]);
+  const float vs3 = c1 * (w[pv] - w[pv - 1]) + c2 * (w[pv + 1] - w[pv - 2]);
+  const float e4 = c1 * (u[pv + VY] - u[pv]) + c2 * (u[pv + 2 * VY] - u[pv - VY]) +
+                   c1 * (v[pv] - v[pv - VS]) + c2 * (v[pv + VS] - v[pv - 2 * VS]);
+  const float e5 = c1 * (u[pv + 1] - u[pv]) + c2 * (u[pv + 2] - u[pv - 1]) +
+                   c1 * (w[pv] - w[pv - VS]) + c2 * (w[pv + VS] - w[pv - 2 * VS]);
+  const float e6 = c1 * (v[pv + 1] - v[pv]) + c2 * (v[pv + 2] - v[pv - 1]) +
+                   c1 * (w[pv + VY] - w[pv]) + c2 * (w[pv + 2 * VY] - w[pv - VY]);
 
   // materials of the cell (kernel.cu:962-1070)
   auto sum8 = [&](const float* m) {
@@ -272,9 +274,11 @@ __global__ void k_adj_images(const AdjArgs a) {
     const float* u = a.fu;
     const float* v = a.fv;
     const float* w = a.fw;
-    const float Z = m1(i) * (u[p + S] - w[p + S] + w[p]) - (u[p] - w[p] + w[p - S]) +
-                    (u[p + S] - u[p]) + (v[p] - w[p + Y] + w[p]) -
-                    m2(j) * (v[p - Y] - w[p] + w[p - Y]) + (v[p] - v[p - Y]);
+    const long long VS = a.vb.S, VY = a.vb.Y;
+    const long long q = (long long)i * VS + (long long)j * VY + a.g.top() - a.vb.off;
+    const float Z = m1(i) * (u[q + VS] - w[q + VS] + w[q]) - (u[q] - w[q] + w[q - VS]) +
+                    (u[q + VS] - u[q]) + (v[q] - w[q + VY] + w[q]) -
+                    m2(j) * (v[q - VY] - w[q] + w[q - VY]) + (v[q] - v[q - VY]);
     a.glm[(long long)i * a.lam_mu_ld + j] += -Z * Aw(i, j);
   }
   // the image writes and reads of this column are all done by this thread
@@ -336,9 +340,10 @@ __global__ void k_adj_vel_cell(const AdjArgs a) {
   const float fd1 = a.dth / r1, fd2 = a.dth / r2, fd3 = a.dth / r3;
   const float dc = a.dcrjx[i] * a.dcrjy[j] * a.dcrjz[k];
   // fd * D(sigma) * dc of the forward update = u' - dc u
-  const float su = a.fu[p] - dc * a.bu[p];
-  const float sv = a.fv[p] - dc * a.bv[p];
-  const float sw = a.fw[p] - dc * a.bw[p];
+  const long long pv = (long long)i * a.vb.S + (long long)j * a.vb.Y + k - a.vb.off;
+  const float su = a.fu[pv] - dc * a.bu[pv];
+  const float sv = a.fv[pv] - dc * a.bv[pv];
+  const float sw = a.fw[pv] - dc * a.bw[pv];
   const float lu = a.L[LU][p], lv = a.L[LV][p], lw = a.L[LW][p];
   a.L[LU][p] = dc * lu;
   a.L[LV][p] = dc * lv;
@@ -481,9 +486,34 @@ __global__ void k_set_moduli(const float* lambda, const float* mu_, const float*
   d1[p] = rho[c];
 }
 
+// padded velocities -> VelBox rows; rows beyond nk (up to ld) are not read
+__global__ void k_pack_vel(const float* __restrict__ u, const float* __restrict__ v,
+                           const float* __restrict__ w, float* __restrict__ du,
+                           float* __restrict__ dv, float* __restrict__ dw, const VelBox b,
+                           long long S, long long Y) {
+  const int kk = blockIdx.x * 32 + threadIdx.x;
+  const int jj = blockIdx.y * 4 + threadIdx.y;
+  const int ii = blockIdx.z;
+  if (kk >= b.nk || jj >= b.nj) return;
+  const long long p = (long long)(b.i0 + ii) * S + (long long)(b.j0 + jj) * Y + b.k0 + kk;
+  const long long q = (long long)ii * b.S + (long long)jj * b.Y + kk;
+  du[q] = u[p];
+  dv[q] = v[p];
+  dw[q] = w[p];
+}
+
 inline unsigned cdiv(long long a, long long b) { return (unsigned)((a + b - 1) / b); }
 
 }  // namespace
+
+cudaError_t awp_launch_pack_vel(const float* u, const float* v, const float* w, float* du,
+                                float* dv, float* dw, const VelBox& b, const AwpGeom& g,
+                                cudaStream_t st) {
+  if (b.ni <= 0 || b.nj <= 0 || b.nk <= 0) return cudaSuccess;
+  k_pack_vel<<<dim3(cdiv(b.nk, 32), cdiv(b.nj, 4), b.ni), dim3(32, 4), 0, st>>>(
+      u, v, w, du, dv, dw, b, g.slice, g.yline);
+  return cudaGetLastError();
+}
 
 cudaError_t awp_launch_adjoint_step(const AdjArgs& a, cudaStream_t st) {
   const int si = a.si1 - a.si0 + 1, sj = a.sj1 - a.sj0 + 1, sk = a.sk1 - a.sk0 + 1;

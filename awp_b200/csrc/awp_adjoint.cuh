@@ -7,11 +7,21 @@
 
 #include "awp_common.h"
 
+// Layout of the stored forward velocities: the box of padded cells
+// [i0, i0+ni) x [j0, j0+nj) x [k0, k0+nk) that the adjoint kernels read, rows
+// of ld >= nk floats.  Padded cell (i, j, k) sits at i*S + j*Y + k - off.
+struct VelBox {
+  int i0, j0, k0, ni, nj, nk, ld;
+  long long S, Y, off;
+  size_t cells() const { return (size_t)ni * nj * ld; }
+};
+
 struct AdjArgs {
   // forward state: velocities before the step (velocity half) and after it
-  // (both halves; free-surface images included)
+  // (both halves; free-surface images included), in the VelBox layout vb
   const float *bu, *bv, *bw;
   const float *fu, *fv, *fw;
+  VelBox vb;
   // adjoint state, updated in place (u v w xx yy zz xy xz yz r1..r6)
   float* L[15];
   // temporaries (zero outside the ranges that write them)
@@ -37,6 +47,11 @@ struct AdjArgs {
 // One step backwards: imaging, stress (+ memory variables, images), velocity;
 // accumulates the material gradients of that step.
 cudaError_t awp_launch_adjoint_step(const AdjArgs& a, cudaStream_t st);
+
+// The forward velocities u, v, w (padded layout) into the VelBox layout.
+cudaError_t awp_launch_pack_vel(const float* u, const float* v, const float* w, float* du,
+                                float* dv, float* dw, const VelBox& b, const AwpGeom& g,
+                                cudaStream_t st);
 
 // Receiver terms: L[comp][idx[r]] += res[r], one thread per distinct
 // (component, cell) c adding the receivers order[first[c] .. first[c+1]) in order.

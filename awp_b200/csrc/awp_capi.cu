@@ -98,7 +98,7 @@ struct awp_ctx {
   TopoArgs targs{};                  // device pointers and constants
   // adjoint workspace, kept between gradient calls of the same size
   float* adj_slab = nullptr;
-  size_t adj_slab_fields = 0;
+  size_t adj_slab_floats = 0;
   long long dev_bytes = 0;
   long long launches = 0;
   // phase timing
@@ -1831,6 +1831,85 @@ int awp_seismograms(awp_ctx* c, int nsteps, int nrec, const int* rec_xyz, const 
   return AWP_OK;
 }
 
+// Forward-state storage of the misfit gradient (two levels).  The last M
+// steps keep their velocities from the first forward pass (no
+// recomputation); the first H = N - M steps are covered by snapshots every
+// L = ceil(sqrt(H)) steps and run forward again, one segment at a time,
+// before their backward sweep.  nsnap > 0 fixes the snapshot count and
+// stores no tail; nsnap = 0 takes the largest M that fits in 90 % of the free
+// device memory (counting the workspace already held).
+struct AdjPlan {
+  VelBox vb;
+  int M = 0, L = 1, nseg = 0;
+  size_t floats = 0;  // workspace, slab pieces on 256-byte boundaries
+};
+static inline size_t slab_round(size_t n) { return (n + 63) / 64 * 64; }
+
+static int adjoint_plan(awp_ctx* c, int nsteps, int nsnap, AdjPlan* out) {
+  const size_t cp = (size_t)c->g.cells_pad();
+  // the stored velocities cover what the adjoint kernels read of them
+  // (velocity range, stress range +-2)
+  const VelArgs va = make_vel_args(c);
+  const StrArgs sa = make_str_args(c);
+  VelBox& vb = out->vb;
+  {
+    const int i0 = std::min(va.i0, sa.i0 - 2), i1 = std::max(va.i1, sa.i1 + 2);
+    const int j0 = std::min(va.j0, sa.j0 - 2), j1 = std::max(va.j1, sa.j1 + 2);
+    const int k0 = std::min(va.k0, sa.k0 - 2) / 4 * 4, k1 = std::max(va.k1, sa.k1 + 2);
+    vb.i0 = i0; vb.j0 = j0; vb.k0 = k0;
+    vb.ni = i1 - i0 + 1; vb.nj = j1 - j0 + 1; vb.nk = k1 - k0 + 1;
+    vb.ld = (vb.nk + 7) / 8 * 8;
+    vb.Y = vb.ld;
+    vb.S = (long long)vb.nj * vb.ld;
+    vb.off = (long long)i0 * vb.S + (long long)j0 * vb.Y + k0;
+  }
+  const size_t cv = vb.cells();
+  auto plan = [&](int M, int* Lp, int* nsegp) -> size_t {  // floats
+    const int H = nsteps - M;
+    int Lh = H > 0 ? (nsnap > 0 ? (H + nsnap - 1) / nsnap : (int)ceil(sqrt((double)H))) : 1;
+    Lh = std::max(1, std::min(Lh, std::max(H, 1)));
+    *Lp = Lh;
+    *nsegp = H > 0 ? (H + Lh - 1) / Lh : 0;
+    return ((size_t)(*nsegp + 1) * 15 + 15 + 17 + 3) * slab_round(cp) +
+           ((size_t)(H > 0 ? Lh + 1 : 0) + (size_t)(M > 0 ? M + 1 : 0)) * 3 * slab_round(cv);
+  };
+  int M = 0;
+  out->floats = plan(0, &out->L, &out->nseg);
+  if (nsnap <= 0) {
+    size_t freeb = 0, totb = 0;
+    CU_TRY(cudaMemGetInfo(&freeb, &totb));
+    const double budget =
+        0.9 * (double)(freeb + c->adj_slab_floats * sizeof(float)) - (256u << 20);
+    int lo = 0, hi = nsteps;  // largest M whose plan fits the budget
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) / 2;
+      int Lm, nm;
+      if ((double)plan(mid, &Lm, &nm) * sizeof(float) <= budget)
+        lo = mid;
+      else
+        hi = mid - 1;
+    }
+    M = lo;
+    out->floats = plan(M, &out->L, &out->nseg);
+  }
+  out->M = M;
+  return AWP_OK;
+}
+
+int awp_adjoint_plan(awp_ctx* c, int nsteps, int nsnap, int* tail_steps, int* segment_steps,
+                     int* snapshots, double* workspace_gb) {
+  int e = check_adjoint_ctx(c);
+  if (e) return e;
+  if (nsteps < 1) return set_error(AWP_ERR_ARG, "nsteps < 1");
+  AdjPlan pl;
+  if ((e = adjoint_plan(c, nsteps, nsnap, &pl))) return e;
+  if (tail_steps) *tail_steps = pl.M;
+  if (segment_steps) *segment_steps = pl.L;
+  if (snapshots) *snapshots = pl.nseg + 1;
+  if (workspace_gb) *workspace_gb = pl.floats * sizeof(float) / 1e9;
+  return AWP_OK;
+}
+
 int awp_misfit_gradient(awp_ctx* c, int nsteps, int nrec, const int* rec_xyz, const int* rec_comp,
                         const float* d_obs, int nsnap, double* misfit, float* seis,
                         float* g_lambda, float* g_mu, float* g_rho) {
@@ -1840,62 +1919,44 @@ int awp_misfit_gradient(awp_ctx* c, int nsteps, int nrec, const int* rec_xyz, co
     return set_error(AWP_ERR_ARG, "bad arguments");
   const size_t cp = (size_t)c->g.cells_pad();
   const size_t fb = cp * sizeof(float);
-  // snapshot spacing: sqrt(N) unless given
-  // Two-level storage.  The last M steps keep their velocities from the first
-  // forward pass (no recomputation); the first H = N - M steps are covered by
-  // snapshots every L = ceil(sqrt(H)) steps and run forward again, one segment
-  // at a time, before their backward sweep.  nsnap > 0 fixes the snapshot
-  // count and stores no tail; nsnap = 0 takes the largest M that fits in 90 %
-  // of the free device memory (counting the workspace already held).
-  auto plan = [&](int M, int* Lp, int* nsegp) -> size_t {
-    const int H = nsteps - M;
-    int Lh = H > 0 ? (nsnap > 0 ? (H + nsnap - 1) / nsnap : (int)ceil(sqrt((double)H))) : 1;
-    Lh = std::max(1, std::min(Lh, std::max(H, 1)));
-    *Lp = Lh;
-    *nsegp = H > 0 ? (H + Lh - 1) / Lh : 0;
-    return (size_t)(*nsegp + 1) * 15 + (size_t)(H > 0 ? Lh + 1 : 0) * 3 +
-           (size_t)(M > 0 ? M + 1 : 0) * 3 + 15 + 17 + 3;
-  };
-  int M = 0, L = 1, nseg = 0;
-  size_t fields = plan(0, &L, &nseg);
-  if (nsnap <= 0) {
-    size_t freeb = 0, totb = 0;
-    CU_TRY(cudaMemGetInfo(&freeb, &totb));
-    const double budget = 0.9 * (double)(freeb + c->adj_slab_fields * fb) - (256u << 20);
-    int lo = 0, hi = nsteps;  // largest M whose plan fits the budget
-    while (lo < hi) {
-      const int mid = (lo + hi + 1) / 2;
-      int Lm, nm;
-      if ((double)plan(mid, &Lm, &nm) * fb <= budget)
-        lo = mid;
-      else
-        hi = mid - 1;
-    }
-    M = lo;
-    fields = plan(M, &L, &nseg);
-  }
+  AdjPlan pl;
+  if ((e = adjoint_plan(c, nsteps, nsnap, &pl))) return e;
+  const VelBox vb = pl.vb;
+  const size_t cv = vb.cells();
+  const int M = pl.M, L = pl.L, nseg = pl.nseg;
+  const size_t floats = pl.floats;
+  const VelArgs va = make_vel_args(c);
+  const StrArgs sa = make_str_args(c);
+  auto rnd = slab_round;
   const int H = nsteps - M;
   // one slab for snapshots, stores, adjoint state, temporaries and gradients,
   // kept in the context for the next call
-  if (c->adj_slab_fields < fields) {
+  if (c->adj_slab_floats < floats) {
     cudaFree(c->adj_slab);
     c->adj_slab = nullptr;
-    c->adj_slab_fields = 0;
+    c->adj_slab_floats = 0;
     size_t freeb = 0, totb = 0;
     CU_TRY(cudaMemGetInfo(&freeb, &totb));
-    if (fields * fb + (64u << 20) > freeb)
+    const double gb = floats * sizeof(float) / 1e9;
+    if (floats * sizeof(float) + (64u << 20) > freeb)
       return set_error(AWP_ERR_NOMEM,
-                       "adjoint needs %.1f GB (%zu fields of %.1f MB: %d snapshots, %d-step "
+                       "adjoint needs %.1f GB (%d snapshots of %.1f MB fields, %d-step "
                        "segments), %.1f GB free",
-                       fields * fb / 1e9, fields, fb / 1e6, nseg + 1, L, freeb / 1e9);
-    if (cudaMalloc((void**)&c->adj_slab, fields * fb) != cudaSuccess) {
+                       gb, nseg + 1, fb / 1e6, L, freeb / 1e9);
+    if (cudaMalloc((void**)&c->adj_slab, floats * sizeof(float)) != cudaSuccess) {
       c->adj_slab = nullptr;
-      return set_error(AWP_ERR_NOMEM, "adjoint workspace of %.1f GB", fields * fb / 1e9);
+      return set_error(AWP_ERR_NOMEM, "adjoint workspace of %.1f GB", gb);
     }
-    c->adj_slab_fields = fields;
+    c->adj_slab_floats = floats;
   }
-  size_t slab_next = 0;
-  auto take = [&]() -> float* { return c->adj_slab + (slab_next++) * cp; };
+  size_t slab_next = 0;  // floats
+  auto take_n = [&](size_t n) -> float* {
+    float* q = c->adj_slab + slab_next;
+    slab_next += rnd(n);
+    return q;
+  };
+  auto take = [&]() -> float* { return take_n(cp); };
+  auto take_v = [&]() -> float* { return take_n(cv); };
   DevBuf b;
   long long* d_idx = nullptr;
   int* d_comp = nullptr;
@@ -1929,10 +1990,10 @@ int awp_misfit_gradient(awp_ctx* c, int nsteps, int nrec, const int* rec_xyz, co
   };
   // tail store: the velocities at step H and after each later step
   std::vector<float*> tail((size_t)(M > 0 ? M + 1 : 0) * 3, nullptr);
-  for (auto& q : tail) q = take();
+  for (auto& q : tail) q = take_v();
   auto keep_vel = [&](float** dst) -> int {
-    for (int q = 0; q < 3; ++q)
-      CU_TRY(cudaMemcpyAsync(dst[q], c->f[AWP_U1 + q], fb, cudaMemcpyDeviceToDevice, st));
+    CU_TRY(awp_launch_pack_vel(c->f[AWP_U1], c->f[AWP_V1], c->f[AWP_W1], dst[0], dst[1], dst[2],
+                               vb, c->g, st));
     return AWP_OK;
   };
   for (int n = 0; n < nsteps; ++n) {
@@ -1962,14 +2023,14 @@ int awp_misfit_gradient(awp_ctx* c, int nsteps, int nrec, const int* rec_xyz, co
   AdjArgs a;
   memset(&a, 0, sizeof(a));
   // adjoint state, temporaries, gradients: 35 consecutive fields of the slab
-  float* const zero0 = c->adj_slab + slab_next * cp;
+  float* const zero0 = c->adj_slab + slab_next;
   for (int q = 0; q < 15; ++q) a.L[q] = take();
   for (int q = 0; q < 11; ++q) a.E[q] = take();
   for (int q = 0; q < 6; ++q) a.V[q] = take();
   a.gd = take();
   a.glam = take();
   a.gmu = take();
-  CU_TRY(cudaMemsetAsync(zero0, 0, 35 * fb, st));
+  CU_TRY(cudaMemsetAsync(zero0, 0, (size_t)(c->adj_slab + slab_next - zero0) * sizeof(float), st));
   if (!(a.glm = b.f((size_t)c->g.nx_pad() * c->g.ny_pad())))
     return set_error(AWP_ERR_NOMEM, "gradients");
   CU_TRY(cudaMemsetAsync(a.glm, 0, sizeof(float) * c->g.nx_pad() * c->g.ny_pad(), st));
@@ -1981,18 +2042,15 @@ int awp_misfit_gradient(awp_ctx* c, int nsteps, int nrec, const int* rec_xyz, co
   a.dth = c->dth; a.dh1 = c->dh1; a.dt = c->p.dt; a.c1 = c->c1; a.c2 = c->c2; a.qthr = c->qthr;
   a.elastic = c->elastic ? 1 : 0;
   a.g = c->g;
-  {
-    const VelArgs v = make_vel_args(c);
-    a.vi0 = v.i0; a.vi1 = v.i1; a.vj0 = v.j0; a.vj1 = v.j1; a.vk0 = v.k0; a.vk1 = v.k1;
-    const StrArgs sa = make_str_args(c);
-    a.si0 = sa.i0; a.si1 = sa.i1; a.sj0 = sa.j0; a.sj1 = sa.j1; a.sk0 = sa.k0; a.sk1 = sa.k1;
-    a.gx_lim = sa.gx_lim; a.gy_min = sa.gy_min; a.lam_mu_ld = sa.lam_mu_ld;
-    a.fj1 = make_fstr_args(c).j1;
-  }
+  a.vb = vb;
+  a.vi0 = va.i0; a.vi1 = va.i1; a.vj0 = va.j0; a.vj1 = va.j1; a.vk0 = va.k0; a.vk1 = va.k1;
+  a.si0 = sa.i0; a.si1 = sa.i1; a.sj0 = sa.j0; a.sj1 = sa.j1; a.sk0 = sa.k0; a.sk1 = sa.k1;
+  a.gx_lim = sa.gx_lim; a.gy_min = sa.gy_min; a.lam_mu_ld = sa.lam_mu_ld;
+  a.fj1 = make_fstr_args(c).j1;
   // segment store: the velocities at the start of a segment and after each
   // of its steps (slot 0 = start)
   std::vector<float*> seg((size_t)(H > 0 ? L + 1 : 0) * 3, nullptr);
-  for (auto& q : seg) q = take();
+  for (auto& q : seg) q = take_v();
   float* const Lvel[3] = {a.L[0], a.L[1], a.L[2]};
   // receivers grouped by (component, cell) for the residual injection
   int* d_first = nullptr;
@@ -2038,13 +2096,10 @@ int awp_misfit_gradient(awp_ctx* c, int nsteps, int nrec, const int* rec_xyz, co
   for (int s = nseg - 1; s >= 0; --s) {
     const int n0 = s * L, n1 = std::min(H, n0 + L);
     if ((e = restore(s))) return e;
-    for (int q = 0; q < 3; ++q)
-      CU_TRY(cudaMemcpyAsync(seg[q], c->f[AWP_U1 + q], fb, cudaMemcpyDeviceToDevice, st));
+    if ((e = keep_vel(&seg[0]))) return e;
     for (int n = n0; n < n1; ++n) {
       if ((e = one_step(c))) return e;
-      float** slot = &seg[(size_t)(n - n0 + 1) * 3];
-      for (int q = 0; q < 3; ++q)
-        CU_TRY(cudaMemcpyAsync(slot[q], c->f[AWP_U1 + q], fb, cudaMemcpyDeviceToDevice, st));
+      if ((e = keep_vel(&seg[(size_t)(n - n0 + 1) * 3]))) return e;
     }
     for (int n = n1 - 1; n >= n0; --n)
       if ((e = back_step(n, &seg[(size_t)(n - n0) * 3], &seg[(size_t)(n - n0 + 1) * 3])))

@@ -266,6 +266,13 @@ int awp_seismograms(awp_ctx* ctx, int nsteps, int nrec, const int* rec_xyz, cons
 int awp_misfit_gradient(awp_ctx* ctx, int nsteps, int nrec, const int* rec_xyz, const int* rec_comp,
                         const float* d_obs, int nsnap, double* misfit, float* seis,
                         float* g_lambda, float* g_mu, float* g_rho);
+/* The forward-state storage awp_misfit_gradient would use for nsteps steps
+ * and this nsnap, from the free device memory now: tail_steps steps keep
+ * their velocities, the others run again in segments of segment_steps steps
+ * from snapshots full states; workspace_gb is the slab it allocates.  Any
+ * output may be NULL. */
+int awp_adjoint_plan(awp_ctx* ctx, int nsteps, int nsnap, int* tail_steps, int* segment_steps,
+                     int* snapshots, double* workspace_gb);
 
 /* Host-only helper (no context, no GPU): the metric arrays of a topography
  * file (INTOPO) for an nx x ny x nz grid of spacing h, as topo_init_metrics /

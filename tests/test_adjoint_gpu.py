@@ -126,6 +126,13 @@ def test_checkpoint_count_does_not_change_the_gradient():
     scn, s, m, xyz, comp, d_obs = setup_case(True, seed=21, steps=steps)
     out = []
     for nsnap in (1, 5, 24, 0):  # 0: the velocities of as many last steps as fit are kept
+        plan = adjoint.adjoint_plan(s, steps, nsnap)
+        if nsnap > 0:  # snapshots at the segment starts plus the final state
+            assert plan["tail_steps"] == 0
+            assert plan["segment_steps"] == -(-steps // nsnap)
+            assert plan["snapshots"] == -(-steps // plan["segment_steps"]) + 1
+        else:  # a small grid: every step keeps its velocities
+            assert plan["tail_steps"] == steps and plan["snapshots"] == 1
         s.set_moduli(*m)
         s.reset()
         out.append(adjoint.misfit_gradient(s, steps, xyz, comp, d_obs, nsnap=nsnap))
