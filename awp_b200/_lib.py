@@ -132,6 +132,7 @@ def load() -> ctypes.CDLL:
     _sig(lib, "awp_seismograms", c_int, [_P, c_int, c_int, _I, _I, _F])
     _sig(lib, "awp_misfit_gradient", c_int,
          [_P, c_int, c_int, _I, _I, _F, c_int, POINTER(c_double), _F, _F, _F, _F])
+    _sig(lib, "awp_adjoint_reserve", c_int, [_P, c_int, c_int])
     _sig(lib, "awp_adjoint_plan", c_int,
          [_P, c_int, c_int, _I, _I, _I, POINTER(c_double)])
     _sig(lib, "awp_input_read", c_int,

@@ -71,6 +71,13 @@ def adjoint_plan(solver, nsteps: int, nsnap: int = 0) -> dict:
             "workspace_gb": gb.value}
 
 
+def adjoint_reserve(solver, nsteps: int, nsnap: int = 0) -> None:
+    """Allocate the workspace ``misfit_gradient`` needs for nsteps steps now
+    (it stays with the solver for later calls)."""
+    check(solver.lib.awp_adjoint_reserve(solver.ctx, int(nsteps), int(nsnap)),
+          "awp_adjoint_reserve")
+
+
 def _autograd_function():
     import torch
 

@@ -44,6 +44,20 @@ enum { VA, VB, VC, VEA, VEB, VEC };
 // ---------------------------------------------------------------------------
 template <bool ELASTIC>
 __global__ void k_adj_stress_cell(const AdjArgs a) {
+  // the relaxation tables in shared memory: the lanes of a warp alternate the
+  // table entry with the parity of k, which a constant-bank read would serve
+  // in two passes
+  __shared__ float tab[40];  // tau1[8], tau2[8], wwo8[8], coeff[16]
+  {
+    const int tid = threadIdx.y * 32 + threadIdx.x;
+    if (tid < 8) {
+      tab[tid] = a.tex.tau1[tid];
+      tab[8 + tid] = a.tex.tau2[tid];
+      tab[16 + tid] = a.tex.wwo8[tid];
+    }
+    if (!ELASTIC && tid < 16) tab[24 + tid] = a.coeff[tid];
+    __syncthreads();
+  }
   const int k = a.sk0 + blockIdx.x * 32 + threadIdx.x;
   const int j = a.sj0 + blockIdx.y * 4 + threadIdx.y;
   const int i = a.si0 + blockIdx.z;
@@ -79,10 +93,10 @@ __global__ void k_adj_stress_cell(const AdjArgs a) {
   const float xl_raw = 8.0f / L8 + xm_raw;
   const float m1_raw = 2.0f / P1, m2_raw = 2.0f / P2, m3_raw = 2.0f / P3;
   const int t = awp_tex_index(a.tex, i, j, k);
-  const float fvx1 = a.tex.tau1[t], fvx2 = a.tex.tau2[t], wwo = a.tex.wwo8[t];
+  const float fvx1 = tab[t], fvx2 = tab[8 + t], wwo = tab[16 + t];
   float c_xm = a.dth, c_h = 0.f, c_q = 0.f, c_m[3] = {a.dth, a.dth, a.dth}, c_hh[3] = {0, 0, 0};
   if (!ELASTIC) {
-    const float cc0 = a.coeff[2 * t], cc1 = a.coeff[2 * t + 1];
+    const float cc0 = tab[24 + 2 * t], cc1 = tab[25 + 2 * t];
     const float hw = awp_qf_weight(0.0625f * sum8(a.qs), wwo, cc0, cc1, a.qthr);
     const float qpaw = awp_qf_weight(0.0625f * sum8(a.qp), wwo, cc0, cc1, a.qthr);
     const float hiw[3] = {awp_qf_weight(0.25f * (a.qs[p] + a.qs[p - 1]), wwo, cc0, cc1, a.qthr),
@@ -104,7 +118,7 @@ __global__ void k_adj_stress_cell(const AdjArgs a) {
   const float be = fvx2, ga = fvx2 * (1.0f - fvx1);
 
   // fstr^T of this column's top three cells (the imaged values above the
-  // surface are cleared later, in k_adj_images_apply): zz(t) += -zz(t+1),
+  // surface are cleared later, in k_adj_vel_cell): zz(t) += -zz(t+1),
   // zz(t-1) += -zz(t+2), xz/yz(t-1) += -xz/yz(t+1), xz/yz(t-2) += -xz/yz(t+2),
   // xz/yz(t) after the imaging is zero
   const int top = a.g.top();
@@ -241,6 +255,14 @@ __global__ void k_adj_stress_gather(const AdjArgs a) {
 // goes to the velocities they were made from, and to lam_mu; the images are
 // overwritten each step, so their adjoint is cleared
 // ---------------------------------------------------------------------------
+// image-adjoint scratch: column (i, j) of the ring-extended surface window
+__device__ __forceinline__ long long img_plane(const AdjArgs& a) {
+  return (long long)(a.si1 - a.si0 + 3) * (a.sj1 - a.sj0 + 3);
+}
+__device__ __forceinline__ long long img_index(const AdjArgs& a, int i, int j) {
+  return (long long)(i - a.si0 + 1) * (a.sj1 - a.sj0 + 3) + (j - a.sj0 + 1);
+}
+
 __global__ void k_adj_images(const AdjArgs a) {
   // targets: the imaged columns and the one-column ring the images also read
   const int j = a.sj0 - 1 + blockIdx.x * blockDim.x + threadIdx.x;
@@ -281,47 +303,15 @@ __global__ void k_adj_images(const AdjArgs a) {
                     m2(j) * (v[q - VY] - w[q] + w[q - VY]) + (v[q] - v[q - VY]);
     a.glm[(long long)i * a.lam_mu_ld + j] += -Z * Aw(i, j);
   }
-  // the image writes and reads of this column are all done by this thread
-  // for (i, j); neighbours only read the image adjoints, so defer the updates
-  // to the second kernel below
-  a.E[E1][p] = du;
-  a.E[E2][p] = dv;
-  a.E[E3][p] = dw;
-  a.E[E4][p] = Aw(i, j);  // to w(top-1)
+  // neighbouring columns read this column's image adjoints, so the updates
+  // wait for the next kernel (k_adj_vel_cell)
+  const long long ip = img_index(a, i, j), np = img_plane(a);
+  a.img[ip] = du;
+  a.img[ip + np] = dv;
+  a.img[ip + 2 * np] = dw;
+  a.img[ip + 3 * np] = Aw(i, j);  // to w(top-1)
 }
 
-__global__ void k_adj_images_apply(const AdjArgs a) {
-  const int j = a.sj0 - 1 + blockIdx.x * blockDim.x + threadIdx.x;
-  const int i = a.si0 - 1 + blockIdx.y;
-  if (j > a.sj1 + 1 || i > a.si1 + 1) return;
-  const long long p = (long long)i * a.g.slice + (long long)j * a.g.yline + a.g.top();
-  a.L[LU][p] += a.E[E1][p];
-  a.L[LV][p] += a.E[E2][p];
-  a.L[LW][p] += a.E[E3][p];
-  if (i >= a.si0 && i <= a.si1 && j >= a.sj0 && j <= a.sj1) {
-    a.L[LW][p - 1] += a.E[E4][p];
-    a.L[LU][p + 1] = 0.f;
-    a.L[LV][p + 1] = 0.f;
-    a.L[LW][p + 1] = 0.f;
-    a.L[LU][p + 2] = 0.f;
-    a.L[LV][p + 2] = 0.f;
-    a.L[LW][p + 2] = 0.f;
-    // the imaged stresses above the surface (fstr writes them each step;
-    // their transpose went to the cells below in k_adj_stress_cell)
-    a.L[LZZ][p + 1] = 0.f;
-    a.L[LZZ][p + 2] = 0.f;
-    a.L[LXZ][p + 1] = 0.f;
-    a.L[LXZ][p + 2] = 0.f;
-    a.L[LYZ][p + 1] = 0.f;
-    a.L[LYZ][p + 2] = 0.f;
-  }
-  // the temporaries at the top layer return to zero for the next step (cells
-  // outside the stress range must read zero in the strain-rate gather)
-  a.E[E1][p] = 0.f;
-  a.E[E2][p] = 0.f;
-  a.E[E3][p] = 0.f;
-  a.E[E4][p] = 0.f;
-}
 
 // ---------------------------------------------------------------------------
 // velocity^T, pointwise part
@@ -344,7 +334,38 @@ __global__ void k_adj_vel_cell(const AdjArgs a) {
   const float su = a.fu[pv] - dc * a.bu[pv];
   const float sv = a.fv[pv] - dc * a.bv[pv];
   const float sw = a.fw[pv] - dc * a.bw[pv];
-  const float lu = a.L[LU][p], lv = a.L[LV][p], lw = a.L[LW][p];
+  float lu = a.L[LU][p], lv = a.L[LV][p], lw = a.L[LW][p];
+  // the image adjoints of the surface columns (k_adj_images) enter here:
+  // u, v, w(top) of the window and its ring, w(top-1) of the window; the
+  // imaged velocities and stresses above the surface return to zero (fstr
+  // and the images rewrite them every step; their transposes went below)
+  const int top = a.g.top();
+  if (k >= top - 1 && k <= top + 2) {
+    const bool ring = i >= a.si0 - 1 && i <= a.si1 + 1 && j >= a.sj0 - 1 && j <= a.sj1 + 1;
+    const bool in = i >= a.si0 && i <= a.si1 && j >= a.sj0 && j <= a.sj1;
+    if (k == top && ring) {
+      const long long ip = img_index(a, i, j), np = img_plane(a);
+      lu += a.img[ip];
+      lv += a.img[ip + np];
+      lw += a.img[ip + 2 * np];
+    } else if (k == top - 1 && in) {
+      lw += a.img[img_index(a, i, j) + 3 * img_plane(a)];
+    } else if (k > top && in) {
+      lu = lv = lw = 0.f;
+    }
+    if (k == top && in) {
+      for (int d = 1; d <= 2; ++d) {
+        if (top + d > a.vk1) {  // cells no thread of this kernel owns
+          a.L[LU][p + d] = 0.f;
+          a.L[LV][p + d] = 0.f;
+          a.L[LW][p + d] = 0.f;
+        }
+        a.L[LZZ][p + d] = 0.f;
+        a.L[LXZ][p + d] = 0.f;
+        a.L[LYZ][p + d] = 0.f;
+      }
+    }
+  }
   a.L[LU][p] = dc * lu;
   a.L[LV][p] = dc * lv;
   a.L[LW][p] = dc * lw;
@@ -525,7 +546,6 @@ cudaError_t awp_launch_adjoint_step(const AdjArgs& a, cudaStream_t st) {
     k_adj_stress_cell<false><<<dim3(cdiv(sk, 32), cdiv(sj, 4), si), blk, 0, st>>>(a);
   k_adj_stress_gather<<<dim3(cdiv(sk + 4, 32), cdiv(sj + 4, 4), si + 4), blk, 0, st>>>(a);
   k_adj_images<<<dim3(cdiv(sj + 2, 128), si + 2), 128, 0, st>>>(a);
-  k_adj_images_apply<<<dim3(cdiv(sj + 2, 128), si + 2), 128, 0, st>>>(a);
   const int vi = a.vi1 - a.vi0 + 1, vj = a.vj1 - a.vj0 + 1, vk = a.vk1 - a.vk0 + 1;
   k_adj_vel_cell<<<dim3(cdiv(vk, 32), cdiv(vj, 4), vi), blk, 0, st>>>(a);
   k_adj_vel_gather<<<dim3(cdiv(vk + 4, 32), cdiv(vj + 4, 4), vi + 4), blk, 0, st>>>(a);

@@ -27,6 +27,9 @@ struct AdjArgs {
   // temporaries (zero outside the ranges that write them)
   float* E[11];  // stress half: adjoint strain rates (6), material weights (5)
   float* V[6];   // velocity half: weighted adjoint velocities (3), density weights (3)
+  // image-adjoint increments of the surface columns and their one-column
+  // ring: 4 planes of (si1 - si0 + 3) x (sj1 - sj0 + 3), (i, j) row-major
+  float* img;
   // gradients on the padded kernel arrays: rho, 1/lambda, 1/mu, and the
   // surface Lame ratio lam_mu (2-D)
   float *gd, *glam, *gmu, *glm;

@@ -1896,6 +1896,40 @@ static int adjoint_plan(awp_ctx* c, int nsteps, int nsnap, AdjPlan* out) {
   return AWP_OK;
 }
 
+// The workspace of a plan: one slab, kept in the context for later calls.
+static int ensure_adjoint_slab(awp_ctx* c, const AdjPlan& pl) {
+  if (c->adj_slab_floats >= pl.floats) return AWP_OK;
+  cudaFree(c->adj_slab);
+  c->adj_slab = nullptr;
+  c->adj_slab_floats = 0;
+  size_t freeb = 0, totb = 0;
+  CU_TRY(cudaMemGetInfo(&freeb, &totb));
+  const double gb = pl.floats * sizeof(float) / 1e9;
+  if (pl.floats * sizeof(float) + (64u << 20) > freeb)
+    return set_error(AWP_ERR_NOMEM,
+                     "adjoint needs %.1f GB (%d snapshots of %.1f MB fields, %d-step "
+                     "segments), %.1f GB free",
+                     gb, pl.nseg + 1, c->g.cells_pad() * 4.0 / 1e6, pl.L, freeb / 1e9);
+  if (cudaMalloc((void**)&c->adj_slab, pl.floats * sizeof(float)) != cudaSuccess) {
+    c->adj_slab = nullptr;
+    return set_error(AWP_ERR_NOMEM, "adjoint workspace of %.1f GB", gb);
+  }
+  c->adj_slab_floats = pl.floats;
+  // touch every page once here, so that the first gradient does not pay the
+  // first-use mapping of the workspace
+  CU_TRY(cudaMemsetAsync(c->adj_slab, 0, pl.floats * sizeof(float), c->stream));
+  return AWP_OK;
+}
+
+int awp_adjoint_reserve(awp_ctx* c, int nsteps, int nsnap) {
+  int e = check_adjoint_ctx(c);
+  if (e) return e;
+  if (nsteps < 1) return set_error(AWP_ERR_ARG, "nsteps < 1");
+  AdjPlan pl;
+  if ((e = adjoint_plan(c, nsteps, nsnap, &pl))) return e;
+  return ensure_adjoint_slab(c, pl);
+}
+
 int awp_adjoint_plan(awp_ctx* c, int nsteps, int nsnap, int* tail_steps, int* segment_steps,
                      int* snapshots, double* workspace_gb) {
   int e = check_adjoint_ctx(c);
@@ -1924,31 +1958,13 @@ int awp_misfit_gradient(awp_ctx* c, int nsteps, int nrec, const int* rec_xyz, co
   const VelBox vb = pl.vb;
   const size_t cv = vb.cells();
   const int M = pl.M, L = pl.L, nseg = pl.nseg;
-  const size_t floats = pl.floats;
   const VelArgs va = make_vel_args(c);
   const StrArgs sa = make_str_args(c);
   auto rnd = slab_round;
   const int H = nsteps - M;
   // one slab for snapshots, stores, adjoint state, temporaries and gradients,
   // kept in the context for the next call
-  if (c->adj_slab_floats < floats) {
-    cudaFree(c->adj_slab);
-    c->adj_slab = nullptr;
-    c->adj_slab_floats = 0;
-    size_t freeb = 0, totb = 0;
-    CU_TRY(cudaMemGetInfo(&freeb, &totb));
-    const double gb = floats * sizeof(float) / 1e9;
-    if (floats * sizeof(float) + (64u << 20) > freeb)
-      return set_error(AWP_ERR_NOMEM,
-                       "adjoint needs %.1f GB (%d snapshots of %.1f MB fields, %d-step "
-                       "segments), %.1f GB free",
-                       gb, nseg + 1, fb / 1e6, L, freeb / 1e9);
-    if (cudaMalloc((void**)&c->adj_slab, floats * sizeof(float)) != cudaSuccess) {
-      c->adj_slab = nullptr;
-      return set_error(AWP_ERR_NOMEM, "adjoint workspace of %.1f GB", gb);
-    }
-    c->adj_slab_floats = floats;
-  }
+  if ((e = ensure_adjoint_slab(c, pl))) return e;
   size_t slab_next = 0;  // floats
   auto take_n = [&](size_t n) -> float* {
     float* q = c->adj_slab + slab_next;
@@ -2047,6 +2063,8 @@ int awp_misfit_gradient(awp_ctx* c, int nsteps, int nrec, const int* rec_xyz, co
   a.si0 = sa.i0; a.si1 = sa.i1; a.sj0 = sa.j0; a.sj1 = sa.j1; a.sk0 = sa.k0; a.sk1 = sa.k1;
   a.gx_lim = sa.gx_lim; a.gy_min = sa.gy_min; a.lam_mu_ld = sa.lam_mu_ld;
   a.fj1 = make_fstr_args(c).j1;
+  if (!(a.img = b.f((size_t)4 * (a.si1 - a.si0 + 3) * (a.sj1 - a.sj0 + 3))))
+    return set_error(AWP_ERR_NOMEM, "image scratch");
   // segment store: the velocities at the start of a segment and after each
   // of its steps (slot 0 = start)
   std::vector<float*> seg((size_t)(H > 0 ? L + 1 : 0) * 3, nullptr);

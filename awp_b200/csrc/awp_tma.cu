@@ -193,6 +193,22 @@ __global__ void __launch_bounds__(NT, 2)
   // media of the current x plane at (j,k), (j-1,k), (j,k-1), (j-1,k-1): the
   // next plane's values of one step are the current plane's of the next
   float cl[4], cmu[4], cqp[4], cqs[4];
+  // relaxation-table entries of this (j, k) column.  The table index depends
+  // on the parity of i only (period 2 along the march), so both are read once
+  // here instead of per plane, where the lanes of a warp (alternating k
+  // parity) would split each constant-bank read in two.
+  float tv1[2], tv2[2], twwo[2], tc0[2] = {0.f, 0.f}, tc1[2] = {0.f, 0.f};
+#pragma unroll
+  for (int q = 0; q < 2; ++q) {
+    const int t = awp_tex_index(a.tex, ib + q, j, k);
+    tv1[q] = a.tex.tau1[t];
+    tv2[q] = a.tex.tau2[t];
+    twwo[q] = a.tex.wwo8[t];
+    if (!ELASTIC) {
+      tc0[q] = a.coeff[2 * t];
+      tc1[q] = a.coeff[2 * t + 1];
+    }
+  }
   for (int i = ib; i <= ie; ++i) {
     // ---- wait for the planes this step reads for the first time ------------
     if (i == ib) {
@@ -256,12 +272,12 @@ __global__ void __launch_bounds__(NT, 2)
     float nl[4], nmu[4], nqp[4], nqs[4];
     m4(Mn, 0, nl[0], nl[1], nl[2], nl[3]);
     m4(Mn, 1, nmu[0], nmu[1], nmu[2], nmu[3]);
-    const int t = awp_tex_index(a.tex, i, j, k);
-    const float f_vx1 = a.tex.tau1[t], f_vx2 = a.tex.tau2[t], f_wwo = a.tex.wwo8[t];
-    float QP8 = 0.f, QS8 = 0.f, cc0 = 0.f, cc1 = 0.f;
+    const bool odd = ((i - ib) & 1) != 0;
+    const float f_vx1 = odd ? tv1[1] : tv1[0], f_vx2 = odd ? tv2[1] : tv2[0],
+                f_wwo = odd ? twwo[1] : twwo[0];
+    float QP8 = 0.f, QS8 = 0.f;
+    const float cc0 = odd ? tc0[1] : tc0[0], cc1 = odd ? tc1[1] : tc1[0];
     if (!ELASTIC) {
-      cc0 = a.coeff[2 * t];
-      cc1 = a.coeff[2 * t + 1];
       m4(Mn, 2, nqp[0], nqp[1], nqp[2], nqp[3]);
       m4(Mn, 3, nqs[0], nqs[1], nqs[2], nqs[3]);
       QP8 = cqp[0] + nqp[0] + cqp[1] + nqp[1] + cqp[2] + nqp[2] + cqp[3] + nqp[3];

@@ -557,13 +557,23 @@ def run_adjoint(args) -> dict:
     s.set_moduli(*m0)
     s.reset()
     adjoint.seismograms(s, min(steps, 20), xyz, comp)  # warm-up
+    # the workspace (snapshots, velocity store) is allocated once per solver
+    # and kept for later gradients; its allocation is timed on its own
+    ms_alloc, _ = timed(lambda: adjoint.adjoint_reserve(s, steps))
     sampler = ClockSampler(torch.cuda.current_device())
     sampler.start()
-    s.reset()
-    ms_fwd, _ = timed(lambda: adjoint.seismograms(s, steps, xyz, comp))
-    s.reset()
-    ms_adj, (J, seis, gl, gm, gr) = timed(
-        lambda: adjoint.misfit_gradient(s, steps, xyz, comp, d_obs))
+    # three forward runs and three gradients, alternating; the means are
+    # reported (single runs of either vary by a few percent with the clocks)
+    fwd_runs, adj_runs = [], []
+    for _ in range(args.adj_reps):
+        s.reset()
+        fwd_runs.append(timed(lambda: adjoint.seismograms(s, steps, xyz, comp))[0])
+        s.reset()
+        ms, (J, seis, gl, gm, gr) = timed(
+            lambda: adjoint.misfit_gradient(s, steps, xyz, comp, d_obs))
+        adj_runs.append(ms)
+    ms_fwd = float(np.mean(fwd_runs))
+    ms_adj = float(np.mean(adj_runs))
     clocks = sampler.stop()
     plan = adjoint.adjoint_plan(s, steps)  # the storage the timed call used
     # finite differences along seeded relative directions
@@ -593,7 +603,8 @@ def run_adjoint(args) -> dict:
         "config": {"workload": scn.description, "grid": [nx, ny, nz], "cells": cells,
                    "receivers": int(len(comp)), "storage": plan,
                    "l2": "state of GBs >> 126 MB L2, no flush needed"},
-        "forward_ms": ms_fwd, "adjoint_ms": ms_adj,
+        "forward_ms": ms_fwd, "adjoint_ms": ms_adj, "workspace_alloc_ms": ms_alloc,
+        "forward_runs_ms": fwd_runs, "adjoint_runs_ms": adj_runs,
         "forward_gcell_updates_s": cells * steps / (ms_fwd * 1e-3) / 1e9,
         "misfit": J,
         "fd_check": {"eps_rel": eps, "directions": fd_rows,
@@ -627,7 +638,8 @@ def run_extras(args) -> dict:
     try:
         a = run_adjoint(sub)
         out["adjoint"] = {k: a[k] for k in ("metric", "value", "unit", "forward_ms",
-                                             "adjoint_ms", "misfit")}
+                                             "adjoint_ms", "workspace_alloc_ms",
+                                             "forward_runs_ms", "adjoint_runs_ms", "misfit")}
         out["adjoint"]["config"] = a["config"]
         out["adjoint"]["fd_check"] = a["fd_check"]
     except Exception as exc:
@@ -645,6 +657,8 @@ def main():
                     choices=["layered_vk", "halfspace", "batched", "adjoint"])
     ap.add_argument("--adj-steps", type=int, default=1500,
                     help="time steps of the misfit-gradient run (--workload adjoint)")
+    ap.add_argument("--adj-reps", type=int, default=3,
+                    help="timed forward runs and gradients, alternating (--workload adjoint)")
     ap.add_argument("--fd-dirs", type=int, default=8,
                     help="finite-difference directions (--workload adjoint)")
     ap.add_argument("--batch-n", type=int, default=96,

@@ -273,6 +273,10 @@ int awp_misfit_gradient(awp_ctx* ctx, int nsteps, int nrec, const int* rec_xyz, 
  * output may be NULL. */
 int awp_adjoint_plan(awp_ctx* ctx, int nsteps, int nsnap, int* tail_steps, int* segment_steps,
                      int* snapshots, double* workspace_gb);
+/* Allocate now the workspace awp_misfit_gradient(nsteps, nsnap) would
+ * allocate on its first call (it stays in the context), so that an inversion
+ * loop or a timing excludes the allocation. */
+int awp_adjoint_reserve(awp_ctx* ctx, int nsteps, int nsnap);
 
 /* Host-only helper (no context, no GPU): the metric arrays of a topography
  * file (INTOPO) for an nx x ny x nz grid of spacing h, as topo_init_metrics /

@@ -127,6 +127,7 @@ def test_checkpoint_count_does_not_change_the_gradient():
     out = []
     for nsnap in (1, 5, 24, 0):  # 0: the velocities of as many last steps as fit are kept
         plan = adjoint.adjoint_plan(s, steps, nsnap)
+        adjoint.adjoint_reserve(s, steps, nsnap)  # the call below reuses it
         if nsnap > 0:  # snapshots at the segment starts plus the final state
             assert plan["tail_steps"] == 0
             assert plan["segment_steps"] == -(-steps // nsnap)
