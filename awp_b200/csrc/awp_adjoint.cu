@@ -40,10 +40,12 @@ enum { VA, VB, VC, VEA, VEB, VEC };
 
 // ---------------------------------------------------------------------------
 // stress^T, pointwise part: memory variables and stresses in place, adjoint
-// strain rates and the material weights of the cell into E[]
+// strain rates of the cell into E[], its material weights added to the sums
+// in E[].  Six 128-thread CTAs per SM (80 registers, a few spilled) run it
+// faster than four without spills: the kernel waits on HBM latency.
 // ---------------------------------------------------------------------------
 template <bool ELASTIC>
-__global__ void k_adj_stress_cell(const AdjArgs a) {
+__global__ void __launch_bounds__(128, 6) k_adj_stress_cell(const AdjArgs a) {
   // the relaxation tables in shared memory: the lanes of a warp alternate the
   // table entry with the parity of k, which a constant-bank read would serve
   // in two passes
@@ -144,6 +146,10 @@ __global__ void k_adj_stress_cell(const AdjArgs a) {
   float rv[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
   if (!ELASTIC)
     for (int q = 0; q < 6; ++q) rv[q] = a.L[LR1 + q][p];
+  // material weights, summed over the time steps (their spatial transposes
+  // are linear and time-invariant, so k_adj_material applies them once)
+  float wacc[5];
+  for (int q = 0; q < 5; ++q) wacc[q] = a.E[GL8 + q][p];
   // normal components
   float PX, PY, PZ, QX = 0.f, QY = 0.f, QZ = 0.f;
   PX = K * lx;
@@ -195,11 +201,11 @@ __global__ void k_adj_stress_cell(const AdjArgs a) {
   // chain to the eight-cell sums
   const float G_xlraw = G_xl * a.dth + G_qpa * c_q;
   const float G_xmraw = G_xm * c_xm + G_h * c_h + G_xlraw;
-  E[GL8][p] = -8.0f / (L8 * L8) * G_xlraw;
-  E[GM8][p] = -16.0f / (M8 * M8) * G_xmraw;
-  E[GP1][p] = GP[0];
-  E[GP2][p] = GP[1];
-  E[GP3][p] = GP[2];
+  E[GL8][p] = wacc[0] + -8.0f / (L8 * L8) * G_xlraw;
+  E[GM8][p] = wacc[1] + -16.0f / (M8 * M8) * G_xmraw;
+  E[GP1][p] = wacc[2] + GP[0];
+  E[GP2][p] = wacc[3] + GP[1];
+  E[GP3][p] = wacc[4] + GP[2];
 }
 
 // ---------------------------------------------------------------------------
@@ -232,22 +238,10 @@ __global__ void k_adj_stress_gather(const AdjArgs a) {
   const float dw = c1 * (e3[q] - e3[q + 1]) + c2 * (e3[q - 1] - e3[q + 2]) +
                    c1 * (e5[q] - e5[q + S]) + c2 * (e5[q - S] - e5[q + 2 * S]) +
                    c1 * (e6[q - Y] - e6[q]) + c2 * (e6[q - 2 * Y] - e6[q + Y]);
-  // box8(p) = {p, p+S, p-Y, p+S-Y, p-1, p+S-1, p-Y-1, p+S-Y-1} contains q for
-  // p in {q, q-S, q+Y, q-S+Y, q+1, q-S+1, q+Y+1, q-S+Y+1}
-  auto box = [&](const float* x) {
-    return x[q] + x[q - S] + x[q + Y] + x[q - S + Y] + x[q + 1] + x[q - S + 1] + x[q + Y + 1] +
-           x[q - S + Y + 1];
-  };
-  const float dl = box(a.E[GL8]);
-  const float dm = box(a.E[GM8]) + a.E[GP1][q] + a.E[GP1][q + 1] + a.E[GP2][q] + a.E[GP2][q + Y] +
-                   a.E[GP3][q] + a.E[GP3][q - S];
   const float lu = a.L[LU][q], lv = a.L[LV][q], lw = a.L[LW][q];
-  const float gl = a.glam[q], gm = a.gmu[q];
   a.L[LU][q] = lu + du;
   a.L[LV][q] = lv + dv;
   a.L[LW][q] = lw + dw;
-  a.glam[q] = gl + dl;
-  a.gmu[q] = gm + dm;
 }
 
 // ---------------------------------------------------------------------------
@@ -335,6 +329,7 @@ __global__ void k_adj_vel_cell(const AdjArgs a) {
   const float sv = a.fv[pv] - dc * a.bv[pv];
   const float sw = a.fw[pv] - dc * a.bw[pv];
   float lu = a.L[LU][p], lv = a.L[LV][p], lw = a.L[LW][p];
+  const float wa = a.V[VEA][p], wb = a.V[VEB][p], wc = a.V[VEC][p];
   // the image adjoints of the surface columns (k_adj_images) enter here:
   // u, v, w(top) of the window and its ring, w(top-1) of the window; the
   // imaged velocities and stresses above the surface return to zero (fstr
@@ -374,9 +369,10 @@ __global__ void k_adj_vel_cell(const AdjArgs a) {
   a.V[VC][p] = fd3 * dc * lw;
   // d fd / d rho_avg = -fd / rho_avg, each of the four densities weighs 1/4:
   // d u' / d d(q) = -1/4 * (fd D dc) / rho_avg
-  a.V[VEA][p] = -0.25f / r1 * su * lu;
-  a.V[VEB][p] = -0.25f / r2 * sv * lv;
-  a.V[VEC][p] = -0.25f / r3 * sw * lw;
+  // summed over the time steps (k_adj_material applies their transposes)
+  a.V[VEA][p] = wa + -0.25f / r1 * su * lu;
+  a.V[VEB][p] = wb + -0.25f / r2 * sv * lv;
+  a.V[VEC][p] = wc + -0.25f / r3 * sw * lw;
 }
 
 // ---------------------------------------------------------------------------
@@ -404,21 +400,46 @@ __global__ void k_adj_vel_gather(const AdjArgs a) {
   const float dyz = c1 * (B[q] - B[q + 1]) + c2 * (B[q - 1] - B[q + 2]) +
                     c1 * (C[q] - C[q + Y]) + c2 * (C[q - Y] - C[q + 2 * Y]);
   const float dzz = c1 * (C[q - 1] - C[q]) + c2 * (C[q - 2] - C[q + 1]);
-  const float* ea = a.V[VEA];
-  const float* eb = a.V[VEB];
-  const float* ec = a.V[VEC];
-  const float dd = ea[q] + ea[q + Y] + ea[q + 1] + ea[q + Y + 1] + eb[q] + eb[q - S] + eb[q + 1] +
-                   eb[q - S + 1] + ec[q] + ec[q - S] + ec[q + Y] + ec[q - S + Y];
   const float lxx = a.L[LXX][q], lxy = a.L[LXY][q], lxz = a.L[LXZ][q];
   const float lyy = a.L[LYY][q], lyz = a.L[LYZ][q], lzz = a.L[LZZ][q];
-  const float gd = a.gd[q];
   a.L[LXX][q] = lxx + dxx;
   a.L[LXY][q] = lxy + dxy;
   a.L[LXZ][q] = lxz + dxz;
   a.L[LYY][q] = lyy + dyy;
   a.L[LYZ][q] = lyz + dyz;
   a.L[LZZ][q] = lzz + dzz;
-  a.gd[q] = gd + dd;
+}
+
+// ---------------------------------------------------------------------------
+// the material weights summed over the steps -> gradients on the padded
+// arrays, once per sweep: each cell's weight goes to every material value its
+// forward averages read
+//   1/lambda, 1/mu : eight-cell sums at the normal-stress node (box8), mu
+//                    pairs at the shear nodes (xy: k-1, xz: j-1, yz: i+1)
+//   rho            : four-cell averages of the three velocity nodes
+// ---------------------------------------------------------------------------
+__global__ void k_adj_material(const AdjArgs a, int i0, int j0, int k0, int ni, int nj,
+                               int nk) {
+  const int k = k0 + blockIdx.x * 32 + threadIdx.x;
+  const int j = j0 + blockIdx.y * 4 + threadIdx.y;
+  const int i = i0 + blockIdx.z;
+  if (k >= k0 + nk || j >= j0 + nj || i >= i0 + ni) return;
+  const long long S = a.g.slice, Y = a.g.yline;
+  const long long q = (long long)i * S + (long long)j * Y + k;
+  // box8(p) = {p, p+S, p-Y, p+S-Y, p-1, p+S-1, p-Y-1, p+S-Y-1} contains q for
+  // p in {q, q-S, q+Y, q-S+Y, q+1, q-S+1, q+Y+1, q-S+Y+1}
+  auto box = [&](const float* x) {
+    return x[q] + x[q - S] + x[q + Y] + x[q - S + Y] + x[q + 1] + x[q - S + 1] + x[q + Y + 1] +
+           x[q - S + Y + 1];
+  };
+  a.glam[q] = box(a.E[GL8]);
+  a.gmu[q] = box(a.E[GM8]) + a.E[GP1][q] + a.E[GP1][q + 1] + a.E[GP2][q] + a.E[GP2][q + Y] +
+             a.E[GP3][q] + a.E[GP3][q - S];
+  const float* ea = a.V[VEA];
+  const float* eb = a.V[VEB];
+  const float* ec = a.V[VEC];
+  a.gd[q] = ea[q] + ea[q + Y] + ea[q + 1] + ea[q + Y + 1] + eb[q] + eb[q - S] + eb[q + 1] +
+            eb[q - S + 1] + ec[q] + ec[q - S] + ec[q + Y] + ec[q - S + Y];
 }
 
 // One thread per distinct (component, cell); receivers sharing a cell are
@@ -571,6 +592,15 @@ cudaError_t awp_launch_sample(const float* u, const float* v, const float* w,
 
 cudaError_t awp_launch_adjoint_fold(const AdjArgs& a, float* g_lambda, float* g_mu,
                                     float* g_rho, cudaStream_t st) {
+  {
+    // every cell a weight can reach: the stress and velocity ranges +-2
+    const int i0 = min(a.si0, a.vi0) - 2, i1 = max(a.si1, a.vi1) + 2;
+    const int j0 = min(a.sj0, a.vj0) - 2, j1 = max(a.sj1, a.vj1) + 2;
+    const int k0 = min(a.sk0, a.vk0) - 2, k1 = max(a.sk1, a.vk1) + 2;
+    const int ni = i1 - i0 + 1, nj = j1 - j0 + 1, nk = k1 - k0 + 1;
+    k_adj_material<<<dim3(cdiv(nk, 32), cdiv(nj, 4), ni), dim3(32, 4), 0, st>>>(a, i0, j0, k0,
+                                                                                ni, nj, nk);
+  }
   const long long n = (long long)a.g.nxt * a.g.nyt * a.g.nzt;
   k_adj_fold<<<cdiv(n, 256), 256, 0, st>>>(a, g_lambda, g_mu, g_rho);
   return cudaGetLastError();

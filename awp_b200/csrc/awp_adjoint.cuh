@@ -25,8 +25,12 @@ struct AdjArgs {
   // adjoint state, updated in place (u v w xx yy zz xy xz yz r1..r6)
   float* L[15];
   // temporaries (zero outside the ranges that write them)
-  float* E[11];  // stress half: adjoint strain rates (6), material weights (5)
-  float* V[6];   // velocity half: weighted adjoint velocities (3), density weights (3)
+  // stress half: adjoint strain rates (6) and material weights (5); velocity
+  // half: weighted adjoint velocities (3) and density weights (3).  The
+  // weights are summed over the steps and turned into gradients once, by
+  // awp_launch_adjoint_fold.
+  float* E[11];
+  float* V[6];
   // image-adjoint increments of the surface columns and their one-column
   // ring: 4 planes of (si1 - si0 + 3) x (sj1 - sj0 + 3), (i, j) row-major
   float* img;
@@ -66,9 +70,10 @@ cudaError_t awp_launch_sample(const float* u, const float* v, const float* w,
                               const long long* idx, const int* comp, int nrec, float* out,
                               cudaStream_t st);
 
-// Gradients on the padded arrays -> interior lambda, mu, rho (layout
-// [nz][ny][nx], surface first): the border-fill copies folded back, the
-// reciprocal moduli and the surface Lame ratio chained through.
+// The summed material weights -> gradients on the padded arrays -> interior
+// lambda, mu, rho (layout [nz][ny][nx], surface first): the border-fill
+// copies folded back, the reciprocal moduli and the surface Lame ratio
+// chained through.
 cudaError_t awp_launch_adjoint_fold(const AdjArgs& a, float* g_lambda, float* g_mu,
                                     float* g_rho, cudaStream_t st);
 
