@@ -155,26 +155,6 @@ __device__ __forceinline__ void str_tile(const StrArgs& a, const int bx, const i
   float* __restrict__ RR[6] = {a.r1 + col, a.r2 + col, a.r3 + col,
                                a.r4 + col, a.r5 + col, a.r6 + col};
 
-  // relaxation-table entries of this (j, k) column: the table index depends
-  // on the parity of i only (period 2 along the march), so both are read once
-  // here instead of per plane, where the lanes of a warp (alternating k
-  // parity) would split each constant-bank read in two
-  float tv1[2] = {0.f, 0.f}, tv2[2] = {0.f, 0.f}, twwo[2] = {0.f, 0.f};
-  float tc0[2] = {0.f, 0.f}, tc1[2] = {0.f, 0.f};
-  if (!TEXARR) {
-#pragma unroll
-    for (int q = 0; q < 2; ++q) {
-      const int t = awp_tex_index(a.tex, ib + q, j, k);
-      tv1[q] = a.tex.tau1[t];
-      tv2[q] = a.tex.tau2[t];
-      twwo[q] = a.tex.wwo8[t];
-      if (!ELASTIC) {
-        tc0[q] = a.coeff_dev ? LDG(a.coeff_dev + 2 * t) : a.coeff[2 * t];
-        tc1[q] = a.coeff_dev ? LDG(a.coeff_dev + 2 * t + 1) : a.coeff[2 * t + 1];
-      }
-    }
-  }
-
   long long o = (long long)ib * S;
   float u_m1 = LDG(U + o - S), u_0 = LDG(U + o), u_p1 = LDG(U + o + S);
   float v_m2 = LDG(V + o - 2 * S), v_m1 = LDG(V + o - S), v_0 = LDG(V + o);
@@ -214,31 +194,33 @@ __device__ __forceinline__ void str_tile(const StrArgs& a, const int bx, const i
     float uk2 = LDG(U + o + 2), vk2 = LDG(V + o + 2);
 
     // memory-variable coefficients for this cell
-    float f_vx1, f_vx2, f_wwo, cc0 = 0.f, cc1 = 0.f;
+    float f_vx1, f_vx2, f_wwo;
+    int cidx;
     if (TEXARR) {
       const long long p = col + o;
       f_vx1 = LDG(a.vx1 + p);
       f_vx2 = LDG(a.vx2 + p);
       f_wwo = LDG(a.wwo + p);
-      const int cidx = 2 * LDG(a.ww + p) - 2;
-      if (!ELASTIC) {
-        if (a.coeff_dev) {
-          cc0 = LDG(a.coeff_dev + cidx);
-          cc1 = LDG(a.coeff_dev + cidx + 1);
-        } else {
-          cc0 = a.coeff[cidx];
-          cc1 = a.coeff[cidx + 1];
-        }
-      }
+      cidx = 2 * LDG(a.ww + p) - 2;
     } else {
-      const bool odd = ((i - ib) & 1) != 0;
-      f_vx1 = odd ? tv1[1] : tv1[0];
-      f_vx2 = odd ? tv2[1] : tv2[0];
-      f_wwo = odd ? twwo[1] : twwo[0];
-      cc0 = odd ? tc0[1] : tc0[0];
-      cc1 = odd ? tc1[1] : tc1[0];
+      const int t = awp_tex_index(a.tex, i, j, k);
+      f_vx1 = a.tex.tau1[t];
+      f_vx2 = a.tex.tau2[t];
+      f_wwo = a.tex.wwo8[t];
+      cidx = 2 * t;
     }
     const float dcrj = LDG(a.dcrjx + i) * dcy * dcz;
+
+    float cc0 = 0.f, cc1 = 0.f;
+    if (!ELASTIC) {
+      if (a.coeff_dev) {
+        cc0 = LDG(a.coeff_dev + cidx);
+        cc1 = LDG(a.coeff_dev + cidx + 1);
+      } else {
+        cc0 = a.coeff[cidx];
+        cc1 = a.coeff[cidx + 1];
+      }
+    }
     const AwpStrCoef cf = awp_stress_coef<ELASTIC>(
         sum8(lam_c, lam_n), sum8(mu_c, mu_n), mu_c.a, mu_c.c, mu_c.b, mu_n.a,
         sum8(qp_c, qp_n), sum8(qs_c, qs_n), qs_c.a, qs_c.c, qs_c.b, qs_n.a, f_vx1, f_vx2, f_wwo,
