@@ -291,12 +291,17 @@ __global__ void __launch_bounds__(32 * TY, TY == 8 ? 2 : 1)
 __device__ __forceinline__ void fstr_cell(const FstrArgs& a, const int i, const int j) {
   if (j > a.j1 || i > a.i1) return;
   const long long p = (long long)i * a.slice + (long long)j * a.yline + a.ktop;
-  a.zz[p + 1] = -a.zz[p];
-  a.zz[p + 2] = -a.zz[p - 1];
-  a.xz[p + 1] = -a.xz[p - 1];
-  a.xz[p + 2] = -a.xz[p - 2];
-  a.yz[p + 1] = -a.yz[p - 1];
-  a.yz[p + 2] = -a.yz[p - 2];
+  // all six reads before the first write (each write could alias a later
+  // read, so in store order every read would wait a full memory round trip)
+  const float zz0 = a.zz[p], zz1 = a.zz[p - 1];
+  const float xz1 = a.xz[p - 1], xz2 = a.xz[p - 2];
+  const float yz1 = a.yz[p - 1], yz2 = a.yz[p - 2];
+  a.zz[p + 1] = -zz0;
+  a.zz[p + 2] = -zz1;
+  a.xz[p + 1] = -xz1;
+  a.xz[p + 2] = -xz2;
+  a.yz[p + 1] = -yz1;
+  a.yz[p + 2] = -yz2;
   a.xz[p] = 0.0f;
   a.yz[p] = 0.0f;
 }
