@@ -177,9 +177,11 @@ def texture_arrays(nx, ny, nz, tau1, tau2, w8):
     return vx1, vx2, ww, wwo
 
 
-def reference_gpu(scn, solver, steps=4, warmup=2) -> dict:
+def reference_gpu(scn, solver, steps=4, warmup=2, topo_path=None) -> dict:
     """The reference's own CUDA build (oracle/_ref/libawpref.so, 8-thread blocks as
-    shipped) on the same workload, inputs taken from the product's set-up."""
+    shipped) on the same workload, inputs taken from the product's set-up; with
+    a topography file, its curvilinear kernels (oracle/_ref/libawpref_topo.so)
+    in place of dvelcx / dstrqc."""
     import torch
     from oracle import refbind
     p = scn.params
@@ -205,7 +207,10 @@ def reference_gpu(scn, solver, steps=4, warmup=2) -> dict:
     del media
     with torch.cuda.stream(torch.cuda.default_stream()):
         # the reference launchers run on the legacy default stream
-        sim = refbind.RefGpuSim(scn, setup)
+        if topo_path:
+            sim = refbind.RefTopoSim(scn, setup, topo_path)
+        else:
+            sim = refbind.RefGpuSim(scn, setup)
         del setup, vx1, vx2, ww, wwo
         sim.step(warmup)
         s0 = torch.cuda.Event(enable_timing=True)
@@ -220,6 +225,11 @@ def reference_gpu(scn, solver, steps=4, warmup=2) -> dict:
            "ms_per_step": ms, "steps": steps,
            "build": "reference src/awp/kernel.cu, nvcc sm_100a -O3 -use_fast_math, "
                     "BLOCK_SIZE 2x2x4 as shipped; launched in the pmcl3d single-rank order"}
+    if topo_path:
+        out["build"] += ("; curvilinear top grid: the reference's topo_velocity_interior_H "
+                         "and topo_stress_{interior,left,right}_H (opt_topography kernels)")
+    if hasattr(sim, "close"):
+        sim.close()
     del sim
     torch.cuda.empty_cache()
     return out
@@ -402,7 +412,7 @@ def run_ours(args, rank, world, dist) -> dict | None:
         try:
             s2 = Solver(default_params(**p))
             s2.upload_media(scn.media)
-            line["reference_gpu_build"] = reference_gpu(scn, s2)
+            line["reference_gpu_build"] = reference_gpu(scn, s2, topo_path=topo_path)
             s2.close()
         except Exception as exc:  # reported, never substituted
             line["reference_gpu_build"] = {"unavailable": f"{type(exc).__name__}: {exc}"}
