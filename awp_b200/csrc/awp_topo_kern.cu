@@ -96,8 +96,16 @@ __global__ void __launch_bounds__(128) k_topo_velocity(const TopoArgs a) {
   const float *__restrict__ s11 = a.xx, *__restrict__ s12 = a.xy, *__restrict__ s13 = a.xz,
               *__restrict__ s22 = a.yy, *__restrict__ s23 = a.yz, *__restrict__ s33 = a.zz;
   const float* __restrict__ rho = a.d1;
-  auto S = [&](const float* __restrict__ s, int ii, int jj, int kk) { return ld(s, X.p(ii, jj, kk)); };
-  auto F = [&](const float* __restrict__ f, int ii, int jj) { return ld(f, X.f(ii, jj)); };
+  // neighbours as 32-bit offsets from this cell (the offsets are constants
+  // times the strides, so each distinct one costs one multiply-add, not a
+  // 64-bit index per load)
+  const long long oc = X.p(i, j, k), ofc = X.f(i, j);
+  auto S = [&](const float* __restrict__ s, int ii, int jj, int kk) {
+    return __ldg(s + oc + ((ii - i) * a.slice + (jj - j) * a.yline + (kk - k)));
+  };
+  auto F = [&](const float* __restrict__ f, int ii, int jj) {
+    return __ldg(f + ofc + ((ii - i) * a.fld + (jj - j)));
+  };
 
   // density at the staggered velocity points (velocity_unroll.cu:140-152)
   const float rho1 = 0.25f * (S(rho, i, j, k - 1) + S(rho, i, j - 1, k - 1)) +
@@ -195,8 +203,16 @@ __global__ void __launch_bounds__(128) k_topo_stress(const TopoArgs a) {
   const int r = (k >= nz - 6) ? nz - 1 - k : -1;
   const Idx X{a.slice, a.yline, a.fld};
   const float *__restrict__ u1 = a.u1, *__restrict__ v1 = a.v1, *__restrict__ w1 = a.w1;
-  auto S = [&](const float* __restrict__ s, int ii, int jj, int kk) { return ld(s, X.p(ii, jj, kk)); };
-  auto F = [&](const float* __restrict__ f, int ii, int jj) { return ld(f, X.f(ii, jj)); };
+  // neighbours as 32-bit offsets from this cell (the offsets are constants
+  // times the strides, so each distinct one costs one multiply-add, not a
+  // 64-bit index per load)
+  const long long oc = X.p(i, j, k), ofc = X.f(i, j);
+  auto S = [&](const float* __restrict__ s, int ii, int jj, int kk) {
+    return __ldg(s + oc + ((ii - i) * a.slice + (jj - j) * a.yline + (kk - k)));
+  };
+  auto F = [&](const float* __restrict__ f, int ii, int jj) {
+    return __ldg(f + ofc + ((ii - i) * a.fld + (jj - j)));
+  };
   const float gc = gk(a.g_c, k), g = gk(a.g, k);
 
   // ---- normal components: Jii = 1 / (f_c g3_c) (stress_attenuation.cu:340-431)
