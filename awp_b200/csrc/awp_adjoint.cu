@@ -64,33 +64,35 @@ __global__ void __launch_bounds__(128, 6) k_adj_stress_cell(const AdjArgs a) {
   const int j = a.sj0 + blockIdx.y * 4 + threadIdx.y;
   const int i = a.si0 + blockIdx.z;
   if (k > a.sk1 || j > a.sj1 || i > a.si1) return;
-  const long long S = a.g.slice, Y = a.g.yline;
+  // stencil neighbours as 32-bit offsets from per-array pointers at the cell
+  const int S = a.g.slice, Y = a.g.yline;
   const long long p = (long long)i * S + (long long)j * Y + k;
   const float c1 = a.c1, c2 = a.c2, DT = a.dt;
 
   // forward strain rates from the velocities after the step (VelBox layout)
-  const float* u = a.fu;
-  const float* v = a.fv;
-  const float* w = a.fw;
-  const long long VS = a.vb.S, VY = a.vb.Y;
-  const long long pv = (long long)i * VS + (long long)j * VY + k - a.vb.off;
-  const float vs1 = c1 * (u[pv + VS] - u[pv]) + c2 * (u[pv + 2 * VS] - u[pv - VS]);
-  const float vs2 = c1 * (v[pv] - v[pv - VY]) + c2 * (v[pv + VY] - v[pv - 2 * VY]);
-  const float vs3 = c1 * (w[pv] - w[pv - 1]) + c2 * (w[pv + 1] - w[pv - 2]);
-  const float e4 = c1 * (u[pv + VY] - u[pv]) + c2 * (u[pv + 2 * VY] - u[pv - VY]) +
-                   c1 * (v[pv] - v[pv - VS]) + c2 * (v[pv + VS] - v[pv - 2 * VS]);
-  const float e5 = c1 * (u[pv + 1] - u[pv]) + c2 * (u[pv + 2] - u[pv - 1]) +
-                   c1 * (w[pv] - w[pv - VS]) + c2 * (w[pv + VS] - w[pv - 2 * VS]);
-  const float e6 = c1 * (v[pv + 1] - v[pv]) + c2 * (v[pv + 2] - v[pv - 1]) +
-                   c1 * (w[pv + VY] - w[pv]) + c2 * (w[pv + 2 * VY] - w[pv - VY]);
+  const int VS = (int)a.vb.S, VY = (int)a.vb.Y;
+  const long long pv = (long long)i * a.vb.S + (long long)j * a.vb.Y + k - a.vb.off;
+  const float* u = a.fu + pv;
+  const float* v = a.fv + pv;
+  const float* w = a.fw + pv;
+  const float vs1 = c1 * (u[VS] - u[0]) + c2 * (u[2 * VS] - u[-VS]);
+  const float vs2 = c1 * (v[0] - v[-VY]) + c2 * (v[VY] - v[-(2 * VY)]);
+  const float vs3 = c1 * (w[0] - w[-1]) + c2 * (w[1] - w[-2]);
+  const float e4 = c1 * (u[VY] - u[0]) + c2 * (u[2 * VY] - u[-VY]) +
+                   c1 * (v[0] - v[-VS]) + c2 * (v[VS] - v[-(2 * VS)]);
+  const float e5 = c1 * (u[1] - u[0]) + c2 * (u[2] - u[-1]) +
+                   c1 * (w[0] - w[-VS]) + c2 * (w[VS] - w[-(2 * VS)]);
+  const float e6 = c1 * (v[1] - v[0]) + c2 * (v[2] - v[-1]) +
+                   c1 * (w[VY] - w[0]) + c2 * (w[2 * VY] - w[-VY]);
 
   // materials of the cell (kernel.cu:962-1070)
-  auto sum8 = [&](const float* m) {
-    return m[p] + m[p + S] + m[p - Y] + m[p + S - Y] + m[p - 1] + m[p + S - 1] + m[p - Y - 1] +
-           m[p + S - Y - 1];
+  auto sum8 = [&](const float* m0) {
+    const float* m = m0 + p;
+    return m[0] + m[S] + m[-Y] + m[S - Y] + m[-1] + m[S - 1] + m[-Y - 1] + m[S - Y - 1];
   };
+  const float* mu = a.mu + p;
   const float L8 = sum8(a.lam), M8 = sum8(a.mu);
-  const float P1 = a.mu[p] + a.mu[p - 1], P2 = a.mu[p] + a.mu[p - Y], P3 = a.mu[p] + a.mu[p + S];
+  const float P1 = mu[0] + mu[-1], P2 = mu[0] + mu[-Y], P3 = mu[0] + mu[S];
   const float xm_raw = 16.0f / M8;
   const float xl_raw = 8.0f / L8 + xm_raw;
   const float m1_raw = 2.0f / P1, m2_raw = 2.0f / P2, m3_raw = 2.0f / P3;
@@ -101,9 +103,10 @@ __global__ void __launch_bounds__(128, 6) k_adj_stress_cell(const AdjArgs a) {
     const float cc0 = tab[24 + 2 * t], cc1 = tab[25 + 2 * t];
     const float hw = awp_qf_weight(0.0625f * sum8(a.qs), wwo, cc0, cc1, a.qthr);
     const float qpaw = awp_qf_weight(0.0625f * sum8(a.qp), wwo, cc0, cc1, a.qthr);
-    const float hiw[3] = {awp_qf_weight(0.25f * (a.qs[p] + a.qs[p - 1]), wwo, cc0, cc1, a.qthr),
-                          awp_qf_weight(0.25f * (a.qs[p] + a.qs[p - Y]), wwo, cc0, cc1, a.qthr),
-                          awp_qf_weight(0.25f * (a.qs[p] + a.qs[p + S]), wwo, cc0, cc1, a.qthr)};
+    const float* qs = a.qs + p;
+    const float hiw[3] = {awp_qf_weight(0.25f * (qs[0] + qs[-1]), wwo, cc0, cc1, a.qthr),
+                          awp_qf_weight(0.25f * (qs[0] + qs[-Y]), wwo, cc0, cc1, a.qthr),
+                          awp_qf_weight(0.25f * (qs[0] + qs[S]), wwo, cc0, cc1, a.qthr)};
     c_h = -hw * a.dh1 * fvx1;
     c_xm = a.dth + DT * c_h;
     c_q = -qpaw * a.dh1 * fvx1;
@@ -218,26 +221,26 @@ __global__ void k_adj_stress_gather(const AdjArgs a) {
   const int j = a.sj0 - 2 + blockIdx.y * 4 + threadIdx.y;
   const int i = a.si0 - 2 + blockIdx.z;
   if (k > a.sk1 + 2 || j > a.sj1 + 2 || i > a.si1 + 2) return;
-  const long long S = a.g.slice, Y = a.g.yline;
+  const int S = a.g.slice, Y = a.g.yline;
   const long long q = (long long)i * S + (long long)j * Y + k;
   const float c1 = a.c1, c2 = a.c2;
-  const float* e1 = a.E[E1];
-  const float* e2 = a.E[E2];
-  const float* e3 = a.E[E3];
-  const float* e4 = a.E[E4];
-  const float* e5 = a.E[E5];
-  const float* e6 = a.E[E6];
+  const float* e1 = a.E[E1] + q;
+  const float* e2 = a.E[E2] + q;
+  const float* e3 = a.E[E3] + q;
+  const float* e4 = a.E[E4] + q;
+  const float* e5 = a.E[E5] + q;
+  const float* e6 = a.E[E6] + q;
   // the sums first, then the read-modify-writes, so that no load waits
   // behind a store
-  const float du = c1 * (e1[q - S] - e1[q]) + c2 * (e1[q - 2 * S] - e1[q + S]) +
-                   c1 * (e4[q - Y] - e4[q]) + c2 * (e4[q - 2 * Y] - e4[q + Y]) +
-                   c1 * (e5[q - 1] - e5[q]) + c2 * (e5[q - 2] - e5[q + 1]);
-  const float dv = c1 * (e2[q] - e2[q + Y]) + c2 * (e2[q - Y] - e2[q + 2 * Y]) +
-                   c1 * (e4[q] - e4[q + S]) + c2 * (e4[q - S] - e4[q + 2 * S]) +
-                   c1 * (e6[q - 1] - e6[q]) + c2 * (e6[q - 2] - e6[q + 1]);
-  const float dw = c1 * (e3[q] - e3[q + 1]) + c2 * (e3[q - 1] - e3[q + 2]) +
-                   c1 * (e5[q] - e5[q + S]) + c2 * (e5[q - S] - e5[q + 2 * S]) +
-                   c1 * (e6[q - Y] - e6[q]) + c2 * (e6[q - 2 * Y] - e6[q + Y]);
+  const float du = c1 * (e1[-S] - e1[0]) + c2 * (e1[-(2 * S)] - e1[S]) +
+                   c1 * (e4[-Y] - e4[0]) + c2 * (e4[-(2 * Y)] - e4[Y]) +
+                   c1 * (e5[-1] - e5[0]) + c2 * (e5[-2] - e5[1]);
+  const float dv = c1 * (e2[0] - e2[Y]) + c2 * (e2[-Y] - e2[2 * Y]) +
+                   c1 * (e4[0] - e4[S]) + c2 * (e4[-S] - e4[2 * S]) +
+                   c1 * (e6[-1] - e6[0]) + c2 * (e6[-2] - e6[1]);
+  const float dw = c1 * (e3[0] - e3[1]) + c2 * (e3[-1] - e3[2]) +
+                   c1 * (e5[0] - e5[S]) + c2 * (e5[-S] - e5[2 * S]) +
+                   c1 * (e6[-Y] - e6[0]) + c2 * (e6[-(2 * Y)] - e6[Y]);
   const float lu = a.L[LU][q], lv = a.L[LV][q], lw = a.L[LW][q];
   a.L[LU][q] = lu + du;
   a.L[LV][q] = lv + dv;
@@ -384,22 +387,22 @@ __global__ void k_adj_vel_gather(const AdjArgs a) {
   const int j = a.vj0 - 2 + blockIdx.y * 4 + threadIdx.y;
   const int i = a.vi0 - 2 + blockIdx.z;
   if (k > a.vk1 + 2 || j > a.vj1 + 2 || i > a.vi1 + 2) return;
-  const long long S = a.g.slice, Y = a.g.yline;
+  const int S = a.g.slice, Y = a.g.yline;
   const long long q = (long long)i * S + (long long)j * Y + k;
   const float c1 = a.c1, c2 = a.c2;
-  const float* A = a.V[VA];
-  const float* B = a.V[VB];
-  const float* C = a.V[VC];
+  const float* A = a.V[VA] + q;
+  const float* B = a.V[VB] + q;
+  const float* C = a.V[VC] + q;
   // the sums first, then the read-modify-writes (no load behind a store)
-  const float dxx = c1 * (A[q] - A[q + S]) + c2 * (A[q - S] - A[q + 2 * S]);
-  const float dxy = c1 * (A[q] - A[q + Y]) + c2 * (A[q - Y] - A[q + 2 * Y]) +
-                    c1 * (B[q - S] - B[q]) + c2 * (B[q - 2 * S] - B[q + S]);
-  const float dxz = c1 * (A[q] - A[q + 1]) + c2 * (A[q - 1] - A[q + 2]) +
-                    c1 * (C[q - S] - C[q]) + c2 * (C[q - 2 * S] - C[q + S]);
-  const float dyy = c1 * (B[q - Y] - B[q]) + c2 * (B[q - 2 * Y] - B[q + Y]);
-  const float dyz = c1 * (B[q] - B[q + 1]) + c2 * (B[q - 1] - B[q + 2]) +
-                    c1 * (C[q] - C[q + Y]) + c2 * (C[q - Y] - C[q + 2 * Y]);
-  const float dzz = c1 * (C[q - 1] - C[q]) + c2 * (C[q - 2] - C[q + 1]);
+  const float dxx = c1 * (A[0] - A[S]) + c2 * (A[-S] - A[2 * S]);
+  const float dxy = c1 * (A[0] - A[Y]) + c2 * (A[-Y] - A[2 * Y]) +
+                    c1 * (B[-S] - B[0]) + c2 * (B[-(2 * S)] - B[S]);
+  const float dxz = c1 * (A[0] - A[1]) + c2 * (A[-1] - A[2]) +
+                    c1 * (C[-S] - C[0]) + c2 * (C[-(2 * S)] - C[S]);
+  const float dyy = c1 * (B[-Y] - B[0]) + c2 * (B[-(2 * Y)] - B[Y]);
+  const float dyz = c1 * (B[0] - B[1]) + c2 * (B[-1] - B[2]) +
+                    c1 * (C[0] - C[Y]) + c2 * (C[-Y] - C[2 * Y]);
+  const float dzz = c1 * (C[-1] - C[0]) + c2 * (C[-2] - C[1]);
   const float lxx = a.L[LXX][q], lxy = a.L[LXY][q], lxz = a.L[LXZ][q];
   const float lyy = a.L[LYY][q], lyz = a.L[LYZ][q], lzz = a.L[LZZ][q];
   a.L[LXX][q] = lxx + dxx;

@@ -572,8 +572,9 @@ def run_adjoint(args) -> dict:
     ms_alloc, _ = timed(lambda: adjoint.adjoint_reserve(s, steps))
     sampler = ClockSampler(torch.cuda.current_device())
     sampler.start()
-    # three forward runs and three gradients, alternating; the means are
-    # reported (single runs of either vary by a few percent with the clocks)
+    # three forward runs and three gradients, alternating; the medians are
+    # reported with every run listed (single runs vary with the power-capped
+    # clocks, a gradient by up to ~20 % on some boxes)
     fwd_runs, adj_runs = [], []
     for _ in range(args.adj_reps):
         s.reset()
@@ -582,8 +583,8 @@ def run_adjoint(args) -> dict:
         ms, (J, seis, gl, gm, gr) = timed(
             lambda: adjoint.misfit_gradient(s, steps, xyz, comp, d_obs))
         adj_runs.append(ms)
-    ms_fwd = float(np.mean(fwd_runs))
-    ms_adj = float(np.mean(adj_runs))
+    ms_fwd = float(np.median(fwd_runs))
+    ms_adj = float(np.median(adj_runs))
     clocks = sampler.stop()
     plan = adjoint.adjoint_plan(s, steps)  # the storage the timed call used
     # finite differences along seeded relative directions
