@@ -216,13 +216,16 @@ __global__ void __launch_bounds__(128, 6) k_adj_stress_cell(const AdjArgs a) {
 // and the untouched k = top+2 values included); material weights -> the
 // gradients of 1/lambda and 1/mu
 // ---------------------------------------------------------------------------
+constexpr int kGch = 4;  // x planes a gather thread marches (register queues along x)
+
 __global__ void k_adj_stress_gather(const AdjArgs a) {
   const int k = a.sk0 - 2 + blockIdx.x * 32 + threadIdx.x;
   const int j = a.sj0 - 2 + blockIdx.y * 4 + threadIdx.y;
-  const int i = a.si0 - 2 + blockIdx.z;
-  if (k > a.sk1 + 2 || j > a.sj1 + 2 || i > a.si1 + 2) return;
+  const int ib = a.si0 - 2 + blockIdx.z * kGch;
+  const int ie = min(ib + kGch - 1, a.si1 + 2);
+  if (k > a.sk1 + 2 || j > a.sj1 + 2) return;
   const int S = a.g.slice, Y = a.g.yline;
-  const long long q = (long long)i * S + (long long)j * Y + k;
+  const long long q = (long long)ib * S + (long long)j * Y + k;
   const float c1 = a.c1, c2 = a.c2;
   const float* e1 = a.E[E1] + q;
   const float* e2 = a.E[E2] + q;
@@ -230,21 +233,37 @@ __global__ void k_adj_stress_gather(const AdjArgs a) {
   const float* e4 = a.E[E4] + q;
   const float* e5 = a.E[E5] + q;
   const float* e6 = a.E[E6] + q;
-  // the sums first, then the read-modify-writes, so that no load waits
-  // behind a store
-  const float du = c1 * (e1[-S] - e1[0]) + c2 * (e1[-(2 * S)] - e1[S]) +
-                   c1 * (e4[-Y] - e4[0]) + c2 * (e4[-(2 * Y)] - e4[Y]) +
-                   c1 * (e5[-1] - e5[0]) + c2 * (e5[-2] - e5[1]);
-  const float dv = c1 * (e2[0] - e2[Y]) + c2 * (e2[-Y] - e2[2 * Y]) +
-                   c1 * (e4[0] - e4[S]) + c2 * (e4[-S] - e4[2 * S]) +
-                   c1 * (e6[-1] - e6[0]) + c2 * (e6[-2] - e6[1]);
-  const float dw = c1 * (e3[0] - e3[1]) + c2 * (e3[-1] - e3[2]) +
-                   c1 * (e5[0] - e5[S]) + c2 * (e5[-S] - e5[2 * S]) +
-                   c1 * (e6[-Y] - e6[0]) + c2 * (e6[-(2 * Y)] - e6[Y]);
-  const float lu = a.L[LU][q], lv = a.L[LV][q], lw = a.L[LW][q];
-  a.L[LU][q] = lu + du;
-  a.L[LV][q] = lv + dv;
-  a.L[LW][q] = lw + dw;
+  float* Lu = a.L[LU] + q;
+  float* Lv = a.L[LV] + q;
+  float* Lw = a.L[LW] + q;
+  // x queues: e1 at x-2, x-1, x; e4, e5 at x-1, x, x+1
+  float e1m2 = e1[-(2 * S)], e1m1 = e1[-S], e1c = e1[0];
+  float e4m1 = e4[-S], e4c = e4[0], e4p1 = e4[S];
+  float e5m1 = e5[-S], e5c = e5[0], e5p1 = e5[S];
+#pragma unroll 1
+  for (int i = ib; i <= ie; ++i) {
+    // the sums first, then the read-modify-writes, so that no load waits
+    // behind a store
+    const float e1p1 = e1[S], e4p2 = e4[2 * S], e5p2 = e5[2 * S];
+    const float du = c1 * (e1m1 - e1c) + c2 * (e1m2 - e1p1) +
+                     c1 * (e4[-Y] - e4c) + c2 * (e4[-(2 * Y)] - e4[Y]) +
+                     c1 * (e5[-1] - e5c) + c2 * (e5[-2] - e5[1]);
+    const float dv = c1 * (e2[0] - e2[Y]) + c2 * (e2[-Y] - e2[2 * Y]) +
+                     c1 * (e4c - e4p1) + c2 * (e4m1 - e4p2) +
+                     c1 * (e6[-1] - e6[0]) + c2 * (e6[-2] - e6[1]);
+    const float dw = c1 * (e3[0] - e3[1]) + c2 * (e3[-1] - e3[2]) +
+                     c1 * (e5c - e5p1) + c2 * (e5m1 - e5p2) +
+                     c1 * (e6[-Y] - e6[0]) + c2 * (e6[-(2 * Y)] - e6[Y]);
+    const float lu = Lu[0], lv = Lv[0], lw = Lw[0];
+    Lu[0] = lu + du;
+    Lv[0] = lv + dv;
+    Lw[0] = lw + dw;
+    e1m2 = e1m1; e1m1 = e1c; e1c = e1p1;
+    e4m1 = e4c; e4c = e4p1; e4p1 = e4p2;
+    e5m1 = e5c; e5c = e5p1; e5p1 = e5p2;
+    e1 += S; e2 += S; e3 += S; e4 += S; e5 += S; e6 += S;
+    Lu += S; Lv += S; Lw += S;
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -385,32 +404,49 @@ __global__ void k_adj_vel_cell(const AdjArgs a) {
 __global__ void k_adj_vel_gather(const AdjArgs a) {
   const int k = a.vk0 - 2 + blockIdx.x * 32 + threadIdx.x;
   const int j = a.vj0 - 2 + blockIdx.y * 4 + threadIdx.y;
-  const int i = a.vi0 - 2 + blockIdx.z;
-  if (k > a.vk1 + 2 || j > a.vj1 + 2 || i > a.vi1 + 2) return;
+  const int ib = a.vi0 - 2 + blockIdx.z * kGch;
+  const int ie = min(ib + kGch - 1, a.vi1 + 2);
+  if (k > a.vk1 + 2 || j > a.vj1 + 2) return;
   const int S = a.g.slice, Y = a.g.yline;
-  const long long q = (long long)i * S + (long long)j * Y + k;
+  const long long q = (long long)ib * S + (long long)j * Y + k;
   const float c1 = a.c1, c2 = a.c2;
   const float* A = a.V[VA] + q;
   const float* B = a.V[VB] + q;
   const float* C = a.V[VC] + q;
-  // the sums first, then the read-modify-writes (no load behind a store)
-  const float dxx = c1 * (A[0] - A[S]) + c2 * (A[-S] - A[2 * S]);
-  const float dxy = c1 * (A[0] - A[Y]) + c2 * (A[-Y] - A[2 * Y]) +
-                    c1 * (B[-S] - B[0]) + c2 * (B[-(2 * S)] - B[S]);
-  const float dxz = c1 * (A[0] - A[1]) + c2 * (A[-1] - A[2]) +
-                    c1 * (C[-S] - C[0]) + c2 * (C[-(2 * S)] - C[S]);
-  const float dyy = c1 * (B[-Y] - B[0]) + c2 * (B[-(2 * Y)] - B[Y]);
-  const float dyz = c1 * (B[0] - B[1]) + c2 * (B[-1] - B[2]) +
-                    c1 * (C[0] - C[Y]) + c2 * (C[-Y] - C[2 * Y]);
-  const float dzz = c1 * (C[-1] - C[0]) + c2 * (C[-2] - C[1]);
-  const float lxx = a.L[LXX][q], lxy = a.L[LXY][q], lxz = a.L[LXZ][q];
-  const float lyy = a.L[LYY][q], lyz = a.L[LYZ][q], lzz = a.L[LZZ][q];
-  a.L[LXX][q] = lxx + dxx;
-  a.L[LXY][q] = lxy + dxy;
-  a.L[LXZ][q] = lxz + dxz;
-  a.L[LYY][q] = lyy + dyy;
-  a.L[LYZ][q] = lyz + dyz;
-  a.L[LZZ][q] = lzz + dzz;
+  float* L[6] = {a.L[LXX] + q, a.L[LXY] + q, a.L[LXZ] + q,
+                 a.L[LYY] + q, a.L[LYZ] + q, a.L[LZZ] + q};
+  // x queues: A at x-1, x, x+1; B, C at x-2, x-1, x
+  float Am1 = A[-S], Ac = A[0], Ap1 = A[S];
+  float Bm2 = B[-(2 * S)], Bm1 = B[-S], Bc = B[0];
+  float Cm2 = C[-(2 * S)], Cm1 = C[-S], Cc = C[0];
+#pragma unroll 1
+  for (int i = ib; i <= ie; ++i) {
+    // the sums first, then the read-modify-writes (no load behind a store)
+    const float Ap2 = A[2 * S], Bp1 = B[S], Cp1 = C[S];
+    const float dxx = c1 * (Ac - Ap1) + c2 * (Am1 - Ap2);
+    const float dxy = c1 * (Ac - A[Y]) + c2 * (A[-Y] - A[2 * Y]) +
+                      c1 * (Bm1 - Bc) + c2 * (Bm2 - Bp1);
+    const float dxz = c1 * (Ac - A[1]) + c2 * (A[-1] - A[2]) +
+                      c1 * (Cm1 - Cc) + c2 * (Cm2 - Cp1);
+    const float dyy = c1 * (B[-Y] - Bc) + c2 * (B[-(2 * Y)] - B[Y]);
+    const float dyz = c1 * (Bc - B[1]) + c2 * (B[-1] - B[2]) +
+                      c1 * (Cc - C[Y]) + c2 * (C[-Y] - C[2 * Y]);
+    const float dzz = c1 * (C[-1] - Cc) + c2 * (C[-2] - C[1]);
+    const float l0 = L[0][0], l1 = L[1][0], l2 = L[2][0];
+    const float l3 = L[3][0], l4 = L[4][0], l5 = L[5][0];
+    L[0][0] = l0 + dxx;
+    L[1][0] = l1 + dxy;
+    L[2][0] = l2 + dxz;
+    L[3][0] = l3 + dyy;
+    L[4][0] = l4 + dyz;
+    L[5][0] = l5 + dzz;
+    Am1 = Ac; Ac = Ap1; Ap1 = Ap2;
+    Bm2 = Bm1; Bm1 = Bc; Bc = Bp1;
+    Cm2 = Cm1; Cm1 = Cc; Cc = Cp1;
+    A += S; B += S; C += S;
+#pragma unroll
+    for (int f = 0; f < 6; ++f) L[f] += S;
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -568,11 +604,13 @@ cudaError_t awp_launch_adjoint_step(const AdjArgs& a, cudaStream_t st) {
     k_adj_stress_cell<true><<<dim3(cdiv(sk, 32), cdiv(sj, 4), si), blk, 0, st>>>(a);
   else
     k_adj_stress_cell<false><<<dim3(cdiv(sk, 32), cdiv(sj, 4), si), blk, 0, st>>>(a);
-  k_adj_stress_gather<<<dim3(cdiv(sk + 4, 32), cdiv(sj + 4, 4), si + 4), blk, 0, st>>>(a);
+  k_adj_stress_gather<<<dim3(cdiv(sk + 4, 32), cdiv(sj + 4, 4), cdiv(si + 4, kGch)), blk, 0,
+                        st>>>(a);
   k_adj_images<<<dim3(cdiv(sj + 2, 128), si + 2), 128, 0, st>>>(a);
   const int vi = a.vi1 - a.vi0 + 1, vj = a.vj1 - a.vj0 + 1, vk = a.vk1 - a.vk0 + 1;
   k_adj_vel_cell<<<dim3(cdiv(vk, 32), cdiv(vj, 4), vi), blk, 0, st>>>(a);
-  k_adj_vel_gather<<<dim3(cdiv(vk + 4, 32), cdiv(vj + 4, 4), vi + 4), blk, 0, st>>>(a);
+  k_adj_vel_gather<<<dim3(cdiv(vk + 4, 32), cdiv(vj + 4, 4), cdiv(vi + 4, kGch)), blk, 0,
+                     st>>>(a);
   return cudaGetLastError();
 }
 
