@@ -41,11 +41,11 @@ enum { VA, VB, VC, VEA, VEB, VEC };
 // ---------------------------------------------------------------------------
 // stress^T, pointwise part: memory variables and stresses in place, adjoint
 // strain rates of the cell into E[], its material weights added to the sums
-// in E[].  Six 128-thread CTAs per SM (80 registers, a few spilled) run it
+// in E[].  Seven 128-thread CTAs per SM (72 registers, some spilled) run it
 // faster than four without spills: the kernel waits on HBM latency.
 // ---------------------------------------------------------------------------
 template <bool ELASTIC>
-__global__ void __launch_bounds__(128, 6) k_adj_stress_cell(const AdjArgs a) {
+__global__ void __launch_bounds__(128, 7) k_adj_stress_cell(const AdjArgs a) {
   // the relaxation tables in shared memory: the lanes of a warp alternate the
   // table entry with the parity of k, which a constant-bank read would serve
   // in two passes

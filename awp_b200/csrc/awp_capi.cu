@@ -2125,9 +2125,10 @@ int awp_misfit_gradient(awp_ctx* c, int nsteps, int nrec, const int* rec_xyz, co
   }
 
   // ---- gradients to the host; the context ends on the final forward state -----------
+  // staged in three strain-rate temporaries of the slab, free after the sweep
+  // (no allocation per call on a device the workspace nearly fills)
   const size_t ni = (size_t)c->g.nxt * c->g.nyt * c->g.nzt;
-  float *gl = b.f(ni), *gm = b.f(ni), *gr = b.f(ni);
-  if (!gl || !gm || !gr) return set_error(AWP_ERR_NOMEM, "gradient staging");
+  float *gl = a.E[0], *gm = a.E[1], *gr = a.E[2];
   CU_TRY(awp_launch_adjoint_fold(a, gl, gm, gr, st));
   if (g_lambda) CU_TRY(cudaMemcpyAsync(g_lambda, gl, ni * sizeof(float), cudaMemcpyDeviceToHost, st));
   if (g_mu) CU_TRY(cudaMemcpyAsync(g_mu, gm, ni * sizeof(float), cudaMemcpyDeviceToHost, st));
