@@ -39,6 +39,26 @@ def ricker_derivative(nt: int, dt: float, f0: float, t0: float | None = None) ->
     return ((-2.0 * dadt) * np.exp(-a) - (1.0 - 2.0 * a) * np.exp(-a) * dadt).astype(np.float64)
 
 
+def workload_meta(name: str, nx=None, ny=None, nz=None) -> tuple[dict, str]:
+    """Solver parameters and description of a named benchmark workload
+    (``layered_vk``, ``halfspace``) at its default or given size, without
+    generating its medium."""
+    if name == "layered_vk":
+        nx, ny, nz = nx or 512, ny or 512, nz or 256
+        h, dt, nsub = 50.0, 0.0035, 200
+        params = dict(nx=nx, ny=ny, nz=nz, dh=h, dt=dt, nd=20, arbc=0.92, npc=0, nve=1,
+                      ifault=5, nst=2, read_step=2, socalq=1)
+        return params, (f"anelastic 1-D gradient + von Karman {nx}x{ny}x{nz}, h={h}, dt={dt}, "
+                        f"{nsub} kinematic subfaults")
+    if name == "halfspace":
+        nx, ny, nz = nx or 128, ny or 128, nz or 128
+        h, dt, f0, steps = 100.0, 0.005, 2.0, 500
+        params = dict(nx=nx, ny=ny, nz=nz, dh=h, dt=dt, nd=20, arbc=0.92, npc=0, nve=1,
+                      ifault=1, nst=steps, read_step=steps, socalq=1)
+        return params, f"elastic half-space {nx}x{ny}x{nz}, h={h}, dt={dt}, Mxy Ricker' {f0} Hz"
+    raise ValueError(f"unknown workload {name}")
+
+
 def halfspace(nx=128, ny=128, nz=128, h=100.0, dt=0.005, steps=500, f0=2.0, m0=1e15,
               vp=6000.0, vs=3464.0, rho=2700.0, nd=20, seed=1) -> Scenario:
     media = np.empty((nz, ny, nx, 5), np.float32)

@@ -419,6 +419,19 @@ def run_ours(args, rank, world, dist) -> dict | None:
     return line
 
 
+def reference_config(args) -> dict:
+    """The workload keys of the GPU arm's `config` (the same model and size),
+    from the scenario's parameters without generating its medium."""
+    from awp_b200 import scenarios
+    g = args.grid or (None, None, None)
+    p, desc = scenarios.workload_meta(args.workload, *g)
+    return {"workload": args.workload, "description": desc,
+            "grid": [p["nx"], p["ny"], p["nz"]], "cells": p["nx"] * p["ny"] * p["nz"],
+            "dh": p["dh"], "dt": p["dt"], "ifault": p["ifault"], "nve": p["nve"],
+            "parallelism": "single GPU's workload, timed on the host cores",
+            "l2": "working set ~7 GB >> 126 MB L2, no flush needed", "topography": None}
+
+
 def run_reference(args, rank) -> dict | None:
     """Reference arm: the reference path's CPU restatement on the host cores,
     W warm-up and K timed steps on a bounded window of the same workload."""
@@ -429,7 +442,7 @@ def run_reference(args, rank) -> dict | None:
             "value": cb["value"], "unit": "Gcell-updates/s", "n_gpus": 1,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
             "impl": "reference", "dtype": "f32", "data": "synthetic (seeded)",
-            "config": {"workload": args.workload},
+            "config": reference_config(args),
             "cpu_baseline": cb,
             "e2e": {"value": cb["value"], "unit": "Gcell-updates/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0},
