@@ -238,10 +238,12 @@ int launch_plasticity(awp_ctx* c) {
 
 // Tensor maps over the context's fields for the TMA-pipelined kernels.
 bool build_tma_maps(awp_ctx* c) {
-  int hx, hy, mx, my, ox, oy;
+  int hx, hy, mx, my, ox, oy, jx, jy, kx, ky;
   awp_tma_box(0, &hx, &hy);
   awp_tma_box(1, &mx, &my);
   awp_tma_box(2, &ox, &oy);
+  awp_tma_box(3, &jx, &jy);
+  awp_tma_box(4, &kx, &ky);
   float** f = c->f;
   const int vh[6] = {AWP_XX, AWP_YY, AWP_ZZ, AWP_XY, AWP_XZ, AWP_YZ};
   const int vo[3] = {AWP_U1, AWP_V1, AWP_W1};
@@ -249,7 +251,10 @@ bool build_tma_maps(awp_ctx* c) {
   const int so[12] = {AWP_XX, AWP_YY, AWP_ZZ, AWP_XY, AWP_XZ, AWP_YZ,
                       AWP_R1, AWP_R2, AWP_R3, AWP_R4, AWP_R5, AWP_R6};
   int bad = 0;
-  for (int q = 0; q < 6; ++q) bad |= awp_tma_encode(&c->vel_maps.halo[q], f[vh[q]], c->g, hx, hy);
+  // velocity: each stress field with the halo its differences read
+  const int vbx[6] = {ox, jx, kx, jx, kx, hx}, vby[6] = {oy, jy, ky, jy, ky, hy};
+  for (int q = 0; q < 6; ++q)
+    bad |= awp_tma_encode(&c->vel_maps.halo[q], f[vh[q]], c->g, vbx[q], vby[q]);
   bad |= awp_tma_encode(&c->vel_maps.media[0], f[AWP_D1], c->g, mx, my);
   for (int q = 0; q < 3; ++q) bad |= awp_tma_encode(&c->vel_maps.own[q], f[vo[q]], c->g, ox, oy);
   for (int q = 0; q < 3; ++q) bad |= awp_tma_encode(&c->str_maps.halo[q], f[vo[q]], c->g, hx, hy);

@@ -39,6 +39,13 @@ constexpr int DH_ = 7;                                // halo ring depth (planes
 constexpr int DM_ = 4;                                // media ring depth (planes i, i+1 + 2)
 constexpr int DO_ = 3;                                // own ring depth (plane i + 2)
 constexpr unsigned kSpinLimit = 1u << 26;
+// velocity kernel: each stress field is staged with only the halo its
+// differences read (xx none, yy and xy j, zz and xz k, yz both), one slot of
+// the ring holding the six tiles at 128-byte multiples
+constexpr int VT_XX = 0, VT_YY = 256, VT_ZZ = 640, VT_XY = 960, VT_XZ = 1344, VT_YZ = 1664,
+              VT_SLOT = 2144;
+constexpr int VJ = TZ;  // row stride of the j-halo tiles (32 x 12)
+constexpr int VK = HX;  // row stride of the k-halo tiles (40 x 8) and of yz (40 x 12)
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) {
   return static_cast<unsigned>(__cvta_generic_to_shared(p));
@@ -375,7 +382,7 @@ __global__ void __launch_bounds__(NT, 2)
 // Rings: stress halo tiles (6 fields, planes i-2..i+2), density (planes i,
 // i+1), own velocity tiles (plane i).
 // ===========================================================================
-__global__ void __launch_bounds__(NT, 2)
+__global__ void __launch_bounds__(NT, 3)
     k_velocity_tma(const VelArgs a, const __grid_constant__ TmaMaps tm, const int ichunk,
                    int* err) {
   extern __shared__ __align__(128) float smem[];
@@ -387,8 +394,8 @@ __global__ void __launch_bounds__(NT, 2)
   const int ie = min(ib + ichunk - 1, a.i1);
   const bool active = (k >= a.k0) && (k <= a.k1) && (j <= a.j1);
 
-  Ring rh{smem, nullptr, DH_, 6 * HTILE, ib - 2};
-  Ring rm{rh.buf + DH_ * 6 * HTILE, nullptr, DM_, MTILE, ib};
+  Ring rh{smem, nullptr, DH_, VT_SLOT, ib - 2};
+  Ring rm{rh.buf + DH_ * VT_SLOT, nullptr, DM_, MTILE, ib};
   Ring ro{rm.buf + DM_ * MTILE, nullptr, DO_, 3 * OTILE, ib};
   uint64_t* bars = reinterpret_cast<uint64_t*>(ro.buf + DO_ * 3 * OTILE);
   rh.bar = bars;
@@ -400,9 +407,14 @@ __global__ void __launch_bounds__(NT, 2)
   auto issue_halo = [&](int p) {
     if (p > ie + 2) return;
     uint64_t* b = rh.bar + ish;
-    mbar_expect_tx(b, 6 * HTILE * 4);
+    mbar_expect_tx(b, VT_SLOT * 4);
     float* d = rh.buf + ish * rh.slot_floats;
-    for (int f = 0; f < 6; ++f) tma_load3(d + f * HTILE, &tm.halo[f], b, kb - 4, jb - 2, p);
+    tma_load3(d + VT_XX, &tm.halo[0], b, kb, jb, p);
+    tma_load3(d + VT_YY, &tm.halo[1], b, kb, jb - 2, p);
+    tma_load3(d + VT_ZZ, &tm.halo[2], b, kb - 4, jb, p);
+    tma_load3(d + VT_XY, &tm.halo[3], b, kb, jb - 2, p);
+    tma_load3(d + VT_XZ, &tm.halo[4], b, kb - 4, jb, p);
+    tma_load3(d + VT_YZ, &tm.halo[5], b, kb - 4, jb - 2, p);
     ish = wrap_add(ish, 1, DH_);
   };
   auto issue_media = [&](int p) {
@@ -438,7 +450,12 @@ __global__ void __launch_bounds__(NT, 2)
   const float c1 = a.c1, c2 = a.c2, dth = a.dth;
   const float dcy = LDG(a.dcrjy + min(j, a.j1)), dcz = LDG(a.dcrjz + min(k, a.k1));
   const long long col = (long long)j * Y + k;
-  const int hoff = (ty + 2) * HX + (tx + 4);
+  const int o_xx = VT_XX + ty * TZ + tx;             // no halo
+  const int o_yy = VT_YY + (ty + 2) * VJ + tx;       // j halo
+  const int o_zz = VT_ZZ + ty * VK + tx + 4;         // k halo
+  const int o_xy = VT_XY + (ty + 2) * VJ + tx;
+  const int o_xz = VT_XZ + ty * VK + tx + 4;
+  const int o_yz = VT_YZ + (ty + 2) * VK + tx + 4;   // both
   const int moff = (ty + 1) * MX + (tx + 4);
   const int ooff = ty * TZ + tx;
   bool ok = true, aborted = false;
@@ -471,21 +488,19 @@ __global__ void __launch_bounds__(NT, 2)
               sh4 = wrap_add(sh, 4, DH_), sm1 = wrap_add(sm, 1, DM_);
 
     // halo fields: 0 xx, 1 yy, 2 zz, 3 xy, 4 xz, 5 yz
-    const float* Hm2 = rh.buf + sh * rh.slot_floats + hoff;
-    const float* Hm1 = rh.buf + sh1 * rh.slot_floats + hoff;
-    const float* H0 = rh.buf + sh2 * rh.slot_floats + hoff;
-    const float* Hp1 = rh.buf + sh3 * rh.slot_floats + hoff;
-    const float* Hp2 = rh.buf + sh4 * rh.slot_floats + hoff;
-    const float xx_m2 = Hm2[0], xx_m1 = Hm1[0], xx_0 = H0[0], xx_p1 = Hp1[0];
-    const float xy_m1 = Hm1[3 * HTILE], xy_0 = H0[3 * HTILE], xy_p1 = Hp1[3 * HTILE],
-                xy_p2 = Hp2[3 * HTILE];
-    const float xz_m1 = Hm1[4 * HTILE], xz_0 = H0[4 * HTILE], xz_p1 = Hp1[4 * HTILE],
-                xz_p2 = Hp2[4 * HTILE];
-    const float* YY = H0 + HTILE;
-    const float* ZZ = H0 + 2 * HTILE;
-    const float* XY = H0 + 3 * HTILE;
-    const float* XZ = H0 + 4 * HTILE;
-    const float* YZ = H0 + 5 * HTILE;
+    const float* Hm2 = rh.buf + sh * rh.slot_floats;
+    const float* Hm1 = rh.buf + sh1 * rh.slot_floats;
+    const float* H0 = rh.buf + sh2 * rh.slot_floats;
+    const float* Hp1 = rh.buf + sh3 * rh.slot_floats;
+    const float* Hp2 = rh.buf + sh4 * rh.slot_floats;
+    const float xx_m2 = Hm2[o_xx], xx_m1 = Hm1[o_xx], xx_0 = H0[o_xx], xx_p1 = Hp1[o_xx];
+    const float xy_m1 = Hm1[o_xy], xy_0 = H0[o_xy], xy_p1 = Hp1[o_xy], xy_p2 = Hp2[o_xy];
+    const float xz_m1 = Hm1[o_xz], xz_0 = H0[o_xz], xz_p1 = Hp1[o_xz], xz_p2 = Hp2[o_xz];
+    const float* YY = H0 + o_yy;
+    const float* ZZ = H0 + o_zz;
+    const float* XY = H0 + o_xy;
+    const float* XZ = H0 + o_xz;
+    const float* YZ = H0 + o_yz;
     const float yz_0 = YZ[0];
 
     const float* Dc = rm.buf + sm * rm.slot_floats + moff;
@@ -500,13 +515,13 @@ __global__ void __launch_bounds__(NT, 2)
 
     const float* O = ro.buf + wo.slot * ro.slot_floats + ooff;
     const float u = awp_vel_update(O[0], fd1, c1, c2, xx_0 - xx_m1, xx_p1 - xx_m2,
-                                   xy_0 - XY[-HX], XY[HX] - XY[-2 * HX], xz_0 - XZ[-1],
+                                   xy_0 - XY[-VJ], XY[VJ] - XY[-2 * VJ], xz_0 - XZ[-1],
                                    XZ[1] - XZ[-2], dcrj);
     const float v = awp_vel_update(O[OTILE], fd2, c1, c2, xy_p1 - xy_0, xy_p2 - xy_m1,
-                                   YY[HX] - YY[0], YY[2 * HX] - YY[-HX], yz_0 - YZ[-1],
+                                   YY[VJ] - YY[0], YY[2 * VJ] - YY[-VJ], yz_0 - YZ[-1],
                                    YZ[1] - YZ[-2], dcrj);
     const float w = awp_vel_update(O[2 * OTILE], fd3, c1, c2, xz_p1 - xz_0, xz_p2 - xz_m1,
-                                   yz_0 - YZ[-HX], YZ[HX] - YZ[-2 * HX], ZZ[1] - ZZ[0],
+                                   yz_0 - YZ[-VK], YZ[VK] - YZ[-2 * VK], ZZ[1] - ZZ[0],
                                    ZZ[2] - ZZ[-1], dcrj);
     if (active) {
       const long long o = (long long)i * S + col;
@@ -543,7 +558,7 @@ size_t stress_smem(bool elastic) {
          sizeof(uint64_t) * (DH_ + DM_ + DO_);
 }
 size_t velocity_smem() {
-  return sizeof(float) * ((size_t)DH_ * 6 * HTILE + (size_t)DM_ * MTILE + (size_t)DO_ * 3 * OTILE) +
+  return sizeof(float) * ((size_t)DH_ * VT_SLOT + (size_t)DM_ * MTILE + (size_t)DO_ * 3 * OTILE) +
          sizeof(uint64_t) * (DH_ + DM_ + DO_);
 }
 
@@ -582,6 +597,8 @@ int awp_tma_box(int group, int* bx, int* by) {
     case 0: *bx = HX; *by = HY; return 0;   // halo
     case 1: *bx = MX; *by = MY; return 0;   // media
     case 2: *bx = TZ; *by = TY; return 0;   // own
+    case 3: *bx = TZ; *by = HY; return 0;   // j halo only
+    case 4: *bx = HX; *by = TY; return 0;   // k halo only
   }
   return 1;
 }

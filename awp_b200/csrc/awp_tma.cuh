@@ -11,7 +11,8 @@
 //   halo  (40 x 12 box): fields read with their j/k neighbours
 //   media (36 x  9 box): fields read at (j|j-1, k|k-1) of planes i and i+1
 //   own   (32 x  8 box): fields read and written at the cell itself
-// velocity kernel: halo = xx yy zz xy xz yz, media = d1, own = u1 v1 w1
+// velocity kernel: halo = xx (own box), yy, xy (32 x 12: j halo), zz, xz
+//                  (40 x 8: k halo), yz (40 x 12); media = d1; own = u1 v1 w1
 // stress kernel  : halo = u1 v1 w1, media = lam mu qp qs, own = xx..yz r1..r6
 struct TmaMaps {
   CUtensorMap halo[6];
@@ -19,7 +20,8 @@ struct TmaMaps {
   CUtensorMap own[12];
 };
 
-// Encode one 3-D tensor map over a padded field; group 0 halo, 1 media, 2 own.
+// Encode one 3-D tensor map over a padded field; box groups: 0 halo (40 x 12),
+// 1 media (36 x 9), 2 own (32 x 8), 3 j halo (32 x 12), 4 k halo (40 x 8).
 int awp_tma_box(int group, int* box_x, int* box_y);
 int awp_tma_encode(CUtensorMap* map, const float* base, const AwpGeom& g, int box_x, int box_y);
 
