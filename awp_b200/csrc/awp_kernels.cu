@@ -28,7 +28,7 @@ namespace {
 // 32 k x 8 j for every kernel; the chunk of x planes and the kernel family vary.
 int g_ichunk = 32;
 // context API kernel family per half-step: TMA-pipelined (1) or read-only path (0)
-int g_tma_vel = 0;
+int g_tma_vel = 1;
 int g_tma_str = 1;
 
 // ===========================================================================

@@ -79,13 +79,33 @@ def autotune_batch(batch, steps: int = 3, timer=None) -> dict:
         batch.synchronize()
         ms = timer(lambda: batch.step(steps))
         table.append({"mode": 0, "ty": ty, "ichunk": ich, "ms_per_step": ms / steps})
-    batch.set_mode(1)
-    batch.step(1)
-    batch.synchronize()
-    ms = timer(lambda: batch.step(steps))
-    table.append({"mode": 1, "ty": None, "ichunk": None, "ms_per_step": ms / steps})
+    # mode 1 captures each instance's launches with the process-wide kernel
+    # families and x chunk in force at capture time: try those too, then put
+    # the process-wide values back (the captured graph keeps its own)
+    lib = batch.lib
+    saved = get_tuning(lib)
+    for tv, ich in itertools.product((1, 0), (16, 32, 64)):
+        set_tuning(lib, "tma_vel", tv)
+        set_tuning(lib, "ichunk", ich)
+        batch.set_mode(0)
+        batch.set_mode(1)  # recapture
+        batch.step(1)
+        batch.synchronize()
+        ms = timer(lambda: batch.step(steps))
+        table.append({"mode": 1, "ty": None, "ichunk": ich, "tma_vel": tv,
+                      "ms_per_step": ms / steps})
     best = min(table, key=lambda r: r["ms_per_step"])
-    batch.set_mode(best["mode"])
-    if best["mode"] == 0:
+    if best["mode"] == 1:
+        set_tuning(lib, "tma_vel", best["tma_vel"])
+        set_tuning(lib, "ichunk", best["ichunk"])
+        batch.set_mode(0)
+        batch.set_mode(1)
+        batch.step(1)  # capture with the chosen values
+        batch.synchronize()
+    else:
+        batch.set_mode(0)
         batch.set_shape(best["ty"], best["ichunk"])
-    return {"chosen": {k: best[k] for k in ("mode", "ty", "ichunk")}, "table": table}
+    for k, v in saved.items():
+        set_tuning(lib, k, v)
+    return {"chosen": {k: best.get(k) for k in ("mode", "ty", "ichunk", "tma_vel")},
+            "table": table}

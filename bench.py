@@ -583,6 +583,10 @@ def run_adjoint(args) -> dict:
     # the workspace (snapshots, velocity store) is allocated once per solver
     # and kept for later gradients; its allocation is timed on its own
     ms_alloc, _ = timed(lambda: adjoint.adjoint_reserve(s, steps))
+    # one untimed gradient: the first pass over a freshly allocated workspace
+    # of ~170 GB runs up to ~50 % slower than the following ones
+    s.reset()
+    adjoint.misfit_gradient(s, steps, xyz, comp, d_obs)
     sampler = ClockSampler(torch.cuda.current_device())
     sampler.start()
     # three forward runs and three gradients, alternating; the medians are
