@@ -1364,7 +1364,15 @@ int batch_capture_instances(awp_batch* b) {
   long long l0 = 0;
   for (awp_ctx* c : b->ctx) l0 += c->launches;
   cudaError_t ce = cudaEventRecord(b->fork, b->stream);
-  for (size_t q = 0; q < b->ctx.size() && !st && ce == cudaSuccess; ++q) {
+  // branches in decreasing size: the largest instances start first, so the
+  // small ones fill the tail (capture order is the graph's launch order)
+  std::vector<size_t> ord(b->ctx.size());
+  for (size_t q = 0; q < ord.size(); ++q) ord[q] = q;
+  std::stable_sort(ord.begin(), ord.end(), [&](size_t x, size_t y) {
+    return b->ctx[x]->g.cells_pad() > b->ctx[y]->g.cells_pad();
+  });
+  for (size_t n = 0; n < ord.size() && !st && ce == cudaSuccess; ++n) {
+    const size_t q = ord[n];
     awp_ctx* c = b->ctx[q];
     cudaStream_t saved = c->stream;
     const bool prof = c->profile;
