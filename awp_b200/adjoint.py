@@ -60,6 +60,28 @@ def misfit_gradient(solver, nsteps: int, rec_xyz, rec_comp, d_obs, nsnap: int = 
     return J.value, seis, g[0], g[1], g[2]
 
 
+def misfit_gradient_shots(solver, nsteps: int, shots, nsnap: int = 0):
+    """Multi-shot misfit on one model: J = sum over shots of each shot's
+    1/2 sum (seis - d_obs)^2 and its gradient (the sum of the shots'
+    gradients).  `shots` is a sequence of (src_pos, src_data, rec_xyz,
+    rec_comp, d_obs), each run from a zero wavefield with its own sources;
+    the solver keeps one workspace for all of them.  Returns (J, g_lambda,
+    g_mu, g_rho) with float64 sums of the float32 per-shot gradients."""
+    J = 0.0
+    g = None
+    for src_pos, src_data, rec_xyz, rec_comp, d_obs in shots:
+        solver.upload_sources(src_pos, src_data)
+        solver.reset()
+        Js, _, gl, gm, gr = misfit_gradient(solver, nsteps, rec_xyz, rec_comp, d_obs, nsnap)
+        J += Js
+        if g is None:
+            g = [x.astype(np.float64) for x in (gl, gm, gr)]
+        else:
+            for acc, x in zip(g, (gl, gm, gr)):
+                acc += x
+    return J, g[0], g[1], g[2]
+
+
 def adjoint_plan(solver, nsteps: int, nsnap: int = 0) -> dict:
     """The forward-state storage ``misfit_gradient`` would use now: steps whose
     velocities are kept, the recomputed segment length, the snapshot count and

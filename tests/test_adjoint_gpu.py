@@ -162,3 +162,51 @@ def test_torch_autograd_function():
     assert np.array_equal(t[1].grad.numpy(), gm)
     assert np.array_equal(t[2].grad.numpy(), gr)
     s.close()
+
+
+def test_multishot_gradient_is_the_sum_of_the_shots():
+    steps = 24
+    scn, s, m, xyz, comp, _ = setup_case(True, seed=41, steps=steps)
+    rng = np.random.default_rng(42)
+    shots = []
+    for q in range(2):
+        pos = scn.src_pos.copy()
+        pos[0, 0] = min(max(int(pos[0, 0]) + (3 if q else -3), 2), scn.params["nx"] - 2)
+        data = (scn.src_data * (1.0 + 0.5 * q)).astype(np.float32)
+        # observed data of the perturbed model for this shot
+        s.upload_sources(pos, data)
+        pert = [(x * (1 + 0.03 * rng.standard_normal(x.shape))).astype(np.float32) for x in m]
+        s.set_moduli(*pert)
+        s.reset()
+        d_obs = adjoint.seismograms(s, steps, xyz, comp)
+        shots.append((pos, data, xyz, comp, d_obs))
+    s.set_moduli(*m)
+    J, gl, gm, gr = adjoint.misfit_gradient_shots(s, steps, shots)
+    Jsum, gsum = 0.0, [np.zeros(x.shape) for x in m]
+    for pos, data, rxyz, rcomp, d_obs in shots:
+        s.upload_sources(pos, data)
+        s.set_moduli(*m)
+        s.reset()
+        Js, _, a, b, c = adjoint.misfit_gradient(s, steps, rxyz, rcomp, d_obs)
+        Jsum += Js
+        for acc, x in zip(gsum, (a, b, c)):
+            acc += x
+    assert J == Jsum
+    for x, y in zip((gl, gm, gr), gsum):
+        assert np.array_equal(x, y)
+    # the summed gradient against central differences of the summed misfit
+    dm = tuple((x * rng.standard_normal(x.shape)).astype(np.float64) for x in m)
+    adj = float(np.sum(gl * dm[0]) + np.sum(gm * dm[1]) + np.sum(gr * dm[2]))
+    eps = 1e-3
+
+    def J_all(mm):
+        tot = 0.0
+        for pos, data, rxyz, rcomp, d_obs in shots:
+            s.upload_sources(pos, data)
+            tot += J_at(s, mm, steps, rxyz, rcomp, d_obs)
+        return tot
+    mp = tuple((x + eps * y).astype(np.float32) for x, y in zip(m, dm))
+    mm_ = tuple((x - eps * y).astype(np.float32) for x, y in zip(m, dm))
+    fd = (J_all(mp) - J_all(mm_)) / (2 * eps)
+    assert abs(adj - fd) <= 1e-3 * abs(adj), (adj, fd)
+    s.close()
