@@ -121,6 +121,7 @@ def load() -> ctypes.CDLL:
     _sig(lib, "awp_batch_set_graph", c_int, [_P, c_int])
     _sig(lib, "awp_batch_set_mode", c_int, [_P, c_int])
     _sig(lib, "awp_batch_get_mode", c_int, [_P])
+    _sig(lib, "awp_batch_set_branches", c_int, [_P, c_int])
     _sig(lib, "awp_batch_info", c_int, [_P, POINTER(c_longlong)])
     _sig(lib, "awp_receivers_init", c_int, [_P, c_char_p, c_longlong])
     _sig(lib, "awp_receivers_count", c_int, [_P, _I])

@@ -1314,6 +1314,7 @@ struct awp_batch {
   BatchLaunch L{};
   int ty = 8, ichunk = 16;
   int mode = 0;  // 0: persistent tile-queue launches; 1: graph of each instance's own launches
+  int branches = 0;  // mode 1: parallel graph branches (0: one per instance)
   std::vector<cudaStream_t> cs;   // mode 1: one capture stream per instance
   std::vector<cudaEvent_t> join;  // mode 1: branch joins
   cudaEvent_t fork = nullptr;
@@ -1371,14 +1372,20 @@ int batch_capture_instances(awp_batch* b) {
   std::stable_sort(ord.begin(), ord.end(), [&](size_t x, size_t y) {
     return b->ctx[x]->g.cells_pad() > b->ctx[y]->g.cells_pad();
   });
+  // instances dealt round-robin (largest first) onto nb branches
+  const size_t nb = b->branches > 0 ? std::min((size_t)b->branches, ord.size()) : ord.size();
+  std::vector<char> used(nb, 0);
   for (size_t n = 0; n < ord.size() && !st && ce == cudaSuccess; ++n) {
-    const size_t q = ord[n];
+    const size_t q = ord[n], br = n % nb;
     awp_ctx* c = b->ctx[q];
     cudaStream_t saved = c->stream;
     const bool prof = c->profile;
-    c->stream = b->cs[q];
+    c->stream = b->cs[br];
     c->profile = false;
-    ce = cudaStreamWaitEvent(b->cs[q], b->fork, 0);
+    if (!used[br]) {
+      ce = cudaStreamWaitEvent(b->cs[br], b->fork, 0);
+      used[br] = 1;
+    }
     if (ce == cudaSuccess) st = phase_velocity(c);
     if (!st && ce == cudaSuccess) st = phase_stress(c);
     if (!st && ce == cudaSuccess && c->ncell > 0) {
@@ -1393,10 +1400,13 @@ int batch_capture_instances(awp_batch* b) {
       }
     }
     if (!st && ce == cudaSuccess) st = phase_fstr(c);
-    if (!st && ce == cudaSuccess) ce = cudaEventRecord(b->join[q], b->cs[q]);
-    if (!st && ce == cudaSuccess) ce = cudaStreamWaitEvent(b->stream, b->join[q], 0);
     c->stream = saved;
     c->profile = prof;
+  }
+  for (size_t br = 0; br < nb && !st && ce == cudaSuccess; ++br) {
+    if (!used[br]) continue;
+    ce = cudaEventRecord(b->join[br], b->cs[br]);
+    if (ce == cudaSuccess) ce = cudaStreamWaitEvent(b->stream, b->join[br], 0);
   }
   if (!st && ce == cudaSuccess) {
     ce = awp_launch_step_advance(b->d_step, b->stream);
@@ -1590,6 +1600,16 @@ int awp_batch_set_mode(awp_batch* b, int mode) {
 }
 
 int awp_batch_get_mode(const awp_batch* b) { return b ? b->mode : -1; }
+
+int awp_batch_set_branches(awp_batch* b, int branches) {
+  if (!b) return set_error(AWP_ERR_ARG, "null batch");
+  if (branches < 0) return set_error(AWP_ERR_ARG, "branches >= 0");
+  if (branches != b->branches) {
+    b->branches = branches;
+    b->dirty = true;
+  }
+  return AWP_OK;
+}
 
 int awp_batch_get_shape(const awp_batch* b, int* ty, int* ichunk) {
   if (!b || !ty || !ichunk) return set_error(AWP_ERR_ARG, "null argument");

@@ -319,6 +319,12 @@ class Batch:
     def mode(self) -> int:
         return self.lib.awp_batch_get_mode(self.batch)
 
+    def set_branches(self, branches: int) -> None:
+        """Mode 1: parallel graph branches the instances are dealt onto
+        (0: one per instance)."""
+        check(self.lib.awp_batch_set_branches(self.batch, int(branches)),
+              "awp_batch_set_branches")
+
     def info(self) -> dict:
         v = (c_longlong * 6)()
         check(self.lib.awp_batch_info(self.batch, v), "awp_batch_info")

@@ -98,6 +98,18 @@ def autotune_batch(batch, steps: int = 3, timer=None) -> dict:
     if best["mode"] == 1:
         set_tuning(lib, "tma_vel", best["tma_vel"])
         set_tuning(lib, "ichunk", best["ichunk"])
+        best["branches"] = 0
+        for nb in (32, 16, 8):  # fewer, longer branches
+            batch.set_branches(nb)
+            batch.step(1)
+            batch.synchronize()
+            ms = timer(lambda: batch.step(steps))
+            row = {"mode": 1, "ty": None, "ichunk": best["ichunk"], "tma_vel": best["tma_vel"],
+                   "branches": nb, "ms_per_step": ms / steps}
+            table.append(row)
+            if row["ms_per_step"] < best["ms_per_step"]:
+                best = row
+        batch.set_branches(best["branches"])
         batch.set_mode(0)
         batch.set_mode(1)
         batch.step(1)  # capture with the chosen values
@@ -107,5 +119,5 @@ def autotune_batch(batch, steps: int = 3, timer=None) -> dict:
         batch.set_shape(best["ty"], best["ichunk"])
     for k, v in saved.items():
         set_tuning(lib, k, v)
-    return {"chosen": {k: best.get(k) for k in ("mode", "ty", "ichunk", "tma_vel")},
+    return {"chosen": {k: best.get(k) for k in ("mode", "ty", "ichunk", "tma_vel", "branches")},
             "table": table}

@@ -227,6 +227,10 @@ int awp_batch_set_graph(awp_batch* batch, int use_graph);
  * images), the step counter advanced after the join.  Same results. */
 int awp_batch_set_mode(awp_batch* batch, int mode);
 int awp_batch_get_mode(const awp_batch* batch);
+/* Mode 1: the instances' launches are dealt, largest first, round-robin onto
+ * `branches` parallel graph branches (0, the default: one branch per
+ * instance). */
+int awp_batch_set_branches(awp_batch* batch, int branches);
 /* info = instances, interior cells, velocity tiles, stress tiles, persistent
  * CTAs of the velocity and stress launches. */
 int awp_batch_info(awp_batch* batch, long long info[6]);
