@@ -67,6 +67,9 @@ def misfit_gradient_shots(solver, nsteps: int, shots, nsnap: int = 0):
     rec_comp, d_obs), each run from a zero wavefield with its own sources;
     the solver keeps one workspace for all of them.  Returns (J, g_lambda,
     g_mu, g_rho) with float64 sums of the float32 per-shot gradients."""
+    shots = list(shots)
+    if not shots:
+        raise ValueError("shots is empty")
     J = 0.0
     g = None
     for src_pos, src_data, rec_xyz, rec_comp, d_obs in shots:

@@ -1014,8 +1014,11 @@ int awp_synchronize(awp_ctx* c) {
   CU_TRY(cudaStreamSynchronize(c->stream));
   int err = 0;
   CU_TRY(cudaMemcpy(&err, c->d_err, sizeof(int), cudaMemcpyDeviceToHost));
-  if (err)
+  if (err) {
+    // reported once: the word is cleared so that later steps report afresh
+    CU_TRY(cudaMemset(c->d_err, 0, sizeof(int)));
     return set_error(AWP_ERR_CUDA, "a TMA pipeline wait ran out of its iteration limit");
+  }
   return AWP_OK;
 }
 

@@ -19,6 +19,7 @@
 
 #include "awp_kernels.cuh"
 #include "awp_stencil.cuh"
+#include "awp_tma.cuh"
 
 #define LDG(p) __ldg(p)
 
@@ -1001,6 +1002,7 @@ cudaError_t awp_launch_stress(const StrArgs& a, bool elastic, cudaStream_t st) {
 
 int awp_tuning_set(const char* key, int value) {
   if (!strcmp(key, "ichunk") && value >= 4 && value <= 1024) { g_ichunk = value; return 0; }
+  if (!strcmp(key, "spin_limit")) return awp_tma_set_spin_limit(value);
   if (value == 0 || value == 1) {
     if (!strcmp(key, "tma")) { g_tma_vel = g_tma_str = value; return 0; }  // both half-steps
     if (!strcmp(key, "tma_vel")) { g_tma_vel = value; return 0; }
@@ -1014,6 +1016,7 @@ int awp_tuning_get(const char* key) {
   if (!strcmp(key, "tma")) return g_tma_vel == g_tma_str ? g_tma_str : -1;
   if (!strcmp(key, "tma_vel")) return g_tma_vel;
   if (!strcmp(key, "tma_str")) return g_tma_str;
+  if (!strcmp(key, "spin_limit")) return (int)awp_tma_get_spin_limit();
   return -1;
 }
 

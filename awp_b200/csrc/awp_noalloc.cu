@@ -68,6 +68,9 @@ extern "C" int awp_check_finite_noalloc(const float* const* fields, int nfields,
   if (!fields || !ok || n < 0) return fail(AWP_ERR_ARG, "null argument or negative size");
   if (nfields < 1 || nfields > AWP_NOALLOC_MAX_FIELDS)
     return fail(AWP_ERR_ARG, "nfields must be 1..AWP_NOALLOC_MAX_FIELDS (32)");
+  // every argument is checked before any work is queued on the stream
+  for (int f = 0; f < nfields; ++f)
+    if (!fields[f]) return fail(AWP_ERR_ARG, "null field pointer");
   unsigned int* scratch = nullptr;
   int st = scratch_on_current_device(&scratch);
   if (st) return st;
@@ -76,7 +79,6 @@ extern "C" int awp_check_finite_noalloc(const float* const* fields, int nfields,
   cudaError_t e = cudaMemsetAsync(scratch, 0, sizeof(unsigned int) * nfields, s);
   if (e != cudaSuccess) return fail(AWP_ERR_CUDA, "cudaMemsetAsync", e);
   for (int f = 0; f < nfields; ++f) {
-    if (!fields[f]) return fail(AWP_ERR_ARG, "null field pointer");
     e = awp_launch_nonfinite(fields[f], n, scratch + f, s);
     if (e != cudaSuccess) return fail(AWP_ERR_CUDA, "k_nonfinite launch", e);
   }

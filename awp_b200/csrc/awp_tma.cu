@@ -38,6 +38,9 @@ constexpr int OTILE = TZ * TY;                        // own tile (floats)
 constexpr int DH_ = 7;                                // halo ring depth (planes i-2..i+2 + 2)
 constexpr int DM_ = 4;                                // media ring depth (planes i, i+1 + 2)
 constexpr int DO_ = 3;                                // own ring depth (plane i + 2)
+// Poll limit of the pipeline waits: the default, and the one the drain of an
+// aborted march always uses (copies already issued must land before the CTA
+// releases its shared memory, whatever limit the march itself ran with).
 constexpr unsigned kSpinLimit = 1u << 26;
 // velocity kernel: each stress field is staged with only the halo its
 // differences read (xx none, yy and xy j, zz and xz k, yz both), one slot of
@@ -70,8 +73,9 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
   return ok != 0;
 }
 // bounded wait: false when the limit ran out
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
-  for (unsigned n = 0; n < kSpinLimit; ++n)
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity,
+                                          unsigned limit = kSpinLimit) {
+  for (unsigned n = 0; n < limit; ++n)
     if (mbar_try_wait(bar, parity)) return true;
   return false;
 }
@@ -119,7 +123,7 @@ __device__ __forceinline__ int wrap_add(int s, int d, int depth) {
 template <bool ELASTIC>
 __global__ void __launch_bounds__(NT, 2)
     k_stress_tma(const StrArgs a, const __grid_constant__ TmaMaps tm, const int ichunk,
-                 int* err) {
+                 int* err, const unsigned spin) {
   constexpr int NM = ELASTIC ? 2 : 4;   // lam, mu (, qp, qs)
   constexpr int NO = ELASTIC ? 6 : 12;  // xx..yz (, r1..r6)
   extern __shared__ __align__(128) float smem[];
@@ -219,12 +223,12 @@ __global__ void __launch_bounds__(NT, 2)
   for (int i = ib; i <= ie; ++i) {
     // ---- wait for the planes this step reads for the first time ------------
     if (i == ib) {
-      for (int q = 0; q < 4 && ok; ++q) ok = mbar_wait(rh.bar + q, 0u);  // planes ib-2..ib+1
-      if (ok) ok = mbar_wait(rm.bar, 0u);                                  // plane ib
+      for (int q = 0; q < 4 && ok; ++q) ok = mbar_wait(rh.bar + q, 0u, spin);  // ib-2..ib+1
+      if (ok) ok = mbar_wait(rm.bar, 0u, spin);                                  // plane ib
     }
-    if (ok) ok = mbar_wait(rh.bar + wh.slot, wh.phase);
-    if (ok) ok = mbar_wait(rm.bar + wm.slot, wm.phase);
-    if (ok) ok = mbar_wait(ro.bar + wo.slot, wo.phase);
+    if (ok) ok = mbar_wait(rh.bar + wh.slot, wh.phase, spin);
+    if (ok) ok = mbar_wait(rm.bar + wm.slot, wm.phase, spin);
+    if (ok) ok = mbar_wait(ro.bar + wo.slot, wo.phase, spin);
     // one barrier per plane: it also tells the producer that every thread is
     // done with the previous step's oldest planes, whose slots it refills
     if (__syncthreads_or(!ok)) {
@@ -384,7 +388,7 @@ __global__ void __launch_bounds__(NT, 2)
 // ===========================================================================
 __global__ void __launch_bounds__(NT, 3)
     k_velocity_tma(const VelArgs a, const __grid_constant__ TmaMaps tm, const int ichunk,
-                   int* err) {
+                   int* err, const unsigned spin) {
   extern __shared__ __align__(128) float smem[];
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TZ + tx;
   const int kb = AWP_ALIGN + blockIdx.x * TZ;
@@ -467,12 +471,12 @@ __global__ void __launch_bounds__(NT, 3)
   for (int i = ib; i <= ie; ++i) {
     // ---- wait for the planes this step reads for the first time ------------
     if (i == ib) {
-      for (int q = 0; q < 4 && ok; ++q) ok = mbar_wait(rh.bar + q, 0u);  // planes ib-2..ib+1
-      if (ok) ok = mbar_wait(rm.bar, 0u);                                  // plane ib
+      for (int q = 0; q < 4 && ok; ++q) ok = mbar_wait(rh.bar + q, 0u, spin);  // ib-2..ib+1
+      if (ok) ok = mbar_wait(rm.bar, 0u, spin);                                  // plane ib
     }
-    if (ok) ok = mbar_wait(rh.bar + wh.slot, wh.phase);
-    if (ok) ok = mbar_wait(rm.bar + wm.slot, wm.phase);
-    if (ok) ok = mbar_wait(ro.bar + wo.slot, wo.phase);
+    if (ok) ok = mbar_wait(rh.bar + wh.slot, wh.phase, spin);
+    if (ok) ok = mbar_wait(rm.bar + wm.slot, wm.phase, spin);
+    if (ok) ok = mbar_wait(ro.bar + wo.slot, wo.phase, spin);
     // one barrier per plane: it also tells the producer that every thread is
     // done with the previous step's oldest planes, whose slots it refills
     if (__syncthreads_or(!ok)) {
@@ -551,6 +555,9 @@ __global__ void __launch_bounds__(NT, 3)
 
 inline unsigned cdiv_u(long long a, long long b) { return (unsigned)((a + b - 1) / b); }
 
+// Poll limit the next launches give their pipeline waits (process-wide).
+unsigned g_spin_limit = kSpinLimit;
+
 size_t stress_smem(bool elastic) {
   const int nm = elastic ? 2 : 4, no = elastic ? 6 : 12;
   return sizeof(float) * ((size_t)DH_ * 3 * HTILE + (size_t)DM_ * nm * MTILE +
@@ -615,12 +622,12 @@ cudaError_t awp_launch_stress_tma(const StrArgs& a, const TmaMaps& tm, bool elas
     e = cudaFuncSetAttribute(k_stress_tma<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)sm);
     if (e != cudaSuccess) return e;
-    k_stress_tma<true><<<grid, block, sm, st>>>(a, tm, ichunk, err);
+    k_stress_tma<true><<<grid, block, sm, st>>>(a, tm, ichunk, err, g_spin_limit);
   } else {
     e = cudaFuncSetAttribute(k_stress_tma<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)sm);
     if (e != cudaSuccess) return e;
-    k_stress_tma<false><<<grid, block, sm, st>>>(a, tm, ichunk, err);
+    k_stress_tma<false><<<grid, block, sm, st>>>(a, tm, ichunk, err, g_spin_limit);
   }
   return cudaGetLastError();
 }
@@ -635,6 +642,14 @@ cudaError_t awp_launch_velocity_tma(const VelArgs& a, const TmaMaps& tm, int ich
   cudaError_t e =
       cudaFuncSetAttribute(k_velocity_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
   if (e != cudaSuccess) return e;
-  k_velocity_tma<<<grid, block, sm, st>>>(a, tm, ichunk, err);
+  k_velocity_tma<<<grid, block, sm, st>>>(a, tm, ichunk, err, g_spin_limit);
   return cudaGetLastError();
 }
+
+int awp_tma_set_spin_limit(long long polls) {
+  if (polls < 0 || polls > (1ll << 30)) return 1;
+  g_spin_limit = (unsigned)polls;
+  return 0;
+}
+
+long long awp_tma_get_spin_limit() { return g_spin_limit; }

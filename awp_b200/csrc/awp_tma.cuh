@@ -29,3 +29,9 @@ cudaError_t awp_launch_stress_tma(const StrArgs& a, const TmaMaps& tm, bool elas
                                   int* err, cudaStream_t st);
 cudaError_t awp_launch_velocity_tma(const VelArgs& a, const TmaMaps& tm, int ichunk, int* err,
                                     cudaStream_t st);
+// Poll limit of the TMA kernels' pipeline waits (0 .. 2^30; default 2^26; 0
+// makes every wait give up at once, which exercises the failure path).  A wait
+// that runs out sets the context's error word; the CTA then drains its issued
+// copies with the default limit and leaves.  Returns 0 or 1 (refused).
+int awp_tma_set_spin_limit(long long polls);
+long long awp_tma_get_spin_limit();

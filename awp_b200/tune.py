@@ -84,6 +84,8 @@ def autotune_batch(batch, steps: int = 3, timer=None) -> dict:
     # the process-wide values back (the captured graph keeps its own)
     lib = batch.lib
     saved = get_tuning(lib)
+    # the mode-1 rows below are one branch per instance (branches = 0)
+    batch.set_branches(0)
     for tv, ich in itertools.product((1, 0), (16, 32, 64)):
         set_tuning(lib, "tma_vel", tv)
         set_tuning(lib, "ichunk", ich)

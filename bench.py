@@ -122,36 +122,48 @@ def build_workload(name: str, grid=None):
     raise SystemExit(f"unknown workload {name}")
 
 
-def cpu_baseline(workload: str, steps: int | None = None, warmup: int = 1,
-                 target_s: float = 12.0) -> dict:
-    """FP32 OpenMP restatement of the reference kernels (oracle/) on the host cores,
-    on a bounded window of the same workload."""
-    from awp_b200 import scenarios
+def host_cpu() -> dict:
+    """The host's processor as lscpu reports it (model, sockets, cores, threads)."""
+    info = {"nproc": os.cpu_count()}
+    try:
+        out = subprocess.run(["lscpu"], capture_output=True, text=True, timeout=10).stdout
+        for ln in out.splitlines():
+            k, _, v = ln.partition(":")
+            k = k.strip()
+            if k in ("Model name", "Socket(s)", "Core(s) per socket", "Thread(s) per core",
+                     "CPU max MHz"):
+                info[k] = v.strip()
+    except Exception:
+        pass
+    return info
+
+
+def cpu_baseline(workload: str, steps: int = 10, warmup: int = 3, grid=None) -> dict:
+    """FP32 OpenMP restatement of the reference kernels (oracle/) on every host
+    core, on the workload's full grid: `warmup` untimed steps, then `steps`
+    timed ones.  FP32 subnormals are flushed to zero on the stepping threads,
+    as the reference's -use_fast_math CUDA build flushes them, so the timing
+    does not depend on how far the wavefield has spread."""
     from oracle import oracle as orc
     from oracle import refbind
-    if workload == "layered_vk":
-        scn = scenarios.layered_vk(nx=160, ny=160, nz=96, nsub=40, steps=20)
-        sample = "160x160x96 window of the layered_vk model (same generator), FP32"
-    else:
-        scn = scenarios.halfspace(nx=128, ny=128, nz=128, steps=20)
-        sample = "128^3 half-space, FP32"
+    scn, _ = build_workload(workload, grid)
+    p = scn.params
     setup = refbind.model_setup(scn)
     ncores = os.cpu_count() or 1
-    sim = orc.OracleSim(scn, setup, precision=32, nthreads=ncores)
+    sim = orc.OracleSim(scn, setup, precision=32, nthreads=ncores, flush_denormals=True)
+    del setup
     sim.step(max(1, warmup))
-    if steps is None:
-        t0 = time.perf_counter()
-        sim.step(2)
-        per = (time.perf_counter() - t0) / 2
-        steps = max(3, min(200, int(target_s / max(per, 1e-6))))
     t0 = time.perf_counter()
     sim.step(steps)
     dt = time.perf_counter() - t0
-    cells = scn.params["nx"] * scn.params["ny"] * scn.params["nz"]
+    cells = p["nx"] * p["ny"] * p["nz"]
     val = cells * steps / dt / 1e9
     sim.close()
     return {"value": val, "unit": "Gcell-updates/s", "cores": ncores, "kind": "port",
-            "sample": f"{sample}, {steps} steps in {dt:.1f} s"}
+            "sample": (f"the full {p['nx']}x{p['ny']}x{p['nz']} grid of the {workload} "
+                       f"workload, FP32 with subnormals flushed, {steps} timed steps after "
+                       f"{max(1, warmup)} warm-up, {dt:.1f} s"),
+            "host": host_cpu()}
 
 
 def texture_arrays(nx, ny, nz, tau1, tau2, w8):
@@ -177,11 +189,14 @@ def texture_arrays(nx, ny, nz, tau1, tau2, w8):
     return vx1, vx2, ww, wwo
 
 
-def reference_gpu(scn, solver, steps=4, warmup=2, topo_path=None) -> dict:
-    """The reference's own CUDA build (oracle/_ref/libawpref.so, 8-thread blocks as
-    shipped) on the same workload, inputs taken from the product's set-up; with
-    a topography file, its curvilinear kernels (oracle/_ref/libawpref_topo.so)
-    in place of dvelcx / dstrqc."""
+def reference_gpu(scn, solver, steps=20, warmup=3, topo_path=None, variant="as_shipped") -> dict:
+    """The reference's own CUDA build on the same workload, inputs taken from
+    the product's set-up: `variant` "as_shipped" (oracle/_ref/libawpref.so,
+    2 x 2 x 4-thread blocks of include/awp/pmcl3d_cons.h) or "block_64x8"
+    (oracle/_ref/libawpref_b64x8.so: the same source with only the launch block
+    raised to 64 z x 8 y threads, as dstrqc_H_new picks it); with a topography
+    file, its curvilinear kernels (oracle/_ref/libawpref_topo.so) in place of
+    dvelcx / dstrqc."""
     import torch
     from oracle import refbind
     p = scn.params
@@ -207,10 +222,15 @@ def reference_gpu(scn, solver, steps=4, warmup=2, topo_path=None) -> dict:
     del media
     with torch.cuda.stream(torch.cuda.default_stream()):
         # the reference launchers run on the legacy default stream
+        lib = None
+        if variant == "block_64x8":
+            if nz % 64 or ny % 8:
+                raise ValueError("the 64x8-block build needs nzt % 64 == 0 and nyt % 8 == 0")
+            lib = os.path.join(refbind.REF_DIR, "libawpref_b64x8.so")
         if topo_path:
-            sim = refbind.RefTopoSim(scn, setup, topo_path)
+            sim = refbind.RefTopoSim(scn, setup, topo_path, path=lib)
         else:
-            sim = refbind.RefGpuSim(scn, setup)
+            sim = refbind.RefGpuSim(scn, setup, path=lib)
         del setup, vx1, vx2, ww, wwo
         sim.step(warmup)
         s0 = torch.cuda.Event(enable_timing=True)
@@ -223,8 +243,11 @@ def reference_gpu(scn, solver, steps=4, warmup=2, topo_path=None) -> dict:
         ms = s0.elapsed_time(s1) / steps
     out = {"value": nx * ny * nz / (ms * 1e-3) / 1e9, "unit": "Gcell-updates/s",
            "ms_per_step": ms, "steps": steps,
-           "build": "reference src/awp/kernel.cu, nvcc sm_100a -O3 -use_fast_math, "
-                    "BLOCK_SIZE 2x2x4 as shipped; launched in the pmcl3d single-rank order"}
+           "build": "reference src/awp/kernel.cu, nvcc sm_100a -O3 -use_fast_math, " +
+                    ("BLOCK_SIZE 2x2x4 as shipped" if variant == "as_shipped" else
+                     "BLOCK_SIZE_Z/Y raised to 64/8 (DEFINITIONS_H), nothing else changed") +
+                    f"; launched in the pmcl3d single-rank order; {steps} steps timed after "
+                    f"{warmup} warm-up"}
     if topo_path:
         out["build"] += ("; curvilinear top grid: the reference's topo_velocity_interior_H "
                          "and topo_stress_{interior,left,right}_H (opt_topography kernels)")
@@ -407,15 +430,18 @@ def run_ours(args, rank, world, dist) -> dict | None:
     if e2e:
         line["e2e"] = e2e
     if world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(args.workload)
+        line["cpu_baseline"] = cpu_baseline(args.workload, steps=10, warmup=3, grid=args.grid)
     if world == 1 and not args.no_ref_gpu:
-        try:
-            s2 = Solver(default_params(**p))
-            s2.upload_media(scn.media)
-            line["reference_gpu_build"] = reference_gpu(scn, s2, topo_path=topo_path)
-            s2.close()
-        except Exception as exc:  # reported, never substituted
-            line["reference_gpu_build"] = {"unavailable": f"{type(exc).__name__}: {exc}"}
+        rg = {}
+        for variant in ("as_shipped", "block_64x8"):
+            try:
+                s2 = Solver(default_params(**p))
+                s2.upload_media(scn.media)
+                rg[variant] = reference_gpu(scn, s2, topo_path=topo_path, variant=variant)
+                s2.close()
+            except Exception as exc:  # reported, never substituted
+                rg[variant] = {"unavailable": f"{type(exc).__name__}: {exc}"}
+        line["reference_gpu_build"] = rg
     return line
 
 
@@ -428,16 +454,16 @@ def reference_config(args) -> dict:
     return {"workload": args.workload, "description": desc,
             "grid": [p["nx"], p["ny"], p["nz"]], "cells": p["nx"] * p["ny"] * p["nz"],
             "dh": p["dh"], "dt": p["dt"], "ifault": p["ifault"], "nve": p["nve"],
-            "parallelism": "single GPU's workload, timed on the host cores",
+            "parallelism": "the single-GPU workload's full grid, timed on the host cores",
             "l2": "working set ~7 GB >> 126 MB L2, no flush needed", "topography": None}
 
 
 def run_reference(args, rank) -> dict | None:
     """Reference arm: the reference path's CPU restatement on the host cores,
-    W warm-up and K timed steps on a bounded window of the same workload."""
+    W warm-up and K timed steps on the workload's full grid."""
     if rank != 0:
         return None
-    cb = cpu_baseline(args.workload, steps=args.steps, warmup=args.warmup)
+    cb = cpu_baseline(args.workload, steps=args.steps, warmup=args.warmup, grid=args.grid)
     return {"metric": "Gcell-updates/s (whole time step) & %HBM roofline on 1 B200",
             "value": cb["value"], "unit": "Gcell-updates/s", "n_gpus": 1,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,

@@ -367,9 +367,12 @@ int awp_phase_times(awp_ctx* ctx, double ms[AWP_NPHASES], long long launches[AWP
 /* Launch-shape tuning of the stencil kernels (process-wide): key "ichunk"
  * (x planes marched per CTA, 4..1024), "tma_vel" / "tma_str" (1: the context
  * API runs the TMA-pipelined velocity / stress kernel, 0: the read-only-path
- * one; results are bit-identical) and "tma" (sets both; reads -1 when they
- * differ).  Returns AWP_OK or AWP_ERR_ARG; awp_get_tuning returns the value
- * or -1 for an unknown key. */
+ * one; results are bit-identical), "tma" (sets both; reads -1 when they
+ * differ) and "spin_limit" (0 .. 2^30, default 2^26: polls of each pipeline
+ * wait of the TMA kernels before it gives up, 0 = give up at once; a wait that
+ * gives up makes the CTA drain its issued copies and leave, and the next
+ * awp_synchronize of the context returns AWP_ERR_CUDA once).  Returns AWP_OK or AWP_ERR_ARG;
+ * awp_get_tuning returns the value or -1 for an unknown key. */
 int awp_set_tuning(const char* key, int value);
 int awp_get_tuning(const char* key);
 

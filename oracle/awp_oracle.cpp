@@ -7,6 +7,7 @@
 
 #include <math.h>
 #include <omp.h>
+#include <xmmintrin.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -723,7 +724,25 @@ struct Oracle : Base {
 
 struct oracle {
   Base* impl;
+  int nthreads = 1;
+  int flush = 0;  // FTZ/DAZ on the stepping threads (CPU baseline mode)
 };
+
+namespace {
+// Flush-to-zero and denormals-are-zero (MXCSR bits 15 and 6) on every thread of
+// the team the stepping loops use, and on the calling thread: the reference's
+// CUDA build compiles with -use_fast_math, which flushes FP32 subnormals, so the
+// CPU baseline times the same arithmetic without the x86 subnormal slow path.
+void set_ftz_daz(int nthreads, bool on) {
+#pragma omp parallel num_threads(nthreads)
+  {
+    const unsigned m = _mm_getcsr();
+    _mm_setcsr(on ? (m | 0x8040u) : (m & ~0x8040u));
+  }
+  const unsigned m = _mm_getcsr();
+  _mm_setcsr(on ? (m | 0x8040u) : (m & ~0x8040u));
+}
+}  // namespace
 
 extern "C" {
 
@@ -731,6 +750,7 @@ oracle* oracle_create(int precision, int nxt, int nyt, int nzt, float dh, float 
                       int nthreads) {
   oracle* o = new oracle;
   if (nthreads <= 0) nthreads = omp_get_max_threads();
+  o->nthreads = nthreads;
   if (precision == 32)
     o->impl = new Oracle<float>(nxt, nyt, nzt, dh, dt, npc, nthreads);
   else if (precision == 65)
@@ -772,7 +792,12 @@ void oracle_add_point_sources(oracle* o, int field, int nq, int nb, const int* i
                               const float* lz, int nsamples, const float* values, int stride) {
   o->impl->add_point_sources(field, nq, nb, ix, iy, iz, lx, ly, lz, nsamples, values, stride);
 }
-void oracle_step(oracle* o, int nve, int n) { o->impl->step(nve, n); }
+void oracle_step(oracle* o, int nve, int n) {
+  if (o->flush) set_ftz_daz(o->nthreads, true);
+  o->impl->step(nve, n);
+  if (o->flush) set_ftz_daz(o->nthreads, false);
+}
+void oracle_set_flush_denormals(oracle* o, int on) { o->flush = on ? 1 : 0; }
 void oracle_set_tangent(oracle* o, int field, const double* t) {
   o->impl->set_tangent_field(field, t);
 }

@@ -62,6 +62,9 @@ void oracle_add_point_sources(oracle* o, int field, int nq, int nb, const int* i
                               const int* iy, const int* iz, const float* lx, const float* ly,
                               const float* lz, int nsamples, const float* values, int stride);
 void oracle_step(oracle* o, int nve, int n);
+/* FP32 subnormals flushed to zero while stepping (as the reference's
+ * -use_fast_math CUDA build does); for the CPU baseline, off by default. */
+void oracle_set_flush_denormals(oracle* o, int on);
 /* Tangent part of a field (precision 65; a no-op / zeros otherwise). */
 void oracle_set_tangent(oracle* o, int field, const double* t);
 void oracle_get_tangent(oracle* o, int field, double* t);

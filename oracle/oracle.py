@@ -50,6 +50,7 @@ def load():
         lib.oracle_get_moment.argtypes = [c_void_p, _F]
         lib.oracle_set_plasticity.argtypes = [c_void_p, c_float, c_float, _F, _F]
         lib.oracle_step.argtypes = [c_void_p, c_int, c_int]
+        lib.oracle_set_flush_denormals.argtypes = [c_void_p, c_int]
         lib.oracle_add_point_sources.argtypes = ([c_void_p, c_int, c_int, c_int] + [_I] * 3 +
                                                  [_F] * 3 + [c_int, _F, c_int])
         lib.oracle_current_step.restype = c_longlong
@@ -66,7 +67,7 @@ def fp(a):
 
 
 class OracleSim:
-    def __init__(self, scn, setup=None, precision=64, nthreads=0):
+    def __init__(self, scn, setup=None, precision=64, nthreads=0, flush_denormals=False):
         lib = load()
         self.lib = lib
         self.scn = scn
@@ -77,6 +78,9 @@ class OracleSim:
         self.setup = setup
         self.o = lib.oracle_create(precision, p["nx"], p["ny"], p["nz"], p["dh"], p["dt"],
                                    p.get("npc", 0), nthreads)
+        # the CPU baseline flushes FP32 subnormals like the reference's
+        # -use_fast_math CUDA build
+        lib.oracle_set_flush_denormals(self.o, 1 if flush_denormals else 0)
         m = setup["media"]
         for k in ("d1", "mu", "lam", "qp", "qs"):
             lib.oracle_set_field(self.o, FIELD[k], fp(np.ascontiguousarray(m[k], np.float32)))

@@ -28,9 +28,10 @@ def make(spec, steps):
     return s
 
 
-@pytest.mark.parametrize("mode,ty,ichunk,graph", [(0, 8, 16, True), (0, 4, 8, True),
-                                                  (0, 8, 32, False), (1, 8, 16, True)])
-def test_batch_equals_plain_runs(mode, ty, ichunk, graph):
+@pytest.mark.parametrize("mode,ty,ichunk,graph,branches",
+                         [(0, 8, 16, True, 0), (0, 4, 8, True, 0), (0, 8, 32, False, 0),
+                          (1, 8, 16, True, 0), (1, 8, 16, True, 2), (1, 8, 16, True, 1)])
+def test_batch_equals_plain_runs(mode, ty, ichunk, graph, branches):
     steps = 12
     plain = [make(sp, steps) for sp in INSTANCES]
     for s in plain:
@@ -45,6 +46,9 @@ def test_batch_equals_plain_runs(mode, ty, ichunk, graph):
     b.set_mode(mode)
     b.set_shape(ty, ichunk)
     b.set_graph(graph)
+    # mode 1 with fewer branches than instances deals several instances'
+    # launches onto one captured branch
+    b.set_branches(branches)
     info = b.info()
     assert info["instances"] == len(INSTANCES)
     b.step(5)

@@ -43,3 +43,16 @@ def test_status_strings_and_defaults():
     assert abs(p.dh - 200.0) < 1e-6 and abs(p.dt - 0.01) < 1e-9
     assert p.nd == 20 and abs(p.arbc - 0.92) < 1e-7 and p.nve == 1 and p.socalq == 1
     assert p.nst == 91 and p.read_step == 91
+
+
+def test_tuning_keys_and_ranges():
+    # host-side settings only: no GPU work is queued
+    lib = _lib.load()
+    assert lib.awp_get_tuning(b"spin_limit") == 1 << 26
+    assert lib.awp_set_tuning(b"spin_limit", -1) != 0
+    assert lib.awp_set_tuning(b"spin_limit", (1 << 30) + 1) != 0
+    assert lib.awp_set_tuning(b"spin_limit", 1 << 20) == 0
+    assert lib.awp_get_tuning(b"spin_limit") == 1 << 20
+    assert lib.awp_set_tuning(b"spin_limit", 1 << 26) == 0
+    assert lib.awp_set_tuning(b"ichunk", 3) != 0
+    assert lib.awp_get_tuning(b"nonsense") == -1
