@@ -468,6 +468,80 @@ void velbuffer_H(const float* u1, const float* v1, const float* w1,
                  int rec_nyt, int rec_nzt, awp_stream_t St, int FOLLOWBATHY,
                  const int* bathy, int d_i);
 
+/* kernel_launch.h:92 -- 2nd-order velocity of the interface layer of grid d_i */
+void dvelc2_H(float* u1, float* v1, float* w1, float* xx, float* yy, float* zz, float* xy,
+              float* xz, float* yz, float* dcrjx, float* dcrjy, float* dcrjz, float* d_1,
+              int nxt, int nyt, awp_stream_t St, int d_i);
+/* kernel_launch.h:97 -- 2nd-order stress of the interface layer of grid d_i,
+ * memory-variable coefficients from the caller's vx1/vx2/ww/wwo arrays */
+void dstrqc2_H(float* xx, float* yy, float* zz, float* xy, float* xz, float* yz, float* r1,
+               float* r2, float* r3, float* r4, float* r5, float* r6, float* u1, float* v1,
+               float* w1, float* lam, float* mu, float* qp, float* qs, float* dcrjx,
+               float* dcrjy, float* dcrjz, int nxt, int nyt, awp_stream_t St, float* coeff,
+               float* d_vx1, float* d_vx2, int* d_ww, float* d_wwo, int s_i, int e_i, int s_j,
+               int e_j, int d_i);
+/* kernel_launch.h:105 -- coarse (grid d_i, "l") to fine (grid d_i-1, "h") */
+void intp3d_H(float* u1l, float* v1l, float* w1l, float* xxl, float* yyl, float* zzl,
+              float* xyl, float* xzl, float* yzl, float* u1h, float* v1h, float* w1h, float* xxh,
+              float* yyh, float* zzh, float* xyh, float* xzh, float* yzh, int nxtl, int nytl,
+              int rank, awp_stream_t St, int d_i);
+/* kernel_launch.h:111 -- fine (grid d_i, "h") to coarse (grid d_i+1, "l") window
+ * average; at one rank the swap-area buffers are not read */
+void swap_H(float* xxl, float* yyl, float* zzl, float* xyl, float* xzl, float* yzl, float* u1l,
+            float* v1l, float* w1l, float* xxh, float* yyh, float* zzh, float* xyh, float* xzh,
+            float* yzh, float* u1h, float* v1h, float* w1h, int nxtl, int nytl, float* buf_L,
+            float* buf_R, float* buf_F, float* buf_B, int rank, awp_stream_t St, int d_i);
+/* kernel_launch.h:74 -- prescribed velocities at the source points (IFAULT 4) */
+void frcvel_H(int i, int READ_STEP, int dim, int* psrc, int npsrc, int tskp, awp_stream_t St,
+              float* axx, float* ayy, float* azz, float* axz, float* ayz, float* axy, float* u1,
+              float* v1, float* w1, int ymin, int ymax, int d_i);
+/* kernel_launch.h:127 -- plane-wave source (IFAULT 6) at k = align+ND+1 */
+void addplanesrc_H(int i, int dim, int NST, awp_stream_t St, float* mu, float* lambda, int ND,
+                   int nxt, int nyt, float* axx, float* ayy, float* azz, float* xx, float* yy,
+                   float* zz, float* xy, float* yz, float* xz, int d_i);
+/* kernel_launch.h:79 -- free-surface velocity images of grid 0 */
+void fvel_H(float* u1, float* v1, float* w1, awp_stream_t St, float* lam_mu, int NX, int rankx,
+            int ranky, int s_i, int e_i, int s_j, int e_j);
+/* kernel_launch.h:82-91, 132-178 -- halo exchanges between ranks: return at
+ * once when both neighbour ranks are -1 (world size 1), like the reference;
+ * any other rank is refused with the launchers' error behaviour */
+void update_bound_y_H(float* u1, float* v1, float* w1, float* f_u1, float* f_v1, float* f_w1,
+                      float* b_u1, float* b_v1, float* b_w1, int nxt, int nzt, awp_stream_t St1,
+                      awp_stream_t St2, int rank_f, int rank_b, int d_i);
+void update_yldfac_buffer_x_H(float* yldfac, float* buf_L, float* buf_R, int nyt, int nzt,
+                              awp_stream_t St1, awp_stream_t St2, int rank_L, int rank_R,
+                              int d_i);
+void update_yldfac_data_x_H(float* yldfac, float* buf_L, float* buf_R, int nyt, int nzt,
+                            awp_stream_t St1, awp_stream_t St2, int rank_L, int rank_R, int d_i);
+void update_yldfac_buffer_y_H(float* yldfac, float* buf_F, float* buf_B, int nxt, int nzt,
+                              awp_stream_t St1, awp_stream_t St2, int rank_F, int rank_B,
+                              int d_i);
+void update_yldfac_data_y_H(float* yldfac, float* buf_F, float* buf_B, int nxt, int nzt,
+                            awp_stream_t St1, awp_stream_t St2, int rank_F, int rank_B, int d_i);
+void update_swapzone_buffer_x_H(float* u1, float* v1, float* w1, float* xx, float* yy, float* zz,
+                                float* xy, float* xz, float* yz, float* buf_L, float* buf_R,
+                                int nyt, awp_stream_t St1, awp_stream_t St2, int rank_L,
+                                int rank_R, int zs, int ze, int meshtp);
+void update_swapzone_data_x_H(float* u1, float* v1, float* w1, float* xx, float* yy, float* zz,
+                              float* xy, float* xz, float* yz, float* buf_L, float* buf_R, int nyt,
+                              awp_stream_t St1, awp_stream_t St2, int rank_L, int rank_R, int zs,
+                              int ze, int meshtp);
+void update_swapzone_buffer_y_H(float* u1, float* v1, float* w1, float* xx, float* yy, float* zz,
+                                float* xy, float* xz, float* yz, float* buf_F, float* buf_B,
+                                int nxt, awp_stream_t St1, awp_stream_t St2, int rank_F,
+                                int rank_B, int zs, int ze, int d_i);
+void update_swapzone_data_y_H(float* u1, float* v1, float* w1, float* xx, float* yy, float* zz,
+                              float* xy, float* xz, float* yz, float* buf_F, float* buf_B, int nxt,
+                              awp_stream_t St1, awp_stream_t St2, int rank_F, int rank_B, int zs,
+                              int ze, int d_i);
+/* kernel_launch.h:11-19 -- device-side debug printing, compiled out in the
+ * reference (kernel.cu:270-296, 3236-3318): no output, no launch */
+void print_const_H(int ngrids);
+void print_nonzero_H(float* array, int nx, int ny, int nz, int d_i, int rank);
+void print_nonzero_mat_H(float* array, int nx, int ny, int nz, int d_i, float* d1, float* mu,
+                         float* lam, float* qp, float* qs, int rank);
+void print_nan_H(float* array, int nx, int ny, int nz, char* vname);
+
 /* Error mode of the launchers above: 1 (default) = print and exit like the
  * reference's CUCHK; 0 = record the error and return. */
 void awp_compat_exit_on_error(int exit_on_error);

@@ -5,6 +5,10 @@
  * library oracle/_ref/libawpref_host.so.  It is test infrastructure: the
  * product never includes it.
  *
+ * It also lets the link-symbol test compile pmcl3d.c and the rest of the
+ * reference's lpmcl3d host files (tests/test_dropin_link.py) to list the
+ * launchers they call; calls it does not declare stay undefined there.
+ *
  * Semantics are those of MPI with a world of exactly one rank:
  *   - rank 0, size 1;
  *   - Bcast is a no-op, Allreduce copies send -> recv;
@@ -36,6 +40,10 @@ typedef int MPI_File;
 #define MPI_INT ((MPI_Datatype)sizeof(int))
 #define MPI_OFFSET ((MPI_Datatype)sizeof(long long))
 #define MPI_BYTE ((MPI_Datatype)1)
+#define MPI_CHAR ((MPI_Datatype)1)
+#define MPI_UINT32_T ((MPI_Datatype)4)
+#define MPI_UINT64_T ((MPI_Datatype)8)
+#define MPI_STATUS_IGNORE ((MPI_Status *)0)
 #ifndef MPI_AINT
 #define MPI_AINT ((MPI_Datatype)sizeof(long long))
 #endif

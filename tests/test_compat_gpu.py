@@ -139,3 +139,134 @@ def test_fstr_and_addsrc_H(libs):
         torch.cuda.synchronize()
     for f in ("xx", "yy", "zz", "xy", "xz", "yz"):
         assert torch.equal(a[f], b[f]), f
+
+
+def _argtypes(lib):
+    V = c_void_p
+    lib.frcvel_H.argtypes = [c_int] * 6 + [V] * 10 + [c_int] * 3
+    lib.addplanesrc_H.argtypes = [c_int, c_int, c_int, V, V, V, c_int, c_int, c_int] + [V] * 9 + \
+        [c_int]
+    lib.fvel_H.argtypes = [V] * 5 + [c_int] * 7
+    lib.velbuffer_H.argtypes = [V] * 8 + [c_int] * 13 + [V, c_int, V, c_int]
+
+
+def test_frcvel_H(libs):
+    """Prescribed velocities (IFAULT 4): interpolated steps, the last
+    prescribed step (restoring force stored in the source arrays) and the
+    static force after it, with and without the x window."""
+    import torch
+    prod, ref = libs
+    nx, ny, nz = 23, 19, 28
+    a = state(nx, ny, nz, 5)
+    b = clone(a)
+    npsrc, rs, tskp = 6, 4, 3
+    psrc = torch.as_tensor(np.array([[3, 4, 5], [10, 11, 1], [20, 2, 27], [5, 5, 5], [1, 1, 1],
+                                     [22, 18, 3]], np.int32)).cuda()
+    srcs = {}
+    for lib, s in ((ref, a), (prod, b)):
+        _argtypes(lib)
+        setconst(lib, nx, ny, nz, 100.0, 0.004)
+        g = torch.Generator(device="cpu").manual_seed(11)
+        comps = [(torch.randn((rs + 1) * npsrc, generator=g) * 0.1).cuda() for _ in range(6)]
+        for window in ((-1, -1), (12, 28)):
+            for i in range(1, rs * tskp + 4):
+                lib.frcvel_H(i, rs, 3, P(psrc), npsrc, tskp, None, *[P(c) for c in comps],
+                             P(s["u1"]), P(s["v1"]), P(s["w1"]), window[0], window[1], 0)
+        torch.cuda.synchronize()
+        srcs[id(lib)] = comps
+    assert prod.awp_compat_last_error() == 0
+    for f in ("u1", "v1", "w1"):
+        assert torch.allclose(a[f], b[f], rtol=1e-6, atol=1e-7), f
+    for ca, cb in zip(srcs[id(ref)], srcs[id(prod)]):
+        assert torch.allclose(ca, cb, rtol=1e-6, atol=1e-6)
+
+
+def test_addplanesrc_H(libs):
+    import torch
+    prod, ref = libs
+    for nx, ny in ((23, 19), (24, 20)):
+        nz = 32
+        a = state(nx, ny, nz, 6)
+        b = clone(a)
+        n_src = 7
+        comps = [torch.randn(n_src, device="cuda") * 1e3 for _ in range(3)]
+        for lib, s in ((ref, a), (prod, b)):
+            _argtypes(lib)
+            setconst(lib, nx, ny, nz, 100.0, 0.004)
+            for step in (0, 3, 6):
+                lib.addplanesrc_H(step, 3, n_src, None, P(s["mu"]), P(s["lam"]), 5, nx, ny,
+                                  *[P(c) for c in comps], P(s["xx"]), P(s["yy"]), P(s["zz"]),
+                                  P(s["xy"]), P(s["yz"]), P(s["xz"]), 0)
+            torch.cuda.synchronize()
+        assert prod.awp_compat_last_error() == 0
+        for f in ("xx", "yy", "zz", "xy", "xz", "yz"):
+            assert torch.equal(a[f], b[f]), (f, (a[f] - b[f]).abs().max().item())
+
+
+def test_fvel_H(libs):
+    import torch
+    prod, ref = libs
+    rng = np.random.default_rng(9)
+    for nx, ny in ((23, 19), (24, 20)):
+        nz = 28
+        a = state(nx, ny, nz, 7)
+        b = clone(a)
+        lam_mu = torch.as_tensor(rng.uniform(0.2, 0.4, (nx + 20, ny + 20)).astype(np.float32))
+        lam_mu = lam_mu.cuda()
+        for lib, s in ((ref, a), (prod, b)):
+            _argtypes(lib)
+            setconst(lib, nx, ny, nz, 100.0, 0.004)
+            lib.fvel_H(P(s["u1"]), P(s["v1"]), P(s["w1"]), None, P(lam_mu), nx, 0, 0, 10, nx + 9,
+                       10, ny + 9)
+            torch.cuda.synchronize()
+        assert prod.awp_compat_last_error() == 0
+        for f in ("u1", "v1", "w1"):
+            assert torch.equal(a[f], b[f]), (f, (a[f] - b[f]).abs().max().item())
+
+
+@pytest.mark.parametrize("nve,bathy", [(1, False), (3, False), (1, True)])
+def test_velbuffer_H(libs, nve, bathy):
+    import torch
+    prod, ref = libs
+    nx, ny, nz = 23, 19, 28
+    s = state(nx, ny, nz, 8)
+    s["neta"] = torch.randn_like(s["u1"])
+    nb = (2, nx - 1, 3, 1, ny - 2, 2, 0, 4, 2)
+    rec = [(nb[3 * q + 1] - nb[3 * q]) // nb[3 * q + 2] + 1 for q in range(3)]
+    ktop = nz + 31
+    bt = np.full((ny + 20, nx + 20), ktop, np.int32)
+    bt[::3, ::2] = ktop - 2
+    bt_d = torch.as_tensor(bt).cuda()
+    out = {}
+    for lib in (ref, prod):
+        _argtypes(lib)
+        setconst(lib, nx, ny, nz, 100.0, 0.004)
+        bufs = [torch.full((int(np.prod(rec)),), -7.0, device="cuda") for _ in range(4)]
+        lib.velbuffer_H(P(s["u1"]), P(s["v1"]), P(s["w1"]), P(s["neta"]), *[P(t) for t in bufs],
+                        nve, *nb, *rec, None, 1 if bathy else 0,
+                        P(bt_d) if bathy else None, 0)
+        torch.cuda.synchronize()
+        out[id(lib)] = bufs
+    assert prod.awp_compat_last_error() == 0
+    for x, y in zip(out[id(ref)], out[id(prod)]):
+        assert torch.equal(x, y)
+
+
+def test_single_rank_exchanges_and_printing(libs):
+    """At world size 1 the halo exchanges return at once (both neighbour ranks
+    -1); a real neighbour is refused with the launchers' error behaviour.  The
+    debug printers print nothing, as in the reference."""
+    prod, _ = libs
+    V = c_void_p
+    prod.update_bound_y_H.argtypes = [V] * 9 + [c_int, c_int, V, V, c_int, c_int, c_int]
+    prod.update_yldfac_data_x_H.argtypes = [V] * 3 + [c_int, c_int, V, V, c_int, c_int, c_int]
+    prod.update_swapzone_buffer_y_H.argtypes = [V] * 11 + [c_int, V, V] + [c_int] * 5
+    prod.print_const_H.argtypes = [c_int]
+    prod.awp_compat_last_error()
+    prod.update_bound_y_H(*([None] * 9), 10, 10, None, None, -1, -1, 0)
+    prod.update_yldfac_data_x_H(None, None, None, 10, 10, None, None, -1, -1, 0)
+    prod.update_swapzone_buffer_y_H(*([None] * 11), 10, None, None, -1, -1, 34, 39, 0)
+    prod.print_const_H(2)
+    assert prod.awp_compat_last_error() == 0
+    prod.update_bound_y_H(*([None] * 9), 10, 10, None, None, 1, -1, 0)
+    assert prod.awp_compat_last_error() != 0
