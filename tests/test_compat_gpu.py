@@ -143,7 +143,7 @@ def test_fstr_and_addsrc_H(libs):
 
 def _argtypes(lib):
     V = c_void_p
-    lib.frcvel_H.argtypes = [c_int] * 6 + [V] * 10 + [c_int] * 3
+    lib.frcvel_H.argtypes = [c_int, c_int, c_int, V, c_int, c_int, V] + [V] * 9 + [c_int] * 3
     lib.addplanesrc_H.argtypes = [c_int, c_int, c_int, V, V, V, c_int, c_int, c_int] + [V] * 9 + \
         [c_int]
     lib.fvel_H.argtypes = [V] * 5 + [c_int] * 7
