@@ -112,6 +112,7 @@ def load() -> ctypes.CDLL:
     _sig(lib, "awp_mesh_grid", c_int, [_P, c_int, POINTER(c_void_p)])
     _sig(lib, "awp_mesh_step", c_int, [_P, c_int])
     _sig(lib, "awp_mesh_synchronize", c_int, [_P])
+    _sig(lib, "awp_mesh_set_stream", c_int, [_P, _P])
     _sig(lib, "awp_batch_create", c_int, [POINTER(c_void_p), c_int, POINTER(c_void_p)])
     _sig(lib, "awp_batch_destroy", c_int, [_P])
     _sig(lib, "awp_batch_step", c_int, [_P, c_int])
@@ -128,11 +129,15 @@ def load() -> ctypes.CDLL:
     _sig(lib, "awp_sourcefile_init", c_int, [_P, c_char_p])
     _sig(lib, "awp_topo_metrics", c_int, [c_char_p, c_int, c_int, c_int, c_float, _F])
     _sig(lib, "awp_topography_init", c_int, [_P, c_char_p])
+    _sig(lib, "awp_set_topo_plasticity", c_int, [_P, c_int])
     _sig(lib, "awp_set_moduli", c_int, [_P, _F, _F, _F])
     _sig(lib, "awp_reset", c_int, [_P])
     _sig(lib, "awp_seismograms", c_int, [_P, c_int, c_int, _I, _I, _F])
     _sig(lib, "awp_misfit_gradient", c_int,
          [_P, c_int, c_int, _I, _I, _F, c_int, POINTER(c_double), _F, _F, _F, _F])
+    _sig(lib, "awp_misfit_gradient_q", c_int,
+         [_P, c_int, c_int, _I, _I, _F, c_int, POINTER(c_double), _F, _F, _F, _F, _F, _F])
+    _sig(lib, "awp_set_qinv", c_int, [_P, _F, _F])
     _sig(lib, "awp_adjoint_reserve", c_int, [_P, c_int, c_int])
     _sig(lib, "awp_adjoint_plan", c_int,
          [_P, c_int, c_int, _I, _I, _I, POINTER(c_double)])

@@ -40,24 +40,37 @@ def seismograms(solver, nsteps: int, rec_xyz, rec_comp) -> np.ndarray:
     return out
 
 
-def misfit_gradient(solver, nsteps: int, rec_xyz, rec_comp, d_obs, nsnap: int = 0):
+def _ptr(x):
+    """ctypes float pointer of a numpy array or of a CUDA tensor's storage."""
+    if isinstance(x, np.ndarray):
+        return x.ctypes.data_as(_F)
+    return ctypes.cast(ctypes.c_void_p(x.data_ptr()), _F)
+
+
+def misfit_gradient(solver, nsteps: int, rec_xyz, rec_comp, d_obs, nsnap: int = 0,
+                    want_q: bool = False, out=None):
     """J = 1/2 sum (seis - d_obs)^2 over nsteps steps from the solver's current
-    state, and dJ/dlambda, dJ/dmu, dJ/drho ([nz][ny][nx]).  Returns
-    (J, seis, g_lambda, g_mu, g_rho)."""
+    state, and dJ/dlambda, dJ/dmu, dJ/drho ([nz][ny][nx]); with want_q also
+    dJ/dQp^-1 and dJ/dQs^-1.  Returns (J, seis, g_lambda, g_mu, g_rho[, g_qpinv,
+    g_qsinv]).  `out` (optional): the gradient arrays to fill -- numpy arrays
+    or contiguous float32 CUDA tensors, written in place by the library."""
     xyz, comp = _i32(rec_xyz).reshape(-1, 3), _i32(rec_comp).reshape(-1)
     d = _f32(d_obs).reshape(nsteps, comp.size)
     p = solver.params
     shape = (p.nz, p.ny, p.nx)
     seis = np.zeros((nsteps, comp.size), np.float32)
-    g = [np.zeros(shape, np.float32) for _ in range(3)]
+    ng = 5 if want_q else 3
+    g = list(out) if out is not None else [np.zeros(shape, np.float32) for _ in range(ng)]
+    if len(g) != ng:
+        raise ValueError(f"out must hold {ng} arrays")
     J = c_double()
-    check(solver.lib.awp_misfit_gradient(solver.ctx, int(nsteps), comp.size,
-                                         xyz.ctypes.data_as(_I), comp.ctypes.data_as(_I),
-                                         d.ctypes.data_as(_F), int(nsnap), byref(J),
-                                         seis.ctypes.data_as(_F),
-                                         *[x.ctypes.data_as(_F) for x in g]),
-          "awp_misfit_gradient")
-    return J.value, seis, g[0], g[1], g[2]
+    ptrs = [_ptr(x) for x in g] + [None] * (5 - ng)
+    check(solver.lib.awp_misfit_gradient_q(solver.ctx, int(nsteps), comp.size,
+                                           xyz.ctypes.data_as(_I), comp.ctypes.data_as(_I),
+                                           d.ctypes.data_as(_F), int(nsnap), byref(J),
+                                           seis.ctypes.data_as(_F), *ptrs),
+          "awp_misfit_gradient_q")
+    return (J.value, seis, *g)
 
 
 def misfit_gradient_shots(solver, nsteps: int, shots, nsnap: int = 0):
@@ -112,14 +125,19 @@ def _autograd_function():
 
         @staticmethod
         def forward(ctx, lam, mu, rho, solver, nsteps, rec_xyz, rec_comp, d_obs, nsnap=0):
-            solver.set_moduli(lam.detach().cpu().numpy(), mu.detach().cpu().numpy(),
-                              rho.detach().cpu().numpy())
+            # the library reads the model and writes the gradients through
+            # device pointers when the tensors live on the GPU (no host copy);
+            # host tensors go through their host memory the same way
+            m = [t.detach().to(torch.float32).contiguous() for t in (lam, mu, rho)]
+            if m[0].is_cuda:
+                torch.cuda.current_stream(m[0].device).synchronize()
+            solver.set_moduli(*m)
             solver.reset()
-            J, _, gl, gm, gr = misfit_gradient(solver, nsteps, rec_xyz, rec_comp, d_obs, nsnap)
-            dev = lam.device
-            ctx.save_for_backward(torch.from_numpy(gl).to(dev), torch.from_numpy(gm).to(dev),
-                                  torch.from_numpy(gr).to(dev))
-            return torch.tensor(J, dtype=torch.float64, device=dev)
+            g = [torch.empty_like(x) for x in m]
+            J, _, gl, gm, gr = misfit_gradient(solver, nsteps, rec_xyz, rec_comp, d_obs, nsnap,
+                                               out=g)
+            ctx.save_for_backward(gl, gm, gr)
+            return torch.tensor(J, dtype=torch.float64, device=lam.device)
 
         @staticmethod
         def backward(ctx, gJ):

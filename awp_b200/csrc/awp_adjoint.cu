@@ -35,7 +35,17 @@
 namespace {
 
 enum { LU, LV, LW, LXX, LYY, LZZ, LXY, LXZ, LYZ, LR1, LR2, LR3, LR4, LR5, LR6 };
-enum { E1, E2, E3, E4, E5, E6, GL8, GM8, GP1, GP2, GP3 };
+enum { E1, E2, E3, E4, E5, E6, GL8, GM8, GP1, GP2, GP3, GQP8, GQS8, GQ1, GQ2, GQ3 };
+
+// d(weight)/dq of the Q(f) weight awp_qf_weight(q, ...): the polynomial
+// c0 (2q)^2 + c1 (2q) over wwo on the low-Q branch, 2 q otherwise (the branch
+// held fixed, as the forward takes it at q)
+__device__ __forceinline__ float qf_dweight(float q, float wwo, float c0, float c1,
+                                            float qthr) {
+  const float x = 2.0f * q;
+  const bool low = (x >= qthr) || (x < 0.f) || (x == 0.f && signbit(x));
+  return low ? (8.0f * c0 * q + 2.0f * c1) / wwo : 2.0f;
+}
 enum { VA, VB, VC, VEA, VEB, VEC };
 
 // ---------------------------------------------------------------------------
@@ -99,14 +109,22 @@ __global__ void __launch_bounds__(128, 7) k_adj_stress_cell(const AdjArgs a) {
   const int t = awp_tex_index(a.tex, i, j, k);
   const float fvx1 = tab[t], fvx2 = tab[8 + t], wwo = tab[16 + t];
   float c_xm = a.dth, c_h = 0.f, c_q = 0.f, c_m[3] = {a.dth, a.dth, a.dth}, c_hh[3] = {0, 0, 0};
+  // derivatives of the Q weights with respect to their averaged arguments
+  float dqpaw = 0.f, dhw = 0.f, dhiw[3] = {0.f, 0.f, 0.f};
   if (!ELASTIC) {
     const float cc0 = tab[24 + 2 * t], cc1 = tab[25 + 2 * t];
-    const float hw = awp_qf_weight(0.0625f * sum8(a.qs), wwo, cc0, cc1, a.qthr);
-    const float qpaw = awp_qf_weight(0.0625f * sum8(a.qp), wwo, cc0, cc1, a.qthr);
+    const float qs8 = 0.0625f * sum8(a.qs), qp8 = 0.0625f * sum8(a.qp);
+    const float hw = awp_qf_weight(qs8, wwo, cc0, cc1, a.qthr);
+    const float qpaw = awp_qf_weight(qp8, wwo, cc0, cc1, a.qthr);
     const float* qs = a.qs + p;
-    const float hiw[3] = {awp_qf_weight(0.25f * (qs[0] + qs[-1]), wwo, cc0, cc1, a.qthr),
-                          awp_qf_weight(0.25f * (qs[0] + qs[-Y]), wwo, cc0, cc1, a.qthr),
-                          awp_qf_weight(0.25f * (qs[0] + qs[S]), wwo, cc0, cc1, a.qthr)};
+    const float qsp[3] = {0.25f * (qs[0] + qs[-1]), 0.25f * (qs[0] + qs[-Y]),
+                          0.25f * (qs[0] + qs[S])};
+    const float hiw[3] = {awp_qf_weight(qsp[0], wwo, cc0, cc1, a.qthr),
+                          awp_qf_weight(qsp[1], wwo, cc0, cc1, a.qthr),
+                          awp_qf_weight(qsp[2], wwo, cc0, cc1, a.qthr)};
+    dhw = qf_dweight(qs8, wwo, cc0, cc1, a.qthr);
+    dqpaw = qf_dweight(qp8, wwo, cc0, cc1, a.qthr);
+    for (int q = 0; q < 3; ++q) dhiw[q] = qf_dweight(qsp[q], wwo, cc0, cc1, a.qthr);
     c_h = -hw * a.dh1 * fvx1;
     c_xm = a.dth + DT * c_h;
     c_q = -qpaw * a.dh1 * fvx1;
@@ -151,8 +169,10 @@ __global__ void __launch_bounds__(128, 7) k_adj_stress_cell(const AdjArgs a) {
     for (int q = 0; q < 6; ++q) rv[q] = a.L[LR1 + q][p];
   // material weights, summed over the time steps (their spatial transposes
   // are linear and time-invariant, so k_adj_material applies them once)
-  float wacc[5];
+  float wacc[5], qacc[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
   for (int q = 0; q < 5; ++q) wacc[q] = a.E[GL8 + q][p];
+  if (!ELASTIC)
+    for (int q = 0; q < 5; ++q) qacc[q] = a.E[GQP8 + q][p];
   // normal components
   float PX, PY, PZ, QX = 0.f, QY = 0.f, QZ = 0.f;
   PX = K * lx;
@@ -173,7 +193,8 @@ __global__ void __launch_bounds__(128, 7) k_adj_stress_cell(const AdjArgs a) {
 
   // shear components
   const float es[3] = {e4, e5, e6};
-  float GP[3], ES[3];
+  const float mraw[3] = {m1_raw, m2_raw, m3_raw};
+  float GP[3], ES[3], GQP[3];
   for (int q = 0; q < 3; ++q) {
     const float l = ls[q], lrv = rv[3 + q];
     ES[q] = (xmu[q] + DT * hh[q] * (wwo - 1.0f)) * K * l + wwo * hh[q] * lrv;
@@ -181,6 +202,8 @@ __global__ void __launch_bounds__(128, 7) k_adj_stress_cell(const AdjArgs a) {
     const float G_hq = es[q] * (DT * (wwo - 1.0f) * K * l + wwo * lrv);
     const float Pq = q == 0 ? P1 : (q == 1 ? P2 : P3);
     GP[q] = -2.0f / (Pq * Pq) * (G_xmu * c_m[q] + G_hq * c_hh[q]);
+    // Qs^-1 pair: hh = m_raw c_hh, xmu = m_raw (dth + DT c_hh), c_hh = -hiw dh1 vx1
+    GQP[q] = (G_hq + DT * G_xmu) * mraw[q] * (-a.dh1 * fvx1) * dhiw[q] * 0.25f;
   }
 
   // stores: the adjoint state in place, then the temporaries
@@ -209,6 +232,15 @@ __global__ void __launch_bounds__(128, 7) k_adj_stress_cell(const AdjArgs a) {
   E[GP1][p] = wacc[2] + GP[0];
   E[GP2][p] = wacc[3] + GP[1];
   E[GP3][p] = wacc[4] + GP[2];
+  if (!ELASTIC) {
+    // Qp^-1 eight-cell sum: qpa = xl_raw c_q, c_q = -qpaw dh1 vx1
+    E[GQP8][p] = qacc[0] + G_qpa * xl_raw * (-a.dh1 * fvx1) * dqpaw * 0.0625f;
+    // Qs^-1 eight-cell sum: h = xm_raw c_h, xm = xm_raw (dth + DT c_h)
+    E[GQS8][p] = qacc[1] + (G_h + DT * G_xm) * xm_raw * (-a.dh1 * fvx1) * dhw * 0.0625f;
+    E[GQ1][p] = qacc[2] + GQP[0];
+    E[GQ2][p] = qacc[3] + GQP[1];
+    E[GQ3][p] = qacc[4] + GQP[2];
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -474,6 +506,11 @@ __global__ void k_adj_material(const AdjArgs a, int i0, int j0, int k0, int ni, 
   a.glam[q] = box(a.E[GL8]);
   a.gmu[q] = box(a.E[GM8]) + a.E[GP1][q] + a.E[GP1][q + 1] + a.E[GP2][q] + a.E[GP2][q + Y] +
              a.E[GP3][q] + a.E[GP3][q - S];
+  if (a.gqp) {  // the inverse quality factors follow the same averages
+    a.gqp[q] = box(a.E[GQP8]);
+    a.gqs[q] = box(a.E[GQS8]) + a.E[GQ1][q] + a.E[GQ1][q + 1] + a.E[GQ2][q] +
+               a.E[GQ2][q + Y] + a.E[GQ3][q] + a.E[GQ3][q - S];
+  }
   const float* ea = a.V[VEA];
   const float* eb = a.V[VEB];
   const float* ec = a.V[VEC];
@@ -547,6 +584,51 @@ __global__ void k_adj_fold(const AdjArgs a, float* g_lambda, float* g_mu, float*
   g_lambda[c] = g_l;
   g_mu[c] = g_m;
   g_rho[c] = gr;
+}
+
+// padded Qp^-1 / Qs^-1 gradients -> interior cells, border-fill copies folded
+__global__ void k_adj_fold_q(const AdjArgs a, float* g_qp, float* g_qs) {
+  const long long n = (long long)a.g.nxt * a.g.nyt * a.g.nzt;
+  const long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  const int x = (int)(c % a.g.nxt), y = (int)((c / a.g.nxt) % a.g.nyt),
+            z = (int)(c / ((long long)a.g.nxt * a.g.nyt));
+  const int lo = 2 + AWP_NGSL, hix = a.g.nxt + 1 + AWP_NGSL, hiy = a.g.nyt + 1 + AWP_NGSL;
+  const int kb = AWP_ALIGN, kt = a.g.nzt + AWP_ALIGN - 1;
+  const int i = x + lo, j = y + lo, k = kt - z;
+  int is[2] = {i, 0}, js[2] = {j, 0}, ks[2] = {k, 0};
+  int ni = 1, nj = 1, nk = 1;
+  if (i == lo) is[ni++] = lo - 1;
+  if (i == hix) is[ni++] = hix + 1;
+  if (j == lo) js[nj++] = lo - 1;
+  if (j == hiy) js[nj++] = hiy + 1;
+  if (k == kb) ks[nk++] = kb - 1;
+  if (k == kt) ks[nk++] = kt + 1;
+  float gp = 0.f, gs = 0.f;
+  for (int ii = 0; ii < ni; ++ii)
+    for (int jj = 0; jj < nj; ++jj)
+      for (int kk = 0; kk < nk; ++kk) {
+        const long long p = (long long)is[ii] * a.g.slice + (long long)js[jj] * a.g.yline + ks[kk];
+        gp += a.gqp[p];
+        gs += a.gqs[p];
+      }
+  g_qp[c] = gp;
+  g_qs[c] = gs;
+}
+
+__global__ void k_set_qinv(const float* qpinv, const float* qsinv, float* qp, float* qs,
+                           const AwpGeom g) {
+  const int lo = 2 + AWP_NGSL, hix = g.nxt + 1 + AWP_NGSL, hiy = g.nyt + 1 + AWP_NGSL;
+  const int kb = AWP_ALIGN, kt = g.nzt + AWP_ALIGN - 1;
+  const int k = kb - 1 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = lo - 1 + blockIdx.y;
+  const int i = lo - 1 + blockIdx.z;
+  if (k > kt + 1 || j > hiy + 1 || i > hix + 1) return;
+  const int ci = min(max(i, lo), hix), cj = min(max(j, lo), hiy), ck = min(max(k, kb), kt);
+  const long long c = (long long)(kt - ck) * g.nxt * g.nyt + (long long)(cj - lo) * g.nxt + (ci - lo);
+  const long long p = (long long)i * g.slice + (long long)j * g.yline + k;
+  qp[p] = qpinv[c];
+  qs[p] = qsinv[c];
 }
 
 __global__ void k_set_moduli(const float* lambda, const float* mu_, const float* rho, float* lam,
@@ -652,5 +734,20 @@ cudaError_t awp_launch_set_moduli(const float* lambda, const float* mu_, const f
                                   cudaStream_t st) {
   const dim3 grid(cdiv(g.nzt + 2, 64), g.nyt + 2, g.nxt + 2);
   k_set_moduli<<<grid, 64, 0, st>>>(lambda, mu_, rho, lam, mu, d1, g);
+  return cudaGetLastError();
+}
+
+cudaError_t awp_launch_adjoint_fold_q(const AdjArgs& a, float* g_qpinv, float* g_qsinv,
+                                      cudaStream_t st) {
+  if (!a.gqp || !a.gqs) return cudaErrorInvalidValue;
+  const long long n = (long long)a.g.nxt * a.g.nyt * a.g.nzt;
+  k_adj_fold_q<<<cdiv(n, 256), 256, 0, st>>>(a, g_qpinv, g_qsinv);
+  return cudaGetLastError();
+}
+
+cudaError_t awp_launch_set_qinv(const float* qpinv, const float* qsinv, float* qp, float* qs,
+                                const AwpGeom& g, cudaStream_t st) {
+  const dim3 grid(cdiv(g.nzt + 2, 64), g.nyt + 2, g.nxt + 2);
+  k_set_qinv<<<grid, 64, 0, st>>>(qpinv, qsinv, qp, qs, g);
   return cudaGetLastError();
 }

@@ -25,18 +25,19 @@ struct AdjArgs {
   // adjoint state, updated in place (u v w xx yy zz xy xz yz r1..r6)
   float* L[15];
   // temporaries (zero outside the ranges that write them)
-  // stress half: adjoint strain rates (6) and material weights (5); velocity
-  // half: weighted adjoint velocities (3) and density weights (3).  The
-  // weights are summed over the steps and turned into gradients once, by
-  // awp_launch_adjoint_fold.
-  float* E[11];
+  // stress half: adjoint strain rates (6), material weights of the moduli (5)
+  // and of the inverse quality factors (5: the Qp^-1 and Qs^-1 eight-cell
+  // sums and the three Qs^-1 pair sums); velocity half: weighted adjoint
+  // velocities (3) and density weights (3).  The weights are summed over the
+  // steps and turned into gradients once, by awp_launch_adjoint_fold.
+  float* E[16];
   float* V[6];
   // image-adjoint increments of the surface columns and their one-column
   // ring: 4 planes of (si1 - si0 + 3) x (sj1 - sj0 + 3), (i, j) row-major
   float* img;
-  // gradients on the padded kernel arrays: rho, 1/lambda, 1/mu, and the
-  // surface Lame ratio lam_mu (2-D)
-  float *gd, *glam, *gmu, *glm;
+  // gradients on the padded kernel arrays: rho, 1/lambda, 1/mu, Qp^-1,
+  // Qs^-1, and the surface Lame ratio lam_mu (2-D)
+  float *gd, *glam, *gmu, *gqp, *gqs, *glm;
   // media and constants of the forward step
   const float *d1, *lam, *mu, *qp, *qs, *lam_mu;
   const float *dcrjx, *dcrjy, *dcrjz;
@@ -76,6 +77,15 @@ cudaError_t awp_launch_sample(const float* u, const float* v, const float* w,
 // chained through.
 cudaError_t awp_launch_adjoint_fold(const AdjArgs& a, float* g_lambda, float* g_mu,
                                     float* g_rho, cudaStream_t st);
+// The summed Q weights -> interior gradients with respect to Qp^-1 and Qs^-1
+// (layout [nz][ny][nx], surface first), the border-fill copies folded back.
+// Runs after awp_launch_adjoint_fold (which forms the padded gradients).
+cudaError_t awp_launch_adjoint_fold_q(const AdjArgs& a, float* g_qpinv, float* g_qsinv,
+                                      cudaStream_t st);
+// Qp^-1 and Qs^-1 from interior arrays into the padded kernel arrays, one-cell
+// border included.
+cudaError_t awp_launch_set_qinv(const float* qpinv, const float* qsinv, float* qp, float* qs,
+                                const AwpGeom& g, cudaStream_t st);
 
 // Moduli and density from interior arrays ([nz][ny][nx], surface first) into
 // the padded kernel arrays (1/lambda, 1/mu, rho), one-cell border included.

@@ -96,6 +96,10 @@ struct awp_ctx {
   awp::TopoMetrics* topo = nullptr;  // host metrics (point-set set-up)
   float* d_topo = nullptr;           // f arrays then g arrays, one allocation
   TopoArgs targs{};                  // device pointers and constants
+  // NVE 3 on a curvilinear top grid: 0 = the reference's single-rank
+  // behaviour (only the middle band is stress-updated, Cartesian), 1 = the
+  // curvilinear stress everywhere before the plasticity return
+  int topo_plastic_consistent = 0;
   // adjoint workspace, kept between gradient calls of the same size
   float* adj_slab = nullptr;
   size_t adj_slab_floats = 0;
@@ -370,7 +374,36 @@ int phase_velocity(awp_ctx* c) {
   return AWP_OK;
 }
 
+// Middle band of the NVE = 3 stress split at one rank: xss2..xse2 x
+// yls2..yre2 (pmcl3d.c:573-631; ylsp = yls, yrep = yre at one rank).
+void middle_band(const awp_ctx* c, int* i0, int* i1, int* j0, int* j1) {
+  const int yls = c->yls, yre = c->yre;
+  int yls2 = (int)(yls + (int)(yre - yls) * 0.25);
+  if (yls2 % 2 != 0) yls2 += 1;
+  int yre2 = (int)(yls + (int)(yre - yls) * 0.75);
+  if (yre2 % 2 == 0) yre2 -= 1;
+  *i0 = AWP_NGSL + 4;
+  *i1 = c->g.nxt + AWP_NGSL - 1;
+  *j0 = std::max(yls2, yls + AWP_NGSL + 2);
+  *j1 = std::min(yre2, yre - AWP_NGSL - 2);
+}
+
 int phase_stress(awp_ctx* c) {
+  if (c->topo && c->p.nve == 3 && !c->topo_plastic_consistent) {
+    // The reference at one rank with NVE = 3 on a curvilinear grid 0: the
+    // band dstrqc_H loops start at grid `usetopo` (pmcl3d.c:1858-1879), the
+    // interior topography stress belongs to the NVE < 3 branch (:1855) and
+    // topo_stress_left/right_H return without a left/right neighbour rank
+    // (src/topography/stress_attenuation.cu:323-325, 430-432); what remains
+    // is the Cartesian dstrqc_H over the middle band of the plasticity
+    // section (pmcl3d.c:2139-2148).
+    PhaseScope ps(c, 1);
+    StrArgs s = make_str_args(c);
+    middle_band(c, &s.i0, &s.i1, &s.j0, &s.j1);
+    CU_TRY(awp_launch_stress(s, c->elastic, c->stream));
+    c->launches++;
+    return AWP_OK;
+  }
   if (c->topo) {  // topo_stress_*_H replace dstrqc on the top grid (pmcl3d.c:1843-1924)
     PhaseScope ps(c, 1);
     CU_TRY(awp_launch_topo_stress(topo_args(c), c->elastic, c->stream));
@@ -519,7 +552,8 @@ int dm_stress(awp_ctx* c) {  // dstrqc2 over xss1..xse3 x yls..yre (pmcl3d.c:193
 struct awp_mesh {
   int ngrids = 0;
   awp_ctx* g[AWP_MAXGRIDS] = {};
-  cudaStream_t stream = nullptr;
+  cudaStream_t stream = nullptr;      // the stream every block runs on
+  cudaStream_t own_stream = nullptr;  // created with the mesh, destroyed with it
   bool prepared = false;
 };
 
@@ -1203,8 +1237,19 @@ int awp_mesh_destroy(awp_mesh* m) {
   if (!m) return AWP_OK;
   if (m->stream) cudaStreamSynchronize(m->stream);
   for (int p = 0; p < m->ngrids; ++p) awp_ctx_destroy(m->g[p]);
-  if (m->stream) cudaStreamDestroy(m->stream);
+  if (m->own_stream) cudaStreamDestroy(m->own_stream);
   delete m;
+  return AWP_OK;
+}
+
+int awp_mesh_set_stream(awp_mesh* m, void* stream) {
+  if (!m) return set_error(AWP_ERR_ARG, "null mesh");
+  CU_TRY(cudaStreamSynchronize(m->stream));
+  m->stream = static_cast<cudaStream_t>(stream);
+  for (int p = 0; p < m->ngrids; ++p) {
+    const int st = awp_set_stream(m->g[p], stream);
+    if (st) return st;
+  }
   return AWP_OK;
 }
 
@@ -1228,11 +1273,12 @@ int awp_mesh_create(const awp_params* grids, int ngrids, awp_mesh** out) {
       return set_error(AWP_ERR_ARG, "grid %d: NZ too small for the interface", p);
   }
   awp_mesh* m = new awp_mesh();
-  cudaError_t e = cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking);
+  cudaError_t e = cudaStreamCreateWithFlags(&m->own_stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) {
     delete m;
     return set_error(AWP_ERR_CUDA, "cudaStreamCreate: %s", cudaGetErrorString(e));
   }
+  m->stream = m->own_stream;
   for (int p = 0; p < ngrids; ++p) {
     int st = awp_ctx_create(&grids[p], &m->g[p]);
     if (st) {
@@ -1692,6 +1738,13 @@ int awp_batch_info(awp_batch* b, long long info[6]) {
   return AWP_OK;
 }
 
+int awp_set_topo_plasticity(awp_ctx* c, int consistent) {
+  if (!c || (consistent != 0 && consistent != 1))
+    return set_error(AWP_ERR_ARG, "null context or mode not 0/1");
+  c->topo_plastic_consistent = consistent;
+  return AWP_OK;
+}
+
 int awp_topography_init(awp_ctx* c, const char* intopo) {
   if (!c || !intopo) return set_error(AWP_ERR_ARG, "null argument");
   if (c->topo) return set_error(AWP_ERR_STATE, "topography already initialised");
@@ -1819,14 +1872,33 @@ int awp_set_moduli(awp_ctx* c, const float* lambda, const float* mu, const float
   DevBuf b;
   float *dl = b.f(n), *dm = b.f(n), *dr = b.f(n);
   if (!dl || !dm || !dr) return set_error(AWP_ERR_NOMEM, "moduli staging");
-  CU_TRY(cudaMemcpyAsync(dl, lambda, n * sizeof(float), cudaMemcpyHostToDevice, c->stream));
-  CU_TRY(cudaMemcpyAsync(dm, mu, n * sizeof(float), cudaMemcpyHostToDevice, c->stream));
-  CU_TRY(cudaMemcpyAsync(dr, rho, n * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+  // host or device arrays alike (unified addressing picks the direction)
+  CU_TRY(cudaMemcpyAsync(dl, lambda, n * sizeof(float), cudaMemcpyDefault, c->stream));
+  CU_TRY(cudaMemcpyAsync(dm, mu, n * sizeof(float), cudaMemcpyDefault, c->stream));
+  CU_TRY(cudaMemcpyAsync(dr, rho, n * sizeof(float), cudaMemcpyDefault, c->stream));
   CU_TRY(awp_launch_set_moduli(dl, dm, dr, c->f[AWP_LAM], c->f[AWP_MU], c->f[AWP_D1], c->g,
                                c->stream));
   CU_TRY(awp_launch_lam_mu(c->f[AWP_LAM], c->f[AWP_MU], c->lam_mu, c->g, c->xls, c->xre, c->yls,
                            c->yre, c->stream));
   CU_TRY(cudaStreamSynchronize(c->stream));
+  return AWP_OK;
+}
+
+int awp_set_qinv(awp_ctx* c, const float* qpinv, const float* qsinv) {
+  if (!c || !qpinv || !qsinv) return set_error(AWP_ERR_ARG, "null argument");
+  if (!c->media_ready) return set_error(AWP_ERR_STATE, "upload media first (layout)");
+  const size_t n = (size_t)c->g.nxt * c->g.nyt * c->g.nzt;
+  bool any = false;
+  for (size_t q = 0; q < n && !any; ++q) any = (qpinv[q] != 0.f) || (qsinv[q] != 0.f);
+  DevBuf b;
+  float *dp = b.f(n), *ds = b.f(n);
+  if (!dp || !ds) return set_error(AWP_ERR_NOMEM, "Q staging");
+  CU_TRY(cudaMemcpyAsync(dp, qpinv, n * sizeof(float), cudaMemcpyDefault, c->stream));
+  CU_TRY(cudaMemcpyAsync(ds, qsinv, n * sizeof(float), cudaMemcpyDefault, c->stream));
+  CU_TRY(awp_launch_set_qinv(dp, ds, c->f[AWP_QP], c->f[AWP_QS], c->g, c->stream));
+  CU_TRY(cudaStreamSynchronize(c->stream));
+  // the elastic specialisation holds exactly when every Q^-1 is zero
+  c->elastic = !any;
   return AWP_OK;
 }
 
@@ -1906,7 +1978,8 @@ static int adjoint_plan(awp_ctx* c, int nsteps, int nsnap, AdjPlan* out) {
     Lh = std::max(1, std::min(Lh, std::max(H, 1)));
     *Lp = Lh;
     *nsegp = H > 0 ? (H + Lh - 1) / Lh : 0;
-    return ((size_t)(*nsegp + 1) * 15 + 15 + 17 + 3) * slab_round(cp) +
+    // snapshots, adjoint state (15), temporaries (16 + 6), gradients (5)
+    return ((size_t)(*nsegp + 1) * 15 + 15 + 22 + 5) * slab_round(cp) +
            ((size_t)(H > 0 ? Lh + 1 : 0) + (size_t)(M > 0 ? M + 1 : 0)) * 3 * slab_round(cv);
   };
   int M = 0;
@@ -1983,6 +2056,14 @@ int awp_adjoint_plan(awp_ctx* c, int nsteps, int nsnap, int* tail_steps, int* se
 int awp_misfit_gradient(awp_ctx* c, int nsteps, int nrec, const int* rec_xyz, const int* rec_comp,
                         const float* d_obs, int nsnap, double* misfit, float* seis,
                         float* g_lambda, float* g_mu, float* g_rho) {
+  return awp_misfit_gradient_q(c, nsteps, nrec, rec_xyz, rec_comp, d_obs, nsnap, misfit, seis,
+                               g_lambda, g_mu, g_rho, nullptr, nullptr);
+}
+
+int awp_misfit_gradient_q(awp_ctx* c, int nsteps, int nrec, const int* rec_xyz,
+                          const int* rec_comp, const float* d_obs, int nsnap, double* misfit,
+                          float* seis, float* g_lambda, float* g_mu, float* g_rho,
+                          float* g_qpinv, float* g_qsinv) {
   int e = check_adjoint_ctx(c);
   if (e) return e;
   if (nsteps < 1 || nrec < 1 || !rec_xyz || !rec_comp || !d_obs || !misfit)
@@ -2074,14 +2155,16 @@ int awp_misfit_gradient(awp_ctx* c, int nsteps, int nrec, const int* rec_xyz, co
   // ---- adjoint state, temporaries, gradients (zeroed) --------------------------------
   AdjArgs a;
   memset(&a, 0, sizeof(a));
-  // adjoint state, temporaries, gradients: 35 consecutive fields of the slab
+  // adjoint state, temporaries, gradients: 42 consecutive fields of the slab
   float* const zero0 = c->adj_slab + slab_next;
   for (int q = 0; q < 15; ++q) a.L[q] = take();
-  for (int q = 0; q < 11; ++q) a.E[q] = take();
+  for (int q = 0; q < 16; ++q) a.E[q] = take();
   for (int q = 0; q < 6; ++q) a.V[q] = take();
   a.gd = take();
   a.glam = take();
   a.gmu = take();
+  a.gqp = take();
+  a.gqs = take();
   CU_TRY(cudaMemsetAsync(zero0, 0, (size_t)(c->adj_slab + slab_next - zero0) * sizeof(float), st));
   if (!(a.glm = b.f((size_t)c->g.nx_pad() * c->g.ny_pad())))
     return set_error(AWP_ERR_NOMEM, "gradients");
@@ -2164,11 +2247,15 @@ int awp_misfit_gradient(awp_ctx* c, int nsteps, int nrec, const int* rec_xyz, co
   // staged in three strain-rate temporaries of the slab, free after the sweep
   // (no allocation per call on a device the workspace nearly fills)
   const size_t ni = (size_t)c->g.nxt * c->g.nyt * c->g.nzt;
-  float *gl = a.E[0], *gm = a.E[1], *gr = a.E[2];
+  float *gl = a.E[0], *gm = a.E[1], *gr = a.E[2], *gqp = a.E[3], *gqs = a.E[4];
   CU_TRY(awp_launch_adjoint_fold(a, gl, gm, gr, st));
-  if (g_lambda) CU_TRY(cudaMemcpyAsync(g_lambda, gl, ni * sizeof(float), cudaMemcpyDeviceToHost, st));
-  if (g_mu) CU_TRY(cudaMemcpyAsync(g_mu, gm, ni * sizeof(float), cudaMemcpyDeviceToHost, st));
-  if (g_rho) CU_TRY(cudaMemcpyAsync(g_rho, gr, ni * sizeof(float), cudaMemcpyDeviceToHost, st));
+  if (g_qpinv || g_qsinv) CU_TRY(awp_launch_adjoint_fold_q(a, gqp, gqs, st));
+  // host or device targets alike (unified addressing picks the direction)
+  if (g_lambda) CU_TRY(cudaMemcpyAsync(g_lambda, gl, ni * sizeof(float), cudaMemcpyDefault, st));
+  if (g_mu) CU_TRY(cudaMemcpyAsync(g_mu, gm, ni * sizeof(float), cudaMemcpyDefault, st));
+  if (g_rho) CU_TRY(cudaMemcpyAsync(g_rho, gr, ni * sizeof(float), cudaMemcpyDefault, st));
+  if (g_qpinv) CU_TRY(cudaMemcpyAsync(g_qpinv, gqp, ni * sizeof(float), cudaMemcpyDefault, st));
+  if (g_qsinv) CU_TRY(cudaMemcpyAsync(g_qsinv, gqs, ni * sizeof(float), cudaMemcpyDefault, st));
   if ((e = restore(nseg))) return e;
   CU_TRY(cudaStreamSynchronize(st));
   return AWP_OK;

@@ -7,8 +7,11 @@
 // reference's single-rank run; the time step itself runs in libawpb200
 // through its C ABI.
 //
-// Scope: one rank (PX = PY = 1, no I/O ranks), one grid, MEDIASTART 0-2,
-// IFAULT 1 and 5, NVE 1 and 3.  Anything else is reported and refused.
+// Scope: one rank (PX = PY = 1, no I/O ranks), one grid or a discontinuous
+// mesh of NGRIDS blocks (each 3x finer than the one below, pmcl3d.c:370-378),
+// MEDIASTART 0-2, IFAULT 1 and 5, NVE 1 and 3.  On a mesh the SOURCEFILE /
+// RECVFILE point sets and the topography belong to the top block (grid 0).
+// Anything else is reported and refused.
 #include <getopt.h>
 #include <math.h>
 #include <stdio.h>
@@ -250,46 +253,60 @@ int main(int argc, char** argv) {
     fprintf(stderr, "pmcl3d: this build runs one rank (PX = PY = 1)\n");
     return 1;
   }
-  if (A.NGRIDS != 1) {
-    fprintf(stderr, "pmcl3d: NGRIDS=%d: discontinuous meshes are not part of this build\n",
-            A.NGRIDS);
+  const int G = A.NGRIDS;
+  if (G < 1 || G > MAXGRIDS) {
+    fprintf(stderr, "pmcl3d: NGRIDS=%d is outside 1..%d\n", G, MAXGRIDS);
     return 1;
   }
   if (A.USEFORCEFILE || A.USESGTFILE) {
     fprintf(stderr, "pmcl3d: FORCEFILE/SGTFILE are not part of this build\n");
     return 1;
   }
-  if (A.NZ[0] % 4 != 0) {  // pmcl3d.c:380-391 (BLOCK_SIZE_Z = 4)
-    fprintf(stderr, "NZT for grid 0 is not divisble by BLOCK_SIZE_Z.\nNZT = %d, BLOCK_SIZE_Z=4\n",
-            A.NZ[0]);
-    return 0;
+  // block sizes of the mesh (pmcl3d.c:370-378): NX, NY, DH are the coarsest
+  // block's, each block above is 3x finer
+  int grdfct[MAXGRIDS], nxt[MAXGRIDS], nyt[MAXGRIDS], nzt[MAXGRIDS];
+  float DHp[MAXGRIDS];
+  grdfct[G - 1] = 1;
+  for (int p = G - 2; p >= 0; --p) grdfct[p] = grdfct[p + 1] * 3;
+  for (int p = 0; p < G; ++p) {
+    DHp[p] = A.DH / grdfct[p];
+    nxt[p] = A.NX * grdfct[p];
+    nyt[p] = A.NY * grdfct[p];
+    nzt[p] = A.NZ[p];
+    if (nzt[p] % 4 != 0) {  // pmcl3d.c:380-391 (BLOCK_SIZE_Z = 4)
+      fprintf(stderr,
+              "NZT for grid %d is not divisble by BLOCK_SIZE_Z.\nNZT = %d, BLOCK_SIZE_Z=4\n", p,
+              nzt[p]);
+      return 0;
+    }
   }
-  const int nxt = A.NX, nyt = A.NY, nzt = A.NZ[0];
   const long nt = (int)(A.TMAX / A.DT) + 1;
 
   // recording points (pmcl3d.c:425-471)
-  int p = 0;
-  if (A.NEDX[p] == -1) A.NEDX[p] = A.NX;
-  if (A.NEDY[p] == -1) A.NEDY[p] = A.NY;
-  if (A.NEDZ[p] == -1) A.NEDZ[p] = A.NZ[p];
-  A.NEDX[p] = A.NEDX[p] - (A.NEDX[p] - A.NBGX[p]) % A.NSKPX[p];
-  A.NEDY[p] = A.NEDY[p] - (A.NEDY[p] - A.NBGY[p]) % A.NSKPY[p];
-  A.NEDZ[p] = A.NEDZ[p] - (A.NEDZ[p] - A.NBGZ[p]) % A.NSKPZ[p];
-  const int recNX = (A.NEDX[p] - A.NBGX[p]) / A.NSKPX[p] + 1;
-  const int recNY = (A.NEDY[p] - A.NBGY[p]) / A.NSKPY[p] + 1;
-  const int recNZ = (A.NEDZ[p] - A.NBGZ[p]) / A.NSKPZ[p] + 1;
-  int rnbgx, rnedx, rnbgy, rnedy, rnbgz, rnedz, rnx, rny, rnz;
-  calc_recording_points(&rnbgx, &rnedx, &rnbgy, &rnedy, &rnbgz, &rnedz, &rnx, &rny, &rnz, nxt,
-                        nyt, nzt, A.NBGX[p], A.NEDX[p], A.NSKPX[p], A.NBGY[p], A.NEDY[p],
-                        A.NSKPY[p], A.NBGZ[p], A.NEDZ[p], A.NSKPZ[p]);
+  int grid_output[MAXGRIDS] = {0}, recNX[MAXGRIDS], recNY[MAXGRIDS], recNZ[MAXGRIDS];
+  int rnbgx[MAXGRIDS], rnedx[MAXGRIDS], rnbgy[MAXGRIDS], rnedy[MAXGRIDS], rnbgz[MAXGRIDS],
+      rnedz[MAXGRIDS], rnx[MAXGRIDS], rny[MAXGRIDS], rnz[MAXGRIDS];
+  for (int p = 0; p < G; ++p) {
+    if (p == 0) {
+      if (A.NEDX[p] == -1) A.NEDX[p] = A.NX * grdfct[p];
+      if (A.NEDY[p] == -1) A.NEDY[p] = A.NY * grdfct[p];
+      if (A.NEDZ[p] == -1) A.NEDZ[p] = A.NZ[p];
+      grid_output[p] = 1;
+    }
+    A.NEDX[p] = A.NEDX[p] - (A.NEDX[p] - A.NBGX[p]) % A.NSKPX[p];
+    A.NEDY[p] = A.NEDY[p] - (A.NEDY[p] - A.NBGY[p]) % A.NSKPY[p];
+    A.NEDZ[p] = A.NEDZ[p] - (A.NEDZ[p] - A.NBGZ[p]) % A.NSKPZ[p];
+    if (A.NEDX[p] > -1 && A.NEDY[p] > -1 && A.NEDZ[p] > -1) grid_output[p] = 1;
+    recNX[p] = (A.NEDX[p] - A.NBGX[p]) / A.NSKPX[p] + 1;
+    recNY[p] = (A.NEDY[p] - A.NBGY[p]) / A.NSKPY[p] + 1;
+    recNZ[p] = (A.NEDZ[p] - A.NBGZ[p]) / A.NSKPZ[p] + 1;
+    calc_recording_points(&rnbgx[p], &rnedx[p], &rnbgy[p], &rnedy[p], &rnbgz[p], &rnedz[p],
+                          &rnx[p], &rny[p], &rnz[p], nxt[p], nyt[p], nzt[p], A.NBGX[p],
+                          A.NEDX[p], A.NSKPX[p], A.NBGY[p], A.NEDY[p], A.NSKPY[p], A.NBGZ[p],
+                          A.NEDZ[p], A.NSKPZ[p]);
+    if (!grid_output[p]) rnx[p] = rny[p] = rnz[p] = 0;
+  }
 
-  awp_params P;
-  awp_params_default(&P);
-  P.nx = nxt; P.ny = nyt; P.nz = nzt;
-  P.dh = A.DH; P.dt = A.DT; P.arbc = A.ARBC; P.npc = A.NPC; P.nd = A.ND;
-  P.nve = (A.NVE == 3) ? 3 : 1;
-  P.fac = A.FAC; P.q0 = A.Q0; P.ex = A.EX; P.fp = A.FP; P.socalq = A.SoCalQ;
-  P.ifault = A.IFAULT; P.nst = A.NST; P.read_step = A.READ_STEP_GPU;
   if (A.IFAULT != 1 && A.IFAULT != 5) {
     fprintf(stderr, "pmcl3d: IFAULT=%d sources are not part of this build\n", A.IFAULT);
     return 1;
@@ -298,8 +315,26 @@ int main(int argc, char** argv) {
     fprintf(stderr, "IFAULT=5 requires NST = READ_STEP =2.\nQuitting.");
     return -1;
   }
-  awp_ctx* ctx = nullptr;
-  AWP(awp_ctx_create(&P, &ctx));
+  awp_params P[MAXGRIDS];
+  for (int p = 0; p < G; ++p) {
+    awp_params_default(&P[p]);
+    P[p].nx = nxt[p]; P[p].ny = nyt[p]; P[p].nz = nzt[p];
+    P[p].dh = DHp[p]; P[p].dt = A.DT; P[p].arbc = A.ARBC; P[p].npc = A.NPC;
+    P[p].nd = A.ND * grdfct[p];  // inicrj with ND*grdfct[p] (pmcl3d.c:1029)
+    P[p].nve = (A.NVE == 3) ? 3 : 1;
+    P[p].fac = A.FAC; P[p].q0 = A.Q0; P[p].ex = A.EX; P[p].fp = A.FP; P[p].socalq = A.SoCalQ;
+    P[p].ifault = A.IFAULT; P[p].nst = A.NST; P[p].read_step = A.READ_STEP_GPU;
+    P[p].grid = p;
+    P[p].ngrids = G;
+  }
+  awp_mesh* mesh = nullptr;
+  awp_ctx* ctx[MAXGRIDS] = {};
+  if (G == 1) {
+    AWP(awp_ctx_create(&P[0], &ctx[0]));
+  } else {
+    AWP(awp_mesh_create(P, G, &mesh));
+    for (int p = 0; p < G; ++p) AWP(awp_mesh_grid(mesh, p, &ctx[p]));
+  }
 
   // ---- sources (inisource, source.c:131-264; sourcefilter.dat, pmcl3d.c:651-675)
   int filtorder = 0;
@@ -313,85 +348,90 @@ int main(int argc, char** argv) {
       printf("b[%d]=%le, a[%d]=%le\n", k, fb[k], k, fa[k]);
     }
     fclose(f);
-    AWP(awp_set_source_filter(ctx, filtorder, fb, fa));
+    for (int p = 0; p < G; ++p) AWP(awp_set_source_filter(ctx[p], filtorder, fb, fa));
   }
-  std::vector<int> spos;
-  std::vector<float> sdat;
-  int nsrc = 0;
-  if (A.NSRC[0] > 0) {
+  std::vector<int> spos[MAXGRIDS];
+  int nsrc[MAXGRIDS] = {0};
+  for (int p = 0; p < G; ++p) {  // INSRC_<p> for every block with sources (pmcl3d.c:702-708)
+    if (A.NSRC[p] <= 0) continue;
     char name[512];
-    snprintf(name, sizeof(name), "%s_%d", A.INSRC.c_str(), 0);
+    snprintf(name, sizeof(name), "%s_%d", A.INSRC.c_str(), p);
     FILE* f = fopen(name, "rb");
     if (!f) {
       printf("can't open file %s", name);
-    } else {
-      std::vector<float> tmp((size_t)A.NST * 6);
-      const int rs = A.READ_STEP_GPU;
-      for (int i = 0; i < A.NSRC[0]; ++i) {
-        int t3[3];
-        if (fread(t3, sizeof(int), 3, f) != 3 ||
-            fread(tmp.data(), sizeof(float), tmp.size(), f) != tmp.size())
-          break;
-        spos.insert(spos.end(), t3, t3 + 3);
-        for (int j = 0; j < rs; ++j)
-          for (int q = 0; q < 6; ++q) sdat.push_back(j < A.NST ? tmp[(size_t)j * 6 + q] : 0.f);
-        ++nsrc;
-      }
-      fclose(f);
+      continue;
     }
-    if (nsrc) AWP(awp_upload_sources(ctx, nsrc, spos.data(), sdat.data()));
+    std::vector<float> tmp((size_t)A.NST * 6), sdat;
+    const int rs = A.READ_STEP_GPU;
+    for (int i = 0; i < A.NSRC[p]; ++i) {
+      int t3[3];
+      if (fread(t3, sizeof(int), 3, f) != 3 ||
+          fread(tmp.data(), sizeof(float), tmp.size(), f) != tmp.size())
+        break;
+      spos[p].insert(spos[p].end(), t3, t3 + 3);
+      for (int j = 0; j < rs; ++j)
+        for (int q = 0; q < 6; ++q) sdat.push_back(j < A.NST ? tmp[(size_t)j * 6 + q] : 0.f);
+      ++nsrc[p];
+    }
+    fclose(f);
+    if (nsrc[p]) AWP(awp_upload_sources(ctx[p], nsrc[p], spos[p].data(), sdat.data()));
   }
   if (A.IFAULT == 5) printf("Using IFAULT=5: kinematic source.\n");
 
-  // ---- media (inimesh, mesh.c:23-614) ---------------------------------------
-  float vse[2] = {0, 0}, vpe[2] = {0, 0}, dde[2] = {0, 0};
-  long long dims[3];
-  AWP(awp_padded_dims(ctx, dims));
-  const size_t ncell = (size_t)dims[0] * dims[1] * dims[2];
-  if (A.MEDIASTART == 0) {
-    float vp, vs, dd;
-    if (A.IDYNA == 1) vp = 6000.0, vs = 3464.0, dd = 2670.0;
-    else vp = 1500.0, vs = 500.0, dd = 2000.0;
-    std::vector<float> lam(ncell, (float)(1. / (dd * (vp * vp - 2. * vs * vs)))),
-        mu(ncell, (float)(1. / (dd * vs * vs))), d1(ncell, dd);
-    AWP(awp_field_upload(ctx, AWP_D1, d1.data()));
-    AWP(awp_field_upload(ctx, AWP_MU, mu.data()));
-    AWP(awp_field_upload(ctx, AWP_LAM, lam.data()));
-    vse[0] = vse[1] = vs; vpe[0] = vpe[1] = vp; dde[0] = dde[1] = dd;
-  } else if (A.MEDIASTART == 1 || A.MEDIASTART == 2) {
-    char name[512];
-    snprintf(name, sizeof(name), "%s_%d", A.INVEL.c_str(), 0);
-    const size_t n = (size_t)A.NVAR * nxt * nyt * nzt;
-    std::vector<float> m(n);
-    FILE* f = fopen(name, "rb");
-    if (!f || fread(m.data(), sizeof(float), n, f) != n) {
-      printf("can't open file %s", name);
+  // ---- media (inimesh, mesh.c:23-614), INVEL_<p> per block (pmcl3d.c:882-892) ---
+  float vse[MAXGRIDS][2] = {}, vpe[MAXGRIDS][2] = {}, dde[MAXGRIDS][2] = {};
+  size_t ncell[MAXGRIDS];
+  long long dims[MAXGRIDS][3];
+  for (int p = 0; p < G; ++p) {
+    AWP(awp_padded_dims(ctx[p], dims[p]));
+    ncell[p] = (size_t)dims[p][0] * dims[p][1] * dims[p][2];
+    if (A.MEDIASTART == 0) {
+      float vp, vs, dd;
+      if (A.IDYNA == 1) vp = 6000.0, vs = 3464.0, dd = 2670.0;
+      else vp = 1500.0, vs = 500.0, dd = 2000.0;
+      std::vector<float> lam(ncell[p], (float)(1. / (dd * (vp * vp - 2. * vs * vs)))),
+          mu(ncell[p], (float)(1. / (dd * vs * vs))), d1(ncell[p], dd);
+      AWP(awp_field_upload(ctx[p], AWP_D1, d1.data()));
+      AWP(awp_field_upload(ctx[p], AWP_MU, mu.data()));
+      AWP(awp_field_upload(ctx[p], AWP_LAM, lam.data()));
+      vse[p][0] = vse[p][1] = vs; vpe[p][0] = vpe[p][1] = vp; dde[p][0] = dde[p][1] = dd;
+    } else if (A.MEDIASTART == 1 || A.MEDIASTART == 2) {
+      char name[512];
+      snprintf(name, sizeof(name), "%s_%d", A.INVEL.c_str(), p);
+      const size_t n = (size_t)A.NVAR * nxt[p] * nyt[p] * nzt[p];
+      std::vector<float> m(n);
+      FILE* f = fopen(name, "rb");
+      if (!f || fread(m.data(), sizeof(float), n, f) != n) {
+        printf("can't open file %s", name);
+        return 1;
+      }
+      fclose(f);
+      AWP(awp_upload_media(ctx[p], A.NVAR, m.data()));
+      AWP(awp_media_extrema(ctx[p], vse[p], vpe[p], dde[p]));
+    } else {
+      fprintf(stderr, "pmcl3d: MEDIASTART=%d (partitioned meshes) is not part of this build\n",
+              A.MEDIASTART);
       return 1;
     }
-    fclose(f);
-    AWP(awp_upload_media(ctx, A.NVAR, m.data()));
-    AWP(awp_media_extrema(ctx, vse, vpe, dde));
-  } else {
-    fprintf(stderr, "pmcl3d: MEDIASTART=%d (partitioned meshes) is not part of this build\n",
-            A.MEDIASTART);
-    return 1;
   }
 
   // ---- CHK statistics file (writeCHK, io.c:9-43) -----------------------------
   FILE* fchk = fopen(A.CHKFILE.c_str(), "w");
   if (fchk) {
-    fprintf(fchk, "-------------------------------------------------------------\n");
-    fprintf(fchk, "GRID NUMBER:\t%d\n", 0);
-    fprintf(fchk, "STABILITY CRITERIA .5 > CMAX*DT/DX:\t%f\n", vpe[1] * A.DT / A.DH);
-    fprintf(fchk, "# OF X,Y,Z NODES PER PROC:\t%d, %d, %d\n", nxt, nyt, nzt);
-    fprintf(fchk, "DISCRETIZATION IN SPACE:\t%f\n", A.DH);
-    fprintf(fchk, "HIGHEST P-VELOCITY ENCOUNTERED:\t%f\n", vpe[1]);
-    fprintf(fchk, "LOWEST P-VELOCITY ENCOUNTERED:\t%f\n", vpe[0]);
-    fprintf(fchk, "HIGHEST S-VELOCITY ENCOUNTERED:\t%f\n", vse[1]);
-    fprintf(fchk, "LOWEST S-VELOCITY ENCOUNTERED:\t%f\n", vse[0]);
-    fprintf(fchk, "HIGHEST DENSITY ENCOUNTERED:\t%f\n", dde[1]);
-    fprintf(fchk, "LOWEST  DENSITY ENCOUNTERED:\t%f\n", dde[0]);
-    fprintf(fchk, "-------------------------------------------------------------\n");
+    for (int p = 0; p < G; ++p) {
+      fprintf(fchk, "-------------------------------------------------------------\n");
+      fprintf(fchk, "GRID NUMBER:\t%d\n", p);
+      fprintf(fchk, "STABILITY CRITERIA .5 > CMAX*DT/DX:\t%f\n", vpe[p][1] * A.DT / DHp[p]);
+      fprintf(fchk, "# OF X,Y,Z NODES PER PROC:\t%d, %d, %d\n", nxt[p], nyt[p], nzt[p]);
+      fprintf(fchk, "DISCRETIZATION IN SPACE:\t%f\n", DHp[p]);
+      fprintf(fchk, "HIGHEST P-VELOCITY ENCOUNTERED:\t%f\n", vpe[p][1]);
+      fprintf(fchk, "LOWEST P-VELOCITY ENCOUNTERED:\t%f\n", vpe[p][0]);
+      fprintf(fchk, "HIGHEST S-VELOCITY ENCOUNTERED:\t%f\n", vse[p][1]);
+      fprintf(fchk, "LOWEST S-VELOCITY ENCOUNTERED:\t%f\n", vse[p][0]);
+      fprintf(fchk, "HIGHEST DENSITY ENCOUNTERED:\t%f\n", dde[p][1]);
+      fprintf(fchk, "LOWEST  DENSITY ENCOUNTERED:\t%f\n", dde[p][0]);
+      fprintf(fchk, "-------------------------------------------------------------\n");
+    }
     fprintf(fchk, "# OF TIME STEPS:\t%ld\n", nt);
     fprintf(fchk, "DISCRETIZATION IN TIME:\t%f\n", A.DT);
     fprintf(fchk, "PML REFLECTION COEFFICIENT:\t%f\n", A.ARBC);
@@ -403,15 +443,10 @@ int main(int argc, char** argv) {
     fclose(fchk);
   }
 
-  // ---- plasticity set-up (inidrpr_hoekbrown_light, mesh.c:1178-1401) ----------
+  // ---- plasticity set-up per block (inidrpr_hoekbrown_light, mesh.c:1178-1401) --
   if (A.NVE == 3) {
-    std::vector<float> d1(ncell), mu(ncell), lam(ncell), sigma2(ncell, 0.f), cohes(ncell, 0.f),
-        phi(ncell, 0.f);
-    AWP(awp_field_download(ctx, AWP_D1, d1.data()));
-    AWP(awp_field_download(ctx, AWP_MU, mu.data()));
-    AWP(awp_field_download(ctx, AWP_LAM, lam.data()));
-    float strike[3] = {0, 0, 0}, dip[3] = {0, 90, 0}, fmajor = 0, fminor = 0, sigma_ci = 0, GSI = 0,
-          mi = 0, gsi100 = 1;
+    float strike[3] = {0, 0, 0}, dip[3] = {0, 90, 0}, fmajor = 0, fminor = 0, sigma_ci0 = 0,
+          GSI = 0, mi = 0, gsi100 = 1;
     int sigma_ci_type = 0, fltpos = 0;
     FILE* fid = fopen("nonlinear.dat", "r");
     if (!fid) {
@@ -421,96 +456,118 @@ int main(int argc, char** argv) {
     char line[512];
     if (fgets(line, sizeof line, fid)) sscanf(line, "%f %f", strike, strike + 2);
     if (fgets(line, sizeof line, fid)) sscanf(line, "%f %f", &fmajor, &fminor);
-    if (fgets(line, sizeof line, fid)) sscanf(line, "%d %f", &sigma_ci_type, &sigma_ci);
+    if (fgets(line, sizeof line, fid)) sscanf(line, "%d %f", &sigma_ci_type, &sigma_ci0);
     if (fgets(line, sizeof line, fid)) sscanf(line, "%f", &GSI);
     if (fgets(line, sizeof line, fid)) sscanf(line, "%f", &mi);
     if (fgets(line, sizeof line, fid)) sscanf(line, "%f", &gsi100);
     if (fgets(line, sizeof line, fid)) sscanf(line, "%d", &fltpos);
     fclose(fid);
-    const long S = dims[1] * dims[2], Y = dims[2];
-    auto at = [&](int i, int j, int k) { return (size_t)(i * S + j * Y + k); };
-    const int sInd = nzt + ALIGN - 1;
-    const float dh = A.DH;
-    for (int j = 2; j < nyt + 2 + 2 * NGSL; j++)
-      for (int i = 2; i < nxt + 2 + 2 * NGSL; i++) {
-        sigma2[at(i, j, sInd)] = -dh / 2. * d1[at(i, j, sInd)] * 9.81;
-        sigma2[at(i, j, sInd + 1)] = sigma2[at(i, j, sInd)];
-        for (int k = sInd - 1; k >= ALIGN - 2; k--)
-          sigma2[at(i, j, k)] = sigma2[at(i, j, k + 1)] - dh * d1[at(i, j, k)] * 9.81;
-      }
-    for (int k = ALIGN; k <= sInd + 1; k++)
-      for (int j = 2; j < nyt + 2 + 2 * NGSL; j++)
-        for (int i = 2; i < nxt + 2 + 2 * NGSL; i++) {
-          const float depth = 0.5 * dh + dh * (sInd - k);
-          float GSI_wallrock = GSI + (100. - GSI) * (depth - 0.5 * dh) / gsi100, GSI_core, GSI_d;
-          if (GSI_wallrock > 100) GSI_wallrock = 100;
-          if (depth < 4000.) GSI_core = GSI;
-          else if (depth >= 4000. && depth <= 6000.)
-            GSI_core = GSI + (depth - 4000.) / 2000. * (GSI_wallrock - GSI);
-          else GSI_core = GSI_wallrock;
-          const int ypos = j - 2 - NGSL;
-          const float fltdist = fabsf((float)ypos + 0.5 - (float)fltpos) * dh;
-          if (fltdist < 225.) GSI_d = GSI_core;
-          else if (fltdist >= 225. && fltdist <= 750.)
-            GSI_d = GSI_core + (GSI_wallrock - GSI_core) * (fltdist - 225.) / (750. - 225.);
-          else GSI_d = GSI_wallrock;
-          const size_t q = at(i, j, k);
-          if (sigma_ci_type == 3) {
-            const float tvp = sqrt((1. / lam[q] + 2. / mu[q]) / d1[q]);
-            const float itime = 1. / tvp / 3.28 * 1.e6;
-            sigma_ci = 1.4138e7 * powf(itime, -3.) * 1.e6;
-          } else if (sigma_ci_type == 12) {
-            const float tvp = sqrt((1. / lam[q] + 2. / mu[q]) / d1[q]) / 1.e3;
-            sigma_ci = 0.77 * pow(tvp, 2.93) * 1.e6;
-          }
-          hoek_brown(-sigma2[q], sigma_ci, GSI_d, mi, 0, 1, &phi[q], &cohes[q]);
-          const float tvs = sqrtf(1. / (mu[q] * d1[q]));
-          if (tvs > 2000.) cohes[q] = 1.e12;
-          else if (tvs < 750.) {
-            cohes[q] = 0.f;
-            phi[q] = 35.f;
-          }
+    for (int p = 0; p < G; ++p) {
+      std::vector<float> d1(ncell[p]), mu(ncell[p]), lam(ncell[p]), sigma2(ncell[p], 0.f),
+          cohes(ncell[p], 0.f), phi(ncell[p], 0.f);
+      AWP(awp_field_download(ctx[p], AWP_D1, d1.data()));
+      AWP(awp_field_download(ctx[p], AWP_MU, mu.data()));
+      AWP(awp_field_download(ctx[p], AWP_LAM, lam.data()));
+      const long S = dims[p][1] * dims[p][2], Y = dims[p][2];
+      auto at = [&](int i, int j, int k) { return (size_t)(i * S + j * Y + k); };
+      const int nx = nxt[p], ny = nyt[p], nz = nzt[p];
+      const int sInd = nz + ALIGN - 1;
+      const float dh = DHp[p];
+      float sigma_ci = sigma_ci0;
+      for (int j = 2; j < ny + 2 + 2 * NGSL; j++)
+        for (int i = 2; i < nx + 2 + 2 * NGSL; i++) {
+          sigma2[at(i, j, sInd)] = -dh / 2. * d1[at(i, j, sInd)] * 9.81;
+          sigma2[at(i, j, sInd + 1)] = sigma2[at(i, j, sInd)];
+          for (int k = sInd - 1; k >= ALIGN - 2; k--)
+            sigma2[at(i, j, k)] = sigma2[at(i, j, k + 1)] - dh * d1[at(i, j, k)] * 9.81;
         }
-    // no yielding around source nodes (pmcl3d.c:963-988)
-    for (int s = 0; s < nsrc; ++s) {
-      const int idx = spos[3 * s] + 1 + NGSL, idy = spos[3 * s + 1] + 1 + NGSL;
-      const int idz = (nzt + 1 - spos[3 * s + 2]) + ALIGN - 1;
-      for (int xi = idx - 1; xi < idx + 2; xi++)
-        for (int yi = idy - 2; yi < idy + 2; yi++)
-          for (int zi = idz - 1; zi < idz + 2; zi++) {
-            const bool dox = xi >= 0 && xi < nxt + 2 * NGSL + 1;
-            const bool doy = yi >= 0 && yi < nyt + 2 * NGSL + 1;
-            const bool doz = zi >= 0 && yi < nzt + 2 * NGSL + 1;
-            if (dox && doy && doz) cohes[at(xi, yi, zi)] = 1.e18;
+      for (int k = ALIGN; k <= sInd + 1; k++)
+        for (int j = 2; j < ny + 2 + 2 * NGSL; j++)
+          for (int i = 2; i < nx + 2 + 2 * NGSL; i++) {
+            const float depth = 0.5 * dh + dh * (sInd - k);
+            float GSI_wallrock = GSI + (100. - GSI) * (depth - 0.5 * dh) / gsi100, GSI_core,
+                  GSI_d;
+            if (GSI_wallrock > 100) GSI_wallrock = 100;
+            if (depth < 4000.) GSI_core = GSI;
+            else if (depth >= 4000. && depth <= 6000.)
+              GSI_core = GSI + (depth - 4000.) / 2000. * (GSI_wallrock - GSI);
+            else GSI_core = GSI_wallrock;
+            const int ypos = j - 2 - NGSL;
+            const float fltdist = fabsf((float)ypos + 0.5 - (float)fltpos) * dh;
+            if (fltdist < 225.) GSI_d = GSI_core;
+            else if (fltdist >= 225. && fltdist <= 750.)
+              GSI_d = GSI_core + (GSI_wallrock - GSI_core) * (fltdist - 225.) / (750. - 225.);
+            else GSI_d = GSI_wallrock;
+            const size_t q = at(i, j, k);
+            if (sigma_ci_type == 3) {
+              const float tvp = sqrt((1. / lam[q] + 2. / mu[q]) / d1[q]);
+              const float itime = 1. / tvp / 3.28 * 1.e6;
+              sigma_ci = 1.4138e7 * powf(itime, -3.) * 1.e6;
+            } else if (sigma_ci_type == 12) {
+              const float tvp = sqrt((1. / lam[q] + 2. / mu[q]) / d1[q]) / 1.e3;
+              sigma_ci = 0.77 * pow(tvp, 2.93) * 1.e6;
+            }
+            hoek_brown(-sigma2[q], sigma_ci, GSI_d, mi, 0, 1, &phi[q], &cohes[q]);
+            const float tvs = sqrtf(1. / (mu[q] * d1[q]));
+            if (tvs > 2000.) cohes[q] = 1.e12;
+            else if (tvs < 750.) {
+              cohes[q] = 0.f;
+              phi[q] = 35.f;
+            }
           }
+      // no yielding around source nodes (pmcl3d.c:963-988)
+      for (int s = 0; s < nsrc[p]; ++s) {
+        const int idx = spos[p][3 * s] + 1 + NGSL, idy = spos[p][3 * s + 1] + 1 + NGSL;
+        const int idz = (nz + 1 - spos[p][3 * s + 2]) + ALIGN - 1;
+        for (int xi = idx - 1; xi < idx + 2; xi++)
+          for (int yi = idy - 2; yi < idy + 2; yi++)
+            for (int zi = idz - 1; zi < idz + 2; zi++) {
+              const bool dox = xi >= 0 && xi < nx + 2 * NGSL + 1;
+              const bool doy = yi >= 0 && yi < ny + 2 * NGSL + 1;
+              const bool doz = zi >= 0 && yi < nz + 2 * NGSL + 1;
+              if (dox && doy && doz) cohes[at(xi, yi, zi)] = 1.e18;
+            }
+      }
+      AWP(awp_upload_plasticity(ctx[p], sigma2.data(), cohes.data(), phi.data(), fmajor, fminor,
+                                strike, dip));
     }
-    AWP(awp_upload_plasticity(ctx, sigma2.data(), cohes.data(), phi.data(), fmajor, fminor,
-                              strike, dip));
   }
 
   // ---- curvilinear topography of grid 0 (pmcl3d.c:1522-1548) --------------------
-  if (A.USETOPO) AWP(awp_topography_init(ctx, A.INTOPO.c_str()));
+  if (A.USETOPO) AWP(awp_topography_init(ctx[0], A.INTOPO.c_str()));
 
   // ---- SOURCEFILE / RECVFILE point sets (pmcl3d.c:1563-1568, 1603-1607) ---------
-  if (A.USESOURCEFILE) AWP(awp_sourcefile_init(ctx, A.SOURCEFILE.c_str()));
-  if (A.USERECVFILE) AWP(awp_receivers_init(ctx, A.RECVFILE.c_str(), nt));
+  if (A.USESOURCEFILE) AWP(awp_sourcefile_init(ctx[0], A.SOURCEFILE.c_str()));
+  if (A.USERECVFILE) AWP(awp_receivers_init(ctx[0], A.RECVFILE.c_str(), nt));
 
   // ---- output buffers ------------------------------------------------------------
-  const size_t rec = (size_t)rnx * rny * rnz;
-  std::vector<float> Bufx(rec * A.WRITE_STEP), Bufy(rec * A.WRITE_STEP), Bufz(rec * A.WRITE_STEP),
-      Bufeta(A.NVE == 3 ? rec * A.WRITE_STEP : 0);
-  float *d_bx = nullptr, *d_by = nullptr, *d_bz = nullptr, *d_be = nullptr;
-  std::vector<float> stage(rec);
-  if (rec) {
-    // device staging through the library's own allocation-free API is not
-    // needed: the gather writes straight into host-visible pinned memory
-    AWP(awp_alloc_host_pinned((void**)&d_bx, rec * sizeof(float)));
-    AWP(awp_alloc_host_pinned((void**)&d_by, rec * sizeof(float)));
-    AWP(awp_alloc_host_pinned((void**)&d_bz, rec * sizeof(float)));
-    if (A.NVE == 3) AWP(awp_alloc_host_pinned((void**)&d_be, rec * sizeof(float)));
+  size_t rec[MAXGRIDS];
+  std::vector<float> Bufx[MAXGRIDS], Bufy[MAXGRIDS], Bufz[MAXGRIDS], Bufeta[MAXGRIDS];
+  float *d_bx[MAXGRIDS] = {}, *d_by[MAXGRIDS] = {}, *d_bz[MAXGRIDS] = {}, *d_be[MAXGRIDS] = {};
+  for (int p = 0; p < G; ++p) {
+    rec[p] = (size_t)rnx[p] * rny[p] * rnz[p];
+    Bufx[p].resize(rec[p] * A.WRITE_STEP);
+    Bufy[p].resize(rec[p] * A.WRITE_STEP);
+    Bufz[p].resize(rec[p] * A.WRITE_STEP);
+    Bufeta[p].resize(A.NVE == 3 ? rec[p] * A.WRITE_STEP : 0);
+    if (rec[p]) {
+      // the gather writes straight into host-visible pinned memory
+      AWP(awp_alloc_host_pinned((void**)&d_bx[p], rec[p] * sizeof(float)));
+      AWP(awp_alloc_host_pinned((void**)&d_by[p], rec[p] * sizeof(float)));
+      AWP(awp_alloc_host_pinned((void**)&d_bz[p], rec[p] * sizeof(float)));
+      if (A.NVE == 3) AWP(awp_alloc_host_pinned((void**)&d_be[p], rec[p] * sizeof(float)));
+    }
   }
   mkdir(A.OUT.c_str(), 0755);
   fchk = fopen(A.CHKFILE.c_str(), "a+");
+  auto step_all = [&](int n) {
+    if (mesh) AWP(awp_mesh_step(mesh, n));
+    else AWP(awp_step(ctx[0], n));
+  };
+  auto sync_all = [&]() {
+    if (mesh) AWP(awp_mesh_synchronize(mesh));
+    else AWP(awp_synchronize(ctx[0]));
+  };
 
   time_init = now() - time_init;
   printf("Initialization completed in %f s.\n", time_init);
@@ -523,9 +580,9 @@ int main(int argc, char** argv) {
   if ((A.NPC == 0 || A.NPC == 2) && (A.NVE == 1 || A.NVE == 3)) {
     time_un -= now();
     for (cur_step = 1; cur_step <= nt; cur_step++) {
-      AWP(awp_step(ctx, 1));
+      step_all(1);
       if (cur_step % 10 == 0) {
-        AWP(awp_synchronize(ctx));
+        sync_all();
         const double elapsed = now() + time_un;
         const double step_s = elapsed / cur_step;
         printf("%ld  \t\t %4.3f s \t %4.3f s \t %3.5f s/step \t %5.3f step/s \t %2.2f %%  \n",
@@ -534,34 +591,38 @@ int main(int argc, char** argv) {
         fflush(stdout);
       }
       if (cur_step % A.NTISKP == 0) {
-        if (rec) {
-          AWP(awp_gather_output(ctx, rnbgx, rnedx, A.NSKPX[0], rnbgy, rnedy, A.NSKPY[0], rnbgz,
-                                rnedz, A.NSKPZ[0], d_bx, d_by, d_bz, d_be));
-          AWP(awp_synchronize(ctx));
-          const long idtmp = ((cur_step / A.NTISKP + A.WRITE_STEP - 1) % A.WRITE_STEP) * rec;
-          memcpy(Bufx.data() + idtmp, d_bx, rec * 4);
-          memcpy(Bufy.data() + idtmp, d_by, rec * 4);
-          memcpy(Bufz.data() + idtmp, d_bz, rec * 4);
-          if (A.NVE == 3) memcpy(Bufeta.data() + idtmp, d_be, rec * 4);
+        for (int p = 0; p < G; ++p) {
+          if (!rec[p]) continue;
+          AWP(awp_gather_output(ctx[p], rnbgx[p], rnedx[p], A.NSKPX[p], rnbgy[p], rnedy[p],
+                                A.NSKPY[p], rnbgz[p], rnedz[p], A.NSKPZ[p], d_bx[p], d_by[p],
+                                d_bz[p], d_be[p]));
+          sync_all();
+          const long idtmp = ((cur_step / A.NTISKP + A.WRITE_STEP - 1) % A.WRITE_STEP) * rec[p];
+          memcpy(Bufx[p].data() + idtmp, d_bx[p], rec[p] * 4);
+          memcpy(Bufy[p].data() + idtmp, d_by[p], rec[p] * 4);
+          memcpy(Bufz[p].data() + idtmp, d_bz[p], rec[p] * 4);
+          if (A.NVE == 3) memcpy(Bufeta[p].data() + idtmp, d_be[p], rec[p] * 4);
         }
-        if ((cur_step / A.NTISKP) % A.WRITE_STEP == 0 && rec) {
+        for (int p = 0; p < G; ++p) {
+          if ((cur_step / A.NTISKP) % A.WRITE_STEP != 0 || !rec[p]) continue;
           // file view of pmcl3d.c:489-521 at one rank: WRITE_STEP x rec_NZ x
           // rec_NY x rec_NX floats, this rank's rec_nzt x rec_nyt x rec_nxt
           // points at the origin (rows beyond them stay empty)
           const char* base[4] = {"SX", "SY", "SZ", "Eta"};
-          std::vector<float>* bufs[4] = {&Bufx, &Bufy, &Bufz, &Bufeta};
-          const size_t fsz = (size_t)A.WRITE_STEP * recNZ * recNY * recNX;
+          std::vector<float>* bufs[4] = {&Bufx[p], &Bufy[p], &Bufz[p], &Bufeta[p]};
+          const size_t fsz = (size_t)A.WRITE_STEP * recNZ[p] * recNY[p] * recNX[p];
           std::vector<float> file(fsz);
           for (int c = 0; c < (A.NVE == 3 ? 4 : 3); ++c) {
             std::fill(file.begin(), file.end(), 0.f);
             const float* b = bufs[c]->data();
             for (int t = 0; t < A.WRITE_STEP; ++t)
-              for (int z = 0; z < rnz; ++z)
-                for (int y = 0; y < rny; ++y)
-                  memcpy(&file[(((size_t)t * recNZ + z) * recNY + y) * recNX],
-                         b + (((size_t)t * rnz + z) * rny + y) * rnx, rnx * sizeof(float));
+              for (int z = 0; z < rnz[p]; ++z)
+                for (int y = 0; y < rny[p]; ++y)
+                  memcpy(&file[(((size_t)t * recNZ[p] + z) * recNY[p] + y) * recNX[p]],
+                         b + (((size_t)t * rnz[p] + z) * rny[p] + y) * rnx[p],
+                         rnx[p] * sizeof(float));
             char fn[600];
-            snprintf(fn, sizeof fn, "%s/%s_%1d_%07ld", A.OUT.c_str(), base[c], 0, cur_step);
+            snprintf(fn, sizeof fn, "%s/%s_%1d_%07ld", A.OUT.c_str(), base[c], p, cur_step);
             FILE* fo = fopen(fn, "wb");
             if (!fo) die("open output", AWP_ERR_IO);
             fwrite(file.data(), sizeof(float), fsz, fo);
@@ -577,30 +638,39 @@ int main(int argc, char** argv) {
         }
       }
     }
-    AWP(awp_synchronize(ctx));
+    sync_all();
     time_un += now();
   }
-  if (A.IFAULT == 5 && nsrc) {
-    std::vector<float> mom(nsrc);
-    AWP(awp_download_moment(ctx, mom.data()));
+  if (A.IFAULT == 5) {
     float tmom = 0.0f;
-    for (float m : mom) tmom += m;
-    printf("rank %d: moment=%e\n", 0, tmom);
-    const float mag = 2. / 3. * (log10f(tmom) - 9.1);
-    printf("Total M0=%e, Mw=%4.1f\n", tmom, mag);
+    for (int p = 0; p < G; ++p) {
+      if (!nsrc[p]) continue;
+      std::vector<float> mom(nsrc[p]);
+      AWP(awp_download_moment(ctx[p], mom.data()));
+      for (float m : mom) tmom += m;
+    }
+    if (tmom != 0.0f) {
+      printf("rank %d: moment=%e\n", 0, tmom);
+      const float mag = 2. / 3. * (log10f(tmom) - 9.1);
+      printf("Total M0=%e, Mw=%4.1f\n", tmom, mag);
+    }
   }
   if (fchk) {
     fprintf(fchk, "END\n");
     fclose(fchk);
   }
+  long long cells = 0;
+  for (int p = 0; p < G; ++p) cells += (long long)nxt[p] * nyt[p] * nzt[p];
   if (nt > 0 && cur_step > 1)
     printf("%ld steps in %.3f s: %.6f s per time step, %.3f Gcell-updates/s\n", cur_step - 1,
-           time_un, time_un / (cur_step - 1),
-           (double)nxt * nyt * nzt * (cur_step - 1) / time_un / 1e9);
-  if (d_bx) awp_free_host_pinned(d_bx);
-  if (d_by) awp_free_host_pinned(d_by);
-  if (d_bz) awp_free_host_pinned(d_bz);
-  if (d_be) awp_free_host_pinned(d_be);
-  awp_ctx_destroy(ctx);
+           time_un, time_un / (cur_step - 1), (double)cells * (cur_step - 1) / time_un / 1e9);
+  for (int p = 0; p < G; ++p) {
+    if (d_bx[p]) awp_free_host_pinned(d_bx[p]);
+    if (d_by[p]) awp_free_host_pinned(d_by[p]);
+    if (d_bz[p]) awp_free_host_pinned(d_bz[p]);
+    if (d_be[p]) awp_free_host_pinned(d_be[p]);
+  }
+  if (mesh) awp_mesh_destroy(mesh);
+  else awp_ctx_destroy(ctx[0]);
   return 0;
 }

@@ -300,3 +300,65 @@ def write_topography(path, nx, ny, h, amplitude=1000.0, width=5000.0, rough_rms=
         np.asarray([nx, ny, padding], np.int32).tofile(fh)
         elev.astype(np.float32).tofile(fh)
     return elev.astype(np.float32)
+
+
+def lithostatic_sigma2(d1_padded, nx, ny, nz, dh):
+    """Vertical lithostatic stress on the padded grid from the padded density,
+    as pmcl3d's Drucker-Prager set-up forms it (mesh.c:1274-1282): -dh/2 rho g
+    in the surface cell and the image above it, then rho g dh more per cell
+    downwards, accumulated in double and stored as float cell by cell."""
+    top = nz + 31
+    s2 = np.zeros_like(d1_padded, dtype=np.float32)
+    sl = (slice(2, nx + 18), slice(2, ny + 18))
+    d = d1_padded[sl[0], sl[1], :].astype(np.float64)
+    cur = (-dh / 2.0 * d[:, :, top] * 9.81).astype(np.float32)
+    s2[sl[0], sl[1], top] = cur
+    s2[sl[0], sl[1], top + 1] = cur
+    for k in range(top - 1, 29, -1):
+        cur = (cur.astype(np.float64) - dh * d[:, :, k] * 9.81).astype(np.float32)
+        s2[sl[0], sl[1], k] = cur
+    return s2
+
+
+def config3_blocks(nxc=213, nyc=213, nz_fine=320, nz_coarse=96, h_fine=40.0, dt=0.0028,
+                   steps=3000, src_depth_m=8000.0, f0=2.0, m0=1e16, seed=4, vp_cap=6300.0):
+    """Topography + discontinuous mesh + plasticity + attenuation workload: a
+    fine block of (3 nxc) x (3 nyc) x nz_fine cells at h_fine over a 3x coarser
+    block of nxc x nyc x nz_coarse (the fine block must be a multiple of 3 in x
+    and y, so 640 becomes 639); each block carries the anelastic 1-D gradient
+    (vs 1000..3500 m/s over the whole depth, vp = 1.73 vs, Gardner density,
+    Qs = 50 vs[km/s], Qp = 2 Qs) with its own seeded von Karman perturbation;
+    a moment-tensor point source (Mxy Ricker', IFAULT 1) at src_depth_m in the
+    fine block.  dt keeps vp dt / h below 0.45 on the fine block.  Returns the
+    two block Scenarios (params carry grid / ngrids)."""
+    h_coarse = 3 * h_fine
+    depth_total = nz_fine * h_fine + nz_coarse * h_coarse
+    blocks = []
+    for p, (nx, ny, nz, h, z0) in enumerate([(3 * nxc, 3 * nyc, nz_fine, h_fine, 0.0),
+                                             (nxc, nyc, nz_coarse, h_coarse,
+                                              nz_fine * h_fine)]):
+        zc = z0 + (np.arange(nz, dtype=np.float32) + 0.5) * h  # file k = 0 is the top
+        vs1d = 1000.0 + 2500.0 * zc / depth_total
+        pert = np.clip(von_karman((nz, ny, nx), h, 500.0, 0.1, 0.05, seed + 10 * p), -0.15, 0.15)
+        vs = vs1d[:, None, None] * (1.0 + pert)
+        del pert
+        vp = np.minimum(1.73 * vs, vp_cap).astype(np.float32)
+        vs = (vp / 1.73).astype(np.float32)
+        rho = (310.0 * vp ** 0.25).astype(np.float32)
+        qs = (50.0 * vs / 1000.0).astype(np.float32)
+        media = np.stack([vp, vs, rho, (2.0 * qs).astype(np.float32), qs], axis=-1)
+        del vp, vs, rho, qs
+        nst = steps + 2
+        if p == 0:
+            pos = np.array([[nx // 2, ny // 2, int(round(src_depth_m / h))]], np.int32)
+            data = np.zeros((1, nst, 6), np.float32)
+            data[0, :, 5] = ricker_derivative(nst, dt, f0) * m0
+        else:
+            pos = np.zeros((0, 3), np.int32)
+            data = np.zeros((0, nst, 6), np.float32)
+        params = dict(nx=nx, ny=ny, nz=nz, dh=h, dt=dt, nd=20 * (3 if p == 0 else 1),
+                      arbc=0.92, npc=0, nve=3, ifault=1, nst=nst, read_step=nst, socalq=1,
+                      grid=p, ngrids=2)
+        blocks.append(Scenario(f"config3_{p}", params, media, pos, data, steps,
+                               f"block {p}: {nx}x{ny}x{nz} at h={h}"))
+    return blocks

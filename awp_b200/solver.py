@@ -133,14 +133,41 @@ class Solver:
                                              c_float(fmajor), c_float(fminor),
                                              _fptr(st), _fptr(dp)), "awp_upload_plasticity")
 
-    def set_moduli(self, lam: np.ndarray, mu: np.ndarray, rho: np.ndarray) -> None:
-        """Lame moduli and density of the interior, arrays [nz][ny][nx] (surface
-        first), into the kernel arrays; Q stays from the media upload."""
-        a = [np.ascontiguousarray(x, np.float32) for x in (lam, mu, rho)]
+    def _model_ptrs(self, arrays):
+        """float pointers of [nz][ny][nx] model arrays: numpy arrays (host) or
+        contiguous float32 torch tensors (host or CUDA, passed in place)."""
         n = self.params.nx * self.params.ny * self.params.nz
-        if any(x.size != n for x in a):
-            raise ValueError("moduli arrays must have nz*ny*nx elements")
-        check(self.lib.awp_set_moduli(self.ctx, *[_fptr(x) for x in a]), "awp_set_moduli")
+        keep, ptrs = [], []
+        for x in arrays:
+            if isinstance(x, np.ndarray) or not hasattr(x, "data_ptr"):
+                x = np.ascontiguousarray(x, np.float32)
+                size = x.size
+                ptrs.append(_fptr(x))
+            else:
+                import torch
+                if x.dtype != torch.float32 or not x.is_contiguous():
+                    raise ValueError("model tensors must be contiguous float32")
+                size = x.numel()
+                ptrs.append(ctypes.cast(ctypes.c_void_p(x.data_ptr()), ctypes.POINTER(c_float)))
+            if size != n:
+                raise ValueError("model arrays must have nz*ny*nx elements")
+            keep.append(x)
+        return keep, ptrs
+
+    def set_moduli(self, lam, mu, rho) -> None:
+        """Lame moduli and density of the interior, arrays [nz][ny][nx] (surface
+        first; numpy arrays or float32 tensors, CUDA tensors by device
+        pointer), into the kernel arrays; Q stays from the media upload."""
+        keep, ptrs = self._model_ptrs((lam, mu, rho))
+        check(self.lib.awp_set_moduli(self.ctx, *ptrs), "awp_set_moduli")
+        del keep
+
+    def set_qinv(self, qpinv, qsinv) -> None:
+        """Inverse quality factors Qp^-1, Qs^-1 of the interior ([nz][ny][nx],
+        surface first) into the kernel arrays; moduli and density stay."""
+        keep, ptrs = self._model_ptrs((qpinv, qsinv))
+        check(self.lib.awp_set_qinv(self.ctx, *ptrs), "awp_set_qinv")
+        del keep
 
     def reset(self) -> None:
         """Wavefield and memory variables to zero, back to step 0."""
@@ -150,6 +177,13 @@ class Solver:
         """Curvilinear topography of this (top) grid from an INTOPO elevation
         file; call before receivers() and sourcefile()."""
         check(self.lib.awp_topography_init(self.ctx, intopo.encode()), "awp_topography_init")
+
+    def set_topo_plasticity(self, consistent: bool) -> None:
+        """NVE 3 on a curvilinear top grid: False (default) keeps the
+        reference's single-rank behaviour (Cartesian stress on the middle band
+        only), True runs the curvilinear stress everywhere before the return."""
+        check(self.lib.awp_set_topo_plasticity(self.ctx, 1 if consistent else 0),
+              "awp_set_topo_plasticity")
 
     def receivers(self, recvfile: str, nt: int) -> None:
         """RECVFILE receivers (ASCII v2); records the current step at once."""
@@ -238,13 +272,16 @@ class Mesh:
     x and y than the one above.  ``grid(p)`` gives block p's Solver for
     uploads and field access; ``step`` advances the whole mesh."""
 
-    def __init__(self, params_list):
+    def __init__(self, params_list, stream: int | None = None):
         self.lib = _lib.load()
         n = len(params_list)
         arr = (awp_params * n)(*params_list)
         m = c_void_p()
         check(self.lib.awp_mesh_create(arr, n, byref(m)), "awp_mesh_create")
         self.mesh = m
+        if stream is not None:
+            check(self.lib.awp_mesh_set_stream(self.mesh, c_void_p(stream)),
+                  "awp_mesh_set_stream")
         self.grids = []
         for p in range(n):
             ctx = c_void_p()

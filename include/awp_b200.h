@@ -195,6 +195,9 @@ int awp_mesh_grid(awp_mesh* mesh, int p, awp_ctx** ctx);
  * free-surface images of block 0.  The first call applies checkmesh
  * (mesh.c:1404-1443) to the media of every coarser block. */
 int awp_mesh_step(awp_mesh* mesh, int nsteps);
+/* Run every block of the mesh on this cudaStream_t (NULL = the legacy default
+ * stream) from now on; the mesh's own stream stays until awp_mesh_destroy. */
+int awp_mesh_set_stream(awp_mesh* mesh, void* cuda_stream);
 int awp_mesh_synchronize(awp_mesh* mesh);
 
 /* ------------------------------------------------------------------------ */
@@ -239,8 +242,8 @@ int awp_batch_info(awp_batch* batch, long long info[6]);
 /* Materials, seismograms and the adjoint gradient (single grid, Cartesian,  */
 /* NVE 1/2, IFAULT 1 sources)                                                */
 /* ------------------------------------------------------------------------ */
-/* Lame moduli and density of the interior, host arrays [nz][ny][nx] (surface
- * first, the mesh-file order), into the kernel arrays (1/lambda, 1/mu, rho
+/* Lame moduli and density of the interior, arrays [nz][ny][nx] in host or
+ * device memory (surface first, the mesh-file order), into the kernel arrays (1/lambda, 1/mu, rho
  * with the one-cell border copy of the media set-up) and the surface ratio
  * lambda/(lambda+2mu).  Q and the memory-variable set-up of the last media
  * upload stay (upload media first). */
@@ -255,7 +258,8 @@ int awp_seismograms(awp_ctx* ctx, int nsteps, int nrec, const int* rec_xyz, cons
                     float* seis);
 /* The same forward run with the misfit J = 1/2 sum_n sum_r (seis - d_obs)^2
  * and its gradient with respect to lambda, mu, rho of every interior cell
- * (host arrays [nz][ny][nx], surface first; Q held fixed), by the discrete
+ * (arrays [nz][ny][nx] in host or device memory, surface first; Q held
+ * fixed), by the discrete
  * adjoint of the time step: hand-written transposes of the velocity, stress,
  * memory-variable, free-surface-image and imaging updates.  Forward states:
  * with nsnap > 0, nsnap full-state snapshots in device memory, each segment
@@ -270,6 +274,21 @@ int awp_seismograms(awp_ctx* ctx, int nsteps, int nrec, const int* rec_xyz, cons
 int awp_misfit_gradient(awp_ctx* ctx, int nsteps, int nrec, const int* rec_xyz, const int* rec_comp,
                         const float* d_obs, int nsnap, double* misfit, float* seis,
                         float* g_lambda, float* g_mu, float* g_rho);
+/* The same gradient plus, where attenuation is on, the gradient with respect
+ * to the inverse quality factors Qp^-1 and Qs^-1 of every interior cell (host
+ * arrays [nz][ny][nx], surface first; lambda, mu, rho held fixed): the
+ * adjoint of the memory-variable coefficients through the Q(f) weights of
+ * dstrqc (kernel.cu:974-1040), each weight's branch (low-Q polynomial or
+ * linear) held as the forward takes it.  g_qpinv / g_qsinv may be NULL; on
+ * an elastic context (every Q^-1 zero) they come back zero. */
+int awp_misfit_gradient_q(awp_ctx* ctx, int nsteps, int nrec, const int* rec_xyz,
+                          const int* rec_comp, const float* d_obs, int nsnap, double* misfit,
+                          float* seis, float* g_lambda, float* g_mu, float* g_rho,
+                          float* g_qpinv, float* g_qsinv);
+/* Inverse quality factors Qp^-1, Qs^-1 of the interior (host arrays
+ * [nz][ny][nx], surface first) into the kernel arrays with the one-cell
+ * border copy of the media set-up; moduli and density stay. */
+int awp_set_qinv(awp_ctx* ctx, const float* qpinv, const float* qsinv);
 /* The forward-state storage awp_misfit_gradient would use for nsteps steps
  * and this nsnap, from the free device memory now: tail_steps steps keep
  * their velocities, the others run again in segments of segment_steps steps
@@ -305,6 +324,16 @@ int awp_topo_metrics(const char* path, int nx, int ny, int nz, float h, float* o
  * Returns AWP_ERR_IO for an unreadable file, AWP_ERR_ARG for sizes or padding
  * that do not fit the context. */
 int awp_topography_init(awp_ctx* ctx, const char* intopo);
+/* Stress update of a curvilinear top grid with plasticity (NVE = 3).
+ * consistent = 0 (default): the reference's single-rank behaviour -- with
+ * NVE = 3 pmcl3d skips the curvilinear interior stress and runs the Cartesian
+ * dstrqc only over the middle band xss2..xse2 x yls2..yre2 of grid 0
+ * (pmcl3d.c:1855-1879, 2139-2148; topo_stress_left/right_H return at one
+ * rank, src/topography/stress_attenuation.cu:323-325, 430-432).
+ * consistent = 1: a documented change of behaviour -- the curvilinear stress
+ * (and memory variables) on the whole window, then the plasticity return, as
+ * NVE 1/2 do plus the return. */
+int awp_set_topo_plasticity(awp_ctx* ctx, int consistent);
 
 /* Advance nsteps time steps (pmcl3d.c:1628-2487 order: velocity, stress +
  * attenuation, SOURCEFILE and INSRC sources, plasticity, free-surface stress

@@ -222,12 +222,15 @@ class RefMeshSim:
     dvelc2, intp3d, swap3 (swap-area exchanges are no-ops at one rank), dstrqc
     per block, dstrqc2, sources, intp3d, swap3, fstr on block 0."""
 
-    def __init__(self, scns, setups, path=None):
+    def __init__(self, scns, setups, path=None, intopo=None):
         import torch
         self.torch = torch
         self.n = len(scns)
         self.sims = [RefGpuSim(s, st, path=path, defer_consts=True)
-                     for s, st in zip(scns, setups)]
+                     if (p > 0 or intopo is None) else
+                     RefTopoSim(s, st, intopo, path=path, defer_consts=True)
+                     for p, (s, st) in enumerate(zip(scns, setups))]
+        self.nve = scns[0].params.get("nve", 1)
         lib = self.sims[0].lib
         self.lib = lib
         V = c_void_p
@@ -240,9 +243,15 @@ class RefMeshSim:
         nyt = np.array([s.params["ny"] for s in scns], np.int32)
         nzt = np.array([s.params["nz"] for s in scns], np.int32)
         z9 = np.zeros(9, np.float32)
+        Rz, RzT, fmajor, fminor = z9, z9, 0.0, 0.0
+        if self.nve == 3:  # one principal-stress frame for every block (nonlinear.dat)
+            pl = setups[0]["plast"]
+            Rz = np.ascontiguousarray(pl["Rz"], np.float32)
+            RzT = np.ascontiguousarray(pl["RzT"], np.float32)
+            fmajor, fminor = float(pl["fmajor"]), float(pl["fminor"])
         lib.SetDeviceConstValue(fptr(DH), c_float(scns[0].params["dt"]), nxt.ctypes.data_as(_I),
                                 nyt.ctypes.data_as(_I), nzt.ctypes.data_as(_I), self.n,
-                                c_float(0.0), c_float(0.0), fptr(z9), fptr(z9))
+                                c_float(fmajor), c_float(fminor), fptr(Rz), fptr(RzT))
         # zeroed swap-area buffers (never read at one rank, pmcl3d.c:1434-1508)
         self.zbuf = torch.zeros(1 << 16, device="cuda")
         for p, sim in enumerate(self.sims):
@@ -299,6 +308,9 @@ class RefMeshSim:
             for sim in self.sims:
                 sim.sources()
             self._interfaces()
+            if self.nve == 3:  # yield factor and return per grid (pmcl3d.c:2108-2209)
+                for sim in self.sims:
+                    sim.plasticity()
             sim0 = self.sims[0]
             nx, ny = sim0.nx, sim0.ny
             P = sim0.ptr
@@ -687,13 +699,14 @@ class RefTopoSim(RefGpuSim):
     topo_velocity_interior_H and topo_stress_{interior,left,right}_H in place of
     dvelcx / dstrqc, pmcl3d.c:1522-1548, 1661-1698, 1841-1924).  The
     free-surface imaging, sources and receivers stay the Cartesian ones, as in
-    pmcl3d.  NVE=3 is not modelled: with topography the reference's plasticity
-    branch runs the Cartesian dstrqc on the curvilinear grid."""
+    pmcl3d.  With NVE=3 the reference at one rank runs no curvilinear stress on
+    grid 0 (the interior launch belongs to the NVE < 3 branch, pmcl3d.c:1841-1857,
+    and topo_stress_left/right_H return without neighbour ranks): the stress
+    of grid 0 is the Cartesian dstrqc_H over the middle band of the plasticity
+    section (RefGpuSim.plasticity)."""
 
-    def __init__(self, scn, setup, intopo, path=None, topo_path=None):
-        if scn.params.get("nve", 1) == 3:
-            raise ValueError("RefTopoSim models NVE 1 and 2 only")
-        super().__init__(scn, setup, path=path)
+    def __init__(self, scn, setup, intopo, path=None, topo_path=None, defer_consts=False):
+        super().__init__(scn, setup, path=path, defer_consts=defer_consts)
         topo_path = topo_path or os.path.join(REF_DIR, "libawpref_topo.so")
         if not os.path.exists(topo_path):
             raise FileNotFoundError(f"{topo_path} missing: run `make -C oracle ref`")
@@ -727,7 +740,8 @@ class RefTopoSim(RefGpuSim):
         self.tl.ref_topo_velocity(self.T)
 
     def stress_all(self):
-        self.tl.ref_topo_stress(self.T)
+        if self.nve != 3:
+            self.tl.ref_topo_stress(self.T)
         for hook in self.after_stress:
             hook(self, self.cur)
 
