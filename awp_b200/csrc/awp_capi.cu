@@ -388,31 +388,13 @@ void middle_band(const awp_ctx* c, int* i0, int* i1, int* j0, int* j1) {
   *j1 = std::min(yre2, yre - AWP_NGSL - 2);
 }
 
-int phase_stress(awp_ctx* c) {
-  if (c->topo && c->p.nve == 3 && !c->topo_plastic_consistent) {
-    // The reference at one rank with NVE = 3 on a curvilinear grid 0: the
-    // band dstrqc_H loops start at grid `usetopo` (pmcl3d.c:1858-1879), the
-    // interior topography stress belongs to the NVE < 3 branch (:1855) and
-    // topo_stress_left/right_H return without a left/right neighbour rank
-    // (src/topography/stress_attenuation.cu:323-325, 430-432); what remains
-    // is the Cartesian dstrqc_H over the middle band of the plasticity
-    // section (pmcl3d.c:2139-2148).
-    PhaseScope ps(c, 1);
-    StrArgs s = make_str_args(c);
-    middle_band(c, &s.i0, &s.i1, &s.j0, &s.j1);
-    CU_TRY(awp_launch_stress(s, c->elastic, c->stream));
-    c->launches++;
-    return AWP_OK;
-  }
-  if (c->topo) {  // topo_stress_*_H replace dstrqc on the top grid (pmcl3d.c:1843-1924)
-    PhaseScope ps(c, 1);
-    CU_TRY(awp_launch_topo_stress(topo_args(c), c->elastic, c->stream));
-    c->launches++;
-    return AWP_OK;
-  }
+// Cartesian stress (+ memory variables) over i0..i1 x j0..j1 of the stress
+// window, with the kernel family the tuning selects.
+int launch_cart_stress(awp_ctx* c, int i0, int i1, int j0, int j1) {
+  if (i1 < i0 || j1 < j0) return AWP_OK;
   const bool tma = c->tma_ok && awp_tuning_get("tma_str") == 1;
-  PhaseScope ps(c, 1);
   StrArgs s = make_str_args(c);
+  s.i0 = i0; s.i1 = i1; s.j0 = j0; s.j1 = j1;
   if (tma)
     CU_TRY(awp_launch_stress_tma(s, c->str_maps, c->elastic, awp_tuning_get("ichunk"),
                                  c->d_err, c->stream));
@@ -420,6 +402,36 @@ int phase_stress(awp_ctx* c) {
     CU_TRY(awp_launch_stress(s, c->elastic, c->stream));
   c->launches++;
   return AWP_OK;
+}
+
+// NVE = 3 splits the stress update (pmcl3d.c:1858-1924, 2139-2148): the
+// middle band xss2..xse2 x yls2..yre2 is updated in the plasticity section,
+// after the sources and the mesh-interface exchanges, the rest here.  On a
+// curvilinear grid 0 the reference at one rank runs no other stress at all:
+// its band loops start at grid `usetopo` (pmcl3d.c:1858-1879), the interior
+// topography stress belongs to the NVE < 3 branch (:1855) and
+// topo_stress_left/right_H return without a neighbour rank
+// (src/topography/stress_attenuation.cu:323-325, 430-432).
+bool stress_split(const awp_ctx* c) {
+  return c->p.nve == 3 && (!c->topo || !c->topo_plastic_consistent);
+}
+
+int phase_stress(awp_ctx* c) {
+  if (c->topo && c->p.nve == 3 && !c->topo_plastic_consistent) return AWP_OK;
+  if (c->topo) {  // topo_stress_*_H replace dstrqc on the top grid (pmcl3d.c:1843-1924)
+    PhaseScope ps(c, 1);
+    CU_TRY(awp_launch_topo_stress(topo_args(c), c->elastic, c->stream));
+    c->launches++;
+    return AWP_OK;
+  }
+  PhaseScope ps(c, 1);
+  if (!stress_split(c)) return launch_cart_stress(c, c->xls, c->xre, c->yls, c->yre);
+  int i0, i1, j0, j1, st;
+  middle_band(c, &i0, &i1, &j0, &j1);
+  if ((st = launch_cart_stress(c, i0, i1, c->yls, j0 - 1))) return st;  // xss2, front
+  if ((st = launch_cart_stress(c, i0, i1, j1 + 1, c->yre))) return st;  // xss2, back
+  if ((st = launch_cart_stress(c, c->xls, i0 - 1, c->yls, c->yre))) return st;  // xss1
+  return launch_cart_stress(c, i1 + 1, c->xre, c->yls, c->yre);                 // xss3
 }
 
 int phase_sources(awp_ctx* c) {
@@ -443,8 +455,15 @@ int phase_sources(awp_ctx* c) {
 
 int phase_plasticity(awp_ctx* c) {
   if (c->p.nve != 3) return AWP_OK;
+  int st;
+  if (stress_split(c)) {  // the middle band of the stress split (pmcl3d.c:2139-2148)
+    PhaseScope ps(c, 1);
+    int i0, i1, j0, j1;
+    middle_band(c, &i0, &i1, &j0, &j1);
+    if ((st = launch_cart_stress(c, i0, i1, j0, j1))) return st;
+  }
   PhaseScope ps(c, 3);
-  int st = launch_plasticity(c);
+  st = launch_plasticity(c);
   if (st) return st;
   c->launches += 2;
   return AWP_OK;

@@ -1003,6 +1003,7 @@ cudaError_t awp_launch_stress(const StrArgs& a, bool elastic, cudaStream_t st) {
 int awp_tuning_set(const char* key, int value) {
   if (!strcmp(key, "ichunk") && value >= 4 && value <= 1024) { g_ichunk = value; return 0; }
   if (!strcmp(key, "spin_limit")) return awp_tma_set_spin_limit(value);
+  if (!strcmp(key, "l2_promotion")) return awp_tma_set_l2_promotion(value);
   if (value == 0 || value == 1) {
     if (!strcmp(key, "tma")) { g_tma_vel = g_tma_str = value; return 0; }  // both half-steps
     if (!strcmp(key, "tma_vel")) { g_tma_vel = value; return 0; }
@@ -1017,6 +1018,7 @@ int awp_tuning_get(const char* key) {
   if (!strcmp(key, "tma_vel")) return g_tma_vel;
   if (!strcmp(key, "tma_str")) return g_tma_str;
   if (!strcmp(key, "spin_limit")) return (int)awp_tma_get_spin_limit();
+  if (!strcmp(key, "l2_promotion")) return awp_tma_get_l2_promotion();
   return -1;
 }
 

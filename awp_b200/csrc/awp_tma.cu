@@ -584,6 +584,18 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 
 }  // namespace
 
+// L2 promotion of the tensor maps' fetches (process-wide; read when a
+// context encodes its maps): 0 none, 1 64 B, 2 128 B, 3 256 B.
+static int g_l2_promotion = 3;
+
+int awp_tma_set_l2_promotion(int mode) {
+  if (mode < 0 || mode > 3) return 1;
+  g_l2_promotion = mode;
+  return 0;
+}
+
+int awp_tma_get_l2_promotion() { return g_l2_promotion; }
+
 int awp_tma_encode(CUtensorMap* map, const float* base, const AwpGeom& g, int box_x, int box_y) {
   auto fn = encode_fn();
   if (!fn) return 1;
@@ -595,7 +607,11 @@ int awp_tma_encode(CUtensorMap* map, const float* base, const AwpGeom& g, int bo
   const CUresult r =
       fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(base), dims, strides, box,
          estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-         CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+         g_l2_promotion == 0   ? CU_TENSOR_MAP_L2_PROMOTION_NONE
+         : g_l2_promotion == 1 ? CU_TENSOR_MAP_L2_PROMOTION_L2_64B
+         : g_l2_promotion == 2 ? CU_TENSOR_MAP_L2_PROMOTION_L2_128B
+                               : CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return r == CUDA_SUCCESS ? 0 : 2;
 }
 

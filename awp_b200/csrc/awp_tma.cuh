@@ -35,3 +35,7 @@ cudaError_t awp_launch_velocity_tma(const VelArgs& a, const TmaMaps& tm, int ich
 // copies with the default limit and leaves.  Returns 0 or 1 (refused).
 int awp_tma_set_spin_limit(long long polls);
 long long awp_tma_get_spin_limit();
+// L2 promotion of the TMA fetches for tensor maps encoded from now on (0 none,
+// 1 64 B, 2 128 B, 3 256 B, the default).  Returns 0 or 1 (refused).
+int awp_tma_set_l2_promotion(int mode);
+int awp_tma_get_l2_promotion();

@@ -7,10 +7,17 @@
 //             dtopo_vel_112 (kernels/optimized_velocity.cu:1040-1629),
 //   stress:   dtopo_str_111 / dtopo_str_112 (kernels/stress_attenuation.cu:73-1415),
 // launched by topo_velocity_*_H (velocity.cu) and topo_stress_*_H
-// (stress_attenuation.cu).  Here each half-step is one kernel: a thread owns
-// one (i, j, k) cell, k fastest across the warp for coalesced loads, and the
-// vertical operators switch between the interior stencil and the boundary
-// closure row r = nz-1-k (tables in awp_topo_tables.h) per thread.
+// (stress_attenuation.cu).  Here each half-step is one kernel.  A warp owns 32
+// consecutive k of one (i, j) column and every lane loads the values of its
+// own level only: the vertical operators (7-point differences of horizontal
+// interpolants, 4-point differences) take the neighbouring levels from the
+// neighbouring lanes by warp shuffles, so each value crosses the memory system
+// once per column instead of once per stencil point.  Warps overlap by three
+// levels on each side (tiles of 26 output levels; the top tile outputs its 29
+// levels under the surface), the halo lanes only feeding their neighbours.
+// The boundary-closure rows r = nz-1-k of the summation-by-parts tables
+// (awp_topo_tables.h) read the top levels of the column, which all sit in the
+// top tile, by broadcast shuffles.
 //
 // Term structure (f = surface function interpolants, g = vertical metric;
 // relative indices, k = 0 the bottom point of the grid):
@@ -34,51 +41,86 @@ constexpr float kP0 = (float)-0.0625, kP1 = (float)0.5625;
 constexpr float kD0 = (float)0.0416666666666667, kD1 = (float)-1.1250000000000000;
 constexpr float kZ0 = (float)-0.0026041666666667, kZ1 = (float)0.0937500000000000,
                 kZ2 = (float)-0.6796875000000000;
+constexpr unsigned kAll = 0xffffffffu;
+constexpr int kTileOut = 26;  // output levels of a tile below the top one
 
-struct Idx {
-  int slice, yline, fld;
-  __device__ __forceinline__ long long p(int i, int j, int k) const {
-    return (long long)(i + AWP_NGSL + 2) * slice + (long long)(j + AWP_NGSL + 2) * yline +
-           (k + AWP_ALIGN);
-  }
-  __device__ __forceinline__ long long f(int i, int j) const {
-    return (long long)(i + AWP_NGSL + 2) * fld + (j + AWP_NGSL + 2 + AWP_ALIGN);
-  }
-};
-
-__device__ __forceinline__ float ld(const float* __restrict__ a, long long o) { return __ldg(a + o); }
 __device__ __forceinline__ float gk(const float* __restrict__ g, int k) {
   return __ldg(g + k + AWP_ALIGN);
 }
 __device__ __forceinline__ float inv(float x) { return (float)(1.0 / (double)x); }
 
-// 7-point vertical difference at k (interior: c[n] at k-3+n, the centre
-// weight is zero) or boundary row r (T[r][m] at nz-1-m, m = NT-1 .. 0).
-template <int NT, class Fn>
-__device__ __forceinline__ float zdiff7(int k, int r, int nz, const float (&T)[6][NT], Fn v) {
-  if (r < 0)
-    return kZ0 * v(k - 3) + kZ1 * v(k - 2) + kZ2 * v(k - 1) - kZ2 * v(k + 1) - kZ1 * v(k + 2) -
-           kZ0 * v(k + 3);
-  float s = 0.f;
+// Column position of a warp: tile t = 0 holds the top 32 levels, tile t > 0
+// the 32 levels starting 26 t lower.  A lane outputs its level when it is not
+// a halo lane (three at each end; the top tile has no upper halo) and k >= 3
+// (the reference leaves the three bottom points to the mesh coupling,
+// dm_offset = 3).
+struct ColPos {
+  int k, r, lane;
+  bool top, out;
+  __device__ ColPos(int nz, int tile) {
+    lane = threadIdx.x;
+    top = (tile == 0);
+    k = nz - 32 - kTileOut * tile + lane;
+    r = (top && lane >= 26) ? 31 - lane : -1;  // boundary row nz-1-k of the top six
+    out = lane >= 3 && (top || lane <= 28) && k >= 3;
+  }
+};
+
+// 7-point vertical difference at the lane's level of a value v(k) held one
+// level per lane (interior coefficients), or boundary row r of T in the top
+// tile.  Summation order as the reference's operators.
+template <int NT>
+__device__ __forceinline__ float zd7(float v, const ColPos& c, const float (&T)[6][NT]) {
+  const float m3 = __shfl_up_sync(kAll, v, 3), m2 = __shfl_up_sync(kAll, v, 2),
+              m1 = __shfl_up_sync(kAll, v, 1), p1 = __shfl_down_sync(kAll, v, 1),
+              p2 = __shfl_down_sync(kAll, v, 2), p3 = __shfl_down_sync(kAll, v, 3);
+  float s = kZ0 * m3 + kZ1 * m2 + kZ2 * m1 - kZ2 * p1 - kZ1 * p2 - kZ0 * p3;
+  if (c.top) {  // warp-uniform: the closure rows of the top six levels
+    const int rr = c.r < 0 ? 0 : c.r;
+    float b = 0.f;
 #pragma unroll
-  for (int m = NT - 1; m >= 0; --m) s += T[r][m] * v(nz - 1 - m);
+    for (int m = NT - 1; m >= 0; --m) b += T[rr][m] * __shfl_sync(kAll, v, 31 - m);
+    if (c.r >= 0) s = b;
+  }
   return s;
 }
 
-// 4-point vertical difference: half-point form (dhz4: k-2..k+1) or node form
-// (dz4: k-1..k+2), or the boundary row.
-template <int NT, class Fn>
-__device__ __forceinline__ float zdiff4(int k, int r, int nz, bool half, const float (&T)[6][NT],
-                                        Fn v) {
-  if (r < 0) {
-    const int b = half ? k - 2 : k - 1;
-    return kD0 * v(b) + kD1 * v(b + 1) - kD1 * v(b + 2) - kD0 * v(b + 3);
-  }
-  float s = 0.f;
+// 4-point vertical difference: half-point form (k-2..k+1) or node form
+// (k-1..k+2), or boundary row r.
+template <int NT>
+__device__ __forceinline__ float zd4(float v, const ColPos& c, bool half,
+                                     const float (&T)[6][NT]) {
+  const float m2 = __shfl_up_sync(kAll, v, 2), m1 = __shfl_up_sync(kAll, v, 1),
+              p1 = __shfl_down_sync(kAll, v, 1), p2 = __shfl_down_sync(kAll, v, 2);
+  float s = half ? kD0 * m2 + kD1 * m1 - kD1 * v - kD0 * p1
+                 : kD0 * m1 + kD1 * v - kD1 * p1 - kD0 * p2;
+  if (c.top) {
+    const int rr = c.r < 0 ? 0 : c.r;
+    float b = 0.f;
 #pragma unroll
-  for (int m = NT - 1; m >= 0; --m) s += T[r][m] * v(nz - 1 - m);
+    for (int m = NT - 1; m >= 0; --m) b += T[rr][m] * __shfl_sync(kAll, v, 31 - m);
+    if (c.r >= 0) s = b;
+  }
   return s;
 }
+
+struct Cell {
+  long long o;   // padded index of (i, j, k)
+  long long of;  // index of (i, j) in the 2-D metric arrays
+  int S, Y, F;
+  __device__ Cell(const TopoArgs& a, int i, int j, int k)
+      : o((long long)(i + AWP_NGSL + 2) * a.slice + (long long)(j + AWP_NGSL + 2) * a.yline +
+          (k + AWP_ALIGN)),
+        of((long long)(i + AWP_NGSL + 2) * a.fld + (j + AWP_NGSL + 2 + AWP_ALIGN)),
+        S(a.slice), Y(a.yline), F(a.fld) {}
+  // 3-D field at (i+di, j+dj, k); 2-D metric at (i+di, j+dj)
+  __device__ __forceinline__ float at(const float* __restrict__ s, int di, int dj) const {
+    return __ldg(s + o + (di * S + dj * Y));
+  }
+  __device__ __forceinline__ float fm(const float* __restrict__ f, int di, int dj) const {
+    return __ldg(f + of + (di * F + dj));
+  }
+};
 
 }  // namespace
 
@@ -86,105 +128,84 @@ __device__ __forceinline__ float zdiff4(int k, int r, int nz, bool half, const f
 // Velocity
 // ===========================================================================
 __global__ void __launch_bounds__(128) k_topo_velocity(const TopoArgs a) {
-  const int k = 3 + blockIdx.x * 32 + threadIdx.x;  // dm_offset = 3 (velocity_unroll.cu:420)
+  const ColPos c(a.nz, blockIdx.x);
   const int j = blockIdx.y * 4 + threadIdx.y;
   const int i = blockIdx.z;
-  const int nz = a.nz;
-  if (k >= nz || j >= a.ny || i >= a.nx) return;
-  const int r = (k >= nz - 6) ? nz - 1 - k : -1;
-  const Idx X{a.slice, a.yline, a.fld};
+  if (j >= a.ny || i >= a.nx) return;  // whole warps
+  const int k = c.k;
+  const Cell X(a, i, j, k);
   const float *__restrict__ s11 = a.xx, *__restrict__ s12 = a.xy, *__restrict__ s13 = a.xz,
               *__restrict__ s22 = a.yy, *__restrict__ s23 = a.yz, *__restrict__ s33 = a.zz;
-  const float* __restrict__ rho = a.d1;
-  // neighbours as 32-bit offsets from this cell (the offsets are constants
-  // times the strides, so each distinct one costs one multiply-add, not a
-  // 64-bit index per load)
-  const long long oc = X.p(i, j, k), ofc = X.f(i, j);
-  auto S = [&](const float* __restrict__ s, int ii, int jj, int kk) {
-    return __ldg(s + oc + ((ii - i) * a.slice + (jj - j) * a.yline + (kk - k)));
-  };
-  auto F = [&](const float* __restrict__ f, int ii, int jj) {
-    return __ldg(f + ofc + ((ii - i) * a.fld + (jj - j)));
-  };
 
-  // density at the staggered velocity points (velocity_unroll.cu:140-152)
-  const float rho1 = 0.25f * (S(rho, i, j, k - 1) + S(rho, i, j - 1, k - 1)) +
-                     0.25f * (S(rho, i, j, k) + S(rho, i, j - 1, k));
-  const float rho2 = 0.25f * (S(rho, i, j, k - 1) + S(rho, i - 1, j, k - 1)) +
-                     0.25f * (S(rho, i, j, k) + S(rho, i - 1, j, k));
-  const float rho3 = 0.25f * (S(rho, i, j, k) + S(rho, i - 1, j, k)) +
-                     0.25f * (S(rho, i, j - 1, k) + S(rho, i - 1, j - 1, k));
-  const float g3c = gk(a.g3_c, k), g3 = gk(a.g3, k);
-  const float Ai1 = (float)((double)a.nu / (double)(F(a.f_1, i, j) * g3c * rho1));
-  const float Ai2 = (float)((double)a.nu / (double)(F(a.f_2, i, j) * g3c * rho2));
-  const float Ai3 = (float)((double)a.nu / (double)(F(a.f_c, i, j) * g3 * rho3));
-  const float dcrj = ld(a.dcrjx, i + AWP_NGSL + 2) * ld(a.dcrjy, j + AWP_NGSL + 2) *
-                     ld(a.dcrjz, k + AWP_ALIGN);
+  // density at the staggered velocity points (velocity_unroll.cu:140-152); the
+  // k-1 values from the lane below
+  const float r00 = X.at(a.d1, 0, 0), r0m = X.at(a.d1, 0, -1), rm0 = X.at(a.d1, -1, 0),
+              rmm = X.at(a.d1, -1, -1);
+  const float r00k = __shfl_up_sync(kAll, r00, 1), r0mk = __shfl_up_sync(kAll, r0m, 1),
+              rm0k = __shfl_up_sync(kAll, rm0, 1);
+  const float rho1 = 0.25f * (r00k + r0mk) + 0.25f * (r00 + r0m);
+  const float rho2 = 0.25f * (r00k + rm0k) + 0.25f * (r00 + rm0);
+  const float rho3 = 0.25f * (r00 + rm0) + 0.25f * (r0m + rmm);
+  const float g3c = gk(a.g3_c, k), g3 = gk(a.g3, k), gc = gk(a.g_c, k), gg = gk(a.g, k);
+  const float fc = X.fm(a.f_c, 0, 0);
+  const float Ai1 = (float)((double)a.nu / (double)(X.fm(a.f_1, 0, 0) * g3c * rho1));
+  const float Ai2 = (float)((double)a.nu / (double)(X.fm(a.f_2, 0, 0) * g3c * rho2));
+  const float Ai3 = (float)((double)a.nu / (double)(fc * g3 * rho3));
+  const float dcrj = __ldg(a.dcrjx + i + AWP_NGSL + 2) * __ldg(a.dcrjy + j + AWP_NGSL + 2) *
+                     __ldg(a.dcrjz + k + AWP_ALIGN);
 
   // --- u1 -------------------------------------------------------------------
-  float s1 = -kD1 * F(a.f_c, i, j) * g3c * S(s11, i, j, k) + kD0 * F(a.f_c, i - 2, j) * g3c * S(s11, i - 2, j, k) +
-       kD1 * F(a.f_c, i - 1, j) * g3c * S(s11, i - 1, j, k) -
-       kD0 * F(a.f_c, i + 1, j) * g3c * S(s11, i + 1, j, k);
-  s1 += -kD1 * F(a.f, i, j) * g3c * S(s12, i, j, k) + kD0 * F(a.f, i, j - 2) * g3c * S(s12, i, j - 2, k) +
-        kD1 * F(a.f, i, j - 1) * g3c * S(s12, i, j - 1, k) -
-        kD0 * F(a.f, i, j + 1) * g3c * S(s12, i, j + 1, k);
-  s1 += zdiff4(k, r, nz, true, kTopoVelDhz4r, [&](int kk) { return S(s13, i, j, kk); });
+  const float x11_0 = X.at(s11, 0, 0), x11_m2 = X.at(s11, -2, 0), x11_m1 = X.at(s11, -1, 0),
+              x11_p1 = X.at(s11, 1, 0);
+  const float y12_0 = X.at(s12, 0, 0), y12_m2 = X.at(s12, 0, -2), y12_m1 = X.at(s12, 0, -1),
+              y12_p1 = X.at(s12, 0, 1);
+  float s1 = -kD1 * fc * g3c * x11_0 + kD0 * X.fm(a.f_c, -2, 0) * g3c * x11_m2 +
+             kD1 * X.fm(a.f_c, -1, 0) * g3c * x11_m1 - kD0 * X.fm(a.f_c, 1, 0) * g3c * x11_p1;
+  const float ff = X.fm(a.f, 0, 0);
+  s1 += -kD1 * ff * g3c * y12_0 + kD0 * X.fm(a.f, 0, -2) * g3c * y12_m2 +
+        kD1 * X.fm(a.f, 0, -1) * g3c * y12_m1 - kD0 * X.fm(a.f, 0, 1) * g3c * y12_p1;
+  const float x13_0 = X.at(s13, 0, 0);
+  s1 += zd4(x13_0, c, true, kTopoVelDhz4r);
   {
-    auto px = [&](int kk) {  // phx4 on s11 at i-2..i+1
-      return gk(a.g_c, kk) * (kP1 * S(s11, i, j, kk) + kP0 * S(s11, i - 2, j, kk) +
-                              kP1 * S(s11, i - 1, j, kk) + kP0 * S(s11, i + 1, j, kk));
-    };
-    auto py = [&](int kk) {  // phy4 on s12 at j-2..j+1
-      return gk(a.g_c, kk) * (kP1 * S(s12, i, j, kk) + kP0 * S(s12, i, j - 2, kk) +
-                              kP1 * S(s12, i, j - 1, kk) + kP0 * S(s12, i, j + 1, kk));
-    };
-    s1 = s1 - F(a.f1_1, i, j) * zdiff7(k, r, nz, kTopoVelDhpz4r, px);
-    s1 = s1 - F(a.f2_1, i, j) * zdiff7(k, r, nz, kTopoVelDhpz4r, py);
+    const float px = gc * (kP1 * x11_0 + kP0 * x11_m2 + kP1 * x11_m1 + kP0 * x11_p1);
+    const float py = gc * (kP1 * y12_0 + kP0 * y12_m2 + kP1 * y12_m1 + kP0 * y12_p1);
+    s1 = s1 - X.fm(a.f1_1, 0, 0) * zd7(px, c, kTopoVelDhpz4r);
+    s1 = s1 - X.fm(a.f2_1, 0, 0) * zd7(py, c, kTopoVelDhpz4r);
   }
   // --- u2 -------------------------------------------------------------------
-  float s2 = zdiff4(k, r, nz, true, kTopoVelDhz4r, [&](int kk) { return S(s23, i, j, kk); });
-  s2 += kD1 * F(a.f, i, j) * g3c * S(s12, i, j, k) + kD0 * F(a.f, i - 1, j) * g3c * S(s12, i - 1, j, k) -
-        kD1 * F(a.f, i + 1, j) * g3c * S(s12, i + 1, j, k) -
-        kD0 * F(a.f, i + 2, j) * g3c * S(s12, i + 2, j, k);
-  s2 += kD1 * F(a.f_c, i, j) * g3c * S(s22, i, j, k) +
-        kD0 * F(a.f_c, i, j - 1) * g3c * S(s22, i, j - 1, k) -
-        kD1 * F(a.f_c, i, j + 1) * g3c * S(s22, i, j + 1, k) -
-        kD0 * F(a.f_c, i, j + 2) * g3c * S(s22, i, j + 2, k);
+  const float x23_0 = X.at(s23, 0, 0);
+  float s2 = zd4(x23_0, c, true, kTopoVelDhz4r);
+  const float x12_m1 = X.at(s12, -1, 0), x12_p1 = X.at(s12, 1, 0), x12_p2 = X.at(s12, 2, 0);
+  s2 += kD1 * ff * g3c * y12_0 + kD0 * X.fm(a.f, -1, 0) * g3c * x12_m1 -
+        kD1 * X.fm(a.f, 1, 0) * g3c * x12_p1 - kD0 * X.fm(a.f, 2, 0) * g3c * x12_p2;
+  const float y22_0 = X.at(s22, 0, 0), y22_m1 = X.at(s22, 0, -1), y22_p1 = X.at(s22, 0, 1),
+              y22_p2 = X.at(s22, 0, 2);
+  s2 += kD1 * fc * g3c * y22_0 + kD0 * X.fm(a.f_c, 0, -1) * g3c * y22_m1 -
+        kD1 * X.fm(a.f_c, 0, 1) * g3c * y22_p1 - kD0 * X.fm(a.f_c, 0, 2) * g3c * y22_p2;
   {
-    auto px = [&](int kk) {  // px4 on s12 at i-1..i+2
-      return gk(a.g_c, kk) * (kP1 * S(s12, i, j, kk) + kP0 * S(s12, i - 1, j, kk) +
-                              kP1 * S(s12, i + 1, j, kk) + kP0 * S(s12, i + 2, j, kk));
-    };
-    auto py = [&](int kk) {  // py4 on s22 at j-1..j+2
-      return gk(a.g_c, kk) * (kP1 * S(s22, i, j, kk) + kP0 * S(s22, i, j - 1, kk) +
-                              kP1 * S(s22, i, j + 1, kk) + kP0 * S(s22, i, j + 2, kk));
-    };
-    s2 = s2 - F(a.f1_2, i, j) * zdiff7(k, r, nz, kTopoVelDhpz4r, px);
-    s2 = s2 - F(a.f2_2, i, j) * zdiff7(k, r, nz, kTopoVelDhpz4r, py);
+    const float px = gc * (kP1 * y12_0 + kP0 * x12_m1 + kP1 * x12_p1 + kP0 * x12_p2);
+    const float py = gc * (kP1 * y22_0 + kP0 * y22_m1 + kP1 * y22_p1 + kP0 * y22_p2);
+    s2 = s2 - X.fm(a.f1_2, 0, 0) * zd7(px, c, kTopoVelDhpz4r);
+    s2 = s2 - X.fm(a.f2_2, 0, 0) * zd7(py, c, kTopoVelDhpz4r);
   }
   // --- u3 -------------------------------------------------------------------
-  float s3 = -kD1 * F(a.f_2, i, j) * g3 * S(s23, i, j, k) +
-             kD0 * F(a.f_2, i, j - 2) * g3 * S(s23, i, j - 2, k) +
-             kD1 * F(a.f_2, i, j - 1) * g3 * S(s23, i, j - 1, k) -
-             kD0 * F(a.f_2, i, j + 1) * g3 * S(s23, i, j + 1, k);
-  s3 += kD1 * F(a.f_1, i, j) * g3 * S(s13, i, j, k) + kD0 * F(a.f_1, i - 1, j) * g3 * S(s13, i - 1, j, k) -
-        kD1 * F(a.f_1, i + 1, j) * g3 * S(s13, i + 1, j, k) -
-        kD0 * F(a.f_1, i + 2, j) * g3 * S(s13, i + 2, j, k);
-  s3 += zdiff4(k, r, nz, false, kTopoVelDz4r, [&](int kk) { return S(s33, i, j, kk); });
+  const float f2 = X.fm(a.f_2, 0, 0), f1 = X.fm(a.f_1, 0, 0);
+  const float y23_m2 = X.at(s23, 0, -2), y23_m1 = X.at(s23, 0, -1), y23_p1 = X.at(s23, 0, 1);
+  float s3 = -kD1 * f2 * g3 * x23_0 + kD0 * X.fm(a.f_2, 0, -2) * g3 * y23_m2 +
+             kD1 * X.fm(a.f_2, 0, -1) * g3 * y23_m1 - kD0 * X.fm(a.f_2, 0, 1) * g3 * y23_p1;
+  const float x13_m1 = X.at(s13, -1, 0), x13_p1 = X.at(s13, 1, 0), x13_p2 = X.at(s13, 2, 0);
+  s3 += kD1 * f1 * g3 * x13_0 + kD0 * X.fm(a.f_1, -1, 0) * g3 * x13_m1 -
+        kD1 * X.fm(a.f_1, 1, 0) * g3 * x13_p1 - kD0 * X.fm(a.f_1, 2, 0) * g3 * x13_p2;
+  s3 += zd4(X.at(s33, 0, 0), c, false, kTopoVelDz4r);
   {
-    auto px = [&](int kk) {  // px4 on s13 at i-1..i+2, weighted by g
-      return gk(a.g, kk) * (kP1 * S(s13, i, j, kk) + kP0 * S(s13, i - 1, j, kk) +
-                            kP1 * S(s13, i + 1, j, kk) + kP0 * S(s13, i + 2, j, kk));
-    };
-    auto py = [&](int kk) {  // phy4 on s23 at j-2..j+1
-      return gk(a.g, kk) * (kP1 * S(s23, i, j, kk) + kP0 * S(s23, i, j - 2, kk) +
-                            kP1 * S(s23, i, j - 1, kk) + kP0 * S(s23, i, j + 1, kk));
-    };
-    s3 = s3 - F(a.f1_c, i, j) * zdiff7(k, r, nz, kTopoVelDphz4r, px);
-    s3 = s3 - F(a.f2_c, i, j) * zdiff7(k, r, nz, kTopoVelDphz4r, py);
+    const float px = gg * (kP1 * x13_0 + kP0 * x13_m1 + kP1 * x13_p1 + kP0 * x13_p2);
+    const float py = gg * (kP1 * x23_0 + kP0 * y23_m2 + kP1 * y23_m1 + kP0 * y23_p1);
+    s3 = s3 - X.fm(a.f1_c, 0, 0) * zd7(px, c, kTopoVelDphz4r);
+    s3 = s3 - X.fm(a.f2_c, 0, 0) * zd7(py, c, kTopoVelDphz4r);
   }
 
-  const long long o = X.p(i, j, k);
+  if (!c.out) return;
+  const long long o = X.o;
   a.u1[o] = (a.u1[o] + Ai1 * s1) * dcrj;
   a.v1[o] = (a.v1[o] + Ai2 * s2) * dcrj;
   a.w1[o] = (a.w1[o] + Ai3 * s3) * dcrj;
@@ -195,113 +216,97 @@ __global__ void __launch_bounds__(128) k_topo_velocity(const TopoArgs a) {
 // ===========================================================================
 template <bool ELASTIC>
 __global__ void __launch_bounds__(128) k_topo_stress(const TopoArgs a) {
-  const int k = 3 + blockIdx.x * 32 + threadIdx.x;  // dm_offset = 3 (stress_attenuation.cu:177)
+  const ColPos c(a.nz, blockIdx.x);
   const int j = a.s_j + blockIdx.y * 4 + threadIdx.y;
   const int i = a.s_i + blockIdx.z;
-  const int nz = a.nz;
-  if (k >= nz || j >= a.e_j || i >= a.e_i) return;
-  const int r = (k >= nz - 6) ? nz - 1 - k : -1;
-  const Idx X{a.slice, a.yline, a.fld};
+  if (j >= a.e_j || i >= a.e_i) return;  // whole warps
+  const int k = c.k, r = c.r;
+  const Cell X(a, i, j, k);
   const float *__restrict__ u1 = a.u1, *__restrict__ v1 = a.v1, *__restrict__ w1 = a.w1;
-  // neighbours as 32-bit offsets from this cell (the offsets are constants
-  // times the strides, so each distinct one costs one multiply-add, not a
-  // 64-bit index per load)
-  const long long oc = X.p(i, j, k), ofc = X.f(i, j);
-  auto S = [&](const float* __restrict__ s, int ii, int jj, int kk) {
-    return __ldg(s + oc + ((ii - i) * a.slice + (jj - j) * a.yline + (kk - k)));
-  };
-  auto F = [&](const float* __restrict__ f, int ii, int jj) {
-    return __ldg(f + ofc + ((ii - i) * a.fld + (jj - j)));
-  };
   const float gc = gk(a.g_c, k), g = gk(a.g, k);
 
-  // ---- normal components: Jii = 1 / (f_c g3_c) (stress_attenuation.cu:340-431)
-  const float Jii = inv(F(a.f_c, i, j) * gk(a.g3_c, k));
+  // every vertical difference of a horizontal interpolant is one difference
+  // of the interpolated column (the metric weights do not depend on k)
   float d[9];
+  // ---- normal components: Jii = 1 / (f_c g3_c) (stress_attenuation.cu:340-431)
+  const float Jii = inv(X.fm(a.f_c, 0, 0) * gk(a.g3_c, k));
+  const float u_0 = X.at(u1, 0, 0), u_xm1 = X.at(u1, -1, 0), u_xp1 = X.at(u1, 1, 0),
+              u_xp2 = X.at(u1, 2, 0);
+  const float v_0 = X.at(v1, 0, 0), v_ym2 = X.at(v1, 0, -2), v_ym1 = X.at(v1, 0, -1),
+              v_yp1 = X.at(v1, 0, 1);
+  const float w_0 = X.at(w1, 0, 0);
   {
-    auto zu = [&](int ii, int jj) {
-      return zdiff7(k, r, nz, kTopoStrPhdz4r, [&](int kk) { return S(u1, ii, jj, kk); });
-    };
-    auto zv = [&](int ii, int jj) {
-      return zdiff7(k, r, nz, kTopoStrPhdz4r, [&](int kk) { return S(v1, ii, jj, kk); });
-    };
-    d[0] = kD1 * S(u1, i, j, k) + kD0 * S(u1, i - 1, j, k) - kD1 * S(u1, i + 1, j, k) -
-           kD0 * S(u1, i + 2, j, k) -
-           Jii * gc *
-               (kP0 * F(a.f1_1, i - 1, j) * zu(i - 1, j) + kP1 * F(a.f1_1, i, j) * zu(i, j) +
-                kP1 * F(a.f1_1, i + 1, j) * zu(i + 1, j) + kP0 * F(a.f1_1, i + 2, j) * zu(i + 2, j));
-    d[1] = -kD1 * S(v1, i, j, k) + kD0 * S(v1, i, j - 2, k) + kD1 * S(v1, i, j - 1, k) -
-           kD0 * S(v1, i, j + 1, k) -
-           Jii * gc *
-               (kP1 * F(a.f2_2, i, j) * zv(i, j) + kP0 * F(a.f2_2, i, j - 2) * zv(i, j - 2) +
-                kP1 * F(a.f2_2, i, j - 1) * zv(i, j - 1) + kP0 * F(a.f2_2, i, j + 1) * zv(i, j + 1));
-    d[2] = Jii * zdiff4(k, r, nz, true, kTopoStrDhz4r, [&](int kk) { return S(w1, i, j, kk); });
+    const float iu = kP0 * X.fm(a.f1_1, -1, 0) * u_xm1 + kP1 * X.fm(a.f1_1, 0, 0) * u_0 +
+                     kP1 * X.fm(a.f1_1, 1, 0) * u_xp1 + kP0 * X.fm(a.f1_1, 2, 0) * u_xp2;
+    d[0] = kD1 * u_0 + kD0 * u_xm1 - kD1 * u_xp1 - kD0 * u_xp2 -
+           Jii * gc * zd7(iu, c, kTopoStrPhdz4r);
+    const float iv = kP1 * X.fm(a.f2_2, 0, 0) * v_0 + kP0 * X.fm(a.f2_2, 0, -2) * v_ym2 +
+                     kP1 * X.fm(a.f2_2, 0, -1) * v_ym1 + kP0 * X.fm(a.f2_2, 0, 1) * v_yp1;
+    d[1] = -kD1 * v_0 + kD0 * v_ym2 + kD1 * v_ym1 - kD0 * v_yp1 -
+           Jii * gc * zd7(iv, c, kTopoStrPhdz4r);
+    d[2] = Jii * zd4(w_0, c, true, kTopoStrDhz4r);
   }
   // ---- xy: J12i = 1 / (f g3_c); the interior rows read g3_c six points
   // higher (stress_attenuation.cu:471), the boundary rows at k (:1149)
   {
-    const float J12i = inv(F(a.f, i, j) * gk(a.g3_c, r < 0 ? k + 6 : k));
-    auto zu = [&](int ii, int jj) {
-      return zdiff7(k, r, nz, kTopoStrPhdz4r, [&](int kk) { return S(u1, ii, jj, kk); });
-    };
-    auto zv = [&](int ii, int jj) {
-      return zdiff7(k, r, nz, kTopoStrPhdz4r, [&](int kk) { return S(v1, ii, jj, kk); });
-    };
-    d[3] = kD1 * S(u1, i, j, k) + kD0 * S(u1, i, j - 1, k) - kD1 * S(u1, i, j + 1, k) -
-           kD0 * S(u1, i, j + 2, k) -
-           J12i * gc *
-               (kP1 * F(a.f2_1, i, j) * zu(i, j) + kP0 * F(a.f2_1, i, j - 1) * zu(i, j - 1) +
-                kP1 * F(a.f2_1, i, j + 1) * zu(i, j + 1) + kP0 * F(a.f2_1, i, j + 2) * zu(i, j + 2));
-    d[4] = -kD1 * S(v1, i, j, k) + kD0 * S(v1, i - 2, j, k) + kD1 * S(v1, i - 1, j, k) -
-           kD0 * S(v1, i + 1, j, k) -
-           J12i * gc *
-               (kP1 * F(a.f1_2, i, j) * zv(i, j) + kP0 * F(a.f1_2, i - 2, j) * zv(i - 2, j) +
-                kP1 * F(a.f1_2, i - 1, j) * zv(i - 1, j) + kP0 * F(a.f1_2, i + 1, j) * zv(i + 1, j));
+    const float J12i = inv(X.fm(a.f, 0, 0) * gk(a.g3_c, r < 0 ? k + 6 : k));
+    const float u_ym1 = X.at(u1, 0, -1), u_yp1 = X.at(u1, 0, 1), u_yp2 = X.at(u1, 0, 2);
+    const float iu = kP1 * X.fm(a.f2_1, 0, 0) * u_0 + kP0 * X.fm(a.f2_1, 0, -1) * u_ym1 +
+                     kP1 * X.fm(a.f2_1, 0, 1) * u_yp1 + kP0 * X.fm(a.f2_1, 0, 2) * u_yp2;
+    d[3] = kD1 * u_0 + kD0 * u_ym1 - kD1 * u_yp1 - kD0 * u_yp2 -
+           J12i * gc * zd7(iu, c, kTopoStrPhdz4r);
+    const float v_xm2 = X.at(v1, -2, 0), v_xm1 = X.at(v1, -1, 0), v_xp1 = X.at(v1, 1, 0);
+    const float iv = kP1 * X.fm(a.f1_2, 0, 0) * v_0 + kP0 * X.fm(a.f1_2, -2, 0) * v_xm2 +
+                     kP1 * X.fm(a.f1_2, -1, 0) * v_xm1 + kP0 * X.fm(a.f1_2, 1, 0) * v_xp1;
+    d[4] = -kD1 * v_0 + kD0 * v_xm2 + kD1 * v_xm1 - kD0 * v_xp1 -
+           J12i * gc * zd7(iv, c, kTopoStrPhdz4r);
   }
   // ---- xz: J13i = 1 / (f_1 g3) (:550-598, :1254-1317)
   {
-    const float J13i = inv(F(a.f_1, i, j) * gk(a.g3, k));
-    auto zw = [&](int ii, int jj) {
-      return zdiff7(k, r, nz, kTopoStrPdhz4r, [&](int kk) { return S(w1, ii, jj, kk); });
-    };
-    d[5] = J13i * zdiff4(k, r, nz, false, kTopoStrDz4r, [&](int kk) { return S(u1, i, j, kk); });
-    d[6] = -kD1 * S(w1, i, j, k) + kD0 * S(w1, i - 2, j, k) + kD1 * S(w1, i - 1, j, k) -
-           kD0 * S(w1, i + 1, j, k) -
-           J13i * g *
-               (kP1 * F(a.f1_c, i, j) * zw(i, j) + kP0 * F(a.f1_c, i - 2, j) * zw(i - 2, j) +
-                kP1 * F(a.f1_c, i - 1, j) * zw(i - 1, j) + kP0 * F(a.f1_c, i + 1, j) * zw(i + 1, j));
+    const float J13i = inv(X.fm(a.f_1, 0, 0) * gk(a.g3, k));
+    d[5] = J13i * zd4(u_0, c, false, kTopoStrDz4r);
+    const float w_xm2 = X.at(w1, -2, 0), w_xm1 = X.at(w1, -1, 0), w_xp1 = X.at(w1, 1, 0);
+    const float iw = kP1 * X.fm(a.f1_c, 0, 0) * w_0 + kP0 * X.fm(a.f1_c, -2, 0) * w_xm2 +
+                     kP1 * X.fm(a.f1_c, -1, 0) * w_xm1 + kP0 * X.fm(a.f1_c, 1, 0) * w_xp1;
+    d[6] = -kD1 * w_0 + kD0 * w_xm2 + kD1 * w_xm1 - kD0 * w_xp1 -
+           J13i * g * zd7(iw, c, kTopoStrPdhz4r);
   }
   // ---- yz: J23i = 1 / (f_2 g3) (:600-650, :1319-1380)
   {
-    const float J23i = inv(F(a.f_2, i, j) * gk(a.g3, k));
-    auto zw = [&](int ii, int jj) {
-      return zdiff7(k, r, nz, kTopoStrPdhz4r, [&](int kk) { return S(w1, ii, jj, kk); });
-    };
-    d[7] = J23i * zdiff4(k, r, nz, false, kTopoStrDz4r, [&](int kk) { return S(v1, i, j, kk); });
-    d[8] = kD1 * S(w1, i, j, k) + kD0 * S(w1, i, j - 1, k) - kD1 * S(w1, i, j + 1, k) -
-           kD0 * S(w1, i, j + 2, k) -
-           J23i * g *
-               (kP1 * F(a.f2_c, i, j) * zw(i, j) + kP0 * F(a.f2_c, i, j - 1) * zw(i, j - 1) +
-                kP1 * F(a.f2_c, i, j + 1) * zw(i, j + 1) + kP0 * F(a.f2_c, i, j + 2) * zw(i, j + 2));
+    const float J23i = inv(X.fm(a.f_2, 0, 0) * gk(a.g3, k));
+    d[7] = J23i * zd4(v_0, c, false, kTopoStrDz4r);
+    const float w_ym1 = X.at(w1, 0, -1), w_yp1 = X.at(w1, 0, 1), w_yp2 = X.at(w1, 0, 2);
+    const float iw = kP1 * X.fm(a.f2_c, 0, 0) * w_0 + kP0 * X.fm(a.f2_c, 0, -1) * w_ym1 +
+                     kP1 * X.fm(a.f2_c, 0, 1) * w_yp1 + kP0 * X.fm(a.f2_c, 0, 2) * w_yp2;
+    d[8] = kD1 * w_0 + kD0 * w_ym1 - kD1 * w_yp1 - kD0 * w_yp2 -
+           J23i * g * zd7(iw, c, kTopoStrPdhz4r);
   }
 
-  // ---- material coefficients and the update (as the Cartesian dstrqc)
-  const long long o = X.p(i, j, k);
+  // ---- material coefficients and the update (as the Cartesian dstrqc); the
+  // k-1 neighbours of the eight-cell sums from the lane below
   const int S1 = a.slice, Y1 = a.yline;
+  const long long o = X.o;
   auto sum8 = [&](const float* __restrict__ m) {
-    return ld(m, o) + ld(m, o + S1) + ld(m, o - Y1) + ld(m, o + S1 - Y1) + ld(m, o - 1) +
-           ld(m, o + S1 - 1) + ld(m, o - Y1 - 1) + ld(m, o + S1 - Y1 - 1);
+    const float q0 = __ldg(m + o), q1 = __ldg(m + o + S1), q2 = __ldg(m + o - Y1),
+                q3 = __ldg(m + o + S1 - Y1);
+    return q0 + q1 + q2 + q3 + __shfl_up_sync(kAll, q0, 1) + __shfl_up_sync(kAll, q1, 1) +
+           __shfl_up_sync(kAll, q2, 1) + __shfl_up_sync(kAll, q3, 1);
   };
+  const float L8 = sum8(a.lam), M8 = sum8(a.mu);
+  const float QP8 = ELASTIC ? 0.f : sum8(a.qp), QS8 = ELASTIC ? 0.f : sum8(a.qs);
+  const float mu0 = __ldg(a.mu + o), muk = __shfl_up_sync(kAll, mu0, 1);
+  const float qs0 = ELASTIC ? 0.f : __ldg(a.qs + o);
+  const float qsk = __shfl_up_sync(kAll, qs0, 1);
+  if (!c.out) return;
   const int ia = i + AWP_NGSL + 2, ja = j + AWP_NGSL + 2, ka = k + AWP_ALIGN;
   const int t = awp_tex_index(a.tex, ia, ja, ka);
   const float f_vx1 = a.tex.tau1[t], f_vx2 = a.tex.tau2[t], f_wwo = a.tex.wwo8[t];
   const float cc0 = ELASTIC ? 0.f : a.coeff[2 * t], cc1 = ELASTIC ? 0.f : a.coeff[2 * t + 1];
   const AwpStrCoef cf = awp_stress_coef<ELASTIC>(
-      sum8(a.lam), sum8(a.mu), ld(a.mu, o), ld(a.mu, o - 1), ld(a.mu, o - Y1), ld(a.mu, o + S1),
-      ELASTIC ? 0.f : sum8(a.qp), ELASTIC ? 0.f : sum8(a.qs), ld(a.qs, o), ld(a.qs, o - 1),
-      ld(a.qs, o - Y1), ld(a.qs, o + S1), f_vx1, f_vx2, f_wwo, cc0, cc1, a.qthr, a.dth, a.dh1,
-      a.DT);
-  const float dcrj = ld(a.dcrjx, ia) * ld(a.dcrjy, ja) * ld(a.dcrjz, ka);
+      L8, M8, mu0, muk, __ldg(a.mu + o - Y1), __ldg(a.mu + o + S1), QP8, QS8, qs0, qsk,
+      ELASTIC ? 0.f : __ldg(a.qs + o - Y1), ELASTIC ? 0.f : __ldg(a.qs + o + S1), f_vx1, f_vx2,
+      f_wwo, cc0, cc1, a.qthr, a.dth, a.dh1, a.DT);
+  const float dcrj = __ldg(a.dcrjx + ia) * __ldg(a.dcrjy + ja) * __ldg(a.dcrjz + ka);
   float* const SG[6] = {a.xx, a.yy, a.zz, a.xy, a.xz, a.yz};
   float* const RR[6] = {a.r1, a.r2, a.r3, a.r4, a.r5, a.r6};
   float sg[6], rr[6];
@@ -318,10 +323,16 @@ __global__ void __launch_bounds__(128) k_topo_stress(const TopoArgs a) {
   }
 }
 
+// Tiles of a column: the top one, then one per 26 levels below it until a
+// tile reaches level 0.
+static unsigned column_tiles(int nz) {
+  return 1u + (nz > 32 ? (unsigned)((nz - 32 + kTileOut - 1) / kTileOut) : 0u);
+}
+
 cudaError_t awp_launch_topo_velocity(const TopoArgs& a, cudaStream_t st) {
   if (a.nz < 12 || a.nx < 1 || a.ny < 1) return cudaErrorInvalidValue;
   const dim3 block(32, 4, 1);
-  const dim3 grid((a.nz - 3 + 31) / 32, (a.ny + 3) / 4, a.nx);
+  const dim3 grid(column_tiles(a.nz), (a.ny + 3) / 4, a.nx);
   k_topo_velocity<<<grid, block, 0, st>>>(a);
   return cudaGetLastError();
 }
@@ -330,7 +341,7 @@ cudaError_t awp_launch_topo_stress(const TopoArgs& a, bool elastic, cudaStream_t
   if (a.nz < 12) return cudaErrorInvalidValue;
   if (a.e_i <= a.s_i || a.e_j <= a.s_j) return cudaSuccess;
   const dim3 block(32, 4, 1);
-  const dim3 grid((a.nz - 3 + 31) / 32, (a.e_j - a.s_j + 3) / 4, a.e_i - a.s_i);
+  const dim3 grid(column_tiles(a.nz), (a.e_j - a.s_j + 3) / 4, a.e_i - a.s_i);
   if (elastic)
     k_topo_stress<true><<<grid, block, 0, st>>>(a);
   else

@@ -400,7 +400,10 @@ int awp_phase_times(awp_ctx* ctx, double ms[AWP_NPHASES], long long launches[AWP
  * differ) and "spin_limit" (0 .. 2^30, default 2^26: polls of each pipeline
  * wait of the TMA kernels before it gives up, 0 = give up at once; a wait that
  * gives up makes the CTA drain its issued copies and leave, and the next
- * awp_synchronize of the context returns AWP_ERR_CUDA once).  Returns AWP_OK or AWP_ERR_ARG;
+ * awp_synchronize of the context returns AWP_ERR_CUDA once) and
+ * "l2_promotion" (0 none, 1 64 B, 2 128 B, 3 256 B (default): the L2 fetch
+ * granule of the TMA tiles, applied to contexts created afterwards; results
+ * do not change).  Returns AWP_OK or AWP_ERR_ARG;
  * awp_get_tuning returns the value or -1 for an unknown key. */
 int awp_set_tuning(const char* key, int value);
 int awp_get_tuning(const char* key);

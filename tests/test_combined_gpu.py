@@ -85,7 +85,9 @@ def test_topography_on_a_mesh_matches_reference(tmp_path):
 
 def test_plasticity_on_a_mesh_matches_reference():
     steps = 14
-    scns = scenarios.dm_small(nxc=10, nyc=8, nzs=(36, 24), steps=steps, q=True)
+    # the reference's NVE 3 strips need every block wider than 2 ngsl + a
+    # middle band in y (pmcl3d.c:573-631): coarse block 24 x 32
+    scns = scenarios.dm_small(nxc=24, nyc=32, nzs=(36, 24), steps=steps, q=True)
     for s in scns:
         s.params["nve"] = 3
         s.src_data = (s.src_data * 30.0).astype(np.float32)  # strong enough to yield
