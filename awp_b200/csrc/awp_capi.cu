@@ -1136,7 +1136,8 @@ int awp_gather_output(awp_ctx* c, int nbgx, int nedx, int nskpx, int nbgy, int n
   a.rec_nyt = (nedy - nbgy) / nskpy + 1;
   a.rec_nzt = (nedz - nbgz) / nskpz + 1;
   a.slice = c->g.slice; a.yline = c->g.yline; a.ktop = c->g.top();
-  a.w_shift = 1;
+  // w one cell below the recorded level on grid 0 only (kernel.cu:3975-3986)
+  a.w_shift = (c->p.grid == 0) ? 1 : 0;
   CU_TRY(awp_launch_velbuffer(a, c->stream));
   return AWP_OK;
 }

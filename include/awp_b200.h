@@ -351,7 +351,8 @@ int awp_field_upload(awp_ctx* ctx, int field, const float* host);
 int awp_field_device_ptr(awp_ctx* ctx, int field, float** dev_ptr);
 
 /* Surface / volume output gather of velbuffer (kernel.cu:3948-4011) into
- * caller buffers (device or pinned host), one value per recording point,
+ * caller buffers (device or pinned host), one value per recording point (on
+ * grid 0 the w component one cell below the recorded level, as velbuffer),
  * x fastest: rec_n = ((ned-nbg)/nskp+1) per axis, indices 0-based as
  * calcRecordingPoints (calc.c:9-72) returns them. */
 int awp_gather_output(awp_ctx* ctx, int nbgx, int nedx, int nskpx, int nbgy,

@@ -90,6 +90,9 @@ def compare_files(out, frames, axes, full, nt, ntiskp, wstep):
                     fr = frames[p][c][n0 + t]
                     want[t, :fr.shape[0], :fr.shape[1], :fr.shape[2]] = fr
                 assert got.size == want.size, (p, c, got.size, want.size)
+                if not np.any(want):  # before the wavefield reaches the points
+                    assert not np.any(got), (p, c, step)
+                    continue
                 errs[(p, c, step)] = rel_l2(got, want.ravel())
                 checked += 1
     assert checked > 0
@@ -133,7 +136,7 @@ def test_single_grid_output_matches_reference(tmp_path):
 def test_two_block_mesh_run_matches_reference(tmp_path):
     """pmcl3d -G 2 (a 3x finer block over a coarse one) against RefMeshSim:
     output of the top block's surface and of a plane of the coarse block."""
-    nt, ntiskp, wstep = 12, 2, 3
+    nt, ntiskp, wstep = 36, 2, 3
     scns = scenarios.dm_small(nxc=10, nyc=8, nzs=(36, 24), steps=nt, q=True)
     for p, s in enumerate(scns):
         write_block(s, tmp_path, p)
