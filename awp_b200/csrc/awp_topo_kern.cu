@@ -125,275 +125,215 @@ struct Cell {
 }  // namespace
 
 // ===========================================================================
-// Velocity: each warp marches a chunk of x planes of its (j, k) column; the x
-// stencils come from register queues (every value of the column loaded once
-// per chunk), the j neighbours of the current plane from L1.
+// Velocity
 // ===========================================================================
-__global__ void __launch_bounds__(128) k_topo_velocity(const TopoArgs a, const int ichunk) {
+__global__ void __launch_bounds__(128) k_topo_velocity(const TopoArgs a) {
   const ColPos c(a.nz, blockIdx.x);
   const int j = blockIdx.y * 4 + threadIdx.y;
-  const int ib = blockIdx.z * ichunk;
-  const int ie = min(ib + ichunk, a.nx) - 1;
-  if (j >= a.ny) return;  // whole warps
+  const int i = blockIdx.z;
+  if (j >= a.ny || i >= a.nx) return;  // whole warps
   const int k = c.k;
-  Cell X(a, ib, j, k);
-  const long long S = a.slice, F = a.fld;
+  const Cell X(a, i, j, k);
   const float *__restrict__ s11 = a.xx, *__restrict__ s12 = a.xy, *__restrict__ s13 = a.xz,
               *__restrict__ s22 = a.yy, *__restrict__ s23 = a.yz, *__restrict__ s33 = a.zz;
-  const float g3c = gk(a.g3_c, k), g3 = gk(a.g3, k), gc = gk(a.g_c, k), gg = gk(a.g, k);
-  const float dcjk = __ldg(a.dcrjy + j + AWP_NGSL + 2), dckk = __ldg(a.dcrjz + k + AWP_ALIGN);
-  // x queues of this column (index 0 = the oldest plane)
-  float q11[4] = {X.at(s11, -2, 0), X.at(s11, -1, 0), X.at(s11, 0, 0), 0.f};  // i-2..i+1
-  float q12[4] = {X.at(s12, -1, 0), X.at(s12, 0, 0), X.at(s12, 1, 0), 0.f};   // i-1..i+2
-  float q13[4] = {X.at(s13, -1, 0), X.at(s13, 0, 0), X.at(s13, 1, 0), 0.f};   // i-1..i+2
-  float qfc[4] = {X.fm(a.f_c, -2, 0), X.fm(a.f_c, -1, 0), X.fm(a.f_c, 0, 0), 0.f};  // i-2..i+1
-  float qf[4] = {X.fm(a.f, -1, 0), X.fm(a.f, 0, 0), X.fm(a.f, 1, 0), 0.f};          // i-1..i+2
-  float qf1[4] = {X.fm(a.f_1, -1, 0), X.fm(a.f_1, 0, 0), X.fm(a.f_1, 1, 0), 0.f};   // i-1..i+2
-  float rm0 = X.at(a.d1, -1, 0), rmm = X.at(a.d1, -1, -1);  // density of plane i-1
-  for (int i = ib; i <= ie; ++i) {
-    q11[3] = X.at(s11, 1, 0);
-    q12[3] = X.at(s12, 2, 0);
-    q13[3] = X.at(s13, 2, 0);
-    qfc[3] = X.fm(a.f_c, 1, 0);
-    qf[3] = X.fm(a.f, 2, 0);
-    qf1[3] = X.fm(a.f_1, 2, 0);
-    // density at the staggered velocity points (velocity_unroll.cu:140-152);
-    // the k-1 values from the lane below
-    const float r00 = X.at(a.d1, 0, 0), r0m = X.at(a.d1, 0, -1);
-    const float r00k = __shfl_up_sync(kAll, r00, 1), r0mk = __shfl_up_sync(kAll, r0m, 1),
-                rm0k = __shfl_up_sync(kAll, rm0, 1);
-    const float rho1 = 0.25f * (r00k + r0mk) + 0.25f * (r00 + r0m);
-    const float rho2 = 0.25f * (r00k + rm0k) + 0.25f * (r00 + rm0);
-    const float rho3 = 0.25f * (r00 + rm0) + 0.25f * (r0m + rmm);
-    const float fc = qfc[2], ff = qf[1], f1 = qf1[1], f2 = X.fm(a.f_2, 0, 0);
-    const float Ai1 = (float)((double)a.nu / (double)(f1 * g3c * rho1));
-    const float Ai2 = (float)((double)a.nu / (double)(f2 * g3c * rho2));
-    const float Ai3 = (float)((double)a.nu / (double)(fc * g3 * rho3));
-    const float dcrj = __ldg(a.dcrjx + i + AWP_NGSL + 2) * dcjk * dckk;
 
-    // --- u1 -----------------------------------------------------------------
-    const float y12_m2 = X.at(s12, 0, -2), y12_m1 = X.at(s12, 0, -1), y12_p1 = X.at(s12, 0, 1);
-    float s1 = -kD1 * fc * g3c * q11[2] + kD0 * qfc[0] * g3c * q11[0] +
-               kD1 * qfc[1] * g3c * q11[1] - kD0 * qfc[3] * g3c * q11[3];
-    s1 += -kD1 * ff * g3c * q12[1] + kD0 * X.fm(a.f, 0, -2) * g3c * y12_m2 +
-          kD1 * X.fm(a.f, 0, -1) * g3c * y12_m1 - kD0 * X.fm(a.f, 0, 1) * g3c * y12_p1;
-    s1 += zd4(q13[1], c, true, kTopoVelDhz4r);
-    {
-      const float px = gc * (kP1 * q11[2] + kP0 * q11[0] + kP1 * q11[1] + kP0 * q11[3]);
-      const float py = gc * (kP1 * q12[1] + kP0 * y12_m2 + kP1 * y12_m1 + kP0 * y12_p1);
-      s1 = s1 - X.fm(a.f1_1, 0, 0) * zd7(px, c, kTopoVelDhpz4r);
-      s1 = s1 - X.fm(a.f2_1, 0, 0) * zd7(py, c, kTopoVelDhpz4r);
-    }
-    // --- u2 -----------------------------------------------------------------
-    const float x23_0 = X.at(s23, 0, 0);
-    float s2 = zd4(x23_0, c, true, kTopoVelDhz4r);
-    s2 += kD1 * ff * g3c * q12[1] + kD0 * qf[0] * g3c * q12[0] - kD1 * qf[2] * g3c * q12[2] -
-          kD0 * qf[3] * g3c * q12[3];
-    const float y22_0 = X.at(s22, 0, 0), y22_m1 = X.at(s22, 0, -1), y22_p1 = X.at(s22, 0, 1),
-                y22_p2 = X.at(s22, 0, 2);
-    s2 += kD1 * fc * g3c * y22_0 + kD0 * X.fm(a.f_c, 0, -1) * g3c * y22_m1 -
-          kD1 * X.fm(a.f_c, 0, 1) * g3c * y22_p1 - kD0 * X.fm(a.f_c, 0, 2) * g3c * y22_p2;
-    {
-      const float px = gc * (kP1 * q12[1] + kP0 * q12[0] + kP1 * q12[2] + kP0 * q12[3]);
-      const float py = gc * (kP1 * y22_0 + kP0 * y22_m1 + kP1 * y22_p1 + kP0 * y22_p2);
-      s2 = s2 - X.fm(a.f1_2, 0, 0) * zd7(px, c, kTopoVelDhpz4r);
-      s2 = s2 - X.fm(a.f2_2, 0, 0) * zd7(py, c, kTopoVelDhpz4r);
-    }
-    // --- u3 -----------------------------------------------------------------
-    const float y23_m2 = X.at(s23, 0, -2), y23_m1 = X.at(s23, 0, -1), y23_p1 = X.at(s23, 0, 1);
-    float s3 = -kD1 * f2 * g3 * x23_0 + kD0 * X.fm(a.f_2, 0, -2) * g3 * y23_m2 +
-               kD1 * X.fm(a.f_2, 0, -1) * g3 * y23_m1 - kD0 * X.fm(a.f_2, 0, 1) * g3 * y23_p1;
-    s3 += kD1 * f1 * g3 * q13[1] + kD0 * qf1[0] * g3 * q13[0] - kD1 * qf1[2] * g3 * q13[2] -
-          kD0 * qf1[3] * g3 * q13[3];
-    s3 += zd4(X.at(s33, 0, 0), c, false, kTopoVelDz4r);
-    {
-      const float px = gg * (kP1 * q13[1] + kP0 * q13[0] + kP1 * q13[2] + kP0 * q13[3]);
-      const float py = gg * (kP1 * x23_0 + kP0 * y23_m2 + kP1 * y23_m1 + kP0 * y23_p1);
-      s3 = s3 - X.fm(a.f1_c, 0, 0) * zd7(px, c, kTopoVelDphz4r);
-      s3 = s3 - X.fm(a.f2_c, 0, 0) * zd7(py, c, kTopoVelDphz4r);
-    }
-    if (c.out) {
-      const long long o = X.o;
-      a.u1[o] = (a.u1[o] + Ai1 * s1) * dcrj;
-      a.v1[o] = (a.v1[o] + Ai2 * s2) * dcrj;
-      a.w1[o] = (a.w1[o] + Ai3 * s3) * dcrj;
-    }
-    // advance the queues and the cell to plane i+1
-#pragma unroll
-    for (int q = 0; q < 3; ++q) {
-      q11[q] = q11[q + 1]; q12[q] = q12[q + 1]; q13[q] = q13[q + 1];
-      qfc[q] = qfc[q + 1]; qf[q] = qf[q + 1]; qf1[q] = qf1[q + 1];
-    }
-    rm0 = r00;
-    rmm = r0m;
-    X.o += S;
-    X.of += F;
+  // density at the staggered velocity points (velocity_unroll.cu:140-152); the
+  // k-1 values from the lane below
+  const float r00 = X.at(a.d1, 0, 0), r0m = X.at(a.d1, 0, -1), rm0 = X.at(a.d1, -1, 0),
+              rmm = X.at(a.d1, -1, -1);
+  const float r00k = __shfl_up_sync(kAll, r00, 1), r0mk = __shfl_up_sync(kAll, r0m, 1),
+              rm0k = __shfl_up_sync(kAll, rm0, 1);
+  const float rho1 = 0.25f * (r00k + r0mk) + 0.25f * (r00 + r0m);
+  const float rho2 = 0.25f * (r00k + rm0k) + 0.25f * (r00 + rm0);
+  const float rho3 = 0.25f * (r00 + rm0) + 0.25f * (r0m + rmm);
+  const float g3c = gk(a.g3_c, k), g3 = gk(a.g3, k), gc = gk(a.g_c, k), gg = gk(a.g, k);
+  const float fc = X.fm(a.f_c, 0, 0);
+  const float Ai1 = (float)((double)a.nu / (double)(X.fm(a.f_1, 0, 0) * g3c * rho1));
+  const float Ai2 = (float)((double)a.nu / (double)(X.fm(a.f_2, 0, 0) * g3c * rho2));
+  const float Ai3 = (float)((double)a.nu / (double)(fc * g3 * rho3));
+  const float dcrj = __ldg(a.dcrjx + i + AWP_NGSL + 2) * __ldg(a.dcrjy + j + AWP_NGSL + 2) *
+                     __ldg(a.dcrjz + k + AWP_ALIGN);
+
+  // --- u1 -------------------------------------------------------------------
+  const float x11_0 = X.at(s11, 0, 0), x11_m2 = X.at(s11, -2, 0), x11_m1 = X.at(s11, -1, 0),
+              x11_p1 = X.at(s11, 1, 0);
+  const float y12_0 = X.at(s12, 0, 0), y12_m2 = X.at(s12, 0, -2), y12_m1 = X.at(s12, 0, -1),
+              y12_p1 = X.at(s12, 0, 1);
+  float s1 = -kD1 * fc * g3c * x11_0 + kD0 * X.fm(a.f_c, -2, 0) * g3c * x11_m2 +
+             kD1 * X.fm(a.f_c, -1, 0) * g3c * x11_m1 - kD0 * X.fm(a.f_c, 1, 0) * g3c * x11_p1;
+  const float ff = X.fm(a.f, 0, 0);
+  s1 += -kD1 * ff * g3c * y12_0 + kD0 * X.fm(a.f, 0, -2) * g3c * y12_m2 +
+        kD1 * X.fm(a.f, 0, -1) * g3c * y12_m1 - kD0 * X.fm(a.f, 0, 1) * g3c * y12_p1;
+  const float x13_0 = X.at(s13, 0, 0);
+  s1 += zd4(x13_0, c, true, kTopoVelDhz4r);
+  {
+    const float px = gc * (kP1 * x11_0 + kP0 * x11_m2 + kP1 * x11_m1 + kP0 * x11_p1);
+    const float py = gc * (kP1 * y12_0 + kP0 * y12_m2 + kP1 * y12_m1 + kP0 * y12_p1);
+    s1 = s1 - X.fm(a.f1_1, 0, 0) * zd7(px, c, kTopoVelDhpz4r);
+    s1 = s1 - X.fm(a.f2_1, 0, 0) * zd7(py, c, kTopoVelDhpz4r);
   }
+  // --- u2 -------------------------------------------------------------------
+  const float x23_0 = X.at(s23, 0, 0);
+  float s2 = zd4(x23_0, c, true, kTopoVelDhz4r);
+  const float x12_m1 = X.at(s12, -1, 0), x12_p1 = X.at(s12, 1, 0), x12_p2 = X.at(s12, 2, 0);
+  s2 += kD1 * ff * g3c * y12_0 + kD0 * X.fm(a.f, -1, 0) * g3c * x12_m1 -
+        kD1 * X.fm(a.f, 1, 0) * g3c * x12_p1 - kD0 * X.fm(a.f, 2, 0) * g3c * x12_p2;
+  const float y22_0 = X.at(s22, 0, 0), y22_m1 = X.at(s22, 0, -1), y22_p1 = X.at(s22, 0, 1),
+              y22_p2 = X.at(s22, 0, 2);
+  s2 += kD1 * fc * g3c * y22_0 + kD0 * X.fm(a.f_c, 0, -1) * g3c * y22_m1 -
+        kD1 * X.fm(a.f_c, 0, 1) * g3c * y22_p1 - kD0 * X.fm(a.f_c, 0, 2) * g3c * y22_p2;
+  {
+    const float px = gc * (kP1 * y12_0 + kP0 * x12_m1 + kP1 * x12_p1 + kP0 * x12_p2);
+    const float py = gc * (kP1 * y22_0 + kP0 * y22_m1 + kP1 * y22_p1 + kP0 * y22_p2);
+    s2 = s2 - X.fm(a.f1_2, 0, 0) * zd7(px, c, kTopoVelDhpz4r);
+    s2 = s2 - X.fm(a.f2_2, 0, 0) * zd7(py, c, kTopoVelDhpz4r);
+  }
+  // --- u3 -------------------------------------------------------------------
+  const float f2 = X.fm(a.f_2, 0, 0), f1 = X.fm(a.f_1, 0, 0);
+  const float y23_m2 = X.at(s23, 0, -2), y23_m1 = X.at(s23, 0, -1), y23_p1 = X.at(s23, 0, 1);
+  float s3 = -kD1 * f2 * g3 * x23_0 + kD0 * X.fm(a.f_2, 0, -2) * g3 * y23_m2 +
+             kD1 * X.fm(a.f_2, 0, -1) * g3 * y23_m1 - kD0 * X.fm(a.f_2, 0, 1) * g3 * y23_p1;
+  const float x13_m1 = X.at(s13, -1, 0), x13_p1 = X.at(s13, 1, 0), x13_p2 = X.at(s13, 2, 0);
+  s3 += kD1 * f1 * g3 * x13_0 + kD0 * X.fm(a.f_1, -1, 0) * g3 * x13_m1 -
+        kD1 * X.fm(a.f_1, 1, 0) * g3 * x13_p1 - kD0 * X.fm(a.f_1, 2, 0) * g3 * x13_p2;
+  s3 += zd4(X.at(s33, 0, 0), c, false, kTopoVelDz4r);
+  {
+    const float px = gg * (kP1 * x13_0 + kP0 * x13_m1 + kP1 * x13_p1 + kP0 * x13_p2);
+    const float py = gg * (kP1 * x23_0 + kP0 * y23_m2 + kP1 * y23_m1 + kP0 * y23_p1);
+    s3 = s3 - X.fm(a.f1_c, 0, 0) * zd7(px, c, kTopoVelDphz4r);
+    s3 = s3 - X.fm(a.f2_c, 0, 0) * zd7(py, c, kTopoVelDphz4r);
+  }
+
+  if (!c.out) return;
+  const long long o = X.o;
+  a.u1[o] = (a.u1[o] + Ai1 * s1) * dcrj;
+  a.v1[o] = (a.v1[o] + Ai2 * s2) * dcrj;
+  a.w1[o] = (a.w1[o] + Ai3 * s3) * dcrj;
 }
 
 // ===========================================================================
-// Stress and memory variables, marched like the velocity
+// Stress and memory variables
 // ===========================================================================
 template <bool ELASTIC>
-__global__ void __launch_bounds__(128) k_topo_stress(const TopoArgs a, const int ichunk) {
+__global__ void __launch_bounds__(128) k_topo_stress(const TopoArgs a) {
   const ColPos c(a.nz, blockIdx.x);
   const int j = a.s_j + blockIdx.y * 4 + threadIdx.y;
-  const int ib = a.s_i + blockIdx.z * ichunk;
-  const int ie = min(ib + ichunk, a.e_i) - 1;
-  if (j >= a.e_j) return;  // whole warps
+  const int i = a.s_i + blockIdx.z;
+  if (j >= a.e_j || i >= a.e_i) return;  // whole warps
   const int k = c.k, r = c.r;
-  Cell X(a, ib, j, k);
-  const long long S = a.slice, F = a.fld;
-  const int Y1 = a.yline;
+  const Cell X(a, i, j, k);
   const float *__restrict__ u1 = a.u1, *__restrict__ v1 = a.v1, *__restrict__ w1 = a.w1;
-  const float gc = gk(a.g_c, k), g = gk(a.g, k), g3c = gk(a.g3_c, k), g3 = gk(a.g3, k);
-  // the interior xy rows read g3_c six points higher (stress_attenuation.cu:471),
-  // the boundary rows at k (:1149)
-  const float g3c12 = gk(a.g3_c, r < 0 ? k + 6 : k);
-  const int ja = j + AWP_NGSL + 2, ka = k + AWP_ALIGN;
-  const float dcjk = __ldg(a.dcrjy + ja), dckk = __ldg(a.dcrjz + ka);
-  // x queues of this column (index 0 = the oldest plane)
-  float qu[4] = {X.at(u1, -1, 0), X.at(u1, 0, 0), X.at(u1, 1, 0), 0.f};   // i-1..i+2
-  float qv[4] = {X.at(v1, -2, 0), X.at(v1, -1, 0), X.at(v1, 0, 0), 0.f};  // i-2..i+1
-  float qw[4] = {X.at(w1, -2, 0), X.at(w1, -1, 0), X.at(w1, 0, 0), 0.f};  // i-2..i+1
-  float q11[4] = {X.fm(a.f1_1, -1, 0), X.fm(a.f1_1, 0, 0), X.fm(a.f1_1, 1, 0), 0.f};  // i-1..
-  float q12[4] = {X.fm(a.f1_2, -2, 0), X.fm(a.f1_2, -1, 0), X.fm(a.f1_2, 0, 0), 0.f};  // i-2..
-  float q1c[4] = {X.fm(a.f1_c, -2, 0), X.fm(a.f1_c, -1, 0), X.fm(a.f1_c, 0, 0), 0.f};  // i-2..
-  // media of plane i at (j, k) and (j-1, k); the next plane's loaded per step
-  float lam0 = __ldg(a.lam + X.o), lamj = __ldg(a.lam + X.o - Y1);
-  float mu0 = __ldg(a.mu + X.o), muj = __ldg(a.mu + X.o - Y1);
-  float qp0 = 0.f, qpj = 0.f, qs0 = 0.f, qsj = 0.f;
-  if (!ELASTIC) {
-    qp0 = __ldg(a.qp + X.o); qpj = __ldg(a.qp + X.o - Y1);
-    qs0 = __ldg(a.qs + X.o); qsj = __ldg(a.qs + X.o - Y1);
+  const float gc = gk(a.g_c, k), g = gk(a.g, k);
+
+  // every vertical difference of a horizontal interpolant is one difference
+  // of the interpolated column (the metric weights do not depend on k)
+  float d[9];
+  // ---- normal components: Jii = 1 / (f_c g3_c) (stress_attenuation.cu:340-431)
+  const float Jii = inv(X.fm(a.f_c, 0, 0) * gk(a.g3_c, k));
+  const float u_0 = X.at(u1, 0, 0), u_xm1 = X.at(u1, -1, 0), u_xp1 = X.at(u1, 1, 0),
+              u_xp2 = X.at(u1, 2, 0);
+  const float v_0 = X.at(v1, 0, 0), v_ym2 = X.at(v1, 0, -2), v_ym1 = X.at(v1, 0, -1),
+              v_yp1 = X.at(v1, 0, 1);
+  const float w_0 = X.at(w1, 0, 0);
+  {
+    const float iu = kP0 * X.fm(a.f1_1, -1, 0) * u_xm1 + kP1 * X.fm(a.f1_1, 0, 0) * u_0 +
+                     kP1 * X.fm(a.f1_1, 1, 0) * u_xp1 + kP0 * X.fm(a.f1_1, 2, 0) * u_xp2;
+    d[0] = kD1 * u_0 + kD0 * u_xm1 - kD1 * u_xp1 - kD0 * u_xp2 -
+           Jii * gc * zd7(iu, c, kTopoStrPhdz4r);
+    const float iv = kP1 * X.fm(a.f2_2, 0, 0) * v_0 + kP0 * X.fm(a.f2_2, 0, -2) * v_ym2 +
+                     kP1 * X.fm(a.f2_2, 0, -1) * v_ym1 + kP0 * X.fm(a.f2_2, 0, 1) * v_yp1;
+    d[1] = -kD1 * v_0 + kD0 * v_ym2 + kD1 * v_ym1 - kD0 * v_yp1 -
+           Jii * gc * zd7(iv, c, kTopoStrPhdz4r);
+    d[2] = Jii * zd4(w_0, c, true, kTopoStrDhz4r);
   }
+  // ---- xy: J12i = 1 / (f g3_c); the interior rows read g3_c six points
+  // higher (stress_attenuation.cu:471), the boundary rows at k (:1149)
+  {
+    const float J12i = inv(X.fm(a.f, 0, 0) * gk(a.g3_c, r < 0 ? k + 6 : k));
+    const float u_ym1 = X.at(u1, 0, -1), u_yp1 = X.at(u1, 0, 1), u_yp2 = X.at(u1, 0, 2);
+    const float iu = kP1 * X.fm(a.f2_1, 0, 0) * u_0 + kP0 * X.fm(a.f2_1, 0, -1) * u_ym1 +
+                     kP1 * X.fm(a.f2_1, 0, 1) * u_yp1 + kP0 * X.fm(a.f2_1, 0, 2) * u_yp2;
+    d[3] = kD1 * u_0 + kD0 * u_ym1 - kD1 * u_yp1 - kD0 * u_yp2 -
+           J12i * gc * zd7(iu, c, kTopoStrPhdz4r);
+    const float v_xm2 = X.at(v1, -2, 0), v_xm1 = X.at(v1, -1, 0), v_xp1 = X.at(v1, 1, 0);
+    const float iv = kP1 * X.fm(a.f1_2, 0, 0) * v_0 + kP0 * X.fm(a.f1_2, -2, 0) * v_xm2 +
+                     kP1 * X.fm(a.f1_2, -1, 0) * v_xm1 + kP0 * X.fm(a.f1_2, 1, 0) * v_xp1;
+    d[4] = -kD1 * v_0 + kD0 * v_xm2 + kD1 * v_xm1 - kD0 * v_xp1 -
+           J12i * gc * zd7(iv, c, kTopoStrPhdz4r);
+  }
+  // ---- xz: J13i = 1 / (f_1 g3) (:550-598, :1254-1317)
+  {
+    const float J13i = inv(X.fm(a.f_1, 0, 0) * gk(a.g3, k));
+    d[5] = J13i * zd4(u_0, c, false, kTopoStrDz4r);
+    const float w_xm2 = X.at(w1, -2, 0), w_xm1 = X.at(w1, -1, 0), w_xp1 = X.at(w1, 1, 0);
+    const float iw = kP1 * X.fm(a.f1_c, 0, 0) * w_0 + kP0 * X.fm(a.f1_c, -2, 0) * w_xm2 +
+                     kP1 * X.fm(a.f1_c, -1, 0) * w_xm1 + kP0 * X.fm(a.f1_c, 1, 0) * w_xp1;
+    d[6] = -kD1 * w_0 + kD0 * w_xm2 + kD1 * w_xm1 - kD0 * w_xp1 -
+           J13i * g * zd7(iw, c, kTopoStrPdhz4r);
+  }
+  // ---- yz: J23i = 1 / (f_2 g3) (:600-650, :1319-1380)
+  {
+    const float J23i = inv(X.fm(a.f_2, 0, 0) * gk(a.g3, k));
+    d[7] = J23i * zd4(v_0, c, false, kTopoStrDz4r);
+    const float w_ym1 = X.at(w1, 0, -1), w_yp1 = X.at(w1, 0, 1), w_yp2 = X.at(w1, 0, 2);
+    const float iw = kP1 * X.fm(a.f2_c, 0, 0) * w_0 + kP0 * X.fm(a.f2_c, 0, -1) * w_ym1 +
+                     kP1 * X.fm(a.f2_c, 0, 1) * w_yp1 + kP0 * X.fm(a.f2_c, 0, 2) * w_yp2;
+    d[8] = kD1 * w_0 + kD0 * w_ym1 - kD1 * w_yp1 - kD0 * w_yp2 -
+           J23i * g * zd7(iw, c, kTopoStrPdhz4r);
+  }
+
+  // ---- material coefficients and the update (as the Cartesian dstrqc); the
+  // k-1 neighbours of the eight-cell sums from the lane below
+  const int S1 = a.slice, Y1 = a.yline;
+  const long long o = X.o;
+  auto sum8 = [&](const float* __restrict__ m) {
+    const float q0 = __ldg(m + o), q1 = __ldg(m + o + S1), q2 = __ldg(m + o - Y1),
+                q3 = __ldg(m + o + S1 - Y1);
+    return q0 + q1 + q2 + q3 + __shfl_up_sync(kAll, q0, 1) + __shfl_up_sync(kAll, q1, 1) +
+           __shfl_up_sync(kAll, q2, 1) + __shfl_up_sync(kAll, q3, 1);
+  };
+  const float L8 = sum8(a.lam), M8 = sum8(a.mu);
+  const float QP8 = ELASTIC ? 0.f : sum8(a.qp), QS8 = ELASTIC ? 0.f : sum8(a.qs);
+  const float mu0 = __ldg(a.mu + o), muk = __shfl_up_sync(kAll, mu0, 1);
+  const float qs0 = ELASTIC ? 0.f : __ldg(a.qs + o);
+  const float qsk = __shfl_up_sync(kAll, qs0, 1);
+  if (!c.out) return;
+  const int ia = i + AWP_NGSL + 2, ja = j + AWP_NGSL + 2, ka = k + AWP_ALIGN;
+  const int t = awp_tex_index(a.tex, ia, ja, ka);
+  const float f_vx1 = a.tex.tau1[t], f_vx2 = a.tex.tau2[t], f_wwo = a.tex.wwo8[t];
+  const float cc0 = ELASTIC ? 0.f : a.coeff[2 * t], cc1 = ELASTIC ? 0.f : a.coeff[2 * t + 1];
+  const AwpStrCoef cf = awp_stress_coef<ELASTIC>(
+      L8, M8, mu0, muk, __ldg(a.mu + o - Y1), __ldg(a.mu + o + S1), QP8, QS8, qs0, qsk,
+      ELASTIC ? 0.f : __ldg(a.qs + o - Y1), ELASTIC ? 0.f : __ldg(a.qs + o + S1), f_vx1, f_vx2,
+      f_wwo, cc0, cc1, a.qthr, a.dth, a.dh1, a.DT);
+  const float dcrj = __ldg(a.dcrjx + ia) * __ldg(a.dcrjy + ja) * __ldg(a.dcrjz + ka);
   float* const SG[6] = {a.xx, a.yy, a.zz, a.xy, a.xz, a.yz};
   float* const RR[6] = {a.r1, a.r2, a.r3, a.r4, a.r5, a.r6};
-  for (int i = ib; i <= ie; ++i) {
-    qu[3] = X.at(u1, 2, 0);
-    qv[3] = X.at(v1, 1, 0);
-    qw[3] = X.at(w1, 1, 0);
-    q11[3] = X.fm(a.f1_1, 2, 0);
-    q12[3] = X.fm(a.f1_2, 1, 0);
-    q1c[3] = X.fm(a.f1_c, 1, 0);
-    const float u_0 = qu[1], v_0 = qv[2], w_0 = qw[2];
-
-    // every vertical difference of a horizontal interpolant is one difference
-    // of the interpolated column (the metric weights do not depend on k)
-    float d[9];
-    // ---- normal components: Jii = 1 / (f_c g3_c) (stress_attenuation.cu:340-431)
-    const float Jii = inv(X.fm(a.f_c, 0, 0) * g3c);
-    {
-      const float iu = kP0 * q11[0] * qu[0] + kP1 * q11[1] * u_0 + kP1 * q11[2] * qu[2] +
-                       kP0 * q11[3] * qu[3];
-      d[0] = kD1 * u_0 + kD0 * qu[0] - kD1 * qu[2] - kD0 * qu[3] -
-             Jii * gc * zd7(iu, c, kTopoStrPhdz4r);
-      const float v_ym2 = X.at(v1, 0, -2), v_ym1 = X.at(v1, 0, -1), v_yp1 = X.at(v1, 0, 1);
-      const float iv = kP1 * X.fm(a.f2_2, 0, 0) * v_0 + kP0 * X.fm(a.f2_2, 0, -2) * v_ym2 +
-                       kP1 * X.fm(a.f2_2, 0, -1) * v_ym1 + kP0 * X.fm(a.f2_2, 0, 1) * v_yp1;
-      d[1] = -kD1 * v_0 + kD0 * v_ym2 + kD1 * v_ym1 - kD0 * v_yp1 -
-             Jii * gc * zd7(iv, c, kTopoStrPhdz4r);
-      d[2] = Jii * zd4(w_0, c, true, kTopoStrDhz4r);
-    }
-    // ---- xy: J12i = 1 / (f g3_c)
-    {
-      const float J12i = inv(X.fm(a.f, 0, 0) * g3c12);
-      const float u_ym1 = X.at(u1, 0, -1), u_yp1 = X.at(u1, 0, 1), u_yp2 = X.at(u1, 0, 2);
-      const float iu = kP1 * X.fm(a.f2_1, 0, 0) * u_0 + kP0 * X.fm(a.f2_1, 0, -1) * u_ym1 +
-                       kP1 * X.fm(a.f2_1, 0, 1) * u_yp1 + kP0 * X.fm(a.f2_1, 0, 2) * u_yp2;
-      d[3] = kD1 * u_0 + kD0 * u_ym1 - kD1 * u_yp1 - kD0 * u_yp2 -
-             J12i * gc * zd7(iu, c, kTopoStrPhdz4r);
-      const float iv = kP1 * q12[2] * v_0 + kP0 * q12[0] * qv[0] + kP1 * q12[1] * qv[1] +
-                       kP0 * q12[3] * qv[3];
-      d[4] = -kD1 * v_0 + kD0 * qv[0] + kD1 * qv[1] - kD0 * qv[3] -
-             J12i * gc * zd7(iv, c, kTopoStrPhdz4r);
-    }
-    // ---- xz: J13i = 1 / (f_1 g3) (:550-598, :1254-1317)
-    {
-      const float J13i = inv(X.fm(a.f_1, 0, 0) * g3);
-      d[5] = J13i * zd4(u_0, c, false, kTopoStrDz4r);
-      const float iw = kP1 * q1c[2] * w_0 + kP0 * q1c[0] * qw[0] + kP1 * q1c[1] * qw[1] +
-                       kP0 * q1c[3] * qw[3];
-      d[6] = -kD1 * w_0 + kD0 * qw[0] + kD1 * qw[1] - kD0 * qw[3] -
-             J13i * g * zd7(iw, c, kTopoStrPdhz4r);
-    }
-    // ---- yz: J23i = 1 / (f_2 g3) (:600-650, :1319-1380)
-    {
-      const float J23i = inv(X.fm(a.f_2, 0, 0) * g3);
-      d[7] = J23i * zd4(v_0, c, false, kTopoStrDz4r);
-      const float w_ym1 = X.at(w1, 0, -1), w_yp1 = X.at(w1, 0, 1), w_yp2 = X.at(w1, 0, 2);
-      const float iw = kP1 * X.fm(a.f2_c, 0, 0) * w_0 + kP0 * X.fm(a.f2_c, 0, -1) * w_ym1 +
-                       kP1 * X.fm(a.f2_c, 0, 1) * w_yp1 + kP0 * X.fm(a.f2_c, 0, 2) * w_yp2;
-      d[8] = kD1 * w_0 + kD0 * w_ym1 - kD1 * w_yp1 - kD0 * w_yp2 -
-             J23i * g * zd7(iw, c, kTopoStrPdhz4r);
-    }
-
-    // ---- material coefficients (eight-cell sums over planes i, i+1) and the
-    // update as the Cartesian dstrqc; k-1 values from the lane below
-    const long long o = X.o;
-    const float lamn = __ldg(a.lam + o + S), lamnj = __ldg(a.lam + o + S - Y1);
-    const float mun = __ldg(a.mu + o + S), munj = __ldg(a.mu + o + S - Y1);
-    auto sum8 = [&](float q0, float q1, float q2, float q3) {
-      return q0 + q1 + q2 + q3 + __shfl_up_sync(kAll, q0, 1) + __shfl_up_sync(kAll, q1, 1) +
-             __shfl_up_sync(kAll, q2, 1) + __shfl_up_sync(kAll, q3, 1);
-    };
-    const float L8 = sum8(lam0, lamn, lamj, lamnj), M8 = sum8(mu0, mun, muj, munj);
-    const float muk = __shfl_up_sync(kAll, mu0, 1);
-    float QP8 = 0.f, QS8 = 0.f, qsk = 0.f, qpn = 0.f, qpnj = 0.f, qsn = 0.f, qsnj = 0.f;
-    if (!ELASTIC) {
-      qpn = __ldg(a.qp + o + S); qpnj = __ldg(a.qp + o + S - Y1);
-      qsn = __ldg(a.qs + o + S); qsnj = __ldg(a.qs + o + S - Y1);
-      QP8 = sum8(qp0, qpn, qpj, qpnj);
-      QS8 = sum8(qs0, qsn, qsj, qsnj);
-      qsk = __shfl_up_sync(kAll, qs0, 1);
-    }
-    if (c.out) {
-      const int ia = i + AWP_NGSL + 2;
-      const int t = awp_tex_index(a.tex, ia, ja, ka);
-      const float f_vx1 = a.tex.tau1[t], f_vx2 = a.tex.tau2[t], f_wwo = a.tex.wwo8[t];
-      const float cc0 = ELASTIC ? 0.f : a.coeff[2 * t], cc1 = ELASTIC ? 0.f : a.coeff[2 * t + 1];
-      const AwpStrCoef cf = awp_stress_coef<ELASTIC>(
-          L8, M8, mu0, muk, muj, mun, QP8, QS8, qs0, qsk, qsj, qsn, f_vx1, f_vx2, f_wwo, cc0,
-          cc1, a.qthr, a.dth, a.dh1, a.DT);
-      const float dcrj = __ldg(a.dcrjx + ia) * dcjk * dckk;
-      float sg[6], rr[6];
+  float sg[6], rr[6];
 #pragma unroll
-      for (int q = 0; q < 6; ++q) {
-        sg[q] = SG[q][o];
-        rr[q] = ELASTIC ? 0.f : RR[q][o];
-      }
-      awp_stress_update<ELASTIC>(sg, rr, cf, f_vx1, f_vx2, f_wwo, a.DT, dcrj, d);
+  for (int q = 0; q < 6; ++q) {
+    sg[q] = SG[q][o];
+    rr[q] = ELASTIC ? 0.f : RR[q][o];
+  }
+  awp_stress_update<ELASTIC>(sg, rr, cf, f_vx1, f_vx2, f_wwo, a.DT, dcrj, d);
 #pragma unroll
-      for (int q = 0; q < 6; ++q) {
-        SG[q][o] = sg[q];
-        if (!ELASTIC) RR[q][o] = rr[q];
-      }
-    }
-    // advance to plane i+1
-#pragma unroll
-    for (int q = 0; q < 3; ++q) {
-      qu[q] = qu[q + 1]; qv[q] = qv[q + 1]; qw[q] = qw[q + 1];
-      q11[q] = q11[q + 1]; q12[q] = q12[q + 1]; q1c[q] = q1c[q + 1];
-    }
-    lam0 = lamn; lamj = lamnj; mu0 = mun; muj = munj;
-    qp0 = qpn; qpj = qpnj; qs0 = qsn; qsj = qsnj;
-    X.o += S;
-    X.of += F;
+  for (int q = 0; q < 6; ++q) {
+    SG[q][o] = sg[q];
+    if (!ELASTIC) RR[q][o] = rr[q];
   }
 }
 
+// Tiles of a column: the top one, then one per 26 levels below it until a
+// tile reaches level 0.
 static unsigned column_tiles(int nz) {
   return 1u + (nz > 32 ? (unsigned)((nz - 32 + kTileOut - 1) / kTileOut) : 0u);
 }
 
-// x planes a warp marches (register queues along x)
-constexpr int kTopoChunk = 16;
-
 cudaError_t awp_launch_topo_velocity(const TopoArgs& a, cudaStream_t st) {
   if (a.nz < 12 || a.nx < 1 || a.ny < 1) return cudaErrorInvalidValue;
   const dim3 block(32, 4, 1);
-  const dim3 grid(column_tiles(a.nz), (a.ny + 3) / 4, (a.nx + kTopoChunk - 1) / kTopoChunk);
-  k_topo_velocity<<<grid, block, 0, st>>>(a, kTopoChunk);
+  const dim3 grid(column_tiles(a.nz), (a.ny + 3) / 4, a.nx);
+  k_topo_velocity<<<grid, block, 0, st>>>(a);
   return cudaGetLastError();
 }
 
@@ -401,11 +341,10 @@ cudaError_t awp_launch_topo_stress(const TopoArgs& a, bool elastic, cudaStream_t
   if (a.nz < 12) return cudaErrorInvalidValue;
   if (a.e_i <= a.s_i || a.e_j <= a.s_j) return cudaSuccess;
   const dim3 block(32, 4, 1);
-  const dim3 grid(column_tiles(a.nz), (a.e_j - a.s_j + 3) / 4,
-                  (a.e_i - a.s_i + kTopoChunk - 1) / kTopoChunk);
+  const dim3 grid(column_tiles(a.nz), (a.e_j - a.s_j + 3) / 4, a.e_i - a.s_i);
   if (elastic)
-    k_topo_stress<true><<<grid, block, 0, st>>>(a, kTopoChunk);
+    k_topo_stress<true><<<grid, block, 0, st>>>(a);
   else
-    k_topo_stress<false><<<grid, block, 0, st>>>(a, kTopoChunk);
+    k_topo_stress<false><<<grid, block, 0, st>>>(a);
   return cudaGetLastError();
 }

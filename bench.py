@@ -806,7 +806,12 @@ def run_config3(args) -> dict:
 
     torch.cuda.set_device(0)
     hbm, peak_kind = peaks()
-    blocks = scenarios.config3_blocks(steps=args.steps + args.warmup + 4)
+    kw = {}
+    if args.grid:  # profiling cases: coarse nx, ny and the fine block's nz
+        kw = dict(nxc=args.grid[0], nyc=args.grid[1], nz_fine=args.grid[2],
+                  nz_coarse=max(12, args.grid[2] // 3 // 4 * 4),
+                  src_depth_m=40.0 * args.grid[2] * 0.6)
+    blocks = scenarios.config3_blocks(steps=args.steps + args.warmup + 4, **kw)
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
     m = Mesh([default_params(**b.params) for b in blocks], stream=stream.cuda_stream)
@@ -826,6 +831,7 @@ def run_config3(args) -> dict:
                                width=5000.0, rough_rms=100.0, seed=4)
     m.grid(0).topography(topo)
     cells = sum(b.params["nx"] * b.params["ny"] * b.params["nz"] for b in blocks)
+    block_params = [b.params for b in blocks]
     del blocks
 
     def timed(nsteps):
@@ -864,8 +870,10 @@ def run_config3(args) -> dict:
         "value": value, "unit": "Gcell-updates/s", "n_gpus": 1, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
-        "config": {"workload": "config3", "blocks": ["639x639x320 h=40 (curvilinear)",
-                                                     "213x213x96 h=120"],
+        "config": {"workload": "config3",
+                   "blocks": [f"{q['nx']}x{q['ny']}x{q['nz']} h={q['dh']:g}" +
+                              (" (curvilinear)" if n == 0 else "")
+                              for n, q in enumerate(block_params)],
                    "cells": cells, "dt": p0["dt"], "nve": 3,
                    "topography": "Gaussian hill 1 km / 5 km width + 100 m rms roughness (seed 4)",
                    "plasticity": "cohesion 1 MPa, friction 30 deg, lithostatic sigma2",

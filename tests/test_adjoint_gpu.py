@@ -277,7 +277,10 @@ def test_q_gradient_matches_oracle_and_finite_differences(shape, qrange):
     assert J == J0 and np.array_equal(gl, gl0) and np.array_equal(gr, gr0)
     assert np.abs(gqp).max() > 0 and np.abs(gqs).max() > 0
     rng = np.random.default_rng(52)
-    eps = 1e-3
+    # the misfit is far more curved in Q^-1 than in the moduli (the Q(f)
+    # weights are quadratic in Q^-1 on the low-Q branch): central differences
+    # take eps = 1e-4 here to keep their truncation error below the bar
+    eps = 1e-4
     for d in range(2):
         dq = tuple((x * rng.standard_normal(x.shape)).astype(np.float64) for x in qinv)
         adj = float(np.sum(gqp * dq[0]) + np.sum(gqs * dq[1]))
