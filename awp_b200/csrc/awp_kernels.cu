@@ -467,24 +467,25 @@ __global__ void k_addkinsrc(const KinSrcArgs a) {
 // ===========================================================================
 // Plasticity (drprecpc_calc_opt / drprecpc_app / rotate_principal)
 // ===========================================================================
-__device__ __forceinline__ void matmul3(const float* a, const float* b, float* c) {
-  for (int i = 0; i < 3; i++)
-    for (int j = 0; j < 3; j++)
-      for (int k = 0; k < 3; k++) c[i * 3 + j] += a[i * 3 + k] * b[k * 3 + j];
-}
-
-__device__ __forceinline__ void rotate_principal(const PlastParams& pp, float sigma2,
-                                                 float pfluid, float* ssp) {
-  float ss[9], tmp[9];
-  for (int k = 0; k < 9; k++) ss[k] = tmp[k] = ssp[k] = 0.f;
-  ss[0] = (sigma2 + pfluid) * pp.fmajor;
-  ss[4] = sigma2 + pfluid;
-  ss[8] = (sigma2 + pfluid) * pp.fminor;
-  matmul3(pp.RzT, ss, tmp);
-  matmul3(tmp, pp.Rz, ssp);
-  ssp[0] -= pfluid;
-  ssp[4] -= pfluid;
-  ssp[8] -= pfluid;
+// One component (I, J) of rotate_principal (the initial stress in the model
+// frame): ssp = Rz^T diag(s fmajor, s, s fminor) Rz - pfluid I with
+// s = sigma2 + pfluid, both products summed over k = 0, 1, 2 in order as the
+// reference's matmul.  In the first product the two off-diagonal terms of
+// each sum multiply an exact zero and add +-0, so its entry (I, k) is the one
+// rounded product RzT[I][k] * diag[k]; forming only that product and only the
+// components a kernel uses gives the same bits as the full 3 x 3 products.
+template <int I, int J>
+__device__ __forceinline__ float principal(const PlastParams& pp, float sigma2, float pfluid) {
+  const float s = sigma2 + pfluid;
+  const float d0 = s * pp.fmajor, d2 = s * pp.fminor;
+  const float t0 = pp.RzT[I * 3 + 0] * d0, t1 = pp.RzT[I * 3 + 1] * s,
+              t2 = pp.RzT[I * 3 + 2] * d2;
+  float c = 0.f;
+  c += t0 * pp.Rz[0 * 3 + J];
+  c += t1 * pp.Rz[1 * 3 + J];
+  c += t2 * pp.Rz[2 * 3 + J];
+  if (I == J) c -= pfluid;
+  return c;
 }
 
 __device__ __forceinline__ float pfluid_at(const PlastParams& pp, int k) {
@@ -502,21 +503,19 @@ __global__ void k_plast_calc(const PlastCalcArgs a) {
   const long long pos = (long long)i * S + (long long)j * Y + k;
   const long long pos_ip1 = pos + S, pos_jm1 = pos - Y, pos_km1 = pos - 1;
   const float pfluid = pfluid_at(pp, k);
-  float ini[9], ini_ip1[9];
-  rotate_principal(pp, a.sigma2[pos], pfluid, ini);
-  rotate_principal(pp, a.sigma2[pos_ip1], pfluid, ini_ip1);
-  const float iixx = 0.5f * (ini[0] + ini_ip1[0]);
-  const float iiyy = 0.5f * (ini[4] + ini_ip1[4]);
-  const float iizz = 0.5f * (ini[8] + ini_ip1[8]);
+  const float s2 = a.sigma2[pos], s2_ip1 = a.sigma2[pos_ip1];
+  const float iixx = 0.5f * (principal<0, 0>(pp, s2, pfluid) + principal<0, 0>(pp, s2_ip1, pfluid));
+  const float iiyy = 0.5f * (principal<1, 1>(pp, s2, pfluid) + principal<1, 1>(pp, s2_ip1, pfluid));
+  const float iizz = 0.5f * (principal<2, 2>(pp, s2, pfluid) + principal<2, 2>(pp, s2_ip1, pfluid));
   float Sxx = a.xx[pos] + iixx;
   float Syy = a.yy[pos] + iiyy;
   float Szz = a.zz[pos] + iizz;
   float Sxz = 0.25f * (a.xz[pos] + a.xz[pos_ip1] + a.xz[pos_km1] + a.xz[pos_ip1 - 1]) +
-              0.5f * (ini[2] + ini_ip1[2]);
+              0.5f * (principal<0, 2>(pp, s2, pfluid) + principal<0, 2>(pp, s2_ip1, pfluid));
   float Syz = 0.25f * (a.yz[pos] + a.yz[pos_jm1] + a.yz[pos_km1] + a.yz[pos_jm1 - 1]) +
-              0.5f * (ini[5] + ini_ip1[5]);
+              0.5f * (principal<1, 2>(pp, s2, pfluid) + principal<1, 2>(pp, s2_ip1, pfluid));
   float Sxy = 0.25f * (a.xy[pos] + a.xy[pos_ip1] + a.xy[pos_jm1] + a.xy[pos_ip1 - Y]) +
-              0.5f * (ini[1] + ini_ip1[1]);
+              0.5f * (principal<0, 1>(pp, s2, pfluid) + principal<0, 1>(pp, s2_ip1, pfluid));
   const float mu_i = a.mu[pos], mu_ip1 = a.mu[pos_ip1];
   const float Tv = pp.dh / sqrt(1.0f / (mu_i * a.d1[pos]));
   const float Sxxp = Sxx, Syyp = Syy, Szzp = Szz, Sxyp = Sxy, Sxzp = Sxz, Syzp = Syz;
@@ -575,15 +574,16 @@ __global__ void k_plast_app(const PlastAppArgs a) {
   const float pfluid = (depth > 0) ? (depth + pp.dh / 2.) * 9.81e3 : pp.dh / 2. * 9.81e3;
   const float pfluid_kp1 =
       (depth_kp1 > 0) ? (depth_kp1 + pp.dh / 2.) * 9.81e3 : pp.dh / 2. * 9.81e3;
-  float ini[9], ini_ip1[9], ini_kp1[9], ini_ip1kp1[9];
-  float ini_jp1[9], ini_ip1jp1[9], ini_jp1kp1[9], ini_ip1jp1kp1[9];
   const float yf = a.yldfac[pos];
   if (yf < 1.) {
-    rotate_principal(pp, a.sigma2[pos], pfluid, ini);
-    rotate_principal(pp, a.sigma2[pos_ip1], pfluid_kp1, ini_ip1);
-    const float iixx = 0.5 * (ini[0] + ini_ip1[0]);
-    const float iiyy = 0.5 * (ini[4] + ini_ip1[4]);
-    const float iizz = 0.5 * (ini[8] + ini_ip1[8]);
+    const float s2 = a.sigma2[pos];
+    const float s2_ip1 = a.sigma2[pos_ip1];
+    const float iixx =
+        0.5 * (principal<0, 0>(pp, s2, pfluid) + principal<0, 0>(pp, s2_ip1, pfluid_kp1));
+    const float iiyy =
+        0.5 * (principal<1, 1>(pp, s2, pfluid) + principal<1, 1>(pp, s2_ip1, pfluid_kp1));
+    const float iizz =
+        0.5 * (principal<2, 2>(pp, s2, pfluid) + principal<2, 2>(pp, s2_ip1, pfluid_kp1));
     const float Sxx = a.xx[pos] + iixx, Syy = a.yy[pos] + iiyy, Szz = a.zz[pos] + iizz;
     const float sigma_m = (Sxx + Syy + Szz) / 3.;
     const float SDxx = a.xx[pos] + iixx - sigma_m;
@@ -595,31 +595,26 @@ __global__ void k_plast_app(const PlastAppArgs a) {
   }
   float iyldfac = 0.25 * (a.yldfac[pos_im1] + yf + a.yldfac[pos_im1kp1] + a.yldfac[pos_kp1]);
   if (iyldfac < 1.) {
-    rotate_principal(pp, a.sigma2[pos], pfluid, ini);
-    rotate_principal(pp, a.sigma2[pos_kp1], pfluid_kp1, ini_kp1);
-    const float iist = 0.5 * (ini[2] + ini_kp1[2]);
+    const float iist = 0.5 * (principal<0, 2>(pp, a.sigma2[pos], pfluid) +
+                              principal<0, 2>(pp, a.sigma2[pos_kp1], pfluid_kp1));
     a.xz[pos] = (a.xz[pos] + iist) * iyldfac - iist;
   }
   iyldfac = 0.25 * (yf + a.yldfac[pos_jp1] + a.yldfac[pos_jp1kp1] + a.yldfac[pos_kp1]);
   if (iyldfac < 1.) {
-    rotate_principal(pp, a.sigma2[pos], pfluid, ini);
-    rotate_principal(pp, a.sigma2[pos_ip1], pfluid, ini_ip1);
-    rotate_principal(pp, a.sigma2[pos_kp1], pfluid_kp1, ini_kp1);
-    rotate_principal(pp, a.sigma2[pos_ip1kp1], pfluid_kp1, ini_ip1kp1);
-    rotate_principal(pp, a.sigma2[pos_jp1], pfluid, ini_jp1);
-    rotate_principal(pp, a.sigma2[pos_ip1jp1], pfluid, ini_ip1jp1);
-    rotate_principal(pp, a.sigma2[pos_jp1kp1], pfluid_kp1, ini_jp1kp1);
-    rotate_principal(pp, a.sigma2[pos_ip1jp1kp1], pfluid_kp1, ini_ip1jp1kp1);
-    const float iist = 0.125 * (ini[5] + ini_ip1[5] + ini_kp1[5] + ini_ip1kp1[5] +
-                                ini_jp1[5] + ini_ip1jp1[5] + ini_jp1kp1[5] +
-                                ini_ip1jp1kp1[5]);
+    const float iist = 0.125 * (principal<1, 2>(pp, a.sigma2[pos], pfluid) +
+                                principal<1, 2>(pp, a.sigma2[pos_ip1], pfluid) +
+                                principal<1, 2>(pp, a.sigma2[pos_kp1], pfluid_kp1) +
+                                principal<1, 2>(pp, a.sigma2[pos_ip1kp1], pfluid_kp1) +
+                                principal<1, 2>(pp, a.sigma2[pos_jp1], pfluid) +
+                                principal<1, 2>(pp, a.sigma2[pos_ip1jp1], pfluid) +
+                                principal<1, 2>(pp, a.sigma2[pos_jp1kp1], pfluid_kp1) +
+                                principal<1, 2>(pp, a.sigma2[pos_ip1jp1kp1], pfluid_kp1));
     a.yz[pos] = (a.yz[pos] + iist) * iyldfac - iist;
   }
   iyldfac = 0.25 * (yf + a.yldfac[pos_jp1] + a.yldfac[pos_im1] + a.yldfac[pos_im1jp1]);
   if (iyldfac < 1.) {
-    rotate_principal(pp, a.sigma2[pos], pfluid, ini);
-    rotate_principal(pp, a.sigma2[pos_jp1], pfluid, ini_jp1);
-    const float iist = 0.5 * (ini[1] + ini_jp1[1]);
+    const float iist = 0.5 * (principal<0, 1>(pp, a.sigma2[pos], pfluid) +
+                              principal<0, 1>(pp, a.sigma2[pos_jp1], pfluid));
     a.xy[pos] = (a.xy[pos] + iist) * iyldfac - iist;
   }
 }
