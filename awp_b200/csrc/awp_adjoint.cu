@@ -54,7 +54,9 @@ enum { VA, VB, VC, VEA, VEB, VEC };
 // in E[].  Seven 128-thread CTAs per SM (72 registers, some spilled) run it
 // faster than four without spills: the kernel waits on HBM latency.
 // ---------------------------------------------------------------------------
-template <bool ELASTIC>
+// WANTQ: also accumulate the Q^-1 weights (anelastic runs that ask for the
+// Q^-1 gradients); without it the five Q sums are neither read nor written.
+template <bool ELASTIC, bool WANTQ>
 __global__ void __launch_bounds__(128, 7) k_adj_stress_cell(const AdjArgs a) {
   // the relaxation tables in shared memory: the lanes of a warp alternate the
   // table entry with the parity of k, which a constant-bank read would serve
@@ -171,7 +173,7 @@ __global__ void __launch_bounds__(128, 7) k_adj_stress_cell(const AdjArgs a) {
   // are linear and time-invariant, so k_adj_material applies them once)
   float wacc[5], qacc[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
   for (int q = 0; q < 5; ++q) wacc[q] = a.E[GL8 + q][p];
-  if (!ELASTIC)
+  if (!ELASTIC && WANTQ)
     for (int q = 0; q < 5; ++q) qacc[q] = a.E[GQP8 + q][p];
   // normal components
   float PX, PY, PZ, QX = 0.f, QY = 0.f, QZ = 0.f;
@@ -232,7 +234,7 @@ __global__ void __launch_bounds__(128, 7) k_adj_stress_cell(const AdjArgs a) {
   E[GP1][p] = wacc[2] + GP[0];
   E[GP2][p] = wacc[3] + GP[1];
   E[GP3][p] = wacc[4] + GP[2];
-  if (!ELASTIC) {
+  if (!ELASTIC && WANTQ) {
     // Qp^-1 eight-cell sum: qpa = xl_raw c_q, c_q = -qpaw dh1 vx1
     E[GQP8][p] = qacc[0] + G_qpa * xl_raw * (-a.dh1 * fvx1) * dqpaw * 0.0625f;
     // Qs^-1 eight-cell sum: h = xm_raw c_h, xm = xm_raw (dth + DT c_h)
@@ -682,10 +684,13 @@ cudaError_t awp_launch_adjoint_step(const AdjArgs& a, cudaStream_t st) {
   const int si = a.si1 - a.si0 + 1, sj = a.sj1 - a.sj0 + 1, sk = a.sk1 - a.sk0 + 1;
   const dim3 blk(32, 4);
   // the imaging (fstr) transpose runs inside k_adj_stress_cell
+  const dim3 sgrid(cdiv(sk, 32), cdiv(sj, 4), si);
   if (a.elastic)
-    k_adj_stress_cell<true><<<dim3(cdiv(sk, 32), cdiv(sj, 4), si), blk, 0, st>>>(a);
+    k_adj_stress_cell<true, false><<<sgrid, blk, 0, st>>>(a);
+  else if (a.want_q)
+    k_adj_stress_cell<false, true><<<sgrid, blk, 0, st>>>(a);
   else
-    k_adj_stress_cell<false><<<dim3(cdiv(sk, 32), cdiv(sj, 4), si), blk, 0, st>>>(a);
+    k_adj_stress_cell<false, false><<<sgrid, blk, 0, st>>>(a);
   k_adj_stress_gather<<<dim3(cdiv(sk + 4, 32), cdiv(sj + 4, 4), cdiv(si + 4, kGch)), blk, 0,
                         st>>>(a);
   k_adj_images<<<dim3(cdiv(sj + 2, 128), si + 2), 128, 0, st>>>(a);

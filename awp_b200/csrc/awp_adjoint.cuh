@@ -45,6 +45,7 @@ struct AdjArgs {
   float coeff[16];
   float dth, dh1, dt, c1, c2, qthr;
   int elastic;
+  int want_q;  // accumulate the Q^-1 weights (the caller asked for g_qpinv / g_qsinv)
   AwpGeom g;
   int vi0, vi1, vj0, vj1, vk0, vk1;  // velocity update range (inclusive, padded)
   int si0, si1, sj0, sj1, sk0, sk1;  // stress update range

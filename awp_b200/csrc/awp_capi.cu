@@ -2196,6 +2196,7 @@ int awp_misfit_gradient_q(awp_ctx* c, int nsteps, int nrec, const int* rec_xyz,
   memcpy(a.coeff, c->coeff, sizeof(a.coeff));
   a.dth = c->dth; a.dh1 = c->dh1; a.dt = c->p.dt; a.c1 = c->c1; a.c2 = c->c2; a.qthr = c->qthr;
   a.elastic = c->elastic ? 1 : 0;
+  a.want_q = (!c->elastic && (g_qpinv || g_qsinv)) ? 1 : 0;
   a.g = c->g;
   a.vb = vb;
   a.vi0 = va.i0; a.vi1 = va.i1; a.vj0 = va.j0; a.vj1 = va.j1; a.vk0 = va.k0; a.vk1 = va.k1;
