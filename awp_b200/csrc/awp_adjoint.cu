@@ -48,22 +48,47 @@ __device__ __forceinline__ float qf_dweight(float q, float wwo, float c0, float 
 }
 enum { VA, VB, VC, VEA, VEB, VEC };
 
+// Per-thread asynchronous 4-byte copy global -> shared (cp.async); a thread
+// reads back only its own slots, after cp.async.wait_all.
+__device__ __forceinline__ void cpa4(float* s, const float* g) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(
+                   (unsigned)__cvta_generic_to_shared(s)),
+               "l"(g)
+               : "memory");
+}
+__device__ __forceinline__ void cpa_wait() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+#ifndef AWP_ADJ_STAGE
+#define AWP_ADJ_STAGE 1  // stage the stress transpose's once-read values
+#endif
+#ifndef AWP_ADJ_MINB
+#define AWP_ADJ_MINB 7  // CTAs per SM the stress transpose's registers allow
+#endif
+
 // ---------------------------------------------------------------------------
 // stress^T, pointwise part: memory variables and stresses in place, adjoint
 // strain rates of the cell into E[], its material weights added to the sums
-// in E[].  Seven 128-thread CTAs per SM (72 registers, some spilled) run it
-// faster than four without spills: the kernel waits on HBM latency.
+// in E[].  Seven 128-thread CTAs per SM (72 registers) run it faster than
+// four without spills: the kernel waits on HBM latency.  The values it reads
+// once and late (the cell's adjoint stresses, memory variables and weight
+// sums) are copied to shared memory by cp.async when a thread starts, which
+// takes them out of the registers (840 against 860 ms for a 600-step
+// gradient at 256 x 256 x 128).
 // ---------------------------------------------------------------------------
 // WANTQ: also accumulate the Q^-1 weights (anelastic runs that ask for the
 // Q^-1 gradients); without it the five Q sums are neither read nor written.
 template <bool ELASTIC, bool WANTQ>
-__global__ void __launch_bounds__(128, 7) k_adj_stress_cell(const AdjArgs a) {
+__global__ void __launch_bounds__(128, AWP_ADJ_MINB) k_adj_stress_cell(const AdjArgs a) {
+  // the cell's own adjoint stresses and memory variables and its weight sums,
+  // read once and late: copied to shared memory when the thread starts
+  // (slots 0-5 stresses, 6-11 memory variables, 12-16 moduli sums, 17-21 Q sums)
+  __shared__ float stg[AWP_ADJ_STAGE ? 22 : 1][128];
+  const int tid = threadIdx.y * 32 + threadIdx.x;
   // the relaxation tables in shared memory: the lanes of a warp alternate the
   // table entry with the parity of k, which a constant-bank read would serve
   // in two passes
   __shared__ float tab[40];  // tau1[8], tau2[8], wwo8[8], coeff[16]
   {
-    const int tid = threadIdx.y * 32 + threadIdx.x;
     if (tid < 8) {
       tab[tid] = a.tex.tau1[tid];
       tab[8 + tid] = a.tex.tau2[tid];
@@ -80,6 +105,22 @@ __global__ void __launch_bounds__(128, 7) k_adj_stress_cell(const AdjArgs a) {
   const int S = a.g.slice, Y = a.g.yline;
   const long long p = (long long)i * S + (long long)j * Y + k;
   const float c1 = a.c1, c2 = a.c2, DT = a.dt;
+  if (AWP_ADJ_STAGE) {
+#pragma unroll
+    for (int q = 0; q < 6; ++q) cpa4(&stg[q][tid], a.L[LXX + q] + p);
+    if (!ELASTIC) {
+#pragma unroll
+      for (int q = 0; q < 6; ++q) cpa4(&stg[6 + q][tid], a.L[LR1 + q] + p);
+    }
+#pragma unroll
+    for (int q = 0; q < 5; ++q) cpa4(&stg[12 + q][tid], a.E[GL8 + q] + p);
+    if (!ELASTIC && WANTQ) {
+#pragma unroll
+      for (int q = 0; q < 5; ++q) cpa4(&stg[17 + q][tid], a.E[GQP8 + q] + p);
+    }
+  }
+  // the cell's value of a staged array
+  auto own = [&](int slot, const float* f) { return AWP_ADJ_STAGE ? stg[slot][tid] : f[p]; };
 
   // forward strain rates from the velocities after the step (VelBox layout)
   const int VS = (int)a.vb.S, VY = (int)a.vb.Y;
@@ -149,7 +190,7 @@ __global__ void __launch_bounds__(128, 7) k_adj_stress_cell(const AdjArgs a) {
   const int top = a.g.top();
   auto fs = [&](int f) -> float {  // adjoint of the field after the stress update
     const float* Lf = a.L[f];
-    float v = Lf[p];
+    float v = own(f - LXX, Lf);
     if (k == top) {
       if (f == LZZ) v -= Lf[p + 1];
       if (f == LXZ || f == LYZ) v = 0.f;
@@ -164,17 +205,18 @@ __global__ void __launch_bounds__(128, 7) k_adj_stress_cell(const AdjArgs a) {
   // every load of the adjoint state before the first store: the stores below
   // go to other arrays (or other cells of the same array), and issuing the
   // loads together keeps them from waiting on one another
-  const float lx = a.L[LXX][p], ly = a.L[LYY][p], lz = fs(LZZ);
+  if (AWP_ADJ_STAGE) cpa_wait();
+  const float lx = own(0, a.L[LXX]), ly = own(1, a.L[LYY]), lz = fs(LZZ);
   const float ls[3] = {fs(LXY), fs(LXZ), fs(LYZ)};
   float rv[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
   if (!ELASTIC)
-    for (int q = 0; q < 6; ++q) rv[q] = a.L[LR1 + q][p];
+    for (int q = 0; q < 6; ++q) rv[q] = own(6 + q, a.L[LR1 + q]);
   // material weights, summed over the time steps (their spatial transposes
   // are linear and time-invariant, so k_adj_material applies them once)
   float wacc[5], qacc[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
-  for (int q = 0; q < 5; ++q) wacc[q] = a.E[GL8 + q][p];
+  for (int q = 0; q < 5; ++q) wacc[q] = own(12 + q, a.E[GL8 + q]);
   if (!ELASTIC && WANTQ)
-    for (int q = 0; q < 5; ++q) qacc[q] = a.E[GQP8 + q][p];
+    for (int q = 0; q < 5; ++q) qacc[q] = own(17 + q, a.E[GQP8 + q]);
   // normal components
   float PX, PY, PZ, QX = 0.f, QY = 0.f, QZ = 0.f;
   PX = K * lx;

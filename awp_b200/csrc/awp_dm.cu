@@ -207,15 +207,18 @@ __global__ void k_intp3d(const DmPairArgs a) {
         H[ph + (long long)(ii - 1 + oi) * hi.slice + (long long)(jj - 1 + oj) * hi.yline] = s;
       }
   };
-  patch(lo.xz, hi.xz, 0, 0);
-  patch(lo.yz, hi.yz, 1, 1);
-  patch(lo.w1, hi.w1, 1, 0);
-  patch(lo.xx, hi.xx, 1, 0);
-  patch(lo.yy, hi.yy, 1, 0);
-  patch(lo.zz, hi.zz, 1, 0);
-  patch(lo.u1, hi.u1, 0, 0);
-  patch(lo.v1, hi.v1, 1, 1);
-  patch(lo.xy, hi.xy, 0, 1);
+  // one field per blockIdx.z (the nine patches of a column are independent)
+  switch (blockIdx.z) {
+    case 0: patch(lo.xz, hi.xz, 0, 0); break;
+    case 1: patch(lo.yz, hi.yz, 1, 1); break;
+    case 2: patch(lo.w1, hi.w1, 1, 0); break;
+    case 3: patch(lo.xx, hi.xx, 1, 0); break;
+    case 4: patch(lo.yy, hi.yy, 1, 0); break;
+    case 5: patch(lo.zz, hi.zz, 1, 0); break;
+    case 6: patch(lo.u1, hi.u1, 0, 0); break;
+    case 7: patch(lo.v1, hi.v1, 1, 1); break;
+    default: patch(lo.xy, hi.xy, 0, 1); break;
+  }
 }
 
 // ===========================================================================
@@ -237,6 +240,10 @@ __device__ __forceinline__ float window(const DmGrid& hi, const float* H, int ih
   return sum;
 }
 
+// One thread per (coarse column, window): the fifteen window sums of a column
+// are independent, and each keeps its 125 terms in the reference's order, so
+// spreading them over blockIdx.z shortens every thread's dependent chain
+// fifteen-fold without changing a bit.
 __global__ void k_swap3(const DmPairArgs a, double inv_total) {
   const int j = AWP_NGSL + blockIdx.x * blockDim.x + threadIdx.x;
   const int i = AWP_NGSL + blockIdx.y * blockDim.y + threadIdx.y;
@@ -244,26 +251,30 @@ __global__ void k_swap3(const DmPairArgs a, double inv_total) {
   const DmGrid &lo = a.lo, &hi = a.hi;
   const int i2 = (i - 2 - AWP_NGSL) * 3 + 2 + AWP_NGSL, i3 = i2 + 1;
   const int j2 = (j - 2 - AWP_NGSL) * 3 + 2 + AWP_NGSL, j3 = j2 + 1;
-  long long pl = at(lo, i, j, AWP_ALIGN + lo.nzt - 2);
-  int kh = AWP_ALIGN + 3;
-  lo.u1[pl] = window(hi, hi.u1, i2, j2, kh, inv_total);
-  lo.v1[pl] = window(hi, hi.v1, i3, j3, kh, inv_total);
-  lo.xy[pl] = window(hi, hi.xy, i2, j3, kh, inv_total);
-  lo.xx[pl] = window(hi, hi.xx, i3, j2, kh, inv_total);
-  lo.yy[pl] = window(hi, hi.yy, i3, j2, kh, inv_total);
-  lo.zz[pl] = window(hi, hi.zz, i3, j2, kh, inv_total);
-  kh = AWP_ALIGN + 4;
-  lo.xz[pl] = window(hi, hi.xz, i2, j2, kh, inv_total);
-  lo.w1[pl] = window(hi, hi.w1, i3, j2, kh, inv_total);
-  lo.yz[pl] = window(hi, hi.yz, i3, j3, kh, inv_total);
-  pl = at(lo, i, j, AWP_ALIGN + lo.nzt - 1);
-  kh = AWP_ALIGN + 6;
-  lo.u1[pl] = window(hi, hi.u1, i2, j2, kh, inv_total);
-  lo.v1[pl] = window(hi, hi.v1, i3, j3, kh, inv_total);
-  lo.xy[pl] = window(hi, hi.xy, i2, j3, kh, inv_total);
-  lo.xx[pl] = window(hi, hi.xx, i3, j2, kh, inv_total);
-  lo.yy[pl] = window(hi, hi.yy, i3, j2, kh, inv_total);
-  lo.zz[pl] = window(hi, hi.zz, i3, j2, kh, inv_total);
+  // window w: destination field and level (0: nzt-2, 1: nzt-1), fine-grid
+  // source point (i2 or i3, j2 or j3) and level kh
+  float* dst;
+  const float* src;
+  int si, sj, kh, lev;
+  switch (blockIdx.z) {
+    case 0: dst = lo.u1; src = hi.u1; si = i2; sj = j2; kh = 3; lev = 0; break;
+    case 1: dst = lo.v1; src = hi.v1; si = i3; sj = j3; kh = 3; lev = 0; break;
+    case 2: dst = lo.xy; src = hi.xy; si = i2; sj = j3; kh = 3; lev = 0; break;
+    case 3: dst = lo.xx; src = hi.xx; si = i3; sj = j2; kh = 3; lev = 0; break;
+    case 4: dst = lo.yy; src = hi.yy; si = i3; sj = j2; kh = 3; lev = 0; break;
+    case 5: dst = lo.zz; src = hi.zz; si = i3; sj = j2; kh = 3; lev = 0; break;
+    case 6: dst = lo.xz; src = hi.xz; si = i2; sj = j2; kh = 4; lev = 0; break;
+    case 7: dst = lo.w1; src = hi.w1; si = i3; sj = j2; kh = 4; lev = 0; break;
+    case 8: dst = lo.yz; src = hi.yz; si = i3; sj = j3; kh = 4; lev = 0; break;
+    case 9: dst = lo.u1; src = hi.u1; si = i2; sj = j2; kh = 6; lev = 1; break;
+    case 10: dst = lo.v1; src = hi.v1; si = i3; sj = j3; kh = 6; lev = 1; break;
+    case 11: dst = lo.xy; src = hi.xy; si = i2; sj = j3; kh = 6; lev = 1; break;
+    case 12: dst = lo.xx; src = hi.xx; si = i3; sj = j2; kh = 6; lev = 1; break;
+    case 13: dst = lo.yy; src = hi.yy; si = i3; sj = j2; kh = 6; lev = 1; break;
+    default: dst = lo.zz; src = hi.zz; si = i3; sj = j2; kh = 6; lev = 1; break;
+  }
+  dst[at(lo, i, j, AWP_ALIGN + lo.nzt - 2 + lev)] =
+      window(hi, src, si, sj, AWP_ALIGN + kh, inv_total);
 }
 
 // ===========================================================================
@@ -302,7 +313,7 @@ cudaError_t awp_launch_dstrqc2(const DmStr2Args& a, cudaStream_t st) {
 
 cudaError_t awp_launch_intp3d(const DmPairArgs& a, cudaStream_t st) {
   const dim3 block(32, 4);
-  k_intp3d<<<dim3(cdiv(a.lo.nyt + 4, 32), cdiv(a.lo.nxt + 4, 4)), block, 0, st>>>(a);
+  k_intp3d<<<dim3(cdiv(a.lo.nyt + 4, 32), cdiv(a.lo.nxt + 4, 4), 9), block, 0, st>>>(a);
   return cudaGetLastError();
 }
 
@@ -313,7 +324,8 @@ cudaError_t awp_launch_swap3(const DmPairArgs& a, cudaStream_t st) {
       for (int kk = -AWP_WWL; kk <= AWP_WWL; kk++)
         total += (1. + AWP_WWL - abs(jj)) * (1. + AWP_WWL - abs(ii)) * (1. + AWP_WWL - abs(kk));
   const dim3 block(32, 4);
-  k_swap3<<<dim3(cdiv(a.lo.nyt + 5, 32), cdiv(a.lo.nxt + 5, 4)), block, 0, st>>>(a, 1. / total);
+  k_swap3<<<dim3(cdiv(a.lo.nyt + 5, 32), cdiv(a.lo.nxt + 5, 4), 15), block, 0, st>>>(a,
+                                                                                 1. / total);
   return cudaGetLastError();
 }
 

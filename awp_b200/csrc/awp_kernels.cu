@@ -574,48 +574,57 @@ __global__ void k_plast_app(const PlastAppArgs a) {
   const float pfluid = (depth > 0) ? (depth + pp.dh / 2.) * 9.81e3 : pp.dh / 2. * 9.81e3;
   const float pfluid_kp1 =
       (depth_kp1 > 0) ? (depth_kp1 + pp.dh / 2.) * 9.81e3 : pp.dh / 2. * 9.81e3;
-  const float yf = a.yldfac[pos];
+  // every input first (the yield factors, the cell's stresses and the eight
+  // sigma2 of its stencil), so the loads overlap instead of following the
+  // branches one after another; the branches then read registers
+  const float yf = a.yldfac[pos], y_im1 = a.yldfac[pos_im1], y_kp1 = a.yldfac[pos_kp1],
+              y_jp1 = a.yldfac[pos_jp1], y_im1kp1 = a.yldfac[pos_im1kp1],
+              y_jp1kp1 = a.yldfac[pos_jp1kp1], y_im1jp1 = a.yldfac[pos_im1jp1];
+  const float sxx = a.xx[pos], syy = a.yy[pos], szz = a.zz[pos], sxz = a.xz[pos],
+              syz = a.yz[pos], sxy = a.xy[pos];
+  const float s2 = a.sigma2[pos], s2_ip1 = a.sigma2[pos_ip1], s2_kp1 = a.sigma2[pos_kp1],
+              s2_jp1 = a.sigma2[pos_jp1], s2_ip1kp1 = a.sigma2[pos_ip1kp1],
+              s2_ip1jp1 = a.sigma2[pos_ip1jp1], s2_jp1kp1 = a.sigma2[pos_jp1kp1],
+              s2_ip1jp1kp1 = a.sigma2[pos_ip1jp1kp1];
   if (yf < 1.) {
-    const float s2 = a.sigma2[pos];
-    const float s2_ip1 = a.sigma2[pos_ip1];
     const float iixx =
         0.5 * (principal<0, 0>(pp, s2, pfluid) + principal<0, 0>(pp, s2_ip1, pfluid_kp1));
     const float iiyy =
         0.5 * (principal<1, 1>(pp, s2, pfluid) + principal<1, 1>(pp, s2_ip1, pfluid_kp1));
     const float iizz =
         0.5 * (principal<2, 2>(pp, s2, pfluid) + principal<2, 2>(pp, s2_ip1, pfluid_kp1));
-    const float Sxx = a.xx[pos] + iixx, Syy = a.yy[pos] + iiyy, Szz = a.zz[pos] + iizz;
+    const float Sxx = sxx + iixx, Syy = syy + iiyy, Szz = szz + iizz;
     const float sigma_m = (Sxx + Syy + Szz) / 3.;
-    const float SDxx = a.xx[pos] + iixx - sigma_m;
-    const float SDyy = a.yy[pos] + iiyy - sigma_m;
-    const float SDzz = a.zz[pos] + iizz - sigma_m;
+    const float SDxx = sxx + iixx - sigma_m;
+    const float SDyy = syy + iiyy - sigma_m;
+    const float SDzz = szz + iizz - sigma_m;
     a.xx[pos] = SDxx * yf + sigma_m - iixx;
     a.yy[pos] = SDyy * yf + sigma_m - iiyy;
     a.zz[pos] = SDzz * yf + sigma_m - iizz;
   }
-  float iyldfac = 0.25 * (a.yldfac[pos_im1] + yf + a.yldfac[pos_im1kp1] + a.yldfac[pos_kp1]);
+  float iyldfac = 0.25 * (y_im1 + yf + y_im1kp1 + y_kp1);
   if (iyldfac < 1.) {
-    const float iist = 0.5 * (principal<0, 2>(pp, a.sigma2[pos], pfluid) +
-                              principal<0, 2>(pp, a.sigma2[pos_kp1], pfluid_kp1));
-    a.xz[pos] = (a.xz[pos] + iist) * iyldfac - iist;
+    const float iist =
+        0.5 * (principal<0, 2>(pp, s2, pfluid) + principal<0, 2>(pp, s2_kp1, pfluid_kp1));
+    a.xz[pos] = (sxz + iist) * iyldfac - iist;
   }
-  iyldfac = 0.25 * (yf + a.yldfac[pos_jp1] + a.yldfac[pos_jp1kp1] + a.yldfac[pos_kp1]);
+  iyldfac = 0.25 * (yf + y_jp1 + y_jp1kp1 + y_kp1);
   if (iyldfac < 1.) {
-    const float iist = 0.125 * (principal<1, 2>(pp, a.sigma2[pos], pfluid) +
-                                principal<1, 2>(pp, a.sigma2[pos_ip1], pfluid) +
-                                principal<1, 2>(pp, a.sigma2[pos_kp1], pfluid_kp1) +
-                                principal<1, 2>(pp, a.sigma2[pos_ip1kp1], pfluid_kp1) +
-                                principal<1, 2>(pp, a.sigma2[pos_jp1], pfluid) +
-                                principal<1, 2>(pp, a.sigma2[pos_ip1jp1], pfluid) +
-                                principal<1, 2>(pp, a.sigma2[pos_jp1kp1], pfluid_kp1) +
-                                principal<1, 2>(pp, a.sigma2[pos_ip1jp1kp1], pfluid_kp1));
-    a.yz[pos] = (a.yz[pos] + iist) * iyldfac - iist;
+    const float iist = 0.125 * (principal<1, 2>(pp, s2, pfluid) +
+                                principal<1, 2>(pp, s2_ip1, pfluid) +
+                                principal<1, 2>(pp, s2_kp1, pfluid_kp1) +
+                                principal<1, 2>(pp, s2_ip1kp1, pfluid_kp1) +
+                                principal<1, 2>(pp, s2_jp1, pfluid) +
+                                principal<1, 2>(pp, s2_ip1jp1, pfluid) +
+                                principal<1, 2>(pp, s2_jp1kp1, pfluid_kp1) +
+                                principal<1, 2>(pp, s2_ip1jp1kp1, pfluid_kp1));
+    a.yz[pos] = (syz + iist) * iyldfac - iist;
   }
-  iyldfac = 0.25 * (yf + a.yldfac[pos_jp1] + a.yldfac[pos_im1] + a.yldfac[pos_im1jp1]);
+  iyldfac = 0.25 * (yf + y_jp1 + y_im1 + y_im1jp1);
   if (iyldfac < 1.) {
-    const float iist = 0.5 * (principal<0, 1>(pp, a.sigma2[pos], pfluid) +
-                              principal<0, 1>(pp, a.sigma2[pos_jp1], pfluid));
-    a.xy[pos] = (a.xy[pos] + iist) * iyldfac - iist;
+    const float iist =
+        0.5 * (principal<0, 1>(pp, s2, pfluid) + principal<0, 1>(pp, s2_jp1, pfluid));
+    a.xy[pos] = (sxy + iist) * iyldfac - iist;
   }
 }
 
