@@ -227,54 +227,72 @@ __global__ void k_intp3d(const DmPairArgs a) {
 // products in double, each partial sum rounded to float like the reference's
 // float accumulator.
 // ===========================================================================
-__device__ __forceinline__ float window(const DmGrid& hi, const float* H, int ihc, int jhc,
-                                        int kh, double inv_total) {
-  float sum = 0.0f;
-  for (int jj = -AWP_WWL; jj <= AWP_WWL; ++jj)
-    for (int ii = -AWP_WWL; ii <= AWP_WWL; ++ii)
-      for (int kk = -AWP_WWL; kk <= AWP_WWL; ++kk) {
-        const double c = inv_total * (1. + AWP_WWL - abs(ii)) * (1. + AWP_WWL - abs(jj)) *
-                         (1. + AWP_WWL - abs(kk));
-        sum = (float)__fma_rn(c, (double)H[at(hi, ihc + ii, jhc + jj, kh + kk)], (double)sum);
-      }
-  return sum;
-}
+// A CTA takes 2 (i) x 32 (j) coarse columns and goes through the nine fields
+// one after another: it copies the fine-grid box the field's windows read
+// (9 x 99 x 8 points: fine i2-2 .. i3+2 and j2-2 .. j3+2 of its columns,
+// levels align+1 .. align+8) into shared memory with k-contiguous,
+// sector-wide loads, then each of its threads forms one window of one column
+// (a field has one or two: levels nzt-2 and nzt-1), its 125 terms in the
+// reference's order from shared memory.  Read straight from global memory the
+// windows' stride-3 j columns cost a sector per 4-byte load; the box copy
+// reads each sector once.
+constexpr int kSwTI = 2, kSwTJ = 32;
+constexpr int kSwBI = 3 * (kSwTI - 1) + 6, kSwBJ = 3 * (kSwTJ - 1) + 6, kSwBK = 8;
+constexpr int kSwKS = 9;  // padded k stride: lanes 3 j apart fall in distinct banks
 
-// One thread per (coarse column, window): the fifteen window sums of a column
-// are independent, and each keeps its 125 terms in the reference's order, so
-// spreading them over blockIdx.z shortens every thread's dependent chain
-// fifteen-fold without changing a bit.
-__global__ void k_swap3(const DmPairArgs a, double inv_total) {
-  const int j = AWP_NGSL + blockIdx.x * blockDim.x + threadIdx.x;
-  const int i = AWP_NGSL + blockIdx.y * blockDim.y + threadIdx.y;
-  if (i >= a.lo.nxt + AWP_NGSL + 5 || j >= a.lo.nyt + AWP_NGSL + 5) return;
+__global__ void __launch_bounds__(128) k_swap3(const DmPairArgs a, double inv_total) {
+  __shared__ float box[kSwBI * kSwBJ * kSwKS];
   const DmGrid &lo = a.lo, &hi = a.hi;
-  const int i2 = (i - 2 - AWP_NGSL) * 3 + 2 + AWP_NGSL, i3 = i2 + 1;
-  const int j2 = (j - 2 - AWP_NGSL) * 3 + 2 + AWP_NGSL, j3 = j2 + 1;
-  // window w: destination field and level (0: nzt-2, 1: nzt-1), fine-grid
-  // source point (i2 or i3, j2 or j3) and level kh
-  float* dst;
-  const float* src;
-  int si, sj, kh, lev;
-  switch (blockIdx.z) {
-    case 0: dst = lo.u1; src = hi.u1; si = i2; sj = j2; kh = 3; lev = 0; break;
-    case 1: dst = lo.v1; src = hi.v1; si = i3; sj = j3; kh = 3; lev = 0; break;
-    case 2: dst = lo.xy; src = hi.xy; si = i2; sj = j3; kh = 3; lev = 0; break;
-    case 3: dst = lo.xx; src = hi.xx; si = i3; sj = j2; kh = 3; lev = 0; break;
-    case 4: dst = lo.yy; src = hi.yy; si = i3; sj = j2; kh = 3; lev = 0; break;
-    case 5: dst = lo.zz; src = hi.zz; si = i3; sj = j2; kh = 3; lev = 0; break;
-    case 6: dst = lo.xz; src = hi.xz; si = i2; sj = j2; kh = 4; lev = 0; break;
-    case 7: dst = lo.w1; src = hi.w1; si = i3; sj = j2; kh = 4; lev = 0; break;
-    case 8: dst = lo.yz; src = hi.yz; si = i3; sj = j3; kh = 4; lev = 0; break;
-    case 9: dst = lo.u1; src = hi.u1; si = i2; sj = j2; kh = 6; lev = 1; break;
-    case 10: dst = lo.v1; src = hi.v1; si = i3; sj = j3; kh = 6; lev = 1; break;
-    case 11: dst = lo.xy; src = hi.xy; si = i2; sj = j3; kh = 6; lev = 1; break;
-    case 12: dst = lo.xx; src = hi.xx; si = i3; sj = j2; kh = 6; lev = 1; break;
-    case 13: dst = lo.yy; src = hi.yy; si = i3; sj = j2; kh = 6; lev = 1; break;
-    default: dst = lo.zz; src = hi.zz; si = i3; sj = j2; kh = 6; lev = 1; break;
+  const int tid = threadIdx.y * 32 + threadIdx.x;
+  const int i0 = AWP_NGSL + blockIdx.y * kSwTI, j0 = AWP_NGSL + blockIdx.x * kSwTJ;
+  const int imax = lo.nxt + AWP_NGSL + 4, jmax = lo.nyt + AWP_NGSL + 4;
+  // fine box origin (i2 - 2, j2 - 2 of the first column) and the extent the
+  // valid columns read
+  const int fi0 = (i0 - 2 - AWP_NGSL) * 3 + AWP_NGSL, fj0 = (j0 - 2 - AWP_NGSL) * 3 + AWP_NGSL;
+  const int nbi = 3 * (min(i0 + kSwTI - 1, imax) - i0) + 6;
+  const int nbj = 3 * (min(j0 + kSwTJ - 1, jmax) - j0) + 6;
+  // this thread's column and window slot (level 0 or 1)
+  const int c = tid & 63, lev = tid >> 6;
+  const int ci = c >> 5, cj = c & 31;
+  const int i = i0 + ci, j = j0 + cj;
+  const bool valid = i <= imax && j <= jmax;
+#pragma unroll 1
+  for (int f = 0; f < 9; ++f) {
+    float* dst;
+    const float* src;
+    int kh0, nwin, di, dj;  // level-0 window at kh0 (level 1 at 6); source i3 / j3 if di / dj
+    switch (f) {
+      case 0: dst = lo.u1; src = hi.u1; kh0 = 3; nwin = 2; di = 0; dj = 0; break;
+      case 1: dst = lo.v1; src = hi.v1; kh0 = 3; nwin = 2; di = 1; dj = 1; break;
+      case 2: dst = lo.xy; src = hi.xy; kh0 = 3; nwin = 2; di = 0; dj = 1; break;
+      case 3: dst = lo.xx; src = hi.xx; kh0 = 3; nwin = 2; di = 1; dj = 0; break;
+      case 4: dst = lo.yy; src = hi.yy; kh0 = 3; nwin = 2; di = 1; dj = 0; break;
+      case 5: dst = lo.zz; src = hi.zz; kh0 = 3; nwin = 2; di = 1; dj = 0; break;
+      case 6: dst = lo.xz; src = hi.xz; kh0 = 4; nwin = 1; di = 0; dj = 0; break;
+      case 7: dst = lo.w1; src = hi.w1; kh0 = 4; nwin = 1; di = 1; dj = 0; break;
+      default: dst = lo.yz; src = hi.yz; kh0 = 4; nwin = 1; di = 1; dj = 1; break;
+    }
+    __syncthreads();  // the previous field's windows are done with the box
+    for (int t = tid; t < nbi * nbj * kSwBK; t += 128) {
+      const int bk = t % kSwBK, r = t / kSwBK, bj = r % nbj, bi = r / nbj;
+      box[(bi * kSwBJ + bj) * kSwKS + bk] = src[at(hi, fi0 + bi, fj0 + bj, AWP_ALIGN + 1 + bk)];
+    }
+    __syncthreads();
+    if (valid && lev < nwin) {
+      const int kh = lev ? 6 : kh0;
+      const int bi = 3 * ci + di + 2, bj = 3 * cj + dj + 2, bk = kh - 1;
+      float sum = 0.0f;
+      for (int jj = -AWP_WWL; jj <= AWP_WWL; ++jj)
+        for (int ii = -AWP_WWL; ii <= AWP_WWL; ++ii)
+          for (int kk = -AWP_WWL; kk <= AWP_WWL; ++kk) {
+            const double w = inv_total * (1. + AWP_WWL - abs(ii)) * (1. + AWP_WWL - abs(jj)) *
+                             (1. + AWP_WWL - abs(kk));
+            const float h = box[((bi + ii) * kSwBJ + bj + jj) * kSwKS + bk + kk];
+            sum = (float)__fma_rn(w, (double)h, (double)sum);
+          }
+      dst[at(lo, i, j, AWP_ALIGN + lo.nzt - 2 + lev)] = sum;
+    }
   }
-  dst[at(lo, i, j, AWP_ALIGN + lo.nzt - 2 + lev)] =
-      window(hi, src, si, sj, AWP_ALIGN + kh, inv_total);
 }
 
 // ===========================================================================
@@ -323,9 +341,8 @@ cudaError_t awp_launch_swap3(const DmPairArgs& a, cudaStream_t st) {
     for (int ii = -AWP_WWL; ii <= AWP_WWL; ii++)
       for (int kk = -AWP_WWL; kk <= AWP_WWL; kk++)
         total += (1. + AWP_WWL - abs(jj)) * (1. + AWP_WWL - abs(ii)) * (1. + AWP_WWL - abs(kk));
-  const dim3 block(32, 4);
-  k_swap3<<<dim3(cdiv(a.lo.nyt + 5, 32), cdiv(a.lo.nxt + 5, 4), 15), block, 0, st>>>(a,
-                                                                                 1. / total);
+  k_swap3<<<dim3(cdiv(a.lo.nyt + 5, kSwTJ), cdiv(a.lo.nxt + 5, kSwTI)), dim3(32, 4), 0, st>>>(
+      a, 1. / total);
   return cudaGetLastError();
 }
 

@@ -576,7 +576,12 @@ __global__ void k_plast_app(const PlastAppArgs a) {
       (depth_kp1 > 0) ? (depth_kp1 + pp.dh / 2.) * 9.81e3 : pp.dh / 2. * 9.81e3;
   // every input first (the yield factors, the cell's stresses and the eight
   // sigma2 of its stencil), so the loads overlap instead of following the
-  // branches one after another; the branches then read registers
+  // branches one after another; the branches then read registers.  The
+  // reference's double-precision scalings here (0.5, 0.25, 0.125 and the
+  // division by 3 of a float sum, rounded back to float) are formed in float:
+  // the scalings are exact, and for float operands the double quotient
+  // rounded to float is the correctly rounded float quotient (double rounding
+  // is innocuous for division at 53 >= 2 * 24 + 2 bits; Figueroa 1995).
   const float yf = a.yldfac[pos], y_im1 = a.yldfac[pos_im1], y_kp1 = a.yldfac[pos_kp1],
               y_jp1 = a.yldfac[pos_jp1], y_im1kp1 = a.yldfac[pos_im1kp1],
               y_jp1kp1 = a.yldfac[pos_jp1kp1], y_im1jp1 = a.yldfac[pos_im1jp1];
@@ -586,15 +591,15 @@ __global__ void k_plast_app(const PlastAppArgs a) {
               s2_jp1 = a.sigma2[pos_jp1], s2_ip1kp1 = a.sigma2[pos_ip1kp1],
               s2_ip1jp1 = a.sigma2[pos_ip1jp1], s2_jp1kp1 = a.sigma2[pos_jp1kp1],
               s2_ip1jp1kp1 = a.sigma2[pos_ip1jp1kp1];
-  if (yf < 1.) {
+  if (yf < 1.f) {
     const float iixx =
-        0.5 * (principal<0, 0>(pp, s2, pfluid) + principal<0, 0>(pp, s2_ip1, pfluid_kp1));
+        0.5f * (principal<0, 0>(pp, s2, pfluid) + principal<0, 0>(pp, s2_ip1, pfluid_kp1));
     const float iiyy =
-        0.5 * (principal<1, 1>(pp, s2, pfluid) + principal<1, 1>(pp, s2_ip1, pfluid_kp1));
+        0.5f * (principal<1, 1>(pp, s2, pfluid) + principal<1, 1>(pp, s2_ip1, pfluid_kp1));
     const float iizz =
-        0.5 * (principal<2, 2>(pp, s2, pfluid) + principal<2, 2>(pp, s2_ip1, pfluid_kp1));
+        0.5f * (principal<2, 2>(pp, s2, pfluid) + principal<2, 2>(pp, s2_ip1, pfluid_kp1));
     const float Sxx = sxx + iixx, Syy = syy + iiyy, Szz = szz + iizz;
-    const float sigma_m = (Sxx + Syy + Szz) / 3.;
+    const float sigma_m = __fdiv_rn(Sxx + Syy + Szz, 3.0f);
     const float SDxx = sxx + iixx - sigma_m;
     const float SDyy = syy + iiyy - sigma_m;
     const float SDzz = szz + iizz - sigma_m;
@@ -602,15 +607,15 @@ __global__ void k_plast_app(const PlastAppArgs a) {
     a.yy[pos] = SDyy * yf + sigma_m - iiyy;
     a.zz[pos] = SDzz * yf + sigma_m - iizz;
   }
-  float iyldfac = 0.25 * (y_im1 + yf + y_im1kp1 + y_kp1);
-  if (iyldfac < 1.) {
+  float iyldfac = 0.25f * (y_im1 + yf + y_im1kp1 + y_kp1);
+  if (iyldfac < 1.f) {
     const float iist =
-        0.5 * (principal<0, 2>(pp, s2, pfluid) + principal<0, 2>(pp, s2_kp1, pfluid_kp1));
+        0.5f * (principal<0, 2>(pp, s2, pfluid) + principal<0, 2>(pp, s2_kp1, pfluid_kp1));
     a.xz[pos] = (sxz + iist) * iyldfac - iist;
   }
-  iyldfac = 0.25 * (yf + y_jp1 + y_jp1kp1 + y_kp1);
-  if (iyldfac < 1.) {
-    const float iist = 0.125 * (principal<1, 2>(pp, s2, pfluid) +
+  iyldfac = 0.25f * (yf + y_jp1 + y_jp1kp1 + y_kp1);
+  if (iyldfac < 1.f) {
+    const float iist = 0.125f * (principal<1, 2>(pp, s2, pfluid) +
                                 principal<1, 2>(pp, s2_ip1, pfluid) +
                                 principal<1, 2>(pp, s2_kp1, pfluid_kp1) +
                                 principal<1, 2>(pp, s2_ip1kp1, pfluid_kp1) +
@@ -620,10 +625,10 @@ __global__ void k_plast_app(const PlastAppArgs a) {
                                 principal<1, 2>(pp, s2_ip1jp1kp1, pfluid_kp1));
     a.yz[pos] = (syz + iist) * iyldfac - iist;
   }
-  iyldfac = 0.25 * (yf + y_jp1 + y_im1 + y_im1jp1);
-  if (iyldfac < 1.) {
+  iyldfac = 0.25f * (yf + y_jp1 + y_im1 + y_im1jp1);
+  if (iyldfac < 1.f) {
     const float iist =
-        0.5 * (principal<0, 1>(pp, s2, pfluid) + principal<0, 1>(pp, s2_jp1, pfluid));
+        0.5f * (principal<0, 1>(pp, s2, pfluid) + principal<0, 1>(pp, s2_jp1, pfluid));
     a.xy[pos] = (sxy + iist) * iyldfac - iist;
   }
 }
