@@ -227,8 +227,8 @@ __global__ void k_intp3d(const DmPairArgs a) {
 // products in double, each partial sum rounded to float like the reference's
 // float accumulator.
 // ===========================================================================
-// A CTA takes 2 (i) x 32 (j) coarse columns and goes through the nine fields
-// one after another: it copies the fine-grid box the field's windows read
+// A CTA takes 2 (i) x 32 (j) coarse columns of one field (blockIdx.z): it
+// copies the fine-grid box the field's windows read
 // (9 x 99 x 8 points: fine i2-2 .. i3+2 and j2-2 .. j3+2 of its columns,
 // levels align+1 .. align+8) into shared memory with k-contiguous,
 // sector-wide loads, then each of its threads forms one window of one column
@@ -240,7 +240,14 @@ constexpr int kSwTI = 2, kSwTJ = 32;
 constexpr int kSwBI = 3 * (kSwTI - 1) + 6, kSwBJ = 3 * (kSwTJ - 1) + 6, kSwBK = 8;
 constexpr int kSwKS = 9;  // padded k stride: lanes 3 j apart fall in distinct banks
 
-__global__ void __launch_bounds__(128) k_swap3(const DmPairArgs a, double inv_total) {
+// The 125 tent weights of a window in the sum's order (jj, ii, kk), formed on
+// the host as the reference forms them on the device, in double:
+// (1 / total) * (3 - |ii|) * (3 - |jj|) * (3 - |kk|) left to right.
+struct SwapWeights {
+  double w[125];
+};
+
+__global__ void __launch_bounds__(128) k_swap3(const DmPairArgs a, const SwapWeights sw) {
   __shared__ float box[kSwBI * kSwBJ * kSwKS];
   const DmGrid &lo = a.lo, &hi = a.hi;
   const int tid = threadIdx.y * 32 + threadIdx.x;
@@ -256,8 +263,8 @@ __global__ void __launch_bounds__(128) k_swap3(const DmPairArgs a, double inv_to
   const int ci = c >> 5, cj = c & 31;
   const int i = i0 + ci, j = j0 + cj;
   const bool valid = i <= imax && j <= jmax;
-#pragma unroll 1
-  for (int f = 0; f < 9; ++f) {
+  {
+    const int f = blockIdx.z;  // one field per CTA
     float* dst;
     const float* src;
     int kh0, nwin, di, dj;  // level-0 window at kh0 (level 1 at 6); source i3 / j3 if di / dj
@@ -272,7 +279,6 @@ __global__ void __launch_bounds__(128) k_swap3(const DmPairArgs a, double inv_to
       case 7: dst = lo.w1; src = hi.w1; kh0 = 4; nwin = 1; di = 1; dj = 0; break;
       default: dst = lo.yz; src = hi.yz; kh0 = 4; nwin = 1; di = 1; dj = 1; break;
     }
-    __syncthreads();  // the previous field's windows are done with the box
     for (int t = tid; t < nbi * nbj * kSwBK; t += 128) {
       const int bk = t % kSwBK, r = t / kSwBK, bj = r % nbj, bi = r / nbj;
       box[(bi * kSwBJ + bj) * kSwKS + bk] = src[at(hi, fi0 + bi, fj0 + bj, AWP_ALIGN + 1 + bk)];
@@ -282,13 +288,13 @@ __global__ void __launch_bounds__(128) k_swap3(const DmPairArgs a, double inv_to
       const int kh = lev ? 6 : kh0;
       const int bi = 3 * ci + di + 2, bj = 3 * cj + dj + 2, bk = kh - 1;
       float sum = 0.0f;
+      int q = 0;
       for (int jj = -AWP_WWL; jj <= AWP_WWL; ++jj)
         for (int ii = -AWP_WWL; ii <= AWP_WWL; ++ii)
-          for (int kk = -AWP_WWL; kk <= AWP_WWL; ++kk) {
-            const double w = inv_total * (1. + AWP_WWL - abs(ii)) * (1. + AWP_WWL - abs(jj)) *
-                             (1. + AWP_WWL - abs(kk));
+#pragma unroll
+          for (int kk = -AWP_WWL; kk <= AWP_WWL; ++kk, ++q) {
             const float h = box[((bi + ii) * kSwBJ + bj + jj) * kSwKS + bk + kk];
-            sum = (float)__fma_rn(w, (double)h, (double)sum);
+            sum = (float)__fma_rn(sw.w[q], (double)h, (double)sum);
           }
       dst[at(lo, i, j, AWP_ALIGN + lo.nzt - 2 + lev)] = sum;
     }
@@ -341,8 +347,16 @@ cudaError_t awp_launch_swap3(const DmPairArgs& a, cudaStream_t st) {
     for (int ii = -AWP_WWL; ii <= AWP_WWL; ii++)
       for (int kk = -AWP_WWL; kk <= AWP_WWL; kk++)
         total += (1. + AWP_WWL - abs(jj)) * (1. + AWP_WWL - abs(ii)) * (1. + AWP_WWL - abs(kk));
-  k_swap3<<<dim3(cdiv(a.lo.nyt + 5, kSwTJ), cdiv(a.lo.nxt + 5, kSwTI)), dim3(32, 4), 0, st>>>(
-      a, 1. / total);
+  const double inv_total = 1. / total;
+  SwapWeights sw;
+  int q = 0;
+  for (int jj = -AWP_WWL; jj <= AWP_WWL; jj++)
+    for (int ii = -AWP_WWL; ii <= AWP_WWL; ii++)
+      for (int kk = -AWP_WWL; kk <= AWP_WWL; kk++)
+        sw.w[q++] = inv_total * (1. + AWP_WWL - abs(ii)) * (1. + AWP_WWL - abs(jj)) *
+                    (1. + AWP_WWL - abs(kk));
+  k_swap3<<<dim3(cdiv(a.lo.nyt + 5, kSwTJ), cdiv(a.lo.nxt + 5, kSwTI), 9), dim3(32, 4), 0, st>>>(
+      a, sw);
   return cudaGetLastError();
 }
 
