@@ -623,9 +623,9 @@ def run_adjoint(args) -> dict:
     adjoint.misfit_gradient(s, steps, xyz, comp, d_obs)
     sampler = ClockSampler(torch.cuda.current_device())
     sampler.start()
-    # three forward runs and three gradients, alternating; the medians are
-    # reported with every run listed (single runs vary with the power-capped
-    # clocks, a gradient by up to ~20 % on some boxes)
+    # --adj-reps (default five) forward runs and gradients, alternating; the
+    # medians are reported with every run listed (single runs vary with the
+    # power-capped clocks, a gradient by up to ~20 % on some boxes)
     fwd_runs, adj_runs = [], []
     for _ in range(args.adj_reps):
         s.reset()
@@ -933,7 +933,7 @@ def main():
                     help="shots of the multi-shot gradient (--workload shots)")
     ap.add_argument("--adj-steps", type=int, default=1500,
                     help="time steps of the misfit-gradient run (--workload adjoint)")
-    ap.add_argument("--adj-reps", type=int, default=3,
+    ap.add_argument("--adj-reps", type=int, default=5,
                     help="timed forward runs and gradients, alternating (--workload adjoint)")
     ap.add_argument("--fd-dirs", type=int, default=8,
                     help="finite-difference directions (--workload adjoint)")
