@@ -95,6 +95,7 @@ def load() -> ctypes.CDLL:
     _sig(lib, "awp_upload_media", c_int, [_P, c_int, _F])
     _sig(lib, "awp_upload_media_device", c_int, [_P, c_int, c_void_p])
     _sig(lib, "awp_upload_sources", c_int, [_P, c_int, _I, _F])
+    _sig(lib, "awp_upload_plane_wave", c_int, [_P, c_int, c_void_p, c_void_p, c_void_p])
     _sig(lib, "awp_set_source_filter", c_int, [_P, c_int, _D, _D])
     _sig(lib, "awp_download_moment", c_int, [_P, _F])
     _sig(lib, "awp_upload_plasticity", c_int, [_P, _F, _F, _F, c_float, c_float, _F, _F])

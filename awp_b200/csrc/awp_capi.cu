@@ -77,6 +77,8 @@ struct awp_ctx {
   float* d_src[6] = {};
   float* d_mom = nullptr;
   double* d_filt = nullptr;
+  float* d_plane[3] = {};  // IFAULT 6 plane-wave series (x, y, z), plane_n samples each
+  int plane_n = 0;
   int filtorder = 0;
   double filt_b[AWP_MAXFILT] = {}, filt_a[AWP_MAXFILT] = {};
   // plasticity
@@ -450,6 +452,25 @@ int phase_sources(awp_ctx* c) {
     if (st) return st;
     if (c->ncell) c->launches++;
   }
+  // IFAULT 6: addplanesrc_H(cur_step, ...) while cur_step < NST, on the grid
+  // that holds the plane wave (the bottom one, pmcl3d.c:2035-2041); the loop
+  // counter starts at 1, so sample 0 of the series is never applied
+  if (c->p.ifault == 6 && c->plane_n > 0 && c->cur_step < c->plane_n) {
+    PhaseScope ps(c, 2);
+    PlaneSrcArgs a;
+    a.n = (int)c->cur_step;
+    a.nx = c->p.nx + 4 + (c->p.nx % 2);  // rows of the shipped 2 x 2 launch blocks
+    a.ny = c->p.ny + 4 + (c->p.ny % 2);
+    a.k = AWP_ALIGN + c->p.nd + 1;
+    a.mu = c->f[AWP_MU]; a.lambda = c->f[AWP_LAM];
+    a.axx = c->d_plane[0]; a.ayy = c->d_plane[1]; a.azz = c->d_plane[2];
+    a.xx = c->f[AWP_XX]; a.yy = c->f[AWP_YY]; a.zz = c->f[AWP_ZZ];
+    a.xz = c->f[AWP_XZ]; a.yz = c->f[AWP_YZ];
+    a.slice = c->g.slice; a.yline = c->g.yline;
+    a.DT = c->p.dt; a.DH = c->p.dh;
+    CU_TRY(awp_launch_planesrc(a, c->stream));
+    c->launches++;
+  }
   return AWP_OK;
 }
 
@@ -687,6 +708,7 @@ int awp_ctx_destroy(awp_ctx* c) {
   cudaFree(c->d_cell_pos); cudaFree(c->d_cell_first); cudaFree(c->d_order);
   for (int i = 0; i < 6; ++i) cudaFree(c->d_src[i]);
   cudaFree(c->d_mom); cudaFree(c->d_filt); cudaFree(c->d_neta_mult); cudaFree(c->d_flag);
+  for (int q = 0; q < 3; ++q) cudaFree(c->d_plane[q]);
   cudaFree(c->d_ext);
   cudaFree(c->d_err);
   for (auto& e : c->ev_used) { cudaEventDestroy(e.a); cudaEventDestroy(e.b); }
@@ -712,7 +734,7 @@ int awp_ctx_create(const awp_params* p, awp_ctx** out) {
                      "NVE=%d: the time loop runs only for NVE 1 or 3 (pmcl3d.c:1624)", p->nve);
   if (p->npc != 0 && p->npc != 2)
     return set_error(AWP_ERR_UNSUPPORTED, "NPC=%d (only 0 and 2 run the loop)", p->npc);
-  if (p->ifault != 1 && p->ifault != 5 && p->ifault != 0)
+  if (p->ifault != 1 && p->ifault != 5 && p->ifault != 0 && p->ifault != 6)
     return set_error(AWP_ERR_UNSUPPORTED, "IFAULT=%d", p->ifault);
   const long long cells = (long long)(p->nx + 20) * (p->ny + 20) * (p->nz + 64);
   if (cells >= (1LL << 31))
@@ -911,6 +933,29 @@ int awp_upload_media(awp_ctx* c, int nvar, const float* host_media) {
 }
 int awp_upload_media_device(awp_ctx* c, int nvar, const float* dev_media) {
   return upload_media_impl(c, nvar, dev_media, true);
+}
+
+int awp_upload_plane_wave(awp_ctx* c, int nst, const float* vx, const float* vy,
+                          const float* vz) {
+  if (!c) return set_error(AWP_ERR_ARG, "null context");
+  if (c->p.ifault != 6) return set_error(AWP_ERR_STATE, "the context runs IFAULT=%d, not 6", c->p.ifault);
+  if (nst < 1 || !vx || !vy || !vz) return set_error(AWP_ERR_ARG, "bad plane-wave series");
+  if (nst != c->p.nst)
+    return set_error(AWP_ERR_ARG, "the series holds %d samples, NST is %d (ini_plane_wave)", nst,
+                     c->p.nst);
+  const float* in[3] = {vx, vy, vz};
+  for (int q = 0; q < 3; ++q) {
+    cudaFree(c->d_plane[q]);
+    c->d_plane[q] = nullptr;
+  }
+  c->plane_n = 0;
+  int st;
+  for (int q = 0; q < 3; ++q) {
+    if ((st = ctx_alloc(c, (void**)&c->d_plane[q], (size_t)nst * 4))) return st;
+    CU_TRY(cudaMemcpy(c->d_plane[q], in[q], (size_t)nst * 4, cudaMemcpyDefault));
+  }
+  c->plane_n = nst;
+  return AWP_OK;
 }
 
 int awp_upload_sources(awp_ctx* c, int nsrc, const int* pos, const float* data) {
@@ -1586,10 +1631,11 @@ int awp_batch_create(awp_ctx* const* ctxs, int n, awp_batch** out) {
     awp_ctx* c = ctxs[q];
     if (!c) return set_error(AWP_ERR_ARG, "instance %d is null", q);
     if (!c->media_ready) return set_error(AWP_ERR_STATE, "instance %d: media not uploaded", q);
-    if (c->p.ngrids != 1 || c->p.nve == 3 || c->topo || c->recv || c->srcf)
+    if (c->p.ngrids != 1 || c->p.nve == 3 || c->topo || c->recv || c->srcf ||
+        c->p.ifault == 6)
       return set_error(AWP_ERR_UNSUPPORTED,
                        "instance %d: a batch holds single-grid Cartesian runs without "
-                       "plasticity, receivers or SOURCEFILE sources", q);
+                       "plasticity, receivers, SOURCEFILE or plane-wave sources", q);
     if (c->cur_step != ctxs[0]->cur_step)
       return set_error(AWP_ERR_STATE, "instances must start at the same step");
     for (int r = 0; r < q; ++r)

@@ -188,34 +188,6 @@ __global__ void k_frcvel(const FrcvelArgs a) {
   }
 }
 
-// addplanesrc_cu (kernel.cu:3897-3925): a plane-wave source (IFAULT 6) on the
-// level k = align + ND + 1 of every (i, j) from 4 to nxt+7 (nyt+7), the
-// launched rows rounded up to the shipped 2 x 2 blocks.  The reference forms
-// the increments in double.
-struct PlaneSrcArgs {
-  int n, nx, ny, k;
-  const float *mu, *lambda, *axx, *ayy, *azz;
-  float *xx, *yy, *zz, *xz, *yz;
-  int slice, yline;
-  float DT, DH;
-};
-
-__global__ void k_addplanesrc(const PlaneSrcArgs a) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  if (i >= a.nx || j >= a.ny) return;
-  const long long pos = (long long)(i + 4) * a.slice + (long long)(j + 4) * a.yline + a.k;
-  const float vtst = a.DT / a.DH;  // float quotient, as the reference forms it
-  const double v2 = __dmul_rn((double)vtst, 2.0);
-  const double mu = a.mu[pos], la = a.lambda[pos];
-  a.xz[pos] = (float)__fma_rn(-__ddiv_rn(v2, mu), (double)a.axx[a.n], (double)a.xz[pos]);
-  a.yz[pos] = (float)__fma_rn(-__ddiv_rn(v2, mu), (double)a.ayy[a.n], (double)a.yz[pos]);
-  a.xx[pos] = (float)__fma_rn(-__ddiv_rn(v2, la), (double)a.azz[a.n], (double)a.xx[pos]);
-  a.yy[pos] = (float)__fma_rn(-__ddiv_rn(v2, la), (double)a.azz[a.n], (double)a.yy[pos]);
-  a.zz[pos] = (float)__fma_rn(-__ddiv_rn(v2, __fma_rn(2.0, mu, la)), (double)a.azz[a.n],
-                              (double)a.zz[pos]);
-}
-
 // fvel (kernel.cu:1949-2033): free-surface velocity images at k = top + 1 of
 // grid 0 from the velocities at and below the surface.  Every (i, j) of the
 // launch reads only levels top and top - 1, so the reference's sequential
@@ -584,8 +556,7 @@ void addplanesrc_H(int i, int dim, int NST, awp_stream_t St, float* mu, float* l
   a.slice = gc.slice; a.yline = gc.yline;
   a.DT = s.DT;
   a.DH = gc.DH;
-  k_addplanesrc<<<dim3(cdiv(a.nx, 16), cdiv(a.ny, 16)), dim3(16, 16), 0, St>>>(a);
-  check(cudaGetLastError(), "addplanesrc_H");
+  check(awp_launch_planesrc(a, St), "addplanesrc_H");
 }
 
 void fvel_H(float* u1, float* v1, float* w1, awp_stream_t St, float* lam_mu, int NX, int rankx,

@@ -634,6 +634,29 @@ __global__ void k_plast_app(const PlastAppArgs a) {
 }
 
 // ===========================================================================
+// Plane-wave source (IFAULT 6)
+// ===========================================================================
+// addplanesrc_cu (kernel.cu:3897-3925): a plane-wave source (IFAULT 6) on the
+// level k = align + ND + 1 of every (i, j) from 4 to nxt+7 (nyt+7), the
+// launched rows rounded up to the shipped 2 x 2 blocks.  The reference forms
+// the increments in double.
+__global__ void k_addplanesrc(const PlaneSrcArgs a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i >= a.nx || j >= a.ny) return;
+  const long long pos = (long long)(i + 4) * a.slice + (long long)(j + 4) * a.yline + a.k;
+  const float vtst = a.DT / a.DH;  // float quotient, as the reference forms it
+  const double v2 = __dmul_rn((double)vtst, 2.0);
+  const double mu = a.mu[pos], la = a.lambda[pos];
+  a.xz[pos] = (float)__fma_rn(-__ddiv_rn(v2, mu), (double)a.axx[a.n], (double)a.xz[pos]);
+  a.yz[pos] = (float)__fma_rn(-__ddiv_rn(v2, mu), (double)a.ayy[a.n], (double)a.yz[pos]);
+  a.xx[pos] = (float)__fma_rn(-__ddiv_rn(v2, la), (double)a.azz[a.n], (double)a.xx[pos]);
+  a.yy[pos] = (float)__fma_rn(-__ddiv_rn(v2, la), (double)a.azz[a.n], (double)a.yy[pos]);
+  a.zz[pos] = (float)__fma_rn(-__ddiv_rn(v2, __fma_rn(2.0, mu, la)), (double)a.azz[a.n],
+                              (double)a.zz[pos]);
+}
+
+// ===========================================================================
 // Output gather (velbuffer, kernel.cu:3948-4011)
 // ===========================================================================
 __global__ void k_velbuffer(const VelBufArgs a) {
@@ -1044,6 +1067,12 @@ cudaError_t awp_launch_addsrc(const SrcArgs& a, cudaStream_t st) {
     k_addsrc<<<cdiv_u(a.ncell, 128), 128, 0, st>>>(a);
   else
     k_addsrc_direct<<<cdiv_u(a.ncell, 128), 128, 0, st>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t awp_launch_planesrc(const PlaneSrcArgs& a, cudaStream_t st) {
+  if (a.nx <= 0 || a.ny <= 0) return cudaSuccess;
+  k_addplanesrc<<<dim3(cdiv_u(a.nx, 16), cdiv_u(a.ny, 16)), dim3(16, 16), 0, st>>>(a);
   return cudaGetLastError();
 }
 

@@ -158,7 +158,19 @@ struct MediaArgs {
 int awp_tuning_set(const char* key, int value);
 int awp_tuning_get(const char* key);
 
+// addplanesrc_cu (kernel.cu:3897-3925): a plane-wave source (IFAULT 6) on the
+// level k = align + ND + 1 of the bottom grid, every (i, j) from 4 to
+// 3 + nx (ny), sample n of the three input series.
+struct PlaneSrcArgs {
+  int n, nx, ny, k;
+  const float *mu, *lambda, *axx, *ayy, *azz;
+  float *xx, *yy, *zz, *xz, *yz;
+  int slice, yline;
+  float DT, DH;
+};
+
 // Launchers (awp_kernels.cu).  All are asynchronous on `st`.
+cudaError_t awp_launch_planesrc(const PlaneSrcArgs& a, cudaStream_t st);
 cudaError_t awp_launch_velocity(const VelArgs& a, cudaStream_t st);
 cudaError_t awp_launch_stress(const StrArgs& a, bool elastic, cudaStream_t st);
 cudaError_t awp_launch_fstr(const FstrArgs& a, cudaStream_t st);

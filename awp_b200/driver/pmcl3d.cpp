@@ -9,7 +9,7 @@
 //
 // Scope: one rank (PX = PY = 1, no I/O ranks), one grid or a discontinuous
 // mesh of NGRIDS blocks (each 3x finer than the one below, pmcl3d.c:370-378),
-// MEDIASTART 0-2, IFAULT 1 and 5, NVE 1 and 3.  On a mesh the SOURCEFILE /
+// MEDIASTART 0-2, IFAULT 1, 5 and 6, NVE 1 and 3.  On a mesh the SOURCEFILE /
 // RECVFILE point sets and the topography belong to the top block (grid 0).
 // Anything else is reported and refused.
 #include <getopt.h>
@@ -307,9 +307,21 @@ int main(int argc, char** argv) {
     if (!grid_output[p]) rnx[p] = rny[p] = rnz[p] = 0;
   }
 
-  if (A.IFAULT != 1 && A.IFAULT != 5) {
+  if (A.IFAULT != 1 && A.IFAULT != 5 && A.IFAULT != 6) {
     fprintf(stderr, "pmcl3d: IFAULT=%d sources are not part of this build\n", A.IFAULT);
     return 1;
+  }
+  if (A.IFAULT == 6) {  // pmcl3d.c:751-761
+    printf("Using plane wave input at grid position %d in grid %d\n", A.NZ[G - 1] - A.ND - 1,
+           G - 1);
+    if (A.READ_STEP != A.NST) {
+      fprintf(stderr, "Error.  READ_STEP should be equal NST for IFAULT=6\n");
+      return 1;
+    }
+    if (A.NST < 1) {
+      fprintf(stderr, "Error.  NST=%d, but should be > 0 for IFAULT=6.\n", A.NST);
+      return 1;
+    }
   }
   if (A.IFAULT == 5 && (A.NST != 2 || A.READ_STEP != 2)) {  // pmcl3d.c:680-688
     fprintf(stderr, "IFAULT=5 requires NST = READ_STEP =2.\nQuitting.");
@@ -353,7 +365,7 @@ int main(int argc, char** argv) {
   std::vector<int> spos[MAXGRIDS];
   int nsrc[MAXGRIDS] = {0};
   for (int p = 0; p < G; ++p) {  // INSRC_<p> for every block with sources (pmcl3d.c:702-708)
-    if (A.NSRC[p] <= 0) continue;
+    if (A.NSRC[p] <= 0 || !(A.IFAULT < 3 || A.IFAULT == 5)) continue;
     char name[512];
     snprintf(name, sizeof(name), "%s_%d", A.INSRC.c_str(), p);
     FILE* f = fopen(name, "rb");
@@ -377,6 +389,26 @@ int main(int argc, char** argv) {
     if (nsrc[p]) AWP(awp_upload_sources(ctx[p], nsrc[p], spos[p].data(), sdat.data()));
   }
   if (A.IFAULT == 5) printf("Using IFAULT=5: kinematic source.\n");
+  if (A.IFAULT == 6) {  // ini_plane_wave (source.c:797-833): NST lines "vx vy vz"
+    std::vector<float> pv[3];
+    FILE* f = fopen(A.INSRC.c_str(), "r");
+    if (!f) {
+      perror(("Could not open " + A.INSRC).c_str());
+      return 1;
+    }
+    for (int i = 0; i < A.NST; ++i) {
+      float v[3];
+      if (fscanf(f, "%e %e %e\n", v, v + 1, v + 2) < 3) {
+        fprintf(stderr, "pmcl3d: %s holds fewer than NST=%d samples\n", A.INSRC.c_str(),
+                A.NST);
+        fclose(f);
+        return 1;
+      }
+      for (int q = 0; q < 3; ++q) pv[q].push_back(v[q]);
+    }
+    fclose(f);
+    AWP(awp_upload_plane_wave(ctx[G - 1], A.NST, pv[0].data(), pv[1].data(), pv[2].data()));
+  }
 
   // ---- media (inimesh, mesh.c:23-614), INVEL_<p> per block (pmcl3d.c:882-892) ---
   float vse[MAXGRIDS][2] = {}, vpe[MAXGRIDS][2] = {}, dde[MAXGRIDS][2] = {};

@@ -113,6 +113,16 @@ class Solver:
                                           pos.ctypes.data_as(ctypes.POINTER(c_int)),
                                           _fptr(data)), "awp_upload_sources")
 
+    def upload_plane_wave(self, vx, vy, vz) -> None:
+        """IFAULT=6 plane-wave input: three float series of NST samples (the
+        columns of the INSRC text file, ini_plane_wave)."""
+        xs = [np.ascontiguousarray(v, dtype=np.float32) for v in (vx, vy, vz)]
+        n = int(xs[0].size)
+        if any(x.size != n for x in xs):
+            raise ValueError("the three plane-wave series differ in length")
+        check(self.lib.awp_upload_plane_wave(self.ctx, n, *[c_void_p(x.ctypes.data) for x in xs]),
+              "awp_upload_plane_wave")
+
     def set_source_filter(self, b, a) -> None:
         b = np.ascontiguousarray(b, dtype=np.float64)
         a = np.ascontiguousarray(a, dtype=np.float64)

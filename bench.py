@@ -591,7 +591,7 @@ def run_adjoint(args) -> dict:
     from awp_b200 import Solver, adjoint, default_params, scenarios
 
     nx, ny, nz = args.grid if args.grid else (256, 256, 128)
-    steps = args.adj_steps
+    steps = args.adj_steps or 1500
     scn, m_true, m0, xyz, comp = scenarios.adjoint_case(nx=nx, ny=ny, nz=nz, steps=steps)
     stream = torch.cuda.Stream()
     s = Solver(default_params(**scn.params), stream=stream.cuda_stream)
@@ -713,7 +713,7 @@ def run_shots(args, rank, world, dist) -> dict | None:
 
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
     nx, ny, nz = args.grid if args.grid else (384, 384, 192)
-    steps = args.adj_steps
+    steps = args.adj_steps or 1000
     scn = scenarios.layered_vk(nx=nx, ny=ny, nz=nz, h=100.0, dt=0.005, steps=steps, nsub=1,
                                seed_medium=7, seed_src=8)
     rng = np.random.default_rng(9)
@@ -931,8 +931,9 @@ def main():
                              "shots"])
     ap.add_argument("--shots", type=int, default=32,
                     help="shots of the multi-shot gradient (--workload shots)")
-    ap.add_argument("--adj-steps", type=int, default=1500,
-                    help="time steps of the misfit-gradient run (--workload adjoint)")
+    ap.add_argument("--adj-steps", type=int, default=None,
+                    help="time steps of a misfit-gradient run: config 4's 1500 for "
+                         "--workload adjoint, config 5b's 1000 per shot for --workload shots")
     ap.add_argument("--adj-reps", type=int, default=5,
                     help="timed forward runs and gradients, alternating (--workload adjoint)")
     ap.add_argument("--fd-dirs", type=int, default=8,

@@ -121,6 +121,15 @@ int awp_free_host_pinned(void* ptr);
  * IFAULT=5 only samples 0 and 1 are used and hold the subfault parameters
  * (kernel.cu:3788-3809). */
 int awp_upload_sources(awp_ctx* ctx, int nsrc, const int* pos, const float* data);
+/* Plane-wave input (IFAULT=6; ini_plane_wave, source.c:797-833, and
+ * addplanesrc_H, pmcl3d.c:2035-2041): three series of NST samples (vx, vy, vz,
+ * the three columns of the INSRC text file), host or device pointers.  Every
+ * step with cur_step < NST subtracts 2 dt/h times sample cur_step, scaled by
+ * mu (xz, yz from vx, vy) and by lambda / lambda + 2 mu (xx, yy, zz from vz),
+ * from the stresses of level align + ND + 1 of the grid -- the bottom grid of
+ * a mesh.  Sample 0 is never applied (the loop counter starts at 1). */
+int awp_upload_plane_wave(awp_ctx* ctx, int nst, const float* vx, const float* vy,
+                          const float* vz);
 /* Optional IIR/FIR filter of the kinematic source time function
  * (sourcefilter.dat, pmcl3d.c:651-673): b[order+1], a[order+1]. */
 int awp_set_source_filter(awp_ctx* ctx, int order, const double* b, const double* a);

@@ -75,6 +75,8 @@ struct Base {
   virtual void set_filter(int order, const double* b, const double* a) = 0;
   virtual void get_moment(float* m) = 0;
   virtual void set_plasticity(float fmajor, float fminor, const float* Rz, const float* RzT) = 0;
+  virtual void set_plane_wave(int n, int nd, const float* vx, const float* vy,
+                              const float* vz) = 0;
   virtual void add_point_sources(int field, int nq, int nb, const int* ix, const int* iy,
                                  const int* iz, const float* lx, const float* ly, const float* lz,
                                  int nsamples, const float* values, int stride) = 0;
@@ -105,6 +107,9 @@ struct Oracle : Base {
   std::vector<double> filt_state;
   // plasticity
   T fmajor = 0, fminor = 0, Rz[9] = {}, RzT[9] = {};
+  // IFAULT 6 plane wave (ini_plane_wave) and the level it enters
+  std::vector<T> plane[3];
+  int plane_n = 0, plane_nd = 0;
   // SOURCEFILE moment tensors, one entry per stress component
   struct PointSrc {
     int field, nq, nb, nsamples, stride;
@@ -686,6 +691,33 @@ struct Oracle : Base {
     }
   }
 
+  void set_plane_wave(int n, int nd, const float* vx, const float* vy,
+                      const float* vz) override {
+    const float* in[3] = {vx, vy, vz};
+    for (int q = 0; q < 3; ++q) plane[q].assign(in[q], in[q] + n);
+    plane_n = n;
+    plane_nd = nd;
+  }
+
+  // addplanesrc_cu (kernel.cu:3897-3925): sample ti of the plane wave on level
+  // align + ND + 1, every (i, j) of the reference's launch (rows 4 .. 3 + nx
+  // rounded up to its 2 x 2 blocks); the kernel arrays hold 1/mu and 1/lambda
+  void addplanesrc(int ti) {
+    const int nx = nxt + 4 + (nxt % 2), ny = nyt + 4 + (nyt % 2);
+    const T vtst = DT / DH;
+    const int k = ALIGN + plane_nd + 1;
+    for (int i = 4; i < 4 + nx; ++i)
+      for (int j = 4; j < 4 + ny; ++j) {
+        const long long pos = idx(i, j, k);
+        const T mu = f[MU][pos], la = f[LAM][pos];
+        f[XZ][pos] = f[XZ][pos] - vtst * T(2) / mu * plane[0][ti];
+        f[YZ][pos] = f[YZ][pos] - vtst * T(2) / mu * plane[1][ti];
+        f[XX][pos] = f[XX][pos] - vtst * T(2) / la * plane[2][ti];
+        f[YY][pos] = f[YY][pos] - vtst * T(2) / la * plane[2][ti];
+        f[ZZ][pos] = f[ZZ][pos] - vtst * T(2) / (la + T(2) * mu) * plane[2][ti];
+      }
+  }
+
   void step(int nve, int n) override {
     for (int s = 0; s < n; ++s) {
       if (cur == 0 && !initial_done) {
@@ -698,6 +730,7 @@ struct Oracle : Base {
       point_sources();  // sources_add_cartesian (pmcl3d.c:1987-2004)
       if (ifault == 1 && cur < nst) addsrc((int)cur);
       if (ifault == 5) addkinsrc((int)cur);
+      if (ifault == 6 && cur < plane_n) addplanesrc((int)cur);
       if (nve == 3) plasticity();
       fstr();
     }
@@ -783,6 +816,10 @@ void oracle_set_filter(oracle* o, int order, const double* b, const double* a) {
   o->impl->set_filter(order, b, a);
 }
 void oracle_get_moment(oracle* o, float* m) { o->impl->get_moment(m); }
+void oracle_set_plane_wave(oracle* o, int n, int nd, const float* vx, const float* vy,
+                           const float* vz) {
+  o->impl->set_plane_wave(n, nd, vx, vy, vz);
+}
 void oracle_set_plasticity(oracle* o, float fmajor, float fminor, const float* Rz,
                            const float* RzT) {
   o->impl->set_plasticity(fmajor, fminor, Rz, RzT);

@@ -51,6 +51,8 @@ void oracle_set_filter(oracle* o, int order, const double* b, const double* a);
 void oracle_get_moment(oracle* o, float* mom);
 
 /* Plasticity (NVE=3): principal-stress frame; sigma2/cohes/phi via set_field. */
+void oracle_set_plane_wave(oracle* o, int n, int nd, const float* vx, const float* vy,
+                           const float* vz);
 void oracle_set_plasticity(oracle* o, float fmajor, float fminor, const float* Rz,
                            const float* RzT);
 

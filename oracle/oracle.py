@@ -49,6 +49,7 @@ def load():
         lib.oracle_set_filter.argtypes = [c_void_p, c_int, POINTER(c_double), POINTER(c_double)]
         lib.oracle_get_moment.argtypes = [c_void_p, _F]
         lib.oracle_set_plasticity.argtypes = [c_void_p, c_float, c_float, _F, _F]
+        lib.oracle_set_plane_wave.argtypes = [c_void_p, c_int, c_int, _F, _F, _F]
         lib.oracle_step.argtypes = [c_void_p, c_int, c_int]
         lib.oracle_set_flush_denormals.argtypes = [c_void_p, c_int]
         lib.oracle_add_point_sources.argtypes = ([c_void_p, c_int, c_int, c_int] + [_I] * 3 +
@@ -112,6 +113,14 @@ class OracleSim:
 
     def compute_lam_mu(self):
         self.lib.oracle_compute_lam_mu(self.o)
+
+    def set_plane_wave(self, vx, vy, vz):
+        """IFAULT 6 plane-wave series (ini_plane_wave), entering on level
+        align + ND + 1 of this grid."""
+        xs = [np.ascontiguousarray(v, np.float32) for v in (vx, vy, vz)]
+        self._plane = xs
+        self.lib.oracle_set_plane_wave(self.o, int(xs[0].size), int(self.p["nd"]),
+                                       *[x.ctypes.data_as(_F) for x in xs])
 
     def set_plasticity(self, fmajor, fminor, Rz, RzT):
         self.lib.oracle_set_plasticity(self.o, fmajor, fminor,

@@ -506,7 +506,10 @@ class RefGpuSim:
         lib.addkinsrc_H.argtypes = [c_int, c_int, V, c_int, V] + [V] * 15 + [c_int]
         lib.drprecpc_calc_H_opt.argtypes = [V] * 13 + [c_int] * 5 + [V, c_int]
         lib.drprecpc_app_H.argtypes = [V] * 9 + [c_int] * 5 + [V, c_int]
+        lib.addplanesrc_H.argtypes = [c_int, c_int, c_int, V, V, V, c_int, c_int, c_int] + \
+            [V] * 9 + [c_int]
         self.lib = lib
+        self.plane = None
         self.scn = scn
         p = scn.params
         self.p = p
@@ -638,9 +641,22 @@ class RefGpuSim:
         for hook in self.after_stress:
             hook(self, self.cur)
 
+    def set_plane_wave(self, vx, vy, vz):
+        """IFAULT 6 input series (ini_plane_wave, source.c:797-833) on the device."""
+        self.plane = [self.torch.as_tensor(np.ascontiguousarray(v, np.float32)).cuda()
+                      for v in (vx, vy, vz)]
+
     def sources(self):
         f = self.f
         P = self.ptr
+        if self.p["ifault"] == 6:
+            # addplanesrc_H while cur_step < NST (pmcl3d.c:2035-2041)
+            if self.plane is not None and self.cur < self.p["nst"]:
+                self.lib.addplanesrc_H(self.cur, 3, self.p["nst"], None, P(f["mu"]), P(f["lam"]),
+                                       self.p["nd"], self.nx, self.ny,
+                                       *[P(t) for t in self.plane], P(f["xx"]), P(f["yy"]),
+                                       P(f["zz"]), P(f["xy"]), P(f["yz"]), P(f["xz"]), self.grid)
+            return
         if self.p["ifault"] < 4 and self.cur < self.p["nst"]:
             self.source_step += 1
             if self.npsrc:

@@ -33,6 +33,14 @@ def test_nz_block_rule(tmp_path):
     assert r.returncode == 0 and "not divisble by BLOCK_SIZE_Z" in r.stderr
 
 
+def test_plane_wave_needs_read_step_equal_nst(tmp_path):
+    # pmcl3d.c:751-761: IFAULT=6 reads NST samples and wants READ_STEP == NST
+    r = run(["-X", 16, "-Y", 16, "-Z", 16, "-I", 6, "-N", 20, "-R", 10], tmp_path)
+    assert r.returncode == 1 and "READ_STEP should be equal NST" in r.stderr
+    r = run(["-X", 16, "-Y", 16, "-Z", 16, "-I", 6, "-N", 0, "-R", 0], tmp_path)
+    assert r.returncode == 1 and "should be > 0 for IFAULT=6" in r.stderr
+
+
 def test_unknown_option_prints_usage(tmp_path):
     r = run(["--BOGUS", "1"], tmp_path)
     assert r.returncode != 0
