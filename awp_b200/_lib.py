@@ -107,6 +107,8 @@ def load() -> ctypes.CDLL:
     _sig(lib, "awp_field_device_ptr", c_int, [_P, c_int, POINTER(c_void_p)])
     _sig(lib, "awp_gather_output", c_int,
          [_P] + [c_int] * 9 + [c_void_p] * 4)
+    _sig(lib, "awp_compute_bathymetry", c_int, [_P, _I])
+    _sig(lib, "awp_set_bathymetry", c_int, [_P, _I])
     _sig(lib, "awp_check_finite", c_int, [_P, _I])
     _sig(lib, "awp_mesh_create", c_int, [POINTER(awp_params), c_int, POINTER(c_void_p)])
     _sig(lib, "awp_mesh_destroy", c_int, [_P])
@@ -126,8 +128,10 @@ def load() -> ctypes.CDLL:
     _sig(lib, "awp_batch_set_branches", c_int, [_P, c_int])
     _sig(lib, "awp_batch_info", c_int, [_P, POINTER(c_longlong)])
     _sig(lib, "awp_receivers_init", c_int, [_P, c_char_p, c_longlong])
+    _sig(lib, "awp_sgt_init", c_int, [_P, c_char_p, c_longlong])
     _sig(lib, "awp_receivers_count", c_int, [_P, _I])
     _sig(lib, "awp_sourcefile_init", c_int, [_P, c_char_p])
+    _sig(lib, "awp_forcefile_init", c_int, [_P, c_char_p])
     _sig(lib, "awp_topo_metrics", c_int, [c_char_p, c_int, c_int, c_int, c_float, _F])
     _sig(lib, "awp_topography_init", c_int, [_P, c_char_p])
     _sig(lib, "awp_set_topo_plasticity", c_int, [_P, c_int])

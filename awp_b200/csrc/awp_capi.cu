@@ -79,6 +79,9 @@ struct awp_ctx {
   double* d_filt = nullptr;
   float* d_plane[3] = {};  // IFAULT 6 plane-wave series (x, y, z), plane_n samples each
   int plane_n = 0;
+  // FOLLOWBATHY surface level per padded (i, j) column, [j][i] (pmcl3d.c:905-930)
+  int* d_bathy = nullptr;
+  std::vector<int> bathy;
   int filtorder = 0;
   double filt_b[AWP_MAXFILT] = {}, filt_a[AWP_MAXFILT] = {};
   // plasticity
@@ -93,7 +96,10 @@ struct awp_ctx {
   long long cur_step = 0;
   bool initial_src_done = false;
   RecvState* recv = nullptr;     // RECVFILE receivers
+  RecvState* sgt = nullptr;      // SGTFILE stress receivers
+  RecvState* sgt_mat = nullptr;  // SGTFILE material output (one write)
   SrcFileState* srcf = nullptr;  // SOURCEFILE moment-tensor sources
+  SrcFileState* forcef = nullptr;  // FORCEFILE boundary forces (curvilinear block)
   // curvilinear topography of the top grid (topo_t of the reference)
   awp::TopoMetrics* topo = nullptr;  // host metrics (point-set set-up)
   float* d_topo = nullptr;           // f arrays then g arrays, one allocation
@@ -446,6 +452,14 @@ int phase_sources(awp_ctx* c) {
                      sizeof(g_errmsg)))
       return AWP_ERR_IO;
   }
+  if (c->forcef) {  // forces_read + forces_add after the moments (pmcl3d.c:1989-1994)
+    PhaseScope ps(c, 2);
+    float* const vel[3] = {f[AWP_U1], f[AWP_V1], f[AWP_W1]};
+    if (awp_srcf_read(c->forcef, c->cur_step, c->stream, g_errmsg, sizeof(g_errmsg)) ||
+        awp_forcef_add(c->forcef, c->cur_step, vel, f[AWP_D1], c->stream, &c->launches,
+                       g_errmsg, sizeof(g_errmsg)))
+      return AWP_ERR_IO;
+  }
   if ((c->p.ifault < 4 && c->cur_step < c->p.nst) || c->p.ifault == 5) {
     PhaseScope ps(c, 2);
     int st = launch_sources(c, (int)c->cur_step);
@@ -509,13 +523,24 @@ int phase_fstr(awp_ctx* c) {
   return AWP_OK;
 }
 
+// sgt_write (receivers/sgt.c:92-127) of the six stresses at the current step
+int sgt_record(awp_ctx* c) {
+  float** f = c->f;
+  const float* const stress[6] = {f[AWP_XX], f[AWP_YY], f[AWP_ZZ],
+                                  f[AWP_XY], f[AWP_XZ], f[AWP_YZ]};
+  if (c->sgt && awp_recv_record_fields(c->sgt, c->cur_step, stress, c->stream, &c->launches,
+                                       g_errmsg, sizeof(g_errmsg)))
+    return AWP_ERR_IO;
+  return AWP_OK;
+}
+
 int phase_receivers(awp_ctx* c) {
   float** f = c->f;
   if (c->recv &&  // receivers_write (pmcl3d.c:2246-2247)
       awp_recv_record(c->recv, c->cur_step, f[AWP_U1], f[AWP_V1], f[AWP_W1], c->stream,
                       &c->launches, g_errmsg, sizeof(g_errmsg)))
     return AWP_ERR_IO;
-  return AWP_OK;
+  return sgt_record(c);  // pmcl3d.c:2248-2249
 }
 
 int one_step(awp_ctx* c) {
@@ -699,7 +724,10 @@ int awp_ctx_destroy(awp_ctx* c) {
   if (!c) return AWP_OK;
   if (c->stream) cudaStreamSynchronize(c->stream);
   awp_recv_destroy(c->recv);
+  awp_recv_destroy(c->sgt);
+  awp_recv_destroy(c->sgt_mat);
   awp_srcf_destroy(c->srcf);
+  awp_srcf_destroy(c->forcef);
   delete c->topo;
   cudaFree(c->d_topo);
   cudaFree(c->adj_slab);
@@ -709,6 +737,7 @@ int awp_ctx_destroy(awp_ctx* c) {
   for (int i = 0; i < 6; ++i) cudaFree(c->d_src[i]);
   cudaFree(c->d_mom); cudaFree(c->d_filt); cudaFree(c->d_neta_mult); cudaFree(c->d_flag);
   for (int q = 0; q < 3; ++q) cudaFree(c->d_plane[q]);
+  cudaFree(c->d_bathy);
   cudaFree(c->d_ext);
   cudaFree(c->d_err);
   for (auto& e : c->ev_used) { cudaEventDestroy(e.a); cudaEventDestroy(e.b); }
@@ -734,7 +763,7 @@ int awp_ctx_create(const awp_params* p, awp_ctx** out) {
                      "NVE=%d: the time loop runs only for NVE 1 or 3 (pmcl3d.c:1624)", p->nve);
   if (p->npc != 0 && p->npc != 2)
     return set_error(AWP_ERR_UNSUPPORTED, "NPC=%d (only 0 and 2 run the loop)", p->npc);
-  if (p->ifault != 1 && p->ifault != 5 && p->ifault != 0 && p->ifault != 6)
+  if (p->ifault != 1 && p->ifault != 2 && p->ifault != 5 && p->ifault != 0 && p->ifault != 6)
     return set_error(AWP_ERR_UNSUPPORTED, "IFAULT=%d", p->ifault);
   const long long cells = (long long)(p->nx + 20) * (p->ny + 20) * (p->nz + 64);
   if (cells >= (1LL << 31))
@@ -962,9 +991,10 @@ int awp_upload_sources(awp_ctx* c, int nsrc, const int* pos, const float* data) 
   if (!c) return set_error(AWP_ERR_ARG, "null context");
   if (nsrc < 0 || (nsrc > 0 && (!pos || !data))) return set_error(AWP_ERR_ARG, "bad sources");
   const int rs = c->p.read_step;
-  if (c->p.ifault == 1 && rs < c->p.nst)
+  if ((c->p.ifault == 1 || c->p.ifault == 2) && rs < c->p.nst)
     return set_error(AWP_ERR_UNSUPPORTED,
-                     "IFAULT=1 holds all NST samples on the device (READ_STEP >= NST)");
+                     "IFAULT=%d holds all NST samples on the device (READ_STEP >= NST)",
+                     c->p.ifault);
   const int stride = (c->p.ifault == 5) ? 2 : rs;
   // group by target cell (file order kept inside a cell)
   std::map<long long, std::vector<int>> cells;
@@ -1169,6 +1199,25 @@ int awp_gather_output(awp_ctx* c, int nbgx, int nedx, int nskpx, int nbgy, int n
                       float* bufz, float* bufeta) {
   if (!c || !bufx || !bufy || !bufz) return set_error(AWP_ERR_ARG, "null argument");
   if (nskpx < 1 || nskpy < 1 || nskpz < 1) return set_error(AWP_ERR_ARG, "skip < 1");
+  // every read inside the padded arrays: columns 2+ngsl+nbg .. 2+ngsl+ned, and
+  // the levels top-k (w one lower on grid 0) or bathy-k
+  const int shift = (c->p.grid == 0) ? 1 : 0;
+  const bool follow = c->p.grid == 0 && c->d_bathy;
+  if (nbgx < 0 || nbgy < 0 || nbgz < 0 || nedx < nbgx || nedy < nbgy || nedz < nbgz ||
+      2 + AWP_NGSL + nedx >= c->g.nx_pad() || 2 + AWP_NGSL + nedy >= c->g.ny_pad() ||
+      (!follow && c->g.top() - nedz - shift < 0))
+    return set_error(AWP_ERR_ARG, "output window outside the grid");
+  if (follow) {  // koz = bathy - k (- 1 at the top level) >= 0 at every recorded column
+    const long long ld = c->g.nx_pad();
+    for (int j = nbgy; j <= nedy; j += nskpy)
+      for (int i = nbgx; i <= nedx; i += nskpx) {
+        const int b = c->bathy[(size_t)(2 + AWP_NGSL + j) * ld + 2 + AWP_NGSL + i];
+        if (b - nedz - (b == c->g.top() ? 1 : 0) < 0)
+          return set_error(AWP_ERR_ARG,
+                           "recorded depth %d is below the bathymetry level %d at column "
+                           "(%d, %d)", nedz, b, i, j);
+      }
+  }
   VelBufArgs a;
   memset(&a, 0, sizeof(a));
   a.u1 = c->f[AWP_U1]; a.v1 = c->f[AWP_V1]; a.w1 = c->f[AWP_W1]; a.neta = c->f[AWP_NETA];
@@ -1182,8 +1231,58 @@ int awp_gather_output(awp_ctx* c, int nbgx, int nedx, int nskpx, int nbgy, int n
   a.rec_nzt = (nedz - nbgz) / nskpz + 1;
   a.slice = c->g.slice; a.yline = c->g.yline; a.ktop = c->g.top();
   // w one cell below the recorded level on grid 0 only (kernel.cu:3975-3986)
-  a.w_shift = (c->p.grid == 0) ? 1 : 0;
+  a.w_shift = shift;
+  if (follow) {
+    a.bathy = c->d_bathy;
+    a.bathy_ld = (int)c->g.nx_pad();
+  }
   CU_TRY(awp_launch_velbuffer(a, c->stream));
+  return AWP_OK;
+}
+
+int awp_compute_bathymetry(awp_ctx* c, int* bathy) {
+  if (!c || !bathy) return set_error(AWP_ERR_ARG, "null argument");
+  if (!c->media_ready) return set_error(AWP_ERR_STATE, "media not uploaded");
+  const size_t n = (size_t)c->g.cells_pad();
+  std::vector<float> mu(n), d1(n);
+  CU_TRY(cudaStreamSynchronize(c->stream));
+  CU_TRY(cudaMemcpy(mu.data(), c->f[AWP_MU], n * 4, cudaMemcpyDeviceToHost));
+  CU_TRY(cudaMemcpy(d1.data(), c->f[AWP_D1], n * 4, cudaMemcpyDeviceToHost));
+  const long long nxp = c->g.nx_pad(), nyp = c->g.ny_pad();
+  // pmcl3d.c:909-925: the highest level below the top with vs above 1 mm/s
+  for (long long i = 0; i < nxp; ++i)
+    for (long long j = 0; j < nyp; ++j) {
+      int level = 0;
+      for (int k = c->g.top(); k > AWP_ALIGN; --k) {
+        const size_t q = (size_t)(i * c->g.slice + j * c->g.yline + k);
+        const float prod = mu[q] * d1[q];
+        const float vs = (float)sqrt(1. / (double)prod);
+        if (vs > 0.001f) {
+          level = k;
+          break;
+        }
+      }
+      bathy[j * nxp + i] = level;
+    }
+  return AWP_OK;
+}
+
+int awp_set_bathymetry(awp_ctx* c, const int* bathy) {
+  if (!c) return set_error(AWP_ERR_ARG, "null context");
+  cudaFree(c->d_bathy);
+  c->d_bathy = nullptr;
+  c->bathy.clear();
+  if (!bathy) return AWP_OK;
+  if (c->p.grid != 0) return set_error(AWP_ERR_STATE, "FOLLOWBATHY applies to grid 0 only");
+  const size_t n = (size_t)(c->g.nx_pad() * c->g.ny_pad());
+  for (size_t q = 0; q < n; ++q)
+    if (bathy[q] < 0 || bathy[q] > c->g.top())
+      return set_error(AWP_ERR_ARG, "bathymetry level %d outside 0..%d at column %zu", bathy[q],
+                       c->g.top(), q);
+  int st;
+  if ((st = ctx_alloc(c, (void**)&c->d_bathy, n * sizeof(int)))) return st;
+  CU_TRY(cudaMemcpy(c->d_bathy, bathy, n * sizeof(int), cudaMemcpyHostToDevice));
+  c->bathy.assign(bathy, bathy + n);
   return AWP_OK;
 }
 
@@ -1203,6 +1302,38 @@ int awp_receivers_init(awp_ctx* c, const char* recvfile, long long nt) {
   return AWP_OK;
 }
 
+int awp_sgt_init(awp_ctx* c, const char* sgtfile, long long nt) {
+  if (!c || !sgtfile) return set_error(AWP_ERR_ARG, "null argument");
+  if (nt < 1) return set_error(AWP_ERR_ARG, "nt must be >= 1");
+  if (c->sgt) return set_error(AWP_ERR_STATE, "SGT output already initialised");
+  if (!c->media_ready) return set_error(AWP_ERR_STATE, "media not uploaded");
+  RecvState *r = nullptr, *m = nullptr;
+  const int e = awp_sgt_create(sgtfile, nt, c->g, c->p.dh, c->topo, &r, &m, g_errmsg,
+                               sizeof(g_errmsg));
+  if (e) return e < 0 ? AWP_ERR_CUDA : AWP_ERR_IO;
+  c->sgt = r;
+  c->sgt_mat = m;
+  // sgt_write_material_properties (sgt.c:70-90, pmcl3d.c:1575-1578): the
+  // reference writes the inverse-lambda array to the "d1" file as well, and so
+  // does this build; then "lami" (1/lambda) and "mui" (1/mu)
+  const std::string base = awp_recv_base(c->sgt_mat, 0);
+  const struct {
+    const char* suffix;
+    const float* field;
+  } out[3] = {{"d1", c->f[AWP_LAM]}, {"lami", c->f[AWP_LAM]}, {"mui", c->f[AWP_MU]}};
+  for (const auto& o : out)
+    if (awp_recv_write_once(c->sgt_mat, o.field, (base + o.suffix).c_str(), c->stream,
+                            &c->launches, g_errmsg, sizeof(g_errmsg)))
+      return AWP_ERR_IO;
+  // the state before the first step (pmcl3d.c:1605), which holds the step-1
+  // source sample the reference adds before the loop (pmcl3d.c:1175-1187)
+  if (c->ncell) {
+    const int s = initial_source(c);
+    if (s) return s;
+  }
+  return sgt_record(c);
+}
+
 int awp_receivers_count(awp_ctx* c, int counts[3]) {
   if (!c || !counts) return set_error(AWP_ERR_ARG, "null argument");
   for (int q = 0; q < 3; ++q) counts[q] = awp_recv_length(c->recv, q);
@@ -1219,6 +1350,24 @@ int awp_sourcefile_init(awp_ctx* c, const char* sourcefile) {
   c->srcf = s;
   // sources_read(0) before the loop (pmcl3d.c:1607)
   if (awp_srcf_read(c->srcf, c->cur_step, c->stream, g_errmsg, sizeof(g_errmsg)))
+    return AWP_ERR_IO;
+  return AWP_OK;
+}
+
+int awp_forcefile_init(awp_ctx* c, const char* forcefile) {
+  if (!c || !forcefile) return set_error(AWP_ERR_ARG, "null argument");
+  if (c->forcef) return set_error(AWP_ERR_STATE, "FORCEFILE already initialised");
+  if (!c->topo)
+    return set_error(AWP_ERR_STATE,
+                     "FORCEFILE forces act on a curvilinear top block: initialise the "
+                     "topography first");
+  SrcFileState* s = nullptr;
+  const int e = awp_forcef_create(forcefile, c->g, c->p.dh, c->p.dt, c->topo, &s, g_errmsg,
+                                  sizeof(g_errmsg));
+  if (e) return e < 0 ? AWP_ERR_CUDA : AWP_ERR_IO;
+  c->forcef = s;
+  // forces_read(0) before the loop (pmcl3d.c:1608)
+  if (awp_srcf_read(c->forcef, c->cur_step, c->stream, g_errmsg, sizeof(g_errmsg)))
     return AWP_ERR_IO;
   return AWP_OK;
 }
@@ -1250,7 +1399,7 @@ int awp_input_read(const char* path, long long hdr[8], char* file, int filecap, 
 static int point_coefs(const char* path, const char* intopo, int grid_type, int nxt, int nyt,
                        int nzt, float h, long long cap, int* count, int* indices, int* ix,
                        int* iy, int* iz, float* lx, float* ly, float* lz) {
-  if (!path || !count || grid_type < 0 || grid_type > 8) return AWP_ERR_ARG;
+  if (!path || !count || grid_type < 0 || grid_type > 9) return AWP_ERR_ARG;
   awp::InputFile in;
   int e = awp::read_input(path, &in);
   if (e) return e;
@@ -1631,8 +1780,8 @@ int awp_batch_create(awp_ctx* const* ctxs, int n, awp_batch** out) {
     awp_ctx* c = ctxs[q];
     if (!c) return set_error(AWP_ERR_ARG, "instance %d is null", q);
     if (!c->media_ready) return set_error(AWP_ERR_STATE, "instance %d: media not uploaded", q);
-    if (c->p.ngrids != 1 || c->p.nve == 3 || c->topo || c->recv || c->srcf ||
-        c->p.ifault == 6)
+    if (c->p.ngrids != 1 || c->p.nve == 3 || c->topo || c->recv || c->srcf || c->forcef ||
+        c->sgt || c->p.ifault == 6)
       return set_error(AWP_ERR_UNSUPPORTED,
                        "instance %d: a batch holds single-grid Cartesian runs without "
                        "plasticity, receivers, SOURCEFILE or plane-wave sources", q);
@@ -1814,9 +1963,10 @@ int awp_set_topo_plasticity(awp_ctx* c, int consistent) {
 int awp_topography_init(awp_ctx* c, const char* intopo) {
   if (!c || !intopo) return set_error(AWP_ERR_ARG, "null argument");
   if (c->topo) return set_error(AWP_ERR_STATE, "topography already initialised");
-  if (c->recv || c->srcf)
+  if (c->recv || c->srcf || c->forcef || c->sgt)
     return set_error(AWP_ERR_STATE,
-                     "topography must be initialised before receivers and SOURCEFILE sources");
+                     "topography must be initialised before receivers, SGT output, "
+                     "SOURCEFILE sources and FORCEFILE forces");
   if (c->p.grid != 0)
     return set_error(AWP_ERR_ARG, "topography belongs to the top grid (grid 0) only");
   const int nx = c->g.nxt, ny = c->g.nyt, nz = c->g.nzt;
@@ -1885,13 +2035,15 @@ namespace {
 int check_adjoint_ctx(awp_ctx* c) {
   if (!c) return set_error(AWP_ERR_ARG, "null context");
   if (!c->media_ready) return set_error(AWP_ERR_STATE, "media not uploaded");
-  if (c->p.ngrids != 1 || c->p.nve == 3 || c->topo || c->recv || c->srcf)
+  if (c->p.ngrids != 1 || c->p.nve == 3 || c->topo || c->recv || c->srcf || c->forcef ||
+      c->sgt)
     return set_error(AWP_ERR_UNSUPPORTED,
                      "the adjoint covers single-grid Cartesian runs without plasticity, "
-                     "receiver files or SOURCEFILE sources");
-  if (c->ncell > 0 && c->p.ifault != 1)
+                     "receiver or SGT files or SOURCEFILE sources");
+  if (c->ncell > 0 && c->p.ifault != 1 && c->p.ifault != 2)
     return set_error(AWP_ERR_UNSUPPORTED,
-                     "the adjoint takes IFAULT 1 sources (the kinematic source depends on mu)");
+                     "the adjoint takes IFAULT 1 or 2 sources (the kinematic source depends on "
+                     "mu)");
   return AWP_OK;
 }
 

@@ -187,7 +187,9 @@ int find_grid_numbers(const InputFile& in, const BlockDesc* blocks, int ngrids,
 }
 
 // padding of the component grids of grids_init (topography/grids.c:24-37)
-int component_padding(GridType t) { return t <= GT_Z ? 0 : AWP_NGSL / 2; }
+// topography/grids.c:26-40: velocity and material grids without padding,
+// stress grids with ngsl / 2
+int component_padding(GridType t) { return (t <= GT_Z || t == GT_NODE) ? 0 : AWP_NGSL / 2; }
 
 }  // namespace
 
@@ -258,10 +260,10 @@ int read_input(const char* path, InputFile* out) {
 }
 
 void grid_shift(GridType t, int s[3]) {
-  // grid/shift.c:80-151: u1 (1,1,1), u2 (0,0,1), u3 (0,1,0), normal stresses
-  // (0,1,1), xy (1,0,1), xz (1,1,0), yz (0,0,0)
-  static const int tab[9][3] = {{1, 1, 1}, {0, 0, 1}, {0, 1, 0}, {0, 1, 1}, {0, 1, 1},
-                                {0, 1, 1}, {1, 0, 1}, {1, 1, 0}, {0, 0, 0}};
+  // grid/shift.c:76-151: u1 (1,1,1), u2 (0,0,1), u3 (0,1,0), normal stresses
+  // (0,1,1), xy (1,0,1), xz (1,1,0), yz (0,0,0), material node (1,0,0)
+  static const int tab[10][3] = {{1, 1, 1}, {0, 0, 1}, {0, 1, 0}, {0, 1, 1}, {0, 1, 1},
+                                 {0, 1, 1}, {1, 0, 1}, {1, 1, 0}, {0, 0, 0}, {1, 0, 0}};
   s[0] = tab[t][0];
   s[1] = tab[t][1];
   s[2] = tab[t][2];

@@ -61,7 +61,7 @@ struct InputFile {
 int read_input(const char* path, InputFile* out);
 
 // Staggered component of a point set (topography/grids.c:45-90, grid/shift.c).
-enum GridType { GT_X = 0, GT_Y, GT_Z, GT_XX, GT_YY, GT_ZZ, GT_XY, GT_XZ, GT_YZ };
+enum GridType { GT_X = 0, GT_Y, GT_Z, GT_XX, GT_YY, GT_ZZ, GT_XY, GT_XZ, GT_YZ, GT_NODE };
 void grid_shift(GridType t, int shift[3]);
 
 // One grid block of a (possibly discontinuous) mesh, top block first.

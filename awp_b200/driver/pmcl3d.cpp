@@ -1,17 +1,19 @@
 // pmcl3d -- single-rank drop-in for the reference's pmcl3d executable.
 //
 // Same command line (src/awp/command.c), same input files (INVEL mesh,
-// INSRC sources, sourcefilter.dat, nonlinear.dat, SOURCEFILE and RECVFILE
-// point sets, INTOPO topography) and the same output files (OUT/SX_0_%07ld, SY, SZ, Eta; the
-// CHKFILE statistics log; the receiver files <file>_<x|y|z>_<step>) as the
-// reference's single-rank run; the time step itself runs in libawpb200
-// through its C ABI.
+// INSRC sources or plane wave, sourcefilter.dat, nonlinear.dat, SOURCEFILE,
+// RECVFILE, FORCEFILE and SGTFILE point sets, INTOPO topography) and the same output
+// files (OUT/SX_0_%07ld, SY, SZ, Eta; the CHKFILE statistics log; the receiver
+// files <file>_<x|y|z>_<step>; the SGT files <file>_<Gxx..Gyz>_<step> and the
+// material files <file>_<d1|lami|mui>) as the reference's single-rank run; the
+// time step itself runs in libawpb200 through its C ABI.
 //
 // Scope: one rank (PX = PY = 1, no I/O ranks), one grid or a discontinuous
 // mesh of NGRIDS blocks (each 3x finer than the one below, pmcl3d.c:370-378),
-// MEDIASTART 0-2, IFAULT 1, 5 and 6, NVE 1 and 3.  On a mesh the SOURCEFILE /
-// RECVFILE point sets and the topography belong to the top block (grid 0).
-// Anything else is reported and refused.
+// MEDIASTART 0-3, IFAULT 1, 2, 5 and 6, NVE 1 and 3, FOLLOWBATHY 0 and 1.  On a
+// mesh the SOURCEFILE / RECVFILE / FORCEFILE / SGTFILE point sets and the
+// topography belong to the top block (grid 0).  Anything else is reported and
+// refused.
 #include <getopt.h>
 #include <math.h>
 #include <stdio.h>
@@ -21,6 +23,7 @@
 #include <sys/time.h>
 #include <unistd.h>
 
+#include <algorithm>
 #include <string>
 #include <vector>
 
@@ -258,10 +261,6 @@ int main(int argc, char** argv) {
     fprintf(stderr, "pmcl3d: NGRIDS=%d is outside 1..%d\n", G, MAXGRIDS);
     return 1;
   }
-  if (A.USEFORCEFILE || A.USESGTFILE) {
-    fprintf(stderr, "pmcl3d: FORCEFILE/SGTFILE are not part of this build\n");
-    return 1;
-  }
   // block sizes of the mesh (pmcl3d.c:370-378): NX, NY, DH are the coarsest
   // block's, each block above is 3x finer
   int grdfct[MAXGRIDS], nxt[MAXGRIDS], nyt[MAXGRIDS], nzt[MAXGRIDS];
@@ -307,7 +306,7 @@ int main(int argc, char** argv) {
     if (!grid_output[p]) rnx[p] = rny[p] = rnz[p] = 0;
   }
 
-  if (A.IFAULT != 1 && A.IFAULT != 5 && A.IFAULT != 6) {
+  if (A.IFAULT != 1 && A.IFAULT != 2 && A.IFAULT != 5 && A.IFAULT != 6) {
     fprintf(stderr, "pmcl3d: IFAULT=%d sources are not part of this build\n", A.IFAULT);
     return 1;
   }
@@ -335,7 +334,9 @@ int main(int argc, char** argv) {
     P[p].nd = A.ND * grdfct[p];  // inicrj with ND*grdfct[p] (pmcl3d.c:1029)
     P[p].nve = (A.NVE == 3) ? 3 : 1;
     P[p].fac = A.FAC; P[p].q0 = A.Q0; P[p].ex = A.EX; P[p].fp = A.FP; P[p].socalq = A.SoCalQ;
-    P[p].ifault = A.IFAULT; P[p].nst = A.NST; P[p].read_step = A.READ_STEP_GPU;
+    // IFAULT 2 windows of READ_STEP samples are assembled here into all NST
+    P[p].ifault = A.IFAULT; P[p].nst = A.NST;
+    P[p].read_step = (A.IFAULT == 2) ? std::max(A.NST, 1) : A.READ_STEP_GPU;
     P[p].grid = p;
     P[p].ngrids = G;
   }
@@ -366,6 +367,66 @@ int main(int argc, char** argv) {
   int nsrc[MAXGRIDS] = {0};
   for (int p = 0; p < G; ++p) {  // INSRC_<p> for every block with sources (pmcl3d.c:702-708)
     if (A.NSRC[p] <= 0 || !(A.IFAULT < 3 || A.IFAULT == 5)) continue;
+    if (A.IFAULT == 2) {
+      // read_src_ifault_2 (source.c:15-128) at rank 0: the header
+      // "<INSRC>_<p>0000000" (npsrc, two words, positions), then the READ_STEP
+      // windows "<INSRC_I2>_<p>0000000_<idx>", idx from 1, of six component
+      // arrays (xx yy zz xz yz xy), each time-major with the sources fastest;
+      // the time loop reads window idx at step (idx-1)*READ_STEP
+      // (pmcl3d.c:2442-2461) while it is below NST
+      char name[600];
+      snprintf(name, sizeof(name), "%s_%d%07d", A.INSRC.c_str(), p, 0);
+      FILE* f = fopen(name, "rb");
+      if (!f) continue;  // no sources in this partition
+      printf("SOURCE reading first time: %s\n", name);
+      int np = 0, dummy[2];
+      if (fread(&np, sizeof(int), 1, f) != 1 || fread(dummy, sizeof(int), 2, f) != 2 || np < 0) {
+        fclose(f);
+        fprintf(stderr, "pmcl3d: %s: bad header\n", name);
+        return 1;
+      }
+      std::vector<int> pos((size_t)np * 3);
+      if (fread(pos.data(), sizeof(int), pos.size(), f) != pos.size()) {
+        fclose(f);
+        fprintf(stderr, "pmcl3d: %s: %d positions expected\n", name, np);
+        return 1;
+      }
+      fclose(f);
+      if (np == 0) continue;
+      const int RS = A.READ_STEP, N = std::max(A.NST, 1);
+      if (RS < 1) {
+        fprintf(stderr, "pmcl3d: IFAULT=2 needs READ_STEP >= 1\n");
+        return 1;
+      }
+      std::vector<float> sdat((size_t)np * N * 6, 0.f), win((size_t)np * RS);
+      for (int idx = 1; (long)(idx - 1) * RS < N; ++idx) {
+        snprintf(name, sizeof(name), "%s_%d%07d_%03d", A.INSRC_I2.c_str(), p, 0, idx);
+        printf("SOURCE reading: %s\n", name);
+        FILE* g = fopen(name, "rb");
+        if (!g) {
+          printf("ERROR! Rank=%d: Cannot open file: %s\n", 0, name);
+          return 1;
+        }
+        for (int q = 0; q < 6; ++q) {
+          if (fread(win.data(), sizeof(float), win.size(), g) != win.size()) {
+            fclose(g);
+            fprintf(stderr, "pmcl3d: %s: short window\n", name);
+            return 1;
+          }
+          for (int t = 0; t < RS; ++t) {
+            const long step = (long)(idx - 1) * RS + t;
+            if (step >= N) break;
+            for (int s = 0; s < np; ++s)
+              sdat[((size_t)s * N + step) * 6 + q] = win[(size_t)t * np + s];
+          }
+        }
+        fclose(g);
+      }
+      nsrc[p] = np;
+      spos[p] = pos;
+      AWP(awp_upload_sources(ctx[p], np, pos.data(), sdat.data()));
+      continue;
+    }
     char name[512];
     snprintf(name, sizeof(name), "%s_%d", A.INSRC.c_str(), p);
     FILE* f = fopen(name, "rb");
@@ -427,9 +488,14 @@ int main(int argc, char** argv) {
       AWP(awp_field_upload(ctx[p], AWP_MU, mu.data()));
       AWP(awp_field_upload(ctx[p], AWP_LAM, lam.data()));
       vse[p][0] = vse[p][1] = vs; vpe[p][0] = vpe[p][1] = vp; dde[p][0] = dde[p][1] = dd;
-    } else if (A.MEDIASTART == 1 || A.MEDIASTART == 2) {
+    } else if (A.MEDIASTART >= 1 && A.MEDIASTART <= 3) {
       char name[512];
-      snprintf(name, sizeof(name), "%s_%d", A.INVEL.c_str(), p);
+      if (A.MEDIASTART < 3) {
+        snprintf(name, sizeof(name), "%s_%d", A.INVEL.c_str(), p);
+      } else {  // the partition of rank 0 (mesh.c:138-141), the same name for every block
+        snprintf(name, sizeof(name), "input_rst/mediapart/media%07d.bin", 0);
+        printf("Rank=%d, reading file=%s\n", 0, name);
+      }
       const size_t n = (size_t)A.NVAR * nxt[p] * nyt[p] * nzt[p];
       std::vector<float> m(n);
       FILE* f = fopen(name, "rb");
@@ -441,10 +507,33 @@ int main(int argc, char** argv) {
       AWP(awp_upload_media(ctx[p], A.NVAR, m.data()));
       AWP(awp_media_extrema(ctx[p], vse[p], vpe[p], dde[p]));
     } else {
-      fprintf(stderr, "pmcl3d: MEDIASTART=%d (partitioned meshes) is not part of this build\n",
-              A.MEDIASTART);
+      fprintf(stderr, "pmcl3d: MEDIASTART=%d is not part of this build\n", A.MEDIASTART);
       return 1;
     }
+  }
+
+  // ---- FOLLOWBATHY surface levels of grid 0 (pmcl3d.c:905-930) ---------------
+  if (A.FOLLOWBATHY == 1) {
+    const long long nxp = dims[0][0], nyp = dims[0][1];
+    std::vector<int> bathy((size_t)(nxp * nyp));
+    AWP(awp_compute_bathymetry(ctx[0], bathy.data()));
+    std::vector<float> mu(ncell[0]), d1(ncell[0]);
+    AWP(awp_field_download(ctx[0], AWP_MU, mu.data()));
+    AWP(awp_field_download(ctx[0], AWP_D1, d1.data()));
+    mkdir("debug", 0755);
+    FILE* fb = fopen("debug/bathy.0000", "w");
+    if (fb) {
+      for (long long i = 0; i < nxp; ++i)
+        for (long long j = 0; j < nyp; ++j) {
+          const int k = bathy[(size_t)(j * nxp + i)];
+          if (k == 0) continue;
+          const size_t q = (size_t)((i * nyp + j) * dims[0][2] + k);
+          const float tmpvs = (float)sqrt(1. / (mu[q] * d1[q]));
+          fprintf(fb, "%lld %lld %d %e\n", i, j, k, tmpvs);
+        }
+      fclose(fb);
+    }
+    AWP(awp_set_bathymetry(ctx[0], bathy.data()));
   }
 
   // ---- CHK statistics file (writeCHK, io.c:9-43) -----------------------------
@@ -568,9 +657,19 @@ int main(int argc, char** argv) {
   // ---- curvilinear topography of grid 0 (pmcl3d.c:1522-1548) --------------------
   if (A.USETOPO) AWP(awp_topography_init(ctx[0], A.INTOPO.c_str()));
 
-  // ---- SOURCEFILE / RECVFILE point sets (pmcl3d.c:1563-1568, 1603-1607) ---------
+  // ---- SOURCEFILE / RECVFILE / SGTFILE point sets (pmcl3d.c:1563-1578, 1603-1607) -
   if (A.USESOURCEFILE) AWP(awp_sourcefile_init(ctx[0], A.SOURCEFILE.c_str()));
   if (A.USERECVFILE) AWP(awp_receivers_init(ctx[0], A.RECVFILE.c_str(), nt));
+  // FORCEFILE boundary forces (pmcl3d.c:1569-1571, 1608, 1989-1994): added in
+  // the curvilinear branch of the time loop only, so without topography the
+  // reference reads them and never applies them
+  if (A.USEFORCEFILE) {
+    if (A.USETOPO) AWP(awp_forcefile_init(ctx[0], A.FORCEFILE.c_str()));
+    else printf("FORCEFILE %s: forces act with topography only; not applied\n",
+                A.FORCEFILE.c_str());
+  }
+  // SGTFILE stress receivers and material output (pmcl3d.c:1572-1578, 1605)
+  if (A.USESGTFILE) AWP(awp_sgt_init(ctx[0], A.SGTFILE.c_str(), nt));
 
   // ---- output buffers ------------------------------------------------------------
   size_t rec[MAXGRIDS];

@@ -10,7 +10,9 @@ topography/sources/source.c:434-447, topography/receivers/receiver.c:47-113):
 * SOURCEFILE rates: ``<file>_<xx|yy|zz|xy|xz|yz>``, float32, source-major,
   ``steps`` samples per source;
 * receiver output: ``<file>_<x|y|z>_<step>``, float32, receiver-major,
-  ``num_writes`` rings of ``gpu_buffer_size*cpu_buffer_size`` samples each.
+  ``num_writes`` rings of ``gpu_buffer_size*cpu_buffer_size`` samples each;
+  SGT output the same as ``<file>_<Gxx..Gyz>_<step>`` (topography/receivers/sgt.c)
+  plus one sample per point in ``<file>_d1``, ``<file>_lami``, ``<file>_mui``.
 """
 from __future__ import annotations
 
@@ -21,6 +23,7 @@ import numpy as np
 
 COMPONENTS_SRC = ("xx", "yy", "zz", "xy", "xz", "yz")
 COMPONENTS_RECV = ("x", "y", "z")
+COMPONENTS_SGT = ("Gxx", "Gyy", "Gzz", "Gxy", "Gxz", "Gyz")
 
 
 def write_input(path, file, coords, types=None, *, steps=1, stride=1, degree=3,
@@ -59,14 +62,16 @@ def receiver_file_name(base, comp, step, nt, gpu, cpu, num_writes, stride):
     return f"{base}_{comp}_{receiver_file_step(step, gpu, cpu, num_writes, stride):0{zeros}d}"
 
 
-def read_receiver_series(base, nrecv, nt, gpu, cpu, num_writes, stride):
+def read_receiver_series(base, nrecv, nt, gpu, cpu, num_writes, stride,
+                         components=COMPONENTS_RECV):
     """Reassemble the recorded samples of every complete file of a run:
     returns {comp: float32 [nrecv][nsamples]} with sample s taken at step
-    s*stride, s from 0."""
+    s*stride, s from 0 (components: COMPONENTS_RECV for a RECVFILE,
+    COMPONENTS_SGT for an SGTFILE)."""
     ne = gpu * cpu
     unit = ne * num_writes * stride
     out = {}
-    for comp in COMPONENTS_RECV:
+    for comp in components:
         series = []
         fstep = unit
         while True:

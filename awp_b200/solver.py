@@ -8,7 +8,7 @@ raised as :class:`awp_b200._lib.AwpError` carrying the library's status code.
 from __future__ import annotations
 
 import ctypes
-from ctypes import byref, c_float, c_int, c_longlong, c_void_p
+from ctypes import POINTER, byref, c_float, c_int, c_longlong, c_void_p
 
 import numpy as np
 
@@ -200,6 +200,13 @@ class Solver:
         check(self.lib.awp_receivers_init(self.ctx, recvfile.encode(), int(nt)),
               "awp_receivers_init")
 
+    def sgt(self, sgtfile: str, nt: int) -> None:
+        """SGTFILE stress receivers and material output (ASCII v2); writes the
+        material files and records the current stresses at once (with the
+        step-1 source sample of IFAULT < 4 added first, as the reference has
+        it before its loop: upload the sources before this call)."""
+        check(self.lib.awp_sgt_init(self.ctx, sgtfile.encode(), int(nt)), "awp_sgt_init")
+
     def receiver_counts(self) -> tuple[int, int, int]:
         c = (c_int * 3)()
         check(self.lib.awp_receivers_count(self.ctx, c), "awp_receivers_count")
@@ -208,6 +215,11 @@ class Solver:
     def sourcefile(self, sourcefile: str) -> None:
         """SOURCEFILE moment-tensor sources (ASCII v2 + <file>_<xx..yz> rates)."""
         check(self.lib.awp_sourcefile_init(self.ctx, sourcefile.encode()), "awp_sourcefile_init")
+
+    def forcefile(self, forcefile: str) -> None:
+        """FORCEFILE boundary forces on the curvilinear top block (ASCII v2
+        + <file>_<fx|fy|fz> rates); after topography()."""
+        check(self.lib.awp_forcefile_init(self.ctx, forcefile.encode()), "awp_forcefile_init")
 
     # -- time stepping -----------------------------------------------------
     def step(self, n: int = 1) -> None:
@@ -247,6 +259,26 @@ class Solver:
                                          nbgz, nedz, nskpz, c_void_p(bufx), c_void_p(bufy),
                                          c_void_p(bufz), c_void_p(bufeta or None)),
               "awp_gather_output")
+
+    def bathymetry(self) -> np.ndarray:
+        """FOLLOWBATHY surface level per padded column of this grid's media,
+        int32 [ny_pad][nx_pad], as pmcl3d derives it (0 where no level has
+        vs > 0.001)."""
+        nxp, nyp = self.shape[0], self.shape[1]
+        out = np.zeros((nyp, nxp), np.int32)
+        check(self.lib.awp_compute_bathymetry(self.ctx, out.ctypes.data_as(POINTER(c_int))),
+              "awp_compute_bathymetry")
+        return out
+
+    def set_bathymetry(self, bathy: np.ndarray | None) -> None:
+        """Make gather() follow the given surface levels ([ny_pad][nx_pad]
+        int32), or plain levels again with None."""
+        if bathy is None:
+            check(self.lib.awp_set_bathymetry(self.ctx, None), "awp_set_bathymetry")
+            return
+        b = np.ascontiguousarray(bathy, np.int32).reshape(self.shape[1], self.shape[0])
+        check(self.lib.awp_set_bathymetry(self.ctx, b.ctypes.data_as(POINTER(c_int))),
+              "awp_set_bathymetry")
 
     def check_finite(self) -> bool:
         ok = c_int()

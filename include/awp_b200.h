@@ -68,9 +68,10 @@ typedef struct awp_params {
   int nve;           /* -V         1 = anelastic, 3 = anelastic + plasticity      */
   float fac, q0, ex, fp; /* -l -h --EX -p   Q(f) parameters                       */
   int socalq;        /* -s         SoCal vp/vs floor (1 = on)                     */
-  int ifault;        /* -I         1 = point moment-rate source, 5 = kinematic    */
+  int ifault;        /* -I         1 = point moment-rate source, 2 = the same from
+                                   split files, 5 = kinematic, 6 = plane wave     */
   int nst;           /* -N         source time samples                            */
-  int read_step;     /* -R/-Q      samples held per source (IFAULT 1: >= nst)      */
+  int read_step;     /* -R/-Q      samples held per source (IFAULT 1, 2: >= nst)   */
   int grid;          /*            block of a discontinuous mesh, 0 = top (finest)  */
   int ngrids;        /* -G         blocks of the mesh (1 = a single grid)          */
 } awp_params;
@@ -119,7 +120,9 @@ int awp_free_host_pinned(void* ptr);
  * pos[nsrc][3] = (x, y, z) 1-based with z counted down from the surface;
  * data[nsrc][read_step][6] = (xx, yy, zz, xz, yz, xy) per time sample.  For
  * IFAULT=5 only samples 0 and 1 are used and hold the subfault parameters
- * (kernel.cu:3788-3809). */
+ * (kernel.cu:3788-3809).  IFAULT=2 adds as IFAULT=1 (addsrc, pmcl3d.c:2008-2016);
+ * its split files (read_src_ifault_2, source.c:15-128) are assembled by the
+ * caller into all NST samples. */
 int awp_upload_sources(awp_ctx* ctx, int nsrc, const int* pos, const float* data);
 /* Plane-wave input (IFAULT=6; ini_plane_wave, source.c:797-833, and
  * addplanesrc_H, pmcl3d.c:2035-2041): three series of NST samples (vx, vy, vz,
@@ -158,6 +161,18 @@ int awp_receivers_init(awp_ctx* ctx, const char* recvfile, long long nt);
 /* Receivers inside the domain per component (x, y, z). */
 int awp_receivers_count(awp_ctx* ctx, int counts[3]);
 
+/* Strain Green tensor output of an ASCII v2 SGTFILE (replaces sgt_init /
+ * sgt_write_material_properties / sgt_write, src/topography/receivers/sgt.c,
+ * and their calls at pmcl3d.c:1572-1578, 1605, 2248-2249): receivers of the six
+ * stresses on their staggered grids, written like awp_receivers_init's as
+ * "<file>_<Gxx|Gyy|Gzz|Gxy|Gxz|Gyz>_<step>", and once, at this call, the
+ * material on the node grid as "<file>_d1", "<file>_lami" and "<file>_mui"
+ * (1/lambda and 1/mu; "_d1" holds 1/lambda too, as the reference writes it).
+ * Needs the media; the current stresses are recorded at once, after the
+ * step-1 source sample of IFAULT < 4 that the reference adds before its loop
+ * (pmcl3d.c:1175-1187), so upload the sources first. */
+int awp_sgt_init(awp_ctx* ctx, const char* sgtfile, long long nt);
+
 /* Moment-tensor sources of an ASCII v2 SOURCEFILE (replaces sources_init /
  * sources_read / sources_add_cartesian, src/topography/sources/sources.c:27-78,
  * and their calls at pmcl3d.c:1563-1565, 1607, 1987-2004).  Rates are read
@@ -166,11 +181,24 @@ int awp_receivers_count(awp_ctx* ctx, int counts[3]);
  * `stride` steps with Lagrange weights: sigma -= dt/h^3 * w * M(t). */
 int awp_sourcefile_init(awp_ctx* ctx, const char* sourcefile);
 
+/* Boundary forces of an ASCII v2 FORCEFILE on the curvilinear top block
+ * (replaces forces_init / forces_read / forces_add,
+ * src/topography/sources/forces.c:24-96, cusource_add_force_H,
+ * src/topography/sources/source.cu:101-157, and their calls at
+ * pmcl3d.c:1569-1571, 1608, 1989-1994).  Every point must be a boundary point
+ * (type 1).  Rates "<file>_<fx|fy|fz>" as for SOURCEFILE, added to u1, v1, w1
+ * after the stress update: v += dt/h^3 * w * F(t) * q / (f dg rho), with the
+ * SBP boundary weight q, the staggered metric f dg of the component and rho
+ * read ngsl cells further in x and y than the cell, as the reference indexes
+ * it.  Needs the topography first; refused where that density index would
+ * leave the grid. */
+int awp_forcefile_init(awp_ctx* ctx, const char* forcefile);
+
 /* Host-only helpers (no context, no GPU) that expose the point-set set-up for
  * checks: the ASCII v2 reader (readers/input.c:35-42; hdr = length,
  * gpu_buffer_size, cpu_buffer_size, steps, num_writes, stride, degree, major
  * version) and the Lagrange interpolation of one staggered component
- * (grid_type 0..8 = x, y, z, xx, yy, zz, xy, xz, yz) on one grid block
+ * (grid_type 0..9 = x, y, z, xx, yy, zz, xy, xz, yz, material node) on one grid block
  * (source.c:137-400).  They return 0 or the reference's error code. */
 int awp_input_read(const char* path, long long hdr[8], char* file, int filecap, float* x,
                    float* y, float* z, int* type, long long cap);
@@ -367,6 +395,17 @@ int awp_field_device_ptr(awp_ctx* ctx, int field, float** dev_ptr);
 int awp_gather_output(awp_ctx* ctx, int nbgx, int nedx, int nskpx, int nbgy,
                       int nedy, int nskpy, int nbgz, int nedz, int nskpz,
                       float* bufx, float* bufy, float* bufz, float* bufeta);
+
+/* FOLLOWBATHY=1 (pmcl3d.c:905-930, kernel.cu:3975-3983): the surface level of
+ * every padded (i, j) column of grid 0, int[ny+4+2*ngsl][nx+4+2*ngsl] (x
+ * fastest).  awp_compute_bathymetry fills it from the context's media as
+ * pmcl3d does (the highest level k > align, from the top down, whose
+ * sqrt(1/(mu*d1)) exceeds 0.001; 0 where none does); awp_set_bathymetry makes
+ * awp_gather_output on this grid read level bathy-k of each column (w one cell
+ * lower where the level is the top one), or clears it with NULL.  A gather
+ * whose depth reaches below level 0 of a recorded column is refused. */
+int awp_compute_bathymetry(awp_ctx* ctx, int* bathy);
+int awp_set_bathymetry(awp_ctx* ctx, const int* bathy);
 
 /* Device-side non-finite sentinel over velocities and stresses: *ok = 1 when
  * every value is finite. */

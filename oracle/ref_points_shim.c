@@ -2,7 +2,8 @@
  * Test infrastructure only: drives the reference's own point-set device code
  * (src/interpolation/interpolation.cu: cuinterp_init / cuinterp_interp_H, the
  * receiver gather; src/topography/sources/source.cu: cusource_add_cartesian_H,
- * the SOURCEFILE add) on caller device buffers, for GPU parity checks.  Built
+ * the SOURCEFILE add, and cusource_add_force_H, the FORCEFILE add) on caller
+ * device buffers, for GPU parity checks.  Built
  * into oracle/_ref/libawpref_points.so by oracle/Makefile from the reference
  * sources where they lie.
  *
@@ -142,6 +143,16 @@ void ref_pts_srcadd_curv(void *h, float *d_field, const float *d_values, float h
                          const float *d_f, int ny, const float *d_dg) {
   ref_pts_t *p = (ref_pts_t *)h;
   cusource_add_curvilinear_H(&p->I, d_field, d_values, hh, dt, d_f, ny, d_dg);
+}
+
+/* cusource_add_force_H (FORCEFILE, forces.c:74-94): the force rate into a
+ * velocity component, scaled by -quad_weight / (f dg rho). */
+void ref_pts_force(void *h, float *d_field, const float *d_values, const float *d_d1, float hh,
+                   float dt, float quad_weight, const float *d_f, int nx, int ny, int nz,
+                   const float *d_dg) {
+  ref_pts_t *p = (ref_pts_t *)h;
+  cusource_add_force_H(&p->I, d_field, d_values, d_d1, hh, dt, quad_weight, d_f, nx, ny, nz,
+                       d_dg);
 }
 
 void ref_pts_destroy(void *h) {

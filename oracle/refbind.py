@@ -347,6 +347,9 @@ class RefPoints:
                                                 c_void_p, c_int, c_void_p]
             lib.ref_pts_interp.argtypes = [c_void_p, c_void_p, c_void_p]
             lib.ref_pts_srcadd.argtypes = [c_void_p, c_void_p, c_void_p, c_float, c_float]
+            lib.ref_pts_force.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p, c_float,
+                                          c_float, c_float, c_void_p, c_int, c_int, c_int,
+                                          c_void_p]
             lib.ref_pts_destroy.argtypes = [c_void_p]
             cls._lib = lib
         return cls._lib
@@ -376,6 +379,13 @@ class RefPoints:
     def srcadd_curv(self, d_field_ptr, d_values_ptr, h, dt, d_f_ptr, d_dg_ptr):
         self.lib().ref_pts_srcadd_curv(self.h, c_void_p(d_field_ptr), c_void_p(d_values_ptr), h,
                                        dt, c_void_p(d_f_ptr), self.ny, c_void_p(d_dg_ptr))
+
+    def force(self, d_field_ptr, d_values_ptr, d_d1_ptr, h, dt, quad_weight, d_f_ptr, nx, nz,
+              d_dg_ptr):
+        """cusource_add_force_H on a velocity component (forces.c:74-94)."""
+        self.lib().ref_pts_force(self.h, c_void_p(d_field_ptr), c_void_p(d_values_ptr),
+                                 c_void_p(d_d1_ptr), h, dt, quad_weight, c_void_p(d_f_ptr), nx,
+                                 self.ny, nz, c_void_p(d_dg_ptr))
 
     def close(self):
         if self.h:

@@ -55,8 +55,9 @@ def write_block(scn, d, p):
             np.asarray(scn.src_data[s], np.float32).tofile(fh)
 
 
-def velbuffer_frames(lib, sims, axes, nt, ntiskp):
-    """Per grid, the reference's velbuffer_H gathered every ntiskp steps."""
+def velbuffer_frames(lib, sims, axes, nt, ntiskp, bathy=None):
+    """Per grid, the reference's velbuffer_H gathered every ntiskp steps
+    (FOLLOWBATHY=1 on grid 0 with `bathy`, a device int32 tensor)."""
     V = c_void_p
     lib.velbuffer_H.argtypes = [V] * 8 + [c_int] * 13 + [V, c_int, V, c_int]
     frames = {p: {c: [] for c in "XYZ"} for p in axes}
@@ -69,7 +70,10 @@ def velbuffer_frames(lib, sims, axes, nt, ntiskp):
             bufs = [torch.zeros(rec, device="cuda") for _ in range(4)]
             lib.velbuffer_H(*[c_void_p(sim.f[f].data_ptr()) for f in ("u1", "v1", "w1", "neta")],
                             *[c_void_p(b.data_ptr()) for b in bufs], 1, bx, ex, sx, by, ey, sy,
-                            bz, ez, sz, nxr, nyr, nzr, None, 0, None, p)
+                            bz, ez, sz, nxr, nyr, nzr, None,
+                            1 if (bathy is not None and p == 0) else 0,
+                            c_void_p(bathy.data_ptr()) if (bathy is not None and p == 0)
+                            else None, p)
             torch.cuda.synchronize()
             for c, b in zip("XYZ", bufs):
                 frames[p][c].append(b.cpu().numpy().reshape(nzr, nyr, nxr))
@@ -176,3 +180,61 @@ def test_two_block_mesh_run_matches_reference(tmp_path):
     compare_files(os.path.join(tmp_path, "out"), frames, axes, full, nt, ntiskp, wstep)
     chk = open(os.path.join(tmp_path, "chk")).read()
     assert chk.count("GRID NUMBER:") == 2 and chk.strip().endswith("END")
+
+
+def reference_bathymetry(mu, d1):
+    """pmcl3d.c:909-925 restated: per padded column the highest level
+    k > align from the top down with sqrt(1/(mu*d1)) > 0.001 (float product,
+    double reciprocal and root, float compare), 0 where none; [j][i]."""
+    align = refbind.ALIGN
+    nxp, nyp, nzp = mu.shape
+    top = nzp - align - 1
+    out = np.zeros((nyp, nxp), np.int32)
+    vs = np.sqrt(1.0 / (mu * d1).astype(np.float64)).astype(np.float32)
+    for k in range(top, align, -1):
+        hit = (vs[:, :, k] > np.float32(0.001)).T & (out == 0)
+        out[hit] = k
+    return out
+
+
+def test_followbathy_output_matches_reference(tmp_path):
+    """FOLLOWBATHY=1: a near-fluid top layer (vs 0.5 mm/s, three cells thick)
+    over half of the surface; the driver's output files against the
+    reference's velbuffer_H with the surface levels pmcl3d derives, and the
+    library's levels against that derivation."""
+    nt, ntiskp, wstep = 32, 2, 4
+    scn = scenarios.random_small(nx=24, ny=20, nz=32, steps=nt, seed=29, ifault=1, nsrc=2)
+    p = scn.params
+    scn.media[:3, :, : p["nx"] // 2, 1] = 0.0005
+    write_block(scn, tmp_path, 0)
+    tmax = (nt - 1) * p["dt"] + p["dt"] * 0.5
+    r = run_driver(["-X", p["nx"], "-Y", p["ny"], "-Z", p["nz"], "-H", p["dh"], "-t", p["dt"],
+                    "-T", tmax, "-D", p["nd"], "-A", p["arbc"], "-V", 1, "-B", 1, "-n", 5,
+                    "-I", 1, "-S", scn.src_pos.shape[0], "-N", p["nst"], "-R", p["nst"],
+                    "--INVEL", "media", "--INSRC", "src", "-o", "out", "-c", "chk", "-r",
+                    ntiskp, "-W", wstep, "--NBGX", 1, "--NEDX", p["nx"], "--NSKPX", 1,
+                    "--NBGY", 1, "--NEDY", p["ny"], "--NSKPY", 1, "--NBGZ", 1, "--NEDZ", 3,
+                    "--NSKPZ", 1, "--FOLLOWBATHY", 1], tmp_path)
+    assert os.path.getsize(os.path.join(tmp_path, "debug", "bathy.0000")) > 0, r.stdout
+    ax = (recording(p["nx"], 1, p["nx"], 1), recording(p["ny"], 1, p["ny"], 1),
+          recording(p["nz"], 1, 3, 1, nz_axis=True))
+    axes = {0: [a[0] for a in ax]}
+    full = {0: tuple(a[1] for a in ax)}
+    ref = refbind.RefGpuSim(scn, refbind.model_setup(scn))
+    bathy = reference_bathymetry(ref.f["mu"].cpu().numpy(), ref.f["d1"].cpu().numpy())
+    top = ref.f["mu"].shape[2] - refbind.ALIGN - 1
+    inner = bathy[refbind.NGSL + 2: refbind.NGSL + 2 + p["ny"],
+                  refbind.NGSL + 2: refbind.NGSL + 2 + p["nx"]]
+    assert (inner[:, : p["nx"] // 2] == top - 3).all() and (inner[:, p["nx"] // 2:] == top).all()
+
+    from awp_b200 import Solver, default_params
+    s = Solver(default_params(**p))
+    s.upload_media(scn.media)
+    assert np.array_equal(s.bathymetry(), bathy)
+    s.close()
+
+    dev = torch.from_numpy(bathy).cuda()
+    frames, grab = velbuffer_frames(ref.lib, [ref], axes, nt, ntiskp, bathy=dev)
+    ref.after_step.append(lambda sim, n: grab(n) if n % ntiskp == 0 else None)
+    ref.step(nt)
+    compare_files(os.path.join(tmp_path, "out"), frames, axes, full, nt, ntiskp, wstep)

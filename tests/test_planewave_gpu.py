@@ -40,10 +40,36 @@ def plane_series(nst, dt, seed=5):
 
 
 def case(steps=30, q=True, nz=32):
+    """A homogeneous medium (constant Q where q): the plane enters rows 4 .. 3 +
+    nx of the padded grid, six of them in the ghost region, where both builds
+    read the media as they are; the tests fill the whole padded arrays as
+    MEDIASTART 0 does (mesh.c:80-87).  With the ghost media left zero, as the
+    reference's inimesh leaves them for MEDIASTART >= 1 at one rank, its
+    division by mu there gives inf in both builds."""
     scn = scenarios.random_small(nx=24, ny=20, nz=nz, q=q, ifault=1, steps=steps, seed=17,
                                  nsrc=1)
+    # vp, vs, rho, then qp, qs where the run is anelastic
+    for col, v in enumerate((3400.0, 2000.0, 2500.0, 150.0, 75.0)[: 5 if q else 3]):
+        scn.media[..., col] = v
     scn.params.update(ifault=6, nst=steps, read_step=steps, nd=6)
     return scn
+
+
+def fill_padding(s, ref=None, oracle=None):
+    """The product's interior d1 / 1/mu / 1/lambda (homogeneous) over the whole
+    padded arrays, in the product, the reference binding and the oracle."""
+    full = {}
+    for f in ("d1", "mu", "lam"):
+        a = s.field(f)
+        v = a[a.shape[0] // 2, a.shape[1] // 2, a.shape[2] // 2]
+        full[f] = np.full(a.shape, v, np.float32)
+        s.set_field(f, full[f])
+        if ref is not None:
+            assert ref.f[f][a.shape[0] // 2, a.shape[1] // 2, a.shape[2] // 2].item() == v
+            ref.f[f].fill_(float(v))
+        if oracle is not None:
+            oracle.set_field(f, full[f])
+    return full
 
 
 @pytest.mark.parametrize("q", [True, False])
@@ -55,13 +81,14 @@ def test_plane_wave_matches_reference_and_oracle(q):
     setup = refbind.model_setup(scn)
     ref = refbind.RefGpuSim(scn, setup)
     ref.set_plane_wave(vx, vy, vz)
-    ref.step(steps)
     s = Solver(default_params(**p))
     s.upload_media(scn.media)
+    o = orc.OracleSim(scn, setup, 64)
+    fill_padding(s, ref, o)
+    ref.step(steps)
     s.upload_plane_wave(vx, vy, vz)
     s.step(steps)
     s.synchronize()
-    o = orc.OracleSim(scn, setup, 64)
     o.set_plane_wave(vx, vy, vz)
     o.step(steps)
     assert np.abs(ref.field("xx")).max() > 0
@@ -102,13 +129,14 @@ def test_driver_plane_wave_run(tmp_path):
     p = scn.params
     vx, vy, vz = plane_series(p["nst"], p["dt"])
     scn.media.astype(np.float32).tofile(os.path.join(tmp_path, "media_0"))
+    # nine decimals: every float32 sample reads back exactly through fscanf "%e"
     with open(os.path.join(tmp_path, "planewave.txt"), "w") as fh:
         for a, b, c in zip(vx, vy, vz):
-            fh.write(f"{a:e} {b:e} {c:e}\n")
+            fh.write(f"{a:.9e} {b:.9e} {c:.9e}\n")
     ntiskp, wstep = 2, 4
     tmax = (nt - 1) * p["dt"] + p["dt"] * 0.5
     args = ["-X", p["nx"], "-Y", p["ny"], "-Z", p["nz"], "-H", p["dh"], "-t", p["dt"],
-            "-T", tmax, "-D", p["nd"], "-A", p["arbc"], "-V", 1, "-B", 1, "-n", 5,
+            "-T", tmax, "-D", p["nd"], "-A", p["arbc"], "-V", 1, "-B", 0, "-n", 5,
             "-I", 6, "-S", 0, "-N", p["nst"], "-R", p["nst"],
             "--INVEL", "media", "--INSRC", "planewave.txt", "-o", "out", "-c", "chk",
             "-r", ntiskp, "-W", wstep, "--NBGX", 1, "--NEDX", p["nx"], "--NSKPX", 1,
@@ -120,7 +148,14 @@ def test_driver_plane_wave_run(tmp_path):
     assert "Using plane wave input" in r.stdout
     import torch
     s = Solver(default_params(**p))
-    s.upload_media(scn.media)
+    # MEDIASTART 0 (mesh.c:80-87, the driver's homogeneous fill): vp 1500, vs 500,
+    # rho 2000 over the whole padded grid
+    shape = s.field("d1").shape
+    vp, vs, dd = 1500.0, 500.0, 2000.0
+    s.set_field("d1", np.full(shape, dd, np.float32))
+    s.set_field("mu", np.full(shape, np.float32(1.0 / (dd * vs * vs)), np.float32))
+    s.set_field("lam", np.full(shape, np.float32(1.0 / (dd * (vp * vp - 2.0 * vs * vs))),
+                               np.float32))
     s.upload_plane_wave(vx, vy, vz)
     rec = p["nx"] * p["ny"]
     bufs = [torch.zeros(rec, device="cuda") for _ in range(3)]

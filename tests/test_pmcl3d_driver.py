@@ -160,3 +160,76 @@ def test_point_sets_match_library(tmp_path, topo):
     for c in "xyz":
         assert got[c].shape == (2, 12) and np.any(got[c] != 0)
         assert np.array_equal(got[c], want[c]), c
+
+
+@pytest.mark.gpu
+def test_partitioned_media_file(tmp_path):
+    """MEDIASTART=3 reads rank 0's partition, input_rst/mediapart/media0000000.bin
+    (mesh.c:138-141), with the layout of MEDIASTART 1: both runs write the same
+    surface files."""
+    scn = scenarios.random_small(nx=16, ny=16, nz=16, steps=6, seed=13, ifault=1, nsrc=1)
+    p = scn.params
+    outs = {}
+    for ms in (1, 3):
+        d = tmp_path / f"ms{ms}"
+        d.mkdir()
+        write_inputs(scn, d)
+        if ms == 3:
+            os.makedirs(d / "input_rst" / "mediapart")
+            os.rename(d / "media_0", d / "input_rst" / "mediapart" / "media0000000.bin")
+        args = ["-X", p["nx"], "-Y", p["ny"], "-Z", p["nz"], "-H", p["dh"], "-t", p["dt"],
+                "-T", 5.5 * p["dt"], "-D", p["nd"], "-V", 1, "-B", ms, "-n", 5,
+                "-I", 1, "-S", 1, "-N", p["nst"], "-R", p["nst"], "--INVEL", "media",
+                "--INSRC", "src", "-o", "out", "-c", "chk", "-r", 1, "-W", 2]
+        r = run(args, d)
+        assert r.returncode == 0, r.stderr + r.stdout
+        outs[ms] = sorted(os.listdir(d / "out"))
+        assert outs[ms]
+        for f in outs[ms]:
+            outs[(ms, f)] = np.fromfile(d / "out" / f, np.float32)
+    assert outs[1] == outs[3]
+    for f in outs[1]:
+        assert np.array_equal(outs[(1, f)], outs[(3, f)]), f
+    assert any(np.abs(outs[(1, f)]).max() > 0 for f in outs[1])
+
+
+@pytest.mark.gpu
+def test_split_sources_equal_point_sources(tmp_path):
+    """IFAULT=2 (read_src_ifault_2, source.c:15-128): the header
+    "<INSRC>_0" + rank and the READ_STEP windows "<INSRC_I2>_0" + rank +
+    "_<idx>" hold the same series as an IFAULT=1 file; both runs write the
+    same surface files bit for bit (the last window partly past NST)."""
+    scn = scenarios.random_small(nx=16, ny=16, nz=16, steps=10, seed=17, ifault=1, nsrc=3)
+    p = scn.params
+    nst, rs = p["nst"], 5
+    np_ = scn.src_pos.shape[0]
+    data = np.asarray(scn.src_data, np.float32).reshape(np_, -1, 6)[:, :nst]
+    outs = {}
+    for ifault in (1, 2):
+        d = tmp_path / f"if{ifault}"
+        d.mkdir()
+        write_inputs(scn, d)
+        if ifault == 2:
+            with open(d / "tpsrc_00000000", "wb") as fh:
+                np.array([np_, 0, 0], np.int32).tofile(fh)
+                np.asarray(scn.src_pos, np.int32).reshape(-1).tofile(fh)
+            for idx in range(1, -(-nst // rs) + 1):
+                win = np.zeros((6, rs, np_), np.float32)
+                t0 = (idx - 1) * rs
+                n = min(rs, nst - t0)
+                win[:, :n, :] = data[:, t0:t0 + n, :].transpose(2, 1, 0)
+                win.tofile(d / f"fault_0{0:07d}_{idx:03d}")
+        args = ["-X", p["nx"], "-Y", p["ny"], "-Z", p["nz"], "-H", p["dh"], "-t", p["dt"],
+                "-T", 9.5 * p["dt"], "-D", p["nd"], "-V", 1, "-B", 1, "-n", 5,
+                "-I", ifault, "-S", np_, "-N", nst, "-R", nst if ifault == 1 else rs,
+                "--INVEL", "media", "--INSRC", "src" if ifault == 1 else "tpsrc",
+                "--INSRC_I2", "fault", "-o", "out", "-c", "chk", "-r", 1, "-W", 2]
+        r = run(args, d)
+        assert r.returncode == 0, r.stderr + r.stdout
+        outs[ifault] = sorted(os.listdir(d / "out"))
+        for f in outs[ifault]:
+            outs[(ifault, f)] = np.fromfile(d / "out" / f, np.float32)
+    assert outs[1] == outs[2] and outs[1]
+    for f in outs[1]:
+        assert np.array_equal(outs[(1, f)], outs[(2, f)]), f
+    assert any(np.abs(outs[(1, f)]).max() > 0 for f in outs[1])

@@ -112,7 +112,7 @@ def random_points(rng, n, nx, ny, nz, h, surface_frac=0.3):
 
 
 @pytest.mark.parametrize("degree", [0, 1, 2, 3, 4])
-@pytest.mark.parametrize("grid_type", range(9))
+@pytest.mark.parametrize("grid_type", range(10))  # 9: the material node grid
 def test_interpolation_matches_reference(ref_host, tmp_path, degree, grid_type):
     nx, ny, nz, h = 24, 20, 32, 50.0
     rng = np.random.default_rng(100 + 10 * degree + grid_type)

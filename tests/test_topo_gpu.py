@@ -195,6 +195,94 @@ def test_sourcefile_and_receivers_match_reference(tmp_path):
     s.close()
 
 
+def test_forcefile_matches_reference(tmp_path):
+    """FORCEFILE boundary forces on the curvilinear block (forces_add,
+    forces.c:67-96; cusource_add_force, source.cu:118-157) against the
+    reference's own device code on its topography metrics, hooked after the
+    stress update as pmcl3d.c:1989-1994 places it."""
+    steps = 12
+    scn = scenarios.random_small(nx=28, ny=24, nz=32, q=True, ifault=1, steps=steps, seed=12,
+                                 nsrc=1)
+    p = scn.params
+    nx, ny, nz, h, dt = p["nx"], p["ny"], p["nz"], p["dh"], p["dt"]
+    tpath = str(tmp_path / "topo.bin")
+    hill(tpath, p)
+    gpu, cpu, nsamples, degree = 2, 3, 18, 3
+    coords = np.stack([np.array([6.2, 13.7, 17.4]) * h, np.array([7.3, 12.9, 9.6]) * h,
+                       np.zeros(3)], 1)
+    base = str(tmp_path / "force")
+    fpath = str(tmp_path / "force.txt")
+    pointfiles.write_input(fpath, base, coords, [1, 1, 1], degree=degree, gpu_buffer_size=gpu,
+                           cpu_buffer_size=cpu, steps=nsamples)
+    rng = np.random.default_rng(21)
+    rates = (rng.standard_normal((3, nsamples, 3)) * 1e9).astype(np.float32)
+    for c, name in enumerate(("fx", "fy", "fz")):
+        np.ascontiguousarray(rates[:, :, c]).tofile(f"{base}_{name}")
+
+    s = Solver(default_params(**p))
+    s.upload_media(scn.media)
+    s.upload_sources(scn.src_pos, scn.src_data)
+    with pytest.raises(RuntimeError):
+        s.forcefile(fpath)  # the topography comes first
+    s.topography(tpath)
+    s.forcefile(fpath)
+    s.step(steps)
+    s.synchronize()
+
+    setup = refbind.model_setup(scn)
+    ref = refbind.RefTopoSim(scn, setup, tpath)
+    (d_f, d_f1, d_f2, d_fc, d_g3, d_g3c), _ = ref.metric_ptrs()
+    fnorm = metrics_f(tpath, nx, ny, nz, h)
+    fpts = {c: refbind.RefPoints(fpath, GT[c], nx, ny, nz, h, ftopo=fnorm) for c in "xyz"}
+    host = refbind.RefHost()
+    own = {c: torch.as_tensor(host.point_coefs(fpath, GT[c], nx, ny, nz, h)["indices"],
+                              device="cuda").long() for c in "xyz"}
+    assert all(len(v) == 3 for v in own.values())
+    dev_rates = torch.from_numpy(rates).cuda()
+    fld = {"x": "u1", "y": "v1", "z": "w1"}
+    # forces.c:84-96: metric and SBP weight per component
+    met = {"x": (d_f1, d_g3c, 2.9022824945274315), "y": (d_f2, d_g3c, 2.9022824945274315),
+           "z": (d_fc, d_g3, 3.55599789310935)}
+
+    def add(sim, step):
+        for ci, c in enumerate("xyz"):
+            v = dev_rates[own[c], step, ci].contiguous()
+            fm, dg, q = met[c]
+            fpts[c].force(sim.f[fld[c]].data_ptr(), v.data_ptr(), sim.f["d1"].data_ptr(), h, dt,
+                          q, fm, nx, nz, dg)
+
+    ref.after_stress.append(add)
+    ref.step(steps)
+    assert float(torch.abs(ref.f["w1"]).max()) > 0
+    rep = {}
+    for f in FIELDS:
+        rep[f] = rel_l2(s.field(f), ref.field(f))
+        assert rep[f] <= REL_REF, (f, rep[f])
+    print("\nFORCEFILE rel L2 vs reference build:", {k: f"{v:.1e}" for k, v in rep.items()})
+    for rp in fpts.values():
+        rp.close()
+    ref.close()
+    s.close()
+
+
+def test_forcefile_rules(tmp_path):
+    """Volume (type 0) points are refused as forces_boundary_check refuses them."""
+    scn = scenarios.random_small(nx=28, ny=24, nz=32, q=False, ifault=1, steps=4, seed=3,
+                                 nsrc=1)
+    p = scn.params
+    tpath = str(tmp_path / "topo.bin")
+    hill(tpath, p)
+    coords = np.array([[6.2 * p["dh"], 7.3 * p["dh"], -2.0 * p["dh"]]])
+    fpath = str(tmp_path / "force.txt")
+    pointfiles.write_input(fpath, str(tmp_path / "force"), coords, [0], degree=1, steps=4)
+    s = Solver(default_params(**p))
+    s.upload_media(scn.media)
+    s.topography(tpath)
+    with pytest.raises(RuntimeError, match="boundary"):
+        s.forcefile(fpath)
+    s.close()
+
+
 def metrics_f(path, nx, ny, nz, h):
     """The normalised surface function of the product's metric set-up (pinned
     bit for bit to the reference's host code by the CPU tests)."""
