@@ -8,7 +8,7 @@ from __future__ import annotations
 
 import ctypes
 import os
-from ctypes import POINTER, c_char_p, c_double, c_float, c_int, c_longlong, c_void_p
+from ctypes import CFUNCTYPE, POINTER, c_char_p, c_double, c_float, c_int, c_longlong, c_void_p
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "lib", "libawpb200.so")
@@ -32,6 +32,10 @@ FIELDS = ["u1", "v1", "w1", "xx", "yy", "zz", "xy", "xz", "yz",
           "sigma2", "cohes", "phi", "yldfac", "neta"]
 FIELD_ID = {n: i for i, n in enumerate(FIELDS)}
 
+
+# int (*)(void* user, int first, int n, float* vx, float* vy, float* vz)
+FRAME_READER = CFUNCTYPE(c_int, c_void_p, c_int, c_int, POINTER(c_float), POINTER(c_float),
+                         POINTER(c_float))
 
 class AwpError(RuntimeError):
     """A non-zero status returned by the library."""
@@ -132,6 +136,8 @@ def load() -> ctypes.CDLL:
     _sig(lib, "awp_receivers_count", c_int, [_P, _I])
     _sig(lib, "awp_sourcefile_init", c_int, [_P, c_char_p])
     _sig(lib, "awp_forcefile_init", c_int, [_P, c_char_p])
+    _sig(lib, "awp_velocity_forcing_init", c_int,
+         [_P, c_int, _I, c_int, c_int, c_int, FRAME_READER, c_void_p])
     _sig(lib, "awp_topo_metrics", c_int, [c_char_p, c_int, c_int, c_int, c_float, _F])
     _sig(lib, "awp_topography_init", c_int, [_P, c_char_p])
     _sig(lib, "awp_set_topo_plasticity", c_int, [_P, c_int])
@@ -201,6 +207,7 @@ def declared_symbols(header: str | None = None) -> list[str]:
     header = header or os.path.join(HERE, "..", "include", "awp_b200.h")
     text = open(header).read()
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    text = re.sub(r"\btypedef\b[^;]*;", "", text)  # callback types declare no symbol
     names = re.findall(r"\b([A-Za-z_][A-Za-z0-9_]*)\s*\(", text)
     skip = {"if", "for", "while", "return", "sizeof", "defined"}
     out = []

@@ -79,6 +79,17 @@ struct awp_ctx {
   double* d_filt = nullptr;
   float* d_plane[3] = {};  // IFAULT 6 plane-wave series (x, y, z), plane_n samples each
   int plane_n = 0;
+  // IFAULT 4: velocities prescribed at points (frcvel_cu), windows of frc_w
+  // frames with one carry slot in front (pmcl3d.c:714-722, 792-805, 1821-1826)
+  int frc_n = 0, frc_frames = 0, frc_tskp = 1, frc_w = 0, frc_next = 0;
+  long long frc_s = 0;  // source_step of pmcl3d
+  int* d_frc_pos = nullptr;
+  float* d_frc[3] = {};
+  float* h_frc = nullptr;  // pinned staging of one window, 3 * frc_w * frc_n
+  cudaEvent_t frc_h2d = nullptr;
+  bool frc_pending = false;
+  awp_frame_reader frc_read = nullptr;
+  void* frc_user = nullptr;
   // FOLLOWBATHY surface level per padded (i, j) column, [j][i] (pmcl3d.c:905-930)
   int* d_bathy = nullptr;
   std::vector<int> bathy;
@@ -543,15 +554,80 @@ int phase_receivers(awp_ctx* c) {
   return sgt_record(c);  // pmcl3d.c:2248-2249
 }
 
+// IFAULT 4: the next window of frames from the caller's reader into slots
+// 1..frc_w of the device arrays (read_src_ifault_4 + Cpy2Device_source,
+// source.c:469-680, swap.c:323-353); slot 0 carries the last frame of the
+// window before, which frcvel_cu itself moves there.
+int frc_fill(awp_ctx* c) {
+  if (c->frc_pending) {  // the staging buffer of the window before has been copied
+    CU_TRY(cudaEventSynchronize(c->frc_h2d));
+    c->frc_pending = false;
+  }
+  const size_t n = (size_t)c->frc_w * c->frc_n;
+  float* h = c->h_frc;
+  const int first = c->frc_next * c->frc_w;
+  const int r = c->frc_read(c->frc_user, first, c->frc_w, h, h + n, h + 2 * n);
+  if (r) return set_error(AWP_ERR_IO, "velocity frame reader failed on frames %d..%d (%d)", first,
+                          first + c->frc_w - 1, r);
+  for (int q = 0; q < 3; ++q)
+    CU_TRY(cudaMemcpyAsync(c->d_frc[q] + c->frc_n, h + (size_t)q * n, n * sizeof(float),
+                           cudaMemcpyHostToDevice, c->stream));
+  CU_TRY(cudaEventRecord(c->frc_h2d, c->stream));
+  c->frc_pending = true;
+  c->frc_next++;
+  return AWP_OK;
+}
+
+// frcvel_H on grid 0 after the velocity update and its mesh coupling
+// (pmcl3d.c:1821-1826): the step counter advances, then the kernel sets (or,
+// past the last frame, pushes) the velocities at the points.
+int phase_forcing(awp_ctx* c) {
+  if (!c->d_frc_pos) return AWP_OK;
+  PhaseScope ps(c, 2);
+  c->frc_s += 1;
+  FrcvelArgs a;
+  memset(&a, 0, sizeof(a));
+  a.i = (int)c->frc_s;
+  a.read_step = c->frc_w;
+  a.dim = 3;
+  a.npsrc = c->frc_n;
+  a.tskp = c->frc_tskp;
+  a.xmin = -1;
+  a.xmax = -1;
+  a.psrc = c->d_frc_pos;
+  a.axx = c->d_frc[0]; a.ayy = c->d_frc[1]; a.azz = c->d_frc[2];
+  a.u1 = c->f[AWP_U1]; a.v1 = c->f[AWP_V1]; a.w1 = c->f[AWP_W1];
+  a.slice = c->g.slice; a.yline = c->g.yline;
+  a.DT = c->p.dt;
+  CU_TRY(awp_launch_frcvel(a, c->stream));
+  c->launches++;
+  return AWP_OK;
+}
+
+// End of a step: a new window every frc_w * tskp steps while frames remain,
+// and the step counter restarts (pmcl3d.c:2442-2486).
+int phase_forcing_window(awp_ctx* c) {
+  if (!c->d_frc_pos) return AWP_OK;
+  const long long cs = c->cur_step, wt = (long long)c->frc_w * c->frc_tskp;
+  if (cs < (long long)c->frc_frames * c->frc_tskp - 1 && (cs + 1) % wt == 0) {
+    const int st = frc_fill(c);
+    if (st) return st;
+    c->frc_s = 0;
+  }
+  return AWP_OK;
+}
+
 int one_step(awp_ctx* c) {
   int st;
   if ((st = phase_begin(c))) return st;
   if ((st = phase_velocity(c))) return st;
+  if ((st = phase_forcing(c))) return st;
   if ((st = phase_stress(c))) return st;
   if ((st = phase_sources(c))) return st;
   if ((st = phase_plasticity(c))) return st;
   if ((st = phase_fstr(c))) return st;
-  return phase_receivers(c);
+  if ((st = phase_receivers(c))) return st;
+  return phase_forcing_window(c);
 }
 
 }  // namespace
@@ -670,6 +746,7 @@ int mesh_step(awp_mesh* m) {
   for (int p = 0; p < n - 1; ++p)
     if ((st = dm_velocity(g[p]))) return st;
   if ((st = dm_interfaces(g, n, m->stream))) return st;
+  if ((st = phase_forcing(g[0]))) return st;
   for (int p = 0; p < n; ++p)
     if ((st = phase_stress(g[p]))) return st;
   for (int p = 0; p < n - 1; ++p)
@@ -682,7 +759,7 @@ int mesh_step(awp_mesh* m) {
   if ((st = phase_fstr(g[0]))) return st;
   for (int p = 0; p < n; ++p)
     if ((st = phase_receivers(g[p]))) return st;
-  return AWP_OK;
+  return phase_forcing_window(g[0]);
 }
 
 }  // namespace
@@ -738,6 +815,10 @@ int awp_ctx_destroy(awp_ctx* c) {
   cudaFree(c->d_mom); cudaFree(c->d_filt); cudaFree(c->d_neta_mult); cudaFree(c->d_flag);
   for (int q = 0; q < 3; ++q) cudaFree(c->d_plane[q]);
   cudaFree(c->d_bathy);
+  cudaFree(c->d_frc_pos);
+  for (int q = 0; q < 3; ++q) cudaFree(c->d_frc[q]);
+  if (c->h_frc) cudaFreeHost(c->h_frc);
+  if (c->frc_h2d) cudaEventDestroy(c->frc_h2d);
   cudaFree(c->d_ext);
   cudaFree(c->d_err);
   for (auto& e : c->ev_used) { cudaEventDestroy(e.a); cudaEventDestroy(e.b); }
@@ -763,7 +844,7 @@ int awp_ctx_create(const awp_params* p, awp_ctx** out) {
                      "NVE=%d: the time loop runs only for NVE 1 or 3 (pmcl3d.c:1624)", p->nve);
   if (p->npc != 0 && p->npc != 2)
     return set_error(AWP_ERR_UNSUPPORTED, "NPC=%d (only 0 and 2 run the loop)", p->npc);
-  if (p->ifault != 1 && p->ifault != 2 && p->ifault != 5 && p->ifault != 0 && p->ifault != 6)
+  if (p->ifault < 0 || p->ifault > 6 || p->ifault == 3)
     return set_error(AWP_ERR_UNSUPPORTED, "IFAULT=%d", p->ifault);
   const long long cells = (long long)(p->nx + 20) * (p->ny + 20) * (p->nz + 64);
   if (cells >= (1LL << 31))
@@ -1240,6 +1321,47 @@ int awp_gather_output(awp_ctx* c, int nbgx, int nedx, int nskpx, int nbgy, int n
   return AWP_OK;
 }
 
+int awp_velocity_forcing_init(awp_ctx* c, int npsrc, const int* pos, int nframes, int tskp,
+                              int window, awp_frame_reader read, void* user) {
+  if (!c || !pos || !read) return set_error(AWP_ERR_ARG, "null argument");
+  if (c->p.ifault != 4) return set_error(AWP_ERR_STATE, "the context runs IFAULT=%d, not 4", c->p.ifault);
+  if (c->p.grid != 0) return set_error(AWP_ERR_STATE, "frcvel acts on grid 0 (pmcl3d.c:1821)");
+  if (c->d_frc_pos) return set_error(AWP_ERR_STATE, "velocity forcing already initialised");
+  if (c->cur_step != 0) return set_error(AWP_ERR_STATE, "velocity forcing before the first step");
+  if (npsrc < 1 || tskp < 1 || window < 1 || nframes < window || nframes % window)
+    return set_error(AWP_ERR_ARG,
+                     "npsrc, tskp, window >= 1 and frames a multiple of the window required "
+                     "(%d points, tskp %d, %d frames, window %d)", npsrc, tskp, nframes, window);
+  // frcvel_cu's cell of a point: (x + 1 + ngsl, y + 1 + ngsl, z + align - 1)
+  for (int j = 0; j < npsrc; ++j) {
+    const long long ix = pos[3 * j] + 1 + AWP_NGSL, iy = pos[3 * j + 1] + 1 + AWP_NGSL,
+                    iz = pos[3 * j + 2] + AWP_ALIGN - 1;
+    if (ix < 0 || ix >= c->g.nx_pad() || iy < 0 || iy >= c->g.ny_pad() || iz < 0 ||
+        iz >= c->g.yline)
+      return set_error(AWP_ERR_ARG, "point %d (%d, %d, %d) lies outside the padded grid", j,
+                       pos[3 * j], pos[3 * j + 1], pos[3 * j + 2]);
+  }
+  int st;
+  const size_t slots = (size_t)(window + 1) * npsrc;
+  if ((st = ctx_alloc(c, (void**)&c->d_frc_pos, (size_t)npsrc * 3 * sizeof(int)))) return st;
+  CU_TRY(cudaMemcpy(c->d_frc_pos, pos, (size_t)npsrc * 3 * sizeof(int), cudaMemcpyHostToDevice));
+  for (int q = 0; q < 3; ++q) {
+    if ((st = ctx_alloc(c, (void**)&c->d_frc[q], slots * sizeof(float)))) return st;
+    CU_TRY(cudaMemset(c->d_frc[q], 0, slots * sizeof(float)));  // carry slot of window 1: zero
+  }
+  CU_TRY(cudaMallocHost((void**)&c->h_frc, 3 * (size_t)window * npsrc * sizeof(float)));
+  CU_TRY(cudaEventCreateWithFlags(&c->frc_h2d, cudaEventDisableTiming));
+  c->frc_n = npsrc;
+  c->frc_frames = nframes;
+  c->frc_tskp = tskp;
+  c->frc_w = window;
+  c->frc_next = 0;
+  c->frc_read = read;
+  c->frc_user = user;
+  c->frc_s = 1;  // source_step before the loop (pmcl3d.c:1175)
+  return frc_fill(c);
+}
+
 int awp_compute_bathymetry(awp_ctx* c, int* bathy) {
   if (!c || !bathy) return set_error(AWP_ERR_ARG, "null argument");
   if (!c->media_ready) return set_error(AWP_ERR_STATE, "media not uploaded");
@@ -1270,6 +1392,10 @@ int awp_compute_bathymetry(awp_ctx* c, int* bathy) {
 int awp_set_bathymetry(awp_ctx* c, const int* bathy) {
   if (!c) return set_error(AWP_ERR_ARG, "null context");
   cudaFree(c->d_bathy);
+  cudaFree(c->d_frc_pos);
+  for (int q = 0; q < 3; ++q) cudaFree(c->d_frc[q]);
+  if (c->h_frc) cudaFreeHost(c->h_frc);
+  if (c->frc_h2d) cudaEventDestroy(c->frc_h2d);
   c->d_bathy = nullptr;
   c->bathy.clear();
   if (!bathy) return AWP_OK;
@@ -1781,10 +1907,11 @@ int awp_batch_create(awp_ctx* const* ctxs, int n, awp_batch** out) {
     if (!c) return set_error(AWP_ERR_ARG, "instance %d is null", q);
     if (!c->media_ready) return set_error(AWP_ERR_STATE, "instance %d: media not uploaded", q);
     if (c->p.ngrids != 1 || c->p.nve == 3 || c->topo || c->recv || c->srcf || c->forcef ||
-        c->sgt || c->p.ifault == 6)
+        c->sgt || c->p.ifault == 6 || c->p.ifault == 4)
       return set_error(AWP_ERR_UNSUPPORTED,
                        "instance %d: a batch holds single-grid Cartesian runs without "
-                       "plasticity, receivers, SOURCEFILE or plane-wave sources", q);
+                       "plasticity, receivers, SOURCEFILE, plane-wave or prescribed-velocity "
+                       "sources", q);
     if (c->cur_step != ctxs[0]->cur_step)
       return set_error(AWP_ERR_STATE, "instances must start at the same step");
     for (int r = 0; r < q; ++r)
@@ -2040,6 +2167,8 @@ int check_adjoint_ctx(awp_ctx* c) {
     return set_error(AWP_ERR_UNSUPPORTED,
                      "the adjoint covers single-grid Cartesian runs without plasticity, "
                      "receiver or SGT files or SOURCEFILE sources");
+  if (c->d_frc_pos)
+    return set_error(AWP_ERR_UNSUPPORTED, "the adjoint does not cover prescribed velocities");
   if (c->ncell > 0 && c->p.ifault != 1 && c->p.ifault != 2)
     return set_error(AWP_ERR_UNSUPPORTED,
                      "the adjoint takes IFAULT 1 or 2 sources (the kinematic source depends on "

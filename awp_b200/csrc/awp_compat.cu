@@ -134,60 +134,6 @@ void single_rank_only(int rank_a, int rank_b, const char* func) {
   check(cudaErrorNotSupported, func);
 }
 
-// frcvel_cu (kernel.cu:1836-1934): prescribed velocities at the source points
-// (IFAULT 4), linearly interpolated between input samples tskp steps apart;
-// on the last prescribed step the restoring force is stored in the source
-// arrays and applied on every later step.  One thread per source point.
-struct FrcvelArgs {
-  int i, read_step, dim, npsrc, tskp, xmin, xmax;
-  const int* psrc;
-  float *axx, *ayy, *azz, *u1, *v1, *w1;
-  int slice, yline;
-  float DT;
-};
-
-__global__ void k_frcvel(const FrcvelArgs a) {
-  const int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= a.npsrc) return;
-  const int i = a.i - 1;
-  const float ts = (float)a.tskp;
-  int i0 = (int)((float)a.tskp * floorf((float)((double)i + 1.0) / ts));
-  int i1 = (int)((float)a.tskp * ceilf((float)((double)i + 1.0) / ts));
-  const float pfact = (float)(i + 1 - i0) / ts;
-  i0 /= a.tskp;
-  i1 /= a.tskp;
-  const int idx = a.psrc[j * a.dim] + 1 + AWP_NGSL;
-  const int idy = a.psrc[j * a.dim + 1] + 1 + AWP_NGSL;
-  const int idz = a.psrc[j * a.dim + 2] + AWP_ALIGN - 1;
-  const long long pos = (long long)idx * a.slice + (long long)idy * a.yline + idz;
-  const bool above = (a.xmin == -1) || (idx >= a.xmin);
-  const bool below = (a.xmax == -1) || (idx <= a.xmax);
-  if (!(above && below)) return;
-  const int n = a.npsrc;
-  if (i < a.read_step * a.tskp) {
-    const float up = a.axx[i0 * n + j], vp = a.ayy[i0 * n + j], wp = a.azz[i0 * n + j];
-    const float un = a.axx[i1 * n + j], vn = a.ayy[i1 * n + j], wn = a.azz[i1 * n + j];
-    const float ui = __fmaf_rn(__fsub_rn(un, up), pfact, up);
-    const float vi = __fmaf_rn(__fsub_rn(vn, vp), pfact, vp);
-    const float wi = __fmaf_rn(__fsub_rn(wn, wp), pfact, wp);
-    if (i == a.read_step * a.tskp - 1) {
-      a.axx[j] = a.axx[i1 * n + j];
-      a.ayy[j] = a.ayy[i1 * n + j];
-      a.azz[j] = a.azz[i1 * n + j];
-      a.axx[i1 * n + j] = (un - a.u1[pos]) / a.DT;
-      a.ayy[i1 * n + j] = (vn - a.v1[pos]) / a.DT;
-      a.azz[i1 * n + j] = (wn - a.w1[pos]) / a.DT;
-    }
-    a.u1[pos] = ui;
-    a.v1[pos] = vi;
-    a.w1[pos] = wi;
-  } else {
-    a.u1[pos] = __fmaf_rn(a.axx[a.read_step * n + j], a.DT, a.u1[pos]);
-    a.v1[pos] = __fmaf_rn(a.ayy[a.read_step * n + j], a.DT, a.v1[pos]);
-    a.w1[pos] = __fmaf_rn(a.azz[a.read_step * n + j], a.DT, a.w1[pos]);
-  }
-}
-
 // fvel (kernel.cu:1949-2033): free-surface velocity images at k = top + 1 of
 // grid 0 from the velocities at and below the surface.  Every (i, j) of the
 // launch reads only levels top and top - 1, so the reference's sequential
@@ -535,8 +481,7 @@ void frcvel_H(int i, int READ_STEP, int dim, int* psrc, int npsrc, int tskp, awp
   a.axx = axx; a.ayy = ayy; a.azz = azz; a.u1 = u1; a.v1 = v1; a.w1 = w1;
   a.slice = gc.slice; a.yline = gc.yline;
   a.DT = s.DT;
-  k_frcvel<<<cdiv(npsrc, 256), 256, 0, St>>>(a);
-  check(cudaGetLastError(), "frcvel_H");
+  check(awp_launch_frcvel(a, St), "frcvel_H");
 }
 
 void addplanesrc_H(int i, int dim, int NST, awp_stream_t St, float* mu, float* lambda, int ND,

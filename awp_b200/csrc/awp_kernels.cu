@@ -1070,6 +1070,54 @@ cudaError_t awp_launch_addsrc(const SrcArgs& a, cudaStream_t st) {
   return cudaGetLastError();
 }
 
+__global__ void k_frcvel(const FrcvelArgs a) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= a.npsrc) return;
+  const int i = a.i - 1;
+  const float ts = (float)a.tskp;
+  int i0 = (int)((float)a.tskp * floorf((float)((double)i + 1.0) / ts));
+  int i1 = (int)((float)a.tskp * ceilf((float)((double)i + 1.0) / ts));
+  const float pfact = (float)(i + 1 - i0) / ts;
+  i0 /= a.tskp;
+  i1 /= a.tskp;
+  const int idx = a.psrc[j * a.dim] + 1 + AWP_NGSL;
+  const int idy = a.psrc[j * a.dim + 1] + 1 + AWP_NGSL;
+  const int idz = a.psrc[j * a.dim + 2] + AWP_ALIGN - 1;
+  const long long pos = (long long)idx * a.slice + (long long)idy * a.yline + idz;
+  const bool above = (a.xmin == -1) || (idx >= a.xmin);
+  const bool below = (a.xmax == -1) || (idx <= a.xmax);
+  if (!(above && below)) return;
+  const int n = a.npsrc;
+  if (i < a.read_step * a.tskp) {
+    const float up = a.axx[i0 * n + j], vp = a.ayy[i0 * n + j], wp = a.azz[i0 * n + j];
+    const float un = a.axx[i1 * n + j], vn = a.ayy[i1 * n + j], wn = a.azz[i1 * n + j];
+    const float ui = __fmaf_rn(__fsub_rn(un, up), pfact, up);
+    const float vi = __fmaf_rn(__fsub_rn(vn, vp), pfact, vp);
+    const float wi = __fmaf_rn(__fsub_rn(wn, wp), pfact, wp);
+    if (i == a.read_step * a.tskp - 1) {
+      a.axx[j] = a.axx[i1 * n + j];
+      a.ayy[j] = a.ayy[i1 * n + j];
+      a.azz[j] = a.azz[i1 * n + j];
+      a.axx[i1 * n + j] = (un - a.u1[pos]) / a.DT;
+      a.ayy[i1 * n + j] = (vn - a.v1[pos]) / a.DT;
+      a.azz[i1 * n + j] = (wn - a.w1[pos]) / a.DT;
+    }
+    a.u1[pos] = ui;
+    a.v1[pos] = vi;
+    a.w1[pos] = wi;
+  } else {
+    a.u1[pos] = __fmaf_rn(a.axx[a.read_step * n + j], a.DT, a.u1[pos]);
+    a.v1[pos] = __fmaf_rn(a.ayy[a.read_step * n + j], a.DT, a.v1[pos]);
+    a.w1[pos] = __fmaf_rn(a.azz[a.read_step * n + j], a.DT, a.w1[pos]);
+  }
+}
+
+cudaError_t awp_launch_frcvel(const FrcvelArgs& a, cudaStream_t st) {
+  if (a.npsrc <= 0) return cudaSuccess;
+  k_frcvel<<<cdiv_u(a.npsrc, 256), 256, 0, st>>>(a);
+  return cudaGetLastError();
+}
+
 cudaError_t awp_launch_planesrc(const PlaneSrcArgs& a, cudaStream_t st) {
   if (a.nx <= 0 || a.ny <= 0) return cudaSuccess;
   k_addplanesrc<<<dim3(cdiv_u(a.nx, 16), cdiv_u(a.ny, 16)), dim3(16, 16), 0, st>>>(a);

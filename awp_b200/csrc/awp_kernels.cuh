@@ -169,8 +169,21 @@ struct PlaneSrcArgs {
   float DT, DH;
 };
 
+// frcvel_cu (kernel.cu:1836-1934): prescribed velocities at the source points
+// (IFAULT 4), linearly interpolated between input samples tskp steps apart;
+// on the last prescribed step the restoring force is stored in the source
+// arrays and applied on every later step.  One thread per source point.
+struct FrcvelArgs {
+  int i, read_step, dim, npsrc, tskp, xmin, xmax;
+  const int* psrc;
+  float *axx, *ayy, *azz, *u1, *v1, *w1;
+  int slice, yline;
+  float DT;
+};
+
 // Launchers (awp_kernels.cu).  All are asynchronous on `st`.
 cudaError_t awp_launch_planesrc(const PlaneSrcArgs& a, cudaStream_t st);
+cudaError_t awp_launch_frcvel(const FrcvelArgs& a, cudaStream_t st);
 cudaError_t awp_launch_velocity(const VelArgs& a, cudaStream_t st);
 cudaError_t awp_launch_stress(const StrArgs& a, bool elastic, cudaStream_t st);
 cudaError_t awp_launch_fstr(const FstrArgs& a, cudaStream_t st);

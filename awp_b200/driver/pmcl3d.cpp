@@ -10,7 +10,7 @@
 //
 // Scope: one rank (PX = PY = 1, no I/O ranks), one grid or a discontinuous
 // mesh of NGRIDS blocks (each 3x finer than the one below, pmcl3d.c:370-378),
-// MEDIASTART 0-3, IFAULT 1, 2, 5 and 6, NVE 1 and 3, FOLLOWBATHY 0 and 1.  On a
+// MEDIASTART 0-3, IFAULT 1, 2, 4, 5 and 6, NVE 1 and 3, FOLLOWBATHY 0 and 1.  On a
 // mesh the SOURCEFILE / RECVFILE / FORCEFILE / SGTFILE point sets and the
 // topography belong to the top block (grid 0).  Anything else is reported and
 // refused.
@@ -220,6 +220,51 @@ void die(const char* what, int st) {
     if (st_) die(#call, st_);      \
   } while (0)
 
+// IFAULT 4: frames of a previous run's volume output, the sub-volume of
+// read_awp_subvolume (source.c:377-461) -- frame t of a file is nx*ny*nz
+// floats; the rows of x0..x1-1 at every (k, j), k from the bottom of the file
+// up with SEISM-IO output, else the file's k = nz-1-k walked from k1-1 down
+// to k0 -- in the order of the points of read_src_ifault_4.
+struct FrameFiles {
+  std::string name[3];
+  int dim[3];
+  int ext[6];  // global half-open extents x0 x1 y0 y1 z0 z1 in the files
+  int seismio;
+};
+
+int read_frames(void* user, int first, int n, float* vx, float* vy, float* vz) {
+  const FrameFiles& F = *(const FrameFiles*)user;
+  float* out[3] = {vx, vy, vz};
+  const long long nx = F.dim[0], ny = F.dim[1], nz = F.dim[2], nel = nx * ny * nz;
+  const int x0 = F.ext[0], x1 = F.ext[1], y0 = F.ext[2], y1 = F.ext[3], z0 = F.ext[4],
+            z1 = F.ext[5];
+  const int nx1 = x1 - x0;
+  for (int q = 0; q < 3; ++q) {
+    FILE* f = fopen(F.name[q].c_str(), "rb");
+    if (!f) {
+      fprintf(stderr, "pmcl3d: cannot open %s\n", F.name[q].c_str());
+      return 1;
+    }
+    float* o = out[q];
+    for (int t = first; t < first + n; ++t)
+      for (int kk = 0; kk < z1 - z0; ++kk) {
+        const long long kp = F.seismio ? (long long)(z0 + kk) : nz - (z1 - 1 - kk) - 1;
+        for (int j = y0; j < y1; ++j) {
+          const long long at = (long long)t * nel + kp * nx * ny + (long long)j * nx + x0;
+          if (fseeko(f, (off_t)(at * (long long)sizeof(float)), SEEK_SET) ||
+              fread(o, sizeof(float), nx1, f) != (size_t)nx1) {
+            fclose(f);
+            fprintf(stderr, "pmcl3d: %s: frame %d outside the file\n", F.name[q].c_str(), t);
+            return 2;
+          }
+          o += nx1;
+        }
+      }
+    fclose(f);
+  }
+  return 0;
+}
+
 // hoek_brown (mesh.c:1139-1176)
 void hoek_brown(float sigma_0, float sigma_ci, float GSI, float mi, float D, int tunnel,
                 float* phi, float* cohes) {
@@ -306,7 +351,7 @@ int main(int argc, char** argv) {
     if (!grid_output[p]) rnx[p] = rny[p] = rnz[p] = 0;
   }
 
-  if (A.IFAULT != 1 && A.IFAULT != 2 && A.IFAULT != 5 && A.IFAULT != 6) {
+  if (A.IFAULT != 1 && A.IFAULT != 2 && A.IFAULT != 4 && A.IFAULT != 5 && A.IFAULT != 6) {
     fprintf(stderr, "pmcl3d: IFAULT=%d sources are not part of this build\n", A.IFAULT);
     return 1;
   }
@@ -448,6 +493,78 @@ int main(int argc, char** argv) {
     }
     fclose(f);
     if (nsrc[p]) AWP(awp_upload_sources(ctx[p], nsrc[p], spos[p].data(), sdat.data()));
+  }
+  static FrameFiles frames;  // read by the library at every window
+  if (A.IFAULT == 4) {
+    // read_src_ifault_4 (source.c:469-680) at rank 0: the INSRC text gives the
+    // x, y, z extents of the prescribed volume, the dimensions of the previous
+    // run's output, the offset of this grid in it, the file mask (%c = X, Y,
+    // Z), the SEISM-IO flag and the output step of that run
+    FILE* f = fopen(A.INSRC.c_str(), "r");
+    if (!f) {
+      perror("could not open INSRC file");
+      return 1;
+    }
+    int ext[6] = {0}, dim[3] = {0}, off[3] = {0}, seismio = 0, tskp = 1;
+    char line[1024], mask[512] = "";
+    int got = 0;
+    if (fgets(line, sizeof line, f)) got += sscanf(line, "%d %d", ext, ext + 1);
+    if (fgets(line, sizeof line, f)) got += sscanf(line, "%d %d", ext + 2, ext + 3);
+    if (fgets(line, sizeof line, f)) got += sscanf(line, "%d %d", ext + 4, ext + 5);
+    if (fgets(line, sizeof line, f)) got += sscanf(line, "%d %d %d", dim, dim + 1, dim + 2);
+    if (fgets(line, sizeof line, f)) got += sscanf(line, "%d %d %d", off, off + 1, off + 2);
+    if (fgets(line, sizeof line, f)) got += sscanf(line, "%511s", mask);
+    if (fgets(line, sizeof line, f)) got += sscanf(line, "%d", &seismio);
+    if (fgets(line, sizeof line, f)) got += sscanf(line, "%d", &tskp);
+    fclose(f);
+    if (got != 15) {
+      fprintf(stderr, "pmcl3d: %s: eight lines of IFAULT=4 parameters expected\n",
+              A.INSRC.c_str());
+      return 1;
+    }
+    printf("fbc_pmask=\"%s\"\nfbc_seismio=%d\nfbc_tskp=%d\n", mask, seismio, tskp);
+    // one rank: nbx = nby = 1 - 2*loop = -1, so the local extents are the
+    // file's, clipped to the grid and its ghost cells
+    const int westm = 1 - NGSL, eastm = nxt[0] + NGSL, southm = 1 - NGSL, northm = nyt[0] + NGSL;
+    int extl[6] = {std::max(ext[0], westm), std::min(ext[1], eastm), std::max(ext[2], southm),
+                   std::min(ext[3], northm), ext[4], ext[5]};
+    long long npsrc = -1;
+    if (extl[0] < eastm && extl[1] > westm && extl[2] < northm && extl[3] > southm)
+      npsrc = (long long)(extl[1] - extl[0] + 1) * (extl[3] - extl[2] + 1) *
+              (extl[5] - extl[4] + 1);
+    printf("(0) npsrc=%lld\n", npsrc);
+    if (npsrc > 0) {
+      std::vector<int> pos;
+      pos.reserve((size_t)npsrc * 3);
+      for (int kk = 0; kk <= extl[5] - extl[4]; ++kk) {
+        const int k = seismio ? extl[5] - kk : extl[4] + kk;
+        for (int j = extl[2]; j <= extl[3]; ++j)
+          for (int i = extl[0]; i <= extl[1]; ++i) {
+            pos.push_back(i);
+            pos.push_back(j);
+            pos.push_back(nzt[0] - k + 1);
+          }
+      }
+      // background_velocity_reader (source.c:684-793): global extents
+      frames.ext[0] = extl[0] + off[0] - 1; frames.ext[1] = extl[1] + off[0];
+      frames.ext[2] = extl[2] + off[1] - 1; frames.ext[3] = extl[3] + off[1];
+      frames.ext[4] = extl[4] + off[2] - 1; frames.ext[5] = extl[5] + off[2];
+      // the mask names the component with %c (sprintf(xfile, fbc_pmask, 'X'))
+      const std::string m = mask;
+      const size_t at = m.find("%c");
+      if (at == std::string::npos || m.find('%', at + 2) != std::string::npos ||
+          m.find('%') != at) {
+        fprintf(stderr, "pmcl3d: %s: the file mask must hold one %%c\n", mask);
+        return 1;
+      }
+      for (int q = 0; q < 3; ++q) {
+        frames.name[q] = m.substr(0, at) + "XYZ"[q] + m.substr(at + 2);
+        frames.dim[q] = dim[q];
+      }
+      frames.seismio = seismio;
+      AWP(awp_velocity_forcing_init(ctx[0], (int)npsrc, pos.data(), A.NST, tskp,
+                                    A.READ_STEP_GPU, read_frames, &frames));
+    }
   }
   if (A.IFAULT == 5) printf("Using IFAULT=5: kinematic source.\n");
   if (A.IFAULT == 6) {  // ini_plane_wave (source.c:797-833): NST lines "vx vy vz"

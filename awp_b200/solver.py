@@ -221,6 +221,33 @@ class Solver:
         + <file>_<fx|fy|fz> rates); after topography()."""
         check(self.lib.awp_forcefile_init(self.ctx, forcefile.encode()), "awp_forcefile_init")
 
+    def velocity_forcing(self, pos, vx, vy, vz, tskp: int, window: int) -> None:
+        """IFAULT=4 prescribed velocities: pos int32 [npsrc][3] (read_src_ifault_4
+        positions), frames vx, vy, vz float32 [nframes][npsrc] handed to the
+        library window by window, tskp steps per frame."""
+        pos = np.ascontiguousarray(pos, np.int32).reshape(-1, 3)
+        frames = [np.ascontiguousarray(a, np.float32) for a in (vx, vy, vz)]
+        npsrc = pos.shape[0]
+        nframes = frames[0].shape[0]
+        for a in frames:
+            assert a.shape == (nframes, npsrc), (a.shape, nframes, npsrc)
+
+        def read(_user, first, n, px, py, pz):
+            try:
+                for a, ptr in zip(frames, (px, py, pz)):
+                    dst = np.ctypeslib.as_array(ptr, shape=(n * npsrc,))
+                    dst[:] = a[first:first + n].reshape(-1)
+                return 0
+            except Exception:  # noqa: BLE001 - reported to the library as a status
+                return 1
+
+        self._frame_reader = _lib.FRAME_READER(read)  # kept alive with the context
+        self._frames = (pos, frames)
+        check(self.lib.awp_velocity_forcing_init(self.ctx, npsrc,
+                                                 pos.ctypes.data_as(POINTER(c_int)), nframes,
+                                                 int(tskp), int(window), self._frame_reader,
+                                                 None), "awp_velocity_forcing_init")
+
     # -- time stepping -----------------------------------------------------
     def step(self, n: int = 1) -> None:
         check(self.lib.awp_step(self.ctx, int(n)), "awp_step")

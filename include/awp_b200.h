@@ -69,7 +69,8 @@ typedef struct awp_params {
   float fac, q0, ex, fp; /* -l -h --EX -p   Q(f) parameters                       */
   int socalq;        /* -s         SoCal vp/vs floor (1 = on)                     */
   int ifault;        /* -I         1 = point moment-rate source, 2 = the same from
-                                   split files, 5 = kinematic, 6 = plane wave     */
+                                   split files, 4 = prescribed velocities,
+                                   5 = kinematic, 6 = plane wave                  */
   int nst;           /* -N         source time samples                            */
   int read_step;     /* -R/-Q      samples held per source (IFAULT 1, 2: >= nst)   */
   int grid;          /*            block of a discontinuous mesh, 0 = top (finest)  */
@@ -172,6 +173,22 @@ int awp_receivers_count(awp_ctx* ctx, int counts[3]);
  * step-1 source sample of IFAULT < 4 that the reference adds before its loop
  * (pmcl3d.c:1175-1187), so upload the sources first. */
 int awp_sgt_init(awp_ctx* ctx, const char* sgtfile, long long nt);
+
+/* IFAULT=4 prescribed velocities (frcvel_cu, kernel.cu:1836-1934; read_src_ifault_4,
+ * source.c:469-680; pmcl3d.c:714-722, 792-805, 1821-1826, 2442-2486): on grid
+ * 0, after the velocity update, the velocities at `npsrc` points
+ * (pos[npsrc][3] as read_src_ifault_4 forms them: the cell is (x + 1 + ngsl,
+ * y + 1 + ngsl, z + align - 1)) take the frames of a previous run,
+ * interpolated linearly over `tskp` steps per frame; after the last of
+ * `nframes` frames the restoring force of the last prescribed step is added
+ * every step.  Frames arrive in windows of `window` frames: `read` fills
+ * vx, vy, vz [nframes_asked][npsrc] with frames first..first+n-1 (0 = ok),
+ * at set-up and whenever the step loop reaches the end of a window, as
+ * pmcl3d's reader rank delivers them.  nframes must be a multiple of
+ * `window`.  Before the first step. */
+typedef int (*awp_frame_reader)(void* user, int first, int n, float* vx, float* vy, float* vz);
+int awp_velocity_forcing_init(awp_ctx* ctx, int npsrc, const int* pos, int nframes, int tskp,
+                              int window, awp_frame_reader read, void* user);
 
 /* Moment-tensor sources of an ASCII v2 SOURCEFILE (replaces sources_init /
  * sources_read / sources_add_cartesian, src/topography/sources/sources.c:27-78,

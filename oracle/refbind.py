@@ -574,9 +574,11 @@ class RefGpuSim:
         self._fz = fz
         self.cur = 0
         self.source_step = 1
-        # callables(sim, step): after the stress update (SOURCEFILE adds,
+        # callables(sim, step): after the velocity update (IFAULT 4 frcvel,
+        # pmcl3d.c:1821-1826), after the stress update (SOURCEFILE adds,
         # pmcl3d.c:1987-2004) and after the free-surface imaging (receivers,
         # pmcl3d.c:2246-2247)
+        self.after_velocity = []
         self.after_stress = []
         self.after_step = []
         if p["ifault"] == 1 and self.npsrc and not defer_consts:
@@ -706,6 +708,8 @@ class RefGpuSim:
         for _ in range(n):
             self.cur += 1
             self.velocity()
+            for hook in self.after_velocity:
+                hook(self, self.cur)
             self.stress_all()
             self.sources()
             if self.nve == 3:

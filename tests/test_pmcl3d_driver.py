@@ -195,7 +195,9 @@ def test_partitioned_media_file(tmp_path):
 
 @pytest.mark.gpu
 def test_split_sources_equal_point_sources(tmp_path):
-    """IFAULT=2 (read_src_ifault_2, source.c:15-128): the header
+    """IFAULT=2 (read_src_ifault_2, source.c:15-128), READ_STEP < NST as the
+    files intend it (the reference's own window refresh has no defined result
+    there, swap.c:345-353): the header
     "<INSRC>_0" + rank and the READ_STEP windows "<INSRC_I2>_0" + rank +
     "_<idx>" hold the same series as an IFAULT=1 file; both runs write the
     same surface files bit for bit (the last window partly past NST)."""
