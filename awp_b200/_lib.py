@@ -33,6 +33,10 @@ FIELDS = ["u1", "v1", "w1", "xx", "yy", "zz", "xy", "xz", "yz",
 FIELD_ID = {n: i for i, n in enumerate(FIELDS)}
 
 
+# int (*)(void* user, int set): the halo exchange hook of a sub-domain
+EXCHANGE_FN = CFUNCTYPE(c_int, c_void_p, c_int)
+HALO_VELOCITY, HALO_STRESS, HALO_MEDIA, HALO_PLANES = 1, 2, 4, 4
+
 # int (*)(void* user, int first, int n, float* vx, float* vy, float* vz)
 FRAME_READER = CFUNCTYPE(c_int, c_void_p, c_int, c_int, POINTER(c_float), POINTER(c_float),
                          POINTER(c_float))
@@ -119,6 +123,13 @@ def load() -> ctypes.CDLL:
     _sig(lib, "awp_mesh_grid", c_int, [_P, c_int, POINTER(c_void_p)])
     _sig(lib, "awp_mesh_step", c_int, [_P, c_int])
     _sig(lib, "awp_mesh_synchronize", c_int, [_P])
+    _sig(lib, "awp_set_subdomain", c_int, [_P, c_int, c_int])
+    _sig(lib, "awp_halo_copy", c_int, [_P, c_int, c_int, c_int, c_int, c_void_p])
+    _sig(lib, "awp_set_exchange", c_int, [_P, EXCHANGE_FN, c_void_p])
+    _sig(lib, "awp_decomp_create", c_int, [POINTER(c_void_p), c_int, POINTER(c_void_p)])
+    _sig(lib, "awp_decomp_step", c_int, [_P, c_int])
+    _sig(lib, "awp_decomp_synchronize", c_int, [_P])
+    _sig(lib, "awp_decomp_destroy", c_int, [_P])
     _sig(lib, "awp_mesh_set_stream", c_int, [_P, _P])
     _sig(lib, "awp_batch_create", c_int, [POINTER(c_void_p), c_int, POINTER(c_void_p)])
     _sig(lib, "awp_batch_destroy", c_int, [_P])

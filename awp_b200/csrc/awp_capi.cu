@@ -90,6 +90,11 @@ struct awp_ctx {
   bool frc_pending = false;
   awp_frame_reader frc_read = nullptr;
   void* frc_user = nullptr;
+  // x-slab sub-domain of a decomposed grid: global width and offset of this
+  // part (0 = the whole grid), and the caller's halo exchange hook
+  int sub_nxg = 0, sub_x0 = 0;
+  awp_exchange_fn xch = nullptr;
+  void* xch_user = nullptr;
   // FOLLOWBATHY surface level per padded (i, j) column, [j][i] (pmcl3d.c:905-930)
   int* d_bathy = nullptr;
   std::vector<int> bathy;
@@ -173,7 +178,8 @@ StrArgs make_str_args(awp_ctx* c) {
   a.k1 = (c->p.grid == 0) ? c->g.top() : c->g.top() - 2;
   a.fs = (c->p.grid == 0) ? 1 : 0;
   a.ktop = c->g.top();
-  a.gx_lim = c->p.nx + AWP_NGSL + 1;                      // g_i < NX, rankx = 0
+  // g_i < NX (rankx = 0): the global last column, in this part's indices
+  a.gx_lim = (c->sub_nxg ? c->sub_nxg - c->sub_x0 : c->p.nx) + AWP_NGSL + 1;
   a.gy_min = (c->p.npc == 2) ? INT_MIN : AWP_NGSL + 3;     // g_j > 1 || NPC == 2
   a.dth = c->dth; a.dh1 = c->dh1; a.dt = c->p.dt; a.c1 = c->c1; a.c2 = c->c2;
   a.qthr = c->qthr;
@@ -617,17 +623,51 @@ int phase_forcing_window(awp_ctx* c) {
   return AWP_OK;
 }
 
+// The caller's halo exchange of a sub-domain (awp_set_exchange): at the start
+// of a step the stresses and velocities (the last step's stress update wrote
+// the free-surface velocity images, and the first step's starts from the
+// source sample added before the loop), after the velocity update the
+// velocities.
+int exchange(awp_ctx* c, int set) {
+  if (!c->xch) return AWP_OK;
+  const int r = c->xch(c->xch_user, set);
+  if (r) return set_error(AWP_ERR_IO, "halo exchange hook failed (%d)", r);
+  return AWP_OK;
+}
+
 int one_step(awp_ctx* c) {
   int st;
   if ((st = phase_begin(c))) return st;
+  if ((st = exchange(c, AWP_HALO_VELOCITY | AWP_HALO_STRESS))) return st;
   if ((st = phase_velocity(c))) return st;
   if ((st = phase_forcing(c))) return st;
+  if ((st = exchange(c, AWP_HALO_VELOCITY))) return st;
   if ((st = phase_stress(c))) return st;
   if ((st = phase_sources(c))) return st;
   if ((st = phase_plasticity(c))) return st;
   if ((st = phase_fstr(c))) return st;
   if ((st = phase_receivers(c))) return st;
   return phase_forcing_window(c);
+}
+
+// Fields of a halo set, in enum order.
+int halo_fields(int set, int* out) {
+  int n = 0;
+  if (set & AWP_HALO_VELOCITY)
+    for (int f = AWP_U1; f <= AWP_W1; ++f) out[n++] = f;
+  if (set & AWP_HALO_STRESS)
+    for (int f = AWP_XX; f <= AWP_YZ; ++f) out[n++] = f;
+  if (set & AWP_HALO_MEDIA)
+    for (int f = AWP_D1; f <= AWP_QS; ++f) out[n++] = f;
+  return n;
+}
+
+// First plane of a halo: the `planes` interior planes next to `side` (send),
+// or the ghost planes beyond it (receive).
+long long halo_plane(const awp_ctx* c, int side, bool ghost, int planes) {
+  const long long lo = 2 + AWP_NGSL, hi = c->p.nx + 2 + AWP_NGSL;  // first / one-past interior
+  if (side == 0) return ghost ? lo - planes : lo;
+  return ghost ? hi : hi - planes;
 }
 
 }  // namespace
@@ -1362,6 +1402,57 @@ int awp_velocity_forcing_init(awp_ctx* c, int npsrc, const int* pos, int nframes
   return frc_fill(c);
 }
 
+int awp_set_subdomain(awp_ctx* c, int nx_global, int x0) {
+  if (!c) return set_error(AWP_ERR_ARG, "null context");
+  if (c->media_ready || c->cur_step != 0)
+    return set_error(AWP_ERR_STATE, "sub-domain before the media and the first step");
+  if (c->p.ngrids != 1 || c->topo || c->p.nve == 3 || c->p.npc >= 2 || c->p.ifault == 4 ||
+      c->p.ifault == 6)
+    return set_error(AWP_ERR_UNSUPPORTED,
+                     "x-slab sub-domains cover single-grid Cartesian runs without plasticity, "
+                     "periodic sides, prescribed velocities or plane waves");
+  if (x0 < 0 || x0 % 2 || nx_global < c->p.nx || x0 + c->p.nx > nx_global)
+    return set_error(AWP_ERR_ARG,
+                     "sub-domain x0=%d (even, >= 0) of width %d outside a grid of %d", x0,
+                     c->p.nx, nx_global);
+  // the sponge of the whole grid, this part's planes of it (inicrj, cerjan.c:5-64)
+  const int nxp = (int)c->g.nx_pad(), nyp = (int)c->g.ny_pad(), nzp = (int)c->g.nz_pad();
+  std::vector<float> cx(nx_global + 4 + AWP_NGSL2, 1.0f), cy(nyp, 1.0f), cz(nzp, 1.0f);
+  awp::inicrj(c->p.arbc, nx_global, c->p.ny, c->p.nz, nx_global, c->p.ny, c->p.nd,
+              c->p.grid == c->p.ngrids - 1 ? 1 : 0, c->p.npc, cx.data(), cy.data(), cz.data());
+  CU_TRY(cudaMemcpy(c->dcrjx, cx.data() + x0, (size_t)nxp * 4, cudaMemcpyHostToDevice));
+  c->sub_nxg = nx_global;
+  c->sub_x0 = x0;
+  return AWP_OK;
+}
+
+int awp_set_exchange(awp_ctx* c, awp_exchange_fn fn, void* user) {
+  if (!c) return set_error(AWP_ERR_ARG, "null context");
+  if (fn && !c->sub_nxg) return set_error(AWP_ERR_STATE, "halo exchange without a sub-domain");
+  c->xch = fn;
+  c->xch_user = user;
+  return AWP_OK;
+}
+
+int awp_halo_copy(awp_ctx* c, int unpack, int side, int set, int planes, float* buf) {
+  if (!c || !buf) return set_error(AWP_ERR_ARG, "null argument");
+  if ((side != 0 && side != 1) || set <= 0 || set > 7 || planes < 1 || planes > AWP_NGSL ||
+      planes > c->p.nx)
+    return set_error(AWP_ERR_ARG, "halo side %d, set %d, planes %d (1..%d)", side, set, planes,
+                     AWP_NGSL);
+  int fid[16];
+  const int nf = halo_fields(set, fid);
+  const long long plane0 = halo_plane(c, side, unpack != 0, planes);
+  const size_t n = (size_t)planes * c->g.slice;
+  for (int q = 0; q < nf; ++q) {
+    float* field = c->f[fid[q]] + plane0 * c->g.slice;
+    float* b = buf + (size_t)q * n;
+    CU_TRY(cudaMemcpyAsync(unpack ? field : b, unpack ? b : field, n * sizeof(float),
+                           cudaMemcpyDefault, c->stream));
+  }
+  return AWP_OK;
+}
+
 int awp_compute_bathymetry(awp_ctx* c, int* bathy) {
   if (!c || !bathy) return set_error(AWP_ERR_ARG, "null argument");
   if (!c->media_ready) return set_error(AWP_ERR_STATE, "media not uploaded");
@@ -1414,6 +1505,8 @@ int awp_set_bathymetry(awp_ctx* c, const int* bathy) {
 
 int awp_receivers_init(awp_ctx* c, const char* recvfile, long long nt) {
   if (!c || !recvfile) return set_error(AWP_ERR_ARG, "null argument");
+  if (c->sub_nxg)
+    return set_error(AWP_ERR_UNSUPPORTED, "point sets on an x-slab sub-domain");
   if (nt < 1) return set_error(AWP_ERR_ARG, "nt must be >= 1");
   if (c->recv) return set_error(AWP_ERR_STATE, "receivers already initialised");
   RecvState* r = nullptr;
@@ -1430,6 +1523,8 @@ int awp_receivers_init(awp_ctx* c, const char* recvfile, long long nt) {
 
 int awp_sgt_init(awp_ctx* c, const char* sgtfile, long long nt) {
   if (!c || !sgtfile) return set_error(AWP_ERR_ARG, "null argument");
+  if (c->sub_nxg)
+    return set_error(AWP_ERR_UNSUPPORTED, "point sets on an x-slab sub-domain");
   if (nt < 1) return set_error(AWP_ERR_ARG, "nt must be >= 1");
   if (c->sgt) return set_error(AWP_ERR_STATE, "SGT output already initialised");
   if (!c->media_ready) return set_error(AWP_ERR_STATE, "media not uploaded");
@@ -1468,6 +1563,8 @@ int awp_receivers_count(awp_ctx* c, int counts[3]) {
 
 int awp_sourcefile_init(awp_ctx* c, const char* sourcefile) {
   if (!c || !sourcefile) return set_error(AWP_ERR_ARG, "null argument");
+  if (c->sub_nxg)
+    return set_error(AWP_ERR_UNSUPPORTED, "point sets on an x-slab sub-domain");
   if (c->srcf) return set_error(AWP_ERR_STATE, "SOURCEFILE already initialised");
   SrcFileState* s = nullptr;
   const int e = awp_srcf_create(sourcefile, c->g, c->p.dh, c->p.dt, c->topo, &s, g_errmsg,
@@ -1482,6 +1579,8 @@ int awp_sourcefile_init(awp_ctx* c, const char* sourcefile) {
 
 int awp_forcefile_init(awp_ctx* c, const char* forcefile) {
   if (!c || !forcefile) return set_error(AWP_ERR_ARG, "null argument");
+  if (c->sub_nxg)
+    return set_error(AWP_ERR_UNSUPPORTED, "point sets on an x-slab sub-domain");
   if (c->forcef) return set_error(AWP_ERR_STATE, "FORCEFILE already initialised");
   if (!c->topo)
     return set_error(AWP_ERR_STATE,
@@ -1656,6 +1755,136 @@ int awp_mesh_step(awp_mesh* m, int nsteps) {
       return set_error(AWP_ERR_STATE, "grid %d: NVE=3 needs awp_upload_plasticity first", p);
   for (int s = 0; s < nsteps; ++s) {
     int st = mesh_step(m);
+    if (st) return st;
+  }
+  return AWP_OK;
+}
+
+// ---------------------------------------------------------------------------
+// x-slab decomposition stepped in lockstep on one device: the parts' phases in
+// order, the halo planes copied between neighbours in device memory.
+// ---------------------------------------------------------------------------
+struct awp_decomp {
+  int n = 0;
+  awp_ctx* part[AWP_MAXPARTS] = {};
+  int planes = AWP_HALO_PLANES;
+  cudaStream_t stream = nullptr;
+  bool prepared = false;
+};
+
+namespace {
+
+int decomp_exchange(awp_decomp* d, int set) {
+  int fid[16];
+  const int nf = halo_fields(set, fid);
+  const int H = d->planes;
+  for (int p = 0; p + 1 < d->n; ++p) {
+    awp_ctx *L = d->part[p], *R = d->part[p + 1];
+    const size_t n = (size_t)H * L->g.slice;
+    for (int q = 0; q < nf; ++q) {
+      const int f = fid[q];
+      CU_TRY(cudaMemcpyAsync(R->f[f] + halo_plane(R, 0, true, H) * R->g.slice,
+                             L->f[f] + halo_plane(L, 1, false, H) * L->g.slice,
+                             n * sizeof(float), cudaMemcpyDeviceToDevice, d->stream));
+      CU_TRY(cudaMemcpyAsync(L->f[f] + halo_plane(L, 1, true, H) * L->g.slice,
+                             R->f[f] + halo_plane(R, 0, false, H) * R->g.slice,
+                             n * sizeof(float), cudaMemcpyDeviceToDevice, d->stream));
+    }
+  }
+  return AWP_OK;
+}
+
+int decomp_step(awp_decomp* d) {
+  int st;
+  awp_ctx* const* c = d->part;
+  for (int p = 0; p < d->n; ++p)
+    if ((st = phase_begin(c[p]))) return st;
+  if ((st = decomp_exchange(d, AWP_HALO_VELOCITY | AWP_HALO_STRESS))) return st;
+  for (int p = 0; p < d->n; ++p)
+    if ((st = phase_velocity(c[p]))) return st;
+  if ((st = decomp_exchange(d, AWP_HALO_VELOCITY))) return st;
+  for (int p = 0; p < d->n; ++p)
+    if ((st = phase_stress(c[p]))) return st;
+  for (int p = 0; p < d->n; ++p)
+    if ((st = phase_sources(c[p]))) return st;
+  for (int p = 0; p < d->n; ++p)
+    if ((st = phase_fstr(c[p]))) return st;
+  return AWP_OK;
+}
+
+}  // namespace
+
+int awp_decomp_create(awp_ctx** parts, int n, awp_decomp** out) {
+  if (!parts || !out) return set_error(AWP_ERR_ARG, "null argument");
+  *out = nullptr;
+  if (n < 1 || n > AWP_MAXPARTS) return set_error(AWP_ERR_ARG, "%d parts (1..%d)", n, AWP_MAXPARTS);
+  int dev0 = -1;
+  for (int p = 0; p < n; ++p) {
+    awp_ctx* c = parts[p];
+    if (!c || !c->sub_nxg) return set_error(AWP_ERR_STATE, "part %d has no sub-domain", p);
+    if (c->xch) return set_error(AWP_ERR_STATE, "part %d has its own exchange hook", p);
+    if (c->p.ny != parts[0]->p.ny || c->p.nz != parts[0]->p.nz ||
+        c->sub_nxg != parts[0]->sub_nxg)
+      return set_error(AWP_ERR_ARG, "part %d: ny, nz and the global nx must agree", p);
+    const int want = p == 0 ? 0 : parts[p - 1]->sub_x0 + parts[p - 1]->p.nx;
+    if (c->sub_x0 != want)
+      return set_error(AWP_ERR_ARG, "part %d starts at x=%d, not %d", p, c->sub_x0, want);
+    if (c->p.nx < AWP_NGSL / 2) return set_error(AWP_ERR_ARG, "part %d narrower than its halo", p);
+    int dev = -1;
+    cudaPointerAttributes at;
+    CU_TRY(cudaPointerGetAttributes(&at, c->f[AWP_U1]));
+    dev = at.device;
+    if (p == 0) dev0 = dev;
+    else if (dev != dev0) return set_error(AWP_ERR_ARG, "part %d is on another device", p);
+  }
+  if (parts[n - 1]->sub_x0 + parts[n - 1]->p.nx != parts[0]->sub_nxg)
+    return set_error(AWP_ERR_ARG, "the parts do not cover the grid");
+  awp_decomp* d = new awp_decomp();
+  d->n = n;
+  for (int p = 0; p < n; ++p) d->part[p] = parts[p];
+  if (cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete d;
+    return set_error(AWP_ERR_CUDA, "stream");
+  }
+  for (int p = 0; p < n; ++p) {
+    cudaStreamSynchronize(parts[p]->stream);
+    awp_set_stream(parts[p], d->stream);
+  }
+  *out = d;
+  return AWP_OK;
+}
+
+int awp_decomp_destroy(awp_decomp* d) {
+  if (!d) return AWP_OK;
+  cudaStreamSynchronize(d->stream);
+  for (int p = 0; p < d->n; ++p) awp_set_stream(d->part[p], nullptr);
+  cudaStreamDestroy(d->stream);
+  delete d;
+  return AWP_OK;
+}
+
+int awp_decomp_step(awp_decomp* d, int nsteps) {
+  if (!d) return set_error(AWP_ERR_ARG, "null decomposition");
+  if (!d->prepared) {
+    // the media halos once; each part keeps its own elastic specialisation
+    // (with Q^-1 identically zero the anelastic update reduces exactly to it)
+    for (int p = 0; p < d->n; ++p)
+      if (!d->part[p]->media_ready) return set_error(AWP_ERR_STATE, "part %d has no media", p);
+    const int st = decomp_exchange(d, AWP_HALO_MEDIA);
+    if (st) return st;
+    d->prepared = true;
+  }
+  for (int s = 0; s < nsteps; ++s) {
+    const int st = decomp_step(d);
+    if (st) return st;
+  }
+  return AWP_OK;
+}
+
+int awp_decomp_synchronize(awp_decomp* d) {
+  if (!d) return set_error(AWP_ERR_ARG, "null decomposition");
+  for (int p = 0; p < d->n; ++p) {
+    const int st = awp_synchronize(d->part[p]);
     if (st) return st;
   }
   return AWP_OK;
@@ -1907,7 +2136,7 @@ int awp_batch_create(awp_ctx* const* ctxs, int n, awp_batch** out) {
     if (!c) return set_error(AWP_ERR_ARG, "instance %d is null", q);
     if (!c->media_ready) return set_error(AWP_ERR_STATE, "instance %d: media not uploaded", q);
     if (c->p.ngrids != 1 || c->p.nve == 3 || c->topo || c->recv || c->srcf || c->forcef ||
-        c->sgt || c->p.ifault == 6 || c->p.ifault == 4)
+        c->sgt || c->p.ifault == 6 || c->p.ifault == 4 || c->sub_nxg)
       return set_error(AWP_ERR_UNSUPPORTED,
                        "instance %d: a batch holds single-grid Cartesian runs without "
                        "plasticity, receivers, SOURCEFILE, plane-wave or prescribed-velocity "
@@ -2089,6 +2318,7 @@ int awp_set_topo_plasticity(awp_ctx* c, int consistent) {
 
 int awp_topography_init(awp_ctx* c, const char* intopo) {
   if (!c || !intopo) return set_error(AWP_ERR_ARG, "null argument");
+  if (c->sub_nxg) return set_error(AWP_ERR_UNSUPPORTED, "topography on an x-slab sub-domain");
   if (c->topo) return set_error(AWP_ERR_STATE, "topography already initialised");
   if (c->recv || c->srcf || c->forcef || c->sgt)
     return set_error(AWP_ERR_STATE,
@@ -2167,8 +2397,9 @@ int check_adjoint_ctx(awp_ctx* c) {
     return set_error(AWP_ERR_UNSUPPORTED,
                      "the adjoint covers single-grid Cartesian runs without plasticity, "
                      "receiver or SGT files or SOURCEFILE sources");
-  if (c->d_frc_pos)
-    return set_error(AWP_ERR_UNSUPPORTED, "the adjoint does not cover prescribed velocities");
+  if (c->d_frc_pos || c->sub_nxg)
+    return set_error(AWP_ERR_UNSUPPORTED,
+                     "the adjoint covers neither prescribed velocities nor sub-domains");
   if (c->ncell > 0 && c->p.ifault != 1 && c->p.ifault != 2)
     return set_error(AWP_ERR_UNSUPPORTED,
                      "the adjoint takes IFAULT 1 or 2 sources (the kinematic source depends on "

@@ -307,6 +307,44 @@ class Solver:
         check(self.lib.awp_set_bathymetry(self.ctx, b.ctypes.data_as(POINTER(c_int))),
               "awp_set_bathymetry")
 
+    def set_stream(self, stream: int | None) -> None:
+        """Run on this cudaStream_t handle from now on (None or 0: the legacy
+        default stream)."""
+        check(self.lib.awp_set_stream(self.ctx, c_void_p(stream or None)), "awp_set_stream")
+
+    # -- x-slab sub-domains -------------------------------------------------
+    def set_subdomain(self, nx_global: int, x0: int) -> None:
+        """This context is the part [x0, x0 + nx) of a grid nx_global wide
+        (before the media)."""
+        check(self.lib.awp_set_subdomain(self.ctx, int(nx_global), int(x0)), "awp_set_subdomain")
+
+    def halo_copy(self, unpack: bool, side: int, hset: int, planes: int, buf: int) -> None:
+        """awp_halo_copy on the context's stream; buf is a device or pinned
+        address of nfields * planes * ny_pad * nz_pad floats."""
+        check(self.lib.awp_halo_copy(self.ctx, int(bool(unpack)), int(side), int(hset),
+                                     int(planes), c_void_p(buf)), "awp_halo_copy")
+
+    def set_exchange(self, fn) -> None:
+        """fn(hset) -> None runs at the two exchange points of every step
+        (None removes it); an exception is reported as a failed step."""
+        if fn is None:
+            self._exchange = None
+            check(self.lib.awp_set_exchange(self.ctx, _lib.EXCHANGE_FN(), None),
+                  "awp_set_exchange")
+            return
+
+        def hook(_user, hset):
+            try:
+                fn(int(hset))
+                return 0
+            except Exception:  # noqa: BLE001 - reported to the library as a status
+                import traceback
+                traceback.print_exc()
+                return 1
+
+        self._exchange = _lib.EXCHANGE_FN(hook)  # kept alive with the context
+        check(self.lib.awp_set_exchange(self.ctx, self._exchange, None), "awp_set_exchange")
+
     def check_finite(self) -> bool:
         ok = c_int()
         check(self.lib.awp_check_finite(self.ctx, byref(ok)), "awp_check_finite")

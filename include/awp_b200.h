@@ -254,6 +254,47 @@ int awp_mesh_step(awp_mesh* mesh, int nsteps);
 int awp_mesh_set_stream(awp_mesh* mesh, void* cuda_stream);
 int awp_mesh_synchronize(awp_mesh* mesh);
 
+/* x-slab domain decomposition (the multi-rank path of pmcl3d.c:1657-1721,
+ * 1838-1924 and swap.c, rebuilt for contiguous slabs: the padded layout's
+ * slowest axis is x, so every halo is a run of whole x planes).  A part is a
+ * context of width nx (its awp_params.nx) at global offset x0 (even, so that
+ * the attenuation parity pattern is the global one) in a grid of nx_global;
+ * awp_set_subdomain is called after awp_ctx_create and before the media,
+ * which are uploaded per part ([nz][ny][nx] of the part).  The sponge is the
+ * whole grid's; sources are given to their owning part in its own
+ * coordinates.  Single-grid Cartesian runs without plasticity, point-set
+ * files, prescribed velocities or plane waves.  At the start of a step the
+ * stresses and velocities (the stress update writes the free-surface
+ * velocity images; before the first step the source sample of the loop's
+ * start is added), after the velocity update the velocities, and once before
+ * the first step the media must reach the neighbours' ghost planes; a
+ * 4th-order stencil reads two planes across, AWP_HALO_PLANES = 4 are sent. */
+#define AWP_HALO_VELOCITY 1 /* u1 v1 w1 */
+#define AWP_HALO_STRESS 2   /* xx yy zz xy xz yz */
+#define AWP_HALO_MEDIA 4    /* d1 mu lam qp qs */
+#define AWP_HALO_PLANES 4
+#define AWP_MAXPARTS 16
+int awp_set_subdomain(awp_ctx* ctx, int nx_global, int x0);
+/* Copy the halo of `set` (fields in enum order, `planes` x planes each, x
+ * fastest within a plane as the padded layout) between the context and `buf`
+ * (device or page-locked host memory, nfields * planes * (ny+4+2*ngsl) *
+ * (nz+2*align) floats) on the context's stream: unpack = 0 reads the planes
+ * inside `side` (0 = low x, 1 = high x) into buf, unpack = 1 writes buf into
+ * the ghost planes beyond it. */
+int awp_halo_copy(awp_ctx* ctx, int unpack, int side, int set, int planes, float* buf);
+/* One process per GPU: awp_step calls `fn(user, set)` at the two exchange
+ * points of every step; it exchanges with the neighbours (awp_halo_copy and
+ * the caller's transport, e.g. NCCL) and returns 0.  NULL removes it. */
+typedef int (*awp_exchange_fn)(void* user, int set);
+int awp_set_exchange(awp_ctx* ctx, awp_exchange_fn fn, void* user);
+/* Several parts on one device stepped in lockstep, the halos copied in device
+ * memory on one stream the decomposition owns (destroy it before the parts). */
+typedef struct awp_decomp awp_decomp;
+int awp_decomp_create(awp_ctx** parts, int nparts, awp_decomp** out);
+int awp_decomp_step(awp_decomp* d, int nsteps);
+int awp_decomp_synchronize(awp_decomp* d);
+int awp_decomp_destroy(awp_decomp* d);
+
 /* ------------------------------------------------------------------------ */
 /* Batched instances: many independent single-grid simulations of uneven     */
 /* sizes (source ensembles, shots) advanced together.                        */
