@@ -35,7 +35,7 @@ FIELD_ID = {n: i for i, n in enumerate(FIELDS)}
 
 # int (*)(void* user, int set): the halo exchange hook of a sub-domain
 EXCHANGE_FN = CFUNCTYPE(c_int, c_void_p, c_int)
-HALO_VELOCITY, HALO_STRESS, HALO_MEDIA, HALO_PLANES = 1, 2, 4, 4
+HALO_VELOCITY, HALO_STRESS, HALO_MEDIA, HALO_YLDFAC, HALO_PLANES = 1, 2, 4, 8, 4
 
 # int (*)(void* user, int first, int n, float* vx, float* vy, float* vz)
 FRAME_READER = CFUNCTYPE(c_int, c_void_p, c_int, c_int, POINTER(c_float), POINTER(c_float),

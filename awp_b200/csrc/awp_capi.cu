@@ -250,6 +250,13 @@ int launch_plasticity(awp_ctx* c) {
   a.k0 = AWP_ALIGN;
   a.k1 = AWP_ALIGN + round_up(c->g.nzt, 4) - 1;
   CU_TRY(awp_launch_plast_calc(a, c->stream));
+  return AWP_OK;
+}
+
+// drprecpc_app (kernel.cu:1650-1778) over the same window: reads the yield
+// factors of the cell and of its -x, +y, +z neighbours
+int launch_plast_app(awp_ctx* c) {
+  float** f = c->f;
   PlastAppArgs b;
   memset(&b, 0, sizeof(b));
   b.xx = f[AWP_XX]; b.yy = f[AWP_YY]; b.zz = f[AWP_ZZ];
@@ -407,8 +414,10 @@ void middle_band(const awp_ctx* c, int* i0, int* i1, int* j0, int* j1) {
   if (yls2 % 2 != 0) yls2 += 1;
   int yre2 = (int)(yls + (int)(yre - yls) * 0.75);
   if (yre2 % 2 == 0) yre2 -= 1;
-  *i0 = AWP_NGSL + 4;
-  *i1 = c->g.nxt + AWP_NGSL - 1;
+  // x range of the whole grid, in this part's indices when it is a sub-domain
+  const int x0 = c->sub_nxg ? c->sub_x0 : 0, nxg = c->sub_nxg ? c->sub_nxg : c->g.nxt;
+  *i0 = std::max(AWP_NGSL + 4 - x0, c->sub_nxg ? c->xls : 0);
+  *i1 = std::min(nxg + AWP_NGSL - 1 - x0, c->sub_nxg ? c->xre : INT_MAX);
   *j0 = std::max(yls2, yls + AWP_NGSL + 2);
   *j1 = std::min(yre2, yre - AWP_NGSL - 2);
 }
@@ -505,6 +514,18 @@ int phase_sources(awp_ctx* c) {
   return AWP_OK;
 }
 
+// The caller's halo exchange of a sub-domain (awp_set_exchange): at the start
+// of a step the stresses and velocities (the last step's stress update wrote
+// the free-surface velocity images, and the first step's starts from the
+// source sample added before the loop), after the velocity update the
+// velocities.
+int exchange(awp_ctx* c, int set) {
+  if (!c->xch) return AWP_OK;
+  const int r = c->xch(c->xch_user, set);
+  if (r) return set_error(AWP_ERR_IO, "halo exchange hook failed (%d)", r);
+  return AWP_OK;
+}
+
 int phase_plasticity(awp_ctx* c) {
   if (c->p.nve != 3) return AWP_OK;
   int st;
@@ -515,9 +536,15 @@ int phase_plasticity(awp_ctx* c) {
     if ((st = launch_cart_stress(c, i0, i1, j0, j1))) return st;
   }
   PhaseScope ps(c, 3);
-  st = launch_plasticity(c);
-  if (st) return st;
-  c->launches += 2;
+  // a sub-domain's ghost planes take the neighbours' updated stresses (the
+  // yield factor averages xz and xy over x) and then their yield factors
+  // (the return averages them over x)
+  if ((st = exchange(c, AWP_HALO_STRESS))) return st;
+  if ((st = launch_plasticity(c))) return st;
+  c->launches++;
+  if ((st = exchange(c, AWP_HALO_YLDFAC))) return st;
+  if ((st = launch_plast_app(c))) return st;
+  c->launches++;
   return AWP_OK;
 }
 
@@ -623,18 +650,6 @@ int phase_forcing_window(awp_ctx* c) {
   return AWP_OK;
 }
 
-// The caller's halo exchange of a sub-domain (awp_set_exchange): at the start
-// of a step the stresses and velocities (the last step's stress update wrote
-// the free-surface velocity images, and the first step's starts from the
-// source sample added before the loop), after the velocity update the
-// velocities.
-int exchange(awp_ctx* c, int set) {
-  if (!c->xch) return AWP_OK;
-  const int r = c->xch(c->xch_user, set);
-  if (r) return set_error(AWP_ERR_IO, "halo exchange hook failed (%d)", r);
-  return AWP_OK;
-}
-
 int one_step(awp_ctx* c) {
   int st;
   if ((st = phase_begin(c))) return st;
@@ -659,6 +674,7 @@ int halo_fields(int set, int* out) {
     for (int f = AWP_XX; f <= AWP_YZ; ++f) out[n++] = f;
   if (set & AWP_HALO_MEDIA)
     for (int f = AWP_D1; f <= AWP_QS; ++f) out[n++] = f;
+  if (set & AWP_HALO_YLDFAC) out[n++] = AWP_YLDFAC;
   return n;
 }
 
@@ -1224,7 +1240,10 @@ int awp_upload_plasticity(awp_ctx* c, const float* sigma2, const float* cohes,
   // visit count of the five drprecpc_calc strips (pmcl3d.c:2121-2181)
   const int nxp = (int)c->g.nx_pad(), nyp = (int)c->g.ny_pad();
   std::vector<unsigned char> mult((size_t)nxp * nyp, 0);
-  const int xl = c->xls, xr = c->xre, yl = c->yls, yr = c->yre;
+  // the whole grid's strips, in this part's indices when it is a sub-domain
+  const int xo = c->sub_nxg ? c->sub_x0 : 0;
+  const int xl = c->xls - xo, xr = (c->sub_nxg ? c->sub_nxg : c->p.nx) + AWP_NGSL + 1 - xo,
+            yl = c->yls, yr = c->yre;
   auto add = [&](int i0, int i1, int j0, int j1) {
     for (int i = i0; i <= i1; ++i)
       for (int j = j0; j <= j1; ++j)
@@ -1406,11 +1425,12 @@ int awp_set_subdomain(awp_ctx* c, int nx_global, int x0) {
   if (!c) return set_error(AWP_ERR_ARG, "null context");
   if (c->media_ready || c->cur_step != 0)
     return set_error(AWP_ERR_STATE, "sub-domain before the media and the first step");
-  if (c->p.ngrids != 1 || c->topo || c->p.nve == 3 || c->p.npc >= 2 || c->p.ifault == 4 ||
-      c->p.ifault == 6)
+  if (c->p.ngrids != 1 || c->topo || c->p.npc >= 2 || c->p.ifault == 4 || c->p.ifault == 6)
     return set_error(AWP_ERR_UNSUPPORTED,
-                     "x-slab sub-domains cover single-grid Cartesian runs without plasticity, "
-                     "periodic sides, prescribed velocities or plane waves");
+                     "x-slab sub-domains cover single-grid Cartesian runs without periodic "
+                     "sides, prescribed velocities or plane waves");
+  if (c->plast_ready)
+    return set_error(AWP_ERR_STATE, "sub-domain before the plasticity inputs");
   if (x0 < 0 || x0 % 2 || nx_global < c->p.nx || x0 + c->p.nx > nx_global)
     return set_error(AWP_ERR_ARG,
                      "sub-domain x0=%d (even, >= 0) of width %d outside a grid of %d", x0,
@@ -1436,12 +1456,14 @@ int awp_set_exchange(awp_ctx* c, awp_exchange_fn fn, void* user) {
 
 int awp_halo_copy(awp_ctx* c, int unpack, int side, int set, int planes, float* buf) {
   if (!c || !buf) return set_error(AWP_ERR_ARG, "null argument");
-  if ((side != 0 && side != 1) || set <= 0 || set > 7 || planes < 1 || planes > AWP_NGSL ||
+  if ((side != 0 && side != 1) || set <= 0 || set > 15 || planes < 1 || planes > AWP_NGSL ||
       planes > c->p.nx)
     return set_error(AWP_ERR_ARG, "halo side %d, set %d, planes %d (1..%d)", side, set, planes,
                      AWP_NGSL);
   int fid[16];
   const int nf = halo_fields(set, fid);
+  for (int q = 0; q < nf; ++q)
+    if (!c->f[fid[q]]) return set_error(AWP_ERR_STATE, "field %d not allocated (NVE)", fid[q]);
   const long long plane0 = halo_plane(c, side, unpack != 0, planes);
   const size_t n = (size_t)planes * c->g.slice;
   for (int q = 0; q < nf; ++q) {
@@ -1807,6 +1829,24 @@ int decomp_step(awp_decomp* d) {
     if ((st = phase_stress(c[p]))) return st;
   for (int p = 0; p < d->n; ++p)
     if ((st = phase_sources(c[p]))) return st;
+  if (c[0]->p.nve == 3) {  // the middle band, the stress halo, the yield factors, their
+                           // halo, the return
+    for (int p = 0; p < d->n; ++p) {
+      int i0, i1, j0, j1;
+      middle_band(c[p], &i0, &i1, &j0, &j1);
+      if ((st = launch_cart_stress(c[p], i0, i1, j0, j1))) return st;
+    }
+    if ((st = decomp_exchange(d, AWP_HALO_STRESS))) return st;
+    for (int p = 0; p < d->n; ++p) {
+      if ((st = launch_plasticity(c[p]))) return st;
+      c[p]->launches++;
+    }
+    if ((st = decomp_exchange(d, AWP_HALO_YLDFAC))) return st;
+    for (int p = 0; p < d->n; ++p) {
+      if ((st = launch_plast_app(c[p]))) return st;
+      c[p]->launches++;
+    }
+  }
   for (int p = 0; p < d->n; ++p)
     if ((st = phase_fstr(c[p]))) return st;
   return AWP_OK;
@@ -1824,8 +1864,8 @@ int awp_decomp_create(awp_ctx** parts, int n, awp_decomp** out) {
     if (!c || !c->sub_nxg) return set_error(AWP_ERR_STATE, "part %d has no sub-domain", p);
     if (c->xch) return set_error(AWP_ERR_STATE, "part %d has its own exchange hook", p);
     if (c->p.ny != parts[0]->p.ny || c->p.nz != parts[0]->p.nz ||
-        c->sub_nxg != parts[0]->sub_nxg)
-      return set_error(AWP_ERR_ARG, "part %d: ny, nz and the global nx must agree", p);
+        c->sub_nxg != parts[0]->sub_nxg || c->p.nve != parts[0]->p.nve)
+      return set_error(AWP_ERR_ARG, "part %d: ny, nz, NVE and the global nx must agree", p);
     const int want = p == 0 ? 0 : parts[p - 1]->sub_x0 + parts[p - 1]->p.nx;
     if (c->sub_x0 != want)
       return set_error(AWP_ERR_ARG, "part %d starts at x=%d, not %d", p, c->sub_x0, want);
@@ -1868,8 +1908,11 @@ int awp_decomp_step(awp_decomp* d, int nsteps) {
   if (!d->prepared) {
     // the media halos once; each part keeps its own elastic specialisation
     // (with Q^-1 identically zero the anelastic update reduces exactly to it)
-    for (int p = 0; p < d->n; ++p)
+    for (int p = 0; p < d->n; ++p) {
       if (!d->part[p]->media_ready) return set_error(AWP_ERR_STATE, "part %d has no media", p);
+      if (d->part[p]->p.nve == 3 && !d->part[p]->plast_ready)
+        return set_error(AWP_ERR_STATE, "part %d: NVE=3 needs awp_upload_plasticity", p);
+    }
     const int st = decomp_exchange(d, AWP_HALO_MEDIA);
     if (st) return st;
     d->prepared = true;

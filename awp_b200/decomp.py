@@ -6,8 +6,9 @@ velocity and stress halos between the kernels of every step
 slowest axis of the padded layout, so each halo is a run of whole x planes:
 one contiguous copy per field and side.  A part is a context made with
 :meth:`Solver.set_subdomain`; the halos of a step are the stresses and
-velocities at its start and the velocities after the velocity update, plus
-the media once (include/awp_b200.h).
+velocities at its start, the velocities after the velocity update and, with
+plasticity, the yield factors between the two plasticity kernels, plus the
+media once (include/awp_b200.h).
 
 * :func:`split_x` -- widths and even offsets of the parts.
 * :class:`LocalDecomposition` -- several parts on one device stepped in
@@ -22,7 +23,7 @@ from ctypes import byref, c_void_p
 import numpy as np
 
 from . import _lib
-from ._lib import HALO_MEDIA, HALO_PLANES, HALO_STRESS, HALO_VELOCITY, check
+from ._lib import HALO_MEDIA, HALO_PLANES, HALO_STRESS, HALO_VELOCITY, HALO_YLDFAC, check
 
 NGSL = 8
 
@@ -72,7 +73,7 @@ def part_sources(pos, data, x0: int, nx: int, first: bool, last: bool):
 def halo_fields(hset: int) -> int:
     """Fields in a halo set."""
     return 3 * bool(hset & HALO_VELOCITY) + 6 * bool(hset & HALO_STRESS) + \
-        5 * bool(hset & HALO_MEDIA)
+        5 * bool(hset & HALO_MEDIA) + bool(hset & HALO_YLDFAC)
 
 
 class LocalDecomposition:
@@ -107,6 +108,13 @@ class LocalDecomposition:
             p, d = part_sources(pos, data, x0, w, q == 0, q == n - 1)
             if len(p):
                 s.upload_sources(p, d)
+
+    def upload_plasticity(self, sigma2, cohes, phi, fmajor, fminor, strike, dip) -> None:
+        """NVE 3 inputs of the whole padded grid; each part takes its planes."""
+        for s, (x0, w) in zip(self.parts, self.layout):
+            sl = slice(x0, x0 + w + 4 + 2 * NGSL)
+            s.upload_plasticity(*(np.ascontiguousarray(np.asarray(a)[sl])
+                                  for a in (sigma2, cohes, phi)), fmajor, fminor, strike, dip)
 
     def step(self, n: int = 1) -> None:
         check(self.lib.awp_decomp_step(self.d, int(n)), "awp_decomp_step")

@@ -390,7 +390,11 @@ def run_ours(args, rank, world, dist) -> dict | None:
         se.upload_sources(scn.src_pos, scn.src_data)
         if topo_path:
             se.topography(topo_path)
+        t_setup = torch.cuda.Event(enable_timing=True)
+        t_setup.record(stream)
         se.step(e2e_steps)
+        t_steps = torch.cuda.Event(enable_timing=True)
+        t_steps.record(stream)
         # free-surface snapshot (velbuffer, NBGZ=NEDZ=1) back to the host
         se.gather(0, p["nx"] - 1, 1, 0, p["ny"] - 1, 1, 0, 0, 1,
                   dev[0].data_ptr(), dev[1].data_ptr(), dev[2].data_ptr())
@@ -399,11 +403,17 @@ def run_ours(args, rank, world, dist) -> dict | None:
         t1.record(stream)
         torch.cuda.synchronize()
         e2e_ms = reduce_max(t0.elapsed_time(t1), dist)
+        setup_ms = t0.elapsed_time(t_setup)
+        steps_ms = t_setup.elapsed_time(t_steps)
         d2h = 3 * rec * 4
         e2e = {"value": world * cells * e2e_steps / (e2e_ms * 1e-3) / 1e9,
                "unit": "Gcell-updates/s", "h2d_bytes_per_step": h2d / e2e_steps,
                "d2h_bytes_per_step": d2h / e2e_steps, "ms_total": e2e_ms,
                "steps": e2e_steps,
+               # where the time goes (rank 0's events): set-up (context, media H2D
+               # and mapping, sources) and the steps, against the timed region's
+               # step time (a long run may sit under the power cap)
+               "setup_ms": setup_ms, "ms_per_step": steps_ms / max(e2e_steps, 1),
                "includes": "the whole run through the C ABI: context create, media H2D + "
                            "on-device inimesh mapping, sources, every time step of the run, "
                            "surface snapshot D2H"}

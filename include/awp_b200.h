@@ -262,16 +262,21 @@ int awp_mesh_synchronize(awp_mesh* mesh);
  * awp_set_subdomain is called after awp_ctx_create and before the media,
  * which are uploaded per part ([nz][ny][nx] of the part).  The sponge is the
  * whole grid's; sources are given to their owning part in its own
- * coordinates.  Single-grid Cartesian runs without plasticity, point-set
- * files, prescribed velocities or plane waves.  At the start of a step the
+ * coordinates; the plasticity inputs are the part's planes of the whole
+ * padded arrays (x0 .. x0 + nx + 4 + 2*ngsl - 1), uploaded after
+ * awp_set_subdomain.  Single-grid Cartesian runs without point-set files,
+ * prescribed velocities or plane waves.  At the start of a step the
  * stresses and velocities (the stress update writes the free-surface
  * velocity images; before the first step the source sample of the loop's
  * start is added), after the velocity update the velocities, and once before
- * the first step the media must reach the neighbours' ghost planes; a
- * 4th-order stencil reads two planes across, AWP_HALO_PLANES = 4 are sent. */
+ * the first step the media must reach the neighbours' ghost planes, and with
+ * NVE 3 the stresses before the yield factors and the yield factors before
+ * the return (the two plasticity kernels average over x); a 4th-order
+ * stencil reads two planes across, AWP_HALO_PLANES = 4 are sent. */
 #define AWP_HALO_VELOCITY 1 /* u1 v1 w1 */
 #define AWP_HALO_STRESS 2   /* xx yy zz xy xz yz */
 #define AWP_HALO_MEDIA 4    /* d1 mu lam qp qs */
+#define AWP_HALO_YLDFAC 8   /* yldfac (NVE 3: between the two plasticity kernels) */
 #define AWP_HALO_PLANES 4
 #define AWP_MAXPARTS 16
 int awp_set_subdomain(awp_ctx* ctx, int nx_global, int x0);

@@ -22,13 +22,30 @@ FIELDS = ["u1", "v1", "w1", "xx", "yy", "zz", "xy", "xz", "yz", "r1", "r2", "r3"
           "r6"]
 
 
-def whole_run(scn, steps):
+def plastic_case(nx, seed, steps, ifault=1):
+    """NVE 3: low cohesions so that cells near the sources yield."""
+    from oracle import refbind
+    scn = scenarios.random_small(nx=nx, ny=24, nz=32, q=True, ifault=ifault, steps=steps,
+                                 seed=seed, nsrc=4)
+    scn.params["nve"] = 3
+    pl = refbind.plasticity_inputs(scn, refbind.model_setup(scn))
+    return scn, pl
+
+
+def plast_args(pl):
+    return pl["sigma2"], pl["cohes"], pl["phi"], pl["fmajor"], pl["fminor"], pl["strike"], \
+        pl["dip"]
+
+
+def whole_run(scn, steps, pl=None):
     s = Solver(default_params(**scn.params))
     s.upload_media(scn.media)
     s.upload_sources(scn.src_pos, scn.src_data)
+    if pl is not None:
+        s.upload_plasticity(*plast_args(pl))
     s.step(steps)
     s.synchronize()
-    out = {f: s.field(f) for f in FIELDS}
+    out = {f: s.field(f) for f in FIELDS + (["yldfac", "neta"] if pl is not None else [])}
     s.close()
     return out
 
@@ -66,6 +83,27 @@ def test_lockstep_parts_equal_whole_grid(nx, nparts, q, ifault):
             assert np.array_equal(got, want[f]), (f, float(np.abs(got - want[f]).max()))
 
 
+@pytest.mark.parametrize("nx,nparts", [(31, 3), (30, 2)])
+def test_lockstep_plastic_parts_equal_whole_grid(nx, nparts):
+    steps = 20
+    scn, pl = plastic_case(nx, 51, steps)
+    want = whole_run(scn, steps, pl)
+    assert np.any(want["yldfac"] < 1.0)  # cells yield
+    with LocalDecomposition(default_params(**scn.params), nparts) as d:
+        d.upload_media(scn.media)
+        d.upload_sources(scn.src_pos, scn.src_data)
+        d.upload_plasticity(*plast_args(pl))
+        d.step(steps)
+        d.synchronize()
+        for f in want:
+            got = d.field(f)
+            if f == "yldfac":  # the inner ghost planes hold the neighbours' values
+                got, w = got[2 + NGSL:-2 - NGSL], want[f][2 + NGSL:-2 - NGSL]
+            else:
+                w = want[f]
+            assert np.array_equal(got, w), (f, float(np.abs(got - w).max()))
+
+
 class _Sent:
     def wait(self):
         pass
@@ -94,12 +132,15 @@ class ThreadComm:
         return _Recv(self.boxes[(src, self.rank, tag)], t)
 
 
-@pytest.mark.parametrize("nx,nparts", [(28, 2), (33, 3)])
-def test_exchange_hook_parts_equal_whole_grid(nx, nparts):
+@pytest.mark.parametrize("nx,nparts,plastic", [(28, 2, False), (33, 3, False), (30, 2, True)])
+def test_exchange_hook_parts_equal_whole_grid(nx, nparts, plastic):
     steps = 16
-    scn = scenarios.random_small(nx=nx, ny=20, nz=32, q=True, ifault=1, steps=steps, seed=43,
-                                 nsrc=4)
-    want = whole_run(scn, steps)
+    if plastic:
+        scn, pl = plastic_case(nx, 53, steps)
+    else:
+        scn, pl = scenarios.random_small(nx=nx, ny=20, nz=32, q=True, ifault=1, steps=steps,
+                                         seed=43, nsrc=4), None
+    want = whole_run(scn, steps, pl)
     layout = split_x(nx, nparts)
     boxes = {(a, b, t): queue.Queue() for a in range(nparts) for b in range(nparts)
              for t in (0, 1)}
@@ -111,6 +152,10 @@ def test_exchange_hook_parts_equal_whole_grid(nx, nparts):
         p, dat = part_sources(scn.src_pos, scn.src_data, x0, w, r == 0, r == nparts - 1)
         if len(p):
             s.upload_sources(p, dat)
+        if pl is not None:
+            sl = slice(x0, x0 + w + 4 + 2 * NGSL)
+            s.upload_plasticity(*[np.ascontiguousarray(a[sl]) for a in plast_args(pl)[:3]],
+                                *plast_args(pl)[3:])
         parts.append(s)
         slabs.append(SlabRank(s, r, nparts, comm=ThreadComm(r, boxes)))
     errors = []
@@ -129,10 +174,13 @@ def test_exchange_hook_parts_equal_whole_grid(nx, nparts):
     for t in threads:
         t.join(timeout=300)
     assert not errors, errors
-    assert all(sl.exchanges == 2 * steps + 1 for sl in slabs)
-    for f in FIELDS:
+    assert all(sl.exchanges == (4 if plastic else 2) * steps + 1 for sl in slabs)
+    for f in want:
         got = assemble(parts, layout, f)
-        assert np.array_equal(got, want[f]), (f, float(np.abs(got - want[f]).max()))
+        w = want[f]
+        if f == "yldfac":
+            got, w = got[2 + NGSL:-2 - NGSL], w[2 + NGSL:-2 - NGSL]
+        assert np.array_equal(got, w), (f, float(np.abs(got - w).max()))
     for s in parts:
         s.close()
 
