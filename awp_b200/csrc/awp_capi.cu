@@ -1425,10 +1425,11 @@ int awp_set_subdomain(awp_ctx* c, int nx_global, int x0) {
   if (!c) return set_error(AWP_ERR_ARG, "null context");
   if (c->media_ready || c->cur_step != 0)
     return set_error(AWP_ERR_STATE, "sub-domain before the media and the first step");
-  if (c->p.ngrids != 1 || c->topo || c->p.npc >= 2 || c->p.ifault == 4 || c->p.ifault == 6)
+  if (c->topo) return set_error(AWP_ERR_STATE, "sub-domain before the topography");
+  if (c->p.ngrids != 1 || c->p.npc >= 2 || c->p.ifault == 4 || c->p.ifault == 6)
     return set_error(AWP_ERR_UNSUPPORTED,
-                     "x-slab sub-domains cover single-grid Cartesian runs without periodic "
-                     "sides, prescribed velocities or plane waves");
+                     "x-slab sub-domains cover single-grid runs without periodic sides, "
+                     "prescribed velocities or plane waves");
   if (c->plast_ready)
     return set_error(AWP_ERR_STATE, "sub-domain before the plasticity inputs");
   if (x0 < 0 || x0 % 2 || nx_global < c->p.nx || x0 + c->p.nx > nx_global)
@@ -1832,6 +1833,7 @@ int decomp_step(awp_decomp* d) {
   if (c[0]->p.nve == 3) {  // the middle band, the stress halo, the yield factors, their
                            // halo, the return
     for (int p = 0; p < d->n; ++p) {
+      if (!stress_split(c[p])) continue;
       int i0, i1, j0, j1;
       middle_band(c[p], &i0, &i1, &j0, &j1);
       if ((st = launch_cart_stress(c[p], i0, i1, j0, j1))) return st;
@@ -2361,7 +2363,6 @@ int awp_set_topo_plasticity(awp_ctx* c, int consistent) {
 
 int awp_topography_init(awp_ctx* c, const char* intopo) {
   if (!c || !intopo) return set_error(AWP_ERR_ARG, "null argument");
-  if (c->sub_nxg) return set_error(AWP_ERR_UNSUPPORTED, "topography on an x-slab sub-domain");
   if (c->topo) return set_error(AWP_ERR_STATE, "topography already initialised");
   if (c->recv || c->srcf || c->forcef || c->sgt)
     return set_error(AWP_ERR_STATE,
@@ -2371,9 +2372,11 @@ int awp_topography_init(awp_ctx* c, const char* intopo) {
     return set_error(AWP_ERR_ARG, "topography belongs to the top grid (grid 0) only");
   const int nx = c->g.nxt, ny = c->g.nyt, nz = c->g.nzt;
   if (nz < 12) return set_error(AWP_ERR_ARG, "topography needs nzt >= 12 (got %d)", nz);
+  // a sub-domain builds the whole grid's metrics and keeps its own planes
+  const int nxg = c->sub_nxg ? c->sub_nxg : nx, x0 = c->sub_nxg ? c->sub_x0 : 0;
   awp::TopoMetrics* m = new awp::TopoMetrics();
-  awp::topo_init_metrics(m, nx, ny, nz, c->p.dh);
-  const int e = awp::topo_read_file(intopo, nx, ny, &m->f);
+  awp::topo_init_metrics(m, nxg, ny, nz, c->p.dh);
+  const int e = awp::topo_read_file(intopo, nxg, ny, &m->f);
   if (e) {
     delete m;
     return set_error(e == 902 ? AWP_ERR_ARG : AWP_ERR_IO,
@@ -2382,6 +2385,23 @@ int awp_topography_init(awp_ctx* c, const char* intopo) {
                      intopo);
   }
   awp::topo_build_metrics(m);
+  if (c->sub_nxg) {
+    awp::TopoMetrics* part = new awp::TopoMetrics();
+    awp::topo_init_metrics(part, nx, ny, nz, c->p.dh);
+    std::vector<float>* dst[10] = {&part->f, &part->f_1, &part->f_2, &part->f_c, &part->f1_1,
+                                   &part->f1_2, &part->f1_c, &part->f2_1, &part->f2_2,
+                                   &part->f2_c};
+    const std::vector<float>* src[10] = {&m->f, &m->f_1, &m->f_2, &m->f_c, &m->f1_1,
+                                         &m->f1_2, &m->f1_c, &m->f2_1, &m->f2_2, &m->f2_c};
+    const size_t row = (size_t)m->ld, rows = (size_t)nx + 4 + AWP_NGSL2;
+    for (int q = 0; q < 10; ++q) {
+      dst[q]->assign(src[q]->begin() + (size_t)x0 * row, src[q]->begin() + (size_t)x0 * row +
+                                                             rows * row);
+    }
+    part->g = m->g; part->g_c = m->g_c; part->g3 = m->g3; part->g3_c = m->g3_c;
+    delete m;
+    m = part;
+  }
   const size_t nf = m->f.size(), ng = m->g.size();
   float* d = nullptr;
   if (ctx_alloc(c, (void**)&d, sizeof(float) * (10 * nf + 4 * ng))) {
@@ -2418,7 +2438,7 @@ int awp_topography_init(awp_ctx* c, const char* intopo) {
   t.dh1 = (float)(1.0 / (double)h);
   // stress window of a rank on every domain boundary: ngsl/2 cells in from
   // each side (topo_set_stress_bounds_*, topography.c:379-420)
-  t.s_i = AWP_NGSL / 2; t.e_i = nx - AWP_NGSL / 2;
+  t.s_i = std::max(AWP_NGSL / 2 - x0, 0); t.e_i = std::min(nxg - AWP_NGSL / 2 - x0, nx);
   t.s_j = AWP_NGSL / 2; t.e_j = ny - AWP_NGSL / 2;
   c->d_topo = d;
   c->topo = m;

@@ -109,6 +109,12 @@ class LocalDecomposition:
             if len(p):
                 s.upload_sources(p, d)
 
+    def topography(self, intopo: str) -> None:
+        """The whole grid's topography file; each part keeps its planes of the
+        metrics."""
+        for s in self.parts:
+            s.topography(intopo)
+
     def upload_plasticity(self, sigma2, cohes, phi, fmajor, fminor, strike, dip) -> None:
         """NVE 3 inputs of the whole padded grid; each part takes its planes."""
         for s, (x0, w) in zip(self.parts, self.layout):

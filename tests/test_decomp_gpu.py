@@ -37,10 +37,12 @@ def plast_args(pl):
         pl["dip"]
 
 
-def whole_run(scn, steps, pl=None):
+def whole_run(scn, steps, pl=None, topo=None):
     s = Solver(default_params(**scn.params))
     s.upload_media(scn.media)
     s.upload_sources(scn.src_pos, scn.src_data)
+    if topo is not None:
+        s.topography(topo)
     if pl is not None:
         s.upload_plasticity(*plast_args(pl))
     s.step(steps)
@@ -101,6 +103,38 @@ def test_lockstep_plastic_parts_equal_whole_grid(nx, nparts):
                 got, w = got[2 + NGSL:-2 - NGSL], want[f][2 + NGSL:-2 - NGSL]
             else:
                 w = want[f]
+            assert np.array_equal(got, w), (f, float(np.abs(got - w).max()))
+
+
+@pytest.mark.parametrize("nx,nparts,plastic", [(32, 2, False), (34, 3, True)])
+def test_lockstep_topography_parts_equal_whole_grid(tmp_path, nx, nparts, plastic):
+    """A curvilinear top grid (Gaussian hill): each part takes its planes of
+    the whole grid's metrics and the stress window of the whole grid."""
+    steps = 16
+    if plastic:
+        scn, pl = plastic_case(nx, 57, steps)
+    else:
+        scn, pl = scenarios.random_small(nx=nx, ny=24, nz=32, q=True, ifault=1, steps=steps,
+                                         seed=59, nsrc=4), None
+    p = scn.params
+    topo = str(tmp_path / "topo.bin")
+    depth = p["dh"] * (p["nz"] - 2)
+    scenarios.write_topography(topo, p["nx"], p["ny"], p["dh"], amplitude=0.15 * depth,
+                               width=5 * p["dh"], rough_rms=0.02 * depth, seed=5)
+    want = whole_run(scn, steps, pl, topo)
+    with LocalDecomposition(default_params(**p), nparts) as d:
+        d.upload_media(scn.media)
+        d.upload_sources(scn.src_pos, scn.src_data)
+        d.topography(topo)
+        if pl is not None:
+            d.upload_plasticity(*plast_args(pl))
+        d.step(steps)
+        d.synchronize()
+        for f in want:
+            got = d.field(f)
+            w = want[f]
+            if f == "yldfac":
+                got, w = got[2 + NGSL:-2 - NGSL], w[2 + NGSL:-2 - NGSL]
             assert np.array_equal(got, w), (f, float(np.abs(got - w).max()))
 
 
