@@ -130,6 +130,7 @@ def load() -> ctypes.CDLL:
     _sig(lib, "awp_decomp_step", c_int, [_P, c_int])
     _sig(lib, "awp_decomp_synchronize", c_int, [_P])
     _sig(lib, "awp_decomp_destroy", c_int, [_P])
+    _sig(lib, "awp_decomp_set_stream", c_int, [_P, c_void_p])
     _sig(lib, "awp_mesh_set_stream", c_int, [_P, _P])
     _sig(lib, "awp_batch_create", c_int, [POINTER(c_void_p), c_int, POINTER(c_void_p)])
     _sig(lib, "awp_batch_destroy", c_int, [_P])

@@ -1467,7 +1467,25 @@ int awp_halo_copy(awp_ctx* c, int unpack, int side, int set, int planes, float* 
     if (!c->f[fid[q]]) return set_error(AWP_ERR_STATE, "field %d not allocated (NVE)", fid[q]);
   const long long plane0 = halo_plane(c, side, unpack != 0, planes);
   const size_t n = (size_t)planes * c->g.slice;
-  for (int q = 0; q < nf; ++q) {
+  cudaPointerAttributes at;
+  const bool dev_buf = cudaPointerGetAttributes(&at, buf) == cudaSuccess &&
+                       at.type == cudaMemoryTypeDevice && !(reinterpret_cast<uintptr_t>(buf) & 15);
+  cudaGetLastError();  // a host pointer may leave a sticky "invalid value" here
+  if (dev_buf) {  // one launch for every field of the set
+    CopySegs cs;
+    cs.nseg = nf;
+    for (int q = 0; q < nf; ++q) {
+      float* field = c->f[fid[q]] + plane0 * c->g.slice;
+      float* b = buf + (size_t)q * n;
+      cs.src[q] = unpack ? b : field;
+      cs.dst[q] = unpack ? field : b;
+      cs.n[q] = (long long)n;
+    }
+    CU_TRY(awp_launch_copy_segments(cs, c->stream));
+    c->launches++;
+    return AWP_OK;
+  }
+  for (int q = 0; q < nf; ++q) {  // host staging: one copy per field
     float* field = c->f[fid[q]] + plane0 * c->g.slice;
     float* b = buf + (size_t)q * n;
     CU_TRY(cudaMemcpyAsync(unpack ? field : b, unpack ? b : field, n * sizeof(float),
@@ -1791,8 +1809,11 @@ struct awp_decomp {
   int n = 0;
   awp_ctx* part[AWP_MAXPARTS] = {};
   int planes = AWP_HALO_PLANES;
-  cudaStream_t stream = nullptr;
+  cudaStream_t stream = nullptr;  // created with the decomposition, destroyed with it
+  cudaStream_t run = nullptr;     // a caller's stream (awp_decomp_set_stream)
+  bool use_run = false;
   bool prepared = false;
+  cudaStream_t active() const { return use_run ? run : stream; }
 };
 
 namespace {
@@ -1801,18 +1822,23 @@ int decomp_exchange(awp_decomp* d, int set) {
   int fid[16];
   const int nf = halo_fields(set, fid);
   const int H = d->planes;
+  // one launch per interface: both directions of every field of the set
   for (int p = 0; p + 1 < d->n; ++p) {
     awp_ctx *L = d->part[p], *R = d->part[p + 1];
-    const size_t n = (size_t)H * L->g.slice;
+    const long long n = (long long)H * L->g.slice;
+    CopySegs cs;
+    cs.nseg = 0;
     for (int q = 0; q < nf; ++q) {
       const int f = fid[q];
-      CU_TRY(cudaMemcpyAsync(R->f[f] + halo_plane(R, 0, true, H) * R->g.slice,
-                             L->f[f] + halo_plane(L, 1, false, H) * L->g.slice,
-                             n * sizeof(float), cudaMemcpyDeviceToDevice, d->stream));
-      CU_TRY(cudaMemcpyAsync(L->f[f] + halo_plane(L, 1, true, H) * L->g.slice,
-                             R->f[f] + halo_plane(R, 0, false, H) * R->g.slice,
-                             n * sizeof(float), cudaMemcpyDeviceToDevice, d->stream));
+      cs.src[cs.nseg] = L->f[f] + halo_plane(L, 1, false, H) * L->g.slice;
+      cs.dst[cs.nseg] = R->f[f] + halo_plane(R, 0, true, H) * R->g.slice;
+      cs.n[cs.nseg++] = n;
+      cs.src[cs.nseg] = R->f[f] + halo_plane(R, 0, false, H) * R->g.slice;
+      cs.dst[cs.nseg] = L->f[f] + halo_plane(L, 1, true, H) * L->g.slice;
+      cs.n[cs.nseg++] = n;
     }
+    CU_TRY(awp_launch_copy_segments(cs, d->active()));
+    L->launches++;
   }
   return AWP_OK;
 }
@@ -1898,6 +1924,7 @@ int awp_decomp_create(awp_ctx** parts, int n, awp_decomp** out) {
 
 int awp_decomp_destroy(awp_decomp* d) {
   if (!d) return AWP_OK;
+  cudaStreamSynchronize(d->active());
   cudaStreamSynchronize(d->stream);
   for (int p = 0; p < d->n; ++p) awp_set_stream(d->part[p], nullptr);
   cudaStreamDestroy(d->stream);
@@ -1923,6 +1950,18 @@ int awp_decomp_step(awp_decomp* d, int nsteps) {
     const int st = decomp_step(d);
     if (st) return st;
   }
+  return AWP_OK;
+}
+
+int awp_decomp_set_stream(awp_decomp* d, void* stream) {
+  if (!d) return set_error(AWP_ERR_ARG, "null decomposition");
+  CU_TRY(cudaStreamSynchronize(d->active()));
+  for (int p = 0; p < d->n; ++p) {
+    const int st = awp_set_stream(d->part[p], stream);
+    if (st) return st;
+  }
+  d->run = static_cast<cudaStream_t>(stream);
+  d->use_run = true;
   return AWP_OK;
 }
 

@@ -15,6 +15,8 @@
 //    switch), so results agree with the reference CUDA build to rounding.
 #include <cuda_runtime.h>
 #include <math.h>
+
+#include <algorithm>
 #include <string.h>
 
 #include "awp_kernels.cuh"
@@ -1110,6 +1112,33 @@ __global__ void k_frcvel(const FrcvelArgs a) {
     a.v1[pos] = __fmaf_rn(a.ayy[a.read_step * n + j], a.DT, a.v1[pos]);
     a.w1[pos] = __fmaf_rn(a.azz[a.read_step * n + j], a.DT, a.w1[pos]);
   }
+}
+
+// Halo planes: whole planes of the padded layout, so every segment is a
+// multiple of 4 floats on 16-byte boundaries; one block row per segment.
+__global__ void k_copy_segments(const CopySegs s) {
+  const int q = blockIdx.y;
+  const float4* __restrict__ src = reinterpret_cast<const float4*>(s.src[q]);
+  float4* __restrict__ dst = reinterpret_cast<float4*>(s.dst[q]);
+  const long long n4 = s.n[q] >> 2;
+  for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < n4;
+       v += (long long)gridDim.x * blockDim.x)
+    dst[v] = src[v];
+}
+
+cudaError_t awp_launch_copy_segments(const CopySegs& s, cudaStream_t st) {
+  if (s.nseg <= 0) return cudaSuccess;
+  if (s.nseg > 32) return cudaErrorInvalidValue;
+  long long mx = 0;
+  for (int q = 0; q < s.nseg; ++q) {
+    if ((s.n[q] & 3) || (reinterpret_cast<uintptr_t>(s.src[q]) & 15) ||
+        (reinterpret_cast<uintptr_t>(s.dst[q]) & 15))
+      return cudaErrorInvalidValue;
+    mx = s.n[q] > mx ? s.n[q] : mx;
+  }
+  const unsigned bx = (unsigned)std::min<long long>(cdiv_u(mx >> 2, 256), 148 * 4 / s.nseg + 1);
+  k_copy_segments<<<dim3(bx, s.nseg), 256, 0, st>>>(s);
+  return cudaGetLastError();
 }
 
 cudaError_t awp_launch_frcvel(const FrcvelArgs& a, cudaStream_t st) {

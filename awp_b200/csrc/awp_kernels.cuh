@@ -181,7 +181,17 @@ struct FrcvelArgs {
   float DT;
 };
 
+// Up to 32 device-to-device copies in one launch (the halo planes of a
+// decomposition): segment q copies n[q] floats, 16-byte aligned, src -> dst.
+struct CopySegs {
+  const float* src[32];
+  float* dst[32];
+  long long n[32];
+  int nseg;
+};
+
 // Launchers (awp_kernels.cu).  All are asynchronous on `st`.
+cudaError_t awp_launch_copy_segments(const CopySegs& s, cudaStream_t st);
 cudaError_t awp_launch_planesrc(const PlaneSrcArgs& a, cudaStream_t st);
 cudaError_t awp_launch_frcvel(const FrcvelArgs& a, cudaStream_t st);
 cudaError_t awp_launch_velocity(const VelArgs& a, cudaStream_t st);

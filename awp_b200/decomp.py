@@ -122,6 +122,11 @@ class LocalDecomposition:
             s.upload_plasticity(*(np.ascontiguousarray(np.asarray(a)[sl])
                                   for a in (sigma2, cohes, phi)), fmajor, fminor, strike, dip)
 
+    def set_stream(self, stream: int | None) -> None:
+        """Run the parts and the halo copies on this cudaStream_t handle."""
+        check(self.lib.awp_decomp_set_stream(self.d, c_void_p(stream or None)),
+              "awp_decomp_set_stream")
+
     def step(self, n: int = 1) -> None:
         check(self.lib.awp_decomp_step(self.d, int(n)), "awp_decomp_step")
 
@@ -198,6 +203,8 @@ class SlabRank:
         """Trade the halo of `hset` with both neighbours (every rank calls
         this at the same points of the step)."""
         n = halo_fields(hset) * self.per_field
+        if n > self.send[0].numel():
+            raise ValueError(f"halo set {hset} exceeds the exchange buffers")
         sides = self._sides()
         for side, _ in sides:
             self.s.halo_copy(False, side, hset, self.planes, self.send[side].data_ptr())

@@ -797,6 +797,87 @@ def run_shots(args, rank, world, dist) -> dict | None:
     }
 
 
+def run_decomp(args, rank, world, dist) -> dict | None:
+    """x-slab domain decomposition of the 512 x 512 x 256 anelastic layered +
+    von Karman run (strong scaling: the grid is fixed).  One process: `--parts`
+    parts on the GPU in lockstep (awp_decomp_*), beside the whole grid on the
+    same GPU, so the line gives the cost of the halo copies.  Under torchrun:
+    one part per rank, halos over NCCL (awp_b200.decomp.SlabRank); the time is
+    the max over ranks."""
+    import torch
+    from awp_b200 import Solver, default_params, scenarios
+    from awp_b200.decomp import (LocalDecomposition, SlabRank, part_media, part_sources,
+                                 split_x)
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+    nx, ny, nz = args.grid if args.grid else (512, 512, 256)
+    scn = scenarios.layered_vk(nx=nx, ny=ny, nz=nz, steps=args.warmup + args.steps + 2)
+    p = scn.params
+    cells = nx * ny * nz
+    stream = torch.cuda.current_stream()
+
+    def timed(step, count):
+        """(max over ranks of the device time of the timed steps, kernels
+        this rank launched in them)."""
+        for _ in range(args.warmup):
+            step()
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        n0 = count()
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        for _ in range(args.steps):
+            step()
+        t1.record(stream)
+        torch.cuda.synchronize()
+        return reduce_max(t0.elapsed_time(t1), dist), count() - n0
+
+    nparts = world if world > 1 else args.parts
+    layout = split_x(nx, nparts)
+    line = {"metric": "Gcell-updates/s (strong scaling of an x-slab decomposition)",
+            "unit": "Gcell-updates/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": True, "scaling": "strong",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "layered_vk_decomp", "grid": [nx, ny, nz], "parts": layout,
+                       "halo_planes": 4,
+                       "l2": "working set ~7 GB >> 126 MB L2, no flush needed"}}
+    if world == 1:
+        whole = Solver(default_params(**p), stream=stream.cuda_stream)
+        whole.upload_media(scn.media)
+        whole.upload_sources(scn.src_pos, scn.src_data)
+        ms_whole, _ = timed(lambda: whole.step(1), lambda: whole.kernel_launches)
+        whole.close()
+        del whole
+        torch.cuda.empty_cache()
+        d = LocalDecomposition(default_params(**p), parts=layout)
+        d.set_stream(stream.cuda_stream)
+        d.upload_media(scn.media)
+        d.upload_sources(scn.src_pos, scn.src_data)
+        ms, launches = timed(lambda: d.step(1),
+                             lambda: sum(s.kernel_launches for s in d.parts))
+        d.close()
+        line["whole_grid_ms_per_step"] = ms_whole / args.steps
+        line["halo_cost_frac"] = ms / ms_whole - 1.0
+    else:
+        x0, w = layout[rank]
+        s = Solver(default_params(**dict(p, nx=w)))
+        s.set_subdomain(nx, x0)
+        s.upload_media(part_media(scn.media, x0, w))
+        ps, ds = part_sources(scn.src_pos, scn.src_data, x0, w, rank == 0, rank == world - 1)
+        if len(ps):
+            s.upload_sources(ps, ds)
+        slab = SlabRank(s, rank, world, group=None)
+        slab.exchange_media()
+        ms, launches = timed(lambda: s.step(1), lambda: s.kernel_launches)
+        s.close()
+    line["value"] = cells * args.steps / (ms * 1e-3) / 1e9
+    line["ms_per_step"] = ms / args.steps
+    line["gpu_launches"] = launches
+    return line if rank == 0 else None
+
+
 def run_config3(args) -> dict:
     """Topography + discontinuous mesh + plasticity + attenuation: a 639 x 639
     x 320 block at h = 40 m (640 is not a multiple of 3) over a 213 x 213 x 96
@@ -938,7 +1019,9 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="layered_vk",
                     choices=["layered_vk", "halfspace", "batched", "adjoint", "config3",
-                             "shots"])
+                             "shots", "decomp"])
+    ap.add_argument("--parts", type=int, default=2,
+                    help="x slabs of --workload decomp on one GPU")
     ap.add_argument("--shots", type=int, default=32,
                     help="shots of the multi-shot gradient (--workload shots)")
     ap.add_argument("--adj-steps", type=int, default=None,
@@ -981,6 +1064,19 @@ def main():
         line = run_adjoint(args) if rank == 0 else None
     elif args.workload == "config3":
         line = run_config3(args) if rank == 0 else None
+    elif args.workload == "decomp":
+        if world > 1:
+            import datetime
+
+            import torch
+            import torch.distributed as dist_mod
+            torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+            dist_mod.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+            dist = dist_mod
+        line = run_decomp(args, rank, world, dist)
+        if dist is not None:
+            dist.barrier()
+            dist.destroy_process_group()
     elif args.workload == "shots":
         if world > 1:
             import datetime

@@ -298,6 +298,8 @@ typedef struct awp_decomp awp_decomp;
 int awp_decomp_create(awp_ctx** parts, int nparts, awp_decomp** out);
 int awp_decomp_step(awp_decomp* d, int nsteps);
 int awp_decomp_synchronize(awp_decomp* d);
+/* Run the parts and the halo copies on this cudaStream_t from now on. */
+int awp_decomp_set_stream(awp_decomp* d, void* cuda_stream);
 int awp_decomp_destroy(awp_decomp* d);
 
 /* ------------------------------------------------------------------------ */
