@@ -108,6 +108,7 @@ struct awp_ctx {
   unsigned int* d_ext = nullptr;  // media extrema (6 float bit patterns)
   int* d_err = nullptr;           // pipeline-wait error word of the TMA kernels
   bool tma_ok = false;            // tensor maps encoded for this context
+  int tma_promo = -1;             // L2 promotion the maps were encoded with
   TmaMaps vel_maps{}, str_maps{};
   long long cur_step = 0;
   bool initial_src_done = false;
@@ -299,6 +300,18 @@ bool build_tma_maps(awp_ctx* c) {
   return bad == 0;
 }
 
+// The maps carry the process-wide L2 promotion of the moment they were
+// encoded; a tuning change re-encodes them before the next TMA launch (host
+// only: the fields and boxes stay the same, so results are unchanged).
+bool tma_ready(awp_ctx* c) {
+  const int promo = awp_tuning_get("l2_promotion");
+  if (c->tma_promo != promo) {
+    c->tma_ok = build_tma_maps(c);
+    c->tma_promo = promo;
+  }
+  return c->tma_ok;
+}
+
 struct PhaseScope {
   awp_ctx* c;
   awp_ctx::PhaseEv ev{};
@@ -395,7 +408,7 @@ int phase_velocity(awp_ctx* c) {
     c->launches++;
     return AWP_OK;
   }
-  const bool tma = c->tma_ok && awp_tuning_get("tma_vel") == 1;
+  const bool tma = awp_tuning_get("tma_vel") == 1 && tma_ready(c);
   PhaseScope ps(c, 0);
   if (tma)
     CU_TRY(awp_launch_velocity_tma(v, c->vel_maps, awp_tuning_get("ichunk"), c->d_err,
@@ -426,7 +439,7 @@ void middle_band(const awp_ctx* c, int* i0, int* i1, int* j0, int* j1) {
 // window, with the kernel family the tuning selects.
 int launch_cart_stress(awp_ctx* c, int i0, int i1, int j0, int j1) {
   if (i1 < i0 || j1 < j0) return AWP_OK;
-  const bool tma = c->tma_ok && awp_tuning_get("tma_str") == 1;
+  const bool tma = awp_tuning_get("tma_str") == 1 && tma_ready(c);
   StrArgs s = make_str_args(c);
   s.i0 = i0; s.i1 = i1; s.j0 = j0; s.j1 = j1;
   if (tma)
@@ -977,6 +990,7 @@ int awp_ctx_create(const awp_params* p, awp_ctx** out) {
     goto fail;
   }
   c->tma_ok = build_tma_maps(c);
+  c->tma_promo = awp_tuning_get("l2_promotion");
   if (cudaStreamSynchronize(c->stream) != cudaSuccess) {
     st = set_error(AWP_ERR_CUDA, "initialisation");
     goto fail;

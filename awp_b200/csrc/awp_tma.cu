@@ -584,8 +584,9 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 
 }  // namespace
 
-// L2 promotion of the tensor maps' fetches (process-wide; read when a
-// context encodes its maps): 0 none, 1 64 B, 2 128 B, 3 256 B.
+// L2 promotion of the tensor maps' fetches (process-wide; a context encodes
+// its maps with the value of the moment and re-encodes them when it changes):
+// 0 none, 1 64 B, 2 128 B, 3 256 B.
 static int g_l2_promotion = 3;
 
 int awp_tma_set_l2_promotion(int mode) {

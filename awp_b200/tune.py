@@ -1,11 +1,13 @@
 """Launch-shape autotuner for the stencil kernels.
 
 Times every candidate (kernel family: TMA-pipelined or read-only path; x
-planes marched per CTA) with the library's own per-phase CUDA events on a live
-context, keeps the fastest per kernel and installs it process-wide through
-awp_set_tuning.  The arithmetic does not depend on the launch shape (every
-cell is computed by exactly one thread with the same expression), so tuning
-never changes results -- tests/test_tuning_gpu.py checks that bit for bit.
+planes marched per CTA; then, for the TMA kernels, the L2 fetch granule of
+their tiles) with the library's own per-phase CUDA events on a live context,
+keeps the fastest per kernel and installs it process-wide through
+awp_set_tuning.  The arithmetic does not depend on the launch shape or on the
+caching (every cell is computed by exactly one thread with the same
+expression), so tuning never changes results -- tests/test_tuning_gpu.py
+checks that bit for bit.
 """
 from __future__ import annotations
 
@@ -13,9 +15,14 @@ import itertools
 
 CANDIDATES = {
     "tma": (1, 0),
-    "ichunk": (16, 32, 64),
+    # longer marches re-read fewer x-halo planes per chunk and keep the CTAs
+    # that share j/k halos closer in time; 512 covers a whole 512-plane grid
+    "ichunk": (16, 32, 64, 128, 256, 512),
 }
-KEYS = ("tma_vel", "tma_str", "ichunk")
+# L2 promotion of the TMA tiles: 3 = 256 B (the library default), 2 = 128 B,
+# 1 = 64 B, 0 = none
+PROMOTIONS = (3, 2, 1, 0)
+KEYS = ("tma_vel", "tma_str", "ichunk", "l2_promotion")
 
 
 def set_tuning(lib, key: str, value: int) -> None:
@@ -58,6 +65,29 @@ def autotune(solver, steps: int = 3) -> dict:
     chosen = {"tma_vel": tv, "tma_str": ts, "ichunk": ich}
     for k, v in chosen.items():
         set_tuning(lib, k, v)
+    promo = lib.awp_get_tuning(b"l2_promotion")
+    if tv == 1 or ts == 1:
+        # the context re-encodes its tensor maps before the next TMA launch
+        solver.profile_phases(True)
+        solver.phase_times()
+        rows = []
+        for pr in PROMOTIONS:
+            set_tuning(lib, "l2_promotion", pr)
+            solver.step(1)  # settle
+            solver.phase_times()
+            solver.step(steps)
+            t = solver.phase_times()
+            rows.append({"l2_promotion": pr, "tma": 1, "ichunk": ich,
+                         "velocity_ms": t["velocity"][0] / max(t["velocity"][1], 1),
+                         "stress_ms": t["stress"][0] / max(t["stress"][1], 1)})
+        solver.profile_phases(False)
+        # only the TMA half-steps depend on it
+        cost = lambda r: (r["velocity_ms"] if tv == 1 else 0.0) + \
+            (r["stress_ms"] if ts == 1 else 0.0)
+        promo = min(rows, key=cost)["l2_promotion"]
+        table.extend(rows)
+    set_tuning(lib, "l2_promotion", promo)
+    chosen["l2_promotion"] = promo
     return {"chosen": chosen, "table": table}
 
 

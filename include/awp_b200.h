@@ -516,8 +516,9 @@ int awp_phase_times(awp_ctx* ctx, double ms[AWP_NPHASES], long long launches[AWP
  * gives up makes the CTA drain its issued copies and leave, and the next
  * awp_synchronize of the context returns AWP_ERR_CUDA once) and
  * "l2_promotion" (0 none, 1 64 B, 2 128 B, 3 256 B (default): the L2 fetch
- * granule of the TMA tiles, applied to contexts created afterwards; results
- * do not change).  Returns AWP_OK or AWP_ERR_ARG;
+ * granule of the TMA tiles; a context re-encodes its tensor maps before its
+ * next TMA launch after a change; results do not change).  Returns AWP_OK or
+ * AWP_ERR_ARG;
  * awp_get_tuning returns the value or -1 for an unknown key. */
 int awp_set_tuning(const char* key, int value);
 int awp_get_tuning(const char* key);
