@@ -325,7 +325,7 @@ def run_ours(args, rank, world, dist) -> dict | None:
     launches0 = s.kernel_launches
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
-    dev_bytes = s.device_bytes()
+    dev_bytes = s.device_bytes
     if dev_bytes < 8 * L2_BYTES:
         # a working set within a few L2 sizes (the 128^3 half-space): write a
         # buffer twice the L2 before each step and time the steps one by one
