@@ -37,7 +37,9 @@ def get_tuning(lib) -> dict:
 def autotune(solver, steps: int = 3) -> dict:
     """Time every (kernel family, ichunk) on `solver` (advancing it), then
     install the fastest family per half-step and the ichunk that minimises
-    their sum.  Returns the choice and the timing table."""
+    their sum; when a TMA family won a half-step, time the L2 promotion
+    granules with that choice and install the fastest.  Returns the choice and
+    the timing table."""
     lib = solver.lib
     table = []
     solver.profile_phases(True)
